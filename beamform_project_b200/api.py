@@ -1,0 +1,368 @@
+"""Python host mirror of the reference's beamformer interface for the hot path.
+
+Names, argument meaning and error behaviour follow the reference's
+include/beamformer headers:
+
+  cuda_stage_api.hpp:21-42   launch_packed_beamformer,
+                             launch_packed_integrated_beamformer,
+                             launch_quantize_integrated_intensity
+  cuda_beamformer.hpp:98-123 cuda_beamform_packed_intensity,
+                             cuda_beamform_packed_integrated_intensity,
+                             cuda_beamform_packed_quantized_integrated_intensity
+  beam_tracker.hpp:60-100    tracker_window_count / tracker_window_direction /
+                             the per-spectrum tracker
+  config.hpp:74-94           Dimensions / validate_dimensions
+  quantization.hpp:16-43     chunk layout
+
+Device-stage functions take torch CUDA tensors and a stream (None = torch's
+current stream) and launch one kernel through the C ABI; they do not
+allocate or synchronise.  Buffer sizes are checked here (the C ABI only sees
+raw pointers), so an undersized tensor is an InvalidArgument, never an
+out-of-bounds access.  Host one-shot functions take numpy arrays and copy in
+and out, like the reference's wrappers.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass
+from enum import IntEnum
+
+import numpy as np
+
+from . import native
+from .native import (BeamformerError, CudaError, DeviceTimeout, InvalidArgument, LogicError,  # noqa: F401
+                     OutOfRange, Unsupported, check)
+
+SPEED_OF_LIGHT = 299_792_458.0
+TWO_PI = 6.283185307179586476925286766559
+LOCAL_FREQUENCY_CHANNELS = 336
+MAXIMUM_BEAMS = 128
+QUANT_CHUNK_FREQ = 16
+QUANT_CHUNK_BEAM = 16
+INTEGRATION_AFTER_UPCHAN = 10
+INTEGRATION_DIRECT = 320
+
+
+class CudaBeamformerKernel(IntEnum):
+    Direct = native.BF_KERNEL_DIRECT
+    Tiled = native.BF_KERNEL_TILED
+    Tensor = native.BF_KERNEL_TENSOR
+
+
+class TrackerMode(IntEnum):
+    ReferenceOrder = 0
+    Streaming = 1
+
+
+@dataclass(frozen=True)
+class Dimensions:
+    n_time: int = 15360
+    n_freq: int = LOCAL_FREQUENCY_CHANNELS
+    n_ant: int = 64
+    n_beams: int = 64
+
+    def c(self) -> native.Dims:
+        return native.dims(self.n_time, self.n_freq, self.n_ant, self.n_beams)
+
+
+def validate_dimensions(dims: Dimensions) -> None:
+    """config.hpp:81-94 (raises InvalidArgument with the reference's text)."""
+    d = dims.c()
+    check(native.lib().bf_validate_dimensions(C.byref(d)))
+
+
+def integrated_time_count(n_time: int, integration_spectra: int) -> int:
+    """temporal_integration.cpp:16-26."""
+    if integration_spectra == 0:
+        raise InvalidArgument(1, "integration_spectra must be positive")
+    if n_time == 0:
+        raise InvalidArgument(1, "n_time must be positive")
+    return -(-n_time // integration_spectra)
+
+
+def quantization_layout(integrated_dims: Dimensions) -> tuple[int, int, int]:
+    """quantization.cpp:34-47: (time_tiles, frequency_tiles, beam_tiles)."""
+    validate_dimensions(integrated_dims)
+    return (integrated_dims.n_time, -(-integrated_dims.n_freq // QUANT_CHUNK_FREQ),
+            -(-integrated_dims.n_beams // QUANT_CHUNK_BEAM))
+
+
+def quantization_parameter_count(integrated_dims: Dimensions) -> int:
+    t, f, b = quantization_layout(integrated_dims)
+    return t * f * b
+
+
+# --------------------------------------------------------------------------
+# device helpers
+# --------------------------------------------------------------------------
+
+def _torch():
+    import torch
+    return torch
+
+
+def _stream_handle(stream) -> int:
+    torch = _torch()
+    if stream is None:
+        return torch.cuda.current_stream().cuda_stream
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+def _dev(t, name: str, dtype, min_elems: int) -> int:
+    torch = _torch()
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise InvalidArgument(1, f"{name} must be a CUDA tensor")
+    if t.dtype != dtype:
+        raise InvalidArgument(1, f"{name} must have dtype {dtype}, got {t.dtype}")
+    if not t.is_contiguous():
+        raise InvalidArgument(1, f"{name} must be contiguous")
+    if t.numel() < min_elems:
+        raise InvalidArgument(1, f"{name} is smaller than dimensions ({t.numel()} < {min_elems})")
+    return t.data_ptr()
+
+
+def _weight_count(kernel: int, d: Dimensions) -> int:
+    if kernel == CudaBeamformerKernel.Tiled:
+        return d.n_freq * (-(-d.n_beams // 32)) * d.n_ant * 32 * 2
+    return d.n_beams * d.n_freq * d.n_ant * 2
+
+
+# --------------------------------------------------------------------------
+# device-stage API (cuda_stage_api.hpp:21-42)
+# --------------------------------------------------------------------------
+
+def launch_packed_beamformer(kernel, stream, packed_voltage, weights, intensity,
+                             dims: Dimensions) -> None:
+    torch = _torch()
+    validate_dimensions(dims)
+    k = int(kernel)
+    v = _dev(packed_voltage, "packed_voltage", torch.uint8, dims.n_time * dims.n_freq * dims.n_ant)
+    w = _dev(weights, "weights", torch.float32, _weight_count(k, dims))
+    o = _dev(intensity, "intensity", torch.float32, dims.n_time * dims.n_freq * dims.n_beams)
+    d = dims.c()
+    check(native.lib().bf_launch_packed_beamformer(k, _stream_handle(stream), v, w, o, C.byref(d)))
+
+
+def launch_packed_integrated_beamformer(kernel, stream, packed_voltage, weights,
+                                        integrated_intensity, dims: Dimensions,
+                                        integration_spectra: int) -> None:
+    torch = _torch()
+    validate_dimensions(dims)
+    k = int(kernel)
+    nw = integrated_time_count(dims.n_time, integration_spectra)
+    v = _dev(packed_voltage, "packed_voltage", torch.uint8, dims.n_time * dims.n_freq * dims.n_ant)
+    w = _dev(weights, "weights", torch.float32, _weight_count(k, dims))
+    o = _dev(integrated_intensity, "integrated_intensity", torch.float32,
+             nw * dims.n_freq * dims.n_beams)
+    d = dims.c()
+    check(native.lib().bf_launch_packed_integrated_beamformer(
+        k, _stream_handle(stream), v, w, o, C.byref(d), int(integration_spectra)))
+
+
+def launch_quantize_integrated_intensity(stream, integrated_intensity, codes, params,
+                                         integrated_dims: Dimensions) -> None:
+    torch = _torch()
+    n = integrated_dims.n_time * integrated_dims.n_freq * integrated_dims.n_beams
+    i = _dev(integrated_intensity, "integrated_intensity", torch.float32, n)
+    c = _dev(codes, "codes", torch.int8, n)
+    p = _dev(params, "params", torch.float32, 2 * quantization_parameter_count(integrated_dims))
+    d = integrated_dims.c()
+    check(native.lib().bf_launch_quantize_integrated_intensity(_stream_handle(stream), i, c, p,
+                                                               C.byref(d)))
+
+
+# --------------------------------------------------------------------------
+# split-precision tensor-core grid
+# --------------------------------------------------------------------------
+
+def split_weight_bytes(dims: Dimensions, n_shards: int = 1) -> int:
+    d = dims.c()
+    return int(native.lib().bf_split_weight_bytes(C.byref(d), int(n_shards)))
+
+
+def prepare_split_weights(stream, weights, split_weights, dims: Dimensions, n_shards: int = 1) -> None:
+    torch = _torch()
+    validate_dimensions(dims)
+    w = _dev(weights, "weights", torch.float32, n_shards * dims.n_beams * dims.n_freq * dims.n_ant * 2)
+    s = _dev(split_weights, "split_weights", torch.uint8, split_weight_bytes(dims, n_shards))
+    d = dims.c()
+    check(native.lib().bf_prepare_split_weights(_stream_handle(stream), w, s, C.byref(d),
+                                                int(n_shards)))
+
+
+def grid_tensor_integrated(stream, packed_voltage, split_weights, integrated, codes, params,
+                           dims: Dimensions, integration_spectra: int, n_shards: int = 1) -> None:
+    torch = _torch()
+    validate_dimensions(dims)
+    nw = integrated_time_count(dims.n_time, integration_spectra)
+    n_out = n_shards * nw * dims.n_freq * dims.n_beams
+    v = _dev(packed_voltage, "packed_voltage", torch.uint8,
+             n_shards * dims.n_time * dims.n_freq * dims.n_ant)
+    s = _dev(split_weights, "split_weights", torch.uint8, split_weight_bytes(dims, n_shards))
+    o = _dev(integrated, "integrated", torch.float32, n_out)
+    c = p = None
+    if codes is not None or params is not None:
+        qd = Dimensions(nw, dims.n_freq, dims.n_ant, dims.n_beams)
+        c = _dev(codes, "codes", torch.int8, n_out)
+        p = _dev(params, "params", torch.float32, 2 * n_shards * quantization_parameter_count(qd))
+    d = dims.c()
+    check(native.lib().bf_grid_tensor_integrated(_stream_handle(stream), v, s, o, c, p,
+                                                 C.byref(d), int(integration_spectra),
+                                                 int(n_shards)))
+
+
+# --------------------------------------------------------------------------
+# tracker
+# --------------------------------------------------------------------------
+
+def tracker(stream, mode, packed_voltage, positions, wave_numbers, window_directions,
+            intensity, integrated, dims: Dimensions, integration_spectra: int) -> None:
+    torch = _torch()
+    validate_dimensions(dims)
+    nw = integrated_time_count(dims.n_time, integration_spectra)
+    v = _dev(packed_voltage, "packed_voltage", torch.uint8, dims.n_time * dims.n_freq * dims.n_ant)
+    pp = _dev(positions, "positions", torch.float32, 3 * dims.n_ant)
+    k = _dev(wave_numbers, "wave_numbers", torch.float64, dims.n_freq)
+    dd = _dev(window_directions, "window_directions", torch.float32, 3 * nw)
+    i = _dev(intensity, "intensity", torch.float32, dims.n_time * dims.n_freq) if intensity is not None else None
+    g = _dev(integrated, "integrated", torch.float32, nw * dims.n_freq) if integrated is not None else None
+    d = dims.c()
+    check(native.lib().bf_tracker(_stream_handle(stream), int(mode), v, pp, k, dd, i, g,
+                                  C.byref(d), int(integration_spectra)))
+
+
+# --------------------------------------------------------------------------
+# synthetic voltages
+# --------------------------------------------------------------------------
+
+def generator_scale(sigma: float) -> float:
+    """float32 multiplier turning the generator's integer draw
+    D = 2 * (sum of eight uniform 16-bit integers) - 8 * 65535, whose variance
+    is 4 * 8 * (65536^2 - 1) / 12, into a value of standard deviation sigma."""
+    std = math.sqrt(4.0 * 8.0 * (65536.0 ** 2 - 1.0) / 12.0)
+    return float(np.float32(sigma / std))
+
+
+def generate_voltage(stream, seed: int, sample_offset: int, sigma: float, mu, epoch_len: int,
+                     out, dims: Dimensions) -> None:
+    torch = _torch()
+    o = _dev(out, "out", torch.uint8, dims.n_time * dims.n_freq * dims.n_ant)
+    m = None
+    if mu is not None:
+        m = _dev(mu, "mu", torch.float32, 2 * dims.n_freq * dims.n_ant)
+    d = dims.c()
+    check(native.lib().bf_generate_voltage(_stream_handle(stream), int(seed), int(sample_offset),
+                                           C.c_float(generator_scale(sigma)), m, int(epoch_len),
+                                           o, C.byref(d)))
+
+
+# --------------------------------------------------------------------------
+# geometry (host; geometry.cpp:34-106, beam_tracker.cpp:44-76)
+# --------------------------------------------------------------------------
+
+def regular_array(rows: int, columns: int, spacing_m: float = 0.6) -> np.ndarray:
+    pos = np.zeros((rows * columns, 3), np.float32)
+    for r in range(rows):
+        for c in range(columns):
+            pos[r * columns + c] = (np.float32(c) * np.float32(spacing_m),
+                                    np.float32(r) * np.float32(spacing_m), 0.0)
+    return pos
+
+
+def default_positions(n_ant: int, spacing_m: float = 0.6) -> np.ndarray:
+    shapes = {32: (4, 8), 64: (8, 8), 128: (8, 16), 256: (16, 16)}
+    if n_ant not in shapes:
+        raise InvalidArgument(1, "default geometry is available only for 32, 64, 128, or 256 antennas")
+    return regular_array(*shapes[n_ant], spacing_m)
+
+
+def channelized_frequencies(n_freq: int = 336, start_hz: float = 300e6,
+                            channel_width_hz: float = 300e3) -> np.ndarray:
+    ch = np.arange(n_freq, dtype=np.float32)
+    return (np.float32(start_hz) + ch * np.float32(channel_width_hz)).astype(np.float32)
+
+
+def direction_from_lm(l: float, m: float) -> np.ndarray:
+    l32, m32 = np.float32(l), np.float32(m)
+    tr = np.float32(l32 * l32) + np.float32(m32 * m32)
+    if not (np.isfinite(l32) and np.isfinite(m32)):
+        raise InvalidArgument(1, "direction cosines l and m must be finite")
+    if tr > np.float32(1.0):
+        raise InvalidArgument(1, "direction cosines must satisfy l*l + m*m <= 1")
+    return np.array([l32, m32, np.sqrt(np.float32(1.0) - tr, dtype=np.float32)], np.float32)
+
+
+def tracker_window_count(n_time: int, integration_spectra: int) -> int:
+    if integration_spectra == 0:
+        raise InvalidArgument(1, "integration_spectra must be positive")
+    return (n_time + integration_spectra - 1) // integration_spectra
+
+
+def tracker_window_directions(l0: float, m0: float, rate_l: float, rate_m: float, n_time: int,
+                              integration_spectra: int) -> np.ndarray:
+    """One direction per window, at the window's first sample (beam_tracker.cpp:52-76)."""
+    W = tracker_window_count(n_time, integration_spectra)
+    out = np.zeros((W, 3), np.float32)
+    for w in range(W):
+        tf = np.float32(w * integration_spectra)
+        l = np.float32(np.float32(l0) + np.float32(tf * np.float32(rate_l)))
+        m = np.float32(np.float32(m0) + np.float32(tf * np.float32(rate_m)))
+        out[w] = direction_from_lm(l, m)
+    return out
+
+
+def wave_numbers(frequencies_hz: np.ndarray) -> np.ndarray:
+    return TWO_PI * frequencies_hz.astype(np.float64) / SPEED_OF_LIGHT
+
+
+# --------------------------------------------------------------------------
+# host one-shot wrappers (cuda_beamformer.hpp:98-123)
+# --------------------------------------------------------------------------
+
+def _to_dev(a: np.ndarray, stream):
+    torch = _torch()
+    t = torch.from_numpy(np.ascontiguousarray(a))
+    return t.pin_memory().to("cuda", non_blocking=True)
+
+
+def cuda_beamform_packed_intensity(packed: np.ndarray, weights: np.ndarray, dims: Dimensions,
+                                   kernel=CudaBeamformerKernel.Direct) -> np.ndarray:
+    torch = _torch()
+    validate_dimensions(dims)
+    v = _to_dev(packed.reshape(-1)[: dims.n_time * dims.n_freq * dims.n_ant], None)
+    w = _to_dev(weights.astype(np.float32).reshape(-1), None)
+    out = torch.empty(dims.n_time * dims.n_freq * dims.n_beams, dtype=torch.float32, device="cuda")
+    launch_packed_beamformer(kernel, None, v, w, out, dims)
+    return out.cpu().numpy()
+
+
+def cuda_beamform_packed_integrated_intensity(packed: np.ndarray, weights: np.ndarray,
+                                              dims: Dimensions, integration_spectra: int,
+                                              kernel=CudaBeamformerKernel.Tiled) -> np.ndarray:
+    torch = _torch()
+    validate_dimensions(dims)
+    nw = integrated_time_count(dims.n_time, integration_spectra)
+    v = _to_dev(packed.reshape(-1)[: dims.n_time * dims.n_freq * dims.n_ant], None)
+    w = _to_dev(weights.astype(np.float32).reshape(-1), None)
+    out = torch.empty(nw * dims.n_freq * dims.n_beams, dtype=torch.float32, device="cuda")
+    launch_packed_integrated_beamformer(kernel, None, v, w, out, dims, integration_spectra)
+    return out.cpu().numpy()
+
+
+def cuda_beamform_packed_quantized_integrated_intensity(
+        packed: np.ndarray, weights: np.ndarray, dims: Dimensions, integration_spectra: int,
+        kernel=CudaBeamformerKernel.Tiled) -> tuple[np.ndarray, np.ndarray]:
+    torch = _torch()
+    nw = integrated_time_count(dims.n_time, integration_spectra)
+    qd = Dimensions(nw, dims.n_freq, dims.n_ant, dims.n_beams)
+    v = _to_dev(packed.reshape(-1)[: dims.n_time * dims.n_freq * dims.n_ant], None)
+    w = _to_dev(weights.astype(np.float32).reshape(-1), None)
+    integ = torch.empty(nw * dims.n_freq * dims.n_beams, dtype=torch.float32, device="cuda")
+    codes = torch.empty_like(integ, dtype=torch.int8)
+    params = torch.empty(2 * quantization_parameter_count(qd), dtype=torch.float32, device="cuda")
+    launch_packed_integrated_beamformer(kernel, None, v, w, integ, dims, integration_spectra)
+    launch_quantize_integrated_intensity(None, integ, codes, params, qd)
+    return codes.cpu().numpy(), params.cpu().numpy().reshape(-1, 2)

@@ -1,0 +1,256 @@
+// capi.cu -- the extern "C" boundary (include/bf_b200.h).
+//
+// Validation and error texts follow the reference so a C++ layer can rethrow
+// the same exception types with the same messages:
+//   validate_dimensions        include/beamformer/config.hpp:81-94
+//   integration checks         src/temporal_integration.cpp:10-26
+//   tracker checks             src/beam_tracker.cpp:29-54
+// Everything here is host code: argument checks, then one kernel launch on
+// the caller's stream.  No allocation, no synchronisation, no exceptions.
+#include "bf_internal.cuh"
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+namespace bf {
+namespace {
+thread_local std::string g_last_error;
+}
+
+bf_status set_error(bf_status code, const std::string& message) {
+    g_last_error = message;
+    return code;
+}
+
+bf_status clear_error() {
+    g_last_error.clear();
+    return BF_OK;
+}
+
+bf_status validate_dims(const bf_dims* dims) {
+    if (dims == nullptr) return set_error(BF_ERR_INVALID_ARGUMENT, "dims must not be null");
+    if (dims->n_time == 0) return set_error(BF_ERR_INVALID_ARGUMENT, "n_time must be positive");
+    if (dims->n_freq != 336) {
+        return set_error(BF_ERR_INVALID_ARGUMENT,
+                         "the local-shard contract requires exactly 336 frequency channels");
+    }
+    const uint64_t a = dims->n_ant;
+    if (a != 32 && a != 64 && a != 128 && a != 256) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "n_ant must be 32, 64, 128, or 256");
+    }
+    if (dims->n_beams == 0 || dims->n_beams > 128) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "n_beams must be between 1 and 128");
+    }
+    return BF_OK;
+}
+
+}  // namespace bf
+
+using namespace bf;
+
+namespace {
+
+bool aligned(const void* p, uintptr_t bytes) {
+    return (reinterpret_cast<uintptr_t>(p) % bytes) == 0;
+}
+
+bf_status check_ptr(const void* p, uintptr_t align, const char* name) {
+    if (p == nullptr) return set_error(BF_ERR_INVALID_ARGUMENT, std::string(name) + " must not be null");
+    if (!aligned(p, align)) {
+        return set_error(BF_ERR_INVALID_ARGUMENT,
+                         std::string(name) + " must be " + std::to_string(align) + "-byte aligned");
+    }
+    return BF_OK;
+}
+
+#define BF_TRY(expr)                  \
+    do {                              \
+        const bf_status _s = (expr);  \
+        if (_s != BF_OK) return _s;   \
+    } while (0)
+
+}  // namespace
+
+extern "C" {
+
+BF_API const char* bf_version(void) { return "beamform_b200 0.1.0 (sm_100a)"; }
+
+BF_API size_t bf_last_error(char* buf, size_t n) {
+    const std::string& e = g_last_error;
+    if (buf != nullptr && n > 0) {
+        const size_t c = e.size() < n - 1 ? e.size() : n - 1;
+        std::memcpy(buf, e.data(), c);
+        buf[c] = '\0';
+    }
+    return e.size();
+}
+
+BF_API bf_status bf_validate_dimensions(const bf_dims* dims) {
+    clear_error();
+    return validate_dims(dims);
+}
+
+BF_API bf_status bf_device_info(char* name_buf, size_t name_len, int* compute_major,
+                                int* compute_minor, uint64_t* global_memory_bytes,
+                                int* driver_version, int* runtime_version) {
+    clear_error();
+    int device = 0;
+    BF_TRY(cuda_status(cudaGetDevice(&device), "cudaGetDevice"));
+    cudaDeviceProp prop{};
+    BF_TRY(cuda_status(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties"));
+    if (name_buf != nullptr && name_len > 0) std::snprintf(name_buf, name_len, "%s", prop.name);
+    if (compute_major) *compute_major = prop.major;
+    if (compute_minor) *compute_minor = prop.minor;
+    if (global_memory_bytes) *global_memory_bytes = prop.totalGlobalMem;
+    if (driver_version) BF_TRY(cuda_status(cudaDriverGetVersion(driver_version), "cudaDriverGetVersion"));
+    if (runtime_version) BF_TRY(cuda_status(cudaRuntimeGetVersion(runtime_version), "cudaRuntimeGetVersion"));
+    return BF_OK;
+}
+
+BF_API bf_status bf_launch_packed_beamformer(int kernel, void* stream,
+                                             const uint8_t* packed_voltage,
+                                             const float* weights, float* intensity,
+                                             const bf_dims* dims) {
+    clear_error();
+    BF_TRY(validate_dims(dims));
+    if (kernel != BF_KERNEL_DIRECT && kernel != BF_KERNEL_TILED) {
+        if (kernel == BF_KERNEL_TENSOR) {
+            return set_error(BF_ERR_UNSUPPORTED,
+                             "the tensor-core kernel produces integrated output only");
+        }
+        return set_error(BF_ERR_INVALID_ARGUMENT, "unknown CUDA beamformer kernel selector");
+    }
+    BF_TRY(check_ptr(packed_voltage, 16, "packed_voltage"));
+    BF_TRY(check_ptr(weights, 8, "weights"));
+    BF_TRY(check_ptr(intensity, 4, "intensity"));
+    return launch_grid_exact(kernel, static_cast<cudaStream_t>(stream), packed_voltage, weights,
+                             intensity, *dims, 1, false);
+}
+
+BF_API bf_status bf_launch_packed_integrated_beamformer(
+    int kernel, void* stream, const uint8_t* packed_voltage, const float* weights,
+    float* integrated_intensity, const bf_dims* dims, uint64_t integration_spectra) {
+    clear_error();
+    BF_TRY(validate_dims(dims));
+    if (integration_spectra == 0) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "integration_spectra must be positive");
+    }
+    if (kernel != BF_KERNEL_DIRECT && kernel != BF_KERNEL_TILED) {
+        if (kernel == BF_KERNEL_TENSOR) {
+            return set_error(BF_ERR_UNSUPPORTED,
+                             "use bf_grid_tensor_integrated with prepared split weights");
+        }
+        return set_error(BF_ERR_INVALID_ARGUMENT, "unknown CUDA beamformer kernel selector");
+    }
+    BF_TRY(check_ptr(packed_voltage, 16, "packed_voltage"));
+    BF_TRY(check_ptr(weights, 8, "weights"));
+    BF_TRY(check_ptr(integrated_intensity, 4, "integrated_intensity"));
+    return launch_grid_exact(kernel, static_cast<cudaStream_t>(stream), packed_voltage, weights,
+                             integrated_intensity, *dims, integration_spectra, true);
+}
+
+BF_API bf_status bf_launch_quantize_integrated_intensity(void* stream,
+                                                         const float* integrated_intensity,
+                                                         int8_t* codes, float* params,
+                                                         const bf_dims* integrated_dims) {
+    clear_error();
+    BF_TRY(validate_dims(integrated_dims));
+    BF_TRY(check_ptr(integrated_intensity, 4, "integrated_intensity"));
+    BF_TRY(check_ptr(codes, 1, "codes"));
+    BF_TRY(check_ptr(params, 8, "params"));
+    return launch_quantize(static_cast<cudaStream_t>(stream), integrated_intensity, codes, params,
+                           *integrated_dims);
+}
+
+BF_API uint64_t bf_split_weight_bytes(const bf_dims* dims, uint64_t n_shards) {
+    if (dims == nullptr) return 0;
+    return split_weight_bytes(*dims, n_shards);
+}
+
+BF_API bf_status bf_prepare_split_weights(void* stream, const float* weights, void* split_weights,
+                                          const bf_dims* dims, uint64_t n_shards) {
+    clear_error();
+    BF_TRY(validate_dims(dims));
+    if (n_shards == 0) return set_error(BF_ERR_INVALID_ARGUMENT, "n_shards must be positive");
+    if (dims->n_ant > 64) {
+        return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernel supports n_ant 32 or 64");
+    }
+    BF_TRY(check_ptr(weights, 8, "weights"));
+    BF_TRY(check_ptr(split_weights, 1024, "split_weights"));
+    return launch_prepare_split(static_cast<cudaStream_t>(stream), weights, split_weights, *dims,
+                                n_shards);
+}
+
+BF_API bf_status bf_grid_tensor_integrated(void* stream, const uint8_t* packed_voltage,
+                                           const void* split_weights, float* integrated,
+                                           int8_t* codes, float* params, const bf_dims* dims,
+                                           uint64_t integration_spectra, uint64_t n_shards) {
+    clear_error();
+    BF_TRY(validate_dims(dims));
+    if (n_shards == 0) return set_error(BF_ERR_INVALID_ARGUMENT, "n_shards must be positive");
+    if (integration_spectra == 0) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "integration_spectra must be positive");
+    }
+    if (integration_spectra % 32 != 0) {
+        return set_error(BF_ERR_UNSUPPORTED,
+                         "the tensor-core kernel needs integration_spectra to be a multiple of 32");
+    }
+    if (dims->n_ant > 64) {
+        return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernel supports n_ant 32 or 64");
+    }
+    if ((codes == nullptr) != (params == nullptr)) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "codes and params must both be given or both be null");
+    }
+    BF_TRY(check_ptr(packed_voltage, 16, "packed_voltage"));
+    BF_TRY(check_ptr(split_weights, 1024, "split_weights"));
+    BF_TRY(check_ptr(integrated, 16, "integrated"));
+    if (codes != nullptr) BF_TRY(check_ptr(params, 8, "params"));
+    return launch_grid_tensor(static_cast<cudaStream_t>(stream), packed_voltage, split_weights,
+                              integrated, codes, params, *dims, integration_spectra, n_shards);
+}
+
+BF_API bf_status bf_tracker(void* stream, int mode, const uint8_t* packed_voltage,
+                            const float* positions, const double* wave_numbers,
+                            const float* window_directions, float* intensity,
+                            float* integrated, const bf_dims* dims,
+                            uint64_t integration_spectra) {
+    clear_error();
+    BF_TRY(validate_dims(dims));
+    if (dims->n_beams != 1) {
+        return set_error(BF_ERR_INVALID_ARGUMENT,
+                         "tracker requires exactly n_beams == 1 (use tracker_beam_count)");
+    }
+    if (integration_spectra == 0) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "tracker integration_spectra must be positive");
+    }
+    if (mode != 0 && mode != 1) return set_error(BF_ERR_INVALID_ARGUMENT, "unknown tracker mode");
+    if (intensity == nullptr && integrated == nullptr) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "intensity and integrated are both null");
+    }
+    BF_TRY(check_ptr(packed_voltage, 16, "packed_voltage"));
+    BF_TRY(check_ptr(positions, 4, "positions"));
+    BF_TRY(check_ptr(wave_numbers, 8, "wave_numbers"));
+    BF_TRY(check_ptr(window_directions, 4, "window_directions"));
+    if (intensity != nullptr) BF_TRY(check_ptr(intensity, 4, "intensity"));
+    if (integrated != nullptr) BF_TRY(check_ptr(integrated, 4, "integrated"));
+    return launch_tracker(static_cast<cudaStream_t>(stream), mode, packed_voltage, positions,
+                          wave_numbers, window_directions, intensity, integrated, *dims,
+                          integration_spectra);
+}
+
+BF_API bf_status bf_generate_voltage(void* stream, uint64_t seed, uint64_t sample_offset,
+                                     float scale, const float* mu, uint64_t epoch_len,
+                                     uint8_t* out, const bf_dims* dims) {
+    clear_error();
+    if (dims == nullptr) return set_error(BF_ERR_INVALID_ARGUMENT, "dims must not be null");
+    if (out == nullptr) return set_error(BF_ERR_INVALID_ARGUMENT, "out must not be null");
+    if (mu != nullptr && epoch_len == 0) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "epoch_len must be positive when mu is given");
+    }
+    if (mu != nullptr) BF_TRY(check_ptr(mu, 8, "mu"));
+    return launch_generate(static_cast<cudaStream_t>(stream), seed, sample_offset, scale, mu,
+                           epoch_len, out, *dims);
+}
+
+}  // extern "C"

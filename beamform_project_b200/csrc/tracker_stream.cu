@@ -1,0 +1,238 @@
+// tracker_stream.cu -- HBM streaming tracker kernel (bf_tracker mode 1).
+//
+// Same product as the reference trackers (src/beam_tracker.cpp:90-146 on the
+// CPU, src/cuda_beam_tracker_v5.cu:137-273 on the GPU): one steering weight
+// set per integration window, per-spectrum power |sum_a w_a x_a|^2 for a
+// single beam, plus (new) the per-window sum.
+//
+// The kernel reads every voltage byte exactly once with 128-bit loads and is
+// meant to run at HBM speed.  At 64 antennas a scalar complex MAC costs about
+// 12 ALU instructions per input byte, which would make the kernel ALU-bound,
+// so the MAC runs on the tensor pipe instead with the voltage fed straight
+// from registers:
+//   * Packed bytes are turned into fp16 pairs with two LOP3s (the nibble is
+//     placed in the mantissa of 1024.0 with its sign bit flipped) and one
+//     half2 subtract / fma -- int4 values are exact in fp16.
+//   * The weights are generated in registers once per window: FP64 delay
+//     and phase, reduced mod 2*pi in FP64, then float sin/cos, and split
+//     into an fp16 hi + lo pair (w = hi + lo to ~2^-22).
+//   * One mma.m16n8k16 (fp16 x fp16 -> fp32) multiplies 16 spectra x 8
+//     antennas by an 8-column weight matrix whose columns are (re, im) x
+//     (hi, lo) of the beam.  The hi and lo partial sums are added in fp32,
+//     then |.|^2.
+//   * Lanes (g, q) of the fragment map to spectra g, g+8 and to the q-th
+//     quarter of the antenna row, so each thread loads its A/4 contiguous
+//     bytes of two rows; the K order of the contraction is permuted to match
+//     the decode (only the weights need to follow it).
+// A CTA of 8 warps takes 8 consecutive channels (512 contiguous bytes per
+// spectrum at 64 antennas) for one window; per-spectrum powers are staged in
+// shared memory so each spectrum's 8 channels are written as one 32-byte
+// sector.
+#include "bf_internal.cuh"
+
+#include <cuda_fp16.h>
+
+namespace bf {
+namespace {
+
+constexpr int kChannelsPerCta = 8;
+
+__device__ __forceinline__ uint32_t lop3_and_xor(uint32_t a, uint32_t b, uint32_t c) {
+    uint32_t r;
+    asm("lop3.b32 %0, %1, %2, %3, 0x6A;" : "=r"(r) : "r"(a), "r"(b), "r"(c));  // (a & b) ^ c
+    return r;
+}
+
+__device__ __forceinline__ uint32_t h2_bits(__half2 h) {
+    return *reinterpret_cast<uint32_t*>(&h);
+}
+__device__ __forceinline__ __half2 bits_h2(uint32_t u) {
+    return *reinterpret_cast<__half2*>(&u);
+}
+
+// Decode one 32-bit word (bytes b0..b3) into four fp16 pairs:
+//   re02 = (re b0, re b2), im02 = (im b0, im b2), re13, im13.
+__device__ __forceinline__ void decode_word(uint32_t w, uint32_t& re02, uint32_t& im02,
+                                            uint32_t& re13, uint32_t& im13) {
+    const __half2 bias_lo = __floats2half2_rn(1032.0f, 1032.0f);
+    const __half2 sixteenth = __floats2half2_rn(0.0625f, 0.0625f);
+    const __half2 bias_hi = __floats2half2_rn(-72.0f, -72.0f);
+    const uint32_t w1 = w >> 8;
+    re02 = h2_bits(__hsub2(bits_h2(lop3_and_xor(w, 0x000F000Fu, 0x64086408u)), bias_lo));
+    im02 = h2_bits(__hfma2(bits_h2(lop3_and_xor(w, 0x00F000F0u, 0x64806480u)), sixteenth, bias_hi));
+    re13 = h2_bits(__hsub2(bits_h2(lop3_and_xor(w1, 0x000F000Fu, 0x64086408u)), bias_lo));
+    im13 = h2_bits(__hfma2(bits_h2(lop3_and_xor(w1, 0x00F000F0u, 0x64806480u)), sixteenth, bias_hi));
+}
+
+__device__ __forceinline__ void mma_16816(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2,
+                                          uint32_t a3, uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+        "{%8,%9}, {%0,%1,%2,%3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// Weight w = exp(i * k * (p . d)): FP64 delay and phase, FP64 reduction of
+// the phase to [-pi, pi], float sin/cos of the reduced argument.
+__device__ __forceinline__ float2 steering_weight(const float* pos, int a, double k, double dx,
+                                                  double dy, double dz) {
+    const double delay = __dadd_rn(__dadd_rn(__dmul_rn((double)pos[3 * a], dx),
+                                             __dmul_rn((double)pos[3 * a + 1], dy)),
+                                   __dmul_rn((double)pos[3 * a + 2], dz));
+    const double phase = k * delay;
+    const double two_pi = 6.283185307179586476925286766559;
+    const double r = phase - two_pi * rint(phase * (1.0 / two_pi));
+    float s, c;
+    sincosf(static_cast<float>(r), &s, &c);
+    return make_float2(c, s);
+}
+
+__device__ __forceinline__ uint16_t split_part(float c, bool lo) {
+    const __half h = __float2half_rn(c);
+    if (!lo) return __half_as_ushort(h);
+    return __half_as_ushort(__float2half_rn(c - __half2float(h)));
+}
+
+template <int A>
+__global__ void __launch_bounds__(kChannelsPerCta * 32)
+tracker_stream_kernel(const uint8_t* __restrict__ v, const float* __restrict__ pos,
+                      const double* __restrict__ kw, const float* __restrict__ dirs,
+                      float* __restrict__ intensity, float* __restrict__ integrated, int n_time,
+                      int n_freq, int spectra) {
+    constexpr int NW = A / 16;          // 32-bit words per thread per spectrum
+    constexpr int kBytes = A / 4;       // bytes per thread per spectrum
+    __shared__ float stage[16][kChannelsPerCta];
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, q = lane & 3;
+    const int win = blockIdx.x;
+    const int f = blockIdx.y * kChannelsPerCta + warp;
+    const bool fvalid = f < n_freq;
+
+    // B fragments for this window: column g in (re_hi, im_hi, re_lo, im_lo, 0...).
+    uint32_t bfrag[NW][2][2];
+    {
+        const bool used = g < 4 && fvalid;
+        const bool is_im = (g & 1) != 0, is_lo = (g >> 1) != 0;
+        const double k = fvalid ? kw[f] : 0.0;
+        const double dx = dirs[3 * win], dy = dirs[3 * win + 1], dz = dirs[3 * win + 2];
+#pragma unroll
+        for (int j = 0; j < NW; ++j) {
+#pragma unroll
+            for (int s = 0; s < 2; ++s) {
+                const int a0 = q * kBytes + 4 * j + s, a1 = a0 + 2;
+                uint32_t xr = 0, xi = 0;
+                if (used) {
+                    const float2 w0 = steering_weight(pos, a0, k, dx, dy, dz);
+                    const float2 w1 = steering_weight(pos, a1, k, dx, dy, dz);
+                    // re: xr*wr - xi*wi ; im: xr*wi + xi*wr
+                    const float cr0 = is_im ? w0.y : w0.x, cr1 = is_im ? w1.y : w1.x;
+                    const float ci0 = is_im ? w0.x : -w0.y, ci1 = is_im ? w1.x : -w1.y;
+                    xr = split_part(cr0, is_lo) | (static_cast<uint32_t>(split_part(cr1, is_lo)) << 16);
+                    xi = split_part(ci0, is_lo) | (static_cast<uint32_t>(split_part(ci1, is_lo)) << 16);
+                }
+                bfrag[j][s][0] = xr;
+                bfrag[j][s][1] = xi;
+            }
+        }
+    }
+
+    const int t_begin = win * spectra;
+    const int t_end = min(t_begin + spectra, n_time);
+    float acc = 0.f;
+    for (int tb = t_begin; tb < t_end; tb += 16) {
+        const int tg = tb + g, tg8 = tb + g + 8;
+        uint32_t wg[NW], wg8[NW];
+        const uint8_t* rg = v + (static_cast<size_t>(tg) * n_freq + f) * A + q * kBytes;
+        const uint8_t* rg8 = v + (static_cast<size_t>(tg8) * n_freq + f) * A + q * kBytes;
+        const bool vg = fvalid && tg < t_end, vg8 = fvalid && tg8 < t_end;
+        if constexpr (A == 32) {
+            const uint2 x0 = vg ? __ldg(reinterpret_cast<const uint2*>(rg)) : make_uint2(0, 0);
+            const uint2 x1 = vg8 ? __ldg(reinterpret_cast<const uint2*>(rg8)) : make_uint2(0, 0);
+            wg[0] = x0.x; wg[1] = x0.y; wg8[0] = x1.x; wg8[1] = x1.y;
+        } else {
+#pragma unroll
+            for (int c = 0; c < NW / 4; ++c) {
+                const uint4 x0 = vg ? __ldg(reinterpret_cast<const uint4*>(rg) + c) : make_uint4(0, 0, 0, 0);
+                const uint4 x1 = vg8 ? __ldg(reinterpret_cast<const uint4*>(rg8) + c) : make_uint4(0, 0, 0, 0);
+                wg[4 * c] = x0.x; wg[4 * c + 1] = x0.y; wg[4 * c + 2] = x0.z; wg[4 * c + 3] = x0.w;
+                wg8[4 * c] = x1.x; wg8[4 * c + 1] = x1.y; wg8[4 * c + 2] = x1.z; wg8[4 * c + 3] = x1.w;
+            }
+        }
+        float d[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+        for (int j = 0; j < NW; ++j) {
+            uint32_t re02g, im02g, re13g, im13g, re02h, im02h, re13h, im13h;
+            decode_word(wg[j], re02g, im02g, re13g, im13g);
+            decode_word(wg8[j], re02h, im02h, re13h, im13h);
+            mma_16816(d, re02g, re02h, im02g, im02h, bfrag[j][0][0], bfrag[j][0][1]);
+            mma_16816(d, re13g, re13h, im13g, im13h, bfrag[j][1][0], bfrag[j][1][1]);
+        }
+        // q == 0 holds (re_hi, im_hi), q == 1 holds (re_lo, im_lo) for rows g, g+8.
+        float p[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) p[i] = __shfl_xor_sync(0xffffffffu, d[i], 1);
+        const float re_g = d[0] + p[0], im_g = d[1] + p[1];
+        const float re_h = d[2] + p[2], im_h = d[3] + p[3];
+        const float pow_g = re_g * re_g + im_g * im_g;
+        const float pow_h = re_h * re_h + im_h * im_h;
+        if (q == 0) acc += pow_g + pow_h;
+        if (intensity != nullptr) {
+            if (q == 0) {
+                stage[g][warp] = pow_g;
+                stage[g + 8][warp] = pow_h;
+            }
+            __syncthreads();
+            if (threadIdx.x < 16 * kChannelsPerCta) {
+                const int r = threadIdx.x / kChannelsPerCta, c = threadIdx.x % kChannelsPerCta;
+                const int fo = blockIdx.y * kChannelsPerCta + c;
+                if (tb + r < t_end && fo < n_freq) {
+                    intensity[static_cast<size_t>(tb + r) * n_freq + fo] = stage[r][c];
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if (integrated != nullptr) {
+        acc += __shfl_xor_sync(0xffffffffu, acc, 4);
+        acc += __shfl_xor_sync(0xffffffffu, acc, 8);
+        acc += __shfl_xor_sync(0xffffffffu, acc, 16);
+        if (lane == 0 && fvalid) integrated[static_cast<size_t>(win) * n_freq + f] = acc;
+    }
+}
+
+}  // namespace
+
+bf_status launch_tracker_stream(cudaStream_t stream, const uint8_t* v, const float* pos,
+                                const double* k, const float* dirs, float* intensity,
+                                float* integrated, const bf_dims& d, uint64_t spectra) {
+    const uint64_t W = window_count(d.n_time, spectra);
+    if (W > 0x7fffffffull || d.n_time > 0x7fffffffull) {
+        return set_error(BF_ERR_OVERFLOW, "CUDA tracker grid exceeds the supported size");
+    }
+    const dim3 grid(static_cast<unsigned>(W),
+                    static_cast<unsigned>((d.n_freq + kChannelsPerCta - 1) / kChannelsPerCta));
+    const dim3 block(kChannelsPerCta * 32);
+    const int T = static_cast<int>(d.n_time), F = static_cast<int>(d.n_freq);
+    const int S = static_cast<int>(spectra);
+    switch (d.n_ant) {
+        case 32:
+            tracker_stream_kernel<32><<<grid, block, 0, stream>>>(v, pos, k, dirs, intensity, integrated, T, F, S);
+            break;
+        case 64:
+            tracker_stream_kernel<64><<<grid, block, 0, stream>>>(v, pos, k, dirs, intensity, integrated, T, F, S);
+            break;
+        case 128:
+            tracker_stream_kernel<128><<<grid, block, 0, stream>>>(v, pos, k, dirs, intensity, integrated, T, F, S);
+            break;
+        case 256:
+            tracker_stream_kernel<256><<<grid, block, 0, stream>>>(v, pos, k, dirs, intensity, integrated, T, F, S);
+            break;
+        default:
+            return set_error(BF_ERR_INVALID_ARGUMENT, "n_ant must be 32, 64, 128, or 256");
+    }
+    return cuda_status(cudaGetLastError(), "tracker_stream_kernel launch");
+}
+
+}  // namespace bf

@@ -1,0 +1,117 @@
+"""ctypes binding of the C ABI in include/bf_b200.h.
+
+The library is built in-tree (python -m beamform_project_b200.build).  There
+is no fallback: if the shared object is missing or cannot be loaded, every
+call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+_LIB_PATH = Path(__file__).resolve().parent / "lib" / "libbf_b200.so"
+_lib = None
+
+BF_OK = 0
+BF_KERNEL_DIRECT, BF_KERNEL_TILED, BF_KERNEL_TENSOR = 0, 1, 2
+
+
+class BeamformerError(RuntimeError):
+    """Base class; `status` holds the bf_status code."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(message)
+        self.status = status
+
+
+class InvalidArgument(BeamformerError, ValueError):
+    """std::invalid_argument in the reference."""
+
+
+class LogicError(BeamformerError):
+    """std::logic_error in the reference."""
+
+
+class CudaError(BeamformerError):
+    """std::runtime_error (CUDA failure) in the reference."""
+
+
+class OverflowError_(BeamformerError, OverflowError):
+    """std::overflow_error in the reference."""
+
+
+class OutOfRange(BeamformerError, IndexError):
+    """std::out_of_range in the reference."""
+
+
+class DeviceTimeout(BeamformerError):
+    """A bounded device wait ran out."""
+
+
+class Unsupported(BeamformerError):
+    """A valid request outside this build's kernels."""
+
+
+_ERRORS = {1: InvalidArgument, 2: LogicError, 3: CudaError, 4: OverflowError_, 5: OutOfRange,
+           6: DeviceTimeout, 7: Unsupported}
+
+
+class Dims(C.Structure):
+    _fields_ = [("n_time", C.c_uint64), ("n_freq", C.c_uint64), ("n_ant", C.c_uint64),
+                ("n_beams", C.c_uint64)]
+
+
+_P = C.c_void_p
+_U64 = C.c_uint64
+_SIGS = {
+    "bf_version": (C.c_char_p, []),
+    "bf_last_error": (C.c_size_t, [C.c_char_p, C.c_size_t]),
+    "bf_validate_dimensions": (C.c_int, [C.POINTER(Dims)]),
+    "bf_device_info": (C.c_int, [C.c_char_p, C.c_size_t, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                 C.POINTER(C.c_uint64), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "bf_launch_packed_beamformer": (C.c_int, [C.c_int, _P, _P, _P, _P, C.POINTER(Dims)]),
+    "bf_launch_packed_integrated_beamformer": (C.c_int, [C.c_int, _P, _P, _P, _P, C.POINTER(Dims), _U64]),
+    "bf_launch_quantize_integrated_intensity": (C.c_int, [_P, _P, _P, _P, C.POINTER(Dims)]),
+    "bf_split_weight_bytes": (_U64, [C.POINTER(Dims), _U64]),
+    "bf_prepare_split_weights": (C.c_int, [_P, _P, _P, C.POINTER(Dims), _U64]),
+    "bf_grid_tensor_integrated": (C.c_int, [_P, _P, _P, _P, _P, _P, C.POINTER(Dims), _U64, _U64]),
+    "bf_tracker": (C.c_int, [_P, C.c_int, _P, _P, _P, _P, _P, _P, C.POINTER(Dims), _U64]),
+    "bf_generate_voltage": (C.c_int, [_P, _U64, _U64, C.c_float, _P, _U64, _P, C.POINTER(Dims)]),
+}
+
+
+def lib() -> C.CDLL:
+    """Load the product library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not _LIB_PATH.exists():
+            raise ImportError(f"{_LIB_PATH} is missing: run python -m beamform_project_b200.build")
+        handle = C.CDLL(str(_LIB_PATH), mode=os.RTLD_NOW | C.RTLD_GLOBAL)
+        for name, (res, args) in _SIGS.items():
+            if hasattr(handle, name):
+                fn = getattr(handle, name)
+                fn.restype = res
+                fn.argtypes = args
+        _lib = handle
+    return _lib
+
+
+def library_path() -> Path:
+    return _LIB_PATH
+
+
+def last_error() -> str:
+    buf = C.create_string_buffer(1024)
+    lib().bf_last_error(buf, len(buf))
+    return buf.value.decode(errors="replace")
+
+
+def check(status: int) -> None:
+    if status != BF_OK:
+        cls = _ERRORS.get(status, BeamformerError)
+        raise cls(status, last_error() or f"bf_status {status}")
+
+
+def dims(n_time: int, n_freq: int, n_ant: int, n_beams: int) -> Dims:
+    return Dims(int(n_time), int(n_freq), int(n_ant), int(n_beams))

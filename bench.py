@@ -1,0 +1,445 @@
+#!/usr/bin/env python3
+"""Benchmark of the fixed-grid beamformer hot path on B200.
+
+Workload (the full-band split-precision grid): 64 antennas on a 2 x 32 grid
+at 0.5 wavelength spacing for 800 MHz; 672 channels over 400-800 MHz (end
+points inclusive) as two shards of 336; T = 32768 spectra; 128 beams on a
+16 x 8 direction-cosine grid; voltages complex int4 with Gaussian-like noise
+sigma = 2.5 plus a point source at per-sample SNR 5 in a seeded on-grid
+direction, generated on the device; weights complex64 (FP64 phase); output
+float32 integrated over 320 spectra plus int8 chunk quantization.
+
+One step = beamform + |.|^2 + integrate + quantize both shards.
+Metric: beam-samples/s = T * F * B / step time.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--kernel tensor|tiled]
+    python bench.py --impl reference ...   # the reference CPU implementation
+
+Under torchrun (N > 1) every rank runs its own independent copy of the
+workload (channel shards are independent; no collective on the data path):
+weak scaling, value = all ranks' beam-samples / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import sys
+import threading
+import time
+from concurrent.futures import ThreadPoolExecutor
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+C_LIGHT = 299_792_458.0
+T_SPECTRA = 32768
+N_SHARDS = 2
+F_SHARD = 336
+N_ANT = 64
+N_BEAMS = 128
+S_INT = 320
+SIGMA = 2.5
+SNR = 5.0
+SEED = 0
+METRIC = "beam-samples/s (T*F*B)"
+
+
+# --------------------------------------------------------------------------
+# workload definition (host side, FP64)
+# --------------------------------------------------------------------------
+
+def workload_geometry():
+    lam = C_LIGHT / 800e6
+    spacing = 0.5 * lam
+    pos = np.zeros((N_ANT, 3), np.float32)
+    for r in range(2):
+        for c in range(32):
+            pos[r * 32 + c] = (c * spacing, r * spacing, 0.0)
+    F = N_SHARDS * F_SHARD
+    freq = (400e6 + np.arange(F) * (400e6 / (F - 1))).astype(np.float32)
+    ls = -0.45 + 0.06 * np.arange(16)
+    ms = -0.21 + 0.06 * np.arange(8)
+    dirs = np.zeros((N_BEAMS, 3), np.float32)
+    for j in range(8):
+        for i in range(16):
+            l, m = np.float32(ls[i]), np.float32(ms[j])
+            dirs[j * 16 + i] = (l, m, np.sqrt(np.float32(1) - (l * l + m * m)))
+    return pos, freq, dirs
+
+
+def steering_phase(pos, freq, dirs):
+    """phase[b][f][a] = 2*pi*f/c * (p_a . d_b) in FP64 (src/weights.cpp:42-55)."""
+    k = 2.0 * math.pi * freq.astype(np.float64) / C_LIGHT
+    delay = dirs.astype(np.float64) @ pos.astype(np.float64).T  # [B][A]
+    return k[None, :, None] * delay[:, None, :]
+
+
+def workload_weights(pos, freq, dirs):
+    ph = steering_phase(pos, freq, dirs)                          # [B][F][A]
+    w = np.stack([np.cos(ph), np.sin(ph)], -1).astype(np.float32)  # [B][F][A][2]
+    # per shard: [shard][B][336][A][2]
+    return np.ascontiguousarray(np.stack([w[:, s * F_SHARD:(s + 1) * F_SHARD] for s in range(N_SHARDS)]))
+
+
+def workload_source(pos, freq, dirs):
+    """mu = A_s * exp(-i phase) of a point source at a seeded on-grid beam."""
+    beam = int(np.random.default_rng(SEED).integers(0, N_BEAMS))
+    amp = SIGMA * math.sqrt(SNR)
+    ph = steering_phase(pos, freq, dirs[beam:beam + 1])[0]          # [F][A]
+    mu = np.stack([amp * np.cos(ph), -amp * np.sin(ph)], -1).astype(np.float32)
+    return beam, [np.ascontiguousarray(mu[s * F_SHARD:(s + 1) * F_SHARD]) for s in range(N_SHARDS)]
+
+
+# --------------------------------------------------------------------------
+# clocks sampled during the timed region (NVML)
+# --------------------------------------------------------------------------
+
+class ClockSampler:
+    REASONS = {
+        0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap",
+        0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+        0x80: "hw_power_brake_slowdown",
+    }
+
+    def __init__(self, device_index: int):
+        self.samples: list[int] = []
+        self.reasons: set[str] = set()
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._ok = False
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self._nv = pynvml
+            self._h = pynvml.nvmlDeviceGetHandleByIndex(device_index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self._h, pynvml.NVML_CLOCK_SM)
+            self._ok = True
+        except Exception:
+            pass
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                self.samples.append(self._nv.nvmlDeviceGetClockInfo(self._h, self._nv.NVML_CLOCK_SM))
+                r = self._nv.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+                for bit, name in self.REASONS.items():
+                    if r & bit and name != "gpu_idle":
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            self._stop.wait(0.05)
+
+    def __enter__(self):
+        if self._ok:
+            self._t = threading.Thread(target=self._run, daemon=True)
+            self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self._ok:
+            self._t.join()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons),
+                    "samples": 0}
+        return {"sm_mhz": statistics.median(self.samples), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(self.reasons), "samples": len(self.samples)}
+
+
+def measured_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get("bf16_tflops_sustained") or d.get("bf16_tflops"), d.get("hbm_gbs"), "measured"
+    return 1400.0, 6650.0, "fallback"
+
+
+# --------------------------------------------------------------------------
+# CPU baseline (reference CPU core, or the oracle port when it is absent)
+# --------------------------------------------------------------------------
+
+def cpu_baseline(v_host_shard0: np.ndarray, w_shard0: np.ndarray, budget_s: float = 12.0,
+                 threads: int | None = None):
+    """Time the reference CPU chain (cpu_beamform_packed_intensity_into ->
+    cpu_integrate_intensity_into -> cpu_quantize_integrated_intensity) on
+    whole 320-spectrum windows of shard 0, one window per host thread, in
+    rounds until about budget_s of wall time.  The reference function is
+    serial; the harness runs independent windows on separate threads."""
+    from oracle import loader as orc
+    kind = "reference" if orc.reference_available() else "port"
+    threads = threads or os.cpu_count() or 1
+    F, A, B = F_SHARD, N_ANT, N_BEAMS
+    W_total = len(v_host_shard0) // S_INT
+
+    def one_window(widx: int):
+        t0 = widx * S_INT
+        v = np.ascontiguousarray(v_host_shard0[t0:t0 + S_INT])
+        if kind == "reference":
+            I = orc.ref_beamform(v, w_shard0, S_INT, F, A, B)
+            integ = orc.ref_integrate(I, S_INT, F, A, B, S_INT)
+            orc.ref_quantize(integ, 1, F, A, B)
+        else:
+            integ = orc.beamform_integrated(v, w_shard0, S_INT, F, A, B, S_INT)
+            orc.quantize(integ, 1, F, B)
+
+    done = 0
+    t_start = time.perf_counter()
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        while True:
+            list(ex.map(one_window, [(done + i) % W_total for i in range(threads)]))
+            done += threads
+            if time.perf_counter() - t_start > budget_s:
+                break
+    el = time.perf_counter() - t_start
+    value = done * S_INT * F * B / el
+    return {"value": value, "unit": "beam-samples/s", "cores": threads, "kind": kind,
+            "sample": f"{done} whole windows of {S_INT} spectra x {F} channels x {B} beams x {A} "
+                      f"antennas (shard 0, one window per thread, {threads} threads), "
+                      f"beamform+integrate+quantize, {el:.1f} s"}
+
+
+# --------------------------------------------------------------------------
+# GPU arm
+# --------------------------------------------------------------------------
+
+def run_gpu(args):
+    import torch
+    from beamform_project_b200 import api, native
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+
+    pos, freq, dirs = workload_geometry()
+    w_host = workload_weights(pos, freq, dirs)
+    beam, mu_host = workload_source(pos, freq, dirs)
+    d = api.Dimensions(T_SPECTRA, F_SHARD, N_ANT, N_BEAMS)
+    W = api.integrated_time_count(T_SPECTRA, S_INT)
+    qd = api.Dimensions(W, F_SHARD, N_ANT, N_BEAMS)
+    n_out = W * F_SHARD * N_BEAMS
+    n_par = 2 * api.quantization_parameter_count(qd)
+
+    volt = torch.empty(N_SHARDS * T_SPECTRA * F_SHARD * N_ANT, dtype=torch.uint8, device=dev)
+    shard_bytes = T_SPECTRA * F_SHARD * N_ANT
+    for s in range(N_SHARDS):
+        api.generate_voltage(None, SEED + 1000 * rank, s * shard_bytes, SIGMA,
+                             torch.from_numpy(mu_host[s]).to(dev), T_SPECTRA,
+                             volt[s * shard_bytes:(s + 1) * shard_bytes], d)
+    weights = torch.from_numpy(w_host).to(dev)
+    integ = torch.empty(N_SHARDS * n_out, dtype=torch.float32, device=dev)
+    codes = torch.empty(N_SHARDS * n_out, dtype=torch.int8, device=dev)
+    params = torch.empty(N_SHARDS * n_par, dtype=torch.float32, device=dev)
+    kernel = args.kernel
+    split = None
+    if kernel == "tensor":
+        split = torch.empty(api.split_weight_bytes(d, N_SHARDS), dtype=torch.uint8, device=dev)
+        api.prepare_split_weights(None, weights, split, d, N_SHARDS)
+    torch.cuda.synchronize()
+
+    main_events = []
+
+    def step(record=False):
+        if record:
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+        if kernel == "tensor":
+            api.grid_tensor_integrated(None, volt, split, integ, codes, params, d, S_INT, N_SHARDS)
+            launches = 1
+        else:
+            launches = 0
+            for s in range(N_SHARDS):
+                api.launch_packed_integrated_beamformer(
+                    api.CudaBeamformerKernel.Direct, None, volt[s * shard_bytes:],
+                    weights[s], integ[s * n_out:], d, S_INT)
+                launches += 1
+            for s in range(N_SHARDS):
+                api.launch_quantize_integrated_intensity(None, integ[s * n_out:], codes[s * n_out:],
+                                                         params[s * n_par:], qd)
+                launches += 1
+        if record:
+            e1.record(stream)
+            main_events.append((e0, e1))
+        return launches
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    launches = 0
+    with ClockSampler(local) as clocks:
+        t0.record(stream)
+        for _ in range(args.steps):
+            launches += step(record=True)
+        t1.record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = t0.elapsed_time(t1)
+    main_ms = statistics.mean(a.elapsed_time(b) for a, b in main_events)
+    if dist:
+        tt = torch.tensor([ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    ms_per_step = ms / args.steps
+    samples_per_step = T_SPECTRA * N_SHARDS * F_SHARD * N_BEAMS
+    value = samples_per_step * world / (ms_per_step / 1e3)
+
+    # end to end through the public API: pinned host voltage in, results out
+    host_v = torch.empty(volt.numel(), dtype=torch.uint8, pin_memory=True)
+    host_v.copy_(volt)
+    host_i = torch.empty(integ.numel(), dtype=torch.float32, pin_memory=True)
+    host_c = torch.empty(codes.numel(), dtype=torch.int8, pin_memory=True)
+    host_p = torch.empty(params.numel(), dtype=torch.float32, pin_memory=True)
+    e2e_steps = max(1, min(args.steps, 5))
+
+    def e2e_step():
+        volt.copy_(host_v, non_blocking=True)
+        step()
+        host_i.copy_(integ, non_blocking=True)
+        host_c.copy_(codes, non_blocking=True)
+        host_p.copy_(params, non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    a0 = torch.cuda.Event(enable_timing=True)
+    a1 = torch.cuda.Event(enable_timing=True)
+    a0.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    a1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = a0.elapsed_time(a1) / e2e_steps
+    if dist:
+        tt = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_ms = float(tt.item())
+    e2e_value = samples_per_step * world / (e2e_ms / 1e3)
+
+    # sanity: the injected source beam is the brightest beam of the band
+    prof = integ.view(N_SHARDS, W, F_SHARD, N_BEAMS).double().sum(dim=(0, 1, 2))
+    peak_ok = int(torch.argmax(prof).item()) == beam
+
+    peak_tflops, hbm_gbs, peak_src = measured_peaks()
+    cmac = T_SPECTRA * N_SHARDS * F_SHARD * N_ANT * N_BEAMS
+    alg_flops = 8 * cmac + 3 * samples_per_step
+    achieved = alg_flops / (main_ms / 1e3) / 1e12
+    roofline = {"bound": "tensor", "achieved": round(achieved, 2), "peak": peak_tflops,
+                "unit": "TFLOP/s", "frac": round(achieved / peak_tflops, 4),
+                "traffic": None, "peak_source": peak_src + " (bf16 dense, sustained)",
+                "kernel": "grid_tensor_kernel" if kernel == "tensor" else "grid_exact_kernel+quantize",
+                "kernel_ms": round(main_ms, 4),
+                "algorithmic_flop_per_launch": alg_flops}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "beam-samples/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int4xfp16->fp32",
+        "data": "synthetic (seeded on-device int4 generator, point source at beam %d)" % beam,
+        "config": {"workload": "full-band split-precision grid: A=64 (2x32), F=672 (2 shards x 336), "
+                               "T=32768, B=128 (16x8), S=320, float32 + int8 chunk codes",
+                   "kernel": kernel, "parallelism": f"independent replicas x{world}",
+                   "l2": "inputs (1.41 GB voltage) exceed L2; no flush"},
+        "roofline": roofline,
+        "e2e": {"value": e2e_value, "unit": "beam-samples/s",
+                "h2d_bytes_per_step": host_v.numel(),
+                "d2h_bytes_per_step": host_i.numel() * 4 + host_c.numel() + host_p.numel() * 4,
+                "ms_per_step": e2e_ms},
+        "gpu_launches": launches,
+        "clocks": clocks.summary(),
+        "source_peak_ok": peak_ok,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v0 = volt[:shard_bytes].cpu().numpy().reshape(T_SPECTRA, F_SHARD, N_ANT)
+        line["cpu_baseline"] = cpu_baseline(v0, w_host[0], budget_s=args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def run_reference(args):
+    """The reference's own CPU implementation on the host cores, same metric."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    pos, freq, dirs = workload_geometry()
+    w_host = workload_weights(pos, freq, dirs)
+    beam, mu_host = workload_source(pos, freq, dirs)
+    from oracle import loader as orc
+    from beamform_project_b200.api import generator_scale
+    # a bounded slice of the same seeded voltages (the oracle generator is
+    # byte-identical to the device generator): one window per host thread
+    threads = os.cpu_count() or 1
+    n_win = min(threads, T_SPECTRA // S_INT)
+    v0 = orc.generate_voltage(SEED, 0, n_win * S_INT, F_SHARD, N_ANT, generator_scale(SIGMA),
+                              mu_host[0][None], T_SPECTRA)
+    vfull = np.zeros((T_SPECTRA, F_SHARD, N_ANT), np.uint8)
+    vfull[:n_win * S_INT] = v0
+    times = []
+    base = None
+    for i in range(args.warmup + args.steps):
+        t = time.perf_counter()
+        base = cpu_baseline(vfull[:n_win * S_INT], w_host[0], budget_s=0.0, threads=threads)
+        if i >= args.warmup:
+            times.append(time.perf_counter() - t)
+    value = base["value"]
+    per_step_samples = n_win * S_INT * F_SHARD * N_BEAMS
+    value = per_step_samples / statistics.mean(times)
+    base["value"] = value
+    line = {"metric": METRIC, "value": value, "unit": "beam-samples/s", "n_gpus": 0,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": statistics.mean(times) * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "impl": "reference",
+            "data": "synthetic (same seeded voltages, first windows of shard 0)",
+            "config": {"workload": "full-band split-precision grid: A=64 (2x32), F=672 (2 shards x 336), "
+                                   "T=32768, B=128 (16x8), S=320, float32 + int8 chunk codes",
+                       "sample": f"{n_win} windows x 320 spectra of shard 0 per step"},
+            "cpu_baseline": base,
+            "e2e": {"value": value, "unit": "beam-samples/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--kernel", default="tensor", choices=["tensor", "tiled"])
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

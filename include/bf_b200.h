@@ -1,0 +1,182 @@
+/*
+ * bf_b200.h -- C ABI of the B200 (sm_100a) voltage-beamformer hot path.
+ *
+ * Plain pointers, sizes and a CUDA stream passed as `void*`: no C++ or torch
+ * types cross this boundary, so any FFI (ctypes, cgo, JNI, N-API) can bind it.
+ * The C++ API in include/beamformer/ (same names and exception types as the
+ * reference's include/beamformer) is a thin layer over these calls.
+ *
+ * Conventions
+ *  - Every call returns bf_status; BF_OK == 0.  On failure the message is kept
+ *    per host thread and read with bf_last_error().  Nothing throws.
+ *  - Device-stage calls ("bf_launch_*", "bf_grid_*", "bf_tracker*",
+ *    "bf_doa_*") take device pointers and a stream, are stream-ordered,
+ *    allocate no memory, take no lock and never synchronise the stream.
+ *    Launch errors are reported as BF_ERR_CUDA; errors raised while the
+ *    kernel runs surface at the caller's next synchronisation.
+ *  - Layouts (little endian, row-major):
+ *      voltage      u8  [T][F][A]  packed complex int4: low nibble = real,
+ *                                  high nibble = imaginary, two's complement
+ *      weights      f32 [B][F][A][2]           canonical (re, im)
+ *      tiled weights f32 [F][ceil(B/32)][A][32][2]  (zero-padded last tile)
+ *      intensity    f32 [T][F][B]
+ *      integrated   f32 [W][F][B], W = ceil(T / S)
+ *      codes        i8  [W][F][B]
+ *      params       f32 [W][ceil(F/16)][ceil(B/16)][2]  (offset, scale)
+ *    Calls that take n_shards process that many independent frequency
+ *    shards stored back to back ([shard][...] for every array).
+ */
+#ifndef BF_B200_H
+#define BF_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define BF_API __declspec(dllexport)
+#else
+#define BF_API __attribute__((visibility("default")))
+#endif
+
+/* Status codes.  The C++ layer maps them back onto the reference's exception
+ * types (src/cuda_beamformer.cu:22-27, include/beamformer/config.hpp:43-94). */
+typedef enum bf_status {
+    BF_OK = 0,
+    BF_ERR_INVALID_ARGUMENT = 1, /* std::invalid_argument */
+    BF_ERR_LOGIC = 2,            /* std::logic_error      */
+    BF_ERR_CUDA = 3,             /* std::runtime_error    */
+    BF_ERR_OVERFLOW = 4,         /* std::overflow_error   */
+    BF_ERR_OUT_OF_RANGE = 5,     /* std::out_of_range     */
+    BF_ERR_TIMEOUT = 6,          /* a bounded device wait ran out */
+    BF_ERR_UNSUPPORTED = 7       /* valid request outside this build's kernels */
+} bf_status;
+
+/* Dimensions: include/beamformer/config.hpp:74-79 (n_time, n_freq, n_ant,
+ * n_beams).  Validation follows validate_dimensions (config.hpp:81-94). */
+typedef struct bf_dims {
+    uint64_t n_time;
+    uint64_t n_freq;
+    uint64_t n_ant;
+    uint64_t n_beams;
+} bf_dims;
+
+/* Kernel selector: include/beamformer/cuda_stage_api.hpp:14-17 (Direct,
+ * Tiled) plus the split-precision tcgen05 tensor-core kernel. */
+typedef enum bf_kernel {
+    BF_KERNEL_DIRECT = 0, /* canonical weights, reference float32 order   */
+    BF_KERNEL_TILED = 1,  /* tiled weights,     reference float32 order   */
+    BF_KERNEL_TENSOR = 2  /* split fp16 weights (bf_prepare_split_weights) */
+} bf_kernel;
+
+/* Library version string. */
+BF_API const char* bf_version(void);
+
+/* Copies the calling thread's last error message into buf (NUL-terminated,
+ * truncated to n) and returns its full length. */
+BF_API size_t bf_last_error(char* buf, size_t n);
+
+/* validate_dimensions: include/beamformer/config.hpp:81-94. */
+BF_API bf_status bf_validate_dimensions(const bf_dims* dims);
+
+/* cuda_device_info: include/beamformer/cuda_beamformer.hpp:42.
+ * name is NUL-terminated into name_buf (name_len bytes). */
+BF_API bf_status bf_device_info(char* name_buf, size_t name_len, int* compute_major,
+                                int* compute_minor, uint64_t* global_memory_bytes,
+                                int* driver_version, int* runtime_version);
+
+/* ------------------------------------------------------------------------ */
+/* Device-stage API: include/beamformer/cuda_stage_api.hpp:21-42            */
+/* ------------------------------------------------------------------------ */
+
+/* launch_packed_beamformer (cuda_stage_api.hpp:21-25): per-spectrum power
+ * [T][F][B].  kernel DIRECT reads canonical weights, TILED reads tiled
+ * weights; both reproduce the reference float32 operation order exactly. */
+BF_API bf_status bf_launch_packed_beamformer(int kernel, void* stream,
+                                             const uint8_t* packed_voltage,
+                                             const float* weights, float* intensity,
+                                             const bf_dims* dims);
+
+/* launch_packed_integrated_beamformer (cuda_stage_api.hpp:27-35): fused
+ * beamform + increasing-time float32 integration over integration_spectra,
+ * writing [W][F][B] with a partial last window.  Any integration length >= 1
+ * is accepted here (the C++ layer keeps the reference's 10/320 rule). */
+BF_API bf_status bf_launch_packed_integrated_beamformer(
+    int kernel, void* stream, const uint8_t* packed_voltage, const float* weights,
+    float* integrated_intensity, const bf_dims* dims, uint64_t integration_spectra);
+
+/* launch_quantize_integrated_intensity (cuda_stage_api.hpp:37-42): one
+ * (offset, scale) pair per 1x16x16 chunk; codes identical to
+ * cpu_quantize_integrated_intensity (src/quantization.cpp:61-161). */
+BF_API bf_status bf_launch_quantize_integrated_intensity(void* stream,
+                                                         const float* integrated_intensity,
+                                                         int8_t* codes, float* params,
+                                                         const bf_dims* integrated_dims);
+
+/* ------------------------------------------------------------------------ */
+/* Split-precision tensor-core grid (tcgen05, sm_100a)                      */
+/* No reference counterpart: the reference grid kernels are scalar float32  */
+/* (src/cuda_beamformer.cu:108-354).  Same inputs, same output layouts.      */
+/* ------------------------------------------------------------------------ */
+
+/* Bytes of the prepared operand for n_shards shards of dims. */
+BF_API uint64_t bf_split_weight_bytes(const bf_dims* dims, uint64_t n_shards);
+
+/* Converts canonical complex64 weights ([shard][B][F][A][2], device) into the
+ * tensor-core operand: each weight as an fp16 hi + lo pair (w = hi + lo to
+ * about 2^-22 relative), in the kernel's swizzled shared-memory image. */
+BF_API bf_status bf_prepare_split_weights(void* stream, const float* weights,
+                                          void* split_weights, const bf_dims* dims,
+                                          uint64_t n_shards);
+
+/* Fused grid beamformer on tcgen05 tensor cores: |X.W|^2, integration over
+ * integration_spectra (must be a multiple of 32) and, when codes and params
+ * are non-NULL, the int8 chunk quantizer.  n_ant must be 32 or 64 and
+ * n_beams <= 128.  integrated may not be NULL (it is also the quantizer's
+ * input). */
+BF_API bf_status bf_grid_tensor_integrated(void* stream, const uint8_t* packed_voltage,
+                                           const void* split_weights, float* integrated,
+                                           int8_t* codes, float* params, const bf_dims* dims,
+                                           uint64_t integration_spectra, uint64_t n_shards);
+
+/* ------------------------------------------------------------------------ */
+/* Tracker: include/beamformer/beam_tracker.hpp:91-100 (per-spectrum         */
+/* [T][F][1]) and cuda_beam_tracker_v5.hpp:69-125 (device resident).         */
+/* ------------------------------------------------------------------------ */
+
+/* One steering direction per window (window_directions [W][3] float,
+ * device), antenna positions [A][3] float (device) and per-channel wave
+ * numbers 2*pi*f/c [F] double (device).  Weights are generated on the GPU
+ * in registers: FP64 phase, reduced mod 2*pi in FP64, float sin/cos.
+ *   mode 0: reference float32 order (matches beam_tracker_cpu bit-exactly up
+ *           to the last bit of the sin/cos of the phase)
+ *   mode 1: streaming tensor-core kernel (fp16 hi+lo weights, fp32 sums)
+ * intensity ([T][F], may be NULL) receives per-spectrum power; integrated
+ * ([W][F], may be NULL) receives the per-window sum. */
+BF_API bf_status bf_tracker(void* stream, int mode, const uint8_t* packed_voltage,
+                            const float* positions, const double* wave_numbers,
+                            const float* window_directions, float* intensity,
+                            float* integrated, const bf_dims* dims,
+                            uint64_t integration_spectra);
+
+/* ------------------------------------------------------------------------ */
+/* Seeded synthetic voltages (no reference counterpart)      */
+/* ------------------------------------------------------------------------ */
+
+/* Approximately Gaussian complex int4 noise (Irwin-Hall of eight 16-bit
+ * uniforms) times `scale`, plus an optional source term mu ([U][F][A][2]
+ * float, device, epoch u = t / epoch_len), rounded half-to-even and clipped
+ * to [-8, 7].  Bit-identical to the CPU restatement in oracle/.  sample_offset
+ * shifts the counter so shards and batches stay independent. */
+BF_API bf_status bf_generate_voltage(void* stream, uint64_t seed, uint64_t sample_offset,
+                                     float scale, const float* mu, uint64_t epoch_len,
+                                     uint8_t* out, const bf_dims* dims);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BF_B200_H */

@@ -1,0 +1,63 @@
+"""Build the oracle (test infrastructure only).
+
+    python oracle/build.py
+
+Products (git-ignored, but shipped to the GPU box with the snapshot):
+    oracle/liboracle.so        C restatement (bf_oracle.c), -ffp-contract=off
+    oracle/_ref/libbfref.so    the reference CPU core, compiled directly from the
+                               reference checkout's own source files plus
+                               ref_shim.cpp; built only when the checkout is
+                               present (it is absent on the GPU box, which uses
+                               the prebuilt file).
+
+The reference sources are compiled with g++ straight from where they lie (no
+CMake, nothing copied).  -ffp-contract=off keeps the float32 operation order
+of the source (no FMA contraction), which is the order the CUDA kernels
+reproduce; -march=x86-64-v2 keeps the binary runnable on any x86-64 host.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+REF = Path(os.environ.get("BF_REFERENCE_ROOT", "/root/reference"))
+REF_SOURCES = ["cpu_beamformer.cpp", "beam_tracker.cpp", "beam_tracker_opt.cpp",
+               "beam_tracker_opt_v2.cpp", "cpu_opt_beam_tracker.cpp", "geometry.cpp",
+               "quantization.cpp", "synthetic_data.cpp", "temporal_integration.cpp",
+               "weights.cpp"]
+
+
+def _stale(out: Path, deps: list[Path]) -> bool:
+    return not out.exists() or any(d.stat().st_mtime > out.stat().st_mtime for d in deps)
+
+
+def build_oracle() -> Path:
+    src = HERE / "bf_oracle.c"
+    out = HERE / "liboracle.so"
+    if _stale(out, [src]):
+        subprocess.run(["gcc", "-O2", "-std=c11", "-fPIC", "-shared", "-ffp-contract=off",
+                        "-fno-fast-math", str(src), "-o", str(out), "-lm"], check=True)
+    return out
+
+
+def build_reference() -> Path | None:
+    out = HERE / "_ref" / "libbfref.so"
+    srcs = [REF / "src" / s for s in REF_SOURCES]
+    if not all(s.exists() for s in srcs):
+        return out if out.exists() else None
+    shim = HERE / "ref_shim.cpp"
+    if _stale(out, srcs + [shim]):
+        out.parent.mkdir(exist_ok=True)
+        subprocess.run(["g++", "-O3", "-std=c++17", "-fPIC", "-shared", "-fopenmp",
+                        "-ffp-contract=off", "-march=x86-64-v2", "-I", str(REF / "include"),
+                        *map(str, srcs), str(shim), "-o", str(out)], check=True)
+    return out
+
+
+if __name__ == "__main__":
+    print(build_oracle())
+    print(build_reference())
+    sys.exit(0)

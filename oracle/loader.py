@@ -1,0 +1,253 @@
+"""ctypes access to the oracle (test infrastructure).
+
+liboracle.so  - C restatement of the reference hot path (oracle/bf_oracle.c)
+libbfref.so   - the reference CPU core compiled from its sources (oracle/_ref)
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use
+this module.  It is the checker, never the thing measured as the product.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent.parent
+_ORACLE = ROOT / "oracle" / "liboracle.so"
+_REF = ROOT / "oracle" / "_ref" / "libbfref.so"
+_o = None
+_r = None
+
+P = C.c_void_p
+U64 = C.c_uint64
+F32 = C.c_float
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def oracle() -> C.CDLL:
+    global _o
+    if _o is None:
+        if not _ORACLE.exists():
+            import subprocess, sys
+            subprocess.run([sys.executable, str(ROOT / "oracle" / "build.py")], check=True)
+        o = C.CDLL(str(_ORACLE))
+        o.orc_generate_weights.argtypes = [U64, U64, U64, P, P, P, P]
+        o.orc_beamform_packed_intensity.argtypes = [P, P, U64, U64, U64, U64, P]
+        o.orc_window_count.argtypes = [U64, U64]
+        o.orc_window_count.restype = U64
+        o.orc_integrate.argtypes = [P, U64, U64, U64, U64, P]
+        o.orc_beamform_integrated.argtypes = [P, P, U64, U64, U64, U64, U64, P, U64, P]
+        o.orc_beamform_integrated_f64.argtypes = [P, P, U64, U64, U64, U64, U64, P, U64, P]
+        o.orc_quantize.argtypes = [P, U64, U64, U64, P, P]
+        o.orc_direction_from_lm.argtypes = [F32, F32, P]
+        o.orc_tracker_window_directions.argtypes = [F32, F32, F32, F32, U64, U64, P]
+        o.orc_tracker_weights.argtypes = [U64, U64, U64, P, P, P, P]
+        o.orc_tracker.argtypes = [P, P, U64, U64, U64, U64, P]
+        o.orc_generate_voltage.argtypes = [U64, U64, U64, U64, U64, F32, P, U64, P]
+        o.orc_covariance_block_i64.argtypes = [P, U64, U64, U64, P]
+        o.orc_unpack.argtypes = [P, U64, P, P]
+        o.orc_pack.argtypes = [C.c_int, C.c_int]
+        _o = o
+    return _o
+
+
+def reference_available() -> bool:
+    return _REF.exists()
+
+
+def reference() -> C.CDLL:
+    global _r
+    if _r is None:
+        r = C.CDLL(str(_REF))
+        r.ref_last_error.restype = C.c_char_p
+        r.ref_cpu_beamform_packed_intensity.argtypes = [P, P, U64, U64, U64, U64, P]
+        r.ref_cpu_integrate.argtypes = [P, U64, U64, U64, U64, U64, P]
+        r.ref_cpu_quantize.argtypes = [P, U64, U64, U64, U64, P, P]
+        r.ref_generate_weights.argtypes = [U64, U64, U64, P, P, P, P]
+        r.ref_generate_tiled_weights.argtypes = [U64, U64, U64, P, P, P, P]
+        r.ref_default_positions.argtypes = [U64, P]
+        r.ref_channelized_frequencies.argtypes = [U64, P]
+        r.ref_tracker_window_direction.argtypes = [F32, F32, F32, F32, U64, U64, P]
+        r.ref_beam_tracker.argtypes = [C.c_int, P, U64, U64, U64, F32, F32, F32, F32, U64, P]
+        r.ref_make_noise.argtypes = [U64, U64, U64, C.c_uint32, P]
+        r.ref_make_one_hot.argtypes = [U64, U64, U64, U64, U64, U64, C.c_int, C.c_int, P]
+        r.ref_make_point_source.argtypes = [U64, U64, U64, P, P, P, F32, P]
+        r.ref_make_moving_point_source.argtypes = [U64, U64, U64, P, P, F32, F32, F32, F32, F32, P]
+        r.ref_set_threads.argtypes = [C.c_int]
+        _r = r
+    return _r
+
+
+def _rcheck(rc: int) -> None:
+    if rc != 0:
+        raise RuntimeError(f"reference error {rc}: {reference().ref_last_error().decode()}")
+
+
+# ---------------- oracle wrappers ----------------
+
+def generate_weights(pos, freq, dirs) -> np.ndarray:
+    A, F, B = len(pos), len(freq), len(dirs)
+    out = np.zeros((B, F, A, 2), np.float32)
+    oracle().orc_generate_weights(A, F, B, _ptr(np.ascontiguousarray(pos, np.float32)),
+                                  _ptr(np.ascontiguousarray(freq, np.float32)),
+                                  _ptr(np.ascontiguousarray(dirs, np.float32)), _ptr(out))
+    return out
+
+
+def beamform(v: np.ndarray, w: np.ndarray, T, F, A, B) -> np.ndarray:
+    out = np.zeros((T, F, B), np.float32)
+    oracle().orc_beamform_packed_intensity(_ptr(v), _ptr(w), T, F, A, B, _ptr(out))
+    return out
+
+
+def integrate(I: np.ndarray, T, F, B, S) -> np.ndarray:
+    W = -(-T // S)
+    out = np.zeros((W, F, B), np.float32)
+    oracle().orc_integrate(_ptr(np.ascontiguousarray(I, np.float32)), T, F, B, S, _ptr(out))
+    return out
+
+
+def beamform_integrated(v, w, T, F, A, B, S, windows=None, f64=False) -> np.ndarray:
+    W = -(-T // S)
+    wl = None if windows is None else np.ascontiguousarray(windows, np.int64)
+    out = np.zeros((W, F, B), np.float64 if f64 else np.float32)
+    fn = oracle().orc_beamform_integrated_f64 if f64 else oracle().orc_beamform_integrated
+    fn(_ptr(v), _ptr(w), T, F, A, B, S, _ptr(wl), 0 if wl is None else len(wl), _ptr(out))
+    return out
+
+
+def quantize(I: np.ndarray, W, F, B):
+    ft, bt = -(-F // 16), -(-B // 16)
+    codes = np.zeros((W, F, B), np.int8)
+    params = np.zeros((W, ft, bt, 2), np.float32)
+    oracle().orc_quantize(_ptr(np.ascontiguousarray(I, np.float32)), W, F, B, _ptr(codes), _ptr(params))
+    return codes, params
+
+
+def tracker_weights(dirs, pos, freq) -> np.ndarray:
+    W, A, F = len(dirs), len(pos), len(freq)
+    out = np.zeros((W, F, A, 2), np.float32)
+    oracle().orc_tracker_weights(W, F, A, _ptr(np.ascontiguousarray(pos, np.float32)),
+                                 _ptr(np.ascontiguousarray(freq, np.float32)),
+                                 _ptr(np.ascontiguousarray(dirs, np.float32)), _ptr(out))
+    return out
+
+
+def tracker(v, window_weights, T, F, A, S) -> np.ndarray:
+    out = np.zeros((T, F), np.float32)
+    oracle().orc_tracker(_ptr(v), _ptr(np.ascontiguousarray(window_weights, np.float32)), T, F, A,
+                         S, _ptr(out))
+    return out
+
+
+def generate_voltage(seed, offset, T, F, A, scale, mu=None, epoch_len=1) -> np.ndarray:
+    out = np.zeros((T, F, A), np.uint8)
+    m = None if mu is None else np.ascontiguousarray(mu, np.float32)
+    oracle().orc_generate_voltage(seed, offset, T, F, A, scale, _ptr(m), epoch_len, _ptr(out))
+    return out
+
+
+def covariance_block(v, T, F, A) -> np.ndarray:
+    R = np.zeros((F, A, A, 2), np.int64)
+    oracle().orc_covariance_block_i64(_ptr(v), T, F, A, _ptr(R))
+    return R
+
+
+def unpack(v: np.ndarray):
+    re = np.zeros(v.shape, np.int8)
+    im = np.zeros(v.shape, np.int8)
+    oracle().orc_unpack(_ptr(np.ascontiguousarray(v)), v.size, _ptr(re), _ptr(im))
+    return re, im
+
+
+# ---------------- reference wrappers ----------------
+
+def ref_beamform(v, w, T, F, A, B) -> np.ndarray:
+    out = np.zeros((T, F, B), np.float32)
+    _rcheck(reference().ref_cpu_beamform_packed_intensity(_ptr(v), _ptr(w), T, F, A, B, _ptr(out)))
+    return out
+
+
+def ref_integrate(I, T, F, A, B, S) -> np.ndarray:
+    out = np.zeros((-(-T // S), F, B), np.float32)
+    _rcheck(reference().ref_cpu_integrate(_ptr(np.ascontiguousarray(I, np.float32)), T, F, A, B, S, _ptr(out)))
+    return out
+
+
+def ref_quantize(I, W, F, A, B):
+    codes = np.zeros((W, F, B), np.int8)
+    params = np.zeros((W, -(-F // 16), -(-B // 16), 2), np.float32)
+    _rcheck(reference().ref_cpu_quantize(_ptr(np.ascontiguousarray(I, np.float32)), W, F, A, B,
+                                         _ptr(codes), _ptr(params)))
+    return codes, params
+
+
+def ref_generate_weights(pos, freq, dirs, tiled=False) -> np.ndarray:
+    A, F, B = len(pos), len(freq), len(dirs)
+    if tiled:
+        out = np.zeros((F, -(-B // 32), A, 32, 2), np.float32)
+        fn = reference().ref_generate_tiled_weights
+    else:
+        out = np.zeros((B, F, A, 2), np.float32)
+        fn = reference().ref_generate_weights
+    _rcheck(fn(A, F, B, _ptr(np.ascontiguousarray(pos, np.float32)),
+               _ptr(np.ascontiguousarray(freq, np.float32)),
+               _ptr(np.ascontiguousarray(dirs, np.float32)), _ptr(out)))
+    return out
+
+
+def ref_default_positions(A) -> np.ndarray:
+    out = np.zeros((A, 3), np.float32)
+    _rcheck(reference().ref_default_positions(A, _ptr(out)))
+    return out
+
+
+def ref_channelized_frequencies(F) -> np.ndarray:
+    out = np.zeros(F, np.float32)
+    _rcheck(reference().ref_channelized_frequencies(F, _ptr(out)))
+    return out
+
+
+def ref_tracker(v, T, F, A, l0, m0, rl, rm, S, variant=0) -> np.ndarray:
+    out = np.zeros((T, F), np.float32)
+    _rcheck(reference().ref_beam_tracker(variant, _ptr(v), T, F, A, l0, m0, rl, rm, S, _ptr(out)))
+    return out
+
+
+def ref_tracker_window_direction(l0, m0, rl, rm, window, S) -> np.ndarray:
+    out = np.zeros(3, np.float32)
+    _rcheck(reference().ref_tracker_window_direction(l0, m0, rl, rm, window, S, _ptr(out)))
+    return out
+
+
+def ref_make_noise(T, F, A, seed) -> np.ndarray:
+    out = np.zeros((T, F, A), np.uint8)
+    _rcheck(reference().ref_make_noise(T, F, A, seed, _ptr(out)))
+    return out
+
+
+def ref_make_one_hot(T, F, A, t, f, a, re=3, im=-2) -> np.ndarray:
+    out = np.zeros((T, F, A), np.uint8)
+    _rcheck(reference().ref_make_one_hot(T, F, A, t, f, a, re, im, _ptr(out)))
+    return out
+
+
+def ref_make_point_source(T, F, A, pos, freq, direction, amplitude=4.0) -> np.ndarray:
+    out = np.zeros((T, F, A), np.uint8)
+    _rcheck(reference().ref_make_point_source(
+        T, F, A, _ptr(np.ascontiguousarray(pos, np.float32)),
+        _ptr(np.ascontiguousarray(freq, np.float32)),
+        _ptr(np.ascontiguousarray(direction, np.float32)), amplitude, _ptr(out)))
+    return out
+
+
+def ref_make_moving_point_source(T, F, A, pos, freq, l0, m0, rl, rm, amplitude=4.0) -> np.ndarray:
+    out = np.zeros((T, F, A), np.uint8)
+    _rcheck(reference().ref_make_moving_point_source(
+        T, F, A, _ptr(np.ascontiguousarray(pos, np.float32)),
+        _ptr(np.ascontiguousarray(freq, np.float32)), l0, m0, rl, rm, amplitude, _ptr(out)))
+    return out

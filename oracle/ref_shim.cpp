@@ -1,0 +1,223 @@
+// ref_shim.cpp -- extern "C" entry points into the reference CPU core.
+//
+// TEST INFRASTRUCTURE ONLY.  oracle/build.py compiles this file together
+// with the reference's own CPU sources (read where they lie in the reference
+// checkout, never copied) into oracle/_ref/libbfref.so.  Tests use it to pin
+// the C restatement (bf_oracle.c) and the CUDA kernels to the reference's
+// actual outputs; bench.py's reference arm times it on the host cores.
+// Every function returns 0 on success or a nonzero code with the exception
+// text available from ref_last_error().
+#include <beamformer/beam_tracker.hpp>
+#include <beamformer/beam_tracker_opt_v2.hpp>
+#include <beamformer/cpu_beamformer.hpp>
+#include <beamformer/geometry.hpp>
+#include <beamformer/quantization.hpp>
+#include <beamformer/synthetic_data.hpp>
+#include <beamformer/temporal_integration.hpp>
+#include <beamformer/weights.hpp>
+
+#include <omp.h>
+
+#include <cstdint>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+using namespace beamformer;
+
+namespace {
+thread_local std::string g_err;
+
+template <class Fn>
+int guarded(Fn&& fn) {
+    try {
+        fn();
+        return 0;
+    } catch (const std::invalid_argument& e) {
+        g_err = e.what();
+        return 1;
+    } catch (const std::logic_error& e) {
+        g_err = e.what();
+        return 2;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return 3;
+    }
+}
+
+Dimensions dims_of(uint64_t t, uint64_t f, uint64_t a, uint64_t b) {
+    return Dimensions{t, f, a, b};
+}
+
+std::vector<Vec3> vec3s(const float* p, size_t n) {
+    std::vector<Vec3> out(n);
+    for (size_t i = 0; i < n; ++i) out[i] = {p[3 * i], p[3 * i + 1], p[3 * i + 2]};
+    return out;
+}
+}  // namespace
+
+extern "C" {
+
+const char* ref_last_error() { return g_err.c_str(); }
+
+void ref_set_threads(int n) { omp_set_num_threads(n); }
+int ref_max_threads() { return omp_get_max_threads(); }
+
+// src/cpu_beamformer.cpp:40-79
+int ref_cpu_beamform_packed_intensity(const uint8_t* v, const float* w, uint64_t T, uint64_t F,
+                                      uint64_t A, uint64_t B, float* out) {
+    return guarded([&] {
+        const Dimensions d = dims_of(T, F, A, B);
+        PackedVoltage pv(v, v + T * F * A);
+        Weights wv(B * F * A);
+        std::memcpy(wv.data(), w, wv.size() * sizeof(ComplexFloat));
+        Intensities I(T * F * B);
+        cpu_beamform_packed_intensity_into(pv, wv, d, I);
+        std::memcpy(out, I.data(), I.size() * sizeof(float));
+    });
+}
+
+// src/temporal_integration.cpp:79-110
+int ref_cpu_integrate(const float* I, uint64_t T, uint64_t F, uint64_t A, uint64_t B,
+                      uint64_t S, float* out) {
+    return guarded([&] {
+        const Dimensions d = dims_of(T, F, A, B);
+        Intensities in(I, I + T * F * B);
+        IntegratedIntensities o(integrated_intensity_count(d, S));
+        cpu_integrate_intensity_into(in, d, S, o);
+        std::memcpy(out, o.data(), o.size() * sizeof(float));
+    });
+}
+
+// src/quantization.cpp:61-161 (integrated dims: n_time = windows)
+int ref_cpu_quantize(const float* I, uint64_t W, uint64_t F, uint64_t A, uint64_t B,
+                     int8_t* codes, float* params) {
+    return guarded([&] {
+        const Dimensions d = dims_of(W, F, A, B);
+        IntegratedIntensities in(I, I + W * F * B);
+        const auto q = cpu_quantize_integrated_intensity(in, d);
+        std::memcpy(codes, q.codes.data(), q.codes.size());
+        std::memcpy(params, q.parameters.data(), q.parameters.size() * 2 * sizeof(float));
+    });
+}
+
+// src/weights.cpp:11-60
+int ref_generate_weights(uint64_t A, uint64_t F, uint64_t B, const float* pos,
+                         const float* freq, const float* dirs, float* out) {
+    return guarded([&] {
+        const Dimensions d = dims_of(1, F, A, B);
+        const auto w = generate_weights(d, vec3s(pos, A), std::vector<float>(freq, freq + F),
+                                        vec3s(dirs, B));
+        std::memcpy(out, w.data(), w.size() * sizeof(ComplexFloat));
+    });
+}
+
+// src/weights.cpp:63-122
+int ref_generate_tiled_weights(uint64_t A, uint64_t F, uint64_t B, const float* pos,
+                               const float* freq, const float* dirs, float* out) {
+    return guarded([&] {
+        const Dimensions d = dims_of(1, F, A, B);
+        const auto w = generate_tiled_weights(d, vec3s(pos, A),
+                                              std::vector<float>(freq, freq + F), vec3s(dirs, B));
+        std::memcpy(out, w.data(), w.size() * sizeof(ComplexFloat));
+    });
+}
+
+// src/geometry.cpp:53-67, :79-95
+int ref_default_positions(uint64_t A, float* out) {
+    return guarded([&] {
+        const auto p = default_positions(A);
+        for (size_t i = 0; i < p.size(); ++i)
+            for (int c = 0; c < 3; ++c) out[3 * i + c] = p[i][c];
+    });
+}
+
+int ref_channelized_frequencies(uint64_t F, float* out) {
+    return guarded([&] {
+        const auto f = channelized_frequencies(F);
+        std::memcpy(out, f.data(), f.size() * sizeof(float));
+    });
+}
+
+// src/beam_tracker.cpp:67-76
+int ref_tracker_window_direction(float l0, float m0, float rl, float rm, uint64_t window,
+                                 uint64_t S, float* out3) {
+    return guarded([&] {
+        TrackerTrajectoryConfig tr;
+        tr.direction_start = direction_from_lm(l0, m0);
+        tr.direction_rate_per_sample = {rl, rm};
+        const auto d = tracker_window_direction(tr, window, S);
+        out3[0] = d[0];
+        out3[1] = d[1];
+        out3[2] = d[2];
+    });
+}
+
+static TrackerConfig tracker_config(float l0, float m0, float rl, float rm, uint64_t S) {
+    TrackerConfig cfg;
+    cfg.trajectory.direction_start = direction_from_lm(l0, m0);
+    cfg.trajectory.direction_rate_per_sample = {rl, rm};
+    cfg.integration_spectra = S;
+    return cfg;
+}
+
+// src/beam_tracker.cpp:90-146 (naive) and src/beam_tracker_opt_v2.cpp:143-311 (OpenMP)
+int ref_beam_tracker(int variant, const uint8_t* v, uint64_t T, uint64_t F, uint64_t A,
+                     float l0, float m0, float rl, float rm, uint64_t S, float* out) {
+    return guarded([&] {
+        const Dimensions d = dims_of(T, F, A, 1);
+        PackedVoltage pv(v, v + T * F * A);
+        Intensities I(T * F);
+        const TrackerConfig cfg = tracker_config(l0, m0, rl, rm, S);
+        if (variant == 0) {
+            beam_tracker_cpu_packed_intensity_into(pv, d, cfg, I);
+        } else {
+            beam_tracker_opt_v2_cpu_packed_intensity_into(pv, d, cfg, I);
+        }
+        std::memcpy(out, I.data(), I.size() * sizeof(float));
+    });
+}
+
+// src/synthetic_data.cpp:50-119
+int ref_make_noise(uint64_t T, uint64_t F, uint64_t A, uint32_t seed, uint8_t* out) {
+    return guarded([&] {
+        const auto v = make_noise(dims_of(T, F, A, 1), seed);
+        std::memcpy(out, v.data(), v.size());
+    });
+}
+
+int ref_make_one_hot(uint64_t T, uint64_t F, uint64_t A, uint64_t t, uint64_t f, uint64_t a,
+                     int re, int im, uint8_t* out) {
+    return guarded([&] {
+        const auto v = make_one_hot(dims_of(T, F, A, 1), t, f, a,
+                                    ComplexInt4{static_cast<int8_t>(re), static_cast<int8_t>(im)});
+        std::memcpy(out, v.data(), v.size());
+    });
+}
+
+int ref_make_point_source(uint64_t T, uint64_t F, uint64_t A, const float* pos,
+                          const float* freq, const float* dir, float amplitude, uint8_t* out) {
+    return guarded([&] {
+        const auto v = make_point_source(dims_of(T, F, A, 1), vec3s(pos, A),
+                                         std::vector<float>(freq, freq + F),
+                                         Vec3{dir[0], dir[1], dir[2]}, amplitude);
+        std::memcpy(out, v.data(), v.size());
+    });
+}
+
+// src/beam_tracker.cpp:148-192
+int ref_make_moving_point_source(uint64_t T, uint64_t F, uint64_t A, const float* pos,
+                                 const float* freq, float l0, float m0, float rl, float rm,
+                                 float amplitude, uint8_t* out) {
+    return guarded([&] {
+        TrackerTrajectoryConfig tr;
+        tr.direction_start = direction_from_lm(l0, m0);
+        tr.direction_rate_per_sample = {rl, rm};
+        const auto v = beam_tracker_make_moving_point_source(
+            dims_of(T, F, A, 1), vec3s(pos, A), std::vector<float>(freq, freq + F), tr, amplitude);
+        std::memcpy(out, v.data(), v.size());
+    });
+}
+
+}  // extern "C"

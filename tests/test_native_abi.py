@@ -1,0 +1,109 @@
+"""The C ABI library loads, exports every declared symbol, and validates its
+arguments on the host (no GPU needed: every check below returns before any
+CUDA call)."""
+from __future__ import annotations
+
+import ctypes as C
+import re
+import subprocess
+from pathlib import Path
+
+import pytest
+
+from beamform_project_b200 import native
+from beamform_project_b200.native import Dims
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def declared_symbols() -> list[str]:
+    names = []
+    for h in (ROOT / "include").glob("*.h"):
+        names += re.findall(r"BF_API\s+[\w\s\*]+?\b(bf_\w+)\s*\(", h.read_text())
+    return sorted(set(names))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = native.lib()
+    syms = declared_symbols()
+    assert len(syms) >= 10
+    out = subprocess.run(["nm", "-D", "--defined-only", str(native.library_path())],
+                         capture_output=True, text=True, check=True).stdout
+    exported = set(re.findall(r"\b(bf_\w+)\b", out))
+    for s in syms:
+        assert s in exported, s
+        assert hasattr(lib, s)
+    assert b"sm_100a" in lib.bf_version()
+
+
+def test_library_is_sm100a_only():
+    out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf",
+                          str(native.library_path())], capture_output=True, text=True).stdout
+    archs = set(re.findall(r"sm_(\d+a?)", out))
+    assert archs == {"100a"}, archs
+
+
+def _d(t=8, f=336, a=32, b=4):
+    return Dims(t, f, a, b)
+
+
+@pytest.mark.parametrize("dims,msg", [
+    (_d(t=0), "n_time must be positive"),
+    (_d(f=672), "336 frequency channels"),
+    (_d(a=48), "n_ant must be 32, 64, 128, or 256"),
+    (_d(b=0), "n_beams must be between 1 and 128"),
+    (_d(b=129), "n_beams must be between 1 and 128"),
+])
+def test_validate_dimensions_matches_reference(dims, msg):
+    lib = native.lib()
+    st = lib.bf_validate_dimensions(C.byref(dims))
+    assert st == 1
+    assert msg in native.last_error()
+    with pytest.raises(native.InvalidArgument, match=msg):
+        native.check(st)
+
+
+def test_stage_calls_validate_before_launch():
+    lib = native.lib()
+    d = _d()
+    fake = C.c_void_p(4096)  # never dereferenced: every call below fails validation first
+    assert lib.bf_launch_packed_beamformer(9, None, fake, fake, fake, C.byref(d)) == 1
+    assert "kernel selector" in native.last_error()
+    assert lib.bf_launch_packed_beamformer(0, None, None, fake, fake, C.byref(d)) == 1
+    assert "packed_voltage must not be null" in native.last_error()
+    assert lib.bf_launch_packed_beamformer(0, None, C.c_void_p(4097), fake, fake, C.byref(d)) == 1
+    assert "16-byte aligned" in native.last_error()
+    assert lib.bf_launch_packed_integrated_beamformer(0, None, fake, fake, fake, C.byref(d), 0) == 1
+    assert "integration_spectra must be positive" in native.last_error()
+    assert lib.bf_launch_packed_beamformer(2, None, fake, fake, fake, C.byref(d)) == 7
+    assert lib.bf_grid_tensor_integrated(None, fake, fake, fake, None, None, C.byref(d), 10, 1) == 7
+    assert "multiple of 32" in native.last_error()
+    assert lib.bf_grid_tensor_integrated(None, fake, fake, fake, fake, None, C.byref(d), 320, 1) == 1
+    d128 = _d(a=128)
+    assert lib.bf_grid_tensor_integrated(None, fake, fake, fake, None, None, C.byref(d128), 320, 1) == 7
+    d1 = _d(b=1)
+    assert lib.bf_tracker(None, 0, fake, fake, fake, fake, fake, None, C.byref(d), 16) == 1
+    assert "n_beams == 1" in native.last_error()
+    assert lib.bf_tracker(None, 0, fake, fake, fake, fake, None, None, C.byref(d1), 16) == 1
+    assert lib.bf_tracker(None, 5, fake, fake, fake, fake, fake, None, C.byref(d1), 16) == 1
+    assert lib.bf_tracker(None, 0, fake, fake, fake, fake, fake, None, C.byref(d1), 0) == 1
+
+
+def test_error_text_is_per_call():
+    lib = native.lib()
+    bad = _d(t=0)
+    assert lib.bf_validate_dimensions(C.byref(bad)) == 1
+    good = _d()
+    assert lib.bf_validate_dimensions(C.byref(good)) == 0
+    assert native.last_error() == ""
+
+
+def test_python_api_checks_buffers_without_gpu():
+    from beamform_project_b200 import api
+    with pytest.raises(api.InvalidArgument):
+        api.validate_dimensions(api.Dimensions(1, 100, 32, 4))
+    assert api.integrated_time_count(32768, 320) == 103
+    assert api.integrated_time_count(1024, 10) == 103
+    assert api.quantization_layout(api.Dimensions(103, 336, 64, 128)) == (103, 21, 8)
+    with pytest.raises(api.InvalidArgument):
+        api.integrated_time_count(10, 0)
