@@ -61,6 +61,7 @@ bf_status launch_tracker(cudaStream_t stream, int mode, const uint8_t* v, const 
 uint64_t split_weight_bytes(const bf_dims& d, uint64_t n_shards);
 bf_status launch_prepare_split(cudaStream_t stream, const float* w, void* split, const bf_dims& d,
                                uint64_t n_shards);
+bf_status take_tc_error(uint32_t* code);
 bf_status launch_grid_tensor(cudaStream_t stream, const uint8_t* v, const void* split,
                              float* integrated, int8_t* codes, float* params, const bf_dims& d,
                              uint64_t spectra, uint64_t n_shards);

@@ -177,7 +177,7 @@ BF_API bf_status bf_prepare_split_weights(void* stream, const float* weights, vo
         return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernel supports n_ant 32 or 64");
     }
     BF_TRY(check_ptr(weights, 8, "weights"));
-    BF_TRY(check_ptr(split_weights, 1024, "split_weights"));
+    BF_TRY(check_ptr(split_weights, 16, "split_weights"));
     return launch_prepare_split(static_cast<cudaStream_t>(stream), weights, split_weights, *dims,
                                 n_shards);
 }
@@ -203,7 +203,7 @@ BF_API bf_status bf_grid_tensor_integrated(void* stream, const uint8_t* packed_v
         return set_error(BF_ERR_INVALID_ARGUMENT, "codes and params must both be given or both be null");
     }
     BF_TRY(check_ptr(packed_voltage, 16, "packed_voltage"));
-    BF_TRY(check_ptr(split_weights, 1024, "split_weights"));
+    BF_TRY(check_ptr(split_weights, 16, "split_weights"));
     BF_TRY(check_ptr(integrated, 16, "integrated"));
     if (codes != nullptr) BF_TRY(check_ptr(params, 8, "params"));
     return launch_grid_tensor(static_cast<cudaStream_t>(stream), packed_voltage, split_weights,
@@ -237,6 +237,11 @@ BF_API bf_status bf_tracker(void* stream, int mode, const uint8_t* packed_voltag
     return launch_tracker(static_cast<cudaStream_t>(stream), mode, packed_voltage, positions,
                           wave_numbers, window_directions, intensity, integrated, *dims,
                           integration_spectra);
+}
+
+BF_API bf_status bf_take_device_error(uint32_t* code) {
+    clear_error();
+    return take_tc_error(code);
 }
 
 BF_API bf_status bf_generate_voltage(void* stream, uint64_t seed, uint64_t sample_offset,

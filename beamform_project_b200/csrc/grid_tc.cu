@@ -1,19 +1,616 @@
-// grid_tc.cu -- split-precision tcgen05 grid beamformer (placeholder).
+// grid_tc.cu -- split-precision tcgen05 fixed-grid beamformer (sm_100a).
+//
+// Same product as the reference's fused grid path (launch_packed_integrated_
+// beamformer + launch_quantize_integrated_intensity, reference
+// src/cuda_beamformer.cu:488-543 and src/cuda_quantize_int8.cu:132-147):
+//   I[w][f][b] = sum_{t in window w} | sum_a w[b][f][a] * x[t][f][a] |^2
+// with the weights used as stored (no conjugate), windows of S spectra and a
+// partial last window, then int8 chunk quantization.
+//
+// Formulation.  Per channel the complex contraction is one real GEMM
+//   D[t][n] = sum_k X[t][k] * Wop[n][k],   M = time, K = 2A, N = 2B,
+// where k enumerates (re, im) of every antenna and n = 2b + (0: re, 1: im)
+// of every beam.  Voltages are exact in fp16; each weight coefficient is an
+// fp16 pair hi + lo with hi = fp16(w), lo = fp16(w - hi), and both products
+// accumulate into the same fp32 TMEM accumulator, so D carries about 22 bits
+// of weight precision.  |.|^2 and the time integration run in the epilogue.
+//
+// CTA organisation (one persistent CTA per SM, 8 warps):
+//   warp 0      TMA producer: raw voltage tiles (128 spectra x A bytes of one
+//               channel, 4-D tensor map, zero fill past T) and the channel's
+//               prepared weight image (1-D bulk copies).
+//   warp 1      TMEM owner and MMA issuer (one thread): 2 x K/16
+//               tcgen05.mma (M=128, N=2B, K=16) per tile, hi then lo.
+//   warps 2-3   unpack: raw int4 bytes -> fp16 in the 128-byte-swizzled
+//               K-major layout the MMA reads (two LOP3s + one half2 op per
+//               value pair; the K order is permuted to follow the decode,
+//               and the prepared weights follow the same permutation).
+//   warps 4-7   epilogue: TMEM -> registers (tcgen05.ld 32x32b), power per
+//               (spectrum, beam), butterfly reduce-scatter over the 32
+//               spectra of each warp, running per-window sums, and the window
+//               total over the four warps in a fixed order.
+// Pipelines: 2 raw stages, 2 fp16 stages, 2 TMEM accumulators (2 x 2B
+// columns), all mbarrier driven; every wait is bounded and records an error
+// code instead of hanging.
+//
+// Work split: units are (shard, channel, group of G tiles) with G tiles =
+// lcm(128, S) spectra, so no integration window crosses a unit; each CTA
+// takes a contiguous range of units (few channel switches, so few weight
+// loads).  S must be a multiple of 32, which keeps every warp's 32 spectra
+// inside one window.
 #include "bf_internal.cuh"
+#include "sm100.cuh"
+
+#include <cuda.h>
+#include <cuda_fp16.h>
+
+#include <mutex>
 
 namespace bf {
 
+__device__ unsigned int g_tc_error = 0;
+
+namespace {
+
+using namespace sm100;
+
+constexpr int kThreads = 256;
+constexpr int kTileM = 128;
+constexpr int kRing = 8;                  // window partial-sum slots
+constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s bound on any wait
+
+struct TcParams {
+    const uint8_t* split;       // prepared weights, [shard][F][hi|lo][K/64][N][128 B]
+    float* integrated;          // [shard][W][F][B]
+    int n_time, n_freq, n_beams, n_beams_pad, n_ant, spectra, n_shards;
+    int tiles_per_channel, group_tiles, groups_per_channel, n_windows;
+    long long n_units;
+};
+
+__device__ __forceinline__ void record_error(unsigned code) { atomicOr(&g_tc_error, code); }
+
+// Decode one packed word (4 antennas) into the 8 fp16 K values of its slot:
+// [re a0, re a2, im a0, im a2, re a1, re a3, im a1, im a3].
+__device__ __forceinline__ uint4 decode4(uint32_t w) {
+    const uint32_t w1 = w >> 8;
+    uint32_t t0, t1, t2, t3;
+    asm("lop3.b32 %0, %1, %2, %3, 0x6A;" : "=r"(t0) : "r"(w), "r"(0x000F000Fu), "r"(0x64086408u));
+    asm("lop3.b32 %0, %1, %2, %3, 0x6A;" : "=r"(t1) : "r"(w), "r"(0x00F000F0u), "r"(0x64806480u));
+    asm("lop3.b32 %0, %1, %2, %3, 0x6A;" : "=r"(t2) : "r"(w1), "r"(0x000F000Fu), "r"(0x64086408u));
+    asm("lop3.b32 %0, %1, %2, %3, 0x6A;" : "=r"(t3) : "r"(w1), "r"(0x00F000F0u), "r"(0x64806480u));
+    const __half2 bias_lo = __float2half2_rn(1032.0f);
+    const __half2 sixteenth = __float2half2_rn(0.0625f);
+    const __half2 bias_hi = __float2half2_rn(-72.0f);
+    __half2 h0 = __hsub2(*reinterpret_cast<__half2*>(&t0), bias_lo);
+    __half2 h1 = __hfma2(*reinterpret_cast<__half2*>(&t1), sixteenth, bias_hi);
+    __half2 h2 = __hsub2(*reinterpret_cast<__half2*>(&t2), bias_lo);
+    __half2 h3 = __hfma2(*reinterpret_cast<__half2*>(&t3), sixteenth, bias_hi);
+    uint4 r;
+    r.x = *reinterpret_cast<uint32_t*>(&h0);
+    r.y = *reinterpret_cast<uint32_t*>(&h1);
+    r.z = *reinterpret_cast<uint32_t*>(&h2);
+    r.w = *reinterpret_cast<uint32_t*>(&h3);
+    return r;
+}
+
+struct Unit {
+    int shard, f, tile_begin, tile_end;
+};
+
+__device__ __forceinline__ Unit unit_of(const TcParams& p, long long u) {
+    Unit r;
+    const long long per_shard = static_cast<long long>(p.n_freq) * p.groups_per_channel;
+    r.shard = static_cast<int>(u / per_shard);
+    const long long rem = u % per_shard;
+    r.f = static_cast<int>(rem / p.groups_per_channel);
+    const int g = static_cast<int>(rem % p.groups_per_channel);
+    r.tile_begin = g * p.group_tiles;
+    r.tile_end = min(r.tile_begin + p.group_tiles, p.tiles_per_channel);
+    return r;
+}
+
+// Shared-memory plan (offsets from a 1024-aligned base).
+struct Smem {
+    uint32_t w_bytes = 0;    // one of hi / lo
+    uint32_t x_bytes = 0;    // one fp16 stage
+    uint32_t raw_bytes = 0;  // one raw stage
+    uint32_t off_w = 0, off_x = 0, off_raw = 0, off_slots = 0, off_bar = 0, total = 0;
+};
+
+__host__ __device__ constexpr Smem smem_plan(int n_ant, int n_beams_pad) {
+    Smem s{};
+    const uint32_t K = 2 * n_ant, N = 2 * n_beams_pad;
+    s.w_bytes = (K / 64) * N * 128;
+    s.x_bytes = (K / 64) * kTileM * 128;
+    s.raw_bytes = kTileM * n_ant;
+    s.off_w = 0;
+    s.off_x = s.off_w + 2 * s.w_bytes;
+    s.off_raw = s.off_x + 2 * s.x_bytes;
+    s.off_slots = s.off_raw + 2 * s.raw_bytes;
+    s.off_bar = s.off_slots + kRing * 4 * n_beams_pad * 4;
+    s.total = s.off_bar + 256;
+    return s;
+}
+
+template <int A, int NB>  // A antennas, NB padded beams (multiple of 16)
+__global__ void __launch_bounds__(kThreads, 1)
+grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
+    constexpr int K = 2 * A;
+    constexpr int N = 2 * NB;
+    constexpr uint32_t ACC_COLS = N;          // fp32 columns per accumulator
+    constexpr uint32_t TMEM_COLS = (2 * N <= 32) ? 32 : (2 * N <= 64) ? 64 : (2 * N <= 128) ? 128
+                                   : (2 * N <= 256) ? 256 : 512;
+    constexpr uint32_t IDESC = idesc_f16_f32(kTileM, N);
+    constexpr Smem S = smem_plan(A, NB);
+
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* w_hi = smem + S.off_w;
+    uint8_t* w_lo = w_hi + S.w_bytes;
+    uint8_t* xs = smem + S.off_x;
+    uint8_t* raw = smem + S.off_raw;
+    float* slots = reinterpret_cast<float*>(smem + S.off_slots);   // [kRing][4][NB]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + S.off_bar);
+    uint64_t* raw_full = bars + 0;    // [2]
+    uint64_t* raw_empty = bars + 2;   // [2]
+    uint64_t* x_full = bars + 4;      // [2]
+    uint64_t* x_empty = bars + 6;     // [2]
+    uint64_t* acc_full = bars + 8;    // [2]
+    uint64_t* acc_empty = bars + 10;  // [2]
+    uint64_t* w_full = bars + 12;
+    uint64_t* w_empty = bars + 13;
+    uint64_t* mma_done = bars + 14;
+    uint32_t* tmem_ptr = reinterpret_cast<uint32_t*>(bars + 16);
+    volatile int* s_fail = reinterpret_cast<volatile int*>(bars + 17);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(&raw_full[i], 1);
+            mbar_init(&raw_empty[i], 2);
+            mbar_init(&x_full[i], 2);
+            mbar_init(&x_empty[i], 1);
+            mbar_init(&acc_full[i], 1);
+            mbar_init(&acc_empty[i], 4);
+        }
+        mbar_init(w_full, 1);
+        mbar_init(w_empty, 1);
+        mbar_init(mma_done, 1);
+        *s_fail = 0;
+        fence_mbar_init();
+    }
+    for (int i = threadIdx.x; i < kRing * 4 * NB; i += kThreads) slots[i] = 0.f;
+    if (warp == 1) tmem_alloc(tmem_ptr, TMEM_COLS);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_ptr;
+
+    const long long u_begin = p.n_units * blockIdx.x / gridDim.x;
+    const long long u_end = p.n_units * (blockIdx.x + 1) / gridDim.x;
+    // A failed (timed-out) wait records its code, raises the CTA-wide flag and
+    // makes every role stop at its next check; nothing waits unboundedly.
+    auto fail = [&](unsigned code) {
+        record_error(code);
+        *s_fail = 1;
+    };
+
+    if (warp == 0) {
+        // ------------------------------------------------------------ producer
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0, w_empty_phase = 0;
+            int armed[2] = {-1, -1};   // parity of the last load issued per raw stage
+            int w_armed = -1;          // parity of the last weight load
+            uint32_t w_loads = 0;
+            int prev_ch = -1;
+            bool stop = false;
+            for (long long u = u_begin; u < u_end && !stop; ++u) {
+                const Unit un = unit_of(p, u);
+                const int ch = un.shard * p.n_freq + un.f;
+                if (ch != prev_ch) {
+                    if (prev_ch >= 0) {
+                        if (!mbar_wait(w_empty, w_empty_phase, kWaitNs)) { fail(1); break; }
+                        w_empty_phase ^= 1;
+                    }
+                    mbar_expect_tx(w_full, 2 * S.w_bytes);
+                    const uint8_t* src = p.split + static_cast<size_t>(ch) * 2 * S.w_bytes;
+                    constexpr uint32_t kChunk = 32768;
+                    for (uint32_t off = 0; off < 2 * S.w_bytes; off += kChunk) {
+                        const uint32_t n = min(kChunk, 2 * S.w_bytes - off);
+                        bulk_g2s(w_hi + off, src + off, n, w_full);
+                    }
+                    w_armed = static_cast<int>(w_loads & 1);
+                    ++w_loads;
+                    prev_ch = ch;
+                }
+                for (int k = un.tile_begin; k < un.tile_end; ++k) {
+                    if (*s_fail) { stop = true; break; }
+                    if (!mbar_wait(&raw_empty[stage], phase ^ 1, kWaitNs)) { fail(2); stop = true; break; }
+                    mbar_expect_tx(&raw_full[stage], S.raw_bytes);
+                    tma_load_4d(raw + stage * S.raw_bytes, &vmap, 0, un.f, k * kTileM, un.shard,
+                                &raw_full[stage]);
+                    armed[stage] = static_cast<int>(phase);
+                    if (++stage == 2) { stage = 0; phase ^= 1; }
+                }
+            }
+            // let every copy this thread issued land before the CTA can exit
+            for (int s = 0; s < 2; ++s) {
+                if (armed[s] >= 0 && !mbar_wait(&raw_full[s], static_cast<uint32_t>(armed[s]), kWaitNs)) fail(256);
+            }
+            if (w_armed >= 0 && !mbar_wait(w_full, static_cast<uint32_t>(w_armed), kWaitNs)) fail(512);
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------------------ MMA issuer
+        if (lane == 0) {
+            int xs_stage = 0, acc_stage = 0;
+            uint32_t x_phase = 0, acc_phase = 0, w_phase = 0;
+            int prev_ch = -1;
+            bool stop = false;
+            const uint32_t w_hi_addr = smem_u32(w_hi), w_lo_addr = smem_u32(w_lo);
+            for (long long u = u_begin; u < u_end && !stop; ++u) {
+                const Unit un = unit_of(p, u);
+                const int ch = un.shard * p.n_freq + un.f;
+                if (ch != prev_ch) {
+                    if (!mbar_wait(w_full, w_phase, kWaitNs)) { fail(4); break; }
+                    w_phase ^= 1;
+                    prev_ch = ch;
+                }
+                bool next_switches = true;
+                if (u + 1 < u_end) {
+                    const Unit nx = unit_of(p, u + 1);
+                    next_switches = (nx.shard * p.n_freq + nx.f) != ch;
+                }
+                for (int k = un.tile_begin; k < un.tile_end; ++k) {
+                    if (*s_fail) { stop = true; break; }
+                    if (!mbar_wait(&x_full[xs_stage], x_phase, kWaitNs)) { fail(8); stop = true; break; }
+                    if (!mbar_wait(&acc_empty[acc_stage], acc_phase ^ 1, kWaitNs)) { fail(16); stop = true; break; }
+                    tc_fence_after();
+                    const uint32_t d_tmem = tmem_base + acc_stage * ACC_COLS;
+                    const uint32_t x_addr = smem_u32(xs + xs_stage * S.x_bytes);
+#pragma unroll
+                    for (int kk = 0; kk < K / 16; ++kk) {
+                        const uint32_t kb = kk / 4, koff = (kk % 4) * 32;
+                        const uint64_t a = smem_desc_sw128(x_addr + kb * (kTileM * 128) + koff);
+                        const uint64_t bh = smem_desc_sw128(w_hi_addr + kb * (N * 128) + koff);
+                        const uint64_t bl = smem_desc_sw128(w_lo_addr + kb * (N * 128) + koff);
+                        mma_f16_ss(d_tmem, a, bh, IDESC, kk > 0 ? 1u : 0u);
+                        mma_f16_ss(d_tmem, a, bl, IDESC, 1u);
+                    }
+                    tc_commit(&x_empty[xs_stage]);
+                    tc_commit(&acc_full[acc_stage]);
+                    if (k + 1 == un.tile_end && next_switches) tc_commit(w_empty);
+                    if (++xs_stage == 2) { xs_stage = 0; x_phase ^= 1; }
+                    if (++acc_stage == 2) { acc_stage = 0; acc_phase ^= 1; }
+                }
+            }
+            // every MMA this thread issued completes before TMEM is released
+            tc_commit(mma_done);
+            if (!mbar_wait(mma_done, 0, kWaitNs)) fail(1024);
+        }
+    } else if (warp < 4) {
+        // ------------------------------------------------------------ unpack
+        const int ut = threadIdx.x - 64;  // 0..63
+        int stage = 0, xs_stage = 0;
+        uint32_t phase = 0, x_phase = 0;
+        bool stop = false;
+        constexpr int kChunks = A / 16;  // 16-byte raw chunks per spectrum
+        for (long long u = u_begin; u < u_end && !stop; ++u) {
+            const Unit un = unit_of(p, u);
+            for (int k = un.tile_begin; k < un.tile_end; ++k) {
+                if (*s_fail) { stop = true; break; }
+                if (!mbar_wait(&raw_full[stage], phase, kWaitNs)) { fail(32); stop = true; break; }
+                if (!mbar_wait(&x_empty[xs_stage], x_phase ^ 1, kWaitNs)) { fail(64); stop = true; break; }
+                const uint8_t* rsrc = raw + stage * S.raw_bytes;
+                uint8_t* xdst = xs + xs_stage * S.x_bytes;
+#pragma unroll 4
+                for (int idx = ut; idx < kTileM * kChunks; idx += 64) {
+                    const int r = idx / kChunks, q = idx % kChunks;
+                    const uint4 w4 = *reinterpret_cast<const uint4*>(rsrc + r * A + q * 16);
+                    const uint32_t words[4] = {w4.x, w4.y, w4.z, w4.w};
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) {
+                        const int kslot = 4 * q + j;           // 16-byte K slot (8 values)
+                        const int kb = kslot >> 3, c16 = kslot & 7;
+                        uint8_t* dst = xdst + kb * (kTileM * 128) + r * 128 + ((c16 ^ (r & 7)) << 4);
+                        *reinterpret_cast<uint4*>(dst) = decode4(words[j]);
+                    }
+                }
+                fence_proxy_async_smem();
+                __syncwarp();
+                if (lane == 0) {
+                    mbar_arrive(&raw_empty[stage]);
+                    mbar_arrive(&x_full[xs_stage]);
+                }
+                if (++stage == 2) { stage = 0; phase ^= 1; }
+                if (++xs_stage == 2) { xs_stage = 0; x_phase ^= 1; }
+            }
+        }
+    } else {
+        // ------------------------------------------------------------ epilogue
+        const int q4 = warp & 3;            // TMEM lane quadrant == 32-spectrum block of the tile
+        const int et = threadIdx.x - 128;   // 0..127
+        int acc_stage = 0;
+        uint32_t acc_phase = 0;
+        constexpr int kLoads = N / 32;      // 16 beams per 32-column load
+        float acc[kLoads];
+#pragma unroll
+        for (int c = 0; c < kLoads; ++c) acc[c] = 0.f;
+        int cur_win = -1;
+        bool failed = false, stop = false;
+        auto flush = [&](int w) {
+            float* s = slots + ((w % kRing) * 4 + q4) * NB;
+            if ((lane & 1) == 0) {
+#pragma unroll
+                for (int c = 0; c < kLoads; ++c) s[16 * c + (lane >> 1)] = acc[c];
+            }
+#pragma unroll
+            for (int c = 0; c < kLoads; ++c) acc[c] = 0.f;
+        };
+        for (long long u = u_begin; u < u_end && !stop; ++u) {
+            const Unit un = unit_of(p, u);
+            for (int k = un.tile_begin; k < un.tile_end; ++k) {
+                if (!failed && !mbar_wait(&acc_full[acc_stage], acc_phase, kWaitNs)) { fail(128); failed = true; }
+                tc_fence_after();
+                const int row0 = k * kTileM + 32 * q4;
+                const int my_win = row0 < p.n_time ? row0 / p.spectra : -1;
+                if (my_win != cur_win && cur_win >= 0) { flush(cur_win); cur_win = -1; }
+                if (my_win >= 0 && !failed) {
+                    const uint32_t taddr = tmem_base + ((32u * q4) << 16) + acc_stage * ACC_COLS;
+#pragma unroll
+                    for (int c = 0; c < kLoads; ++c) {
+                        uint32_t r[32];
+                        tmem_ld_32x32b_x32(taddr + 32 * c, r);
+                        tmem_ld_wait();
+                        float v[16];
+#pragma unroll
+                        for (int j = 0; j < 16; ++j) {
+                            const float re = __uint_as_float(r[2 * j]), im = __uint_as_float(r[2 * j + 1]);
+                            v[j] = re * re + im * im;
+                        }
+                        // butterfly reduce-scatter: lane pair (2m, 2m+1) ends with beam m's sum
+#pragma unroll
+                        for (int i = 0; i < 8; ++i) {
+                            const bool up = lane & 16;
+                            const float send = up ? v[i] : v[i + 8];
+                            const float keep = up ? v[i + 8] : v[i];
+                            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+                        }
+#pragma unroll
+                        for (int i = 0; i < 4; ++i) {
+                            const bool up = lane & 8;
+                            const float send = up ? v[i] : v[i + 4];
+                            const float keep = up ? v[i + 4] : v[i];
+                            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+                        }
+#pragma unroll
+                        for (int i = 0; i < 2; ++i) {
+                            const bool up = lane & 4;
+                            const float send = up ? v[i] : v[i + 2];
+                            const float keep = up ? v[i + 2] : v[i];
+                            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+                        }
+                        {
+                            const bool up = lane & 2;
+                            const float send = up ? v[0] : v[1];
+                            const float keep = up ? v[1] : v[0];
+                            v[0] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+                        }
+                        v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
+                        acc[c] += v[0];
+                    }
+                    cur_win = my_win;
+                }
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0 && !failed) mbar_arrive(&acc_empty[acc_stage]);
+                if (++acc_stage == 2) { acc_stage = 0; acc_phase ^= 1; }
+
+                const int tile_end_row = min((k + 1) * kTileM, p.n_time);
+                if (cur_win >= 0 && min((cur_win + 1) * p.spectra, p.n_time) <= tile_end_row) {
+                    flush(cur_win);
+                    cur_win = -1;
+                }
+                named_barrier(1, 128);
+                // finalize every window whose last spectrum lies in this tile
+                const int first_row = k * kTileM;
+                if (first_row < p.n_time) {
+                    const int w_first = first_row / p.spectra;
+                    const int w_last_in = (tile_end_row - 1) / p.spectra;
+                    for (int w = w_first; w <= w_last_in; ++w) {
+                        const int w_last = min((w + 1) * p.spectra, p.n_time) - 1;
+                        if (w_last < first_row || w_last >= tile_end_row) continue;
+                        float* s = slots + (w % kRing) * 4 * NB;
+                        for (int b = et; b < NB; b += 128) {
+                            const float total = ((s[b] + s[NB + b]) + s[2 * NB + b]) + s[3 * NB + b];
+                            s[b] = s[NB + b] = s[2 * NB + b] = s[3 * NB + b] = 0.f;
+                            if (b < p.n_beams) {
+                                p.integrated[((static_cast<size_t>(un.shard) * p.n_windows + w) * p.n_freq + un.f) *
+                                                 p.n_beams + b] = total;
+                            }
+                        }
+                    }
+                }
+                // one decision for all four warps: stop together or go on together
+                if (named_barrier_or(1, 128, failed || *s_fail != 0)) { stop = true; break; }
+            }
+        }
+    }
+
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem_base, TMEM_COLS);
+    }
+}
+
+// ------------------------------------------------------------------------
+// weight preparation: canonical complex64 -> split fp16 swizzled image
+// ------------------------------------------------------------------------
+__global__ void prepare_split_kernel(const float2* __restrict__ w, uint8_t* __restrict__ out,
+                                     int n_freq, int n_ant, int n_beams, int nb_pad, int n_shards) {
+    const int K = 2 * n_ant, N = 2 * nb_pad;
+    const long long per_channel = static_cast<long long>(N) * K;
+    const long long total = per_channel * n_freq * n_shards;
+    const uint32_t w_bytes = (K / 64) * N * 128;
+    for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const long long ch = i / per_channel;  // shard * F + f
+        const int rem = static_cast<int>(i % per_channel);
+        const int n = rem / K, k = rem % K;
+        const int shard = static_cast<int>(ch / n_freq), f = static_cast<int>(ch % n_freq);
+        // inverse of the decode order: k -> (antenna, component)
+        const int q = k / 32, j = (k % 32) / 8, pslot = k % 8;
+        static constexpr int kAnt[8] = {0, 2, 0, 2, 1, 3, 1, 3};
+        static constexpr int kIm[8] = {0, 0, 1, 1, 0, 0, 1, 1};
+        const int a = 16 * q + 4 * j + kAnt[pslot];
+        const int comp = kIm[pslot];
+        const int b = n >> 1, out_im = n & 1;
+        float coef = 0.f;
+        if (b < n_beams) {
+            const float2 wv = w[((static_cast<size_t>(shard) * n_beams + b) * n_freq + f) * n_ant + a];
+            // re out: x_re*wr - x_im*wi ; im out: x_re*wi + x_im*wr
+            coef = out_im ? (comp ? wv.x : wv.y) : (comp ? -wv.y : wv.x);
+        }
+        const __half hi = __float2half_rn(coef);
+        const __half lo = __float2half_rn(coef - __half2float(hi));
+        const int kb = k / 64, kk = k % 64;
+        const uint32_t off = kb * (N * 128) + n * 128 + ((((kk >> 3) ^ (n & 7))) << 4) + (kk & 7) * 2;
+        uint8_t* base = out + ch * 2 * w_bytes;
+        *reinterpret_cast<__half*>(base + off) = hi;
+        *reinterpret_cast<__half*>(base + w_bytes + off) = lo;
+    }
+}
+
+// ------------------------------------------------------------------------
+// host side
+// ------------------------------------------------------------------------
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*,
+                                   CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                   CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess) {
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+        }
+    });
+    return fn;
+}
+
+int padded_beams(uint64_t b) { return static_cast<int>((b + 15) / 16 * 16); }
+
+template <int A, int NB>
+bf_status launch_tc(cudaStream_t stream, const CUtensorMap& map, const TcParams& p, int sms) {
+    const Smem s = smem_plan(A, NB);
+    const size_t smem = s.total + 1024;
+    auto kern = grid_tensor_kernel<A, NB>;
+    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (err != cudaSuccess) return cuda_status(err, "grid_tensor_kernel smem attribute");
+    const int grid = static_cast<int>(std::min<long long>(sms, p.n_units));
+    kern<<<grid, kThreads, smem, stream>>>(map, p);
+    return cuda_status(cudaGetLastError(), "grid_tensor_kernel launch");
+}
+
+template <int A>
+bf_status dispatch_nb(cudaStream_t stream, const CUtensorMap& map, const TcParams& p, int sms) {
+    switch (p.n_beams_pad) {
+        case 16: return launch_tc<A, 16>(stream, map, p, sms);
+        case 32: return launch_tc<A, 32>(stream, map, p, sms);
+        case 48: return launch_tc<A, 48>(stream, map, p, sms);
+        case 64: return launch_tc<A, 64>(stream, map, p, sms);
+        case 80: return launch_tc<A, 80>(stream, map, p, sms);
+        case 96: return launch_tc<A, 96>(stream, map, p, sms);
+        case 112: return launch_tc<A, 112>(stream, map, p, sms);
+        case 128: return launch_tc<A, 128>(stream, map, p, sms);
+        default: return set_error(BF_ERR_INVALID_ARGUMENT, "n_beams must be between 1 and 128");
+    }
+}
+
+long long gcd_ll(long long a, long long b) { return b == 0 ? a : gcd_ll(b, a % b); }
+
+}  // namespace
+
 uint64_t split_weight_bytes(const bf_dims& d, uint64_t n_shards) {
-    return n_shards * d.n_freq * 2ull * 256ull * 2ull * d.n_ant * 2ull;
+    const uint64_t K = 2 * d.n_ant, N = 2 * static_cast<uint64_t>(padded_beams(d.n_beams));
+    return n_shards * d.n_freq * 2ull * K * N * 2ull;
 }
 
-bf_status launch_prepare_split(cudaStream_t, const float*, void*, const bf_dims&, uint64_t) {
-    return set_error(BF_ERR_UNSUPPORTED, "tensor-core kernel not built");
+bf_status launch_prepare_split(cudaStream_t stream, const float* w, void* split, const bf_dims& d,
+                               uint64_t n_shards) {
+    const int nbp = padded_beams(d.n_beams);
+    const long long total = static_cast<long long>(n_shards) * d.n_freq * 2 * nbp * 2 * d.n_ant;
+    const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, 148LL * 32));
+    prepare_split_kernel<<<blocks, 256, 0, stream>>>(reinterpret_cast<const float2*>(w),
+                                                     static_cast<uint8_t*>(split), static_cast<int>(d.n_freq),
+                                                     static_cast<int>(d.n_ant), static_cast<int>(d.n_beams),
+                                                     nbp, static_cast<int>(n_shards));
+    return cuda_status(cudaGetLastError(), "prepare_split_kernel launch");
 }
 
-bf_status launch_grid_tensor(cudaStream_t, const uint8_t*, const void*, float*, int8_t*, float*,
-                             const bf_dims&, uint64_t, uint64_t) {
-    return set_error(BF_ERR_UNSUPPORTED, "tensor-core kernel not built");
+bf_status launch_grid_tensor(cudaStream_t stream, const uint8_t* v, const void* split, float* integrated,
+                             int8_t* codes, float* params, const bf_dims& d, uint64_t spectra,
+                             uint64_t n_shards) {
+    if (d.n_time >= (1ull << 31) || n_shards > 1024) {
+        return set_error(BF_ERR_OVERFLOW, "CUDA tensor-core grid exceeds the supported size");
+    }
+    EncodeTiledFn enc = encode_fn();
+    if (enc == nullptr) return set_error(BF_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
+    CUtensorMap map;
+    const cuuint64_t dims[4] = {d.n_ant, d.n_freq, d.n_time, n_shards};
+    const cuuint64_t strides[3] = {d.n_ant, d.n_freq * d.n_ant, d.n_time * d.n_freq * d.n_ant};
+    const cuuint32_t box[4] = {static_cast<cuuint32_t>(d.n_ant), 1, static_cast<cuuint32_t>(kTileM), 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, const_cast<uint8_t*>(v), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_error(BF_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string(r));
+
+    TcParams p{};
+    p.split = static_cast<const uint8_t*>(split);
+    p.integrated = integrated;
+    p.n_time = static_cast<int>(d.n_time);
+    p.n_freq = static_cast<int>(d.n_freq);
+    p.n_beams = static_cast<int>(d.n_beams);
+    p.n_beams_pad = padded_beams(d.n_beams);
+    p.n_ant = static_cast<int>(d.n_ant);
+    p.spectra = static_cast<int>(spectra);
+    p.n_shards = static_cast<int>(n_shards);
+    p.tiles_per_channel = static_cast<int>((d.n_time + kTileM - 1) / kTileM);
+    const long long lcm = static_cast<long long>(spectra) / gcd_ll(spectra, kTileM) * kTileM;
+    p.group_tiles = static_cast<int>(lcm / kTileM);
+    p.groups_per_channel = (p.tiles_per_channel + p.group_tiles - 1) / p.group_tiles;
+    p.n_windows = static_cast<int>(window_count(d.n_time, spectra));
+    p.n_units = static_cast<long long>(n_shards) * d.n_freq * p.groups_per_channel;
+
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+
+    bf_status st;
+    if (d.n_ant == 32) st = dispatch_nb<32>(stream, map, p, sms);
+    else if (d.n_ant == 64) st = dispatch_nb<64>(stream, map, p, sms);
+    else return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernel supports n_ant 32 or 64");
+    if (st != BF_OK || codes == nullptr) return st;
+    bf_dims qd{n_shards * p.n_windows, d.n_freq, d.n_ant, d.n_beams};
+    return launch_quantize(stream, integrated, codes, params, qd);
+}
+
+bf_status take_tc_error(uint32_t* code) {
+    unsigned v = 0, zero = 0;
+    cudaError_t e = cudaMemcpyFromSymbol(&v, g_tc_error, sizeof(v));
+    if (e != cudaSuccess) return cuda_status(e, "read device error word");
+    e = cudaMemcpyToSymbol(g_tc_error, &zero, sizeof(zero));
+    if (e != cudaSuccess) return cuda_status(e, "clear device error word");
+    if (code) *code = v;
+    return BF_OK;
 }
 
 }  // namespace bf

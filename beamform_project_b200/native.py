@@ -77,6 +77,7 @@ _SIGS = {
     "bf_prepare_split_weights": (C.c_int, [_P, _P, _P, C.POINTER(Dims), _U64]),
     "bf_grid_tensor_integrated": (C.c_int, [_P, _P, _P, _P, _P, _P, C.POINTER(Dims), _U64, _U64]),
     "bf_tracker": (C.c_int, [_P, C.c_int, _P, _P, _P, _P, _P, _P, C.POINTER(Dims), _U64]),
+    "bf_take_device_error": (C.c_int, [C.POINTER(C.c_uint32)]),
     "bf_generate_voltage": (C.c_int, [_P, _U64, _U64, C.c_float, _P, _U64, _P, C.POINTER(Dims)]),
 }
 
@@ -111,6 +112,13 @@ def check(status: int) -> None:
     if status != BF_OK:
         cls = _ERRORS.get(status, BeamformerError)
         raise cls(status, last_error() or f"bf_status {status}")
+
+
+def take_device_error() -> int:
+    """Read and clear the tensor-core kernels' device error word (0 = none)."""
+    v = C.c_uint32(0)
+    check(lib().bf_take_device_error(C.byref(v)))
+    return int(v.value)
 
 
 def dims(n_time: int, n_freq: int, n_ant: int, n_beams: int) -> Dims:

@@ -142,6 +142,13 @@ BF_API bf_status bf_grid_tensor_integrated(void* stream, const uint8_t* packed_v
                                            int8_t* codes, float* params, const bf_dims* dims,
                                            uint64_t integration_spectra, uint64_t n_shards);
 
+/* Reads and clears the device-side error word of the tensor-core kernels
+ * (0 = no error).  Every wait inside those kernels is bounded; a wait that
+ * runs out sets a bit here (and the kernel returns) instead of hanging.
+ * Synchronous: call after the stream has been synchronised.  No reference
+ * counterpart (the reference kernels have no device-side waits). */
+BF_API bf_status bf_take_device_error(uint32_t* code);
+
 /* ------------------------------------------------------------------------ */
 /* Tracker: include/beamformer/beam_tracker.hpp:91-100 (per-spectrum         */
 /* [T][F][1]) and cuda_beam_tracker_v5.hpp:69-125 (device resident).         */

@@ -69,7 +69,8 @@ def test_known_answers_on_gpu(cuda, orc):
     assert np.allclose(out.reshape(1, F, 5), exp, rtol=1e-5, atol=1e-5)
     wb = orc.generate_weights(pos, freq, np.array([[0, 0, 1]], np.float32))
     vc = np.full((4, F, A), orc.oracle().orc_pack(7, -8), np.uint8)
-    o = api.cuda_beamform_packed_integrated_intensity(vc, wb, api.Dimensions(4, F, A, 1), 320)
+    o = api.cuda_beamform_packed_integrated_intensity(vc, wb, api.Dimensions(4, F, A, 1), 320,
+                                                      kernel=api.CudaBeamformerKernel.Direct)
     assert np.all(o == np.float32(4 * A * A * 113))
 
 
