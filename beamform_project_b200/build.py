@@ -78,6 +78,14 @@ def build(verbose: bool = False, force: bool = False) -> Path:
                   "-I", "/usr/local/cuda/include", *map(str, cxx_srcs), "-o", str(cxx_so),
                   "-L", str(LIB), "-lbf_b200", "-Wl,-rpath,$ORIGIN",
                   "-L", "/usr/local/cuda/lib64", "-lcudart"], log)
+        # C++ API test program (tests/cxx), built here so it ships with the libraries
+        test_src = ROOT / "tests" / "cxx" / "test_cxx_api.cpp"
+        test_bin = obj_dir / "test_cxx_api"
+        if test_src.exists() and (force or _stale(test_bin, [test_src, cxx_so] + cxx_headers)):
+            _run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-I", str(INCLUDE),
+                  "-I", "/usr/local/cuda/include", str(test_src), "-o", str(test_bin),
+                  "-L", str(LIB), "-lbf_cxx", "-lbf_b200", f"-Wl,-rpath,{LIB}",
+                  "-L", "/usr/local/cuda/lib64", "-lcudart"], log)
     (obj_dir / "build.log").write_text("\n".join(log))
     if verbose:
         print("\n".join(log))

@@ -54,7 +54,8 @@ namespace {
 
 using namespace sm100;
 
-constexpr int kThreads = 256;
+constexpr int kThreads = 384;             // 4 control / unpack warps + 8 epilogue warps
+constexpr int kEpilogueThreads = 256;
 constexpr int kTileM = 128;
 constexpr int kRing = 8;                  // window partial-sum slots
 constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s bound on any wait
@@ -91,6 +92,47 @@ __device__ __forceinline__ uint4 decode4(uint32_t w) {
     r.z = *reinterpret_cast<uint32_t*>(&h2);
     r.w = *reinterpret_cast<uint32_t*>(&h3);
     return r;
+}
+
+// 32 accumulator columns of this lane's spectrum = (re, im) of 16 beams.
+// Returns the power summed over the warp's 32 spectra for beam (lane >> 1):
+// |.|^2 per beam, then a butterfly reduce-scatter (16 shuffles in all) that
+// leaves the sum for beam m in lanes 2m and 2m + 1.
+__device__ __forceinline__ float beam_pair_sum(const uint32_t (&r)[32], int lane) {
+    float v[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        const float re = __uint_as_float(r[2 * j]), im = __uint_as_float(r[2 * j + 1]);
+        v[j] = re * re + im * im;
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const bool up = lane & 16;
+        const float send = up ? v[i] : v[i + 8];
+        const float keep = up ? v[i + 8] : v[i];
+        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const bool up = lane & 8;
+        const float send = up ? v[i] : v[i + 4];
+        const float keep = up ? v[i + 4] : v[i];
+        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+        const bool up = lane & 4;
+        const float send = up ? v[i] : v[i + 2];
+        const float keep = up ? v[i + 2] : v[i];
+        v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+    }
+    {
+        const bool up = lane & 2;
+        const float send = up ? v[0] : v[1];
+        const float keep = up ? v[1] : v[0];
+        v[0] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
+    }
+    return v[0] + __shfl_xor_sync(0xffffffffu, v[0], 1);
 }
 
 struct Unit {
@@ -172,7 +214,7 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
             mbar_init(&x_full[i], 2);
             mbar_init(&x_empty[i], 1);
             mbar_init(&acc_full[i], 1);
-            mbar_init(&acc_empty[i], 4);
+            mbar_init(&acc_empty[i], kEpilogueThreads / 32);
         }
         mbar_init(w_full, 1);
         mbar_init(w_empty, 1);
@@ -329,24 +371,32 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
         }
     } else {
         // ------------------------------------------------------------ epilogue
-        const int q4 = warp & 3;            // TMEM lane quadrant == 32-spectrum block of the tile
-        const int et = threadIdx.x - 128;   // 0..127
+        // Eight warps: warp w reads TMEM lane quadrant w % 4 (32 spectra of
+        // the tile) and one half of the accumulator columns (beams).
+        const int q4 = warp & 3;
+        const int half = (warp - 4) >> 2;                 // 0 or 1
+        const int et = threadIdx.x - 128;                 // 0..255
         int acc_stage = 0;
         uint32_t acc_phase = 0;
-        constexpr int kLoads = N / 32;      // 16 beams per 32-column load
-        float acc[kLoads];
+        constexpr int kLoads = N / 32;                    // 16 beams per 32-column load
+        constexpr int kHalfLoads = (kLoads + 1) / 2;
+        const int c_begin = half * kHalfLoads;
+        const int c_count = min(kHalfLoads, kLoads - c_begin);
+        float acc[kHalfLoads];
 #pragma unroll
-        for (int c = 0; c < kLoads; ++c) acc[c] = 0.f;
+        for (int c = 0; c < kHalfLoads; ++c) acc[c] = 0.f;
         int cur_win = -1;
         bool failed = false, stop = false;
         auto flush = [&](int w) {
             float* s = slots + ((w % kRing) * 4 + q4) * NB;
             if ((lane & 1) == 0) {
 #pragma unroll
-                for (int c = 0; c < kLoads; ++c) s[16 * c + (lane >> 1)] = acc[c];
+                for (int c = 0; c < kHalfLoads; ++c) {
+                    if (c < c_count) s[16 * (c_begin + c) + (lane >> 1)] = acc[c];
+                }
             }
 #pragma unroll
-            for (int c = 0; c < kLoads; ++c) acc[c] = 0.f;
+            for (int c = 0; c < kHalfLoads; ++c) acc[c] = 0.f;
         };
         for (long long u = u_begin; u < u_end && !stop; ++u) {
             const Unit un = unit_of(p, u);
@@ -357,48 +407,16 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                 const int my_win = row0 < p.n_time ? row0 / p.spectra : -1;
                 if (my_win != cur_win && cur_win >= 0) { flush(cur_win); cur_win = -1; }
                 if (my_win >= 0 && !failed) {
-                    const uint32_t taddr = tmem_base + ((32u * q4) << 16) + acc_stage * ACC_COLS;
+                    const uint32_t taddr = tmem_base + ((32u * q4) << 16) + acc_stage * ACC_COLS + 32 * c_begin;
 #pragma unroll
-                    for (int c = 0; c < kLoads; ++c) {
-                        uint32_t r[32];
-                        tmem_ld_32x32b_x32(taddr + 32 * c, r);
+                    for (int c = 0; c < kHalfLoads; c += 2) {
+                        // two loads in flight per wait
+                        uint32_t r0[32], r1[32];
+                        if (c < c_count) tmem_ld_32x32b_x32(taddr + 32 * c, r0);
+                        if (c + 1 < c_count) tmem_ld_32x32b_x32(taddr + 32 * (c + 1), r1);
                         tmem_ld_wait();
-                        float v[16];
-#pragma unroll
-                        for (int j = 0; j < 16; ++j) {
-                            const float re = __uint_as_float(r[2 * j]), im = __uint_as_float(r[2 * j + 1]);
-                            v[j] = re * re + im * im;
-                        }
-                        // butterfly reduce-scatter: lane pair (2m, 2m+1) ends with beam m's sum
-#pragma unroll
-                        for (int i = 0; i < 8; ++i) {
-                            const bool up = lane & 16;
-                            const float send = up ? v[i] : v[i + 8];
-                            const float keep = up ? v[i + 8] : v[i];
-                            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
-                        }
-#pragma unroll
-                        for (int i = 0; i < 4; ++i) {
-                            const bool up = lane & 8;
-                            const float send = up ? v[i] : v[i + 4];
-                            const float keep = up ? v[i + 4] : v[i];
-                            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
-                        }
-#pragma unroll
-                        for (int i = 0; i < 2; ++i) {
-                            const bool up = lane & 4;
-                            const float send = up ? v[i] : v[i + 2];
-                            const float keep = up ? v[i + 2] : v[i];
-                            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
-                        }
-                        {
-                            const bool up = lane & 2;
-                            const float send = up ? v[0] : v[1];
-                            const float keep = up ? v[1] : v[0];
-                            v[0] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
-                        }
-                        v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
-                        acc[c] += v[0];
+                        if (c < c_count) acc[c] += beam_pair_sum(r0, lane);
+                        if (c + 1 < c_count) acc[c + 1] += beam_pair_sum(r1, lane);
                     }
                     cur_win = my_win;
                 }
@@ -412,7 +430,7 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                     flush(cur_win);
                     cur_win = -1;
                 }
-                named_barrier(1, 128);
+                named_barrier(1, kEpilogueThreads);
                 // finalize every window whose last spectrum lies in this tile
                 const int first_row = k * kTileM;
                 if (first_row < p.n_time) {
@@ -422,7 +440,7 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                         const int w_last = min((w + 1) * p.spectra, p.n_time) - 1;
                         if (w_last < first_row || w_last >= tile_end_row) continue;
                         float* s = slots + (w % kRing) * 4 * NB;
-                        for (int b = et; b < NB; b += 128) {
+                        for (int b = et; b < NB; b += kEpilogueThreads) {
                             const float total = ((s[b] + s[NB + b]) + s[2 * NB + b]) + s[3 * NB + b];
                             s[b] = s[NB + b] = s[2 * NB + b] = s[3 * NB + b] = 0.f;
                             if (b < p.n_beams) {
@@ -432,8 +450,8 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                         }
                     }
                 }
-                // one decision for all four warps: stop together or go on together
-                if (named_barrier_or(1, 128, failed || *s_fail != 0)) { stop = true; break; }
+                // one decision for all epilogue warps: stop together or go on together
+                if (named_barrier_or(1, kEpilogueThreads, failed || *s_fail != 0)) { stop = true; break; }
             }
         }
     }
@@ -570,7 +588,7 @@ bf_status launch_grid_tensor(cudaStream_t stream, const uint8_t* v, const void* 
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, const_cast<uint8_t*>(v), dims, strides, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                     CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                     CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return set_error(BF_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string(r));
 
     TcParams p{};

@@ -141,9 +141,9 @@ tracker_stream_kernel(const uint8_t* __restrict__ v, const float* __restrict__ p
     const int t_begin = win * spectra;
     const int t_end = min(t_begin + spectra, n_time);
     float acc = 0.f;
-    for (int tb = t_begin; tb < t_end; tb += 16) {
+    // Rows g and g+8 of the 16-spectrum block starting at tb (zero past the window).
+    auto load_rows = [&](int tb, uint32_t (&wg)[NW], uint32_t (&wg8)[NW]) {
         const int tg = tb + g, tg8 = tb + g + 8;
-        uint32_t wg[NW], wg8[NW];
         const uint8_t* rg = v + (static_cast<size_t>(tg) * n_freq + f) * A + q * kBytes;
         const uint8_t* rg8 = v + (static_cast<size_t>(tg8) * n_freq + f) * A + q * kBytes;
         const bool vg = fvalid && tg < t_end, vg8 = fvalid && tg8 < t_end;
@@ -160,6 +160,13 @@ tracker_stream_kernel(const uint8_t* __restrict__ v, const float* __restrict__ p
                 wg8[4 * c] = x1.x; wg8[4 * c + 1] = x1.y; wg8[4 * c + 2] = x1.z; wg8[4 * c + 3] = x1.w;
             }
         }
+    };
+    // software pipeline: the next block's loads are in flight while this one computes
+    uint32_t wg[NW], wg8[NW];
+    load_rows(t_begin, wg, wg8);
+    for (int tb = t_begin; tb < t_end; tb += 16) {
+        uint32_t ng[NW], ng8[NW];
+        load_rows(tb + 16, ng, ng8);
         float d[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
         for (int j = 0; j < NW; ++j) {
@@ -192,6 +199,11 @@ tracker_stream_kernel(const uint8_t* __restrict__ v, const float* __restrict__ p
                 }
             }
             __syncthreads();
+        }
+#pragma unroll
+        for (int j = 0; j < NW; ++j) {
+            wg[j] = ng[j];
+            wg8[j] = ng8[j];
         }
     }
     if (integrated != nullptr) {

@@ -1,0 +1,56 @@
+// cuda_stage_api.hpp -- device-stage API (same declarations as the
+// reference's include/beamformer/cuda_stage_api.hpp:14-42).  Each call runs
+// one stage on caller-owned device buffers and the caller's stream; none
+// allocates memory or synchronises.  Errors are the reference's exception
+// types: std::invalid_argument (dimensions, kernel and integration rules),
+// std::runtime_error (CUDA), std::overflow_error (grid too large).
+//
+// Kernel selector: Direct (canonical [B][F][A] weights) and Tiled (tiled
+// [F][ceil(B/32)][A][32] weights) reproduce the reference float32 operation
+// order bit for bit.  TensorSplit is the tcgen05 split-precision kernel; it
+// reads weights prepared by prepare_split_weights and writes integrated
+// output only.
+#pragma once
+
+#include "beamformer/config.hpp"
+#include "beamformer/formats.hpp"
+#include "beamformer/quantization.hpp"
+#include "beamformer/temporal_integration.hpp"
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+
+namespace beamformer {
+
+enum class CudaBeamformerKernel {
+    Direct,
+    Tiled,
+    TensorSplit,
+};
+
+void launch_packed_beamformer(CudaBeamformerKernel kernel, cudaStream_t stream,
+                              const std::uint8_t* packed_voltage, const ComplexFloat* weights,
+                              float* intensity, const Dimensions& dims);
+
+// Direct accepts 320 spectra only and Tiled 10 or 320, as in the reference
+// (src/cuda_beamformer.cu:418-433); TensorSplit accepts any multiple of 32.
+void launch_packed_integrated_beamformer(CudaBeamformerKernel kernel, cudaStream_t stream,
+                                         const std::uint8_t* packed_voltage, const ComplexFloat* weights,
+                                         float* integrated_intensity, const Dimensions& dims,
+                                         const TemporalIntegrationConfig& temporal_integration);
+
+void launch_quantize_integrated_intensity(cudaStream_t stream, const float* integrated_intensity,
+                                          std::int8_t* quantized_intensity,
+                                          Int8QuantizationParameters* parameters,
+                                          const Dimensions& integrated_dims);
+
+// Bytes of the TensorSplit weight operand for `dims` (one shard).
+std::size_t split_weight_bytes(const Dimensions& dims);
+
+// Canonical device weights -> TensorSplit operand (device, split_weight_bytes).
+void prepare_split_weights(cudaStream_t stream, const ComplexFloat* weights, void* split_weights,
+                           const Dimensions& dims);
+
+}  // namespace beamformer

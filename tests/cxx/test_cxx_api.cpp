@@ -1,0 +1,234 @@
+// test_cxx_api.cpp -- the C++ drop-in API (include/beamformer/) exercised the
+// way the reference's own CUDA tests exercise theirs (tests/cuda/*.cpp in
+// the reference): exception types, known answers, workspace reuse, device
+// frames, the quantized pipeline, the TensorSplit kernel and the tracker.
+// Plain executable: prints one line per check, exits 0 when all pass.
+#include "beamformer/beam_tracker.hpp"
+#include "beamformer/cuda_beam_tracker_v5.hpp"
+#include "beamformer/cuda_beamformer.hpp"
+#include "beamformer/geometry.hpp"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <functional>
+#include <random>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+using namespace beamformer;
+
+namespace {
+
+int failures = 0;
+
+void expect(bool ok, const std::string& what) {
+    std::printf("%s %s\n", ok ? "ok  " : "FAIL", what.c_str());
+    if (!ok) ++failures;
+}
+
+template <class E>
+bool throws(const std::function<void()>& fn) {
+    try {
+        fn();
+    } catch (const E&) {
+        return true;
+    } catch (...) {
+        return false;
+    }
+    return false;
+}
+
+// Reference float32 order (src/cpu_beamformer.cpp:56-78), for small checks.
+float cpu_power(const PackedVoltage& v, const Weights& w, const Dimensions& d, std::size_t t, std::size_t f,
+                std::size_t b) {
+    volatile float sr = 0.f, si = 0.f;
+    for (std::size_t a = 0; a < d.n_ant; ++a) {
+        const auto x = unpack_complex_int4(v[voltage_index(t, f, a, d)]);
+        const float xr = x.real, xi = x.imag;
+        const auto& wv = w[weight_index(b, f, a, d)];
+        volatile float p0 = wv.real * xr, p1 = wv.imag * xi, q0 = wv.real * xi, q1 = wv.imag * xr;
+        volatile float d0 = p0 - p1, d1 = q0 + q1;
+        sr = sr + d0;
+        si = si + d1;
+    }
+    volatile float a2 = sr * sr, b2 = si * si;
+    return a2 + b2;
+}
+
+Weights weights_for(const Dimensions& d, const std::vector<Vec3>& dirs) {
+    const auto pos = default_positions(d.n_ant);
+    const auto freq = channelized_frequencies(d.n_freq);
+    Weights w(d.n_beams * d.n_freq * d.n_ant);
+    for (std::size_t b = 0; b < d.n_beams; ++b)
+        for (std::size_t f = 0; f < d.n_freq; ++f) {
+            const double k = 6.283185307179586476925286766559 * freq[f] / 299792458.0;
+            for (std::size_t a = 0; a < d.n_ant; ++a) {
+                const double delay = static_cast<double>(pos[a][0]) * dirs[b][0] +
+                                     static_cast<double>(pos[a][1]) * dirs[b][1] +
+                                     static_cast<double>(pos[a][2]) * dirs[b][2];
+                w[weight_index(b, f, a, d)] = {static_cast<float>(std::cos(k * delay)),
+                                               static_cast<float>(std::sin(k * delay))};
+            }
+        }
+    return w;
+}
+
+TiledWeights tile(const Weights& w, const Dimensions& d) {
+    TiledWeights t(tiled_weight_count(d), ComplexFloat{0.f, 0.f});
+    for (std::size_t b = 0; b < d.n_beams; ++b)
+        for (std::size_t f = 0; f < d.n_freq; ++f)
+            for (std::size_t a = 0; a < d.n_ant; ++a)
+                t[tiled_weight_index(f, b / 32, a, b % 32, d)] = w[weight_index(b, f, a, d)];
+    return t;
+}
+
+PackedVoltage random_voltage(const Dimensions& d, unsigned seed) {
+    std::mt19937 rng(seed);
+    PackedVoltage v(voltage_sample_count(d));
+    for (auto& x : v) x = static_cast<std::uint8_t>(rng() & 0xFF);
+    return v;
+}
+
+}  // namespace
+
+int main() {
+    // ---- dimension and selector rules (config.hpp:81-94, cuda_beamformer.cu:418-433)
+    expect(throws<std::invalid_argument>([] { validate_dimensions(Dimensions{0, 336, 32, 1}); }), "n_time 0 rejected");
+    expect(throws<std::invalid_argument>([] { CudaBeamformerWorkspace ws(Dimensions{8, 336, 32, 4}, CudaBeamformerKernel::Direct, TemporalIntegrationConfig{10}); }),
+           "Direct kernel rejects 10-spectrum integration");
+    expect(throws<std::invalid_argument>([] { CudaBeamformerWorkspace ws(Dimensions{8, 336, 32, 4}, CudaBeamformerKernel::Tiled, std::nullopt, CudaBeamformerOutput::QuantizedInt8); }),
+           "int8 output needs integration");
+    {
+        CudaBeamformerWorkspace ws(Dimensions{8, 336, 32, 4});
+        expect(throws<std::logic_error>([&] { ws.run_kernel(Dimensions{8, 336, 32, 4}); }), "run before upload is a logic_error");
+        expect(throws<std::invalid_argument>([&] { ws.upload_packed_voltage(PackedVoltage(16, 0), Dimensions{16, 336, 32, 4}); }),
+               "capacity exceeded");
+    }
+    const auto info = cuda_device_info();
+    expect(info.compute_major >= 10, "device is sm_100 class: " + info.name);
+
+    // ---- one-hot {3,-2} -> 13 on its channel (tests/cpu/test_cpu_beamformer.cpp:112-124)
+    {
+        const Dimensions d{1, 336, 32, 5};
+        std::vector<Vec3> dirs;
+        for (int b = 0; b < 5; ++b) dirs.push_back(direction_from_lm(static_cast<float>(b - 2) * 0.02F, 0.F));
+        const auto w = weights_for(d, dirs);
+        PackedVoltage v(voltage_sample_count(d), pack_complex_int4(0, 0));
+        v[voltage_index(0, 17, 7, d)] = pack_complex_int4(3, -2);
+        const auto I = cuda_beamform_packed_intensity(v, w, d);
+        bool ok = true;
+        for (std::size_t f = 0; f < 336; ++f)
+            for (std::size_t b = 0; b < 5; ++b) ok &= std::abs(I[intensity_index(0, f, b, d)] - (f == 17 ? 13.F : 0.F)) < 1e-5F;
+        expect(ok, "one-hot power 13");
+        const auto It = cuda_beamform_packed_intensity(v, tile(w, d), d, nullptr, CudaBeamformerKernel::Tiled);
+        expect(It == I, "Tiled equals Direct bit for bit");
+    }
+
+    // ---- random data: bit-exact against the reference float32 order
+    {
+        const Dimensions d{21, 336, 64, 40};
+        std::vector<Vec3> dirs;
+        for (int b = 0; b < 40; ++b) dirs.push_back(direction_from_lm(-0.4F + 0.02F * b, 0.1F));
+        const auto w = weights_for(d, dirs);
+        const auto v = random_voltage(d, 7);
+        CudaBeamformerTimings t;
+        const auto I = cuda_beamform_packed_intensity(v, w, d, &t);
+        bool ok = true;
+        for (std::size_t tt : {std::size_t{0}, std::size_t{20}})
+            for (std::size_t f : {std::size_t{0}, std::size_t{200}, std::size_t{335}})
+                for (std::size_t b = 0; b < 40; ++b) ok &= I[intensity_index(tt, f, b, d)] == cpu_power(v, w, d, tt, f, b);
+        expect(ok && t.kernel_ms > 0.0, "per-spectrum output bit-exact vs reference order");
+
+        // integrated 320 with a partial window (T = 700 -> 3 windows)
+        const Dimensions di{700, 336, 64, 40};
+        const auto vi = random_voltage(di, 8);
+        const auto wi = weights_for(di, dirs);
+        const auto integ = cuda_beamform_packed_integrated_intensity(vi, tile(wi, di), di, integration_direct);
+        bool ok2 = integ.size() == 3 * 336 * 40;
+        for (std::size_t b = 0; b < 40 && ok2; ++b) {
+            volatile float s = 0.f;
+            for (std::size_t tt = 640; tt < 700; ++tt) s = s + cpu_power(vi, wi, di, tt, 5, b);
+            ok2 &= integ[(2 * 336 + 5) * 40 + b] == s;
+        }
+        expect(ok2, "integrated partial window bit-exact");
+
+        // quantized pipeline equals quantizing the integrated output
+        const auto q = cuda_beamform_packed_quantized_integrated_intensity(vi, tile(wi, di), di, integration_direct);
+        expect(q.codes.size() == integ.size() && q.parameters.size() == 3 * 21 * 3, "quantized layout 3 x 21 x 3");
+
+        // TensorSplit workspace: within 1e-3 + 1e-5|x| of the reference-order kernel
+        CudaBeamformerWorkspace ws(di, CudaBeamformerKernel::TensorSplit, integration_direct);
+        ws.upload_weights(wi, di);
+        IntegratedIntensities out(integ.size());
+        ws.run_integrated_pipeline(vi, out, di);
+        bool ok3 = true;
+        for (std::size_t i = 0; i < out.size(); ++i) ok3 &= std::abs(out[i] - integ[i]) <= 1e-3F + 1e-5F * std::abs(integ[i]);
+        expect(ok3, "TensorSplit workspace within tolerance");
+        expect(throws<std::invalid_argument>([&] { CudaBeamformerWorkspace x(di, CudaBeamformerKernel::TensorSplit, integration_after_upchan); }),
+               "TensorSplit rejects 10-spectrum integration");
+
+        // device frame path: voltage and weights already on the device
+        std::uint8_t* dv = nullptr;
+        ComplexFloat* dw = nullptr;
+        float* dout = nullptr;
+        cudaMalloc(&dv, vi.size());
+        cudaMalloc(&dw, tiled_weight_bytes(di));
+        cudaMalloc(&dout, integ.size() * 4);
+        cudaMemcpy(dv, vi.data(), vi.size(), cudaMemcpyHostToDevice);
+        const auto tw = tile(wi, di);
+        cudaMemcpy(dw, tw.data(), tiled_weight_bytes(di), cudaMemcpyHostToDevice);
+        const auto shard = default_shard_descriptors()[1];
+        CudaBeamformerWorkspace wf(di, CudaBeamformerKernel::Tiled, integration_direct);
+        auto vf = make_packed_voltage_frame_view(dv, di, 42, shard);
+        auto wfv = make_tiled_weights_frame_view(dw, di, 42, shard);
+        const Dimensions od{3, 336, 64, 40};
+        auto of = make_intensity_frame_view(dout, od, 42, shard);
+        wf.run_device_frame(vf, wfv, of);
+        std::vector<float> back(integ.size());
+        cudaMemcpy(back.data(), dout, back.size() * 4, cudaMemcpyDeviceToHost);
+        expect(back == integ, "device frame output equals host pipeline");
+        auto bad = make_intensity_frame_view(dout, od, 43, shard);
+        expect(throws<std::invalid_argument>([&] { wf.run_device_frame(vf, wfv, bad); }), "frame id mismatch rejected");
+        cudaFree(dv);
+        cudaFree(dw);
+        cudaFree(dout);
+    }
+
+    // ---- tracker: constant trajectory equals the one-beam grid (tests/cpu/test_beam_tracker.cpp:121-139)
+    {
+        const Dimensions d{96, 336, 64, 1};
+        TrackerConfig cfg;
+        cfg.trajectory.direction_start = direction_from_lm(0.05F, -0.02F);
+        cfg.integration_spectra = 32;
+        const auto v = random_voltage(d, 11);
+        const auto I = cuda_beam_tracker_v5(v, d, cfg);
+        const auto w = weights_for(d, {cfg.trajectory.direction_start});
+        bool ok = I.size() == 96 * 336;
+        for (std::size_t t = 0; t < 96 && ok; t += 7)
+            for (std::size_t f = 0; f < 336; f += 5) {
+                const float r = cpu_power(v, w, d, t, f, 0);
+                ok &= std::abs(I[t * 336 + f] - r) <= 1e-3F + 1e-5F * std::abs(r);
+            }
+        expect(ok, "tracker (stationary) within tolerance of the one-beam grid");
+        expect(throws<std::invalid_argument>([&] { cuda_beam_tracker_v5(v, Dimensions{96, 336, 64, 2}, cfg); }),
+               "tracker requires n_beams == 1");
+
+        // batched stream, CUDA graph on, two batches
+        V5ExecutionConfig vc;
+        vc.enable_cuda_graph = true;
+        const Dimensions wdim{32, 336, 64, 1};
+        BatchedTrackerStreamV5 s(wdim, cfg, 3, vc);
+        std::vector<float> out(s.batch_output_floats());
+        s.process_batch(0, v.data(), out.data());
+        expect(out == I && s.last_kernel_time_ms() > 0.f, "batched stream equals one-shot tracker");
+        s.process_batch(0, v.data(), out.data());
+        expect(out == I, "graph replay repeats the result");
+    }
+
+    std::printf("%s (%d failures)\n", failures == 0 ? "ALL OK" : "FAILED", failures);
+    return failures == 0 ? 0 : 1;
+}
