@@ -214,6 +214,31 @@ def grid_tensor_integrated(stream, packed_voltage, split_weights, integrated, co
                                                  int(n_shards)))
 
 
+def grid_tensor_workspace_bytes(dims: Dimensions, integration_spectra: int, n_shards: int = 1) -> int:
+    d = dims.c()
+    return int(native.lib().bf_grid_tensor_workspace_bytes(C.byref(d), int(integration_spectra), int(n_shards)))
+
+
+def grid_tensor_quantized(stream, packed_voltage, split_weights, integrated, codes, params, workspace,
+                          dims: Dimensions, integration_spectra: int, n_shards: int = 1) -> None:
+    """Tensor-core grid with the int8 quantizer fused into its epilogue;
+    `workspace` (uint8, grid_tensor_workspace_bytes) is the kernel's scratch."""
+    torch = _torch()
+    validate_dimensions(dims)
+    nw = integrated_time_count(dims.n_time, integration_spectra)
+    n_out = n_shards * nw * dims.n_freq * dims.n_beams
+    qd = Dimensions(nw, dims.n_freq, dims.n_ant, dims.n_beams)
+    v = _dev(packed_voltage, "packed_voltage", torch.uint8, n_shards * dims.n_time * dims.n_freq * dims.n_ant)
+    s = _dev(split_weights, "split_weights", torch.uint8, split_weight_bytes(dims, n_shards))
+    o = _dev(integrated, "integrated", torch.float32, n_out)
+    c = _dev(codes, "codes", torch.int8, n_out)
+    p = _dev(params, "params", torch.float32, 2 * n_shards * quantization_parameter_count(qd))
+    w = _dev(workspace, "workspace", torch.uint8, grid_tensor_workspace_bytes(dims, integration_spectra, n_shards))
+    d = dims.c()
+    check(native.lib().bf_grid_tensor_quantized(_stream_handle(stream), v, s, o, c, p, w, C.byref(d),
+                                                int(integration_spectra), int(n_shards)))
+
+
 # --------------------------------------------------------------------------
 # tracker
 # --------------------------------------------------------------------------

@@ -48,6 +48,68 @@ __device__ __forceinline__ float power_ref(float sr, float si) {
     return __fadd_rn(__fmul_rn(sr, sr), __fmul_rn(si, si));
 }
 
+// One warp quantizes one 1x16x16 chunk (window w, channels 16*ft.., beams
+// 16*bt..) of integrated [W][F][B] exactly as cpu_quantize_integrated_intensity
+// (src/quantization.cpp:61-161): min/max over the finite values,
+// scale = (max - min) / 255, offset = min - (-127.5 * scale), codes
+// clamp(rint((v - offset) / scale), -127, 127), -128 for non-finite values and
+// a zero parameter pair for a chunk holding one.  Correctly rounded
+// intrinsics keep codes and parameters bit-identical to the CPU reference.
+// kCoherent reads through L2 (values written by other CTAs of a running grid).
+template <bool kCoherent>
+__device__ __forceinline__ void quantize_chunk(const float* __restrict in, int8_t* __restrict codes,
+                                               float2* __restrict params, size_t param_index, int win,
+                                               int n_freq, int n_beams, int ft, int bt, int lane) {
+    float vals[8];
+    bool valid[8];
+    float mn = INFINITY, mx = -INFINITY;
+    bool nonfinite = false;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int s = lane + 32 * i;  // local_freq * 16 + local_beam
+        const int f = ft * 16 + (s >> 4), b = bt * 16 + (s & 15);
+        valid[i] = f < n_freq && b < n_beams;
+        vals[i] = 0.f;
+        if (valid[i]) {
+            const float* src = in + (static_cast<size_t>(win) * n_freq + f) * n_beams + b;
+            vals[i] = kCoherent ? __ldcg(src) : *src;
+            if (!isfinite(vals[i])) {
+                nonfinite = true;
+            } else {
+                mn = fminf(mn, vals[i]);
+                mx = fmaxf(mx, vals[i]);
+            }
+        }
+    }
+    nonfinite = __any_sync(0xffffffffu, nonfinite);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    }
+    float offset = 0.f, scale = 0.f;
+    if (!nonfinite && isfinite(mn) && isfinite(mx)) {
+        scale = __fdiv_rn(__fsub_rn(mx, mn), 255.0f);
+        offset = __fsub_rn(mn, __fmul_rn(-127.5f, scale));
+        if (!isfinite(offset) || !isfinite(scale)) offset = scale = 0.f;
+    }
+    if (lane == 0) params[param_index] = make_float2(offset, scale);
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        if (!valid[i]) continue;
+        const int s = lane + 32 * i;
+        const int f = ft * 16 + (s >> 4), b = bt * 16 + (s & 15);
+        int code = 0;
+        if (!isfinite(vals[i])) {
+            code = -128;
+        } else if (scale != 0.f) {
+            code = __float2int_rn(__fdiv_rn(__fsub_rn(vals[i], offset), scale));
+            code = max(-127, min(127, code));
+        }
+        codes[(static_cast<size_t>(win) * n_freq + f) * n_beams + b] = static_cast<int8_t>(code);
+    }
+}
+
 // Kernel launchers (each returns a status, never throws).
 bf_status launch_grid_exact(int kernel, cudaStream_t stream, const uint8_t* v, const float* w,
                             float* out, const bf_dims& d, uint64_t spectra, bool integrate);
@@ -62,8 +124,12 @@ uint64_t split_weight_bytes(const bf_dims& d, uint64_t n_shards);
 bf_status launch_prepare_split(cudaStream_t stream, const float* w, void* split, const bf_dims& d,
                                uint64_t n_shards);
 bf_status take_tc_error(uint32_t* code);
+uint64_t grid_tensor_counter_count(const bf_dims& d, uint64_t spectra, uint64_t n_shards);
+// counters == nullptr: quantize (when codes is given) with a second launch;
+// otherwise quantization is fused into the tensor kernel's epilogue and
+// `counters` (grid_tensor_counter_count entries) is its scratch.
 bf_status launch_grid_tensor(cudaStream_t stream, const uint8_t* v, const void* split,
                              float* integrated, int8_t* codes, float* params, const bf_dims& d,
-                             uint64_t spectra, uint64_t n_shards);
+                             uint64_t spectra, uint64_t n_shards, unsigned* counters);
 
 }  // namespace bf

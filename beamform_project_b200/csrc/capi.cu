@@ -207,7 +207,41 @@ BF_API bf_status bf_grid_tensor_integrated(void* stream, const uint8_t* packed_v
     BF_TRY(check_ptr(integrated, 16, "integrated"));
     if (codes != nullptr) BF_TRY(check_ptr(params, 8, "params"));
     return launch_grid_tensor(static_cast<cudaStream_t>(stream), packed_voltage, split_weights,
-                              integrated, codes, params, *dims, integration_spectra, n_shards);
+                              integrated, codes, params, *dims, integration_spectra, n_shards, nullptr);
+}
+
+BF_API uint64_t bf_grid_tensor_workspace_bytes(const bf_dims* dims, uint64_t integration_spectra,
+                                               uint64_t n_shards) {
+    if (dims == nullptr || integration_spectra == 0) return 0;
+    return grid_tensor_counter_count(*dims, integration_spectra, n_shards) * sizeof(unsigned);
+}
+
+BF_API bf_status bf_grid_tensor_quantized(void* stream, const uint8_t* packed_voltage,
+                                          const void* split_weights, float* integrated, int8_t* codes,
+                                          float* params, void* workspace, const bf_dims* dims,
+                                          uint64_t integration_spectra, uint64_t n_shards) {
+    clear_error();
+    BF_TRY(validate_dims(dims));
+    if (n_shards == 0) return set_error(BF_ERR_INVALID_ARGUMENT, "n_shards must be positive");
+    if (integration_spectra == 0) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "integration_spectra must be positive");
+    }
+    if (integration_spectra % 32 != 0) {
+        return set_error(BF_ERR_UNSUPPORTED,
+                         "the tensor-core kernel needs integration_spectra to be a multiple of 32");
+    }
+    if (dims->n_ant > 64) {
+        return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernel supports n_ant 32 or 64");
+    }
+    BF_TRY(check_ptr(packed_voltage, 16, "packed_voltage"));
+    BF_TRY(check_ptr(split_weights, 16, "split_weights"));
+    BF_TRY(check_ptr(integrated, 16, "integrated"));
+    BF_TRY(check_ptr(codes, 1, "codes"));
+    BF_TRY(check_ptr(params, 8, "params"));
+    BF_TRY(check_ptr(workspace, 4, "workspace"));
+    return launch_grid_tensor(static_cast<cudaStream_t>(stream), packed_voltage, split_weights,
+                              integrated, codes, params, *dims, integration_spectra, n_shards,
+                              static_cast<unsigned*>(workspace));
 }
 
 BF_API bf_status bf_tracker(void* stream, int mode, const uint8_t* packed_voltage,

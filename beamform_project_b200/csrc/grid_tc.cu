@@ -63,8 +63,11 @@ constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s bound on any wait
 struct TcParams {
     const uint8_t* split;       // prepared weights, [shard][F][hi|lo][K/64][N][128 B]
     float* integrated;          // [shard][W][F][B]
+    int8_t* codes;              // [shard][W][F][B] or null (no fused quantization)
+    float2* params;             // [shard][W][ftiles][btiles]
+    unsigned* counters;         // [shard][W][ftiles] arrival counts, zero at launch
     int n_time, n_freq, n_beams, n_beams_pad, n_ant, spectra, n_shards;
-    int tiles_per_channel, group_tiles, groups_per_channel, n_windows;
+    int tiles_per_channel, group_tiles, groups_per_channel, n_windows, ftiles, btiles;
     long long n_units;
 };
 
@@ -151,6 +154,83 @@ __device__ __forceinline__ Unit unit_of(const TcParams& p, long long u) {
     return r;
 }
 
+// ---------------- fused quantization bookkeeping (epilogue thread 0) ----------
+__device__ __forceinline__ unsigned atom_add_acq_rel_gpu(unsigned* addr, unsigned v) {
+    unsigned old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(addr), "r"(v) : "memory");
+    return old;
+}
+
+// Counter bumps issued for the windows finalized in one tile (all of one
+// (shard, channel) unit); windows w0 + i for the bits i of mask.
+struct Pending {
+    unsigned old[8];
+    unsigned mask;
+    int w0, shard, fg;
+    unsigned group;
+};
+
+// Record the windows finalized in a tile (no memory traffic yet).
+__device__ __forceinline__ void record_finalized(const TcParams& p, const Unit& un, int first_row, int tile_end_row,
+                                                 Pending& pd) {
+    pd.mask = 0;
+    if (first_row >= p.n_time) return;
+    pd.w0 = first_row / p.spectra;
+    pd.shard = un.shard;
+    pd.fg = un.f / 16;
+    pd.group = static_cast<unsigned>(min(16, p.n_freq - 16 * pd.fg));
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const int w = pd.w0 + i;
+        const int w_last = min((w + 1) * p.spectra, p.n_time) - 1;
+        if (w < p.n_windows && w_last >= first_row && w_last < tile_end_row) pd.mask |= 1u << i;
+    }
+}
+
+// Bump the counters of recorded windows (acq_rel at GPU scope: releases this
+// CTA's stores of those windows, acquires the other CTAs' when last).
+__device__ __forceinline__ void issue_arrivals(const TcParams& p, const Pending& rec, Pending& pd) {
+    pd = rec;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        if ((rec.mask >> i) & 1u) {
+            const size_t ci = (static_cast<size_t>(rec.shard) * p.n_windows + rec.w0 + i) * p.ftiles + rec.fg;
+            pd.old[i] = atom_add_acq_rel_gpu(&p.counters[ci], 1u);
+        }
+    }
+}
+
+// Publish the windows whose group this CTA completed (bump result == group - 1).
+__device__ __forceinline__ void publish_ready(Pending& pd, volatile int* s_quant, volatile int* s_meta) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        int w = -1;
+        if (((pd.mask >> i) & 1u) && pd.old[i] + 1 == pd.group) w = pd.w0 + i;
+        s_quant[i] = w;
+    }
+    s_meta[0] = pd.shard;
+    s_meta[1] = pd.fg;
+    pd.mask = 0;
+}
+
+// All epilogue threads: quantize every published window's chunks (one warp per
+// 16-beam chunk).  The integrated values of the other CTAs were released by
+// their bumps and acquired by ours; they are read through L2.
+__device__ __forceinline__ void quantize_ready(const TcParams& p, volatile int* s_quant, volatile int* s_meta,
+                                               int et, int lane) {
+    const int shard = s_meta[0], fg = s_meta[1];
+    for (int i = 0; i < 8; ++i) {
+        const int w = s_quant[i];
+        if (w < 0) continue;
+        const size_t shard_off = static_cast<size_t>(shard) * p.n_windows * p.n_freq * p.n_beams;
+        for (int bt = et >> 5; bt < p.btiles; bt += kEpilogueThreads / 32) {
+            const size_t pidx = ((static_cast<size_t>(shard) * p.n_windows + w) * p.ftiles + fg) * p.btiles + bt;
+            quantize_chunk<true>(p.integrated + shard_off, p.codes + shard_off, p.params, pidx, w, p.n_freq,
+                                 p.n_beams, fg, bt, lane);
+        }
+    }
+}
+
 // Shared-memory plan (offsets from a 1024-aligned base).
 struct Smem {
     uint32_t w_bytes = 0;    // one of hi / lo
@@ -204,6 +284,14 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
     uint64_t* mma_done = bars + 14;
     uint32_t* tmem_ptr = reinterpret_cast<uint32_t*>(bars + 16);
     volatile int* s_fail = reinterpret_cast<volatile int*>(bars + 17);
+    volatile int* s_quant = reinterpret_cast<volatile int*>(bars + 18);  // [8] windows to quantize
+    volatile int* s_meta = reinterpret_cast<volatile int*>(bars + 22);   // [2] their shard, channel group
+    Pending pend, recorded;                                               // epilogue thread 0 only
+    pend.mask = 0;
+    recorded.mask = 0;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < 8; ++i) s_quant[i] = -1;
+    }
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
@@ -431,6 +519,9 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                     cur_win = -1;
                 }
                 named_barrier(1, kEpilogueThreads);
+                // quantize the groups this CTA completed one tile ago (list published
+                // by epilogue thread 0 before the barrier)
+                if (p.codes != nullptr) quantize_ready(p, s_quant, s_meta, et, lane);
                 // finalize every window whose last spectrum lies in this tile
                 const int first_row = k * kTileM;
                 if (first_row < p.n_time) {
@@ -452,7 +543,36 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                 }
                 // one decision for all epilogue warps: stop together or go on together
                 if (named_barrier_or(1, kEpilogueThreads, failed || *s_fail != 0)) { stop = true; break; }
+                if (p.codes != nullptr && et == 0) {
+                    // Fused int8 quantization.  A 1x16x16 chunk spans 16 channels that
+                    // other CTAs own: each finished (window, channel) bumps its
+                    // 16-channel group's counter, and the CTA whose bump completes the
+                    // group quantizes the group's chunks for that window.  A GPU-scope
+                    // release waits for the releasing thread's outstanding stores, so the
+                    // bump for a tile's windows is issued one tile after their stores
+                    // (ordered by the barriers in between; the release is cumulative) and
+                    // its result is published one tile later still: both waits overlap
+                    // the tensor work instead of stalling the epilogue.
+                    publish_ready(pend, s_quant, s_meta);
+                    issue_arrivals(p, recorded, pend);
+                    record_finalized(p, un, first_row, tile_end_row, recorded);
+                }
             }
+        }
+        if (p.codes != nullptr && !stop) {
+            // drain the three stages: published list, bumps in flight, recorded windows
+            for (int round = 0; round < 3; ++round) {
+                named_barrier(1, kEpilogueThreads);
+                quantize_ready(p, s_quant, s_meta, et, lane);
+                named_barrier(1, kEpilogueThreads);
+                if (et == 0) {
+                    publish_ready(pend, s_quant, s_meta);
+                    issue_arrivals(p, recorded, pend);
+                    recorded.mask = 0;
+                }
+            }
+            named_barrier(1, kEpilogueThreads);
+            quantize_ready(p, s_quant, s_meta, et, lane);
         }
     }
 
@@ -573,9 +693,13 @@ bf_status launch_prepare_split(cudaStream_t stream, const float* w, void* split,
     return cuda_status(cudaGetLastError(), "prepare_split_kernel launch");
 }
 
+uint64_t grid_tensor_counter_count(const bf_dims& d, uint64_t spectra, uint64_t n_shards) {
+    return n_shards * window_count(d.n_time, spectra) * ((d.n_freq + 15) / 16);
+}
+
 bf_status launch_grid_tensor(cudaStream_t stream, const uint8_t* v, const void* split, float* integrated,
                              int8_t* codes, float* params, const bf_dims& d, uint64_t spectra,
-                             uint64_t n_shards) {
+                             uint64_t n_shards, unsigned* counters) {
     if (d.n_time >= (1ull << 31) || n_shards > 1024) {
         return set_error(BF_ERR_OVERFLOW, "CUDA tensor-core grid exceeds the supported size");
     }
@@ -607,6 +731,18 @@ bf_status launch_grid_tensor(cudaStream_t stream, const uint8_t* v, const void* 
     p.groups_per_channel = (p.tiles_per_channel + p.group_tiles - 1) / p.group_tiles;
     p.n_windows = static_cast<int>(window_count(d.n_time, spectra));
     p.n_units = static_cast<long long>(n_shards) * d.n_freq * p.groups_per_channel;
+    p.ftiles = static_cast<int>((d.n_freq + 15) / 16);
+    p.btiles = static_cast<int>((d.n_beams + 15) / 16);
+    const bool fused = codes != nullptr && counters != nullptr;
+    if (fused) {
+        p.codes = codes;
+        p.params = reinterpret_cast<float2*>(params);
+        p.counters = counters;
+        const cudaError_t e = cudaMemsetAsync(counters, 0,
+                                              grid_tensor_counter_count(d, spectra, n_shards) * sizeof(unsigned),
+                                              stream);
+        if (e != cudaSuccess) return cuda_status(e, "clear quantization counters");
+    }
 
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -616,7 +752,7 @@ bf_status launch_grid_tensor(cudaStream_t stream, const uint8_t* v, const void* 
     if (d.n_ant == 32) st = dispatch_nb<32>(stream, map, p, sms);
     else if (d.n_ant == 64) st = dispatch_nb<64>(stream, map, p, sms);
     else return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernel supports n_ant 32 or 64");
-    if (st != BF_OK || codes == nullptr) return st;
+    if (st != BF_OK || codes == nullptr || fused) return st;
     bf_dims qd{n_shards * p.n_windows, d.n_freq, d.n_ant, d.n_beams};
     return launch_quantize(stream, integrated, codes, params, qd);
 }

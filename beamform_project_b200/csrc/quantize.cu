@@ -28,54 +28,7 @@ quantize_kernel(const float* __restrict__ in, int8_t* __restrict__ codes,
     const long long rest = chunk / btiles;
     const int ft = static_cast<int>(rest % ftiles);
     const int win = static_cast<int>(rest / ftiles);
-
-    float vals[8];
-    bool valid[8];
-    float mn = INFINITY, mx = -INFINITY;
-    bool nonfinite = false;
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        const int s = lane + 32 * i;  // 0..255 = local_freq * 16 + local_beam
-        const int f = ft * 16 + (s >> 4), b = bt * 16 + (s & 15);
-        valid[i] = f < n_freq && b < n_beams;
-        vals[i] = 0.f;
-        if (valid[i]) {
-            vals[i] = in[(static_cast<size_t>(win) * n_freq + f) * n_beams + b];
-            if (!isfinite(vals[i])) {
-                nonfinite = true;
-            } else {
-                mn = fminf(mn, vals[i]);
-                mx = fmaxf(mx, vals[i]);
-            }
-        }
-    }
-    nonfinite = __any_sync(0xffffffffu, nonfinite);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
-        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    }
-    float offset = 0.f, scale = 0.f;
-    if (!nonfinite && isfinite(mn) && isfinite(mx)) {
-        scale = __fdiv_rn(__fsub_rn(mx, mn), 255.0f);
-        offset = __fsub_rn(mn, __fmul_rn(-127.5f, scale));
-        if (!isfinite(offset) || !isfinite(scale)) offset = scale = 0.f;
-    }
-    if (lane == 0) params[chunk] = make_float2(offset, scale);
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        if (!valid[i]) continue;
-        const int s = lane + 32 * i;
-        const int f = ft * 16 + (s >> 4), b = bt * 16 + (s & 15);
-        int code = 0;
-        if (!isfinite(vals[i])) {
-            code = -128;
-        } else if (scale != 0.f) {
-            code = __float2int_rn(__fdiv_rn(__fsub_rn(vals[i], offset), scale));
-            code = max(-127, min(127, code));
-        }
-        codes[(static_cast<size_t>(win) * n_freq + f) * n_beams + b] = static_cast<int8_t>(code);
-    }
+    quantize_chunk<false>(in, codes, params, static_cast<size_t>(chunk), win, n_freq, n_beams, ft, bt, lane);
 }
 
 }  // namespace

@@ -77,6 +77,8 @@ _SIGS = {
     "bf_prepare_split_weights": (C.c_int, [_P, _P, _P, C.POINTER(Dims), _U64]),
     "bf_grid_tensor_integrated": (C.c_int, [_P, _P, _P, _P, _P, _P, C.POINTER(Dims), _U64, _U64]),
     "bf_tracker": (C.c_int, [_P, C.c_int, _P, _P, _P, _P, _P, _P, C.POINTER(Dims), _U64]),
+    "bf_grid_tensor_workspace_bytes": (_U64, [C.POINTER(Dims), _U64, _U64]),
+    "bf_grid_tensor_quantized": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, C.POINTER(Dims), _U64, _U64]),
     "bf_take_device_error": (C.c_int, [C.POINTER(C.c_uint32)]),
     "bf_generate_voltage": (C.c_int, [_P, _U64, _U64, C.c_float, _P, _U64, _P, C.POINTER(Dims)]),
 }

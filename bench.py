@@ -252,9 +252,12 @@ def run_gpu(args):
     if kernel == "tensor":
         split = torch.empty(api.split_weight_bytes(d, N_SHARDS), dtype=torch.uint8, device=dev)
         api.prepare_split_weights(None, weights, split, d, N_SHARDS)
+        workspace = torch.empty(api.grid_tensor_workspace_bytes(d, S_INT, N_SHARDS), dtype=torch.uint8,
+                                device=dev)
     torch.cuda.synchronize()
 
-    main_events = []
+    main_events = []  # CUDA events around the dominant kernel of each timed step
+    qd_all = api.Dimensions(N_SHARDS * W, F_SHARD, N_ANT, N_BEAMS)  # [shard][W] == [shard * W + w]
 
     def step(record=False):
         if record:
@@ -262,8 +265,23 @@ def run_gpu(args):
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
         if kernel == "tensor":
-            api.grid_tensor_integrated(None, volt, split, integ, codes, params, d, S_INT, N_SHARDS)
-            launches = 1
+            if args.fused_quant:
+                # one kernel: beamform, |.|^2, integration and int8 quantization fused
+                api.grid_tensor_quantized(None, volt, split, integ, codes, params, workspace, d, S_INT,
+                                          N_SHARDS)
+                if record:
+                    e1.record(stream)
+                launches = 1
+            else:
+                # tensor kernel (beamform, |.|^2, integration), then the int8 chunk quantizer
+                api.grid_tensor_integrated(None, volt, split, integ, None, None, d, S_INT, N_SHARDS)
+                if record:
+                    e1.record(stream)
+                api.launch_quantize_integrated_intensity(None, integ, codes, params, qd_all)
+                launches = 2
+            if record:
+                main_events.append((e0, e1))
+            return launches
         else:
             launches = 0
             for s in range(N_SHARDS):
@@ -655,6 +673,8 @@ def main():
     ap.add_argument("--kernel", default="tensor", choices=["tensor", "tiled", "stream", "exact"])
     ap.add_argument("--shards", type=int, default=N_SHARDS, choices=[1, 2])
     ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--fused-quant", action="store_true",
+                    help="quantize inside the tensor kernel's epilogue (slower today; see DESIGN.md)")
     ap.add_argument("--t-spectra", type=int, default=TR_T, help="tracker workload length (profiling)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -142,6 +142,25 @@ BF_API bf_status bf_grid_tensor_integrated(void* stream, const uint8_t* packed_v
                                            int8_t* codes, float* params, const bf_dims* dims,
                                            uint64_t integration_spectra, uint64_t n_shards);
 
+/* Bytes of scratch bf_grid_tensor_quantized needs (one 32-bit arrival counter
+ * per window and 16-channel group of every shard). */
+BF_API uint64_t bf_grid_tensor_workspace_bytes(const bf_dims* dims, uint64_t integration_spectra,
+                                               uint64_t n_shards);
+
+/* bf_grid_tensor_integrated with the int8 chunk quantizer fused into the
+ * kernel's epilogue: a chunk spans 16 channels owned by different CTAs, so
+ * the CTA that finishes the last channel of a (window, 16-channel group)
+ * quantizes that group's chunks.  `workspace` (bf_grid_tensor_workspace_bytes,
+ * device memory owned by the caller) holds the arrival counters; the call
+ * clears it on the stream before the kernel runs.  Codes and parameters are
+ * identical to launch_quantize_integrated_intensity on the same integrated
+ * output (src/quantization.cpp:61-161). */
+BF_API bf_status bf_grid_tensor_quantized(void* stream, const uint8_t* packed_voltage,
+                                          const void* split_weights, float* integrated,
+                                          int8_t* codes, float* params, void* workspace,
+                                          const bf_dims* dims, uint64_t integration_spectra,
+                                          uint64_t n_shards);
+
 /* Reads and clears the device-side error word of the tensor-core kernels
  * (0 = no error).  Every wait inside those kernels is bounded; a wait that
  * runs out sets a bit here (and the kernel returns) instead of hanging.

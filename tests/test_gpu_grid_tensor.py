@@ -108,6 +108,41 @@ def test_tensor_grid_known_answers(cuda, orc):
     assert np.all(got == np.float32(S * A * A * 113))
 
 
+@pytest.mark.parametrize("A,B,T,S,shards", [(64, 128, 700, 320, 2), (32, 40, 1024, 32, 1),
+                                            (64, 17, 300, 64, 1)])
+def test_fused_quantization_matches_separate(cuda, orc, A, B, T, S, shards):
+    """The epilogue-fused quantizer gives the same codes and parameters as the
+    stand-alone quantizer on the same integrated output (bit for bit)."""
+    from beamform_project_b200 import api, native
+    torch = cuda
+    d = api.Dimensions(T, F, A, B)
+    W = -(-T // S)
+    qd = api.Dimensions(W, F, A, B)
+    v = torch.from_numpy(np.stack([random_voltage(T, F, A, seed=s + 40) for s in range(shards)])).cuda()
+    w = torch.from_numpy(np.stack([grid_weights(A, F, B, seed=s + 50) for s in range(shards)])).cuda()
+    split = torch.empty(api.split_weight_bytes(d, shards), dtype=torch.uint8, device="cuda")
+    api.prepare_split_weights(None, w, split, d, shards)
+    n_out = shards * W * F * B
+    n_par = shards * 2 * api.quantization_parameter_count(qd)
+    integ = torch.empty(n_out, dtype=torch.float32, device="cuda")
+    codes = torch.full((n_out,), 99, dtype=torch.int8, device="cuda")
+    params = torch.full((n_par,), -1.0, dtype=torch.float32, device="cuda")
+    ws = torch.full((api.grid_tensor_workspace_bytes(d, S, shards),), 7, dtype=torch.uint8, device="cuda")
+    for _ in range(2):  # the second call reuses the (dirty) workspace
+        api.grid_tensor_quantized(None, v, split, integ, codes, params, ws, d, S, shards)
+        torch.cuda.synchronize()
+        assert native.take_device_error() == 0
+        ref_codes = torch.empty_like(codes)
+        ref_params = torch.empty_like(params)
+        api.launch_quantize_integrated_intensity(None, integ, ref_codes, ref_params,
+                                                 api.Dimensions(shards * W, F, A, B))
+        torch.cuda.synchronize()
+        assert torch.equal(codes, ref_codes)
+        assert torch.equal(params, ref_params)
+        got = integ.cpu().numpy().reshape(shards, W, F, B)
+        _check(orc, got[0], v[0].cpu().numpy(), w[0].cpu().numpy(), T, A, B, S)
+
+
 def test_tensor_grid_repeatable(cuda, orc):
     from beamform_project_b200 import api
     T, A, B, S = 1280, 64, 128, 320
