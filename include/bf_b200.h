@@ -161,6 +161,25 @@ BF_API bf_status bf_grid_tensor_quantized(void* stream, const uint8_t* packed_vo
                                           const bf_dims* dims, uint64_t integration_spectra,
                                           uint64_t n_shards);
 
+/* bf_grid_tensor_quantized for callers that cannot allocate device memory
+ * (device memory fixed at start-up, or an FFI caller holding only a stream
+ * and its data buffers).  No counterpart in the reference.
+ * The scratch is a fixed array inside this library (64 KiB on every GPU that
+ * uses it, held until the process exits), so the request may need at most
+ * 16384 counters: n_shards * ceil(n_time / integration_spectra) *
+ * ceil(n_freq / 16) <= 16384; larger requests fail with
+ * BF_ERR_INVALID_ARGUMENT.  The call allocates nothing: it clears the
+ * counters it uses on the stream, then launches.  The first call on a device
+ * looks up that device's address of the array; make that first call before
+ * any stream capture.  All calls share the one array, which keeps the last
+ * call's counts: calls whose kernels overlap on the GPU (different streams,
+ * or different host threads on one device) race on it and must be
+ * serialised by the caller. */
+BF_API bf_status bf_grid_tensor_quantized_static(void* stream, const uint8_t* packed_voltage,
+                                                 const void* split_weights, float* integrated,
+                                                 int8_t* codes, float* params, const bf_dims* dims,
+                                                 uint64_t integration_spectra, uint64_t n_shards);
+
 /* Reads and clears the device-side error word of the tensor-core kernels
  * (0 = no error).  Every wait inside those kernels is bounded; a wait that
  * runs out sets a bit here (and the kernel returns) instead of hanging.
