@@ -260,6 +260,46 @@ def tracker(stream, mode, packed_voltage, positions, wave_numbers, window_direct
 
 
 # --------------------------------------------------------------------------
+# DOA (CpuOptBeamTracker's covariance and scan, cpu_opt_beam_tracker.hpp:91-169)
+# --------------------------------------------------------------------------
+
+def doa_covariance_i32(stream, packed_voltage, covariance, dims: Dimensions, block_len: int) -> None:
+    """Exact int32 block covariance [blocks][F][A][A][2] on int8 tensor cores."""
+    torch = _torch()
+    validate_dimensions(dims)
+    B = dims.n_time // block_len if block_len else 0
+    v = _dev(packed_voltage, "packed_voltage", torch.uint8, dims.n_time * dims.n_freq * dims.n_ant)
+    c = _dev(covariance, "covariance", torch.int32, B * dims.n_freq * dims.n_ant * dims.n_ant * 2)
+    d = dims.c()
+    check(native.lib().bf_doa_covariance_i32(_stream_handle(stream), v, c, C.byref(d), int(block_len)))
+
+
+def doa_workspace_bytes(dims: Dimensions, block_len: int, subarray: int) -> int:
+    d = dims.c()
+    return int(native.lib().bf_doa_workspace_bytes(C.byref(d), int(block_len), int(subarray)))
+
+
+def doa_scan(stream, covariance, positions, wave_numbers, dims: Dimensions, block_len: int, subarray: int,
+             forgetting: float, diag_load: float, l_first: float, l_step: float, n_points: int,
+             m_fixed: float, bartlett, capon, l_est, workspace) -> None:
+    torch = _torch()
+    validate_dimensions(dims)
+    B = dims.n_time // block_len if block_len else 0
+    M = subarray if 0 < subarray < dims.n_ant else dims.n_ant
+    c = _dev(covariance, "covariance", torch.int32, B * dims.n_freq * dims.n_ant * dims.n_ant * 2)
+    pp = _dev(positions, "positions", torch.float32, 3 * M)
+    k = _dev(wave_numbers, "wave_numbers", torch.float64, dims.n_freq)
+    b = _dev(bartlett, "bartlett", torch.float64, B * n_points)
+    cp = _dev(capon, "capon", torch.float64, B * n_points)
+    le = _dev(l_est, "l_est", torch.float64, 2 * B)
+    w = _dev(workspace, "workspace", torch.uint8, doa_workspace_bytes(dims, block_len, subarray))
+    d = dims.c()
+    check(native.lib().bf_doa_scan(_stream_handle(stream), c, pp, k, C.byref(d), int(block_len), int(subarray),
+                                   float(forgetting), float(diag_load), float(l_first), float(l_step),
+                                   int(n_points), float(m_fixed), b, cp, le, w))
+
+
+# --------------------------------------------------------------------------
 # synthetic voltages
 # --------------------------------------------------------------------------
 

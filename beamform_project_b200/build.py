@@ -26,7 +26,7 @@ NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibilit
               "--expt-relaxed-constexpr", "-Xptxas", "-v"] + ARCH
 
 CUDA_SOURCES = ["capi.cu", "grid_exact.cu", "quantize.cu", "generate.cu", "tracker.cu",
-                "tracker_stream.cu", "grid_tc.cu", "no_alloc.cu"]
+                "tracker_stream.cu", "grid_tc.cu", "no_alloc.cu", "doa_cov.cu", "doa_scan.cu"]
 CXX_SOURCES = ["cxx_api.cpp"]
 
 

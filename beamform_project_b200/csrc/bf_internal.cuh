@@ -120,6 +120,13 @@ bf_status launch_generate(cudaStream_t stream, uint64_t seed, uint64_t offset, f
 bf_status launch_tracker(cudaStream_t stream, int mode, const uint8_t* v, const float* pos,
                          const double* k, const float* dirs, float* intensity, float* integrated,
                          const bf_dims& d, uint64_t spectra);
+bf_status launch_doa_covariance(cudaStream_t stream, const uint8_t* v, int32_t* out, const bf_dims& d,
+                                uint64_t block_len);
+uint64_t doa_workspace_bytes(uint64_t n_blocks, uint64_t n_freq, uint64_t M);
+bf_status launch_doa_scan(cudaStream_t stream, const int32_t* R, const float* pos, const double* kw,
+                          const bf_dims& d, uint64_t block_len, uint64_t subarray, double lam, double load,
+                          double l_first, double l_step, uint64_t n, double m_fixed, double* bartlett,
+                          double* capon, double* l_est, void* workspace);
 uint64_t split_weight_bytes(const bf_dims& d, uint64_t n_shards);
 bf_status launch_prepare_split(cudaStream_t stream, const float* w, void* split, const bf_dims& d,
                                uint64_t n_shards);

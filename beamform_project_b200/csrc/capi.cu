@@ -273,6 +273,52 @@ BF_API bf_status bf_tracker(void* stream, int mode, const uint8_t* packed_voltag
                           integration_spectra);
 }
 
+BF_API bf_status bf_doa_covariance_i32(void* stream, const uint8_t* packed_voltage,
+                                       int32_t* covariance, const bf_dims* dims, uint64_t block_len) {
+    clear_error();
+    BF_TRY(validate_dims(dims));
+    if (dims->n_beams != 1) return set_error(BF_ERR_INVALID_ARGUMENT, "the DOA path takes n_beams == 1");
+    BF_TRY(check_ptr(packed_voltage, 16, "packed_voltage"));
+    BF_TRY(check_ptr(covariance, 8, "covariance"));
+    return launch_doa_covariance(static_cast<cudaStream_t>(stream), packed_voltage, covariance, *dims,
+                                 block_len);
+}
+
+BF_API uint64_t bf_doa_workspace_bytes(const bf_dims* dims, uint64_t block_len, uint64_t subarray) {
+    if (dims == nullptr || block_len == 0) return 0;
+    const uint64_t M = (subarray > 0 && subarray < dims->n_ant) ? subarray : dims->n_ant;
+    return doa_workspace_bytes(dims->n_time / block_len, dims->n_freq, M);
+}
+
+BF_API bf_status bf_doa_scan(void* stream, const int32_t* covariance, const float* positions,
+                             const double* wave_numbers, const bf_dims* dims, uint64_t block_len,
+                             uint64_t subarray, double forgetting, double diag_load, double l_first,
+                             double l_step, uint64_t n_points, double m_fixed, double* bartlett,
+                             double* capon, double* l_est, void* workspace) {
+    clear_error();
+    BF_TRY(validate_dims(dims));
+    if (dims->n_beams != 1) return set_error(BF_ERR_INVALID_ARGUMENT, "the DOA path takes n_beams == 1");
+    if (block_len == 0 || dims->n_time % block_len != 0) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "block_len must divide n_time");
+    }
+    if (!(forgetting > 0.0 && forgetting <= 1.0)) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "forgetting factor must be in (0, 1]");
+    }
+    if (!(diag_load >= 0.0) || n_points == 0 || n_points > (1u << 24)) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "diag_load must be >= 0 and n_points in [1, 2^24]");
+    }
+    BF_TRY(check_ptr(covariance, 8, "covariance"));
+    BF_TRY(check_ptr(positions, 4, "positions"));
+    BF_TRY(check_ptr(wave_numbers, 8, "wave_numbers"));
+    BF_TRY(check_ptr(bartlett, 8, "bartlett"));
+    BF_TRY(check_ptr(capon, 8, "capon"));
+    BF_TRY(check_ptr(l_est, 8, "l_est"));
+    BF_TRY(check_ptr(workspace, 16, "workspace"));
+    return launch_doa_scan(static_cast<cudaStream_t>(stream), covariance, positions, wave_numbers, *dims,
+                           block_len, subarray, forgetting, diag_load, l_first, l_step, n_points, m_fixed,
+                           bartlett, capon, l_est, workspace);
+}
+
 BF_API bf_status bf_take_device_error(uint32_t* code) {
     clear_error();
     return take_tc_error(code);

@@ -1,0 +1,317 @@
+// doa_cov.cu -- exact per-block array covariance on int8 tensor cores.
+//
+// Reference: CpuOptBeamTracker forms, per frequency and block of K snapshots,
+// R[f] = (1/K) sum_k x_k x_k^H in std::complex<float>
+// (src/cpu_opt_beam_tracker.cpp:559-602).  Here the block sums are formed
+// exactly in INT32:
+//   R_blk[b][f][i][j] = sum_{t in block b} x_i(t) * conj(x_j(t))
+// (re, im) as int32, for the full A x A Hermitian matrix.  Spatial smoothing,
+// forward-backward averaging, 1/K, diagonal loading and forgetting are linear
+// and run afterwards in FP64 (doa_scan.cu).
+//
+// Formulation: with y(t) the 2A real components (re, im interleaved) of x(t),
+// the Gram matrix G = sum_t y(t) y(t)^T is one tcgen05 kind::i8 GEMM per
+// (block, channel): M = N = 128 components (zero padded for 32 antennas),
+// K = time.  The unpacked tile [t][128 int8] is MN-major for both operands,
+// so one shared-memory tile feeds A and B.  R assembles from G in the
+// epilogue: Re R_ij = G_{2i,2j} + G_{2i+1,2j+1}, Im R_ij = G_{2i+1,2j} -
+// G_{2i,2j+1}.  |x| <= 8 per component, so every sum stays below 2^31 for
+// blocks of up to 2^24 spectra.
+//
+// CTA: warp 0 TMA producer (raw 128-spectrum tiles), warp 1 MMA issuer and
+// TMEM owner, warps 2-3 unpack (int4 -> int8, 128-byte swizzle), warps 4-7
+// epilogue (one 128 x 128 int32 accumulator per (block, channel), two TMEM
+// stages).  All waits are bounded and report through the device error word.
+#include "bf_internal.cuh"
+#include "sm100.cuh"
+
+#include <cuda.h>
+
+#include <algorithm>
+#include <mutex>
+
+namespace bf {
+
+extern __device__ unsigned int g_tc_error;
+
+namespace {
+
+using namespace sm100;
+
+constexpr int kThreads = 256;
+constexpr int kTile = 128;        // spectra per tile
+constexpr int kRawStages = 4;
+constexpr int kXStages = 3;
+constexpr uint32_t kXBytes = kTile * 128;  // one unpacked tile
+constexpr uint64_t kWaitNs = 2000000000ull;
+
+struct CovParams {
+    int32_t* out;             // [blocks][F][A][A][2]
+    int n_freq, n_ant, block_len, n_blocks, tiles_per_block;
+    long long n_units;
+};
+
+__device__ __forceinline__ void cov_error(unsigned code) { atomicOr(&g_tc_error, code << 16); }
+
+// 8 packed bytes (antennas 8c..8c+7) -> 16 int8 components (re, im interleaved).
+__device__ __forceinline__ uint4 expand8(uint32_t w0, uint32_t w1) {
+    auto two = [](uint32_t w, uint32_t& a, uint32_t& b) {
+        const uint32_t lo = w & 0x0F0F0F0Fu, hi = (w >> 4) & 0x0F0F0F0Fu;
+        uint32_t x, y;
+        asm("prmt.b32 %0, %1, %2, 0x5140;" : "=r"(x) : "r"(lo), "r"(hi));
+        asm("prmt.b32 %0, %1, %2, 0x7362;" : "=r"(y) : "r"(lo), "r"(hi));
+        // signed nibble -> int8: (n ^ 8) - 8 in every byte
+        a = __vsub4(x ^ 0x08080808u, 0x08080808u);
+        b = __vsub4(y ^ 0x08080808u, 0x08080808u);
+    };
+    uint4 r;
+    two(w0, r.x, r.y);
+    two(w1, r.z, r.w);
+    return r;
+}
+
+template <int A>
+__global__ void __launch_bounds__(kThreads, 1)
+doa_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovParams p) {
+    constexpr uint32_t RAW = kTile * A;
+    constexpr uint32_t IDESC = idesc_s8_s32_mn(128, 128);
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* xs = smem;                                  // kXStages x 16 KiB
+    uint8_t* raw = smem + kXStages * kXBytes;            // kRawStages x RAW
+    uint64_t* bars = reinterpret_cast<uint64_t*>(raw + kRawStages * RAW);
+    uint64_t* raw_full = bars;                           // [kRawStages]
+    uint64_t* raw_empty = bars + kRawStages;             // [kRawStages]
+    uint64_t* x_full = bars + 2 * kRawStages;            // [kXStages]
+    uint64_t* x_empty = x_full + kXStages;               // [kXStages]
+    uint64_t* acc_full = x_empty + kXStages;             // [2]
+    uint64_t* acc_empty = acc_full + 2;                  // [2]
+    uint64_t* mma_done = acc_empty + 2;
+    uint32_t* tmem_ptr = reinterpret_cast<uint32_t*>(mma_done + 1);
+    volatile int* s_fail = reinterpret_cast<volatile int*>(mma_done + 2);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < kRawStages; ++i) {
+            mbar_init(&raw_full[i], 1);
+            mbar_init(&raw_empty[i], 2);
+        }
+        for (int i = 0; i < kXStages; ++i) {
+            mbar_init(&x_full[i], 2);
+            mbar_init(&x_empty[i], 1);
+        }
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(&acc_full[i], 1);
+            mbar_init(&acc_empty[i], 4);
+        }
+        mbar_init(mma_done, 1);
+        *s_fail = 0;
+        fence_mbar_init();
+    }
+    if (warp == 1) tmem_alloc(tmem_ptr, 256);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_ptr;
+
+    const long long u_begin = p.n_units * blockIdx.x / gridDim.x;
+    const long long u_end = p.n_units * (blockIdx.x + 1) / gridDim.x;
+    auto fail = [&](unsigned code) {
+        cov_error(code);
+        *s_fail = 1;
+    };
+
+    if (warp == 0) {
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            int armed[kRawStages];
+            for (int s = 0; s < kRawStages; ++s) armed[s] = -1;
+            bool stop = false;
+            for (long long u = u_begin; u < u_end && !stop; ++u) {
+                const int b = static_cast<int>(u / p.n_freq), f = static_cast<int>(u % p.n_freq);
+                for (int k = 0; k < p.tiles_per_block; ++k) {
+                    if (*s_fail) { stop = true; break; }
+                    if (!mbar_wait(&raw_empty[stage], phase ^ 1, kWaitNs)) { fail(1); stop = true; break; }
+                    mbar_expect_tx(&raw_full[stage], RAW);
+                    tma_load_4d(raw + stage * RAW, &vmap, 0, f, b * p.block_len + k * kTile, 0, &raw_full[stage]);
+                    armed[stage] = static_cast<int>(phase);
+                    if (++stage == kRawStages) { stage = 0; phase ^= 1; }
+                }
+            }
+            for (int s = 0; s < kRawStages; ++s) {
+                if (armed[s] >= 0 && !mbar_wait(&raw_full[s], static_cast<uint32_t>(armed[s]), kWaitNs)) fail(2);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            int xst = 0, ast = 0;
+            uint32_t xph = 0, aph = 0;
+            bool stop = false;
+            for (long long u = u_begin; u < u_end && !stop; ++u) {
+                if (!mbar_wait(&acc_empty[ast], aph ^ 1, kWaitNs)) { fail(4); break; }
+                tc_fence_after();
+                const uint32_t d_tmem = tmem_base + ast * 128;
+                for (int k = 0; k < p.tiles_per_block; ++k) {
+                    if (*s_fail) { stop = true; break; }
+                    if (!mbar_wait(&x_full[xst], xph, kWaitNs)) { fail(8); stop = true; break; }
+                    tc_fence_after();
+                    const uint32_t xa = smem_u32(xs + xst * kXBytes);
+#pragma unroll
+                    for (int kk = 0; kk < kTile / 32; ++kk) {
+                        const uint64_t desc = smem_desc_sw128_mn(xa + kk * 32 * 128);
+                        mma_i8_ss(d_tmem, desc, desc, IDESC, (k > 0 || kk > 0) ? 1u : 0u);
+                    }
+                    tc_commit(&x_empty[xst]);
+                    if (++xst == kXStages) { xst = 0; xph ^= 1; }
+                }
+                if (stop) break;
+                tc_commit(&acc_full[ast]);
+                if (++ast == 2) { ast = 0; aph ^= 1; }
+            }
+            tc_commit(mma_done);
+            if (!mbar_wait(mma_done, 0, kWaitNs)) fail(16);
+        }
+    } else if (warp < 4) {
+        const int ut = threadIdx.x - 64;  // 0..63
+        int stage = 0, xst = 0;
+        uint32_t phase = 0, xph = 0;
+        bool stop = false;
+        constexpr int kChunks = A / 8;   // 8-antenna chunks per spectrum
+        for (long long u = u_begin; u < u_end && !stop; ++u) {
+            for (int k = 0; k < p.tiles_per_block; ++k) {
+                if (*s_fail) { stop = true; break; }
+                if (!mbar_wait(&raw_full[stage], phase, kWaitNs)) { fail(32); stop = true; break; }
+                if (!mbar_wait(&x_empty[xst], xph ^ 1, kWaitNs)) { fail(64); stop = true; break; }
+                const uint8_t* rsrc = raw + stage * RAW;
+                uint8_t* xdst = xs + xst * kXBytes;
+                for (int idx = ut; idx < kTile * 8; idx += 64) {
+                    const int r = idx >> 3, c = idx & 7;   // spectrum, 16-component chunk
+                    uint4 v = make_uint4(0, 0, 0, 0);
+                    if (c < kChunks) {
+                        const uint2 w = *reinterpret_cast<const uint2*>(rsrc + r * A + c * 8);
+                        v = expand8(w.x, w.y);
+                    }
+                    *reinterpret_cast<uint4*>(xdst + r * 128 + ((c ^ (r & 7)) << 4)) = v;
+                }
+                fence_proxy_async_smem();
+                __syncwarp();
+                if (lane == 0) {
+                    mbar_arrive(&raw_empty[stage]);
+                    mbar_arrive(&x_full[xst]);
+                }
+                if (++stage == kRawStages) { stage = 0; phase ^= 1; }
+                if (++xst == kXStages) { xst = 0; xph ^= 1; }
+            }
+        }
+    } else {
+        const int q4 = warp & 3;
+        const int m = 32 * q4 + lane;       // component row of G
+        const int i = m >> 1, comp = m & 1; // antenna, 0 = re / 1 = im part of R
+        int ast = 0;
+        uint32_t aph = 0;
+        bool stop = false;
+        for (long long u = u_begin; u < u_end && !stop; ++u) {
+            if (!mbar_wait(&acc_full[ast], aph, kWaitNs)) { fail(128); break; }
+            tc_fence_after();
+            const int b = static_cast<int>(u / p.n_freq), f = static_cast<int>(u % p.n_freq);
+            int32_t* row = p.out + ((static_cast<size_t>(b) * p.n_freq + f) * A + i) * A * 2;
+            const uint32_t taddr = tmem_base + ((32u * q4) << 16) + ast * 128;
+#pragma unroll 1
+            for (int c = 0; c < 4; ++c) {
+                uint32_t g[32];
+                tmem_ld_32x32b_x32(taddr + 32 * c, g);
+                tmem_ld_wait();
+#pragma unroll
+                for (int jj = 0; jj < 16; ++jj) {
+                    const int j = 16 * c + jj;
+                    const int32_t own = static_cast<int32_t>(g[2 * jj]);
+                    const int32_t recv = __shfl_xor_sync(0xffffffffu, static_cast<int32_t>(g[2 * jj + 1]), 1);
+                    const int32_t val = comp == 0 ? own + recv : own - recv;
+                    if (i < A && j < A) row[2 * j + comp] = val;
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&acc_empty[ast]);
+            if (++ast == 2) { ast = 0; aph ^= 1; }
+            stop = *s_fail != 0;
+        }
+    }
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        tmem_dealloc(tmem_base, 256);
+    }
+}
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*,
+                                   CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                   CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn_cov() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* ptr = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &ptr, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess) {
+            fn = reinterpret_cast<EncodeTiledFn>(ptr);
+        }
+    });
+    return fn;
+}
+
+template <int A>
+bf_status launch_cov(cudaStream_t stream, const CUtensorMap& map, const CovParams& p) {
+    const size_t smem = kXStages * kXBytes + kRawStages * kTile * A + 256 + 1024;
+    auto kern = doa_cov_kernel<A>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_status(e, "doa_cov_kernel smem attribute");
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = static_cast<int>(std::min<long long>(sms, p.n_units));
+    kern<<<grid, kThreads, smem, stream>>>(map, p);
+    return cuda_status(cudaGetLastError(), "doa_cov_kernel launch");
+}
+
+}  // namespace
+
+bf_status launch_doa_covariance(cudaStream_t stream, const uint8_t* v, int32_t* out, const bf_dims& d,
+                                uint64_t block_len) {
+    if (d.n_ant != 32 && d.n_ant != 64) {
+        return set_error(BF_ERR_UNSUPPORTED, "the tensor-core covariance supports n_ant 32 or 64");
+    }
+    if (block_len == 0 || block_len % kTile != 0 || d.n_time % block_len != 0) {
+        return set_error(BF_ERR_INVALID_ARGUMENT,
+                         "block length must be a positive multiple of 128 that divides n_time");
+    }
+    if (block_len > (1ull << 24) || d.n_time >= (1ull << 31)) {
+        return set_error(BF_ERR_OVERFLOW, "covariance block or stream too long for int32 sums");
+    }
+    EncodeTiledFn enc = encode_fn_cov();
+    if (enc == nullptr) return set_error(BF_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
+    CUtensorMap map;
+    const cuuint64_t dims[4] = {d.n_ant, d.n_freq, d.n_time, 1};
+    const cuuint64_t strides[3] = {d.n_ant, d.n_freq * d.n_ant, d.n_time * d.n_freq * d.n_ant};
+    const cuuint32_t box[4] = {static_cast<cuuint32_t>(d.n_ant), 1, static_cast<cuuint32_t>(kTile), 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, const_cast<uint8_t*>(v), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_error(BF_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string(r));
+    CovParams p{};
+    p.out = out;
+    p.n_freq = static_cast<int>(d.n_freq);
+    p.n_ant = static_cast<int>(d.n_ant);
+    p.block_len = static_cast<int>(block_len);
+    p.n_blocks = static_cast<int>(d.n_time / block_len);
+    p.tiles_per_block = static_cast<int>(block_len / kTile);
+    p.n_units = static_cast<long long>(p.n_blocks) * d.n_freq;
+    return d.n_ant == 32 ? launch_cov<32>(stream, map, p) : launch_cov<64>(stream, map, p);
+}
+
+}  // namespace bf

@@ -115,6 +115,17 @@ __device__ __forceinline__ void mma_f16_ss(uint32_t d_tmem, uint64_t a_desc, uin
         : "memory");
 }
 
+// D[tmem] (+)= A[smem] * B[smem], kind::i8 (signed int8 in, int32 out), cta_group::1.
+__device__ __forceinline__ void mma_i8_ss(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc,
+                                          uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
 // Arrive on `bar` once every tcgen05 operation issued so far by this thread completes.
 __device__ __forceinline__ void tc_commit(uint64_t* bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
@@ -150,6 +161,29 @@ __device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t smem_addr) {
     d |= static_cast<uint64_t>(1u) << 46;                      // descriptor version
     d |= static_cast<uint64_t>(2u) << 61;                      // SWIZZLE_128B
     return d;
+}
+
+// Shared-memory matrix descriptor, MN-major operand in the 128-byte swizzle
+// layout: each K row is 128 bytes of M (or N) elements, 8-row groups 1024
+// bytes apart (SBO); a single 128-byte MN chunk, so no leading offset.
+__device__ __forceinline__ uint64_t smem_desc_sw128_mn(uint32_t smem_addr) {
+    uint64_t d = 0;
+    d |= static_cast<uint64_t>((smem_addr >> 4) & 0x3FFFu);
+    d |= static_cast<uint64_t>(1024u >> 4) << 32;
+    d |= static_cast<uint64_t>(1u) << 46;
+    d |= static_cast<uint64_t>(2u) << 61;
+    return d;
+}
+
+// Instruction descriptor: kind::i8, A = B = signed int8, D = s32, both MN-major.
+__host__ __device__ constexpr uint32_t idesc_s8_s32_mn(uint32_t m, uint32_t n) {
+    return (2u << 4)            // D format s32
+           | (1u << 7)          // A signed int8
+           | (1u << 10)         // B signed int8
+           | (1u << 15)         // A MN-major
+           | (1u << 16)         // B MN-major
+           | ((n >> 3) << 17)
+           | ((m >> 4) << 24);
 }
 
 // Instruction descriptor: kind::f16, A = B = f16, D = f32, both K-major.

@@ -80,6 +80,10 @@ _SIGS = {
     "bf_grid_tensor_workspace_bytes": (_U64, [C.POINTER(Dims), _U64, _U64]),
     "bf_grid_tensor_quantized": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, C.POINTER(Dims), _U64, _U64]),
     "bf_take_device_error": (C.c_int, [C.POINTER(C.c_uint32)]),
+    "bf_doa_covariance_i32": (C.c_int, [_P, _P, _P, C.POINTER(Dims), _U64]),
+    "bf_doa_workspace_bytes": (_U64, [C.POINTER(Dims), _U64, _U64]),
+    "bf_doa_scan": (C.c_int, [_P, _P, _P, _P, C.POINTER(Dims), _U64, _U64, C.c_double, C.c_double,
+                              C.c_double, C.c_double, _U64, C.c_double, _P, _P, _P, _P]),
     "bf_generate_voltage": (C.c_int, [_P, _U64, _U64, C.c_float, _P, _U64, _P, C.POINTER(Dims)]),
 }
 

@@ -208,6 +208,41 @@ BF_API bf_status bf_tracker(void* stream, int mode, const uint8_t* packed_voltag
                             uint64_t integration_spectra);
 
 /* ------------------------------------------------------------------------ */
+/* DOA: covariance and Bartlett / Capon scan.  Reference: CpuOptBeamTracker */
+/* (include/beamformer/cpu_opt_beam_tracker.hpp:91-169, src/cpu_opt_beam_   */
+/* tracker.cpp:226-850, 1619-2454).  dims: n_time = blocks * block_len,     */
+/* n_beams = 1.                                                             */
+/* ------------------------------------------------------------------------ */
+
+/* Exact per-block covariance on int8 tensor cores (tcgen05 kind::i8):
+ * covariance[b][f][i][j] = sum over the block's spectra of x_i * conj(x_j),
+ * (re, im) int32, full A x A Hermitian (A = 32 or 64; block_len a multiple
+ * of 128 dividing n_time).  Replaces the float sums of
+ * spatial_smoothed_covariance_into (src/cpu_opt_beam_tracker.cpp:559-602),
+ * which equal these sums times 1/K. */
+BF_API bf_status bf_doa_covariance_i32(void* stream, const uint8_t* packed_voltage,
+                                       int32_t* covariance, const bf_dims* dims,
+                                       uint64_t block_len);
+
+/* Scratch bytes bf_doa_scan needs. */
+BF_API uint64_t bf_doa_workspace_bytes(const bf_dims* dims, uint64_t block_len,
+                                       uint64_t subarray);
+
+/* FP64 smoothing (sub-arrays of `subarray` elements along the element index,
+ * 0 = none), forward-backward averaging, diagonal loading diag_load*tr/M,
+ * forgetting (S = forgetting*S + (1-forgetting)*R_block per block), FP64
+ * Cholesky, and Bartlett / Capon powers on the grid l = l_first + i*l_step
+ * (i < n_points) at m = m_fixed, summed over frequency; then the argmax and
+ * parabolic peak of each block.  positions: [subarray][3] float (device) of
+ * sub-array 0; wave_numbers [F] double.  Outputs (device): bartlett, capon
+ * [blocks][n_points] double; l_est [blocks][2] double (Bartlett, Capon). */
+BF_API bf_status bf_doa_scan(void* stream, const int32_t* covariance, const float* positions,
+                             const double* wave_numbers, const bf_dims* dims, uint64_t block_len,
+                             uint64_t subarray, double forgetting, double diag_load,
+                             double l_first, double l_step, uint64_t n_points, double m_fixed,
+                             double* bartlett, double* capon, double* l_est, void* workspace);
+
+/* ------------------------------------------------------------------------ */
 /* Seeded synthetic voltages (no reference counterpart)      */
 /* ------------------------------------------------------------------------ */
 

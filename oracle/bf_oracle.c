@@ -354,6 +354,156 @@ ORC_API void orc_generate_voltage(uint64_t seed, uint64_t sample_offset, size_t 
 }
 
 /* ------------------------------------------------------------------------ */
+/* DOA scan in FP64 (restates src/cpu_opt_beam_tracker.cpp in double):       */
+/*  smoothing over sub-arrays along the linear element index and             */
+/*  forward-backward averaging (:605-657), diagonal loading                  */
+/*  eps = load * tr(R) / M applied to each block before forgetting           */
+/*  (:226-237, :1866-1880), forgetting R = lam R + (1 - lam) R_blk           */
+/*  (:1763-1892), Cholesky (:398-415), Capon 1 / ||L^-1 a||^2 (:423-437),    */
+/*  Bartlett a^H R a (:287-302), steering a_i = exp(-j k (x_i l + y_i m))    */
+/*  (:96-106), powers summed over frequency.  The peak is refined by the      */
+/*  vertex of the parabola through the argmax and its neighbours (the        */
+/*  reference's quadratic_interp, :830-850, only accepts convex triples and   */
+/*  so never moves a maximum; here the concave vertex is used).              */
+/* Inputs: R [B][F][A][A][2] int64 block sums of x x^H over K spectra.       */
+/* Outputs: bartlett, capon [B][n]; l_est [B][2] (bartlett, capon).          */
+/* ------------------------------------------------------------------------ */
+ORC_API void orc_doa_scan(const int64_t* R, size_t B, size_t F, size_t A, size_t K,
+                          size_t subarray, double lam, double load, const float* pos,
+                          const double* kw, double l_first, double l_step, size_t n,
+                          double m_fixed, double* bartlett, double* capon, double* l_est) {
+    const size_t M = (subarray > 0 && subarray < A) ? subarray : A;
+    const size_t L = A - M + 1;
+    double* S = (double*)calloc(2 * F * M * M, sizeof(double)); /* folded state */
+    double* E = (double*)calloc(F, sizeof(double));
+    double* Rb = (double*)malloc(sizeof(double) * 2 * M * M);
+    double* Rt = (double*)malloc(sizeof(double) * 2 * M * M);
+    double* Lc = (double*)malloc(sizeof(double) * 2 * M * M);
+    double* ar = (double*)malloc(sizeof(double) * M);
+    double* ai = (double*)malloc(sizeof(double) * M);
+    double* vr = (double*)malloc(sizeof(double) * M);
+    double* vi = (double*)malloc(sizeof(double) * M);
+    for (size_t b = 0; b < B; ++b) {
+        for (size_t l = 0; l < n; ++l) bartlett[b * n + l] = capon[b * n + l] = 0.0;
+        for (size_t f = 0; f < F; ++f) {
+            const int64_t* Rf = R + 2 * (b * F + f) * A * A;
+            /* smoothing: mean over sub-arrays of the 1/K covariance */
+            for (size_t r = 0; r < M; ++r)
+                for (size_t c = 0; c < M; ++c) {
+                    double sr = 0.0, si = 0.0;
+                    for (size_t s = 0; s < L; ++s) {
+                        sr += (double)Rf[2 * ((s + r) * A + s + c)];
+                        si += (double)Rf[2 * ((s + r) * A + s + c) + 1];
+                    }
+                    Rt[2 * (r * M + c)] = sr / (double)K / (double)L;
+                    Rt[2 * (r * M + c) + 1] = si / (double)K / (double)L;
+                }
+            /* forward-backward: 1/2 (R + J conj(R) J) when smoothing */
+            for (size_t r = 0; r < M; ++r)
+                for (size_t c = 0; c < M; ++c) {
+                    double re = Rt[2 * (r * M + c)], im = Rt[2 * (r * M + c) + 1];
+                    if (L > 1) {
+                        const size_t pr = M - 1 - r, pc = M - 1 - c;
+                        re = 0.5 * (re + Rt[2 * (pr * M + pc)]);
+                        im = 0.5 * (im - Rt[2 * (pr * M + pc) + 1]);
+                    }
+                    Rb[2 * (r * M + c)] = re;
+                    Rb[2 * (r * M + c) + 1] = im;
+                }
+            double tr = 0.0;
+            for (size_t r = 0; r < M; ++r) tr += Rb[2 * (r * M + r)];
+            const double eps = load * tr / (double)M;
+            double* Sf = S + 2 * f * M * M;
+            if (b == 0 || lam >= 1.0) {
+                for (size_t i = 0; i < 2 * M * M; ++i) Sf[i] = Rb[i];
+                E[f] = eps;
+            } else {
+                for (size_t i = 0; i < 2 * M * M; ++i) Sf[i] = lam * Sf[i] + (1.0 - lam) * Rb[i];
+                E[f] = lam * E[f] + (1.0 - lam) * eps;
+            }
+            /* Cholesky of S + E I (lower, FP64) */
+            int ok = 1;
+            for (size_t i = 0; i < M && ok; ++i)
+                for (size_t j = 0; j <= i; ++j) {
+                    double sr = Sf[2 * (i * M + j)] + (i == j ? E[f] : 0.0);
+                    double si = Sf[2 * (i * M + j) + 1];
+                    for (size_t k = 0; k < j; ++k) {
+                        const double xr = Lc[2 * (i * M + k)], xi = Lc[2 * (i * M + k) + 1];
+                        const double yr = Lc[2 * (j * M + k)], yi = -Lc[2 * (j * M + k) + 1];
+                        sr -= xr * yr - xi * yi;
+                        si -= xr * yi + xi * yr;
+                    }
+                    if (i == j) {
+                        if (sr <= 1e-300) { ok = 0; break; }
+                        Lc[2 * (i * M + i)] = sqrt(sr);
+                        Lc[2 * (i * M + i) + 1] = 0.0;
+                    } else {
+                        const double d = Lc[2 * (j * M + j)];
+                        Lc[2 * (i * M + j)] = sr / d;
+                        Lc[2 * (i * M + j) + 1] = si / d;
+                    }
+                }
+            for (size_t l = 0; l < n; ++l) {
+                const double lv = l_first + (double)l * l_step;
+                for (size_t i = 0; i < M; ++i) {
+                    const double ph = kw[f] * ((double)pos[3 * i] * lv + (double)pos[3 * i + 1] * m_fixed);
+                    const double rr = ph - 6.283185307179586476925286766559 *
+                                               nearbyint(ph * (1.0 / 6.283185307179586476925286766559));
+                    const float rf = (float)rr;
+                    ar[i] = (double)cosf(rf);
+                    ai[i] = -(double)sinf(rf);
+                }
+                /* Bartlett: sum_rc conj(a_r) S_rc a_c */
+                double pb = 0.0;
+                for (size_t r = 0; r < M; ++r) {
+                    double tr2 = 0.0, ti2 = 0.0;
+                    for (size_t c = 0; c < M; ++c) {
+                        const double sr = Sf[2 * (r * M + c)], si = Sf[2 * (r * M + c) + 1];
+                        tr2 += sr * ar[c] - si * ai[c];
+                        ti2 += sr * ai[c] + si * ar[c];
+                    }
+                    pb += ar[r] * tr2 + ai[r] * ti2; /* Re(conj(a_r) * t) */
+                }
+                bartlett[b * n + l] += pb;
+                if (ok) {
+                    double nrm = 0.0;
+                    for (size_t i = 0; i < M; ++i) {
+                        double sr = ar[i], si = ai[i];
+                        for (size_t k = 0; k < i; ++k) {
+                            const double xr = Lc[2 * (i * M + k)], xi = Lc[2 * (i * M + k) + 1];
+                            sr -= xr * vr[k] - xi * vi[k];
+                            si -= xr * vi[k] + xi * vr[k];
+                        }
+                        const double d = Lc[2 * (i * M + i)];
+                        vr[i] = sr / d;
+                        vi[i] = si / d;
+                        nrm += vr[i] * vr[i] + vi[i] * vi[i];
+                    }
+                    capon[b * n + l] += nrm > 0.0 ? 1.0 / nrm : 0.0;
+                }
+            }
+        }
+        for (int e = 0; e < 2; ++e) {
+            const double* P = (e == 0 ? bartlett : capon) + b * n;
+            size_t best = 0;
+            for (size_t l = 1; l < n; ++l)
+                if (P[l] > P[best]) best = l;
+            double delta = 0.0;
+            if (best > 0 && best + 1 < n) {
+                const double den = P[best - 1] - 2.0 * P[best] + P[best + 1];
+                if (den < 0.0) {
+                    delta = 0.5 * (P[best - 1] - P[best + 1]) / den;
+                    if (delta > 0.5) delta = 0.5;
+                    if (delta < -0.5) delta = -0.5;
+                }
+            }
+            l_est[2 * b + e] = l_first + ((double)best + delta) * l_step;
+        }
+    }
+    free(S); free(E); free(Rb); free(Rt); free(Lc); free(ar); free(ai); free(vr); free(vi);
+}
+
+/* ------------------------------------------------------------------------ */
 /* DOA covariance.  Reference: src/cpu_opt_beam_tracker.cpp:559-602 forms     */
 /* R[f] = (1/K) sum_k x_k x_k^H in std::complex<float> per frequency.  The   */
 /* integer restatement below returns the exact per-block sum in int64       */

@@ -49,6 +49,8 @@ def oracle() -> C.CDLL:
         o.orc_tracker.argtypes = [P, P, U64, U64, U64, U64, P]
         o.orc_generate_voltage.argtypes = [U64, U64, U64, U64, U64, F32, P, U64, P]
         o.orc_covariance_block_i64.argtypes = [P, U64, U64, U64, P]
+        D = C.c_double
+        o.orc_doa_scan.argtypes = [P, U64, U64, U64, U64, U64, D, D, P, P, D, D, U64, D, P, P, P]
         o.orc_unpack.argtypes = [P, U64, P, P]
         o.orc_pack.argtypes = [C.c_int, C.c_int]
         _o = o
@@ -78,6 +80,8 @@ def reference() -> C.CDLL:
         r.ref_make_point_source.argtypes = [U64, U64, U64, P, P, P, F32, P]
         r.ref_make_moving_point_source.argtypes = [U64, U64, U64, P, P, F32, F32, F32, F32, F32, P]
         r.ref_set_threads.argtypes = [C.c_int]
+        r.ref_doa_directions.argtypes = [P, U64, U64, U64, P, P, C.c_int, U64, U64, F32, F32, U64, F32,
+                                         F32, U64, F32, F32, P]
         _r = r
     return _r
 
@@ -155,6 +159,43 @@ def covariance_block(v, T, F, A) -> np.ndarray:
     R = np.zeros((F, A, A, 2), np.int64)
     oracle().orc_covariance_block_i64(_ptr(v), T, F, A, _ptr(R))
     return R
+
+
+def covariance_blocks(v: np.ndarray, K: int) -> np.ndarray:
+    """[B][F][A][A][2] int64 block sums of x x^H (blocks of K spectra)."""
+    T, F, A = v.shape
+    B = T // K
+    out = np.zeros((B, F, A, A, 2), np.int64)
+    for b in range(B):
+        out[b] = covariance_block(np.ascontiguousarray(v[b * K:(b + 1) * K]), K, F, A)
+    return out
+
+
+def doa_scan(R: np.ndarray, K: int, subarray: int, lam: float, load: float, pos_sub: np.ndarray,
+             kw: np.ndarray, l_first: float, l_step: float, n: int, m_fixed: float = 0.0):
+    """FP64 smoothing / forgetting / Bartlett / Capon scan (orc_doa_scan)."""
+    R = np.ascontiguousarray(R, np.int64)
+    B, F, A = R.shape[0], R.shape[1], R.shape[2]
+    bart = np.zeros((B, n), np.float64)
+    cap = np.zeros((B, n), np.float64)
+    lest = np.zeros((B, 2), np.float64)
+    oracle().orc_doa_scan(_ptr(R), B, F, A, K, subarray, lam, load,
+                          _ptr(np.ascontiguousarray(pos_sub, np.float32)),
+                          _ptr(np.ascontiguousarray(kw, np.float64)), l_first, l_step, n, m_fixed,
+                          _ptr(bart), _ptr(cap), _ptr(lest))
+    return bart, cap, lest
+
+
+def ref_doa_directions(v, pos, freq, K, capon=False, G=16, levels=2, fov_l=0.2, fov_m=0.2,
+                       subarray=0, lam=1.0, load=1e-3, l0=0.0, m0=0.0) -> np.ndarray:
+    T, F, A = v.shape
+    W = -(-T // K)
+    out = np.zeros((W, 3), np.float32)
+    _rcheck(reference().ref_doa_directions(_ptr(np.ascontiguousarray(v)), T, F, A,
+                                           _ptr(np.ascontiguousarray(pos, np.float32)),
+                                           _ptr(np.ascontiguousarray(freq, np.float32)), int(capon), G,
+                                           levels, fov_l, fov_m, subarray, lam, load, K, l0, m0, _ptr(out)))
+    return out
 
 
 def unpack(v: np.ndarray):

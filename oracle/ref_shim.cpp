@@ -9,6 +9,7 @@
 // text available from ref_last_error().
 #include <beamformer/beam_tracker.hpp>
 #include <beamformer/beam_tracker_opt_v2.hpp>
+#include <beamformer/cpu_opt_beam_tracker.hpp>
 #include <beamformer/cpu_beamformer.hpp>
 #include <beamformer/geometry.hpp>
 #include <beamformer/quantization.hpp>
@@ -217,6 +218,41 @@ int ref_make_moving_point_source(uint64_t T, uint64_t F, uint64_t A, const float
         const auto v = beam_tracker_make_moving_point_source(
             dims_of(T, F, A, 1), vec3s(pos, A), std::vector<float>(freq, freq + F), tr, amplitude);
         std::memcpy(out, v.data(), v.size());
+    });
+}
+
+// CpuOptBeamTracker (include/beamformer/cpu_opt_beam_tracker.hpp:91-169):
+// run the DOA search over all windows and return each window's direction.
+int ref_doa_directions(const uint8_t* v, uint64_t T, uint64_t F, uint64_t A, const float* pos,
+                       const float* freq, int capon, uint64_t G, uint64_t levels, float fov_l,
+                       float fov_m, uint64_t subarray, float lam, float load, uint64_t K, float l0,
+                       float m0, float* dirs) {
+    return guarded([&] {
+        const Dimensions d = dims_of(T, F, A, 1);
+        CpuOptTrackerConfig cfg;
+        cfg.estimator = capon ? TrackerEstimator::Capon : TrackerEstimator::Bartlett;
+        cfg.coarse_grid_resolution = G;
+        cfg.refinement_levels = levels;
+        cfg.search_fov_l = fov_l;
+        cfg.search_fov_m = fov_m;
+        cfg.spatial_smoothing_subarray_size = subarray;
+        cfg.forgetting_factor = lam;
+        cfg.diagonal_load = load;
+        cfg.integration_spectra = K;
+        CpuOptBeamTracker tracker(vec3s(pos, A), std::vector<float>(freq, freq + F), d, cfg);
+        TrackerTrajectoryConfig prior;
+        prior.direction_start = direction_from_lm(l0, m0);
+        tracker.seed_trajectory(prior);
+        PackedVoltage pv(v, v + T * F * A);
+        Intensities I(T * F);
+        tracker.run_into(pv, I);
+        const std::size_t W = tracker_window_count(T, K);
+        for (std::size_t w = 0; w < W; ++w) {
+            const Vec3 dd = tracker.window_direction(w);
+            dirs[3 * w] = dd[0];
+            dirs[3 * w + 1] = dd[1];
+            dirs[3 * w + 2] = dd[2];
+        }
     });
 }
 

@@ -1,0 +1,121 @@
+"""DOA: exact block covariance on int8 tensor cores and the FP64 scan.
+
+Covariance: bit-exact against the integer restatement (int64 sums of
+x x^H).  Scan: against the FP64 oracle (orc_doa_scan) to 1e-6 relative
+(the only freedom is the last bit of the float sin/cos of the reduced
+phase).  The oracle itself is pinned to the reference's CpuOptBeamTracker
+search on a source (CPU test below).
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+from conftest import random_voltage
+
+F = 336
+C_LIGHT = 299_792_458.0
+
+
+def geometry(A=64):
+    lam = C_LIGHT / 800e6
+    sp = 0.5 * lam
+    cols = 32 if A >= 32 else A
+    pos = np.zeros((A, 3), np.float32)
+    for i in range(A):
+        pos[i] = ((i % cols) * sp, (i // cols) * sp, 0.0)
+    freq = (400e6 + np.arange(F) * (400e6 / 671)).astype(np.float32)
+    kw = 2 * math.pi * freq.astype(np.float64) / C_LIGHT
+    return pos, freq, kw
+
+
+def source_voltage(T, A, sources, sigma=2.0, seed=0, multipath=None):
+    """Complex Gaussian source waveforms (per spectrum and channel) along
+    steering exp(-j k x l); coherent sources share a waveform; noise sigma per
+    component; rounded half-to-even and clipped to int4."""
+    pos, freq, kw = geometry(A)
+    rng = np.random.default_rng(seed)
+    g = (rng.normal(size=(T, F)) + 1j * rng.normal(size=(T, F))) / math.sqrt(2)
+    x = (rng.normal(size=(T, F, A)) + 1j * rng.normal(size=(T, F, A))) * sigma
+    for l, amp, phase in sources:
+        st = np.exp(-1j * kw[:, None] * (pos[:, 0].astype(np.float64) * l)[None, :])
+        x += amp * np.exp(1j * phase) * g[:, :, None] * st[None]
+    if multipath is not None:
+        l, amp, rho = multipath
+        g3 = (rng.normal(size=(T, F)) + 1j * rng.normal(size=(T, F))) / math.sqrt(2)
+        gm = rho * g + math.sqrt(1 - rho * rho) * g3
+        st = np.exp(-1j * kw[:, None] * (pos[:, 0].astype(np.float64) * l)[None, :])
+        x += amp * gm[:, :, None] * st[None]
+    xr = np.clip(np.rint(x.real), -8, 7).astype(np.int64)
+    xi = np.clip(np.rint(x.imag), -8, 7).astype(np.int64)
+    return ((xr & 15) | ((xi & 15) << 4)).astype(np.uint8)
+
+
+def test_oracle_doa_agrees_with_reference_search(ref):
+    """One source: the FP64 1-D scan and the reference's 2-D coarse-to-fine
+    Bartlett search (src/cpu_opt_beam_tracker.cpp:1619-2454) recover the
+    same direction."""
+    pos, freq, kw = geometry()
+    K, B, l_true = 256, 2, 0.23
+    v = source_voltage(K * B, 64, [(l_true, 2.0 * math.sqrt(2), 0.0)], seed=1)
+    R = ref.covariance_blocks(v, K)
+    _, cap, lest = ref.doa_scan(R, K, 8, 0.9, 1e-3, pos[:8], kw, -0.9, 0.001, 1801)
+    dirs = ref.ref_doa_directions(v, pos, freq, K, capon=False, G=16, levels=2, fov_l=0.2, fov_m=0.05,
+                                  subarray=0, lam=0.9, l0=0.2, m0=0.0)
+    for w in range(B):
+        assert abs(lest[w, 0] - l_true) < 0.01 and abs(lest[w, 1] - l_true) < 0.01
+        assert abs(float(dirs[w, 0]) - l_true) < 0.01
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("A,K,B", [(64, 256, 3), (32, 128, 2), (64, 4096, 1)])
+def test_covariance_bit_exact(cuda, orc, A, K, B):
+    from beamform_project_b200 import api, native
+    torch = cuda
+    T = K * B
+    v = random_voltage(T, F, A, seed=A + K)
+    out = torch.full((B * F * A * A * 2,), 12345, dtype=torch.int32, device="cuda")
+    api.doa_covariance_i32(None, torch.from_numpy(v).cuda(), out, api.Dimensions(T, F, A, 1), K)
+    torch.cuda.synchronize()
+    assert native.take_device_error() == 0
+    got = out.cpu().numpy().reshape(B, F, A, A, 2).astype(np.int64)
+    exp = orc.covariance_blocks(v, K)
+    assert np.array_equal(got, exp)
+
+
+@pytest.mark.gpu
+def test_scan_matches_fp64_oracle_and_finds_sources(cuda, orc):
+    from beamform_project_b200 import api, native
+    torch = cuda
+    A, K, B, M, n = 64, 512, 4, 8, 1801
+    pos, freq, kw = geometry(A)
+    amp = 2.0 * math.sqrt(2.0)
+    v = source_voltage(K * B, A, [(-0.14, amp, 0.0), (0.14, amp, 1.1)], seed=3, multipath=(0.5, amp, 0.5))
+    d = api.Dimensions(K * B, F, A, 1)
+    cov = torch.empty(B * F * A * A * 2, dtype=torch.int32, device="cuda")
+    api.doa_covariance_i32(None, torch.from_numpy(v).cuda(), cov, d, K)
+    bart = torch.empty(B * n, dtype=torch.float64, device="cuda")
+    cap = torch.empty(B * n, dtype=torch.float64, device="cuda")
+    lest = torch.empty(2 * B, dtype=torch.float64, device="cuda")
+    ws = torch.empty(api.doa_workspace_bytes(d, K, M), dtype=torch.uint8, device="cuda")
+    api.doa_scan(None, cov, torch.from_numpy(pos[:M]).cuda(), torch.from_numpy(kw).cuda(), d, K, M, 0.9, 1e-3,
+                 -0.9, 0.001, n, 0.0, bart, cap, lest, ws)
+    torch.cuda.synchronize()
+    assert native.take_device_error() == 0
+    R = cov.cpu().numpy().reshape(B, F, A, A, 2).astype(np.int64)
+    assert np.array_equal(R, orc.covariance_blocks(v, K))
+    eb, ec, el = orc.doa_scan(R, K, M, 0.9, 1e-3, pos[:M], kw, -0.9, 0.001, n)
+    gb = bart.cpu().numpy().reshape(B, n)
+    gc = cap.cpu().numpy().reshape(B, n)
+    assert np.allclose(gb, eb, rtol=1e-6, atol=0.0)
+    assert np.allclose(gc, ec, rtol=1e-6, atol=0.0)
+    assert np.allclose(lest.cpu().numpy().reshape(B, 2), el, atol=1e-6)
+    # Capon's two largest local maxima: the coherent pair (0.7 beamwidth apart,
+    # which smoothing along the element index of a 2 x 32 grid does not split)
+    # between the two sources, and the multipath arrival at 0.5
+    P = gc[-1]
+    peaks = [i for i in range(1, n - 1) if P[i] > P[i - 1] and P[i] >= P[i + 1]]
+    top = sorted(-0.9 + 0.001 * i for i in sorted(peaks, key=lambda i: -P[i])[:2])
+    assert -0.14 < top[0] < 0.14 and abs(top[1] - 0.5) < 0.03, top
