@@ -49,6 +49,17 @@ SNR = 5.0
 SEED = 0
 METRIC = "beam-samples/s (T*F*B)"
 
+# DRAM bytes (read + write) per launch of each workload's dominant kernel, from
+# one ncu capture each (dram__bytes_read.sum + dram__bytes_write.sum).  The
+# grid figure was captured on one shard and the tracker figure on T = 32768;
+# both are scaled to a full launch by the units processed.  The captures and
+# their commands are summarised under profiles/.
+NCU_TRAFFIC = {
+    "grid": 2 * (1.472283e9 + 20.583936e6),
+    "tracker": 8 * (704.703488e6 + 3.553024e6),
+    "doa": 1.763518e9 + 172.711936e6,
+}
+
 
 # --------------------------------------------------------------------------
 # workload definition (host side, FP64)
@@ -369,7 +380,9 @@ def run_gpu(args):
     achieved = alg_flops / (main_ms / 1e3) / 1e12
     roofline = {"bound": "tensor", "achieved": round(achieved, 2), "peak": peak_tflops,
                 "unit": "TFLOP/s", "frac": round(achieved / peak_tflops, 4),
-                "traffic": None, "peak_source": peak_src + " (bf16 dense, sustained)",
+                "traffic": (round(NCU_TRAFFIC["grid"]) if kernel == "tensor" and N_SHARDS == 2
+                            and not args.fused_quant else None),
+                "peak_source": peak_src + " (bf16 dense, sustained)",
                 "kernel": "grid_tensor_kernel" if kernel == "tensor" else "grid_exact_kernel+quantize",
                 "kernel_ms": round(main_ms, 4),
                 "algorithmic_flop_per_launch": alg_flops}
@@ -536,7 +549,8 @@ def run_tracker(args):
                    "parallelism": f"independent replicas x{world}",
                    "l2": "inputs (5.64 GB voltage) exceed L2; no flush"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_gbs, "unit": "GB/s",
-                     "frac": round(achieved / hbm_gbs, 4), "traffic": None,
+                     "frac": round(achieved / hbm_gbs, 4),
+                     "traffic": round(NCU_TRAFFIC["tracker"]) if mode == 1 and TR_T == 262144 else None,
                      "peak_source": peak_src + " (copy bandwidth)", "kernel_ms": round(kern_ms, 4),
                      "algorithmic_bytes_per_launch": alg_bytes},
         "per_spectrum_output": {"ms_per_step": ps_ms, "value": samples / (ps_ms / 1e3),
@@ -620,6 +634,204 @@ def run_tracker_reference(args):
     }), flush=True)
 
 
+# --------------------------------------------------------------------------
+# DOA workload: A=64 (2 x 32), F=336 (400-600 MHz), blocks of K=4096 spectra,
+# 16 blocks, forgetting 0.9; noise sigma=2 plus two coherent sources 0.7
+# beamwidth apart at SNR 2 and a 50 %-correlated multipath copy; 8-element
+# smoothing, Bartlett and Capon (load 1e-3 tr/M, FP64 Cholesky) on a
+# 1801-point grid with parabolic peak refinement
+# --------------------------------------------------------------------------
+DOA_K = 4096
+DOA_BLOCKS = 16
+DOA_SIGMA = 2.0
+DOA_SNR = 2.0
+DOA_SUB = 8
+DOA_GRID = (-0.9, 0.001, 1801)
+DOA_EPOCH = 64   # source waveforms change every 64 spectra
+
+
+def doa_inputs(T: int):
+    pos, freq_full, _ = workload_geometry()
+    freq = np.ascontiguousarray(freq_full[:F_SHARD])
+    k = 2.0 * math.pi * freq.astype(np.float64) / C_LIGHT
+    # beamwidth of the 8-element sub-array at the band centre: lambda / aperture
+    bw = (C_LIGHT / float(freq.mean())) / (DOA_SUB * float(pos[1, 0] - pos[0, 0]))
+    l1, l2, l3 = -0.35 * bw, 0.35 * bw, 0.5
+    amp = DOA_SIGMA * math.sqrt(DOA_SNR)
+    U = T // DOA_EPOCH
+    rng = np.random.default_rng(SEED + 4)
+    g1 = (rng.normal(size=(U, F_SHARD)) + 1j * rng.normal(size=(U, F_SHARD))) / math.sqrt(2)
+    g3 = (rng.normal(size=(U, F_SHARD)) + 1j * rng.normal(size=(U, F_SHARD))) / math.sqrt(2)
+    gm = 0.5 * g1 + math.sqrt(0.75) * g3
+    mu = np.zeros((U, F_SHARD, N_ANT), np.complex128)
+    for l, g, ph in ((l1, g1, 0.0), (l2, g1, 1.1), (l3, gm, 0.0)):
+        st = np.exp(-1j * k[:, None] * (pos[:, 0].astype(np.float64) * l)[None, :])  # [F][A]
+        mu += amp * np.exp(1j * ph) * g[:, :, None] * st[None]
+    mu32 = np.stack([mu.real, mu.imag], -1).astype(np.float32)
+    return pos, freq, k, mu32, (l1, l2, l3)
+
+
+def run_doa(args):
+    import torch
+    from beamform_project_b200 import api, native
+    if args.impl == "reference":
+        return run_doa_reference(args)
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    T = DOA_K * DOA_BLOCKS
+    pos, freq, k, mu, truth = doa_inputs(T)
+    d = api.Dimensions(T, F_SHARD, N_ANT, 1)
+    volt = torch.empty(T * F_SHARD * N_ANT, dtype=torch.uint8, device=dev)
+    api.generate_voltage(None, SEED + 5, 0, DOA_SIGMA, torch.from_numpy(mu).to(dev), DOA_EPOCH, volt, d)
+    l0, dl, n = DOA_GRID
+    cov = torch.empty(DOA_BLOCKS * F_SHARD * N_ANT * N_ANT * 2, dtype=torch.int32, device=dev)
+    bart = torch.empty(DOA_BLOCKS * n, dtype=torch.float64, device=dev)
+    cap = torch.empty_like(bart)
+    lest = torch.empty(2 * DOA_BLOCKS, dtype=torch.float64, device=dev)
+    ws = torch.empty(api.doa_workspace_bytes(d, DOA_K, DOA_SUB), dtype=torch.uint8, device=dev)
+    pos_d = torch.from_numpy(np.ascontiguousarray(pos[:DOA_SUB])).to(dev)
+    k_d = torch.from_numpy(k).to(dev)
+    cov_ev, scan_ev = [], []
+
+    def step(record=False):
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)] if record else None
+        if record:
+            e[0].record(stream)
+        api.doa_covariance_i32(None, volt, cov, d, DOA_K)
+        if record:
+            e[1].record(stream)
+        api.doa_scan(None, cov, pos_d, k_d, d, DOA_K, DOA_SUB, 0.9, 1e-3, l0, dl, n, 0.0, bart, cap, lest, ws)
+        if record:
+            e[2].record(stream)
+            cov_ev.append((e[0], e[1]))
+            scan_ev.append((e[1], e[2]))
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    assert native.take_device_error() == 0
+    steps = max(1, min(args.steps, 50))
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        t0.record(stream)
+        for _ in range(steps):
+            step(record=True)
+        t1.record(stream)
+        torch.cuda.synchronize()
+    ms = t0.elapsed_time(t1) / steps
+    cov_ms = statistics.mean(a.elapsed_time(b) for a, b in cov_ev)
+    scan_ms = statistics.mean(a.elapsed_time(b) for a, b in scan_ev)
+    # end to end: pinned host voltage in, spectra and estimates out
+    host_v = torch.empty(volt.numel(), dtype=torch.uint8, pin_memory=True)
+    host_v.copy_(volt)
+    host_b = torch.empty(bart.numel(), dtype=torch.float64, pin_memory=True)
+    host_c = torch.empty_like(host_b, pin_memory=True)
+    host_l = torch.empty(lest.numel(), dtype=torch.float64, pin_memory=True)
+    a0 = torch.cuda.Event(enable_timing=True)
+    a1 = torch.cuda.Event(enable_timing=True)
+    a0.record(stream)
+    for _ in range(max(1, args.e2e_steps)):
+        volt.copy_(host_v, non_blocking=True)
+        step()
+        host_b.copy_(bart, non_blocking=True)
+        host_c.copy_(cap, non_blocking=True)
+        host_l.copy_(lest, non_blocking=True)
+    a1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = a0.elapsed_time(a1) / max(1, args.e2e_steps)
+    samples = T * F_SHARD
+    in_bytes = T * F_SHARD * N_ANT
+    alg_bytes = in_bytes + DOA_BLOCKS * F_SHARD * N_ANT * N_ANT * 8
+    _, hbm_gbs, peak_src = measured_peaks()
+    achieved = alg_bytes / (cov_ms / 1e3) / 1e9
+    est = host_l.numpy().reshape(DOA_BLOCKS, 2)
+    line = {
+        "metric": METRIC, "value": samples / (ms / 1e3), "unit": "beam-samples/s", "n_gpus": 1,
+        "steps": steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int4xint8->int32, fp64",
+        "data": "synthetic (seeded on-device generator; coherent pair + multipath)",
+        "config": {"workload": "DOA: A=64 (2x32), F=336, K=4096 x 16 blocks, forgetting 0.9, 8-element "
+                               "smoothing, Bartlett + Capon on 1801 points (one direction stream: B=1)",
+                   "l2": "inputs (1.41 GB voltage) exceed L2; no flush",
+                   "sources_l": [round(x, 4) for x in truth]},
+        "roofline": {"bound": "hbm", "kernel": "doa_cov_kernel", "achieved": round(achieved, 1),
+                     "peak": hbm_gbs, "unit": "GB/s", "frac": round(achieved / hbm_gbs, 4),
+                     "traffic": round(NCU_TRAFFIC["doa"]),
+                     "peak_source": peak_src + " (copy bandwidth)", "kernel_ms": round(cov_ms, 4),
+                     "algorithmic_bytes_per_launch": alg_bytes},
+        "scan_ms": scan_ms,
+        "l_est_last_block": {"bartlett": float(est[-1, 0]), "capon": float(est[-1, 1])},
+        "e2e": {"value": samples / (e2e_ms / 1e3), "unit": "beam-samples/s", "h2d_bytes_per_step": host_v.numel(),
+                "d2h_bytes_per_step": (host_b.numel() + host_c.numel() + host_l.numel()) * 8, "ms_per_step": e2e_ms},
+        "gpu_launches": 4 * steps,
+        "clocks": clocks.summary(),
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = doa_cpu_baseline(volt[: 2 * DOA_K * F_SHARD * N_ANT].cpu().numpy()
+                                                .reshape(-1, F_SHARD, N_ANT), pos, freq, args.cpu_seconds)
+    print(json.dumps(line), flush=True)
+
+
+def doa_cpu_baseline(v: np.ndarray, pos, freq, budget_s: float):
+    """CpuOptBeamTracker (Capon, coarse grid 16, 2 refinements, 8-element
+    smoothing, forgetting 0.9; OpenMP over frequencies) on whole blocks."""
+    from oracle import loader as orc
+    threads = os.cpu_count() or 1
+    T = v.shape[0]
+    done = 0
+    t0 = time.perf_counter()
+    while True:
+        if orc.reference_available():
+            orc.reference().ref_set_threads(threads)
+            orc.ref_doa_directions(v, pos, freq, DOA_K, capon=True, G=16, levels=2, fov_l=0.4, fov_m=0.05,
+                                   subarray=DOA_SUB, lam=0.9, load=1e-3, l0=0.0, m0=0.0)
+            kind = "reference"
+        else:
+            R = orc.covariance_blocks(v, DOA_K)
+            orc.doa_scan(R, DOA_K, DOA_SUB, 0.9, 1e-3, pos[:DOA_SUB], 2 * math.pi * freq.astype(np.float64) / C_LIGHT,
+                         *DOA_GRID)
+            kind = "port"
+        done += T
+        if time.perf_counter() - t0 > budget_s:
+            break
+    el = time.perf_counter() - t0
+    return {"value": done * F_SHARD / el, "unit": "beam-samples/s", "cores": threads if kind == "reference" else 1,
+            "kind": kind, "sample": f"{done // DOA_K} blocks of {DOA_K} spectra x {F_SHARD} channels "
+                                    f"(CpuOptBeamTracker Capon, G=16, 2 refinements), {el:.1f} s"}
+
+
+def run_doa_reference(args):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    from oracle import loader as orc
+    from beamform_project_b200.api import generator_scale
+    T = 2 * DOA_K
+    pos, freq, k, mu, _ = doa_inputs(DOA_K * DOA_BLOCKS)
+    v = orc.generate_voltage(SEED + 5, 0, T, F_SHARD, N_ANT, generator_scale(DOA_SIGMA),
+                             mu[: T // DOA_EPOCH], DOA_EPOCH)
+    times = []
+    base = None
+    for i in range(args.warmup + args.steps):
+        t = time.perf_counter()
+        base = doa_cpu_baseline(v, pos, freq, budget_s=0.0)
+        if i >= args.warmup:
+            times.append(time.perf_counter() - t)
+    value = T * F_SHARD / statistics.mean(times)
+    base["value"] = value
+    print(json.dumps({
+        "metric": METRIC, "value": value, "unit": "beam-samples/s", "n_gpus": 0, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": statistics.mean(times) * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "fp32", "impl": "reference",
+        "data": "synthetic (same seeded voltages, first 2 blocks)",
+        "config": {"workload": "DOA: A=64 (2x32), F=336, K=4096 x 16 blocks", "sample": "2 blocks per step"},
+        "cpu_baseline": base,
+        "e2e": {"value": value, "unit": "beam-samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
 def run_reference(args):
     """The reference's own CPU implementation on the host cores, same metric."""
     rank = int(os.environ.get("RANK", "0"))
@@ -669,7 +881,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="grid", choices=["grid", "tracker"])
+    ap.add_argument("--workload", default="grid", choices=["grid", "tracker", "doa"])
     ap.add_argument("--kernel", default="tensor", choices=["tensor", "tiled", "stream", "exact"])
     ap.add_argument("--shards", type=int, default=N_SHARDS, choices=[1, 2])
     ap.add_argument("--e2e-steps", type=int, default=5)
@@ -681,6 +893,8 @@ def main():
     args = ap.parse_args()
     if args.workload == "tracker":
         run_tracker(args)
+    elif args.workload == "doa":
+        run_doa(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
