@@ -68,8 +68,9 @@ void validate_cuda_temporal_integration(CudaBeamformerKernel kernel, const Tempo
     validate_temporal_config(t);
     const std::size_t s = t.integration_spectra;
     if (kernel == CudaBeamformerKernel::TensorSplit) {
-        if (s % 32 != 0) {
-            throw std::invalid_argument("the TensorSplit kernel needs integration spectra that are a multiple of 32");
+        if (s > 32 && s % 32 != 0) {
+            throw std::invalid_argument(
+                "the TensorSplit kernel needs integration spectra below 32 or a multiple of 32");
         }
         return;
     }

@@ -39,11 +39,13 @@
 // loads).  S must be a multiple of 32, which keeps every warp's 32 spectra
 // inside one window.
 #include "bf_internal.cuh"
+#include "grid_tc.cuh"
 #include "sm100.cuh"
 
 #include <cuda.h>
 #include <cuda_fp16.h>
 
+#include <climits>
 #include <mutex>
 
 namespace bf {
@@ -61,15 +63,15 @@ constexpr int kRing = 8;                  // window partial-sum slots
 constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s bound on any wait
 
 struct TcParams {
-    const uint8_t* split;       // prepared weights, [shard][F][hi|lo][K/64][N][128 B]
-    float* integrated;          // [shard][W][F][B]
+    TcJob job;                  // plain launches
+    const TcTableHeader* table; // served launches
     int8_t* codes;              // [shard][W][F][B] or null (no fused quantization)
     float2* params;             // [shard][W][ftiles][btiles]
     unsigned* counters;         // [shard][W][ftiles] arrival counts, zero at launch
-    int n_time, n_freq, n_beams, n_beams_pad, n_ant, spectra, n_shards;
-    int tiles_per_channel, group_tiles, groups_per_channel, n_windows, ftiles, btiles;
+    int ftiles, btiles;
     long long n_units;
 };
+
 
 __device__ __forceinline__ void record_error(unsigned code) { atomicOr(&g_tc_error, code); }
 
@@ -140,19 +142,60 @@ __device__ __forceinline__ float beam_pair_sum(const uint32_t (&r)[32], int lane
 
 struct Unit {
     int shard, f, tile_begin, tile_end;
+    int key;  // (job, shard, channel): identifies the weight image
 };
 
-__device__ __forceinline__ Unit unit_of(const TcParams& p, long long u) {
+__device__ __forceinline__ Unit unit_of(const TcJob& jb, int job, long long u) {
     Unit r;
-    const long long per_shard = static_cast<long long>(p.n_freq) * p.groups_per_channel;
-    r.shard = static_cast<int>(u / per_shard);
-    const long long rem = u % per_shard;
-    r.f = static_cast<int>(rem / p.groups_per_channel);
-    const int g = static_cast<int>(rem % p.groups_per_channel);
-    r.tile_begin = g * p.group_tiles;
-    r.tile_end = min(r.tile_begin + p.group_tiles, p.tiles_per_channel);
+    const long long local = u - jb.unit_begin;
+    const long long per_shard = static_cast<long long>(jb.n_freq) * jb.groups_per_channel;
+    r.shard = static_cast<int>(local / per_shard);
+    const long long rem = local % per_shard;
+    r.f = static_cast<int>(rem / jb.groups_per_channel);
+    const int g = static_cast<int>(rem % jb.groups_per_channel);
+    r.tile_begin = g * jb.group_tiles;
+    r.tile_end = min(r.tile_begin + jb.group_tiles, jb.tiles_per_channel);
+    r.key = (job << 16) + r.shard * jb.n_freq + r.f;
     return r;
 }
+
+// Walks the units of a CTA's contiguous range in order, tracking which job
+// each belongs to (a plain launch has the single job p.job).
+template <bool kServed>
+struct JobCursor {
+    const TcJob* jobs = nullptr;
+    int n_jobs = 1, j = 0;
+    long long next_begin = 0;  // unit_begin of job j + 1
+    TcJob jb;
+
+    __device__ __forceinline__ void init(const TcParams& p, long long u) {
+        if constexpr (kServed) {
+            jobs = reinterpret_cast<const TcJob*>(p.table + 1);
+            n_jobs = p.table->n_jobs;
+            int lo = 0, hi = n_jobs - 1;  // last job with unit_begin <= u
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (jobs[mid].unit_begin <= u) lo = mid; else hi = mid - 1;
+            }
+            j = lo;
+            jb = jobs[j];
+            next_begin = j + 1 < n_jobs ? jobs[j + 1].unit_begin : LLONG_MAX;
+        } else {
+            jb = p.job;
+            next_begin = LLONG_MAX;
+        }
+    }
+    __device__ __forceinline__ Unit at(long long u) {
+        if constexpr (kServed) {
+            while (u >= next_begin) {
+                ++j;
+                jb = jobs[j];
+                next_begin = j + 1 < n_jobs ? jobs[j + 1].unit_begin : LLONG_MAX;
+            }
+        }
+        return unit_of(jb, j, u);
+    }
+};
 
 // ---------------- fused quantization bookkeeping (epilogue thread 0) ----------
 __device__ __forceinline__ unsigned atom_add_acq_rel_gpu(unsigned* addr, unsigned v) {
@@ -173,17 +216,18 @@ struct Pending {
 // Record the windows finalized in a tile (no memory traffic yet).
 __device__ __forceinline__ void record_finalized(const TcParams& p, const Unit& un, int first_row, int tile_end_row,
                                                  Pending& pd) {
+    const TcJob& jb = p.job;
     pd.mask = 0;
-    if (first_row >= p.n_time) return;
-    pd.w0 = first_row / p.spectra;
+    if (first_row >= jb.n_time) return;
+    pd.w0 = first_row / jb.spectra;
     pd.shard = un.shard;
     pd.fg = un.f / 16;
-    pd.group = static_cast<unsigned>(min(16, p.n_freq - 16 * pd.fg));
+    pd.group = static_cast<unsigned>(min(16, jb.n_freq - 16 * pd.fg));
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
         const int w = pd.w0 + i;
-        const int w_last = min((w + 1) * p.spectra, p.n_time) - 1;
-        if (w < p.n_windows && w_last >= first_row && w_last < tile_end_row) pd.mask |= 1u << i;
+        const int w_last = min((w + 1) * jb.spectra, jb.n_time) - 1;
+        if (w < jb.n_windows && w_last >= first_row && w_last < tile_end_row) pd.mask |= 1u << i;
     }
 }
 
@@ -194,7 +238,7 @@ __device__ __forceinline__ void issue_arrivals(const TcParams& p, const Pending&
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
         if ((rec.mask >> i) & 1u) {
-            const size_t ci = (static_cast<size_t>(rec.shard) * p.n_windows + rec.w0 + i) * p.ftiles + rec.fg;
+            const size_t ci = (static_cast<size_t>(rec.shard) * p.job.n_windows + rec.w0 + i) * p.ftiles + rec.fg;
             pd.old[i] = atom_add_acq_rel_gpu(&p.counters[ci], 1u);
         }
     }
@@ -218,15 +262,16 @@ __device__ __forceinline__ void publish_ready(Pending& pd, volatile int* s_quant
 // their bumps and acquired by ours; they are read through L2.
 __device__ __forceinline__ void quantize_ready(const TcParams& p, volatile int* s_quant, volatile int* s_meta,
                                                int et, int lane) {
+    const TcJob& jb = p.job;
     const int shard = s_meta[0], fg = s_meta[1];
     for (int i = 0; i < 8; ++i) {
         const int w = s_quant[i];
         if (w < 0) continue;
-        const size_t shard_off = static_cast<size_t>(shard) * p.n_windows * p.n_freq * p.n_beams;
+        const size_t shard_off = static_cast<size_t>(shard) * jb.n_windows * jb.n_freq * jb.n_beams;
         for (int bt = et >> 5; bt < p.btiles; bt += kEpilogueThreads / 32) {
-            const size_t pidx = ((static_cast<size_t>(shard) * p.n_windows + w) * p.ftiles + fg) * p.btiles + bt;
-            quantize_chunk<true>(p.integrated + shard_off, p.codes + shard_off, p.params, pidx, w, p.n_freq,
-                                 p.n_beams, fg, bt, lane);
+            const size_t pidx = ((static_cast<size_t>(shard) * jb.n_windows + w) * p.ftiles + fg) * p.btiles + bt;
+            quantize_chunk<true>(jb.integrated + shard_off, p.codes + shard_off, p.params, pidx, w, jb.n_freq,
+                                 jb.n_beams, fg, bt, lane);
         }
     }
 }
@@ -249,12 +294,15 @@ __host__ __device__ constexpr Smem smem_plan(int n_ant, int n_beams_pad) {
     s.off_x = s.off_w + 2 * s.w_bytes;
     s.off_raw = s.off_x + 2 * s.x_bytes;
     s.off_slots = s.off_raw + 2 * s.raw_bytes;
-    s.off_bar = s.off_slots + kRing * 4 * n_beams_pad * 4;
+    // window partial sums (S >= 32) or the per-warp power staging of short
+    // windows ([8 warps][16 beams][32 spectra] floats), which share the space
+    const uint32_t ring = kRing * 4 * n_beams_pad * 4, staging = (kEpilogueThreads / 32) * 16 * 32 * 4;
+    s.off_bar = s.off_slots + (ring > staging ? ring : staging);
     s.total = s.off_bar + 256;
     return s;
 }
 
-template <int A, int NB>  // A antennas, NB padded beams (multiple of 16)
+template <int A, int NB, bool kServed>  // A antennas, NB padded beams (multiple of 16)
 __global__ void __launch_bounds__(kThreads, 1)
 grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
     constexpr int K = 2 * A;
@@ -271,7 +319,7 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
     uint8_t* w_lo = w_hi + S.w_bytes;
     uint8_t* xs = smem + S.off_x;
     uint8_t* raw = smem + S.off_raw;
-    float* slots = reinterpret_cast<float*>(smem + S.off_slots);   // [kRing][4][NB]
+    float* slots = reinterpret_cast<float*>(smem + S.off_slots);   // [kRing][4][NB] or staging
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + S.off_bar);
     uint64_t* raw_full = bars + 0;    // [2]
     uint64_t* raw_empty = bars + 2;   // [2]
@@ -317,8 +365,10 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
     tc_fence_after();
     const uint32_t tmem_base = *tmem_ptr;
 
-    const long long u_begin = p.n_units * blockIdx.x / gridDim.x;
-    const long long u_end = p.n_units * (blockIdx.x + 1) / gridDim.x;
+    long long n_units = p.n_units;
+    if constexpr (kServed) n_units = p.table->n_units;
+    const long long u_begin = n_units * blockIdx.x / gridDim.x;
+    const long long u_end = n_units * (blockIdx.x + 1) / gridDim.x;
     // A failed (timed-out) wait records its code, raises the CTA-wide flag and
     // makes every role stop at its next check; nothing waits unboundedly.
     auto fail = [&](unsigned code) {
@@ -334,18 +384,21 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
             int armed[2] = {-1, -1};   // parity of the last load issued per raw stage
             int w_armed = -1;          // parity of the last weight load
             uint32_t w_loads = 0;
-            int prev_ch = -1;
+            int prev_key = -1;
             bool stop = false;
+            JobCursor<kServed> cur;
+            if (u_begin < u_end) cur.init(p, u_begin);
             for (long long u = u_begin; u < u_end && !stop; ++u) {
-                const Unit un = unit_of(p, u);
-                const int ch = un.shard * p.n_freq + un.f;
-                if (ch != prev_ch) {
-                    if (prev_ch >= 0) {
+                const Unit un = cur.at(u);
+                const TcJob& jb = cur.jb;
+                if (un.key != prev_key) {
+                    if (prev_key >= 0) {
                         if (!mbar_wait(w_empty, w_empty_phase, kWaitNs)) { fail(1); break; }
                         w_empty_phase ^= 1;
                     }
                     mbar_expect_tx(w_full, 2 * S.w_bytes);
-                    const uint8_t* src = p.split + static_cast<size_t>(ch) * 2 * S.w_bytes;
+                    const uint8_t* src =
+                        jb.split + static_cast<size_t>(un.shard * jb.n_freq + un.f) * 2 * S.w_bytes;
                     constexpr uint32_t kChunk = 32768;
                     for (uint32_t off = 0; off < 2 * S.w_bytes; off += kChunk) {
                         const uint32_t n = min(kChunk, 2 * S.w_bytes - off);
@@ -353,14 +406,25 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                     }
                     w_armed = static_cast<int>(w_loads & 1);
                     ++w_loads;
-                    prev_ch = ch;
+                    prev_key = un.key;
                 }
+                const int R = jb.rows_q;
                 for (int k = un.tile_begin; k < un.tile_end; ++k) {
                     if (*s_fail) { stop = true; break; }
                     if (!mbar_wait(&raw_empty[stage], phase ^ 1, kWaitNs)) { fail(2); stop = true; break; }
-                    mbar_expect_tx(&raw_full[stage], S.raw_bytes);
-                    tma_load_4d(raw + stage * S.raw_bytes, &vmap, 0, un.f, k * kTileM, un.shard,
-                                &raw_full[stage]);
+                    uint8_t* dst = raw + stage * S.raw_bytes;
+                    if (R == 32) {
+                        mbar_expect_tx(&raw_full[stage], S.raw_bytes);
+                        tma_load_4d(dst, &vmap, 0, un.f, jb.t0 + k * kTileM, un.shard, &raw_full[stage]);
+                    } else {
+                        // four R-row boxes, one at the start of each lane quadrant
+                        mbar_expect_tx(&raw_full[stage], 4 * R * A);
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            tma_load_4d(dst + q * 32 * A, &vmap, 0, un.f, jb.t0 + (4 * k + q) * R, un.shard,
+                                        &raw_full[stage]);
+                        }
+                    }
                     armed[stage] = static_cast<int>(phase);
                     if (++stage == 2) { stage = 0; phase ^= 1; }
                 }
@@ -376,21 +440,22 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
         if (lane == 0) {
             int xs_stage = 0, acc_stage = 0;
             uint32_t x_phase = 0, acc_phase = 0, w_phase = 0;
-            int prev_ch = -1;
+            int prev_key = -1;
             bool stop = false;
             const uint32_t w_hi_addr = smem_u32(w_hi), w_lo_addr = smem_u32(w_lo);
+            JobCursor<kServed> cur;
+            if (u_begin < u_end) cur.init(p, u_begin);
             for (long long u = u_begin; u < u_end && !stop; ++u) {
-                const Unit un = unit_of(p, u);
-                const int ch = un.shard * p.n_freq + un.f;
-                if (ch != prev_ch) {
+                const Unit un = cur.at(u);
+                if (un.key != prev_key) {
                     if (!mbar_wait(w_full, w_phase, kWaitNs)) { fail(4); break; }
                     w_phase ^= 1;
-                    prev_ch = ch;
+                    prev_key = un.key;
                 }
                 bool next_switches = true;
                 if (u + 1 < u_end) {
-                    const Unit nx = unit_of(p, u + 1);
-                    next_switches = (nx.shard * p.n_freq + nx.f) != ch;
+                    JobCursor<kServed> ahead = cur;
+                    next_switches = ahead.at(u + 1).key != un.key;
                 }
                 for (int k = un.tile_begin; k < un.tile_end; ++k) {
                     if (*s_fail) { stop = true; break; }
@@ -426,8 +491,11 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
         uint32_t phase = 0, x_phase = 0;
         bool stop = false;
         constexpr int kChunks = A / 16;  // 16-byte raw chunks per spectrum
+        JobCursor<kServed> cur;
+        if (u_begin < u_end) cur.init(p, u_begin);
         for (long long u = u_begin; u < u_end && !stop; ++u) {
-            const Unit un = unit_of(p, u);
+            const Unit un = cur.at(u);
+            const int R = cur.jb.rows_q;
             for (int k = un.tile_begin; k < un.tile_end; ++k) {
                 if (*s_fail) { stop = true; break; }
                 if (!mbar_wait(&raw_full[stage], phase, kWaitNs)) { fail(32); stop = true; break; }
@@ -437,7 +505,8 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
 #pragma unroll 4
                 for (int idx = ut; idx < kTileM * kChunks; idx += 64) {
                     const int r = idx / kChunks, q = idx % kChunks;
-                    const uint4 w4 = *reinterpret_cast<const uint4*>(rsrc + r * A + q * 16);
+                    uint4 w4 = *reinterpret_cast<const uint4*>(rsrc + r * A + q * 16);
+                    if ((r & 31) >= R) w4 = make_uint4(0u, 0u, 0u, 0u);  // spare quadrant rows
                     const uint32_t words[4] = {w4.x, w4.y, w4.z, w4.w};
 #pragma unroll
                     for (int j = 0; j < 4; ++j) {
@@ -459,8 +528,8 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
         }
     } else {
         // ------------------------------------------------------------ epilogue
-        // Eight warps: warp w reads TMEM lane quadrant w % 4 (32 spectra of
-        // the tile) and one half of the accumulator columns (beams).
+        // Eight warps: warp w reads TMEM lane quadrant w % 4 (32 tile rows)
+        // and one half of the accumulator columns (beams).
         const int q4 = warp & 3;
         const int half = (warp - 4) >> 2;                 // 0 or 1
         const int et = threadIdx.x - 128;                 // 0..255
@@ -470,6 +539,7 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
         constexpr int kHalfLoads = (kLoads + 1) / 2;
         const int c_begin = half * kHalfLoads;
         const int c_count = min(kHalfLoads, kLoads - c_begin);
+        float* stg = slots + (warp - 4) * 512;            // short windows: [16 beams][32 rows]
         float acc[kHalfLoads];
 #pragma unroll
         for (int c = 0; c < kHalfLoads; ++c) acc[c] = 0.f;
@@ -486,64 +556,110 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
 #pragma unroll
             for (int c = 0; c < kHalfLoads; ++c) acc[c] = 0.f;
         };
+        // Short windows (S < 32): every window lies inside one lane quadrant.
+        // The 16 powers of each lane's spectrum go to the staging tile
+        // (column = row ^ beam, conflict-free both ways) and the lanes then sum
+        // the (window, beam) pairs of the quadrant.
+        auto short_windows = [&](const uint32_t (&r)[32], int c, const TcJob& jb, const Unit& un, int sq) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const float re = __uint_as_float(r[2 * j]), im = __uint_as_float(r[2 * j + 1]);
+                stg[j * 32 + (lane ^ j)] = re * re + im * im;
+            }
+            __syncwarp();
+            const int sw = jb.spectra, nwin = jb.rows_q / sw;
+            for (int idx = lane; idx < nwin * 16; idx += 32) {
+                const int j = idx & 15, s = idx >> 4;
+                const int w = sq / sw + s;
+                const int b = 16 * (c_begin + c) + j;
+                if (w * sw < jb.n_time && b < jb.n_beams) {
+                    float sum = 0.f;
+                    for (int i = 0; i < sw; ++i) sum += stg[j * 32 + ((s * sw + i) ^ j)];
+                    jb.integrated[((static_cast<size_t>(un.shard) * jb.n_windows + jb.w0 + w) * jb.n_freq + un.f) *
+                                      jb.n_beams + b] = sum;
+                }
+            }
+            __syncwarp();
+        };
+        JobCursor<kServed> cur;
+        if (u_begin < u_end) cur.init(p, u_begin);
         for (long long u = u_begin; u < u_end && !stop; ++u) {
-            const Unit un = unit_of(p, u);
+            const Unit un = cur.at(u);
+            const TcJob& jb = cur.jb;
+            const bool short_win = jb.spectra < 32;
             for (int k = un.tile_begin; k < un.tile_end; ++k) {
                 if (!failed && !mbar_wait(&acc_full[acc_stage], acc_phase, kWaitNs)) { fail(128); failed = true; }
                 tc_fence_after();
-                const int row0 = k * kTileM + 32 * q4;
-                const int my_win = row0 < p.n_time ? row0 / p.spectra : -1;
-                if (my_win != cur_win && cur_win >= 0) { flush(cur_win); cur_win = -1; }
-                if (my_win >= 0 && !failed) {
-                    const uint32_t taddr = tmem_base + ((32u * q4) << 16) + acc_stage * ACC_COLS + 32 * c_begin;
+                const uint32_t taddr = tmem_base + ((32u * q4) << 16) + acc_stage * ACC_COLS + 32 * c_begin;
+                if (short_win) {
+                    const int sq = (4 * k + q4) * jb.rows_q;  // first spectrum of this quadrant
+                    if (!failed && sq < jb.n_time) {
 #pragma unroll
-                    for (int c = 0; c < kHalfLoads; c += 2) {
-                        // two loads in flight per wait
-                        uint32_t r0[32], r1[32];
-                        if (c < c_count) tmem_ld_32x32b_x32(taddr + 32 * c, r0);
-                        if (c + 1 < c_count) tmem_ld_32x32b_x32(taddr + 32 * (c + 1), r1);
-                        tmem_ld_wait();
-                        if (c < c_count) acc[c] += beam_pair_sum(r0, lane);
-                        if (c + 1 < c_count) acc[c + 1] += beam_pair_sum(r1, lane);
+                        for (int c = 0; c < kHalfLoads; c += 2) {
+                            uint32_t r0[32], r1[32];
+                            if (c < c_count) tmem_ld_32x32b_x32(taddr + 32 * c, r0);
+                            if (c + 1 < c_count) tmem_ld_32x32b_x32(taddr + 32 * (c + 1), r1);
+                            tmem_ld_wait();
+                            if (c < c_count) short_windows(r0, c, jb, un, sq);
+                            if (c + 1 < c_count) short_windows(r1, c + 1, jb, un, sq);
+                        }
                     }
-                    cur_win = my_win;
+                } else {
+                    const int row0 = k * kTileM + 32 * q4;
+                    const int my_win = row0 < jb.n_time ? row0 / jb.spectra : -1;
+                    if (my_win != cur_win && cur_win >= 0) { flush(cur_win); cur_win = -1; }
+                    if (my_win >= 0 && !failed) {
+#pragma unroll
+                        for (int c = 0; c < kHalfLoads; c += 2) {
+                            // two loads in flight per wait
+                            uint32_t r0[32], r1[32];
+                            if (c < c_count) tmem_ld_32x32b_x32(taddr + 32 * c, r0);
+                            if (c + 1 < c_count) tmem_ld_32x32b_x32(taddr + 32 * (c + 1), r1);
+                            tmem_ld_wait();
+                            if (c < c_count) acc[c] += beam_pair_sum(r0, lane);
+                            if (c + 1 < c_count) acc[c + 1] += beam_pair_sum(r1, lane);
+                        }
+                        cur_win = my_win;
+                    }
                 }
                 tc_fence_before();
                 __syncwarp();
                 if (lane == 0 && !failed) mbar_arrive(&acc_empty[acc_stage]);
                 if (++acc_stage == 2) { acc_stage = 0; acc_phase ^= 1; }
 
-                const int tile_end_row = min((k + 1) * kTileM, p.n_time);
-                if (cur_win >= 0 && min((cur_win + 1) * p.spectra, p.n_time) <= tile_end_row) {
-                    flush(cur_win);
-                    cur_win = -1;
-                }
-                named_barrier(1, kEpilogueThreads);
-                // quantize the groups this CTA completed one tile ago (list published
-                // by epilogue thread 0 before the barrier)
-                if (p.codes != nullptr) quantize_ready(p, s_quant, s_meta, et, lane);
-                // finalize every window whose last spectrum lies in this tile
+                const int tile_end_row = min((k + 1) * kTileM, jb.n_time);
                 const int first_row = k * kTileM;
-                if (first_row < p.n_time) {
-                    const int w_first = first_row / p.spectra;
-                    const int w_last_in = (tile_end_row - 1) / p.spectra;
-                    for (int w = w_first; w <= w_last_in; ++w) {
-                        const int w_last = min((w + 1) * p.spectra, p.n_time) - 1;
-                        if (w_last < first_row || w_last >= tile_end_row) continue;
-                        float* s = slots + (w % kRing) * 4 * NB;
-                        for (int b = et; b < NB; b += kEpilogueThreads) {
-                            const float total = ((s[b] + s[NB + b]) + s[2 * NB + b]) + s[3 * NB + b];
-                            s[b] = s[NB + b] = s[2 * NB + b] = s[3 * NB + b] = 0.f;
-                            if (b < p.n_beams) {
-                                p.integrated[((static_cast<size_t>(un.shard) * p.n_windows + w) * p.n_freq + un.f) *
-                                                 p.n_beams + b] = total;
+                if (!short_win) {
+                    if (cur_win >= 0 && min((cur_win + 1) * jb.spectra, jb.n_time) <= tile_end_row) {
+                        flush(cur_win);
+                        cur_win = -1;
+                    }
+                    named_barrier(1, kEpilogueThreads);
+                    // quantize the groups this CTA completed one tile ago (list published
+                    // by epilogue thread 0 before the barrier)
+                    if (!kServed && p.codes != nullptr) quantize_ready(p, s_quant, s_meta, et, lane);
+                    // finalize every window whose last spectrum lies in this tile
+                    if (first_row < jb.n_time) {
+                        const int w_first = first_row / jb.spectra;
+                        const int w_last_in = (tile_end_row - 1) / jb.spectra;
+                        for (int w = w_first; w <= w_last_in; ++w) {
+                            const int w_last = min((w + 1) * jb.spectra, jb.n_time) - 1;
+                            if (w_last < first_row || w_last >= tile_end_row) continue;
+                            float* s = slots + (w % kRing) * 4 * NB;
+                            for (int b = et; b < NB; b += kEpilogueThreads) {
+                                const float total = ((s[b] + s[NB + b]) + s[2 * NB + b]) + s[3 * NB + b];
+                                s[b] = s[NB + b] = s[2 * NB + b] = s[3 * NB + b] = 0.f;
+                                if (b < jb.n_beams) {
+                                    jb.integrated[((static_cast<size_t>(un.shard) * jb.n_windows + jb.w0 + w) *
+                                                       jb.n_freq + un.f) * jb.n_beams + b] = total;
+                                }
                             }
                         }
                     }
                 }
                 // one decision for all epilogue warps: stop together or go on together
                 if (named_barrier_or(1, kEpilogueThreads, failed || *s_fail != 0)) { stop = true; break; }
-                if (p.codes != nullptr && et == 0) {
+                if (!kServed && !short_win && p.codes != nullptr && et == 0) {
                     // Fused int8 quantization.  A 1x16x16 chunk spans 16 channels that
                     // other CTAs own: each finished (window, channel) bumps its
                     // 16-channel group's counter, and the CTA whose bump completes the
@@ -559,7 +675,7 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                 }
             }
         }
-        if (p.codes != nullptr && !stop) {
+        if (!kServed && p.codes != nullptr && !stop) {
             // drain the three stages: published list, bumps in flight, recorded windows
             for (int round = 0; round < 3; ++round) {
                 named_barrier(1, kEpilogueThreads);
@@ -645,30 +761,40 @@ EncodeTiledFn encode_fn() {
 
 int padded_beams(uint64_t b) { return static_cast<int>((b + 15) / 16 * 16); }
 
-template <int A, int NB>
-bf_status launch_tc(cudaStream_t stream, const CUtensorMap& map, const TcParams& p, int sms) {
+template <int A, int NB, bool kServed>
+bf_status launch_tc(cudaStream_t stream, const CUtensorMap& map, const TcParams& p, int grid) {
     const Smem s = smem_plan(A, NB);
     const size_t smem = s.total + 1024;
-    auto kern = grid_tensor_kernel<A, NB>;
+    auto kern = grid_tensor_kernel<A, NB, kServed>;
     cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (err != cudaSuccess) return cuda_status(err, "grid_tensor_kernel smem attribute");
-    const int grid = static_cast<int>(std::min<long long>(sms, p.n_units));
     kern<<<grid, kThreads, smem, stream>>>(map, p);
     return cuda_status(cudaGetLastError(), "grid_tensor_kernel launch");
 }
 
 template <int A>
-bf_status dispatch_nb(cudaStream_t stream, const CUtensorMap& map, const TcParams& p, int sms) {
-    switch (p.n_beams_pad) {
-        case 16: return launch_tc<A, 16>(stream, map, p, sms);
-        case 32: return launch_tc<A, 32>(stream, map, p, sms);
-        case 48: return launch_tc<A, 48>(stream, map, p, sms);
-        case 64: return launch_tc<A, 64>(stream, map, p, sms);
-        case 80: return launch_tc<A, 80>(stream, map, p, sms);
-        case 96: return launch_tc<A, 96>(stream, map, p, sms);
-        case 112: return launch_tc<A, 112>(stream, map, p, sms);
-        case 128: return launch_tc<A, 128>(stream, map, p, sms);
+bf_status dispatch_nb(cudaStream_t stream, const CUtensorMap& map, const TcParams& p, int nb_pad, int grid) {
+    switch (nb_pad) {
+        case 16: return launch_tc<A, 16, false>(stream, map, p, grid);
+        case 32: return launch_tc<A, 32, false>(stream, map, p, grid);
+        case 48: return launch_tc<A, 48, false>(stream, map, p, grid);
+        case 64: return launch_tc<A, 64, false>(stream, map, p, grid);
+        case 80: return launch_tc<A, 80, false>(stream, map, p, grid);
+        case 96: return launch_tc<A, 96, false>(stream, map, p, grid);
+        case 112: return launch_tc<A, 112, false>(stream, map, p, grid);
+        case 128: return launch_tc<A, 128, false>(stream, map, p, grid);
         default: return set_error(BF_ERR_INVALID_ARGUMENT, "n_beams must be between 1 and 128");
+    }
+}
+
+template <int A>
+bf_status dispatch_served(cudaStream_t stream, const CUtensorMap& map, const TcParams& p, int nb_pad, int grid) {
+    switch (nb_pad) {
+        case 16: return launch_tc<A, 16, true>(stream, map, p, grid);
+        case 32: return launch_tc<A, 32, true>(stream, map, p, grid);
+        case 64: return launch_tc<A, 64, true>(stream, map, p, grid);
+        case 128: return launch_tc<A, 128, true>(stream, map, p, grid);
+        default: return set_error(BF_ERR_INVALID_ARGUMENT, "served beam classes are 16, 32, 64 and 128");
     }
 }
 
@@ -697,43 +823,74 @@ uint64_t grid_tensor_counter_count(const bf_dims& d, uint64_t spectra, uint64_t 
     return n_shards * window_count(d.n_time, spectra) * ((d.n_freq + 15) / 16);
 }
 
-bf_status launch_grid_tensor(cudaStream_t stream, const uint8_t* v, const void* split, float* integrated,
-                             int8_t* codes, float* params, const bf_dims& d, uint64_t spectra,
-                             uint64_t n_shards, unsigned* counters) {
-    if (d.n_time >= (1ull << 31) || n_shards > 1024) {
-        return set_error(BF_ERR_OVERFLOW, "CUDA tensor-core grid exceeds the supported size");
+long long tc_job_tiling(TcJob& job, int n_time, int spectra, int n_freq, int n_shards) {
+    job.n_time = n_time;
+    job.spectra = spectra;
+    job.n_freq = n_freq;
+    job.n_shards = n_shards;
+    job.rows_q = small_window_rows(spectra);
+    const int rows_per_tile = 4 * job.rows_q;
+    job.tiles_per_channel = (n_time + rows_per_tile - 1) / rows_per_tile;
+    if (spectra < 32) {
+        job.group_tiles = 1;  // windows never cross a tile
+    } else {
+        const long long lcm = static_cast<long long>(spectra) / gcd_ll(spectra, kTileM) * kTileM;
+        job.group_tiles = static_cast<int>(lcm / kTileM);
     }
+    job.groups_per_channel = (job.tiles_per_channel + job.group_tiles - 1) / job.group_tiles;
+    return static_cast<long long>(n_shards) * n_freq * job.groups_per_channel;
+}
+
+int tc_padded_beams(uint64_t b) { return padded_beams(b); }
+
+bf_status encode_voltage_map(CUtensorMap* map, const uint8_t* base, uint64_t n_ant, uint64_t n_freq,
+                             uint64_t n_rows, uint64_t n_shards, uint64_t row_stride, uint64_t shard_stride,
+                             int rows_q) {
     EncodeTiledFn enc = encode_fn();
     if (enc == nullptr) return set_error(BF_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
-    CUtensorMap map;
-    const cuuint64_t dims[4] = {d.n_ant, d.n_freq, d.n_time, n_shards};
-    const cuuint64_t strides[3] = {d.n_ant, d.n_freq * d.n_ant, d.n_time * d.n_freq * d.n_ant};
-    const cuuint32_t box[4] = {static_cast<cuuint32_t>(d.n_ant), 1, static_cast<cuuint32_t>(kTileM), 1};
+    const cuuint64_t dims[4] = {n_ant, n_freq, n_rows, n_shards};
+    const cuuint64_t strides[3] = {n_ant, row_stride, shard_stride};
+    const cuuint32_t box_rows = static_cast<cuuint32_t>(rows_q == 32 ? kTileM : rows_q);
+    const cuuint32_t box[4] = {static_cast<cuuint32_t>(n_ant), 1, box_rows, 1};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
-    CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, const_cast<uint8_t*>(v), dims, strides, box, estr,
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, const_cast<uint8_t*>(base), dims, strides, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                      CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return set_error(BF_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string(r));
+    return BF_OK;
+}
 
+bf_status launch_grid_tensor(cudaStream_t stream, const uint8_t* v, const void* split, float* integrated,
+                             int8_t* codes, float* params, const bf_dims& d, uint64_t spectra,
+                             uint64_t n_shards, unsigned* counters) {
+    if (d.n_time >= (1ull << 31) || n_shards > 1024 || spectra >= (1ull << 30)) {
+        return set_error(BF_ERR_OVERFLOW, "CUDA tensor-core grid exceeds the supported size");
+    }
+    if (d.n_ant != 32 && d.n_ant != 64) {
+        return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernel supports n_ant 32 or 64");
+    }
+    const int S = static_cast<int>(spectra);
     TcParams p{};
-    p.split = static_cast<const uint8_t*>(split);
-    p.integrated = integrated;
-    p.n_time = static_cast<int>(d.n_time);
-    p.n_freq = static_cast<int>(d.n_freq);
-    p.n_beams = static_cast<int>(d.n_beams);
-    p.n_beams_pad = padded_beams(d.n_beams);
-    p.n_ant = static_cast<int>(d.n_ant);
-    p.spectra = static_cast<int>(spectra);
-    p.n_shards = static_cast<int>(n_shards);
-    p.tiles_per_channel = static_cast<int>((d.n_time + kTileM - 1) / kTileM);
-    const long long lcm = static_cast<long long>(spectra) / gcd_ll(spectra, kTileM) * kTileM;
-    p.group_tiles = static_cast<int>(lcm / kTileM);
-    p.groups_per_channel = (p.tiles_per_channel + p.group_tiles - 1) / p.group_tiles;
-    p.n_windows = static_cast<int>(window_count(d.n_time, spectra));
-    p.n_units = static_cast<long long>(n_shards) * d.n_freq * p.groups_per_channel;
+    p.job.split = static_cast<const uint8_t*>(split);
+    p.job.integrated = integrated;
+    p.job.n_beams = static_cast<int>(d.n_beams);
+    p.job.n_windows = static_cast<int>(window_count(d.n_time, spectra));
+    p.job.w0 = 0;
+    p.job.t0 = 0;
+    p.job.unit_begin = 0;
+    p.n_units = tc_job_tiling(p.job, static_cast<int>(d.n_time), S, static_cast<int>(d.n_freq),
+                              static_cast<int>(n_shards));
     p.ftiles = static_cast<int>((d.n_freq + 15) / 16);
     p.btiles = static_cast<int>((d.n_beams + 15) / 16);
-    const bool fused = codes != nullptr && counters != nullptr;
+
+    CUtensorMap map;
+    bf_status st = encode_voltage_map(&map, v, d.n_ant, d.n_freq, d.n_time, n_shards, d.n_freq * d.n_ant,
+                                      d.n_time * d.n_freq * d.n_ant, p.job.rows_q);
+    if (st != BF_OK) return st;
+
+    // Fused quantization runs in the long-window epilogue; short windows
+    // quantize with the separate kernel.
+    const bool fused = codes != nullptr && counters != nullptr && S >= 32;
     if (fused) {
         p.codes = codes;
         p.params = reinterpret_cast<float2*>(params);
@@ -747,14 +904,24 @@ bf_status launch_grid_tensor(cudaStream_t stream, const uint8_t* v, const void* 
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-
-    bf_status st;
-    if (d.n_ant == 32) st = dispatch_nb<32>(stream, map, p, sms);
-    else if (d.n_ant == 64) st = dispatch_nb<64>(stream, map, p, sms);
-    else return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernel supports n_ant 32 or 64");
-    if (st != BF_OK || codes == nullptr || fused) return st;
-    bf_dims qd{n_shards * p.n_windows, d.n_freq, d.n_ant, d.n_beams};
+    const int grid = static_cast<int>(std::min<long long>(sms, p.n_units));
+    if (grid > 0) {
+        const int nbp = padded_beams(d.n_beams);
+        st = d.n_ant == 32 ? dispatch_nb<32>(stream, map, p, nbp, grid) : dispatch_nb<64>(stream, map, p, nbp, grid);
+        if (st != BF_OK) return st;
+    }
+    if (codes == nullptr || fused) return BF_OK;
+    bf_dims qd{n_shards * static_cast<uint64_t>(p.job.n_windows), d.n_freq, d.n_ant, d.n_beams};
     return launch_quantize(stream, integrated, codes, params, qd);
+}
+
+bf_status launch_grid_tensor_served(cudaStream_t stream, const CUtensorMap& map, int n_ant, int nb_pad,
+                                    const TcTableHeader* table, int grid) {
+    TcParams p{};
+    p.table = table;
+    if (n_ant == 32) return dispatch_served<32>(stream, map, p, nb_pad, grid);
+    if (n_ant == 64) return dispatch_served<64>(stream, map, p, nb_pad, grid);
+    return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernel supports n_ant 32 or 64");
 }
 
 bf_status take_tc_error(uint32_t* code) {

@@ -62,9 +62,9 @@ BF_API bf_status bf_grid_tensor_quantized_static(void* stream, const uint8_t* pa
     if (integration_spectra == 0) {
         return set_error(BF_ERR_INVALID_ARGUMENT, "integration_spectra must be positive");
     }
-    if (integration_spectra % 32 != 0) {
+    if (integration_spectra > 32 && integration_spectra % 32 != 0) {
         return set_error(BF_ERR_UNSUPPORTED,
-                         "the tensor-core kernel needs integration_spectra to be a multiple of 32");
+                         "the tensor-core kernel needs integration_spectra below 32 or a multiple of 32");
     }
     if (dims->n_ant > 64) {
         return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernel supports n_ant 32 or 64");

@@ -35,7 +35,8 @@ void launch_packed_beamformer(CudaBeamformerKernel kernel, cudaStream_t stream,
                               float* intensity, const Dimensions& dims);
 
 // Direct accepts 320 spectra only and Tiled 10 or 320, as in the reference
-// (src/cuda_beamformer.cu:418-433); TensorSplit accepts any multiple of 32.
+// (src/cuda_beamformer.cu:418-433); TensorSplit accepts any length below 32
+// and any multiple of 32.
 void launch_packed_integrated_beamformer(CudaBeamformerKernel kernel, cudaStream_t stream,
                                          const std::uint8_t* packed_voltage, const ComplexFloat* weights,
                                          float* integrated_intensity, const Dimensions& dims,

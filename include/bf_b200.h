@@ -133,7 +133,7 @@ BF_API bf_status bf_prepare_split_weights(void* stream, const float* weights,
                                           uint64_t n_shards);
 
 /* Fused grid beamformer on tcgen05 tensor cores: |X.W|^2, integration over
- * integration_spectra (must be a multiple of 32) and, when codes and params
+ * integration_spectra (below 32, or a multiple of 32) and, when codes and params
  * are non-NULL, the int8 chunk quantizer.  n_ant must be 32 or 64 and
  * n_beams <= 128.  integrated may not be NULL (it is also the quantizer's
  * input). */

@@ -168,8 +168,21 @@ int main() {
         bool ok3 = true;
         for (std::size_t i = 0; i < out.size(); ++i) ok3 &= std::abs(out[i] - integ[i]) <= 1e-3F + 1e-5F * std::abs(integ[i]);
         expect(ok3, "TensorSplit workspace within tolerance");
-        expect(throws<std::invalid_argument>([&] { CudaBeamformerWorkspace x(di, CudaBeamformerKernel::TensorSplit, integration_after_upchan); }),
-               "TensorSplit rejects 10-spectrum integration");
+        expect(throws<std::invalid_argument>([&] { CudaBeamformerWorkspace x(di, CudaBeamformerKernel::TensorSplit, TemporalIntegrationConfig{40}); }),
+               "TensorSplit rejects 40-spectrum integration");
+        {
+            // 10-spectrum windows (integration_after_upchan) on the tensor path
+            const auto integ10 = cuda_beamform_packed_integrated_intensity(vi, tile(wi, di), di, integration_after_upchan);
+            CudaBeamformerWorkspace w10(di, CudaBeamformerKernel::TensorSplit, integration_after_upchan);
+            w10.upload_weights(wi, di);
+            IntegratedIntensities o10(integ10.size());
+            w10.run_integrated_pipeline(vi, o10, di);
+            bool ok10 = o10.size() == 70 * 336 * 40;
+            for (std::size_t i = 0; i < o10.size() && ok10; ++i) {
+                ok10 &= std::abs(o10[i] - integ10[i]) <= 1e-3F + 1e-5F * std::abs(integ10[i]);
+            }
+            expect(ok10, "TensorSplit 10-spectrum integration within tolerance");
+        }
 
         // device frame path: voltage and weights already on the device
         std::uint8_t* dv = nullptr;

@@ -61,7 +61,10 @@ def _check(orc, got, v, w, T, A, B, S):
 
 
 @pytest.mark.parametrize("A,B,T,S", [(64, 128, 700, 320), (64, 40, 1024, 64), (32, 16, 300, 32),
-                                     (32, 128, 640, 320), (64, 1, 256, 128), (64, 100, 129, 96)])
+                                     (32, 128, 640, 320), (64, 1, 256, 128), (64, 100, 129, 96),
+                                     # windows shorter than a 32-row lane quadrant
+                                     (32, 16, 1024, 10), (64, 128, 331, 10), (64, 8, 200, 16),
+                                     (32, 33, 77, 1), (64, 64, 250, 3), (64, 40, 100, 20)])
 def test_tensor_grid_within_tolerance(cuda, orc, A, B, T, S):
     from beamform_project_b200 import api
     v = random_voltage(T, F, A, seed=A * B + T)
@@ -109,7 +112,7 @@ def test_tensor_grid_known_answers(cuda, orc):
 
 
 @pytest.mark.parametrize("A,B,T,S,shards", [(64, 128, 700, 320, 2), (32, 40, 1024, 32, 1),
-                                            (64, 17, 300, 64, 1)])
+                                            (64, 17, 300, 64, 1), (64, 17, 300, 10, 2)])
 def test_fused_quantization_matches_separate(cuda, orc, A, B, T, S, shards):
     """The epilogue-fused quantizer gives the same codes and parameters as the
     stand-alone quantizer on the same integrated output (bit for bit)."""

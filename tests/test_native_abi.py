@@ -76,7 +76,7 @@ def test_stage_calls_validate_before_launch():
     assert lib.bf_launch_packed_integrated_beamformer(0, None, fake, fake, fake, C.byref(d), 0) == 1
     assert "integration_spectra must be positive" in native.last_error()
     assert lib.bf_launch_packed_beamformer(2, None, fake, fake, fake, C.byref(d)) == 7
-    assert lib.bf_grid_tensor_integrated(None, fake, fake, fake, None, None, C.byref(d), 10, 1) == 7
+    assert lib.bf_grid_tensor_integrated(None, fake, fake, fake, None, None, C.byref(d), 40, 1) == 7
     assert "multiple of 32" in native.last_error()
     assert lib.bf_grid_tensor_integrated(None, fake, fake, fake, fake, None, C.byref(d), 320, 1) == 1
     d128 = _d(a=128)
