@@ -300,6 +300,24 @@ def doa_scan(stream, covariance, positions, wave_numbers, dims: Dimensions, bloc
 
 
 # --------------------------------------------------------------------------
+# weights (generate_weights, reference src/weights.cpp:11-60) on the device
+# --------------------------------------------------------------------------
+
+def generate_weights(stream, positions, frequencies, directions, weights, dims: Dimensions,
+                     n_shards: int = 1) -> None:
+    """Canonical complex64 weights [shard][B][F][A] from positions [A][3],
+    frequencies [n_shards * F] and unit directions [B][3] (device arrays)."""
+    torch = _torch()
+    validate_dimensions(dims)
+    pp = _dev(positions, "positions", torch.float32, 3 * dims.n_ant)
+    ff = _dev(frequencies, "frequencies", torch.float32, n_shards * dims.n_freq)
+    dd = _dev(directions, "directions", torch.float32, 3 * dims.n_beams)
+    w = _dev(weights, "weights", torch.float32, 2 * n_shards * dims.n_beams * dims.n_freq * dims.n_ant)
+    d = dims.c()
+    check(native.lib().bf_generate_weights(_stream_handle(stream), pp, ff, dd, w, C.byref(d), int(n_shards)))
+
+
+# --------------------------------------------------------------------------
 # synthetic voltages
 # --------------------------------------------------------------------------
 

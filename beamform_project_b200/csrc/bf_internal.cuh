@@ -14,6 +14,12 @@ namespace bf {
 bf_status set_error(bf_status code, const std::string& message);
 bf_status clear_error();
 
+#define BF_RETURN_IF(expr)              \
+    do {                                \
+        const bf_status bf_s_ = (expr); \
+        if (bf_s_ != BF_OK) return bf_s_; \
+    } while (0)
+
 inline bf_status cuda_status(cudaError_t err, const char* what) {
     if (err == cudaSuccess) return BF_OK;
     return set_error(BF_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(err));
@@ -127,9 +133,11 @@ bf_status launch_doa_scan(cudaStream_t stream, const int32_t* R, const float* po
                           const bf_dims& d, uint64_t block_len, uint64_t subarray, double lam, double load,
                           double l_first, double l_step, uint64_t n, double m_fixed, double* bartlett,
                           double* capon, double* l_est, void* workspace);
-uint64_t split_weight_bytes(const bf_dims& d, uint64_t n_shards);
+// nb_pad > 0 pads the beams to nb_pad columns (a multiple of 16 >= n_beams)
+// instead of the next multiple of 16.
+uint64_t split_weight_bytes(const bf_dims& d, uint64_t n_shards, int nb_pad = 0);
 bf_status launch_prepare_split(cudaStream_t stream, const float* w, void* split, const bf_dims& d,
-                               uint64_t n_shards);
+                               uint64_t n_shards, int nb_pad = 0);
 bf_status take_tc_error(uint32_t* code);
 uint64_t grid_tensor_counter_count(const bf_dims& d, uint64_t spectra, uint64_t n_shards);
 // counters == nullptr: quantize (when codes is given) with a second launch;

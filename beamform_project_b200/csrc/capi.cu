@@ -8,6 +8,7 @@
 // Everything here is host code: argument checks, then one kernel launch on
 // the caller's stream.  No allocation, no synchronisation, no exceptions.
 #include "bf_internal.cuh"
+#include "serve.cuh"
 
 #include <cstdio>
 #include <cstring>
@@ -336,6 +337,20 @@ BF_API bf_status bf_generate_voltage(void* stream, uint64_t seed, uint64_t sampl
     if (mu != nullptr) BF_TRY(check_ptr(mu, 8, "mu"));
     return launch_generate(static_cast<cudaStream_t>(stream), seed, sample_offset, scale, mu,
                            epoch_len, out, *dims);
+}
+
+BF_API bf_status bf_generate_weights(void* stream, const float* positions, const float* frequencies,
+                                     const float* directions, float* weights, const bf_dims* dims,
+                                     uint64_t n_shards) {
+    clear_error();
+    BF_TRY(validate_dims(dims));
+    if (n_shards == 0) return set_error(BF_ERR_INVALID_ARGUMENT, "n_shards must be positive");
+    if (positions == nullptr || frequencies == nullptr || directions == nullptr || weights == nullptr) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "positions, frequencies, directions and weights must not be null");
+    }
+    BF_TRY(check_ptr(weights, 8, "weights"));
+    return launch_generate_weights(static_cast<cudaStream_t>(stream), positions, frequencies, directions, weights,
+                                   n_shards, dims->n_freq, dims->n_beams, dims->n_ant);
 }
 
 }  // extern "C"

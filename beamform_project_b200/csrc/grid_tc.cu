@@ -762,12 +762,16 @@ EncodeTiledFn encode_fn() {
 int padded_beams(uint64_t b) { return static_cast<int>((b + 15) / 16 * 16); }
 
 template <int A, int NB, bool kServed>
-bf_status launch_tc(cudaStream_t stream, const CUtensorMap& map, const TcParams& p, int grid) {
+bf_status launch_tc(cudaStream_t stream, const CUtensorMap& map, const TcParams& p, int grid,
+                    bool set_attribute = true) {
     const Smem s = smem_plan(A, NB);
     const size_t smem = s.total + 1024;
     auto kern = grid_tensor_kernel<A, NB, kServed>;
-    cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (err != cudaSuccess) return cuda_status(err, "grid_tensor_kernel smem attribute");
+    if (set_attribute) {
+        cudaError_t err = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (err != cudaSuccess) return cuda_status(err, "grid_tensor_kernel smem attribute");
+    }
+    if (grid == 0) return BF_OK;
     kern<<<grid, kThreads, smem, stream>>>(map, p);
     return cuda_status(cudaGetLastError(), "grid_tensor_kernel launch");
 }
@@ -787,13 +791,17 @@ bf_status dispatch_nb(cudaStream_t stream, const CUtensorMap& map, const TcParam
     }
 }
 
+// Served launches are captured in CUDA graphs: the shared-memory attribute is
+// set once beforehand (grid == 0 sets it without launching) and not during
+// capture.
 template <int A>
 bf_status dispatch_served(cudaStream_t stream, const CUtensorMap& map, const TcParams& p, int nb_pad, int grid) {
+    const bool attr = grid == 0;
     switch (nb_pad) {
-        case 16: return launch_tc<A, 16, true>(stream, map, p, grid);
-        case 32: return launch_tc<A, 32, true>(stream, map, p, grid);
-        case 64: return launch_tc<A, 64, true>(stream, map, p, grid);
-        case 128: return launch_tc<A, 128, true>(stream, map, p, grid);
+        case 16: return launch_tc<A, 16, true>(stream, map, p, grid, attr);
+        case 32: return launch_tc<A, 32, true>(stream, map, p, grid, attr);
+        case 64: return launch_tc<A, 64, true>(stream, map, p, grid, attr);
+        case 128: return launch_tc<A, 128, true>(stream, map, p, grid, attr);
         default: return set_error(BF_ERR_INVALID_ARGUMENT, "served beam classes are 16, 32, 64 and 128");
     }
 }
@@ -802,14 +810,15 @@ long long gcd_ll(long long a, long long b) { return b == 0 ? a : gcd_ll(b, a % b
 
 }  // namespace
 
-uint64_t split_weight_bytes(const bf_dims& d, uint64_t n_shards) {
-    const uint64_t K = 2 * d.n_ant, N = 2 * static_cast<uint64_t>(padded_beams(d.n_beams));
+uint64_t split_weight_bytes(const bf_dims& d, uint64_t n_shards, int nb_pad) {
+    const uint64_t K = 2 * d.n_ant;
+    const uint64_t N = 2 * static_cast<uint64_t>(nb_pad > 0 ? nb_pad : padded_beams(d.n_beams));
     return n_shards * d.n_freq * 2ull * K * N * 2ull;
 }
 
 bf_status launch_prepare_split(cudaStream_t stream, const float* w, void* split, const bf_dims& d,
-                               uint64_t n_shards) {
-    const int nbp = padded_beams(d.n_beams);
+                               uint64_t n_shards, int nb_pad) {
+    const int nbp = nb_pad > 0 ? nb_pad : padded_beams(d.n_beams);
     const long long total = static_cast<long long>(n_shards) * d.n_freq * 2 * nbp * 2 * d.n_ant;
     const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, 148LL * 32));
     prepare_split_kernel<<<blocks, 256, 0, stream>>>(reinterpret_cast<const float2*>(w),

@@ -5,6 +5,7 @@
 #include <cuda.h>
 
 #include "bf_internal.cuh"
+#include "serve.cuh"
 
 namespace bf {
 
@@ -28,15 +29,11 @@ struct TcJob {
     int n_shards;
 };
 
-// Table of a served launch in device memory: this header, then n_jobs TcJob
+// Table of a served launch in device memory: the header, then n_jobs TcJob
 // entries sorted by unit_begin.  All jobs of one table share the tensor map
 // (so its box, i.e. rows_q), the padded beam count, and the window kind
 // (all S < 32 or all S >= 32).
-struct TcTableHeader {
-    long long n_units;
-    int n_jobs;
-    int pad;
-};
+using TcTableHeader = TableHeader;
 
 __host__ __device__ inline int small_window_rows(int spectra) {
     return spectra >= 32 ? 32 : (32 / spectra) * spectra;
@@ -56,6 +53,8 @@ bf_status encode_voltage_map(CUtensorMap* map, const uint8_t* base, uint64_t n_a
 int tc_padded_beams(uint64_t b);
 
 // One persistent launch (grid CTAs) over a device-resident job table.
+// grid == 0 only sets the kernel's shared-memory attribute (call it once
+// before capturing launches in a graph).
 bf_status launch_grid_tensor_served(cudaStream_t stream, const CUtensorMap& map, int n_ant, int nb_pad,
                                     const TcTableHeader* table, int grid);
 

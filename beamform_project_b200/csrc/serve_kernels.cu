@@ -1,0 +1,267 @@
+// serve_kernels.cu -- kernels of the served batch besides the tensor grid:
+// the device weight generator, the multi-job streaming tracker, and the
+// multi-job chunk quantizer.
+#include "bf_internal.cuh"
+#include "serve.cuh"
+#include "tracker_common.cuh"
+
+#include <climits>
+
+namespace bf {
+namespace {
+
+using namespace trk;
+
+constexpr double kTwoPi = 6.283185307179586476925286766559;
+constexpr double kSpeedOfLight = 299792458.0;
+
+// generate_weights (reference src/weights.cpp:38-55) term by term in double:
+// k = 2*pi*f / c, delay = (px*dx + py*dy) + pz*dz, phase = k * delay,
+// then (float) cos / (float) sin of the double phase.
+__global__ void weights_kernel(const float* __restrict__ pos, const float* __restrict__ freq,
+                               const float* __restrict__ dirs, float2* __restrict__ out, int n_shards,
+                               int f_shard, int n_beams, int n_ant) {
+    const long long total = static_cast<long long>(n_shards) * n_beams * f_shard * n_ant;
+    for (long long i = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+         i += static_cast<long long>(gridDim.x) * blockDim.x) {
+        const int a = static_cast<int>(i % n_ant);
+        long long rest = i / n_ant;
+        const int f = static_cast<int>(rest % f_shard);
+        rest /= f_shard;
+        const int b = static_cast<int>(rest % n_beams);
+        const int s = static_cast<int>(rest / n_beams);
+        const double k = __ddiv_rn(__dmul_rn(kTwoPi, static_cast<double>(freq[s * f_shard + f])), kSpeedOfLight);
+        const double delay = __dadd_rn(__dadd_rn(__dmul_rn(static_cast<double>(pos[3 * a]), static_cast<double>(dirs[3 * b])),
+                                                 __dmul_rn(static_cast<double>(pos[3 * a + 1]),
+                                                           static_cast<double>(dirs[3 * b + 1]))),
+                                       __dmul_rn(static_cast<double>(pos[3 * a + 2]), static_cast<double>(dirs[3 * b + 2])));
+        const double phase = __dmul_rn(k, delay);
+        out[i] = make_float2(static_cast<float>(cos(phase)), static_cast<float>(sin(phase)));
+    }
+}
+
+// tracker_direction (reference src/beam_tracker.cpp:52-65) at sample t:
+// l = l0 + (float)t * dl, m = m0 + (float)t * dm, n = sqrt(1 - (l*l + m*m)).
+__device__ __forceinline__ float3 trajectory_direction(const float* tr, long long t) {
+    const float tf = __ll2float_rn(t);
+    const float l = __fadd_rn(tr[0], __fmul_rn(tf, tr[2]));
+    const float m = __fadd_rn(tr[1], __fmul_rn(tf, tr[3]));
+    const float tsq = __fadd_rn(__fmul_rn(l, l), __fmul_rn(m, m));
+    return make_float3(l, m, __fsqrt_rn(__fsub_rn(1.0f, tsq)));
+}
+
+__device__ __forceinline__ int find_job(const long long* begins, int stride_ll, int n_jobs, long long u) {
+    int lo = 0, hi = n_jobs - 1;  // last job whose first unit is <= u
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (begins[static_cast<long long>(mid) * stride_ll] <= u) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// The streaming tracker of tracker_stream.cu generalised to a job table and
+// to up to 8 sources per unit: the m16n8 tile's 8 columns carry
+// (re, im) x (hi, lo) of two sources, so a unit runs up to four tiles over
+// the same decoded voltage.  A unit is (job, window, 8 channels, 8 sources);
+// warp w of the CTA owns channel 8 * group + w.  For one source the
+// arithmetic (fragments, MMA chain, hi + lo combination, window sum order)
+// is that of tracker_stream_kernel, so results agree bit for bit.
+template <int A>
+__global__ void __launch_bounds__(256)
+served_tracker_kernel(const uint8_t* __restrict__ pool, long long row_stride, const TableHeader* table) {
+    constexpr int NW = A / 16;          // 32-bit words per thread per spectrum
+    constexpr int kBytes = A / 4;       // bytes per thread per spectrum
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, q = lane & 3;
+    const TrJob* jobs = reinterpret_cast<const TrJob*>(table + 1);
+    const long long n_units = table->n_units;
+    const int n_jobs = table->n_jobs;
+    for (long long u = blockIdx.x; u < n_units; u += gridDim.x) {
+        const int j = find_job(&jobs[0].unit_begin, sizeof(TrJob) / sizeof(long long), n_jobs, u);
+        const TrJob& jb = jobs[j];
+        const long long local = u - jb.unit_begin;
+        const int sg = static_cast<int>(local % jb.src_groups);
+        const long long rest = local / jb.src_groups;
+        const int fg = static_cast<int>(rest % jb.fgroups);
+        const int w = static_cast<int>(rest / jb.fgroups);
+        const int f = fg * 8 + warp;
+        const bool fvalid = f < jb.n_freq;
+        const int n_src = jb.n_src, S = jb.spectra;
+        const int n_tiles = min(4, (n_src - 8 * sg + 1) / 2);
+        const long long wglob = static_cast<long long>(jb.w0) + w;
+
+        // B fragments: column g of tile nt is (re, im) x (hi, lo) of source
+        // 8 sg + 2 nt + (g >> 2).
+        uint32_t bfrag[4][NW][2][2];
+        {
+            const bool is_im = (g & 1) != 0, is_lo = ((g >> 1) & 1) != 0;
+            const double k = fvalid ? jb.kw[f] : 0.0;
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) {
+                const int src = 8 * sg + 2 * nt + (g >> 2);
+                const bool used = fvalid && nt < n_tiles && src < n_src;
+                double dx = 0.0, dy = 0.0, dz = 0.0;
+                if (used) {
+                    const float3 d = trajectory_direction(jb.traj + 4 * src, wglob * S);
+                    dx = d.x;
+                    dy = d.y;
+                    dz = d.z;
+                }
+#pragma unroll
+                for (int jj = 0; jj < NW; ++jj) {
+#pragma unroll
+                    for (int s = 0; s < 2; ++s) {
+                        const int a0 = q * kBytes + 4 * jj + s, a1 = a0 + 2;
+                        uint32_t xr = 0, xi = 0;
+                        if (used) {
+                            const float2 w0 = steering_weight(jb.pos, a0, k, dx, dy, dz);
+                            const float2 w1 = steering_weight(jb.pos, a1, k, dx, dy, dz);
+                            const float cr0 = is_im ? w0.y : w0.x, cr1 = is_im ? w1.y : w1.x;
+                            const float ci0 = is_im ? w0.x : -w0.y, ci1 = is_im ? w1.x : -w1.y;
+                            xr = split_part(cr0, is_lo) | (static_cast<uint32_t>(split_part(cr1, is_lo)) << 16);
+                            xi = split_part(ci0, is_lo) | (static_cast<uint32_t>(split_part(ci1, is_lo)) << 16);
+                        }
+                        bfrag[nt][jj][s][0] = xr;
+                        bfrag[nt][jj][s][1] = xi;
+                    }
+                }
+            }
+        }
+
+        const int t_begin = w * S, t_end = t_begin + S;  // rows of this launch
+        float pw[4] = {0.f, 0.f, 0.f, 0.f};
+        const uint8_t* base = pool + static_cast<size_t>(f) * A + q * kBytes;
+        auto load_rows = [&](int tb, uint32_t (&wg)[NW], uint32_t (&wg8)[NW]) {
+            const int tg = tb + g, tg8 = tb + g + 8;
+            const uint8_t* rg = base + (jb.t0 + tg) * row_stride;
+            const uint8_t* rg8 = base + (jb.t0 + tg8) * row_stride;
+            const bool vg = fvalid && tg < t_end, vg8 = fvalid && tg8 < t_end;
+            if constexpr (A == 32) {
+                const uint2 x0 = vg ? __ldg(reinterpret_cast<const uint2*>(rg)) : make_uint2(0, 0);
+                const uint2 x1 = vg8 ? __ldg(reinterpret_cast<const uint2*>(rg8)) : make_uint2(0, 0);
+                wg[0] = x0.x; wg[1] = x0.y; wg8[0] = x1.x; wg8[1] = x1.y;
+            } else {
+#pragma unroll
+                for (int c = 0; c < NW / 4; ++c) {
+                    const uint4 x0 = vg ? __ldg(reinterpret_cast<const uint4*>(rg) + c) : make_uint4(0, 0, 0, 0);
+                    const uint4 x1 = vg8 ? __ldg(reinterpret_cast<const uint4*>(rg8) + c) : make_uint4(0, 0, 0, 0);
+                    wg[4 * c] = x0.x; wg[4 * c + 1] = x0.y; wg[4 * c + 2] = x0.z; wg[4 * c + 3] = x0.w;
+                    wg8[4 * c] = x1.x; wg8[4 * c + 1] = x1.y; wg8[4 * c + 2] = x1.z; wg8[4 * c + 3] = x1.w;
+                }
+            }
+        };
+        uint32_t wg[NW], wg8[NW];
+        load_rows(t_begin, wg, wg8);
+        for (int tb = t_begin; tb < t_end; tb += 16) {
+            uint32_t ng[NW], ng8[NW];
+            load_rows(tb + 16, ng, ng8);
+            float d[4][4];
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) d[nt][0] = d[nt][1] = d[nt][2] = d[nt][3] = 0.f;
+#pragma unroll
+            for (int jj = 0; jj < NW; ++jj) {
+                uint32_t re02g, im02g, re13g, im13g, re02h, im02h, re13h, im13h;
+                decode_word(wg[jj], re02g, im02g, re13g, im13g);
+                decode_word(wg8[jj], re02h, im02h, re13h, im13h);
+#pragma unroll
+                for (int nt = 0; nt < 4; ++nt) {
+                    if (nt < n_tiles) {
+                        mma_16816(d[nt], re02g, re02h, im02g, im02h, bfrag[nt][jj][0][0], bfrag[nt][jj][0][1]);
+                        mma_16816(d[nt], re13g, re13h, im13g, im13h, bfrag[nt][jj][1][0], bfrag[nt][jj][1][1]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) {
+                if (nt < n_tiles) {
+                    // q == 0 / 2 hold (re_hi, im_hi) of the tile's first / second
+                    // source, q == 1 / 3 the lo parts, for rows g and g + 8
+                    float p[4];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) p[i] = __shfl_xor_sync(0xffffffffu, d[nt][i], 1);
+                    const float re_g = d[nt][0] + p[0], im_g = d[nt][1] + p[1];
+                    const float re_h = d[nt][2] + p[2], im_h = d[nt][3] + p[3];
+                    const float pow_g = re_g * re_g + im_g * im_g;
+                    const float pow_h = re_h * re_h + im_h * im_h;
+                    pw[nt] += pow_g + pow_h;
+                }
+            }
+#pragma unroll
+            for (int jj = 0; jj < NW; ++jj) {
+                wg[jj] = ng[jj];
+                wg8[jj] = ng8[jj];
+            }
+        }
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+            if (nt < n_tiles) {
+                float acc = pw[nt];
+                acc += __shfl_xor_sync(0xffffffffu, acc, 4);
+                acc += __shfl_xor_sync(0xffffffffu, acc, 8);
+                acc += __shfl_xor_sync(0xffffffffu, acc, 16);
+                const int src = 8 * sg + 2 * nt + (q >> 1);
+                if (g == 0 && (q & 1) == 0 && fvalid && src < n_src) {
+                    jb.integrated[(wglob * jb.n_freq + f) * n_src + src] = acc;
+                }
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) served_quantize_kernel(const TableHeader* table) {
+    const QJob* jobs = reinterpret_cast<const QJob*>(table + 1);
+    const long long n_units = table->n_units;
+    const int n_jobs = table->n_jobs;
+    const int lane = threadIdx.x & 31;
+    const long long warps = static_cast<long long>(gridDim.x) * (blockDim.x >> 5);
+    for (long long u = static_cast<long long>(blockIdx.x) * (blockDim.x >> 5) + (threadIdx.x >> 5); u < n_units;
+         u += warps) {
+        const int j = find_job(&jobs[0].unit_begin, sizeof(QJob) / sizeof(long long), n_jobs, u);
+        const QJob& jb = jobs[j];
+        long long local = u - jb.unit_begin;
+        const int bt = static_cast<int>(local % jb.btiles);
+        local /= jb.btiles;
+        const int ft = static_cast<int>(local % jb.ftiles);
+        local /= jb.ftiles;
+        const int w = static_cast<int>(local % jb.n_win);
+        const int shard = static_cast<int>(local / jb.n_win);
+        const int win = jb.w0 + w;
+        const size_t shard_off = static_cast<size_t>(shard) * jb.n_windows * jb.n_freq * jb.n_beams;
+        const size_t pidx = ((static_cast<size_t>(shard) * jb.n_windows + win) * jb.ftiles + ft) * jb.btiles + bt;
+        quantize_chunk<false>(jb.integrated + shard_off, jb.codes + shard_off, jb.params, pidx, win, jb.n_freq,
+                              jb.n_beams, ft, bt, lane);
+    }
+}
+
+}  // namespace
+
+bf_status launch_generate_weights(cudaStream_t stream, const float* pos, const float* freq, const float* dirs,
+                                  float* out, uint64_t n_shards, uint64_t f_shard, uint64_t n_beams,
+                                  uint64_t n_ant) {
+    const uint64_t total = n_shards * n_beams * f_shard * n_ant;
+    if (total == 0) return BF_OK;
+    if (total > (1ull << 40)) return set_error(BF_ERR_OVERFLOW, "weight array exceeds the supported size");
+    const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((total + 255) / 256, 148ull * 16));
+    weights_kernel<<<blocks, 256, 0, stream>>>(pos, freq, dirs, reinterpret_cast<float2*>(out),
+                                               static_cast<int>(n_shards), static_cast<int>(f_shard),
+                                               static_cast<int>(n_beams), static_cast<int>(n_ant));
+    return cuda_status(cudaGetLastError(), "weights_kernel launch");
+}
+
+bf_status launch_served_tracker(cudaStream_t stream, int n_ant, const uint8_t* pool, uint64_t pool_freq,
+                                const TableHeader* table, int grid) {
+    const long long row_stride = static_cast<long long>(pool_freq) * n_ant;
+    switch (n_ant) {
+        case 32: served_tracker_kernel<32><<<grid, 256, 0, stream>>>(pool, row_stride, table); break;
+        case 64: served_tracker_kernel<64><<<grid, 256, 0, stream>>>(pool, row_stride, table); break;
+        default: return set_error(BF_ERR_UNSUPPORTED, "served trackers support n_ant 32 or 64");
+    }
+    return cuda_status(cudaGetLastError(), "served_tracker_kernel launch");
+}
+
+bf_status launch_served_quantize(cudaStream_t stream, const TableHeader* table, int grid) {
+    served_quantize_kernel<<<grid, 256, 0, stream>>>(table);
+    return cuda_status(cudaGetLastError(), "served_quantize_kernel launch");
+}
+
+}  // namespace bf

@@ -29,70 +29,16 @@
 // shared memory so each spectrum's 8 channels are written as one 32-byte
 // sector.
 #include "bf_internal.cuh"
+#include "tracker_common.cuh"
 
 #include <cuda_fp16.h>
 
 namespace bf {
 namespace {
 
+using namespace trk;
+
 constexpr int kChannelsPerCta = 8;
-
-__device__ __forceinline__ uint32_t lop3_and_xor(uint32_t a, uint32_t b, uint32_t c) {
-    uint32_t r;
-    asm("lop3.b32 %0, %1, %2, %3, 0x6A;" : "=r"(r) : "r"(a), "r"(b), "r"(c));  // (a & b) ^ c
-    return r;
-}
-
-__device__ __forceinline__ uint32_t h2_bits(__half2 h) {
-    return *reinterpret_cast<uint32_t*>(&h);
-}
-__device__ __forceinline__ __half2 bits_h2(uint32_t u) {
-    return *reinterpret_cast<__half2*>(&u);
-}
-
-// Decode one 32-bit word (bytes b0..b3) into four fp16 pairs:
-//   re02 = (re b0, re b2), im02 = (im b0, im b2), re13, im13.
-__device__ __forceinline__ void decode_word(uint32_t w, uint32_t& re02, uint32_t& im02,
-                                            uint32_t& re13, uint32_t& im13) {
-    const __half2 bias_lo = __floats2half2_rn(1032.0f, 1032.0f);
-    const __half2 sixteenth = __floats2half2_rn(0.0625f, 0.0625f);
-    const __half2 bias_hi = __floats2half2_rn(-72.0f, -72.0f);
-    const uint32_t w1 = w >> 8;
-    re02 = h2_bits(__hsub2(bits_h2(lop3_and_xor(w, 0x000F000Fu, 0x64086408u)), bias_lo));
-    im02 = h2_bits(__hfma2(bits_h2(lop3_and_xor(w, 0x00F000F0u, 0x64806480u)), sixteenth, bias_hi));
-    re13 = h2_bits(__hsub2(bits_h2(lop3_and_xor(w1, 0x000F000Fu, 0x64086408u)), bias_lo));
-    im13 = h2_bits(__hfma2(bits_h2(lop3_and_xor(w1, 0x00F000F0u, 0x64806480u)), sixteenth, bias_hi));
-}
-
-__device__ __forceinline__ void mma_16816(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2,
-                                          uint32_t a3, uint32_t b0, uint32_t b1) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
-        "{%8,%9}, {%0,%1,%2,%3};"
-        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-        : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
-}
-
-// Weight w = exp(i * k * (p . d)): FP64 delay and phase, FP64 reduction of
-// the phase to [-pi, pi], float sin/cos of the reduced argument.
-__device__ __forceinline__ float2 steering_weight(const float* pos, int a, double k, double dx,
-                                                  double dy, double dz) {
-    const double delay = __dadd_rn(__dadd_rn(__dmul_rn((double)pos[3 * a], dx),
-                                             __dmul_rn((double)pos[3 * a + 1], dy)),
-                                   __dmul_rn((double)pos[3 * a + 2], dz));
-    const double phase = k * delay;
-    const double two_pi = 6.283185307179586476925286766559;
-    const double r = phase - two_pi * rint(phase * (1.0 / two_pi));
-    float s, c;
-    sincosf(static_cast<float>(r), &s, &c);
-    return make_float2(c, s);
-}
-
-__device__ __forceinline__ uint16_t split_part(float c, bool lo) {
-    const __half h = __float2half_rn(c);
-    if (!lo) return __half_as_ushort(h);
-    return __half_as_ushort(__float2half_rn(c - __half2float(h)));
-}
 
 template <int A>
 __global__ void __launch_bounds__(kChannelsPerCta * 32)

@@ -53,8 +53,12 @@ class Unsupported(BeamformerError):
     """A valid request outside this build's kernels."""
 
 
+class ResourceError(BeamformerError, MemoryError):
+    """A served job whose device state can never fit the server's HBM budget."""
+
+
 _ERRORS = {1: InvalidArgument, 2: LogicError, 3: CudaError, 4: OverflowError_, 5: OutOfRange,
-           6: DeviceTimeout, 7: Unsupported}
+           6: DeviceTimeout, 7: Unsupported, 8: ResourceError}
 
 
 class Dims(C.Structure):
@@ -62,8 +66,31 @@ class Dims(C.Structure):
                 ("n_beams", C.c_uint64)]
 
 
+class ServeConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_jobs", C.c_uint32), ("window_spectra", C.c_uint32),
+                ("pool_spectra", C.c_uint64), ("shard_channels", C.c_uint32), ("max_shards", C.c_uint32),
+                ("pool_seed", C.c_uint64), ("pool_scale", C.c_float), ("pad", C.c_uint32)]
+
+
+class ServeJob(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("n_ant", C.c_uint32), ("n_shards", C.c_uint32), ("n_beams", C.c_uint32),
+                ("n_spectra", C.c_uint64), ("integration_spectra", C.c_uint64), ("pool_offset", C.c_uint64),
+                ("positions", C.c_void_p), ("frequencies", C.c_void_p), ("directions", C.c_void_p),
+                ("trajectories", C.c_void_p), ("quantize", C.c_int32), ("pad", C.c_int32)]
+
+
+class ServeStats(C.Structure):
+    _fields_ = [(n, C.c_uint64) for n in ("steps", "steps_timed", "job_windows", "jobs_submitted", "jobs_admitted",
+                                          "jobs_done", "jobs_cancelled", "jobs_rejected", "live_jobs",
+                                          "queued_jobs", "arena_bytes_in_use", "arena_bytes_peak",
+                                          "graph_captures")] + \
+               [(n, C.c_double) for n in ("beam_samples", "step_ms_total", "step_ms_p50", "step_ms_p99",
+                                          "step_ms_max")] + [("kernel_launches", C.c_uint64)]
+
+
 _P = C.c_void_p
 _U64 = C.c_uint64
+_PP = C.POINTER(C.c_void_p)
 _SIGS = {
     "bf_version": (C.c_char_p, []),
     "bf_last_error": (C.c_size_t, [C.c_char_p, C.c_size_t]),
@@ -85,6 +112,22 @@ _SIGS = {
     "bf_doa_scan": (C.c_int, [_P, _P, _P, _P, C.POINTER(Dims), _U64, _U64, C.c_double, C.c_double,
                               C.c_double, C.c_double, _U64, C.c_double, _P, _P, _P, _P]),
     "bf_generate_voltage": (C.c_int, [_P, _U64, _U64, C.c_float, _P, _U64, _P, C.POINTER(Dims)]),
+    "bf_generate_weights": (C.c_int, [_P, _P, _P, _P, _P, C.POINTER(Dims), _U64]),
+    "bf_serve_job_bytes": (_U64, [C.POINTER(ServeConfig), C.POINTER(ServeJob)]),
+    "bf_serve_create": (C.c_int, [C.POINTER(ServeConfig), _PP]),
+    "bf_serve_create_host_only": (C.c_int, [C.POINTER(ServeConfig), _PP]),
+    "bf_serve_destroy": (C.c_int, [_P]),
+    "bf_serve_submit": (C.c_int, [_P, C.POINTER(ServeJob), C.POINTER(C.c_uint64)]),
+    "bf_serve_step": (C.c_int, [_P, C.POINTER(C.c_uint32)]),
+    "bf_serve_poll": (C.c_int, [_P, _U64, C.POINTER(C.c_int32)]),
+    "bf_serve_result": (C.c_int, [_P, _U64, _PP, _PP, _PP, C.POINTER(C.c_uint64)]),
+    "bf_serve_cancel": (C.c_int, [_P, _U64]),
+    "bf_serve_release": (C.c_int, [_P, _U64]),
+    "bf_serve_sync": (C.c_int, [_P]),
+    "bf_serve_stats_get": (C.c_int, [_P, C.POINTER(ServeStats)]),
+    "bf_serve_step_times": (C.c_int, [_P, C.POINTER(C.c_float), _U64, C.POINTER(C.c_uint64)]),
+    "bf_serve_take_done": (C.c_int, [_P, C.POINTER(C.c_uint64), _U64, C.POINTER(C.c_uint64)]),
+    "bf_serve_stream": (_P, [_P]),
 }
 
 

@@ -52,7 +52,8 @@ typedef enum bf_status {
     BF_ERR_OVERFLOW = 4,         /* std::overflow_error   */
     BF_ERR_OUT_OF_RANGE = 5,     /* std::out_of_range     */
     BF_ERR_TIMEOUT = 6,          /* a bounded device wait ran out */
-    BF_ERR_UNSUPPORTED = 7       /* valid request outside this build's kernels */
+    BF_ERR_UNSUPPORTED = 7,      /* valid request outside this build's kernels */
+    BF_ERR_RESOURCE = 8          /* a served job can never fit the HBM budget */
 } bf_status;
 
 /* Dimensions: include/beamformer/config.hpp:74-79 (n_time, n_freq, n_ant,
@@ -243,7 +244,7 @@ BF_API bf_status bf_doa_scan(void* stream, const int32_t* covariance, const floa
                              double* bartlett, double* capon, double* l_est, void* workspace);
 
 /* ------------------------------------------------------------------------ */
-/* Seeded synthetic voltages (no reference counterpart)      */
+/* Seeded synthetic voltages (no reference counterpart)                     */
 /* ------------------------------------------------------------------------ */
 
 /* Approximately Gaussian complex int4 noise (Irwin-Hall of eight 16-bit
@@ -254,6 +255,123 @@ BF_API bf_status bf_doa_scan(void* stream, const int32_t* covariance, const floa
 BF_API bf_status bf_generate_voltage(void* stream, uint64_t seed, uint64_t sample_offset,
                                      float scale, const float* mu, uint64_t epoch_len,
                                      uint8_t* out, const bf_dims* dims);
+
+/* Device generate_weights (reference src/weights.cpp:11-60): canonical
+ * complex64 weights for n_shards blocks of dims->n_freq channels, written as
+ * [shard][B][F][A][2] float, from positions [A][3], frequencies
+ * [n_shards * F] (Hz) and unit beam directions [B][3] (all float, device).
+ * Double-precision phase, then (float) cos / sin as in the reference. */
+BF_API bf_status bf_generate_weights(void* stream, const float* positions, const float* frequencies,
+                                     const float* directions, float* weights, const bf_dims* dims,
+                                     uint64_t n_shards);
+
+/* ------------------------------------------------------------------------ */
+/* Served, continuously batched mode (no reference counterpart)             */
+/* ------------------------------------------------------------------------ */
+/*
+ * A server owns one CUDA stream, an HBM arena of hbm_budget_bytes for
+ * per-job device state, and device voltage pools (one per antenna count,
+ * [pool_spectra][pool_channels][A] packed bytes from the seeded generator)
+ * that stand in for the ingest buffers.  Jobs are submitted at any time and
+ * queue first-in first-out; each bf_serve_step admits queued jobs while their
+ * state fits the arena and a live slot is free, then runs one served window
+ * (window_spectra spectra) of every live job as one CUDA-graph replay: the
+ * jobs of each kernel class share one persistent launch over a device job
+ * table, rewritten by one copy before the replay.  A job's window k reads
+ * pool rows (pool_offset + k * window_spectra) mod pool_spectra.
+ * Calls are host-side, not thread-safe for one server, and never block on
+ * the GPU except bf_serve_sync, bf_serve_stats (which waits for the steps it
+ * reports) and bf_serve_release of a job the GPU may still be using.
+ */
+typedef struct bf_server bf_server;
+
+typedef enum bf_serve_kind { BF_SERVE_GRID = 0, BF_SERVE_TRACKER = 1 } bf_serve_kind;
+
+typedef enum bf_job_state {
+    BF_JOB_QUEUED = 0,     /* submitted, waiting for HBM or a slot */
+    BF_JOB_LIVE = 1,       /* admitted; windows still to launch */
+    BF_JOB_RUNNING = 2,    /* every window launched, not yet complete on the GPU */
+    BF_JOB_DONE = 3,       /* results complete in device memory */
+    BF_JOB_CANCELLED = 4,  /* cancelled; its state may be released */
+    BF_JOB_UNKNOWN = 5
+} bf_job_state;
+
+typedef struct bf_serve_config {
+    uint64_t hbm_budget_bytes;  /* admission budget for per-job device state */
+    uint32_t max_jobs;          /* live slots */
+    uint32_t window_spectra;    /* spectra per job per step; a multiple of 32 */
+    uint64_t pool_spectra;      /* rows per voltage pool; a multiple of window_spectra */
+    uint32_t shard_channels;    /* channels per shard (336) */
+    uint32_t max_shards;        /* shards per pool row (pool_channels = max_shards * shard_channels) */
+    uint64_t pool_seed;         /* pool for A antennas: bf_generate_voltage(seed + A, 0, scale) */
+    float pool_scale;
+    uint32_t pad;
+} bf_serve_config;
+
+typedef struct bf_serve_job {
+    int32_t kind;                 /* bf_serve_kind */
+    uint32_t n_ant;               /* 32 or 64 */
+    uint32_t n_shards;            /* 1 .. max_shards */
+    uint32_t n_beams;             /* grid: beams (1..128); tracker: sources (1..16) */
+    uint64_t n_spectra;           /* a multiple of window_spectra */
+    uint64_t integration_spectra; /* divides window_spectra; grid: below 32 or a multiple of 32 */
+    uint64_t pool_offset;         /* a multiple of window_spectra */
+    const float* positions;       /* host [n_ant][3] metres */
+    const float* frequencies;     /* host [n_shards * shard_channels] Hz */
+    const float* directions;      /* grid: host [n_beams][3] unit vectors */
+    const float* trajectories;    /* tracker: host [n_beams][4] l0, m0, dl, dm (per spectrum) */
+    int32_t quantize;             /* grid: int8 chunk codes and parameters as well */
+    int32_t pad;
+} bf_serve_job;
+
+typedef struct bf_serve_stats {
+    uint64_t steps;               /* served windows launched */
+    uint64_t steps_timed;         /* of which complete and timed */
+    uint64_t job_windows;         /* job windows launched */
+    uint64_t jobs_submitted, jobs_admitted, jobs_done, jobs_cancelled, jobs_rejected;
+    uint64_t live_jobs, queued_jobs;
+    uint64_t arena_bytes_in_use, arena_bytes_peak;
+    uint64_t graph_captures;
+    double beam_samples;          /* sum over launched job windows of spectra x channels x beams */
+    double step_ms_total;         /* sum of per-step device time (CUDA events) */
+    double step_ms_p50, step_ms_p99, step_ms_max;
+    uint64_t kernel_launches;     /* kernels launched by the steps (one per non-empty class) */
+} bf_serve_stats;
+
+/* Footprint in the arena of one job (0 for an invalid job). */
+BF_API uint64_t bf_serve_job_bytes(const bf_serve_config* config, const bf_serve_job* job);
+BF_API bf_status bf_serve_create(const bf_serve_config* config, bf_server** server);
+/* A scheduler-only server: the same admission, arena accounting, job tables
+ * and job states with no device work (every step completes when issued;
+ * results are not produced).  For testing the host logic without a GPU. */
+BF_API bf_status bf_serve_create_host_only(const bf_serve_config* config, bf_server** server);
+BF_API bf_status bf_serve_destroy(bf_server* server);
+/* Validates and queues a job (host inputs are copied).  BF_ERR_RESOURCE when
+ * its footprint exceeds the whole budget. */
+BF_API bf_status bf_serve_submit(bf_server* server, const bf_serve_job* job, uint64_t* job_id);
+/* Admits what fits, then launches one window of every live job. */
+BF_API bf_status bf_serve_step(bf_server* server, uint32_t* n_live);
+BF_API bf_status bf_serve_poll(bf_server* server, uint64_t job_id, int32_t* state);
+/* Device pointers of a DONE job's results (any may be NULL): integrated
+ * f32, grid [shard][W][F][B] / tracker [W][F_total][sources], W =
+ * n_spectra / integration_spectra; codes i8 and params f32 pairs as in the
+ * quantizer's layout.  Valid until bf_serve_release. */
+BF_API bf_status bf_serve_result(bf_server* server, uint64_t job_id, float** integrated, int8_t** codes,
+                                 float** params, uint64_t* n_windows);
+BF_API bf_status bf_serve_cancel(bf_server* server, uint64_t job_id);
+/* Returns the job's arena block (waits for the GPU if it may still use it). */
+BF_API bf_status bf_serve_release(bf_server* server, uint64_t job_id);
+/* Waits for every launched step; BF_ERR_TIMEOUT if a kernel reported a
+ * bounded wait that ran out. */
+BF_API bf_status bf_serve_sync(bf_server* server);
+BF_API bf_status bf_serve_stats_get(bf_server* server, bf_serve_stats* stats);
+/* Per-step device times (ms) of the timed steps, oldest first. */
+BF_API bf_status bf_serve_step_times(bf_server* server, float* out, uint64_t capacity, uint64_t* count);
+/* Ids of jobs that became DONE since the last call (up to capacity), oldest
+ * first: a completion queue, so callers need not poll every job. */
+BF_API bf_status bf_serve_take_done(bf_server* server, uint64_t* ids, uint64_t capacity, uint64_t* count);
+/* The server's stream (cudaStream_t as void*), for reading results in order. */
+BF_API void* bf_serve_stream(bf_server* server);
 
 #ifdef __cplusplus
 }
