@@ -185,6 +185,7 @@ struct bf_server {
     // counters
     uint64_t job_windows = 0, submitted = 0, admitted = 0, done = 0, cancelled = 0, rejected = 0;
     uint64_t kernel_launches = 0;
+    double predicted_last_us = 0.0;
     double beam_samples = 0.0;
 };
 
@@ -388,6 +389,37 @@ void update_done(bf_server* s) {
     s->running.resize(keep);
 }
 
+// Device-time model of one served window (microseconds), from single-job
+// measurements of every class on a B200 at 1965 MHz: a fixed cost per step
+// (table copy, graph launch), one per non-empty class (launch ramp and
+// tail), and a cost per unit of work.  Grid units: per tile of 128 rows,
+// 0.0115 + 0.0105 * (N * K / (256 * 128)) for windows of at least 32
+// spectra (a unit is three tiles plus its weight load: x 3), x 1.8 per tile
+// for short windows (their epilogue).  Tracker units: 0.015 + S * (0.00016 +
+// 0.00004 * tiles) + 2.1e-5 per (source, antenna) weight.
+constexpr double kStepUs = 12.0;
+constexpr double kClassUs = 8.0;
+
+double job_cost_us(const bf_serve_config& c, const Job& j) {
+    const double win = c.window_spectra, S = static_cast<double>(j.spec.integration_spectra);
+    const double ch = static_cast<double>(j.spec.n_shards) * c.shard_channels;
+    if (j.spec.kind == BF_SERVE_GRID) {
+        const double nk = (2.0 * j.cls.nb_pad) * (2.0 * j.spec.n_ant) / (256.0 * 128.0);
+        const double tile = 0.0115 + 0.0105 * nk;
+        if (j.cls.short_win) {
+            const double tiles = std::ceil(win / (4.0 * j.cls.rows_q));
+            return ch * tiles * tile * 1.8;
+        }
+        return ch * std::ceil(win / 128.0) * tile;
+    }
+    const double n_src = j.spec.n_beams;
+    const double groups = std::ceil(n_src / 8.0);
+    const double per_window_units = groups * std::ceil(ch / 8.0);
+    const double tiles = std::ceil(std::min(8.0, n_src) / 2.0);
+    const double unit = 0.015 + S * (0.00016 + 0.00004 * tiles) + 2.1e-5 * std::min(8.0, n_src) * j.spec.n_ant;
+    return (win / S) * per_window_units * unit;
+}
+
 bf_status encode_pool_map(bf_server* s, int A, int rows_q, CUtensorMap** out) {
     auto key = std::make_pair(A, rows_q);
     auto it = s->maps.find(key);
@@ -407,9 +439,34 @@ bf_status encode_pool_map(bf_server* s, int A, int rows_q, CUtensorMap** out) {
 
 // Admits the queue head while it fits; device uploads and weight preparation
 // are stream-ordered before the step that first uses them.
+double predicted_us(const bf_server* s, const std::vector<uint64_t>& ids, const Job* extra) {
+    std::vector<ClassKey> classes;
+    double us = kStepUs;
+    auto add = [&](const Job& j) {
+        us += job_cost_us(s->cfg, j);
+        if (std::find(classes.begin(), classes.end(), j.cls) == classes.end()) {
+            classes.push_back(j.cls);
+            us += kClassUs;
+        }
+        const ClassKey qk{kQuantClass, 0, 0, 0, 0};
+        if (j.spec.kind == BF_SERVE_GRID && j.spec.quantize &&
+            std::find(classes.begin(), classes.end(), qk) == classes.end()) {
+            classes.push_back(qk);
+            us += kClassUs;
+        }
+    };
+    for (uint64_t id : ids) add(s->jobs.at(id));
+    if (extra != nullptr) add(*extra);
+    return us;
+}
+
 bf_status admit(bf_server* s) {
     while (!s->queue.empty() && s->live.size() < s->cfg.max_jobs) {
         Job& j = s->jobs.at(s->queue.front());
+        if (s->cfg.window_budget_us > 0.f && !s->live.empty() &&
+            predicted_us(s, s->live, &j) > s->cfg.window_budget_us) {
+            break;
+        }
         uint64_t off = 0;
         if (!s->arena.alloc(j.lay.total, &off)) break;
         s->queue.pop_front();
@@ -518,6 +575,7 @@ bf_status step(bf_server* s, uint32_t* n_live) {
     if (n_live) *n_live = static_cast<uint32_t>(s->live.size());
     if (s->live.empty()) return BF_OK;
 
+    s->predicted_last_us = predicted_us(s, s->live, nullptr);
     // classes of this step (grid classes, then the quantizer, then trackers)
     std::map<ClassKey, std::vector<uint64_t>> by_class;
     for (uint64_t id : s->live) {
@@ -622,6 +680,7 @@ bf_status create(const bf_serve_config* cfg, bool host_only, bf_server** out) {
     }
     if (c.max_jobs == 0 || c.max_jobs > 65536) return set_error(BF_ERR_INVALID_ARGUMENT, "max_jobs must be 1..65536");
     if (c.hbm_budget_bytes == 0) return set_error(BF_ERR_INVALID_ARGUMENT, "hbm_budget_bytes must be positive");
+    if (!(c.window_budget_us >= 0.f)) return set_error(BF_ERR_INVALID_ARGUMENT, "window_budget_us must be >= 0");
     std::unique_ptr<bf_server, void (*)(bf_server*)> s(new bf_server(), destroy);
     s->cfg = c;
     s->host_only = host_only;
@@ -928,6 +987,7 @@ static bf_status bf_serve_stats_get_impl(bf_server* s, bf_serve_stats* out) {
     st.graph_captures = s->captures;
     st.beam_samples = s->beam_samples;
     st.kernel_launches = s->kernel_launches;
+    st.predicted_ms_last = s->predicted_last_us * 1e-3;
     if (!s->step_ms.empty()) {
         std::vector<float> v = s->step_ms;
         double total = 0.0;

@@ -63,19 +63,27 @@ __device__ __forceinline__ int find_job(const long long* begins, int stride_ll, 
 // to up to 8 sources per unit: the m16n8 tile's 8 columns carry
 // (re, im) x (hi, lo) of two sources, so a unit runs up to four tiles over
 // the same decoded voltage.  A unit is (job, window, 8 channels, 8 sources);
-// warp w of the CTA owns channel 8 * group + w.  For one source the
-// arithmetic (fragments, MMA chain, hi + lo combination, window sum order)
-// is that of tracker_stream_kernel, so results agree bit for bit.
+// warp w of the CTA owns channel 8 * group + w.  The unit's steering
+// weights are computed once each: the CTA forms the FP64 delays of its 8
+// sources (shared by the 8 channels), each warp the weights of its channel
+// into shared memory, and every lane then gathers its fragment entries.
+// For one source the arithmetic (weights, fragments, MMA chain, hi + lo
+// combination, window sum order) is that of tracker_stream_kernel, so
+// results agree bit for bit.
 template <int A>
 __global__ void __launch_bounds__(256)
 served_tracker_kernel(const uint8_t* __restrict__ pool, long long row_stride, const TableHeader* table) {
     constexpr int NW = A / 16;          // 32-bit words per thread per spectrum
-    constexpr int kBytes = A / 4;       // bytes per thread per spectrum
+    constexpr int kBytes = A / 4;       // bytes (antennas) per thread per spectrum
+    constexpr int kRow = A + 8;         // padded weight row: conflict-free gathers
+    __shared__ double s_delay[8][A];
+    __shared__ float2 s_w[8][8 * kRow + 4];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, q = lane & 3;
     const TrJob* jobs = reinterpret_cast<const TrJob*>(table + 1);
     const long long n_units = table->n_units;
     const int n_jobs = table->n_jobs;
+    auto w_at = [&](int src, int a) -> float2& { return s_w[warp][src * kRow + a + a / kBytes]; };
     for (long long u = blockIdx.x; u < n_units; u += gridDim.x) {
         const int j = find_job(&jobs[0].unit_begin, sizeof(TrJob) / sizeof(long long), n_jobs, u);
         const TrJob& jb = jobs[j];
@@ -87,26 +95,35 @@ served_tracker_kernel(const uint8_t* __restrict__ pool, long long row_stride, co
         const int f = fg * 8 + warp;
         const bool fvalid = f < jb.n_freq;
         const int n_src = jb.n_src, S = jb.spectra;
-        const int n_tiles = min(4, (n_src - 8 * sg + 1) / 2);
+        const int n_here = min(8, n_src - 8 * sg);
+        const int n_tiles = (n_here + 1) / 2;
         const long long wglob = static_cast<long long>(jb.w0) + w;
+
+        __syncthreads();  // the previous unit is done with s_delay
+        for (int i = threadIdx.x; i < n_here * A; i += blockDim.x) {
+            const int sl = i / A, a = i % A;
+            const float3 d = trajectory_direction(jb.traj + 4 * (8 * sg + sl), wglob * S);
+            s_delay[sl][a] = steering_delay(jb.pos, a, d.x, d.y, d.z);
+        }
+        __syncthreads();
+        if (fvalid) {
+            const double k = jb.kw[f];
+            for (int i = lane; i < n_here * A; i += 32) {
+                const int sl = i / A, a = i % A;
+                w_at(sl, a) = steering_from_delay(k, s_delay[sl][a]);
+            }
+        }
+        __syncwarp();
 
         // B fragments: column g of tile nt is (re, im) x (hi, lo) of source
         // 8 sg + 2 nt + (g >> 2).
         uint32_t bfrag[4][NW][2][2];
         {
             const bool is_im = (g & 1) != 0, is_lo = ((g >> 1) & 1) != 0;
-            const double k = fvalid ? jb.kw[f] : 0.0;
 #pragma unroll
             for (int nt = 0; nt < 4; ++nt) {
-                const int src = 8 * sg + 2 * nt + (g >> 2);
-                const bool used = fvalid && nt < n_tiles && src < n_src;
-                double dx = 0.0, dy = 0.0, dz = 0.0;
-                if (used) {
-                    const float3 d = trajectory_direction(jb.traj + 4 * src, wglob * S);
-                    dx = d.x;
-                    dy = d.y;
-                    dz = d.z;
-                }
+                const int sl = 2 * nt + (g >> 2);
+                const bool used = fvalid && nt < n_tiles && sl < n_here;
 #pragma unroll
                 for (int jj = 0; jj < NW; ++jj) {
 #pragma unroll
@@ -114,8 +131,8 @@ served_tracker_kernel(const uint8_t* __restrict__ pool, long long row_stride, co
                         const int a0 = q * kBytes + 4 * jj + s, a1 = a0 + 2;
                         uint32_t xr = 0, xi = 0;
                         if (used) {
-                            const float2 w0 = steering_weight(jb.pos, a0, k, dx, dy, dz);
-                            const float2 w1 = steering_weight(jb.pos, a1, k, dx, dy, dz);
+                            const float2 w0 = w_at(sl, a0);
+                            const float2 w1 = w_at(sl, a1);
                             const float cr0 = is_im ? w0.y : w0.x, cr1 = is_im ? w1.y : w1.x;
                             const float ci0 = is_im ? w0.x : -w0.y, ci1 = is_im ? w1.x : -w1.y;
                             xr = split_part(cr0, is_lo) | (static_cast<uint32_t>(split_part(cr1, is_lo)) << 16);

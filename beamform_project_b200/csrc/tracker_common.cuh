@@ -46,19 +46,30 @@ __device__ __forceinline__ void mma_16816(float (&d)[4], uint32_t a0, uint32_t a
         : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
-// Weight w = exp(i * k * (p . d)): FP64 delay and phase, FP64 reduction of
-// the phase to [-pi, pi], float sin/cos of the reduced argument.
-__device__ __forceinline__ float2 steering_weight(const float* pos, int a, double k, double dx,
-                                                  double dy, double dz) {
-    const double delay = __dadd_rn(__dadd_rn(__dmul_rn((double)pos[3 * a], dx),
-                                             __dmul_rn((double)pos[3 * a + 1], dy)),
-                                   __dmul_rn((double)pos[3 * a + 2], dz));
-    const double phase = k * delay;
-    const double two_pi = 6.283185307179586476925286766559;
-    const double r = phase - two_pi * rint(phase * (1.0 / two_pi));
+// Steering weight w = exp(i * k * (p . d)) in two steps: the FP64 delay
+// p . d (shared by all channels of a direction), then the FP64 phase k * delay
+// reduced mod 2*pi (one fused multiply-add) and float sin/cos of the reduced
+// argument.  Correctly rounded intrinsics fix every rounding, so any kernel
+// that composes these two gets bit-identical weights.
+__device__ __forceinline__ double steering_delay(const float* pos, int a, double dx, double dy, double dz) {
+    return __dadd_rn(__dadd_rn(__dmul_rn(static_cast<double>(pos[3 * a]), dx),
+                               __dmul_rn(static_cast<double>(pos[3 * a + 1]), dy)),
+                     __dmul_rn(static_cast<double>(pos[3 * a + 2]), dz));
+}
+
+__device__ __forceinline__ float2 steering_from_delay(double k, double delay) {
+    constexpr double kTwoPi = 6.283185307179586476925286766559;
+    constexpr double kInvTwoPi = 1.0 / kTwoPi;
+    const double phase = __dmul_rn(k, delay);
+    const double r = __fma_rn(-kTwoPi, rint(__dmul_rn(phase, kInvTwoPi)), phase);
     float s, c;
     sincosf(static_cast<float>(r), &s, &c);
     return make_float2(c, s);
+}
+
+__device__ __forceinline__ float2 steering_weight(const float* pos, int a, double k, double dx,
+                                                  double dy, double dz) {
+    return steering_from_delay(k, steering_delay(pos, a, dx, dy, dz));
 }
 
 __device__ __forceinline__ uint16_t split_part(float c, bool lo) {

@@ -69,7 +69,7 @@ class Dims(C.Structure):
 class ServeConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_jobs", C.c_uint32), ("window_spectra", C.c_uint32),
                 ("pool_spectra", C.c_uint64), ("shard_channels", C.c_uint32), ("max_shards", C.c_uint32),
-                ("pool_seed", C.c_uint64), ("pool_scale", C.c_float), ("pad", C.c_uint32)]
+                ("pool_seed", C.c_uint64), ("pool_scale", C.c_float), ("window_budget_us", C.c_float)]
 
 
 class ServeJob(C.Structure):
@@ -85,7 +85,8 @@ class ServeStats(C.Structure):
                                           "queued_jobs", "arena_bytes_in_use", "arena_bytes_peak",
                                           "graph_captures")] + \
                [(n, C.c_double) for n in ("beam_samples", "step_ms_total", "step_ms_p50", "step_ms_p99",
-                                          "step_ms_max")] + [("kernel_launches", C.c_uint64)]
+                                          "step_ms_max")] + [("kernel_launches", C.c_uint64),
+                                                             ("predicted_ms_last", C.c_double)]
 
 
 _P = C.c_void_p

@@ -68,11 +68,12 @@ class _DeviceArray:
 class Server:
     def __init__(self, hbm_budget_bytes: int, max_jobs: int = 512, window_spectra: int = 320,
                  pool_spectra: int = 20480, shard_channels: int = 336, max_shards: int = 4,
-                 pool_seed: int = 1, pool_sigma: float = 2.0, host_only: bool = False):
+                 pool_seed: int = 1, pool_sigma: float = 2.0, window_budget_us: float = 0.0,
+                 host_only: bool = False):
         from .api import generator_scale
         self.config = native.ServeConfig(int(hbm_budget_bytes), int(max_jobs), int(window_spectra),
                                          int(pool_spectra), int(shard_channels), int(max_shards), int(pool_seed),
-                                         float(generator_scale(pool_sigma)), 0)
+                                         float(generator_scale(pool_sigma)), float(window_budget_us))
         self.host_only = host_only
         self._h = C.c_void_p()
         fn = native.lib().bf_serve_create_host_only if host_only else native.lib().bf_serve_create
@@ -146,10 +147,14 @@ class Server:
                                                   C.byref(n)))
         return int(i.value or 0), int(c.value or 0), int(p.value or 0), int(n.value)
 
-    def result(self, job_id: int):
+    def result(self, job_id: int, floats: bool = True):
         """Host copies of a DONE job's results: integrated (grid [shard][W][F][B],
         tracker [W][F_total][sources]) and, for quantized grid jobs, codes and
-        the (offset, scale) parameters."""
+        the (offset, scale) parameters.  floats=False skips a quantized grid
+        job's float output (its product is the int8 codes).  A DONE job's
+        results are complete, so the copies run on the caller's current
+        stream (into pinned host memory), never on the server's own stream,
+        which the server destroys when it closes."""
         import torch
         spec = self.specs[int(job_id)]
         ip, cp, pp, W = self.result_pointers(job_id)
@@ -158,13 +163,25 @@ class Server:
             shape = (spec.n_shards, W, F, spec.n_beams)
         else:
             shape = (W, spec.n_shards * F, spec.n_beams)
-        integ = torch.as_tensor(_DeviceArray(ip, shape, "<f4"), device="cuda").cpu().numpy()
-        codes = params = None
+        views = []
+        if floats or not cp:
+            views.append((ip, shape, "<f4", torch.float32))
         if cp:
-            codes = torch.as_tensor(_DeviceArray(cp, shape, "|i1"), device="cuda").cpu().numpy()
             npar = spec.n_shards * W * ((F + 15) // 16) * ((spec.n_beams + 15) // 16) * 2
-            params = torch.as_tensor(_DeviceArray(pp, (npar,), "<f4"), device="cuda").cpu().numpy()
-        return integ, codes, params
+            views += [(cp, shape, "|i1", torch.int8), (pp, (npar,), "<f4", torch.float32)]
+        out = []
+        for ptr, shp, ts, dt in views:
+            dev = torch.as_tensor(_DeviceArray(ptr, shp, ts), device="cuda")
+            host = torch.empty(shp, dtype=dt, pin_memory=True)
+            host.copy_(dev, non_blocking=True)
+            out.append(host)
+        torch.cuda.current_stream().synchronize()
+        arrs = [h.numpy() for h in out]
+        if not (floats or not cp):
+            arrs = [None] + arrs
+        if not cp:
+            arrs += [None, None]
+        return tuple(arrs)
 
     # -- reporting
     def stats(self) -> dict:

@@ -944,7 +944,7 @@ def run_serve(args):
     jobs = serve_jobs(args.serve_seconds)
     budget = int(args.serve_budget_gb * 1e9)
     srv = serve.Server(budget, max_jobs=args.serve_max_jobs, pool_spectra=SERVE_POOL, pool_seed=SERVE_SEED + rank,
-                       pool_sigma=SERVE_SIGMA)
+                       pool_sigma=SERVE_SIGMA, window_budget_us=args.serve_window_us)
     stream = torch.cuda.ExternalStream(srv.stream_handle())
     # warm-up: one job of every class of the mix, served to completion
     seen, warm = set(), []
@@ -1002,8 +1002,8 @@ def run_serve(args):
         d2h = [0]
 
         def fetch(jid):
-            integ, codes, params = srv.result(jid)
-            d2h[0] += integ.nbytes + (codes.nbytes + params.nbytes if codes is not None else 0)
+            integ, codes, params = srv.result(jid, floats=False)
+            d2h[0] += sum(a.nbytes for a in (integ, codes, params) if a is not None)
         s0 = srv.stats()["beam_samples"]
         e2 = torch.cuda.Event(enable_timing=True)
         e3 = torch.cuda.Event(enable_timing=True)
@@ -1032,7 +1032,8 @@ def run_serve(args):
                                    f"(seed {SERVE_SEED}), A in {{32,64}}, 1-4 shards of 336, grid B in "
                                    f"{{1,8,32,128}} or tracker 1-16 sources, 0.1-2 s at 2.56 us/spectrum, "
                                    f"S in {{10,320}}, {args.serve_budget_gb:g} GB admission budget, "
-                                   f"320-spectrum served windows",
+                                   f"320-spectrum served windows, window-time admission bound "
+                                   f"{args.serve_window_us:g} us",
                        "jobs": len(jobs), "parallelism": f"independent replicas x{world}",
                        "l2": "voltage pools (2.6 GB) exceed L2; no flush"},
             "serve": {"window_ms_p50": float(np.percentile(times, 50)) if len(times) else None,
@@ -1043,7 +1044,8 @@ def run_serve(args):
                       "jobs_done": st["jobs_done"] - st0["jobs_done"],
                       "arena_peak_gb": st["arena_bytes_peak"] / 1e9, "graph_captures": st["graph_captures"],
                       "mean_live_jobs": (st["job_windows"] - st0["job_windows"]) / max(1, steps),
-                      "gpu_busy_frac": float(times.sum()) / el_ms if el_ms else None},
+                      "gpu_busy_frac": float(times.sum()) / el_ms if el_ms else None,
+                      "window_bound_us": args.serve_window_us},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_gbs, "unit": "GB/s",
                          "frac": round(achieved / hbm_gbs, 4), "traffic": None,
                          "peak_source": peak_src + " (copy bandwidth)",
@@ -1121,8 +1123,11 @@ def main():
     ap.add_argument("--t-spectra", type=int, default=TR_T, help="tracker workload length (profiling)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--serve-seconds", type=float, default=10.0, help="seconds of Poisson arrivals")
-    ap.add_argument("--serve-e2e-seconds", type=float, default=1.0)
+    ap.add_argument("--serve-seconds", type=float, default=2.0,
+                    help="seconds of Poisson arrivals (the full stream is 10)")
+    ap.add_argument("--serve-e2e-seconds", type=float, default=0.2)
+    ap.add_argument("--serve-window-us", type=float, default=480.0,
+                    help="admission bound on the predicted device time of a window (0: memory only)")
     ap.add_argument("--serve-budget-gb", type=float, default=120.0)
     ap.add_argument("--serve-max-jobs", type=int, default=512)
     args = ap.parse_args()

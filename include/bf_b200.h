@@ -305,7 +305,10 @@ typedef struct bf_serve_config {
     uint32_t max_shards;        /* shards per pool row (pool_channels = max_shards * shard_channels) */
     uint64_t pool_seed;         /* pool for A antennas: bf_generate_voltage(seed + A, 0, scale) */
     float pool_scale;
-    uint32_t pad;
+    /* > 0: also admit only while the predicted device time of a window stays
+     * within this many microseconds (a job that alone exceeds it is admitted
+     * when nothing else is live).  0: HBM budget and slots only. */
+    float window_budget_us;
 } bf_serve_config;
 
 typedef struct bf_serve_job {
@@ -336,6 +339,7 @@ typedef struct bf_serve_stats {
     double step_ms_total;         /* sum of per-step device time (CUDA events) */
     double step_ms_p50, step_ms_p99, step_ms_max;
     uint64_t kernel_launches;     /* kernels launched by the steps (one per non-empty class) */
+    double predicted_ms_last;     /* cost model's device time of the last step */
 } bf_serve_stats;
 
 /* Footprint in the arena of one job (0 for an invalid job). */

@@ -166,3 +166,33 @@ def test_request_loop_drains_the_stream():
         assert st["job_windows"] == sum(j.n_spectra // 320 for j in jobs)
         assert st["beam_samples"] == sum(j.beam_samples() for j in jobs)
         assert st["arena_bytes_peak"] <= 40 * 10**9
+
+
+def test_window_time_bound_limits_admission():
+    """With a window-time bound, admission stops while the cost model's
+    prediction for the next window would exceed it; a job that alone exceeds
+    it still runs when nothing else is live."""
+    jobs = serve.poisson_mix(seed=2, duration_s=0.3)
+    with serve.Server(120 * 10**9, max_jobs=512, window_budget_us=300.0, host_only=True) as s:
+        worst = 0.0
+        orig = s.step
+
+        def step():
+            nonlocal worst
+            n = orig()
+            st = s.stats()
+            if n > 1:
+                worst = max(worst, st["predicted_ms_last"])
+            return n
+        s.step = step
+        serve.run_stream(s, jobs)
+        assert s.stats()["jobs_done"] == len(jobs)
+        assert 0.0 < worst <= 0.300 + 1e-9
+    heavy = _tracker(n_spectra=640, S=10, n_src=16, A=64, ns=4)
+    with serve.Server(10**10, window_budget_us=10.0, host_only=True) as s:
+        a = s.submit(heavy)
+        b = s.submit(_tracker())
+        assert s.step() == 1          # alone over the bound: admitted anyway
+        assert s.stats()["predicted_ms_last"] > 0.010
+        s.step()
+        assert s.step() == 1 and s.poll(b) == serve.LIVE and s.poll(a) in (serve.DONE, serve.RUNNING)
