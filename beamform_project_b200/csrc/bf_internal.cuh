@@ -139,6 +139,7 @@ uint64_t split_weight_bytes(const bf_dims& d, uint64_t n_shards, int nb_pad = 0)
 bf_status launch_prepare_split(cudaStream_t stream, const float* w, void* split, const bf_dims& d,
                                uint64_t n_shards, int nb_pad = 0);
 bf_status take_tc_error(uint32_t* code);
+unsigned* device_error_word();
 uint64_t grid_tensor_counter_count(const bf_dims& d, uint64_t spectra, uint64_t n_shards);
 // counters == nullptr: quantize (when codes is given) with a second launch;
 // otherwise quantization is fused into the tensor kernel's epilogue and

@@ -32,26 +32,27 @@
 
 namespace bf {
 
-extern __device__ unsigned int g_tc_error;
-
 namespace {
 
 using namespace sm100;
 
 constexpr int kThreads = 256;
 constexpr int kTile = 128;        // spectra per tile
-constexpr int kRawStages = 4;
+constexpr int kRawStages = 6;
 constexpr int kXStages = 3;
 constexpr uint32_t kXBytes = kTile * 128;  // one unpacked tile
 constexpr uint64_t kWaitNs = 2000000000ull;
 
 struct CovParams {
     int32_t* out;             // [blocks][F][A][A][2]
+    unsigned* err;            // device error word (bits 16 and up)
     int n_freq, n_ant, block_len, n_blocks, tiles_per_block;
     long long n_units;
 };
 
-__device__ __forceinline__ void cov_error(unsigned code) { atomicOr(&g_tc_error, code << 16); }
+__device__ __forceinline__ void cov_error(unsigned* err, unsigned code) {
+    if (err != nullptr) atomicOr(err, code << 16);
+}
 
 // 8 packed bytes (antennas 8c..8c+7) -> 16 int8 components (re, im interleaved).
 __device__ __forceinline__ uint4 expand8(uint32_t w0, uint32_t w1) {
@@ -71,7 +72,7 @@ __device__ __forceinline__ uint4 expand8(uint32_t w0, uint32_t w1) {
 }
 
 template <int A>
-__global__ void __launch_bounds__(kThreads, 1)
+__global__ void __launch_bounds__(kThreads, 2)
 doa_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovParams p) {
     constexpr uint32_t RAW = kTile * A;
     constexpr uint32_t IDESC = idesc_s8_s32_mn(128, 128);
@@ -117,7 +118,7 @@ doa_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovParams p) {
     const long long u_begin = p.n_units * blockIdx.x / gridDim.x;
     const long long u_end = p.n_units * (blockIdx.x + 1) / gridDim.x;
     auto fail = [&](unsigned code) {
-        cov_error(code);
+        cov_error(p.err, code);
         *s_fail = 1;
     };
 
@@ -266,14 +267,17 @@ EncodeTiledFn encode_fn_cov() {
 
 template <int A>
 bf_status launch_cov(cudaStream_t stream, const CUtensorMap& map, const CovParams& p) {
-    const size_t smem = kXStages * kXBytes + kRawStages * kTile * A + 256 + 1024;
+    // at least 100 KB, so that no more than two CTAs (2 x 256 TMEM columns)
+    // share an SM and tcgen05.alloc never has to wait for a column
+    const size_t smem = std::max<size_t>(kXStages * kXBytes + kRawStages * kTile * A + 256 + 1024, 100 * 1024);
     auto kern = doa_cov_kernel<A>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return cuda_status(e, "doa_cov_kernel smem attribute");
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int grid = static_cast<int>(std::min<long long>(sms, p.n_units));
+    // two CTAs per SM (each 256 TMEM columns): twice the tiles in flight
+    const int grid = static_cast<int>(std::min<long long>(2LL * sms, p.n_units));
     kern<<<grid, kThreads, smem, stream>>>(map, p);
     return cuda_status(cudaGetLastError(), "doa_cov_kernel launch");
 }
@@ -305,6 +309,7 @@ bf_status launch_doa_covariance(cudaStream_t stream, const uint8_t* v, int32_t* 
     if (r != CUDA_SUCCESS) return set_error(BF_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string(r));
     CovParams p{};
     p.out = out;
+    p.err = device_error_word();
     p.n_freq = static_cast<int>(d.n_freq);
     p.n_ant = static_cast<int>(d.n_ant);
     p.block_len = static_cast<int>(block_len);

@@ -103,27 +103,35 @@ __global__ void doa_fold_kernel(const int32_t* __restrict R, int n_blocks, int n
     }
 }
 
-// One thread per grid point; channels summed in order inside the thread.
-__global__ void doa_scan_kernel(const Cd* __restrict S, const Cd* __restrict Lf, const int* __restrict ok,
-                                const float* __restrict pos, const double* __restrict kw, int n_freq, int M,
-                                double l_first, double l_step, int n, double m_fixed, double* __restrict bartlett,
-                                double* __restrict capon) {
+// A CTA of 8 warps takes 32 grid points of one block: lane = grid point,
+// warp w sums the channels f = w, w + 8, ... in increasing order, and the
+// eight partial sums are added in warp order at the end (a fixed order, so
+// results are deterministic).
+constexpr int kScanWarps = 8;
+
+__global__ void __launch_bounds__(kScanWarps * 32)
+doa_scan_kernel(const Cd* __restrict S, const Cd* __restrict Lf, const int* __restrict ok,
+                const float* __restrict pos, const double* __restrict kw, int n_freq, int M,
+                double l_first, double l_step, int n, double m_fixed, double* __restrict bartlett,
+                double* __restrict capon) {
     const int b = blockIdx.y;
-    const int l = blockIdx.x * blockDim.x + threadIdx.x;
-    __shared__ Cd sS[kMaxM * kMaxM], sL[kMaxM * kMaxM];
-    __shared__ int sok;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int l = blockIdx.x * 32 + lane;
+    extern __shared__ Cd scan_smem[];              // [warp][S | L][M * M]
+    Cd* sSw = scan_smem + static_cast<size_t>(warp) * 2 * M * M;
+    Cd* sLw = sSw + M * M;
+    __shared__ double red_b[kScanWarps][32], red_c[kScanWarps][32];
     const double lv = l_first + static_cast<double>(l) * l_step;
     double pb = 0.0, pc = 0.0;
-    for (int f = 0; f < n_freq; ++f) {
+    for (int f = warp; f < n_freq; f += kScanWarps) {
         const size_t base = (static_cast<size_t>(b) * n_freq + f) * M * M;
-        __syncthreads();
-        for (int e = threadIdx.x; e < M * M; e += blockDim.x) {
-            sS[e] = S[base + e];
-            sL[e] = Lf[base + e];
+        __syncwarp();
+        for (int e = lane; e < M * M; e += 32) {
+            sSw[e] = S[base + e];
+            sLw[e] = Lf[base + e];
         }
-        if (threadIdx.x == 0) sok = ok[static_cast<size_t>(b) * n_freq + f];
-        __syncthreads();
-        if (l >= n) continue;
+        const int fok = ok[static_cast<size_t>(b) * n_freq + f];
+        __syncwarp();
         Cd a[kMaxM];
         for (int i = 0; i < M; ++i) {
             const double ph = kw[f] * (static_cast<double>(pos[3 * i]) * lv + static_cast<double>(pos[3 * i + 1]) * m_fixed);
@@ -136,33 +144,41 @@ __global__ void doa_scan_kernel(const Cd* __restrict S, const Cd* __restrict Lf,
         for (int r = 0; r < M; ++r) {
             double tr = 0.0, ti = 0.0;
             for (int c = 0; c < M; ++c) {
-                const Cd x = sS[r * M + c];
+                const Cd x = sSw[r * M + c];
                 tr += x.re * a[c].re - x.im * a[c].im;
                 ti += x.re * a[c].im + x.im * a[c].re;
             }
             acc += a[r].re * tr + a[r].im * ti;
         }
         pb += acc;
-        if (sok) {
+        if (fok) {
             Cd v[kMaxM];
             double nrm = 0.0;
             for (int i = 0; i < M; ++i) {
                 double sr = a[i].re, si = a[i].im;
                 for (int k = 0; k < i; ++k) {
-                    const Cd x = sL[i * M + k];
+                    const Cd x = sLw[i * M + k];
                     sr -= x.re * v[k].re - x.im * v[k].im;
                     si -= x.re * v[k].im + x.im * v[k].re;
                 }
-                const double d = sL[i * M + i].re;
+                const double d = sLw[i * M + i].re;
                 v[i] = Cd{sr / d, si / d};
                 nrm += v[i].re * v[i].re + v[i].im * v[i].im;
             }
             pc += nrm > 0.0 ? 1.0 / nrm : 0.0;
         }
     }
-    if (l < n) {
-        bartlett[static_cast<size_t>(b) * n + l] = pb;
-        capon[static_cast<size_t>(b) * n + l] = pc;
+    red_b[warp][lane] = pb;
+    red_c[warp][lane] = pc;
+    __syncthreads();
+    if (warp == 0 && l < n) {
+        double sb = 0.0, sc = 0.0;
+        for (int w = 0; w < kScanWarps; ++w) {
+            sb += red_b[w][lane];
+            sc += red_c[w][lane];
+        }
+        bartlett[static_cast<size_t>(b) * n + l] = sb;
+        capon[static_cast<size_t>(b) * n + l] = sc;
     }
 }
 
@@ -214,9 +230,12 @@ bf_status launch_doa_scan(cudaStream_t stream, const int32_t* R, const float* po
     doa_fold_kernel<<<F, 64, 0, stream>>>(R, B, F, A, M, static_cast<int>(block_len), lam, load, S, E, Lc, ok);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_status(e, "doa_fold_kernel launch");
-    const dim3 grid(static_cast<unsigned>((n + 127) / 128), static_cast<unsigned>(B));
-    doa_scan_kernel<<<grid, 128, 0, stream>>>(S, Lc, ok, pos, kw, F, M, l_first, l_step, static_cast<int>(n),
-                                              m_fixed, bartlett, capon);
+    const dim3 grid(static_cast<unsigned>((n + 31) / 32), static_cast<unsigned>(B));
+    const size_t smem = static_cast<size_t>(kScanWarps) * 2 * M * M * sizeof(Cd);
+    e = cudaFuncSetAttribute(doa_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (e != cudaSuccess) return cuda_status(e, "doa_scan_kernel smem attribute");
+    doa_scan_kernel<<<grid, kScanWarps * 32, smem, stream>>>(S, Lc, ok, pos, kw, F, M, l_first, l_step,
+                                                             static_cast<int>(n), m_fixed, bartlett, capon);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_status(e, "doa_scan_kernel launch");
     doa_peak_kernel<<<B, 64, 0, stream>>>(bartlett, capon, static_cast<int>(n), l_first, l_step, l_est);

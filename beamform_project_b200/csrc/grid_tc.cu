@@ -933,6 +933,22 @@ bf_status launch_grid_tensor_served(cudaStream_t stream, const CUtensorMap& map,
     return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernel supports n_ant 32 or 64");
 }
 
+// Device address of the error word for kernels in other translation units
+// (device globals are per translation unit without relocatable device code).
+unsigned* device_error_word() {
+    static std::mutex mu;
+    static unsigned* addr[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lock(mu);
+    if (addr[dev] == nullptr) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_tc_error) != cudaSuccess) return nullptr;
+        addr[dev] = static_cast<unsigned*>(p);
+    }
+    return addr[dev];
+}
+
 bf_status take_tc_error(uint32_t* code) {
     unsigned v = 0, zero = 0;
     cudaError_t e = cudaMemcpyFromSymbol(&v, g_tc_error, sizeof(v));
