@@ -932,15 +932,11 @@ def run_serve(args):
         return
     import torch
     from beamform_project_b200 import native, serve
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
+    from beamform_project_b200.replicas import Replicas
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    reps = Replicas("nccl", timeout_s=600)
+    world, rank = reps.world, reps.rank
     jobs = serve_jobs(args.serve_seconds)
     budget = int(args.serve_budget_gb * 1e9)
     srv = serve.Server(budget, max_jobs=args.serve_max_jobs, pool_spectra=SERVE_POOL, pool_seed=SERVE_SEED + rank,
@@ -959,8 +955,7 @@ def run_serve(args):
     st0 = srv.stats()
     n_warm_steps = len(srv.step_times())
 
-    if dist:
-        dist.barrier()
+    reps.barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clocks:
@@ -975,11 +970,8 @@ def run_serve(args):
     times = srv.step_times()[n_warm_steps:]
     samples = st["beam_samples"] - st0["beam_samples"]
     steps = st["steps"] - st0["steps"]
-    if dist:
-        t = torch.tensor([el_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        el_ms = float(t.item())
-    value = samples * world / (el_ms / 1e3)
+    el_ms = reps.max(el_ms)
+    value = reps.sum(samples) / (el_ms / 1e3)
 
     # algorithmic bytes: every job window reads its voltage once and writes its outputs
     vbytes = 0
@@ -1060,8 +1052,7 @@ def run_serve(args):
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = serve_cpu_baseline(jobs, budget_s=args.cpu_seconds)
         print(json.dumps(line), flush=True)
-    if dist:
-        dist.destroy_process_group()
+    reps.close()
 
 
 
