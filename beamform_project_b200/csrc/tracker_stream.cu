@@ -107,12 +107,7 @@ tracker_stream_kernel(const uint8_t* __restrict__ v, const float* __restrict__ p
             }
         }
     };
-    // software pipeline: the next block's loads are in flight while this one computes
-    uint32_t wg[NW], wg8[NW];
-    load_rows(t_begin, wg, wg8);
-    for (int tb = t_begin; tb < t_end; tb += 16) {
-        uint32_t ng[NW], ng8[NW];
-        load_rows(tb + 16, ng, ng8);
+    auto process = [&](const uint32_t (&wg)[NW], const uint32_t (&wg8)[NW], int tb) {
         float d[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll
         for (int j = 0; j < NW; ++j) {
@@ -146,10 +141,24 @@ tracker_stream_kernel(const uint8_t* __restrict__ v, const float* __restrict__ p
             }
             __syncthreads();
         }
+    };
+    // software pipeline: the next two blocks' loads are in flight while two
+    // blocks compute (blocks are still summed one by one in increasing time)
+    uint32_t wa[NW], wa8[NW], wb[NW], wb8[NW];
+    load_rows(t_begin, wa, wa8);
+    load_rows(t_begin + 16, wb, wb8);
+    for (int tb = t_begin; tb < t_end; tb += 32) {
+        uint32_t na[NW], na8[NW], nb[NW], nb8[NW];
+        load_rows(tb + 32, na, na8);
+        load_rows(tb + 48, nb, nb8);
+        process(wa, wa8, tb);
+        if (tb + 16 < t_end) process(wb, wb8, tb + 16);  // uniform across the CTA
 #pragma unroll
         for (int j = 0; j < NW; ++j) {
-            wg[j] = ng[j];
-            wg8[j] = ng8[j];
+            wa[j] = na[j];
+            wa8[j] = na8[j];
+            wb[j] = nb[j];
+            wb8[j] = nb8[j];
         }
     }
     if (integrated != nullptr) {
