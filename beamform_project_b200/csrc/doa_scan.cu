@@ -32,14 +32,21 @@ struct Cd {
     double re, im;
 };
 
-// One block of threads per channel; thread 0 walks the blocks in order.
+// One CTA per channel walks the blocks in order (the forgetting recursion).
+// Smoothing, forward-backward and forgetting run over the M x M elements;
+// thread 0 factors S + E I (Cholesky, shared memory); thread j forms column j
+// of L^{-1}; the threads then form Q = L^{-H} L^{-1} = (S + E I)^{-1} by
+// elements, so the scan evaluates Capon's |L^{-1} a|^2 as a^H Q a.
 __global__ void doa_fold_kernel(const int32_t* __restrict R, int n_blocks, int n_freq, int A, int M, int K,
                                 double lam, double load, Cd* __restrict S_out, double* __restrict E_out,
-                                Cd* __restrict L_out, int* __restrict ok_out) {
+                                Cd* __restrict Q_out, int* __restrict ok_out) {
     const int f = blockIdx.x;
     __shared__ Cd Rt[kMaxM * kMaxM];
     __shared__ Cd S[kMaxM * kMaxM];
+    __shared__ Cd Lc[kMaxM * kMaxM];
+    __shared__ Cd Li[kMaxM * kMaxM];
     __shared__ double E;
+    __shared__ int ok;
     const int L = A - M + 1;
     for (int b = 0; b < n_blocks; ++b) {
         const int32_t* Rf = R + (static_cast<size_t>(b) * n_freq + f) * A * A * 2;
@@ -77,9 +84,8 @@ __global__ void doa_fold_kernel(const int32_t* __restrict R, int n_blocks, int n
         if (threadIdx.x == 0) {
             E_out[static_cast<size_t>(b) * n_freq + f] = E;
             // Cholesky of S + E I (lower triangular, FP64)
-            Cd Lc[kMaxM * kMaxM];
-            int ok = 1;
-            for (int i = 0; i < M && ok; ++i) {
+            int good = 1;
+            for (int i = 0; i < M && good; ++i) {
                 for (int j = 0; j <= i; ++j) {
                     double sr = S[i * M + j].re + (i == j ? E : 0.0), si = S[i * M + j].im;
                     for (int k = 0; k < j; ++k) {
@@ -88,7 +94,7 @@ __global__ void doa_fold_kernel(const int32_t* __restrict R, int n_blocks, int n
                         si -= x.im * y.re - x.re * y.im;
                     }
                     if (i == j) {
-                        if (!(sr > 1e-300)) { ok = 0; break; }
+                        if (!(sr > 1e-300)) { good = 0; break; }
                         Lc[i * M + i] = Cd{sqrt(sr), 0.0};
                     } else {
                         const double d = Lc[j * M + j].re;
@@ -96,89 +102,154 @@ __global__ void doa_fold_kernel(const int32_t* __restrict R, int n_blocks, int n
                     }
                 }
             }
-            for (int e = 0; e < M * M; ++e) L_out[base + e] = ok ? Lc[e] : Cd{0.0, 0.0};
-            ok_out[static_cast<size_t>(b) * n_freq + f] = ok;
+            ok = good;
+            ok_out[static_cast<size_t>(b) * n_freq + f] = good;
+        }
+        __syncthreads();
+        if (ok && threadIdx.x < M) {  // column j of L^{-1} by forward substitution
+            const int j = threadIdx.x;
+            for (int i = 0; i < j; ++i) Li[i * M + j] = Cd{0.0, 0.0};
+            Li[j * M + j] = Cd{1.0 / Lc[j * M + j].re, 0.0};
+            for (int i = j + 1; i < M; ++i) {
+                double sr = 0.0, si = 0.0;
+                for (int k = j; k < i; ++k) {
+                    const Cd x = Lc[i * M + k], y = Li[k * M + j];
+                    sr += x.re * y.re - x.im * y.im;
+                    si += x.re * y.im + x.im * y.re;
+                }
+                const double d = Lc[i * M + i].re;
+                Li[i * M + j] = Cd{-sr / d, -si / d};
+            }
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < M * M; e += blockDim.x) {
+            const int i = e / M, j = e % M;
+            double qr = 0.0, qi = 0.0;
+            if (ok) {
+                for (int k = i > j ? i : j; k < M; ++k) {
+                    const Cd x = Li[k * M + i], y = Li[k * M + j];  // conj(x) * y
+                    qr += x.re * y.re + x.im * y.im;
+                    qi += x.re * y.im - x.im * y.re;
+                }
+            }
+            Q_out[base + e] = Cd{qr, qi};
         }
         __syncthreads();
     }
 }
 
-// A CTA of 8 warps takes 32 grid points of one block: lane = grid point,
-// warp w sums the channels f = w, w + 8, ... in increasing order, and the
-// eight partial sums are added in warp order at the end (a fixed order, so
-// results are deterministic).
-constexpr int kScanWarps = 8;
+// A CTA of 16 warps takes 32 grid points and 8 blocks: lane = grid point,
+// warp w the channels f = w, w + 16, ... in increasing order.  The steering
+// vector of (channel, point) is formed once and used for all 8 blocks;
+// Bartlett a^H S a and Capon 1 / (a^H Q a), Q = (S + eps I)^{-1}, are
+// Hermitian quadratic forms (diagonal plus twice the real part of the upper
+// triangle).  Per-warp partial sums are added in warp order at the end (a
+// fixed order, so results are deterministic).
+constexpr int kScanWarps = 16;
+constexpr int kScanBlocks = 8;
 
+template <int M>
 __global__ void __launch_bounds__(kScanWarps * 32)
-doa_scan_kernel(const Cd* __restrict S, const Cd* __restrict Lf, const int* __restrict ok,
-                const float* __restrict pos, const double* __restrict kw, int n_freq, int M,
+doa_scan_kernel(const Cd* __restrict S, const Cd* __restrict Q, const int* __restrict ok,
+                const float* __restrict pos, const double* __restrict kw, int n_blocks, int n_freq,
                 double l_first, double l_step, int n, double m_fixed, double* __restrict bartlett,
                 double* __restrict capon) {
-    const int b = blockIdx.y;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int l = blockIdx.x * 32 + lane;
-    extern __shared__ Cd scan_smem[];              // [warp][S | L][M * M]
-    Cd* sSw = scan_smem + static_cast<size_t>(warp) * 2 * M * M;
-    Cd* sLw = sSw + M * M;
-    __shared__ double red_b[kScanWarps][32], red_c[kScanWarps][32];
+    const int b0 = blockIdx.y * kScanBlocks;
+    const int nb = min(kScanBlocks, n_blocks - b0);
+    extern __shared__ double scan_red[];  // [2][warps][kScanBlocks][32]
     const double lv = l_first + static_cast<double>(l) * l_step;
-    double pb = 0.0, pc = 0.0;
+    double pb[kScanBlocks], pc[kScanBlocks];
+#pragma unroll
+    for (int i = 0; i < kScanBlocks; ++i) pb[i] = pc[i] = 0.0;
+    double px[M], py[M];
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+        px[i] = static_cast<double>(pos[3 * i]);
+        py[i] = static_cast<double>(pos[3 * i + 1]);
+    }
     for (int f = warp; f < n_freq; f += kScanWarps) {
-        const size_t base = (static_cast<size_t>(b) * n_freq + f) * M * M;
-        __syncwarp();
-        for (int e = lane; e < M * M; e += 32) {
-            sSw[e] = S[base + e];
-            sLw[e] = Lf[base + e];
-        }
-        const int fok = ok[static_cast<size_t>(b) * n_freq + f];
-        __syncwarp();
-        Cd a[kMaxM];
+        Cd a[M];
+        double mag[M];
+        const double k = kw[f];
+#pragma unroll
         for (int i = 0; i < M; ++i) {
-            const double ph = kw[f] * (static_cast<double>(pos[3 * i]) * lv + static_cast<double>(pos[3 * i + 1]) * m_fixed);
+            const double ph = k * (px[i] * lv + py[i] * m_fixed);
             const double rr = ph - kTwoPi * rint(ph * (1.0 / kTwoPi));
             float s, c;
             sincosf(static_cast<float>(rr), &s, &c);
             a[i] = Cd{static_cast<double>(c), -static_cast<double>(s)};
+            mag[i] = a[i].re * a[i].re + a[i].im * a[i].im;
         }
-        double acc = 0.0;
-        for (int r = 0; r < M; ++r) {
-            double tr = 0.0, ti = 0.0;
-            for (int c = 0; c < M; ++c) {
-                const Cd x = sSw[r * M + c];
-                tr += x.re * a[c].re - x.im * a[c].im;
-                ti += x.re * a[c].im + x.im * a[c].re;
-            }
-            acc += a[r].re * tr + a[r].im * ti;
-        }
-        pb += acc;
-        if (fok) {
-            Cd v[kMaxM];
-            double nrm = 0.0;
-            for (int i = 0; i < M; ++i) {
-                double sr = a[i].re, si = a[i].im;
-                for (int k = 0; k < i; ++k) {
-                    const Cd x = sLw[i * M + k];
-                    sr -= x.re * v[k].re - x.im * v[k].im;
-                    si -= x.re * v[k].im + x.im * v[k].re;
+        auto quad = [&](const Cd* __restrict X) {
+            double diag = 0.0, off = 0.0;
+#pragma unroll
+            for (int r = 0; r < M; ++r) {
+                diag += X[r * M + r].re * mag[r];
+                double tr = 0.0, ti = 0.0;
+#pragma unroll
+                for (int c = r + 1; c < M; ++c) {
+                    const Cd x = X[r * M + c];
+                    tr += x.re * a[c].re - x.im * a[c].im;
+                    ti += x.re * a[c].im + x.im * a[c].re;
                 }
-                const double d = sLw[i * M + i].re;
-                v[i] = Cd{sr / d, si / d};
-                nrm += v[i].re * v[i].re + v[i].im * v[i].im;
+                off += a[r].re * tr + a[r].im * ti;
             }
-            pc += nrm > 0.0 ? 1.0 / nrm : 0.0;
+            return diag + 2.0 * off;
+        };
+#pragma unroll
+        for (int bi = 0; bi < kScanBlocks; ++bi) {
+            if (bi < nb) {
+                const size_t cell = static_cast<size_t>(b0 + bi) * n_freq + f;
+                pb[bi] += quad(S + cell * M * M);
+                if (ok[cell]) {
+                    const double q = quad(Q + cell * M * M);
+                    pc[bi] += q > 0.0 ? 1.0 / q : 0.0;
+                }
+            }
         }
     }
-    red_b[warp][lane] = pb;
-    red_c[warp][lane] = pc;
+#pragma unroll
+    for (int bi = 0; bi < kScanBlocks; ++bi) {
+        scan_red[((0 * kScanWarps + warp) * kScanBlocks + bi) * 32 + lane] = pb[bi];
+        scan_red[((1 * kScanWarps + warp) * kScanBlocks + bi) * 32 + lane] = pc[bi];
+    }
     __syncthreads();
-    if (warp == 0 && l < n) {
+    if (warp < nb && l < n) {
         double sb = 0.0, sc = 0.0;
         for (int w = 0; w < kScanWarps; ++w) {
-            sb += red_b[w][lane];
-            sc += red_c[w][lane];
+            sb += scan_red[((0 * kScanWarps + w) * kScanBlocks + warp) * 32 + lane];
+            sc += scan_red[((1 * kScanWarps + w) * kScanBlocks + warp) * 32 + lane];
         }
-        bartlett[static_cast<size_t>(b) * n + l] = sb;
-        capon[static_cast<size_t>(b) * n + l] = sc;
+        bartlett[static_cast<size_t>(b0 + warp) * n + l] = sb;
+        capon[static_cast<size_t>(b0 + warp) * n + l] = sc;
+    }
+}
+
+template <int M>
+bf_status launch_scan_m(cudaStream_t stream, const Cd* S, const Cd* Q, const int* ok, const float* pos,
+                        const double* kw, int B, int F, double l_first, double l_step, int n, double m_fixed,
+                        double* bartlett, double* capon) {
+    const dim3 grid(static_cast<unsigned>((n + 31) / 32), static_cast<unsigned>((B + kScanBlocks - 1) / kScanBlocks));
+    const size_t smem = 2ull * kScanWarps * kScanBlocks * 32 * sizeof(double);
+    cudaError_t e = cudaFuncSetAttribute(doa_scan_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(smem));
+    if (e != cudaSuccess) return cuda_status(e, "doa_scan_kernel smem attribute");
+    doa_scan_kernel<M><<<grid, kScanWarps * 32, smem, stream>>>(S, Q, ok, pos, kw, B, F, l_first, l_step, n,
+                                                               m_fixed, bartlett, capon);
+    return cuda_status(cudaGetLastError(), "doa_scan_kernel launch");
+}
+
+template <int M>
+bf_status dispatch_scan(int m, cudaStream_t stream, const Cd* S, const Cd* Q, const int* ok, const float* pos,
+                        const double* kw, int B, int F, double l_first, double l_step, int n, double m_fixed,
+                        double* bartlett, double* capon) {
+    if constexpr (M > kMaxM) {
+        return set_error(BF_ERR_UNSUPPORTED, "the DOA scan supports at most 16 elements after smoothing");
+    } else {
+        if (m == M) return launch_scan_m<M>(stream, S, Q, ok, pos, kw, B, F, l_first, l_step, n, m_fixed, bartlett, capon);
+        return dispatch_scan<M + 1>(m, stream, S, Q, ok, pos, kw, B, F, l_first, l_step, n, m_fixed, bartlett, capon);
     }
 }
 
@@ -224,20 +295,14 @@ bf_status launch_doa_scan(cudaStream_t stream, const int32_t* R, const float* po
     const int B = static_cast<int>(d.n_time / block_len), F = static_cast<int>(d.n_freq);
     const uint64_t cells = static_cast<uint64_t>(B) * F;
     auto* S = static_cast<Cd*>(workspace);
-    Cd* Lc = S + cells * M * M;
+    Cd* Lc = S + cells * M * M;  // the fold writes Q = (S + E I)^{-1} here
     auto* E = reinterpret_cast<double*>(Lc + cells * M * M);
     auto* ok = reinterpret_cast<int*>(E + cells);
     doa_fold_kernel<<<F, 64, 0, stream>>>(R, B, F, A, M, static_cast<int>(block_len), lam, load, S, E, Lc, ok);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_status(e, "doa_fold_kernel launch");
-    const dim3 grid(static_cast<unsigned>((n + 31) / 32), static_cast<unsigned>(B));
-    const size_t smem = static_cast<size_t>(kScanWarps) * 2 * M * M * sizeof(Cd);
-    e = cudaFuncSetAttribute(doa_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    if (e != cudaSuccess) return cuda_status(e, "doa_scan_kernel smem attribute");
-    doa_scan_kernel<<<grid, kScanWarps * 32, smem, stream>>>(S, Lc, ok, pos, kw, F, M, l_first, l_step,
-                                                             static_cast<int>(n), m_fixed, bartlett, capon);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_status(e, "doa_scan_kernel launch");
+    BF_RETURN_IF(dispatch_scan<1>(M, stream, S, Lc, ok, pos, kw, B, F, l_first, l_step, static_cast<int>(n), m_fixed,
+                                  bartlett, capon));
     doa_peak_kernel<<<B, 64, 0, stream>>>(bartlett, capon, static_cast<int>(n), l_first, l_step, l_est);
     return cuda_status(cudaGetLastError(), "doa_peak_kernel launch");
 }
