@@ -32,121 +32,160 @@ struct Cd {
     double re, im;
 };
 
-// One CTA per channel walks the blocks in order (the forgetting recursion).
-// Smoothing, forward-backward and forgetting run over the M x M elements;
-// thread 0 factors S + E I (Cholesky, shared memory); thread j forms column j
-// of L^{-1}; the threads then form Q = L^{-H} L^{-1} = (S + E I)^{-1} by
-// elements, so the scan evaluates Capon's |L^{-1} a|^2 as a^H Q a.
-__global__ void doa_fold_kernel(const int32_t* __restrict R, int n_blocks, int n_freq, int A, int M, int K,
-                                double lam, double load, Cd* __restrict S_out, double* __restrict E_out,
-                                Cd* __restrict Q_out, int* __restrict ok_out) {
-    const int f = blockIdx.x;
+// Fold, in three launches so that only the forgetting recursion is serial:
+//  doa_smooth_kernel  (block, channel) cells in parallel: smoothing over the
+//                     L = A - M + 1 sub-arrays, 1/K, forward-backward, and
+//                     the loading eps = load * tr / M (the averaged matrix is
+//                     parked in the Q slot of the workspace);
+//  doa_forget_kernel  per channel, blocks in order: S = lam S + (1 - lam) R^,
+//                     E = lam E + (1 - lam) eps (first block: S = R^, E = eps);
+//  doa_factor_kernel  cells in parallel: Cholesky L L^H = S + E I (thread 0),
+//                     column j of L^{-1} by thread j, and Q = L^{-H} L^{-1} =
+//                     (S + E I)^{-1} by elements, so the scan evaluates
+//                     Capon's |L^{-1} a|^2 as the quadratic form a^H Q a.
+__global__ void doa_smooth_kernel(const int32_t* __restrict R, int n_freq, int A, int M, int K,
+                                  double load, Cd* __restrict Rhat_out, double* __restrict eps_out) {
+    const int f = blockIdx.x, b = blockIdx.y;
     __shared__ Cd Rt[kMaxM * kMaxM];
-    __shared__ Cd S[kMaxM * kMaxM];
-    __shared__ Cd Lc[kMaxM * kMaxM];
-    __shared__ Cd Li[kMaxM * kMaxM];
-    __shared__ double E;
-    __shared__ int ok;
     const int L = A - M + 1;
-    for (int b = 0; b < n_blocks; ++b) {
-        const int32_t* Rf = R + (static_cast<size_t>(b) * n_freq + f) * A * A * 2;
-        for (int e = threadIdx.x; e < M * M; e += blockDim.x) {
-            const int r = e / M, c = e % M;
-            double sr = 0.0, si = 0.0;
-            for (int s = 0; s < L; ++s) {
-                sr += static_cast<double>(Rf[2 * ((s + r) * A + s + c)]);
-                si += static_cast<double>(Rf[2 * ((s + r) * A + s + c) + 1]);
-            }
-            Rt[e] = Cd{sr / K / L, si / K / L};
+    const int32_t* Rf = R + (static_cast<size_t>(b) * n_freq + f) * A * A * 2;
+    for (int e = threadIdx.x; e < M * M; e += blockDim.x) {
+        const int r = e / M, c = e % M;
+        double sr = 0.0, si = 0.0;
+        for (int s = 0; s < L; ++s) {
+            sr += static_cast<double>(Rf[2 * ((s + r) * A + s + c)]);
+            si += static_cast<double>(Rf[2 * ((s + r) * A + s + c) + 1]);
         }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double tr = 0.0;
-            for (int r = 0; r < M; ++r) {
-                const Cd x = Rt[r * M + r];
-                tr += L > 1 ? 0.5 * (x.re + Rt[(M - 1 - r) * M + (M - 1 - r)].re) : x.re;
-            }
-            const double eps = load * tr / M;
-            E = (b == 0 || lam >= 1.0) ? eps : lam * E + (1.0 - lam) * eps;
+        Rt[e] = Cd{sr / K / L, si / K / L};
+    }
+    __syncthreads();
+    const size_t cell = static_cast<size_t>(b) * n_freq + f;
+    if (threadIdx.x == 0) {
+        double tr = 0.0;
+        for (int r = 0; r < M; ++r) {
+            const Cd x = Rt[r * M + r];
+            tr += L > 1 ? 0.5 * (x.re + Rt[(M - 1 - r) * M + (M - 1 - r)].re) : x.re;
         }
-        for (int e = threadIdx.x; e < M * M; e += blockDim.x) {
-            const int r = e / M, c = e % M;
-            Cd x = Rt[e];
-            if (L > 1) {
-                const Cd y = Rt[(M - 1 - r) * M + (M - 1 - c)];
-                x = Cd{0.5 * (x.re + y.re), 0.5 * (x.im - y.im)};
-            }
-            S[e] = (b == 0 || lam >= 1.0) ? x : Cd{lam * S[e].re + (1.0 - lam) * x.re, lam * S[e].im + (1.0 - lam) * x.im};
+        eps_out[cell] = load * tr / M;
+    }
+    for (int e = threadIdx.x; e < M * M; e += blockDim.x) {
+        const int r = e / M, c = e % M;
+        Cd x = Rt[e];
+        if (L > 1) {
+            const Cd y = Rt[(M - 1 - r) * M + (M - 1 - c)];
+            x = Cd{0.5 * (x.re + y.re), 0.5 * (x.im - y.im)};
         }
-        __syncthreads();
-        const size_t base = (static_cast<size_t>(b) * n_freq + f) * M * M;
-        for (int e = threadIdx.x; e < M * M; e += blockDim.x) S_out[base + e] = S[e];
-        if (threadIdx.x == 0) {
-            E_out[static_cast<size_t>(b) * n_freq + f] = E;
-            // Cholesky of S + E I (lower triangular, FP64)
-            int good = 1;
-            for (int i = 0; i < M && good; ++i) {
-                for (int j = 0; j <= i; ++j) {
-                    double sr = S[i * M + j].re + (i == j ? E : 0.0), si = S[i * M + j].im;
-                    for (int k = 0; k < j; ++k) {
-                        const Cd x = Lc[i * M + k], y = Lc[j * M + k];  // x * conj(y)
-                        sr -= x.re * y.re + x.im * y.im;
-                        si -= x.im * y.re - x.re * y.im;
-                    }
-                    if (i == j) {
-                        if (!(sr > 1e-300)) { good = 0; break; }
-                        Lc[i * M + i] = Cd{sqrt(sr), 0.0};
-                    } else {
-                        const double d = Lc[j * M + j].re;
-                        Lc[i * M + j] = Cd{sr / d, si / d};
-                    }
-                }
-            }
-            ok = good;
-            ok_out[static_cast<size_t>(b) * n_freq + f] = good;
-        }
-        __syncthreads();
-        if (ok && threadIdx.x < M) {  // column j of L^{-1} by forward substitution
-            const int j = threadIdx.x;
-            for (int i = 0; i < j; ++i) Li[i * M + j] = Cd{0.0, 0.0};
-            Li[j * M + j] = Cd{1.0 / Lc[j * M + j].re, 0.0};
-            for (int i = j + 1; i < M; ++i) {
-                double sr = 0.0, si = 0.0;
-                for (int k = j; k < i; ++k) {
-                    const Cd x = Lc[i * M + k], y = Li[k * M + j];
-                    sr += x.re * y.re - x.im * y.im;
-                    si += x.re * y.im + x.im * y.re;
-                }
-                const double d = Lc[i * M + i].re;
-                Li[i * M + j] = Cd{-sr / d, -si / d};
-            }
-        }
-        __syncthreads();
-        for (int e = threadIdx.x; e < M * M; e += blockDim.x) {
-            const int i = e / M, j = e % M;
-            double qr = 0.0, qi = 0.0;
-            if (ok) {
-                for (int k = i > j ? i : j; k < M; ++k) {
-                    const Cd x = Li[k * M + i], y = Li[k * M + j];  // conj(x) * y
-                    qr += x.re * y.re + x.im * y.im;
-                    qi += x.re * y.im - x.im * y.re;
-                }
-            }
-            Q_out[base + e] = Cd{qr, qi};
-        }
-        __syncthreads();
+        Rhat_out[cell * M * M + e] = x;
     }
 }
 
-// A CTA of 16 warps takes 32 grid points and 8 blocks: lane = grid point,
-// warp w the channels f = w, w + 16, ... in increasing order.  The steering
-// vector of (channel, point) is formed once and used for all 8 blocks;
-// Bartlett a^H S a and Capon 1 / (a^H Q a), Q = (S + eps I)^{-1}, are
-// Hermitian quadratic forms (diagonal plus twice the real part of the upper
-// triangle).  Per-warp partial sums are added in warp order at the end (a
+__global__ void doa_forget_kernel(const Cd* __restrict Rhat, int n_blocks, int n_freq, int M, double lam,
+                                  Cd* __restrict S_out, double* __restrict E) {
+    const int f = blockIdx.x;
+    for (int e = threadIdx.x; e < M * M; e += blockDim.x) {
+        Cd s{0.0, 0.0};
+        for (int b = 0; b < n_blocks; ++b) {
+            const size_t at = (static_cast<size_t>(b) * n_freq + f) * M * M + e;
+            const Cd x = Rhat[at];
+            s = (b == 0 || lam >= 1.0) ? x : Cd{lam * s.re + (1.0 - lam) * x.re, lam * s.im + (1.0 - lam) * x.im};
+            S_out[at] = s;
+        }
+    }
+    if (threadIdx.x == 0) {
+        double acc = 0.0;
+        for (int b = 0; b < n_blocks; ++b) {
+            const size_t cell = static_cast<size_t>(b) * n_freq + f;
+            const double eps = E[cell];
+            acc = (b == 0 || lam >= 1.0) ? eps : lam * acc + (1.0 - lam) * eps;
+            E[cell] = acc;
+        }
+    }
+}
+
+__global__ void doa_factor_kernel(const Cd* __restrict S_in, const double* __restrict E_in, int n_freq, int M,
+                                  Cd* __restrict Q_out, int* __restrict ok_out) {
+    const int f = blockIdx.x, b = blockIdx.y;
+    const size_t cell = static_cast<size_t>(b) * n_freq + f;
+    const size_t base = cell * M * M;
+    __shared__ Cd S[kMaxM * kMaxM];
+    __shared__ Cd Lc[kMaxM * kMaxM];
+    __shared__ Cd Li[kMaxM * kMaxM];
+    __shared__ int ok;
+    for (int e = threadIdx.x; e < M * M; e += blockDim.x) S[e] = S_in[base + e];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const double E = E_in[cell];
+        int good = 1;
+        for (int i = 0; i < M && good; ++i) {
+            for (int j = 0; j <= i; ++j) {
+                double sr = S[i * M + j].re + (i == j ? E : 0.0), si = S[i * M + j].im;
+                for (int k = 0; k < j; ++k) {
+                    const Cd x = Lc[i * M + k], y = Lc[j * M + k];  // x * conj(y)
+                    sr -= x.re * y.re + x.im * y.im;
+                    si -= x.im * y.re - x.re * y.im;
+                }
+                if (i == j) {
+                    if (!(sr > 1e-300)) { good = 0; break; }
+                    Lc[i * M + i] = Cd{sqrt(sr), 0.0};
+                } else {
+                    const double d = Lc[j * M + j].re;
+                    Lc[i * M + j] = Cd{sr / d, si / d};
+                }
+            }
+        }
+        ok = good;
+        ok_out[cell] = good;
+    }
+    __syncthreads();
+    if (ok && threadIdx.x < M) {  // column j of L^{-1} by forward substitution
+        const int j = threadIdx.x;
+        for (int i = 0; i < j; ++i) Li[i * M + j] = Cd{0.0, 0.0};
+        Li[j * M + j] = Cd{1.0 / Lc[j * M + j].re, 0.0};
+        for (int i = j + 1; i < M; ++i) {
+            double sr = 0.0, si = 0.0;
+            for (int k = j; k < i; ++k) {
+                const Cd x = Lc[i * M + k], y = Li[k * M + j];
+                sr += x.re * y.re - x.im * y.im;
+                si += x.re * y.im + x.im * y.re;
+            }
+            const double d = Lc[i * M + i].re;
+            Li[i * M + j] = Cd{-sr / d, -si / d};
+        }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < M * M; e += blockDim.x) {
+        const int i = e / M, j = e % M;
+        double qr = 0.0, qi = 0.0;
+        if (ok) {
+            for (int k = i > j ? i : j; k < M; ++k) {
+                const Cd x = Li[k * M + i], y = Li[k * M + j];  // conj(x) * y
+                qr += x.re * y.re + x.im * y.im;
+                qi += x.re * y.im - x.im * y.re;
+            }
+        }
+        Q_out[base + e] = Cd{qr, qi};
+    }
+}
+
+// A CTA of 8 warps takes 32 grid points and 4 blocks: lane = grid point,
+// warp w the channels f = 8 s + w of step s.  The steering vector of
+// (channel, point) is formed once and used for the 4 blocks.  Bartlett
+// a^H S a and Capon 1 / (a^H Q a), Q = (S + eps I)^{-1}, are Hermitian
+// quadratic forms (diagonal plus twice the real part of the upper triangle);
+// the upper triangles of S and Q for the next step's 8 channels x 4 blocks
+// are staged into shared memory with cp.async while the current step
+// computes.  Per-warp partial sums are added in warp order at the end (a
 // fixed order, so results are deterministic).
-constexpr int kScanWarps = 16;
-constexpr int kScanBlocks = 8;
+constexpr int kScanWarps = 8;
+constexpr int kScanBlocks = 4;
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(smem))),
+                 "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 template <int M>
 __global__ void __launch_bounds__(kScanWarps * 32)
@@ -154,11 +193,39 @@ doa_scan_kernel(const Cd* __restrict S, const Cd* __restrict Q, const int* __res
                 const float* __restrict pos, const double* __restrict kw, int n_blocks, int n_freq,
                 double l_first, double l_step, int n, double m_fixed, double* __restrict bartlett,
                 double* __restrict capon) {
+    constexpr int U = M * (M + 1) / 2;                 // upper triangle incl. diagonal
+    constexpr int kPerWarp = kScanBlocks * 2 * U;      // Cd staged per warp and step
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int l = blockIdx.x * 32 + lane;
     const int b0 = blockIdx.y * kScanBlocks;
     const int nb = min(kScanBlocks, n_blocks - b0);
-    extern __shared__ double scan_red[];  // [2][warps][kScanBlocks][32]
+    extern __shared__ Cd scan_stage[];                 // [2][warps][blocks][S | Q][U]
+    __shared__ int s_ok[2][kScanWarps][kScanBlocks];
+    __shared__ double red_b[kScanWarps][kScanBlocks][32], red_c[kScanWarps][kScanBlocks][32];
+    const int n_steps = (n_freq + kScanWarps - 1) / kScanWarps;
+
+    // stage step s: thread t copies elements t, t + 256, ... of the step
+    auto stage = [&](int st, int buf) {
+        Cd* dst = scan_stage + static_cast<size_t>(buf) * kScanWarps * kPerWarp;
+        for (int i = threadIdx.x; i < kScanWarps * kPerWarp; i += blockDim.x) {
+            const int w = i / kPerWarp, rem = i % kPerWarp;
+            const int bi = rem / (2 * U), which = (rem / U) & 1, t = rem % U;
+            const int f = st * kScanWarps + w;
+            if (f >= n_freq || bi >= nb) continue;
+            int r = 0, rest = t;  // upper-triangle index -> (r, c)
+            while (rest >= M - r) { rest -= M - r; ++r; }
+            const int c = r + rest;
+            const size_t cell = static_cast<size_t>(b0 + bi) * n_freq + f;
+            cp_async16(dst + i, (which ? Q : S) + cell * M * M + r * M + c);
+        }
+        if (threadIdx.x < kScanWarps * kScanBlocks) {
+            const int w = threadIdx.x / kScanBlocks, bi = threadIdx.x % kScanBlocks;
+            const int f = st * kScanWarps + w;
+            s_ok[buf][w][bi] = (f < n_freq && bi < nb) ? ok[static_cast<size_t>(b0 + bi) * n_freq + f] : 0;
+        }
+        cp_async_commit();
+    };
+
     const double lv = l_first + static_cast<double>(l) * l_step;
     double pb[kScanBlocks], pc[kScanBlocks];
 #pragma unroll
@@ -169,58 +236,69 @@ doa_scan_kernel(const Cd* __restrict S, const Cd* __restrict Q, const int* __res
         px[i] = static_cast<double>(pos[3 * i]);
         py[i] = static_cast<double>(pos[3 * i + 1]);
     }
-    for (int f = warp; f < n_freq; f += kScanWarps) {
-        Cd a[M];
-        double mag[M];
-        const double k = kw[f];
+    stage(0, 0);
+    for (int st = 0; st < n_steps; ++st) {
+        if (st + 1 < n_steps) stage(st + 1, (st + 1) & 1);
+        else cp_async_commit();  // keep one group per step for wait_group 1
+        cp_async_wait_1();
+        __syncthreads();
+        const int f = st * kScanWarps + warp;
+        if (f < n_freq) {
+            const Cd* base = scan_stage + (static_cast<size_t>(st & 1) * kScanWarps + warp) * kPerWarp;
+            Cd a[M];
+            double mag[M];
+            const double k = kw[f];
 #pragma unroll
-        for (int i = 0; i < M; ++i) {
-            const double ph = k * (px[i] * lv + py[i] * m_fixed);
-            const double rr = ph - kTwoPi * rint(ph * (1.0 / kTwoPi));
-            float s, c;
-            sincosf(static_cast<float>(rr), &s, &c);
-            a[i] = Cd{static_cast<double>(c), -static_cast<double>(s)};
-            mag[i] = a[i].re * a[i].re + a[i].im * a[i].im;
-        }
-        auto quad = [&](const Cd* __restrict X) {
-            double diag = 0.0, off = 0.0;
-#pragma unroll
-            for (int r = 0; r < M; ++r) {
-                diag += X[r * M + r].re * mag[r];
-                double tr = 0.0, ti = 0.0;
-#pragma unroll
-                for (int c = r + 1; c < M; ++c) {
-                    const Cd x = X[r * M + c];
-                    tr += x.re * a[c].re - x.im * a[c].im;
-                    ti += x.re * a[c].im + x.im * a[c].re;
-                }
-                off += a[r].re * tr + a[r].im * ti;
+            for (int i = 0; i < M; ++i) {
+                const double ph = k * (px[i] * lv + py[i] * m_fixed);
+                const double rr = ph - kTwoPi * rint(ph * (1.0 / kTwoPi));
+                float sn, cs;
+                sincosf(static_cast<float>(rr), &sn, &cs);
+                a[i] = Cd{static_cast<double>(cs), -static_cast<double>(sn)};
+                mag[i] = a[i].re * a[i].re + a[i].im * a[i].im;
             }
-            return diag + 2.0 * off;
-        };
+            auto quad = [&](const Cd* X) {
+                double diag = 0.0, off = 0.0;
+                int t = 0;
 #pragma unroll
-        for (int bi = 0; bi < kScanBlocks; ++bi) {
-            if (bi < nb) {
-                const size_t cell = static_cast<size_t>(b0 + bi) * n_freq + f;
-                pb[bi] += quad(S + cell * M * M);
-                if (ok[cell]) {
-                    const double q = quad(Q + cell * M * M);
-                    pc[bi] += q > 0.0 ? 1.0 / q : 0.0;
+                for (int r = 0; r < M; ++r) {
+                    diag += X[t].re * mag[r];
+                    ++t;
+                    double tr = 0.0, ti = 0.0;
+#pragma unroll
+                    for (int c = r + 1; c < M; ++c, ++t) {
+                        const Cd x = X[t];
+                        tr += x.re * a[c].re - x.im * a[c].im;
+                        ti += x.re * a[c].im + x.im * a[c].re;
+                    }
+                    off += a[r].re * tr + a[r].im * ti;
+                }
+                return diag + 2.0 * off;
+            };
+#pragma unroll
+            for (int bi = 0; bi < kScanBlocks; ++bi) {
+                if (bi < nb) {
+                    pb[bi] += quad(base + bi * 2 * U);
+                    if (s_ok[st & 1][warp][bi]) {
+                        const double q = quad(base + bi * 2 * U + U);
+                        pc[bi] += q > 0.0 ? 1.0 / q : 0.0;
+                    }
                 }
             }
         }
+        __syncthreads();  // this buffer is restaged two steps on
     }
 #pragma unroll
     for (int bi = 0; bi < kScanBlocks; ++bi) {
-        scan_red[((0 * kScanWarps + warp) * kScanBlocks + bi) * 32 + lane] = pb[bi];
-        scan_red[((1 * kScanWarps + warp) * kScanBlocks + bi) * 32 + lane] = pc[bi];
+        red_b[warp][bi][lane] = pb[bi];
+        red_c[warp][bi][lane] = pc[bi];
     }
     __syncthreads();
     if (warp < nb && l < n) {
         double sb = 0.0, sc = 0.0;
         for (int w = 0; w < kScanWarps; ++w) {
-            sb += scan_red[((0 * kScanWarps + w) * kScanBlocks + warp) * 32 + lane];
-            sc += scan_red[((1 * kScanWarps + w) * kScanBlocks + warp) * 32 + lane];
+            sb += red_b[w][warp][lane];
+            sc += red_c[w][warp][lane];
         }
         bartlett[static_cast<size_t>(b0 + warp) * n + l] = sb;
         capon[static_cast<size_t>(b0 + warp) * n + l] = sc;
@@ -232,7 +310,7 @@ bf_status launch_scan_m(cudaStream_t stream, const Cd* S, const Cd* Q, const int
                         const double* kw, int B, int F, double l_first, double l_step, int n, double m_fixed,
                         double* bartlett, double* capon) {
     const dim3 grid(static_cast<unsigned>((n + 31) / 32), static_cast<unsigned>((B + kScanBlocks - 1) / kScanBlocks));
-    const size_t smem = 2ull * kScanWarps * kScanBlocks * 32 * sizeof(double);
+    const size_t smem = 2ull * kScanWarps * kScanBlocks * 2 * (M * (M + 1) / 2) * sizeof(Cd);
     cudaError_t e = cudaFuncSetAttribute(doa_scan_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(smem));
     if (e != cudaSuccess) return cuda_status(e, "doa_scan_kernel smem attribute");
@@ -292,15 +370,20 @@ bf_status launch_doa_scan(cudaStream_t stream, const int32_t* R, const float* po
     const int A = static_cast<int>(d.n_ant);
     const int M = (subarray > 0 && subarray < d.n_ant) ? static_cast<int>(subarray) : A;
     if (M > kMaxM) return set_error(BF_ERR_UNSUPPORTED, "the DOA scan supports at most 16 elements after smoothing");
+    if (d.n_time / block_len > 65535) return set_error(BF_ERR_OVERFLOW, "at most 65535 covariance blocks per scan");
     const int B = static_cast<int>(d.n_time / block_len), F = static_cast<int>(d.n_freq);
     const uint64_t cells = static_cast<uint64_t>(B) * F;
     auto* S = static_cast<Cd*>(workspace);
     Cd* Lc = S + cells * M * M;  // the fold writes Q = (S + E I)^{-1} here
     auto* E = reinterpret_cast<double*>(Lc + cells * M * M);
     auto* ok = reinterpret_cast<int*>(E + cells);
-    doa_fold_kernel<<<F, 64, 0, stream>>>(R, B, F, A, M, static_cast<int>(block_len), lam, load, S, E, Lc, ok);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_status(e, "doa_fold_kernel launch");
+    const dim3 cells_grid(static_cast<unsigned>(F), static_cast<unsigned>(B));
+    doa_smooth_kernel<<<cells_grid, 64, 0, stream>>>(R, F, A, M, static_cast<int>(block_len), load, Lc, E);
+    BF_RETURN_IF(cuda_status(cudaGetLastError(), "doa_smooth_kernel launch"));
+    doa_forget_kernel<<<F, 64, 0, stream>>>(Lc, B, F, M, lam, S, E);
+    BF_RETURN_IF(cuda_status(cudaGetLastError(), "doa_forget_kernel launch"));
+    doa_factor_kernel<<<cells_grid, 64, 0, stream>>>(S, E, F, M, Lc, ok);
+    BF_RETURN_IF(cuda_status(cudaGetLastError(), "doa_factor_kernel launch"));
     BF_RETURN_IF(dispatch_scan<1>(M, stream, S, Lc, ok, pos, kw, B, F, l_first, l_step, static_cast<int>(n), m_fixed,
                                   bartlett, capon));
     doa_peak_kernel<<<B, 64, 0, stream>>>(bartlett, capon, static_cast<int>(n), l_first, l_step, l_est);
