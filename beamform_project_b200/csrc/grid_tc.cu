@@ -596,12 +596,18 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                     if (!failed && sq < jb.n_time) {
 #pragma unroll
                         for (int c = 0; c < kHalfLoads; c += 2) {
-                            uint32_t r0[32], r1[32];
+                            uint32_t r0[32];
                             if (c < c_count) tmem_ld_32x32b_x32(taddr + 32 * c, r0);
-                            if (c + 1 < c_count) tmem_ld_32x32b_x32(taddr + 32 * (c + 1), r1);
-                            tmem_ld_wait();
-                            if (c < c_count) short_windows(r0, c, jb, un, sq);
-                            if (c + 1 < c_count) short_windows(r1, c + 1, jb, un, sq);
+                            if constexpr (kHalfLoads > 1) {
+                                uint32_t r1[32];
+                                if (c + 1 < c_count) tmem_ld_32x32b_x32(taddr + 32 * (c + 1), r1);
+                                tmem_ld_wait();
+                                if (c < c_count) short_windows(r0, c, jb, un, sq);
+                                if (c + 1 < c_count) short_windows(r1, c + 1, jb, un, sq);
+                            } else {
+                                tmem_ld_wait();
+                                if (c < c_count) short_windows(r0, c, jb, un, sq);
+                            }
                         }
                     }
                 } else {
@@ -612,12 +618,18 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
 #pragma unroll
                         for (int c = 0; c < kHalfLoads; c += 2) {
                             // two loads in flight per wait
-                            uint32_t r0[32], r1[32];
+                            uint32_t r0[32];
                             if (c < c_count) tmem_ld_32x32b_x32(taddr + 32 * c, r0);
-                            if (c + 1 < c_count) tmem_ld_32x32b_x32(taddr + 32 * (c + 1), r1);
-                            tmem_ld_wait();
-                            if (c < c_count) acc[c] += beam_pair_sum(r0, lane);
-                            if (c + 1 < c_count) acc[c + 1] += beam_pair_sum(r1, lane);
+                            if constexpr (kHalfLoads > 1) {
+                                uint32_t r1[32];
+                                if (c + 1 < c_count) tmem_ld_32x32b_x32(taddr + 32 * (c + 1), r1);
+                                tmem_ld_wait();
+                                if (c < c_count) acc[c] += beam_pair_sum(r0, lane);
+                                if (c + 1 < c_count) acc[c + 1] += beam_pair_sum(r1, lane);
+                            } else {
+                                tmem_ld_wait();
+                                if (c < c_count) acc[c] += beam_pair_sum(r0, lane);
+                            }
                         }
                         cur_win = my_win;
                     }
