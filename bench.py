@@ -56,8 +56,8 @@ METRIC = "beam-samples/s (T*F*B)"
 # their commands are summarised under profiles/.
 NCU_TRAFFIC = {
     "grid": 2 * (1.472283e9 + 20.583936e6),
-    "tracker": 8 * (704.703488e6 + 3.553024e6),
-    "doa": 1.763518e9 + 172.711936e6,
+    "tracker": 8 * (704.703488e6 + 5.743616e6),
+    "doa": 1.409467e9 + 164.409344e6,
 }
 
 
