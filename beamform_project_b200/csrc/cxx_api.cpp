@@ -10,6 +10,7 @@
 // weights resident, voltage uploaded per call, CUDA-event timings per phase.
 #include "beamformer/cuda_beam_tracker_v5.hpp"
 #include "beamformer/cuda_beamformer.hpp"
+#include "beamformer/served.hpp"
 #include "bf_b200.h"
 
 #include <cuda_runtime.h>
@@ -44,6 +45,7 @@ void check(bf_status st) {
         case BF_ERR_OVERFLOW: throw std::overflow_error(msg);
         case BF_ERR_OUT_OF_RANGE: throw std::out_of_range(msg);
         case BF_ERR_UNSUPPORTED: throw std::invalid_argument(msg);
+        case BF_ERR_RESOURCE: throw std::length_error(msg);
         default: throw std::runtime_error(msg);
     }
 }
@@ -840,5 +842,126 @@ std::size_t BatchedTrackerStreamV5::batch_voltage_bytes() const { return voltage
 std::size_t BatchedTrackerStreamV5::batch_output_floats() const {
     return impl_->batch_dims.n_time * impl_->batch_dims.n_freq;
 }
+
+// ---------------------------------------------------------------------------
+// ServedBeamformer (bf_serve_*)
+// ---------------------------------------------------------------------------
+
+namespace {
+
+float generator_scale(float sigma) {
+    // the generator's draw 2 * (sum of eight uniform 16-bit integers) - 8 * 65535
+    // has variance 4 * 8 * (65536^2 - 1) / 12
+    const double sd = std::sqrt(4.0 * 8.0 * (65536.0 * 65536.0 - 1.0) / 12.0);
+    return static_cast<float>(static_cast<double>(sigma) / sd);
+}
+
+}  // namespace
+
+ServedBeamformer::ServedBeamformer(const ServedConfig& c) {
+    bf_serve_config cfg{};
+    cfg.hbm_budget_bytes = c.hbm_budget_bytes;
+    cfg.max_jobs = c.max_jobs;
+    cfg.window_spectra = c.window_spectra;
+    cfg.pool_spectra = c.pool_spectra;
+    cfg.shard_channels = c.shard_channels;
+    cfg.max_shards = c.max_shards;
+    cfg.pool_seed = c.pool_seed;
+    cfg.pool_scale = generator_scale(c.pool_sigma);
+    cfg.window_budget_us = c.window_budget_us;
+    check(bf_serve_create(&cfg, &server_));
+}
+
+ServedBeamformer::~ServedBeamformer() {
+    if (server_ != nullptr) bf_serve_destroy(server_);
+}
+
+std::uint64_t ServedBeamformer::submit(const ServedJob& job) {
+    if (job.positions.size() != job.n_ant) throw std::invalid_argument("position count must match n_ant");
+    bf_serve_job j{};
+    j.kind = job.kind == ServedJobKind::Grid ? BF_SERVE_GRID : BF_SERVE_TRACKER;
+    j.n_ant = static_cast<uint32_t>(job.n_ant);
+    j.n_shards = static_cast<uint32_t>(job.n_shards);
+    j.n_beams = static_cast<uint32_t>(job.n_beams);
+    j.n_spectra = job.n_spectra;
+    j.integration_spectra = job.integration_spectra;
+    j.pool_offset = job.pool_offset;
+    j.positions = job.positions.empty() ? nullptr : job.positions.front().data();
+    j.frequencies = job.frequencies_hz.empty() ? nullptr : job.frequencies_hz.data();
+    if (job.kind == ServedJobKind::Grid) {
+        if (job.directions.size() != job.n_beams) throw std::invalid_argument("beam direction count must match n_beams");
+        j.directions = job.directions.front().data();
+    } else {
+        if (job.trajectories.size() != job.n_beams) throw std::invalid_argument("trajectory count must match n_beams");
+        j.trajectories = job.trajectories.front().data();
+    }
+    j.quantize = job.quantize ? 1 : 0;
+    std::uint64_t id = 0;
+    check(bf_serve_submit(server_, &j, &id));
+    return id;
+}
+
+std::size_t ServedBeamformer::step() {
+    uint32_t n = 0;
+    check(bf_serve_step(server_, &n));
+    return n;
+}
+
+ServedJobState ServedBeamformer::state(std::uint64_t job_id) {
+    int32_t st = BF_JOB_UNKNOWN;
+    check(bf_serve_poll(server_, job_id, &st));
+    return static_cast<ServedJobState>(st);
+}
+
+std::vector<std::uint64_t> ServedBeamformer::take_done() {
+    std::vector<std::uint64_t> ids(256);
+    std::vector<std::uint64_t> out;
+    while (true) {
+        uint64_t n = 0;
+        check(bf_serve_take_done(server_, ids.data(), ids.size(), &n));
+        out.insert(out.end(), ids.begin(), ids.begin() + static_cast<std::ptrdiff_t>(n));
+        if (n < ids.size()) return out;
+    }
+}
+
+ServedResult ServedBeamformer::result(std::uint64_t job_id) {
+    float* integ = nullptr;
+    int8_t* codes = nullptr;
+    float* params = nullptr;
+    uint64_t w = 0;
+    check(bf_serve_result(server_, job_id, &integ, &codes, &params, &w));
+    return ServedResult{integ, codes, params, static_cast<std::size_t>(w)};
+}
+
+void ServedBeamformer::cancel(std::uint64_t job_id) { check(bf_serve_cancel(server_, job_id)); }
+void ServedBeamformer::release(std::uint64_t job_id) { check(bf_serve_release(server_, job_id)); }
+void ServedBeamformer::synchronize() { check(bf_serve_sync(server_)); }
+
+ServedStats ServedBeamformer::stats() {
+    bf_serve_stats st{};
+    check(bf_serve_stats_get(server_, &st));
+    ServedStats out;
+    out.steps = st.steps;
+    out.job_windows = st.job_windows;
+    out.jobs_done = st.jobs_done;
+    out.live_jobs = st.live_jobs;
+    out.queued_jobs = st.queued_jobs;
+    out.arena_bytes_peak = st.arena_bytes_peak;
+    out.graph_captures = st.graph_captures;
+    out.beam_samples = st.beam_samples;
+    out.window_ms_p50 = st.step_ms_p50;
+    out.window_ms_p99 = st.step_ms_p99;
+    return out;
+}
+
+std::vector<float> ServedBeamformer::window_times_ms() {
+    uint64_t n = 0;
+    check(bf_serve_step_times(server_, nullptr, 0, &n));
+    std::vector<float> out(n);
+    if (n > 0) check(bf_serve_step_times(server_, out.data(), n, &n));
+    return out;
+}
+
+void* ServedBeamformer::stream() { return bf_serve_stream(server_); }
 
 }  // namespace beamformer

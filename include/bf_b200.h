@@ -256,6 +256,13 @@ BF_API bf_status bf_generate_voltage(void* stream, uint64_t seed, uint64_t sampl
                                      float scale, const float* mu, uint64_t epoch_len,
                                      uint8_t* out, const bf_dims* dims);
 
+/* Failure-path probe (no reference counterpart): one kernel waits, with the
+ * same bounded mbarrier wait as the tensor-core kernels, on a barrier that
+ * nothing arrives on; after limit_ns (at most 2e9) it gives up and sets bit
+ * 30 of the device error word (read with bf_take_device_error).  Shows that
+ * a wait that runs out surfaces on the host and leaves the context usable. */
+BF_API bf_status bf_probe_bounded_wait(void* stream, uint64_t limit_ns);
+
 /* Device generate_weights (reference src/weights.cpp:11-60): canonical
  * complex64 weights for n_shards blocks of dims->n_freq channels, written as
  * [shard][B][F][A][2] float, from positions [A][3], frequencies

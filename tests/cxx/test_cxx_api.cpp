@@ -7,6 +7,7 @@
 #include "beamformer/cuda_beam_tracker_v5.hpp"
 #include "beamformer/cuda_beamformer.hpp"
 #include "beamformer/geometry.hpp"
+#include "beamformer/served.hpp"
 
 #include <cuda_runtime.h>
 
@@ -240,6 +241,64 @@ int main() {
         expect(out == I && s.last_kernel_time_ms() > 0.f, "batched stream equals one-shot tracker");
         s.process_batch(0, v.data(), out.data());
         expect(out == I, "graph replay repeats the result");
+    }
+
+    {
+        // served mode: one grid and one tracker job give the same bytes alone and in a mix
+        ServedConfig sc;
+        sc.hbm_budget_bytes = 2'000'000'000ULL;
+        sc.pool_spectra = 320 * 8;
+        std::vector<float> freq(2 * 336);
+        for (std::size_t f = 0; f < freq.size(); ++f) freq[f] = 400e6F + static_cast<float>(f) * (400e6F / 671.F);
+        std::vector<Vec3> pos(64);
+        for (std::size_t a = 0; a < 64; ++a) pos[a] = {static_cast<float>(a % 32) * 0.1875F, static_cast<float>(a / 32) * 0.1875F, 0.F};
+        ServedJob g;
+        g.kind = ServedJobKind::Grid;
+        g.n_ant = 64;
+        g.n_shards = 2;
+        g.n_beams = 8;
+        g.n_spectra = 640;
+        g.integration_spectra = 10;
+        g.pool_offset = 320;
+        g.positions = pos;
+        g.frequencies_hz = freq;
+        for (std::size_t b = 0; b < 8; ++b) g.directions.push_back(direction_from_lm(0.03F * static_cast<float>(b), 0.F));
+        ServedJob t = g;
+        t.kind = ServedJobKind::Tracker;
+        t.n_beams = 3;
+        t.integration_spectra = 320;
+        t.directions.clear();
+        t.trajectories = {{0.1F, 0.F, 1e-6F, 0.F}, {-0.1F, 0.05F, 0.F, 0.F}, {0.F, 0.F, 0.F, -1e-6F}};
+        auto run = [&](std::vector<ServedJob> jobs, std::size_t pick) {
+            ServedBeamformer srv(sc);
+            std::vector<std::uint64_t> ids;
+            for (const auto& j : jobs) ids.push_back(srv.submit(j));
+            while (srv.step() > 0) {
+            }
+            srv.synchronize();
+            const ServedResult r = srv.result(ids[pick]);
+            const ServedJob& j = jobs[pick];
+            const std::size_t n = j.kind == ServedJobKind::Grid ? j.n_shards * r.n_windows * 336 * j.n_beams
+                                                                : r.n_windows * j.n_shards * 336 * j.n_beams;
+            std::vector<float> host(n);
+            cudaMemcpy(host.data(), r.integrated, n * sizeof(float), cudaMemcpyDeviceToHost);
+            return host;
+        };
+        const auto ga = run({g}, 0);
+        const auto ta = run({t}, 0);
+        const auto gm = run({t, g, t}, 1);
+        const auto tm = run({g, t}, 1);
+        bool positive = !ga.empty();
+        for (float x : ga) positive &= std::isfinite(x) && x > 0.F;
+        expect(positive && ga.size() == 2 * 64 * 336 * 8, "served grid job produces finite powers");
+        expect(ga == gm && ta == tm, "served jobs are bit-identical alone and in a mix");
+        ServedBeamformer srv(sc);
+        ServedJob big = g;
+        big.n_spectra = 320 * 100000;
+        expect(throws<std::length_error>([&] { srv.submit(big); }), "oversize served job is a length_error");
+        ServedJob bad = g;
+        bad.n_spectra = 100;
+        expect(throws<std::invalid_argument>([&] { srv.submit(bad); }), "served job length must be whole windows");
     }
 
     std::printf("%s (%d failures)\n", failures == 0 ? "ALL OK" : "FAILED", failures);
