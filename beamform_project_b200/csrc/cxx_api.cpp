@@ -206,7 +206,7 @@ struct CudaBeamformerWorkspace::Impl {
     DeviceBuffer<std::uint8_t> voltage;
     DeviceBuffer<ComplexFloat> weights;     // canonical or tiled
     DeviceBuffer<std::uint8_t> split;       // TensorSplit operand
-    DeviceBuffer<float> intensity;          // per-spectrum output (not for TensorSplit)
+    DeviceBuffer<float> intensity;          // per-spectrum output
     DeviceBuffer<float> integrated;
     DeviceBuffer<std::int8_t> codes;
     DeviceBuffer<Int8QuantizationParameters> params;
@@ -225,8 +225,8 @@ struct CudaBeamformerWorkspace::Impl {
             split = DeviceBuffer<std::uint8_t>(split_weight_bytes(cap));
         } else {
             weights = DeviceBuffer<ComplexFloat>(weight_storage_count(cap, kernel));
-            intensity = DeviceBuffer<float>(cap.n_time * cap.n_freq * cap.n_beams);
         }
+        if (!temporal) intensity = DeviceBuffer<float>(cap.n_time * cap.n_freq * cap.n_beams);
         if (temporal) {
             integrated = DeviceBuffer<float>(integrated_intensity_count(cap, *temporal));
             if (output == CudaBeamformerOutput::QuantizedInt8) {
@@ -270,7 +270,9 @@ struct CudaBeamformerWorkspace::Impl {
     void launch(const Dimensions& dims, const std::uint8_t* v, const void* w, float* out) {
         const bf_dims d = to_c(dims);
         if (kernel == CudaBeamformerKernel::TensorSplit) {
-            check(bf_grid_tensor_integrated(stream, v, w, out, nullptr, nullptr, &d, temporal->integration_spectra, 1));
+            // per-spectrum output is integration over one spectrum ([T][F][B] == [W][F][B])
+            check(bf_grid_tensor_integrated(stream, v, w, out, nullptr, nullptr, &d,
+                                            temporal ? temporal->integration_spectra : 1, 1));
         } else if (temporal) {
             check(bf_launch_packed_integrated_beamformer(to_c(kernel), stream, v, static_cast<const float*>(w), out,
                                                          &d, temporal->integration_spectra));
@@ -292,9 +294,8 @@ CudaBeamformerWorkspace::CudaBeamformerWorkspace(const Dimensions& capacity, Cud
     if (output == CudaBeamformerOutput::QuantizedInt8 && !temporal_integration) {
         throw std::invalid_argument("int8 quantization requires a temporal-integration configuration");
     }
-    if (kernel == CudaBeamformerKernel::TensorSplit) {
-        if (!temporal_integration) throw std::invalid_argument("the TensorSplit kernel needs temporal integration");
-        if (capacity.n_ant > 64) throw std::invalid_argument("the TensorSplit kernel supports n_ant 32 or 64");
+    if (kernel == CudaBeamformerKernel::TensorSplit && capacity.n_ant > 64) {
+        throw std::invalid_argument("the TensorSplit kernel supports n_ant 32 or 64");
     }
     const auto t0 = std::chrono::steady_clock::now();
     impl_ = std::make_unique<Impl>(capacity, kernel, temporal_integration, output);
@@ -352,9 +353,6 @@ double CudaBeamformerWorkspace::run_kernel(const Dimensions& dims) {
         throw std::logic_error("packed voltage has not been uploaded for these dimensions");
     }
     m.require_weights(dims);
-    if (m.kernel == CudaBeamformerKernel::TensorSplit) {
-        throw std::logic_error("the TensorSplit workspace produces integrated output only");
-    }
     check_cuda(cudaEventRecord(m.start.e, m.stream), "cudaEventRecord");
     m.launch(Dimensions{dims}, m.voltage.ptr, m.weight_operand(), m.temporal ? m.integrated.ptr : m.intensity.ptr);
     check_cuda(cudaEventRecord(m.kernel_end.e, m.stream), "cudaEventRecord");
@@ -380,7 +378,7 @@ CudaBeamformerTimings CudaBeamformerWorkspace::run_pipeline(const PackedVoltage&
                                                             const Dimensions& dims) {
     auto& m = *impl_;
     m.validate_request(dims);
-    if (m.temporal || m.kernel == CudaBeamformerKernel::TensorSplit) {
+    if (m.temporal) {
         throw std::logic_error("run_pipeline needs a per-spectrum (non-integrating) workspace");
     }
     const std::size_t nv = voltage_sample_count(dims), no = dims.n_time * dims.n_freq * dims.n_beams;

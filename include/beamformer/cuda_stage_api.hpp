@@ -8,8 +8,8 @@
 // Kernel selector: Direct (canonical [B][F][A] weights) and Tiled (tiled
 // [F][ceil(B/32)][A][32] weights) reproduce the reference float32 operation
 // order bit for bit.  TensorSplit is the tcgen05 split-precision kernel; it
-// reads weights prepared by prepare_split_weights and writes integrated
-// output only.
+// reads weights prepared by prepare_split_weights; through this stage API it
+// writes integrated output (the workspace also gives per-spectrum output).
 #pragma once
 
 #include "beamformer/config.hpp"

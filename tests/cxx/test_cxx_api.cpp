@@ -172,6 +172,21 @@ int main() {
         expect(throws<std::invalid_argument>([&] { CudaBeamformerWorkspace x(di, CudaBeamformerKernel::TensorSplit, TemporalIntegrationConfig{40}); }),
                "TensorSplit rejects 40-spectrum integration");
         {
+            // per-spectrum output on the tensor path (workspace without integration)
+            CudaBeamformerWorkspace wps(di, CudaBeamformerKernel::TensorSplit);
+            wps.upload_weights(wi, di);
+            Intensities ps(di.n_time * di.n_freq * di.n_beams);
+            wps.run_pipeline(vi, ps, di);
+            bool okp = true;
+            for (std::size_t tt : {std::size_t{0}, std::size_t{333}, std::size_t{699}})
+                for (std::size_t f : {std::size_t{0}, std::size_t{111}, std::size_t{335}})
+                    for (std::size_t b = 0; b < 40; ++b) {
+                        const float r = cpu_power(vi, wi, di, tt, f, b);
+                        okp &= std::abs(ps[intensity_index(tt, f, b, di)] - r) <= 1e-3F + 1e-5F * std::abs(r);
+                    }
+            expect(okp, "TensorSplit per-spectrum output within tolerance");
+        }
+        {
             // 10-spectrum windows (integration_after_upchan) on the tensor path
             const auto integ10 = cuda_beamform_packed_integrated_intensity(vi, tile(wi, di), di, integration_after_upchan);
             CudaBeamformerWorkspace w10(di, CudaBeamformerKernel::TensorSplit, integration_after_upchan);
