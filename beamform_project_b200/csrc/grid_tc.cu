@@ -261,14 +261,14 @@ __device__ __forceinline__ void publish_ready(Pending& pd, volatile int* s_quant
 // 16-beam chunk).  The integrated values of the other CTAs were released by
 // their bumps and acquired by ours; they are read through L2.
 __device__ __forceinline__ void quantize_ready(const TcParams& p, volatile int* s_quant, volatile int* s_meta,
-                                               int et, int lane) {
+                                               int et, int lane, int epi_warps) {
     const TcJob& jb = p.job;
     const int shard = s_meta[0], fg = s_meta[1];
     for (int i = 0; i < 8; ++i) {
         const int w = s_quant[i];
         if (w < 0) continue;
         const size_t shard_off = static_cast<size_t>(shard) * jb.n_windows * jb.n_freq * jb.n_beams;
-        for (int bt = et >> 5; bt < p.btiles; bt += kEpilogueThreads / 32) {
+        for (int bt = et >> 5; bt < p.btiles; bt += epi_warps) {
             const size_t pidx = ((static_cast<size_t>(shard) * jb.n_windows + w) * p.ftiles + fg) * p.btiles + bt;
             quantize_chunk<true>(jb.integrated + shard_off, p.codes + shard_off, p.params, pidx, w, jb.n_freq,
                                  jb.n_beams, fg, bt, lane);
@@ -312,6 +312,16 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                                    : (2 * N <= 256) ? 256 : 512;
     constexpr uint32_t IDESC = idesc_f16_f32(kTileM, N);
     constexpr Smem S = smem_plan(A, NB);
+    // Warp roles: 0 producer, 1 MMA, then unpack warps, then epilogue warps
+    // (a multiple of four, so epilogue warp w reads TMEM lane quadrant w % 4).
+    // The narrowest beam set (one 32-column load per quadrant) has little
+    // epilogue work and is unpack-bound, so it trades four epilogue warps for
+    // unpack warps (measured: at 32 beams the epilogue would then bind).
+    constexpr int kUnpackWarps = NB <= 16 ? 6 : 2;
+    constexpr int kEpiWarps = kThreads / 32 - 2 - kUnpackWarps;   // 4 or 8
+    constexpr int kEpiThreads = 32 * kEpiWarps;
+    constexpr int kEpiFirstWarp = 2 + kUnpackWarps;
+    static_assert(kEpiWarps % 4 == 0 && kEpiFirstWarp % 4 == 0, "epilogue warps cover whole lane quadrants");
 
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -346,11 +356,11 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
     if (threadIdx.x == 0) {
         for (int i = 0; i < 2; ++i) {
             mbar_init(&raw_full[i], 1);
-            mbar_init(&raw_empty[i], 2);
-            mbar_init(&x_full[i], 2);
+            mbar_init(&raw_empty[i], kUnpackWarps);
+            mbar_init(&x_full[i], kUnpackWarps);
             mbar_init(&x_empty[i], 1);
             mbar_init(&acc_full[i], 1);
-            mbar_init(&acc_empty[i], kEpilogueThreads / 32);
+            mbar_init(&acc_empty[i], kEpiWarps);
         }
         mbar_init(w_full, 1);
         mbar_init(w_empty, 1);
@@ -484,9 +494,9 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
             tc_commit(mma_done);
             if (!mbar_wait(mma_done, 0, kWaitNs)) fail(1024);
         }
-    } else if (warp < 4) {
+    } else if (warp < kEpiFirstWarp) {
         // ------------------------------------------------------------ unpack
-        const int ut = threadIdx.x - 64;  // 0..63
+        const int ut = threadIdx.x - 64;  // 0 .. 32 * kUnpackWarps - 1
         int stage = 0, xs_stage = 0;
         uint32_t phase = 0, x_phase = 0;
         bool stop = false;
@@ -503,7 +513,7 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                 const uint8_t* rsrc = raw + stage * S.raw_bytes;
                 uint8_t* xdst = xs + xs_stage * S.x_bytes;
 #pragma unroll 4
-                for (int idx = ut; idx < kTileM * kChunks; idx += 64) {
+                for (int idx = ut; idx < kTileM * kChunks; idx += 32 * kUnpackWarps) {
                     const int r = idx / kChunks, q = idx % kChunks;
                     uint4 w4 = *reinterpret_cast<const uint4*>(rsrc + r * A + q * 16);
                     if ((r & 31) >= R) w4 = make_uint4(0u, 0u, 0u, 0u);  // spare quadrant rows
@@ -528,18 +538,19 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
         }
     } else {
         // ------------------------------------------------------------ epilogue
-        // Eight warps: warp w reads TMEM lane quadrant w % 4 (32 tile rows)
-        // and one half of the accumulator columns (beams).
+        // Warp w reads TMEM lane quadrant w % 4 (32 tile rows) and, with eight
+        // epilogue warps, one half of the accumulator columns (beams).
         const int q4 = warp & 3;
-        const int half = (warp - 4) >> 2;                 // 0 or 1
-        const int et = threadIdx.x - 128;                 // 0..255
+        constexpr int kHalves = kEpiWarps / 4;
+        const int half = (warp - kEpiFirstWarp) >> 2;     // 0 .. kHalves - 1
+        const int et = threadIdx.x - 32 * kEpiFirstWarp;  // 0 .. kEpiThreads - 1
         int acc_stage = 0;
         uint32_t acc_phase = 0;
         constexpr int kLoads = N / 32;                    // 16 beams per 32-column load
-        constexpr int kHalfLoads = (kLoads + 1) / 2;
+        constexpr int kHalfLoads = (kLoads + kHalves - 1) / kHalves;
         const int c_begin = half * kHalfLoads;
         const int c_count = min(kHalfLoads, kLoads - c_begin);
-        float* stg = slots + (warp - 4) * 512;            // short windows: [16 beams][32 rows]
+        float* stg = slots + (warp - kEpiFirstWarp) * 512;  // short windows: [16 beams][32 rows]
         float acc[kHalfLoads];
 #pragma unroll
         for (int c = 0; c < kHalfLoads; ++c) acc[c] = 0.f;
@@ -567,16 +578,31 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                 stg[j * 32 + (lane ^ j)] = re * re + im * im;
             }
             __syncwarp();
-            const int sw = jb.spectra, nwin = jb.rows_q / sw;
-            for (int idx = lane; idx < nwin * 16; idx += 32) {
-                const int j = idx & 15, s = idx >> 4;
-                const int w = sq / sw + s;
-                const int b = 16 * (c_begin + c) + j;
-                if (w * sw < jb.n_time && b < jb.n_beams) {
-                    float sum = 0.f;
-                    for (int i = 0; i < sw; ++i) sum += stg[j * 32 + ((s * sw + i) ^ j)];
-                    jb.integrated[((static_cast<size_t>(un.shard) * jb.n_windows + jb.w0 + w) * jb.n_freq + un.f) *
-                                      jb.n_beams + b] = sum;
+            // each lane sums two (window, beam) pairs at a time, p and p + 32,
+            // in increasing row order; the loads of both run ahead of the adds
+            const int sw = jb.spectra, npairs = (jb.rows_q / sw) * 16;
+            for (int pb = 0; pb < npairs; pb += 64) {
+                const int p0 = pb + lane, p1 = pb + 32 + lane;
+                const bool v0 = p0 < npairs, v1 = p1 < npairs;
+                const int j0 = p0 & 15, s0 = p0 >> 4, j1 = p1 & 15, s1 = p1 >> 4;
+                const float* row0 = stg + j0 * 32;
+                const float* row1 = stg + j1 * 32;
+                float sum0 = 0.f, sum1 = 0.f;
+#pragma unroll 4
+                for (int i = 0; i < sw; ++i) {
+                    const float x0 = v0 ? row0[(s0 * sw + i) ^ j0] : 0.f;
+                    const float x1 = v1 ? row1[(s1 * sw + i) ^ j1] : 0.f;
+                    sum0 += x0;
+                    sum1 += x1;
+                }
+                const int w0 = sq / sw + s0, w1 = sq / sw + s1;
+                const int b0 = 16 * (c_begin + c) + j0, b1 = 16 * (c_begin + c) + j1;
+                const size_t row_base = static_cast<size_t>(un.shard) * jb.n_windows + jb.w0;
+                if (v0 && w0 * sw < jb.n_time && b0 < jb.n_beams) {
+                    jb.integrated[((row_base + w0) * jb.n_freq + un.f) * jb.n_beams + b0] = sum0;
+                }
+                if (v1 && w1 * sw < jb.n_time && b1 < jb.n_beams) {
+                    jb.integrated[((row_base + w1) * jb.n_freq + un.f) * jb.n_beams + b1] = sum1;
                 }
             }
             __syncwarp();
@@ -641,24 +667,34 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
 
                 const int tile_end_row = min((k + 1) * kTileM, jb.n_time);
                 const int first_row = k * kTileM;
+                const bool fused = !kServed && p.codes != nullptr;
                 if (!short_win) {
                     if (cur_win >= 0 && min((cur_win + 1) * jb.spectra, jb.n_time) <= tile_end_row) {
                         flush(cur_win);
                         cur_win = -1;
                     }
-                    named_barrier(1, kEpilogueThreads);
+                    // Does a window end in this tile (the same for every warp)?  Only
+                    // then (or with fused quantization) do the slots need a barrier.
+                    bool ends = false;
+                    if (first_row < jb.n_time) {
+                        const int w_last_row = tile_end_row - 1;
+                        const int wl = w_last_row / jb.spectra;
+                        ends = min((wl + 1) * jb.spectra, jb.n_time) - 1 == w_last_row ||
+                               (wl > 0 && wl * jb.spectra - 1 >= first_row);
+                    }
+                    if (ends || fused) named_barrier(1, kEpiThreads);
                     // quantize the groups this CTA completed one tile ago (list published
                     // by epilogue thread 0 before the barrier)
-                    if (!kServed && p.codes != nullptr) quantize_ready(p, s_quant, s_meta, et, lane);
+                    if (fused) quantize_ready(p, s_quant, s_meta, et, lane, kEpiWarps);
                     // finalize every window whose last spectrum lies in this tile
-                    if (first_row < jb.n_time) {
+                    if (ends) {
                         const int w_first = first_row / jb.spectra;
                         const int w_last_in = (tile_end_row - 1) / jb.spectra;
                         for (int w = w_first; w <= w_last_in; ++w) {
                             const int w_last = min((w + 1) * jb.spectra, jb.n_time) - 1;
                             if (w_last < first_row || w_last >= tile_end_row) continue;
                             float* s = slots + (w % kRing) * 4 * NB;
-                            for (int b = et; b < NB; b += kEpilogueThreads) {
+                            for (int b = et; b < NB; b += kEpiThreads) {
                                 const float total = ((s[b] + s[NB + b]) + s[2 * NB + b]) + s[3 * NB + b];
                                 s[b] = s[NB + b] = s[2 * NB + b] = s[3 * NB + b] = 0.f;
                                 if (b < jb.n_beams) {
@@ -669,9 +705,16 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                         }
                     }
                 }
-                // one decision for all epilogue warps: stop together or go on together
-                if (named_barrier_or(1, kEpilogueThreads, failed || *s_fail != 0)) { stop = true; break; }
-                if (!kServed && !short_win && p.codes != nullptr && et == 0) {
+                // one decision for all epilogue warps, at the end of each unit (and
+                // every tile with fused quantization): stop together or go on
+                // together; a failed wait only makes the remaining tiles of the
+                // unit skip their work
+                if ((k + 1 == un.tile_end || fused) &&
+                    named_barrier_or(1, kEpiThreads, failed || *s_fail != 0)) {
+                    stop = true;
+                    break;
+                }
+                if (fused && !short_win && et == 0) {
                     // Fused int8 quantization.  A 1x16x16 chunk spans 16 channels that
                     // other CTAs own: each finished (window, channel) bumps its
                     // 16-channel group's counter, and the CTA whose bump completes the
@@ -690,17 +733,17 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
         if (!kServed && p.codes != nullptr && !stop) {
             // drain the three stages: published list, bumps in flight, recorded windows
             for (int round = 0; round < 3; ++round) {
-                named_barrier(1, kEpilogueThreads);
-                quantize_ready(p, s_quant, s_meta, et, lane);
-                named_barrier(1, kEpilogueThreads);
+                named_barrier(1, kEpiThreads);
+                quantize_ready(p, s_quant, s_meta, et, lane, kEpiWarps);
+                named_barrier(1, kEpiThreads);
                 if (et == 0) {
                     publish_ready(pend, s_quant, s_meta);
                     issue_arrivals(p, recorded, pend);
                     recorded.mask = 0;
                 }
             }
-            named_barrier(1, kEpilogueThreads);
-            quantize_ready(p, s_quant, s_meta, et, lane);
+            named_barrier(1, kEpiThreads);
+            quantize_ready(p, s_quant, s_meta, et, lane, kEpiWarps);
         }
     }
 
