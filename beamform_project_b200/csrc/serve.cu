@@ -40,6 +40,7 @@ namespace {
 constexpr uint64_t kAlign = 256;
 constexpr int kEventRing = 256;
 constexpr int kMirrors = 4;
+constexpr int kBranches = 6;
 constexpr double kTwoPi = 6.283185307179586476925286766559;
 constexpr double kSpeedOfLight = 299792458.0;
 
@@ -176,6 +177,8 @@ struct bf_server {
     std::vector<Captured> captured;
     cudaGraphExec_t exec = nullptr;
     uint64_t captures = 0;
+    cudaStream_t side[kBranches] = {};       // graph branches (capture only)
+    cudaEvent_t fork_ev = nullptr, join_ev[kBranches] = {};
 
     // step timing
     cudaEvent_t ev_start[kEventRing] = {}, ev_end[kEventRing] = {};
@@ -531,24 +534,55 @@ bf_status capture_graph(bf_server* s, const std::vector<std::pair<ClassKey, uint
             BF_RETURN_IF(launch_grid_tensor_served(s->stream, *m, c.key.n_ant, c.key.nb_pad, nullptr, 0));
         }
     }
+    // Classes run on parallel branches of the graph (a fork from the server's
+    // stream onto side streams, joined back before the quantizer and at the
+    // end), so one class's CTAs fill the SMs another class's tail leaves idle.
+    // Classes never share an SM (each grid CTA holds a whole register file,
+    // a tracker CTA half of one), so TMEM allocation never waits.
     cudaGraph_t graph = nullptr;
     BF_RETURN_IF(cuda_status(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal), "begin capture"));
-    bf_status st = BF_OK;
+    bf_status st = cuda_status(cudaEventRecord(s->fork_ev, s->stream), "fork the window graph");
+    int branch = 0;
+    bool used[kBranches] = {};
+    auto side = [&]() {
+        const int b = branch++ % kBranches;
+        if (!used[b]) {
+            used[b] = true;
+            if (st == BF_OK) st = cuda_status(cudaStreamWaitEvent(s->side[b], s->fork_ev, 0), "branch wait");
+        }
+        return b;
+    };
+    auto join = [&]() {
+        for (int b = 0; b < kBranches && st == BF_OK; ++b) {
+            if (!used[b]) continue;
+            st = cuda_status(cudaEventRecord(s->join_ev[b], s->side[b]), "branch done");
+            if (st == BF_OK) st = cuda_status(cudaStreamWaitEvent(s->stream, s->join_ev[b], 0), "join the branches");
+            used[b] = false;
+        }
+    };
+    // grid and tracker classes on branches; the quantizer after the grid classes
     for (const auto& c : cap) {
+        if (st != BF_OK) break;
+        if (c.key.kind == kQuantClass) continue;
         const TableHeader* t = reinterpret_cast<const TableHeader*>(s->d_tables + c.offset);
+        const int b = side();
+        if (st != BF_OK) break;
         if (c.key.kind == kGridClass) {
             CUtensorMap* m = nullptr;
             st = encode_pool_map(s, c.key.n_ant, c.key.rows_q, &m);
-            if (st == BF_OK) st = launch_grid_tensor_served(s->stream, *m, c.key.n_ant, c.key.nb_pad, t, s->sms);
-        } else if (c.key.kind == kQuantClass) {
-            st = launch_served_quantize(s->stream, t, s->sms * 8);
+            if (st == BF_OK) st = launch_grid_tensor_served(s->side[b], *m, c.key.n_ant, c.key.nb_pad, t, s->sms);
         } else {
             const int A = c.key.n_ant;
-            st = launch_served_tracker(s->stream, A, s->pool[A == 64 ? 1 : 0],
+            st = launch_served_tracker(s->side[b], A, s->pool[A == 64 ? 1 : 0],
                                        static_cast<uint64_t>(s->cfg.shard_channels) * s->cfg.max_shards, t,
                                        s->sms * 2);
         }
-        if (st != BF_OK) break;
+    }
+    join();
+    for (const auto& c : cap) {
+        if (st != BF_OK || c.key.kind != kQuantClass) continue;
+        st = launch_served_quantize(s->stream, reinterpret_cast<const TableHeader*>(s->d_tables + c.offset),
+                                    s->sms * 8);
     }
     const cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
     if (st != BF_OK) {
@@ -660,6 +694,11 @@ void destroy(bf_server* s) {
         cudaFree(s->pool[0]);
         cudaFree(s->pool[1]);
         cudaFree(s->w_scratch);
+        for (int b = 0; b < kBranches; ++b) {
+            if (s->join_ev[b]) cudaEventDestroy(s->join_ev[b]);
+            if (s->side[b]) cudaStreamDestroy(s->side[b]);
+        }
+        if (s->fork_ev) cudaEventDestroy(s->fork_ev);
         if (s->stream) cudaStreamDestroy(s->stream);
     }
     delete s;
@@ -696,6 +735,11 @@ bf_status create(const bf_serve_config* cfg, bool host_only, bf_server** out) {
         return BF_OK;
     }
     BF_RETURN_IF(cuda_status(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking), "create stream"));
+    for (int b = 0; b < kBranches; ++b) {
+        BF_RETURN_IF(cuda_status(cudaStreamCreateWithFlags(&s->side[b], cudaStreamNonBlocking), "create stream"));
+        BF_RETURN_IF(cuda_status(cudaEventCreateWithFlags(&s->join_ev[b], cudaEventDisableTiming), "create event"));
+    }
+    BF_RETURN_IF(cuda_status(cudaEventCreateWithFlags(&s->fork_ev, cudaEventDisableTiming), "create event"));
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, dev);
