@@ -69,6 +69,7 @@ struct TcParams {
     float2* params;             // [shard][W][ftiles][btiles]
     unsigned* counters;         // [shard][W][ftiles] arrival counts, zero at launch
     int ftiles, btiles;
+    int paired;                 // plain launch: CTA pairs share channel pairs (see JobCursor)
     long long n_units;
 };
 
@@ -185,12 +186,32 @@ struct JobCursor {
             next_begin = LLONG_MAX;
         }
     }
+    // Paired order (plain launches with an even channel count): CTAs 2m and
+    // 2m + 1 walk the same (channel pair, group) sequence, taking the even and
+    // the odd channel of each pair, so the two 64-byte halves of every
+    // 128-byte voltage line are read at about the same time and DRAM fetches
+    // each line once.  u then counts (shard, channel pair, group).
+    int pair_parity = -1;
+
     __device__ __forceinline__ Unit at(long long u) {
         if constexpr (kServed) {
             while (u >= next_begin) {
                 ++j;
                 jb = jobs[j];
                 next_begin = j + 1 < n_jobs ? jobs[j + 1].unit_begin : LLONG_MAX;
+            }
+        } else {
+            if (pair_parity >= 0) {
+                Unit r;
+                const int half_f = jb.n_freq / 2;
+                const long long pi = u / jb.groups_per_channel;
+                const int g = static_cast<int>(u % jb.groups_per_channel);
+                r.shard = static_cast<int>(pi / half_f);
+                r.f = 2 * static_cast<int>(pi % half_f) + pair_parity;
+                r.tile_begin = g * jb.group_tiles;
+                r.tile_end = min(r.tile_begin + jb.group_tiles, jb.tiles_per_channel);
+                r.key = r.shard * jb.n_freq + r.f;
+                return r;
             }
         }
         return unit_of(jb, j, u);
@@ -377,8 +398,16 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
 
     long long n_units = p.n_units;
     if constexpr (kServed) n_units = p.table->n_units;
-    const long long u_begin = n_units * blockIdx.x / gridDim.x;
-    const long long u_end = n_units * (blockIdx.x + 1) / gridDim.x;
+    long long u_begin = n_units * blockIdx.x / gridDim.x;
+    long long u_end = n_units * (blockIdx.x + 1) / gridDim.x;
+    int pair_parity = -1;
+    if (!kServed && p.paired) {  // host guarantees an even channel count and grid
+        const long long pair_units = n_units / 2;
+        const int slots = static_cast<int>(gridDim.x / 2), m = static_cast<int>(blockIdx.x / 2);
+        u_begin = pair_units * m / slots;
+        u_end = pair_units * (m + 1) / slots;
+        pair_parity = static_cast<int>(blockIdx.x & 1);
+    }
     // A failed (timed-out) wait records its code, raises the CTA-wide flag and
     // makes every role stop at its next check; nothing waits unboundedly.
     auto fail = [&](unsigned code) {
@@ -398,6 +427,7 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
             bool stop = false;
             JobCursor<kServed> cur;
             if (u_begin < u_end) cur.init(p, u_begin);
+            cur.pair_parity = pair_parity;
             for (long long u = u_begin; u < u_end && !stop; ++u) {
                 const Unit un = cur.at(u);
                 const TcJob& jb = cur.jb;
@@ -455,6 +485,7 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
             const uint32_t w_hi_addr = smem_u32(w_hi), w_lo_addr = smem_u32(w_lo);
             JobCursor<kServed> cur;
             if (u_begin < u_end) cur.init(p, u_begin);
+            cur.pair_parity = pair_parity;
             for (long long u = u_begin; u < u_end && !stop; ++u) {
                 const Unit un = cur.at(u);
                 if (un.key != prev_key) {
@@ -503,6 +534,7 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
         constexpr int kChunks = A / 16;  // 16-byte raw chunks per spectrum
         JobCursor<kServed> cur;
         if (u_begin < u_end) cur.init(p, u_begin);
+        cur.pair_parity = pair_parity;
         for (long long u = u_begin; u < u_end && !stop; ++u) {
             const Unit un = cur.at(u);
             const int R = cur.jb.rows_q;
@@ -609,6 +641,7 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
         };
         JobCursor<kServed> cur;
         if (u_begin < u_end) cur.init(p, u_begin);
+        cur.pair_parity = pair_parity;
         for (long long u = u_begin; u < u_end && !stop; ++u) {
             const Unit un = cur.at(u);
             const TcJob& jb = cur.jb;
@@ -969,6 +1002,7 @@ bf_status launch_grid_tensor(cudaStream_t stream, const uint8_t* v, const void* 
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int grid = static_cast<int>(std::min<long long>(sms, p.n_units));
+    p.paired = (d.n_freq % 2 == 0 && grid % 2 == 0 && grid >= 2) ? 1 : 0;
     if (grid > 0) {
         const int nbp = padded_beams(d.n_beams);
         st = d.n_ant == 32 ? dispatch_nb<32>(stream, map, p, nbp, grid) : dispatch_nb<64>(stream, map, p, nbp, grid);

@@ -55,7 +55,7 @@ METRIC = "beam-samples/s (T*F*B)"
 # both are scaled to a full launch by the units processed.  The captures and
 # their commands are summarised under profiles/.
 NCU_TRAFFIC = {
-    "grid": 2 * (1.472283e9 + 20.583936e6),
+    "grid": 2 * (767.70e6 + 18.97e6),
     "tracker": 8 * (704.703488e6 + 5.743616e6),
     "doa": 1.409467e9 + 164.409344e6,
 }
