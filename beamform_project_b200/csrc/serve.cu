@@ -971,6 +971,7 @@ static bf_status bf_serve_release_impl(bf_server* s, uint64_t job_id) {
         s->arena.release(j.off, j.lay.total);
     }
     s->live.erase(std::remove(s->live.begin(), s->live.end(), job_id), s->live.end());
+    s->completions.erase(std::remove(s->completions.begin(), s->completions.end(), job_id), s->completions.end());
     s->jobs.erase(it);
     return BF_OK;
 }

@@ -196,3 +196,14 @@ def test_window_time_bound_limits_admission():
         assert s.stats()["predicted_ms_last"] > 0.010
         s.step()
         assert s.step() == 1 and s.poll(b) == serve.LIVE and s.poll(a) in (serve.DONE, serve.RUNNING)
+
+
+def test_released_jobs_leave_the_completion_queue():
+    with serve.Server(10**10, host_only=True) as s:
+        a = s.submit(_grid(n_spectra=320))
+        b = s.submit(_grid(n_spectra=320))
+        s.step()
+        assert s.poll(a) == serve.DONE and s.poll(b) == serve.DONE
+        s.release(a)                    # released before it was taken
+        assert s.take_done() == [b]
+        assert s.take_done() == []
