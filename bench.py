@@ -374,6 +374,38 @@ def run_gpu(args):
     prof = integ.view(N_SHARDS, W, F_SHARD, N_BEAMS).double().sum(dim=(0, 1, 2))
     peak_ok = int(torch.argmax(prof).item()) == beam
 
+    # the plain drop-in beside it: the reference-order float32 kernel (Direct,
+    # bit-identical to the reference CPU core) and the quantizer, same inputs
+    plain = None
+    if kernel == "tensor" and args.plain_steps > 0:
+        integ_p = torch.empty_like(integ)
+        codes_p = torch.empty_like(codes)
+        params_p = torch.empty_like(params)
+
+        def plain_step():
+            for s in range(N_SHARDS):
+                api.launch_packed_integrated_beamformer(api.CudaBeamformerKernel.Direct, None,
+                                                        volt[s * shard_bytes:], weights[s], integ_p[s * n_out:],
+                                                        d, S_INT)
+            api.launch_quantize_integrated_intensity(None, integ_p, codes_p, params_p, qd_all)
+        plain_step()
+        torch.cuda.synchronize()
+        p0 = torch.cuda.Event(enable_timing=True)
+        p1 = torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        for _ in range(args.plain_steps):
+            plain_step()
+        p1.record(stream)
+        torch.cuda.synchronize()
+        plain_ms = p0.elapsed_time(p1) / args.plain_steps
+        ref = integ_p.double()
+        rel = ((integ.double() - ref).abs() / ref.abs().clamp_min(1e-30)).max().item()
+        lsb = (codes.int() - codes_p.int()).abs()
+        plain = {"kernel": "grid_exact_kernel (Direct, reference float32 order) + quantize_kernel",
+                 "ms_per_step": plain_ms, "value": samples_per_step / (plain_ms / 1e3),
+                 "tensor_speedup": plain_ms / ms_per_step, "max_rel_diff_vs_tensor": rel,
+                 "int8_codes_differing": int((lsb > 0).sum().item()), "int8_max_lsb": int(lsb.max().item())}
+
     peak_tflops, hbm_gbs, peak_src = measured_peaks()
     cmac = T_SPECTRA * N_SHARDS * F_SHARD * N_ANT * N_BEAMS
     alg_flops = 8 * cmac + 3 * samples_per_step
@@ -404,6 +436,7 @@ def run_gpu(args):
         "gpu_launches": launches,
         "clocks": clocks.summary(),
         "source_peak_ok": peak_ok,
+        "plain_dropin": plain,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v0 = volt[:shard_bytes].cpu().numpy().reshape(T_SPECTRA, F_SHARD, N_ANT)
@@ -517,6 +550,34 @@ def run_tracker(args):
     torch.cuda.synchronize()
     ps_ms = s0.elapsed_time(s1) / 5
 
+    # the plain drop-in beside it: the reference-order tracker (mode 0, float32
+    # order of the reference CPU tracker), same inputs, same outputs
+    plain = None
+    if mode == api.TrackerMode.Streaming and args.plain_steps > 0:
+        integ_p = torch.empty_like(integ)
+        inten_p = torch.empty_like(inten)
+
+        def plain_step():
+            api.tracker(None, api.TrackerMode.ReferenceOrder, volt, pos_d, k_d, dirs_d, inten_p, integ_p, d, TR_S)
+        plain_step()
+        torch.cuda.synchronize()
+        q0 = torch.cuda.Event(enable_timing=True)
+        q1 = torch.cuda.Event(enable_timing=True)
+        q0.record(stream)
+        for _ in range(args.plain_steps):
+            plain_step()
+        q1.record(stream)
+        torch.cuda.synchronize()
+        plain_ms = q0.elapsed_time(q1) / args.plain_steps
+        step(True)
+        torch.cuda.synchronize()
+        ref = inten_p.double()
+        rel = ((inten.double() - ref).abs() / (1e-3 + ref.abs())).max().item()
+        plain = {"kernel": "tracker_exact_kernel (reference float32 order), per-spectrum + integrated",
+                 "ms_per_step": plain_ms, "value": TR_T * F_SHARD / (plain_ms / 1e3),
+                 "streaming_speedup_per_spectrum_output": plain_ms / ps_ms,
+                 "max_diff_vs_streaming_over_1e-3_plus_abs": rel}
+
     # end to end: pinned host voltage in, integrated powers out
     host_v = torch.empty(volt.numel(), dtype=torch.uint8, pin_memory=True)
     host_v.copy_(volt)
@@ -553,6 +614,7 @@ def run_tracker(args):
                      "traffic": round(NCU_TRAFFIC["tracker"]) if mode == 1 and TR_T == 262144 else None,
                      "peak_source": peak_src + " (copy bandwidth)", "kernel_ms": round(kern_ms, 4),
                      "algorithmic_bytes_per_launch": alg_bytes},
+        "plain_dropin": plain,
         "per_spectrum_output": {"ms_per_step": ps_ms, "value": samples / (ps_ms / 1e3),
                                 "bytes_per_launch": in_bytes + TR_T * F_SHARD * 4,
                                 "achieved_gbs": (in_bytes + TR_T * F_SHARD * 4) / (ps_ms / 1e3) / 1e9},
@@ -1113,6 +1175,8 @@ def main():
                     help="quantize inside the tensor kernel's epilogue (measured slower than the separate kernel)")
     ap.add_argument("--t-spectra", type=int, default=TR_T, help="tracker workload length (profiling)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--plain-steps", type=int, default=2,
+                    help="steps of the plain drop-in (reference-order) kernel timed beside the tensor path")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serve-seconds", type=float, default=2.0,
                     help="seconds of Poisson arrivals (the full stream is 10)")
