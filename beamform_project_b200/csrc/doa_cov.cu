@@ -22,8 +22,8 @@
 // the pair's 2A contiguous bytes (a whole 128-byte line at 64 antennas; a
 // single channel's 64 bytes would make DRAM fetch the neighbour twice).
 // Warp 0 TMA producer (raw 128-spectrum tiles of both channels), warp 1 MMA
-// issuer and TMEM owner, warps 2-7 unpack (int4 -> int8, 128-byte swizzle,
-// one tile per channel), warps 8-11 epilogue (two 128 x 128 int32
+// issuer and TMEM owner, warps 2-11 unpack (int4 -> int8, 128-byte swizzle,
+// one tile per channel), warps 12-15 epilogue (two 128 x 128 int32
 // accumulators per unit, two TMEM stages of 256 columns).  All waits are
 // bounded and report through the device error word.
 #include "bf_internal.cuh"
@@ -40,8 +40,8 @@ namespace {
 
 using namespace sm100;
 
-constexpr int kThreads = 384;
-constexpr int kUnpackWarps = 6;
+constexpr int kThreads = 512;
+constexpr int kUnpackWarps = 10;
 constexpr int kTile = 128;        // spectra per tile
 constexpr int kRawStages = 6;
 constexpr int kXStages = 3;
