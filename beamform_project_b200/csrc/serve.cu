@@ -244,10 +244,10 @@ bf_status validate_job(const bf_serve_config& c, const bf_serve_job* j) {
     if (j->n_spectra == 0 || j->n_spectra % win != 0) {
         return set_error(BF_ERR_INVALID_ARGUMENT, "n_spectra must be a positive multiple of window_spectra");
     }
-    if (j->n_spectra / S > 0x7fffffffull) return set_error(BF_ERR_OVERFLOW, "too many windows in one job");
     if (S == 0 || win % S != 0) {
         return set_error(BF_ERR_INVALID_ARGUMENT, "integration_spectra must divide window_spectra");
     }
+    if (j->n_spectra / S > 0x7fffffffull) return set_error(BF_ERR_OVERFLOW, "too many windows in one job");
     if (j->kind == BF_SERVE_GRID && S > 32 && S % 32 != 0) {
         return set_error(BF_ERR_UNSUPPORTED, "grid jobs need integration_spectra below 32 or a multiple of 32");
     }
@@ -704,10 +704,7 @@ void destroy(bf_server* s) {
     delete s;
 }
 
-bf_status create(const bf_serve_config* cfg, bool host_only, bf_server** out) {
-    if (out == nullptr || cfg == nullptr) return set_error(BF_ERR_INVALID_ARGUMENT, "config and server must not be null");
-    *out = nullptr;
-    const bf_serve_config& c = *cfg;
+bf_status validate_config(const bf_serve_config& c) {
     if (c.window_spectra == 0 || c.window_spectra % 32 != 0 || c.window_spectra > (1u << 20)) {
         return set_error(BF_ERR_INVALID_ARGUMENT, "window_spectra must be a positive multiple of 32");
     }
@@ -720,6 +717,14 @@ bf_status create(const bf_serve_config* cfg, bool host_only, bf_server** out) {
     if (c.max_jobs == 0 || c.max_jobs > 65536) return set_error(BF_ERR_INVALID_ARGUMENT, "max_jobs must be 1..65536");
     if (c.hbm_budget_bytes == 0) return set_error(BF_ERR_INVALID_ARGUMENT, "hbm_budget_bytes must be positive");
     if (!(c.window_budget_us >= 0.f)) return set_error(BF_ERR_INVALID_ARGUMENT, "window_budget_us must be >= 0");
+    return BF_OK;
+}
+
+bf_status create(const bf_serve_config* cfg, bool host_only, bf_server** out) {
+    if (out == nullptr || cfg == nullptr) return set_error(BF_ERR_INVALID_ARGUMENT, "config and server must not be null");
+    *out = nullptr;
+    const bf_serve_config& c = *cfg;
+    BF_RETURN_IF(validate_config(c));
     std::unique_ptr<bf_server, void (*)(bf_server*)> s(new bf_server(), destroy);
     s->cfg = c;
     s->host_only = host_only;
@@ -773,7 +778,10 @@ bf_status create(const bf_serve_config* cfg, bool host_only, bf_server** out) {
 extern "C" {
 
 BF_API uint64_t bf_serve_job_bytes(const bf_serve_config* config, const bf_serve_job* job) {
-    if (config == nullptr || job == nullptr || validate_job(*config, job) != BF_OK) return 0;
+    if (config == nullptr || job == nullptr || validate_config(*config) != BF_OK ||
+        validate_job(*config, job) != BF_OK) {
+        return 0;
+    }
     return layout_of(*config, *job).total;
 }
 

@@ -5,6 +5,8 @@ scheduler-only server runs the same bookkeeping as the device server with
 every step completing when it is issued."""
 from __future__ import annotations
 
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -207,3 +209,14 @@ def test_released_jobs_leave_the_completion_queue():
         s.release(a)                    # released before it was taken
         assert s.take_done() == [b]
         assert s.take_done() == []
+
+
+def test_zero_lengths_are_rejected_not_divided_by():
+    with serve.Server(10**9, host_only=True) as s:
+        with pytest.raises(native.InvalidArgument, match="divide window_spectra"):
+            s.submit(_grid(S=0))
+        cfg = native.ServeConfig()          # all zero: an invalid configuration
+        job = _grid().to_c()
+        assert native.lib().bf_serve_job_bytes(C.byref(cfg), C.byref(job)) == 0
+    with pytest.raises(native.InvalidArgument):
+        serve.Server(10**9, window_spectra=0, host_only=True)
