@@ -400,6 +400,8 @@ void update_done(bf_server* s) {
 // spectra (a unit is three tiles plus its weight load: x 3), x 1.8 per tile
 // for short windows (their epilogue).  Tracker units: 0.015 + S * (0.00016 +
 // 0.00004 * tiles) + 2.1e-5 per (source, antenna) weight.
+// Resident CTAs per SM of the short-window tracker (registers allow four).
+constexpr int kShortTrackerCtasPerSm = 4;
 constexpr double kStepUs = 12.0;
 constexpr double kClassUs = 8.0;
 
@@ -573,9 +575,10 @@ bf_status capture_graph(bf_server* s, const std::vector<std::pair<ClassKey, uint
             if (st == BF_OK) st = launch_grid_tensor_served(s->side[b], *m, c.key.n_ant, c.key.nb_pad, t, s->sms);
         } else {
             const int A = c.key.n_ant;
-            st = launch_served_tracker(s->side[b], A, s->pool[A == 64 ? 1 : 0],
+            const bool short_windows = c.key.short_win != 0;
+            st = launch_served_tracker(s->side[b], A, short_windows, s->pool[A == 64 ? 1 : 0],
                                        static_cast<uint64_t>(s->cfg.shard_channels) * s->cfg.max_shards, t,
-                                       s->sms * 2);
+                                       s->sms * (short_windows ? kShortTrackerCtasPerSm : 2));
         }
     }
     join();
@@ -847,7 +850,7 @@ static bf_status bf_serve_submit_impl(bf_server* s, const bf_serve_job* job, uin
         j.traj.assign(job->trajectories, job->trajectories + 4 * job->n_beams);
         j.kw.resize(F);
         for (uint64_t f = 0; f < F; ++f) j.kw[f] = kTwoPi * static_cast<double>(j.freq[f]) / kSpeedOfLight;
-        j.cls = ClassKey{kTrackerClass, static_cast<int>(job->n_ant), 0, 0, 0};
+        j.cls = ClassKey{kTrackerClass, static_cast<int>(job->n_ant), 0, 0, job->integration_spectra <= 16 ? 1 : 0};
     }
     j.spec.positions = j.spec.frequencies = j.spec.directions = j.spec.trajectories = nullptr;
     j.n_steps = job->n_spectra / s->cfg.window_spectra;

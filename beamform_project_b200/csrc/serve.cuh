@@ -52,9 +52,10 @@ bf_status launch_generate_weights(cudaStream_t stream, const float* pos, const f
                                   uint64_t n_ant);
 
 // One persistent launch (grid CTAs of 256 threads) over a tracker table;
-// voltage rows come from `pool` ([rows][pool_freq][A] bytes).
-bf_status launch_served_tracker(cudaStream_t stream, int n_ant, const uint8_t* pool, uint64_t pool_freq,
-                                const TableHeader* table, int grid);
+// voltage rows come from `pool` ([rows][pool_freq][A] bytes).  A table with
+// short_windows set holds only jobs of at most 16 spectra per window.
+bf_status launch_served_tracker(cudaStream_t stream, int n_ant, bool short_windows, const uint8_t* pool,
+                                uint64_t pool_freq, const TableHeader* table, int grid);
 
 // One persistent launch (grid CTAs of 256 threads, a warp per chunk).
 bf_status launch_served_quantize(cudaStream_t stream, const TableHeader* table, int grid);

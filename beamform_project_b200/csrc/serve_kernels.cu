@@ -65,25 +65,56 @@ __device__ __forceinline__ int find_job(const long long* begins, int stride_ll, 
 // the same decoded voltage.  A unit is (job, window, 8 channels, 8 sources);
 // warp w of the CTA owns channel 8 * group + w.  The unit's steering
 // weights are computed once each: the CTA forms the FP64 delays of its 8
-// sources (shared by the 8 channels), each warp the weights of its channel
-// into shared memory, and every lane then gathers its fragment entries.
+// sources (shared by the 8 channels), each warp the weights of its channel,
+// split at once into the four fp16 parts (re hi, im hi, re lo, im lo) that
+// the fragments hold.  A part row keeps antennas a and a + 2 in one 32-bit
+// word, so each fragment register is one shared-memory load (the im part of
+// a real-row column is the negated word).  Rows are XOR-swizzled so that the
+// 32 lanes of a fragment load hit 32 banks.
+// kShort (windows of at most 16 spectra: one row block) reads the fragments
+// where the MMAs use them instead of holding all four tiles in registers,
+// which leaves room for twice the resident CTAs.
 // For one source the arithmetic (weights, fragments, MMA chain, hi + lo
 // combination, window sum order) is that of tracker_stream_kernel, so
-// results agree bit for bit.
+// results agree bit for bit (split(-x) is -split(x) except for the sign of a
+// zero part, and the powers are sums of squares).
 template <int A>
-__global__ void __launch_bounds__(256)
+struct TrackerFrag {
+    static constexpr int kWords = A / 2;  // 32-bit words per part row
+    // word of part row r holding antennas (a, a + 2), a % 4 in {0, 1}
+    __device__ static int word(int r, int a) {
+        const int pw = ((a >> 2) << 1) | (a & 1);
+        const int swz = A == 64 ? (r & 7) : ((r >> 1) & 3);
+        return r * kWords + (pw ^ swz);
+    }
+    __device__ static int half(int a) { return (a >> 1) & 1; }
+};
+
+template <int A, bool kShort>
+__global__ void __launch_bounds__(256, kShort ? 4 : 2)
 served_tracker_kernel(const uint8_t* __restrict__ pool, long long row_stride, const TableHeader* table) {
     constexpr int NW = A / 16;          // 32-bit words per thread per spectrum
     constexpr int kBytes = A / 4;       // bytes (antennas) per thread per spectrum
-    constexpr int kRow = A + 8;         // padded weight row: conflict-free gathers
+    using Frag = TrackerFrag<A>;
+    constexpr int kWarpWords = 8 * 4 * Frag::kWords;  // 8 sources x 4 parts
     __shared__ double s_delay[8][A];
-    __shared__ float2 s_w[8][8 * kRow + 4];
+    __shared__ uint32_t s_frag[8][kWarpWords];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, q = lane & 3;
     const TrJob* jobs = reinterpret_cast<const TrJob*>(table + 1);
     const long long n_units = table->n_units;
     const int n_jobs = table->n_jobs;
-    auto w_at = [&](int src, int a) -> float2& { return s_w[warp][src * kRow + a + a / kBytes]; };
+    uint32_t* frag = s_frag[warp];
+    // fragment column g: part (g & 3) of source 2 nt + (g >> 2); the xi word
+    // takes the other component, negated for the real columns
+    const int part_r = g & 3, part_i = (g & 3) ^ 1;
+    const uint32_t neg_i = (g & 1) != 0 ? 0u : 0x80008000u;
+    auto frag_pair = [&](int nt, int jj, int s, bool used, uint32_t& xr, uint32_t& xi) {
+        const int sl = 2 * nt + (g >> 2);
+        const int a0 = q * kBytes + 4 * jj + s;
+        xr = used ? frag[Frag::word(sl * 4 + part_r, a0)] : 0u;
+        xi = used ? frag[Frag::word(sl * 4 + part_i, a0)] ^ neg_i : 0u;
+    };
     for (long long u = blockIdx.x; u < n_units; u += gridDim.x) {
         const int j = find_job(&jobs[0].unit_begin, sizeof(TrJob) / sizeof(long long), n_jobs, u);
         const TrJob& jb = jobs[j];
@@ -99,7 +130,7 @@ served_tracker_kernel(const uint8_t* __restrict__ pool, long long row_stride, co
         const int n_tiles = (n_here + 1) / 2;
         const long long wglob = static_cast<long long>(jb.w0) + w;
 
-        __syncthreads();  // the previous unit is done with s_delay
+        __syncthreads();  // the previous unit is done with s_delay and s_frag
         for (int i = threadIdx.x; i < n_here * A; i += blockDim.x) {
             const int sl = i / A, a = i % A;
             const float3 d = trajectory_direction(jb.traj + 4 * (8 * sg + sl), wglob * S);
@@ -108,39 +139,30 @@ served_tracker_kernel(const uint8_t* __restrict__ pool, long long row_stride, co
         __syncthreads();
         if (fvalid) {
             const double k = jb.kw[f];
+            uint16_t* frag16 = reinterpret_cast<uint16_t*>(frag);
             for (int i = lane; i < n_here * A; i += 32) {
                 const int sl = i / A, a = i % A;
-                w_at(sl, a) = steering_from_delay(k, s_delay[sl][a]);
+                const float2 wv = steering_from_delay(k, s_delay[sl][a]);
+                const int h = Frag::half(a);
+                frag16[2 * Frag::word(sl * 4 + 0, a) + h] = split_part(wv.x, false);
+                frag16[2 * Frag::word(sl * 4 + 1, a) + h] = split_part(wv.y, false);
+                frag16[2 * Frag::word(sl * 4 + 2, a) + h] = split_part(wv.x, true);
+                frag16[2 * Frag::word(sl * 4 + 3, a) + h] = split_part(wv.y, true);
             }
         }
         __syncwarp();
 
-        // B fragments: column g of tile nt is (re, im) x (hi, lo) of source
-        // 8 sg + 2 nt + (g >> 2).
-        uint32_t bfrag[4][NW][2][2];
-        {
-            const bool is_im = (g & 1) != 0, is_lo = ((g >> 1) & 1) != 0;
+        // B fragments of the long form: column g of tile nt is (re, im) x
+        // (hi, lo) of source 8 sg + 2 nt + (g >> 2).
+        uint32_t bfrag[kShort ? 1 : 4][NW][2][2];
+        if constexpr (!kShort) {
 #pragma unroll
             for (int nt = 0; nt < 4; ++nt) {
-                const int sl = 2 * nt + (g >> 2);
-                const bool used = fvalid && nt < n_tiles && sl < n_here;
+                const bool used = fvalid && nt < n_tiles && 2 * nt + (g >> 2) < n_here;
 #pragma unroll
                 for (int jj = 0; jj < NW; ++jj) {
 #pragma unroll
-                    for (int s = 0; s < 2; ++s) {
-                        const int a0 = q * kBytes + 4 * jj + s, a1 = a0 + 2;
-                        uint32_t xr = 0, xi = 0;
-                        if (used) {
-                            const float2 w0 = w_at(sl, a0);
-                            const float2 w1 = w_at(sl, a1);
-                            const float cr0 = is_im ? w0.y : w0.x, cr1 = is_im ? w1.y : w1.x;
-                            const float ci0 = is_im ? w0.x : -w0.y, ci1 = is_im ? w1.x : -w1.y;
-                            xr = split_part(cr0, is_lo) | (static_cast<uint32_t>(split_part(cr1, is_lo)) << 16);
-                            xi = split_part(ci0, is_lo) | (static_cast<uint32_t>(split_part(ci1, is_lo)) << 16);
-                        }
-                        bfrag[nt][jj][s][0] = xr;
-                        bfrag[nt][jj][s][1] = xi;
-                    }
+                    for (int s = 0; s < 2; ++s) frag_pair(nt, jj, s, used, bfrag[nt][jj][s][0], bfrag[nt][jj][s][1]);
                 }
             }
         }
@@ -171,7 +193,7 @@ served_tracker_kernel(const uint8_t* __restrict__ pool, long long row_stride, co
         load_rows(t_begin, wg, wg8);
         for (int tb = t_begin; tb < t_end; tb += 16) {
             uint32_t ng[NW], ng8[NW];
-            load_rows(tb + 16, ng, ng8);
+            if constexpr (!kShort) load_rows(tb + 16, ng, ng8);
             float d[4][4];
 #pragma unroll
             for (int nt = 0; nt < 4; ++nt) d[nt][0] = d[nt][1] = d[nt][2] = d[nt][3] = 0.f;
@@ -183,8 +205,17 @@ served_tracker_kernel(const uint8_t* __restrict__ pool, long long row_stride, co
 #pragma unroll
                 for (int nt = 0; nt < 4; ++nt) {
                     if (nt < n_tiles) {
-                        mma_16816(d[nt], re02g, re02h, im02g, im02h, bfrag[nt][jj][0][0], bfrag[nt][jj][0][1]);
-                        mma_16816(d[nt], re13g, re13h, im13g, im13h, bfrag[nt][jj][1][0], bfrag[nt][jj][1][1]);
+                        if constexpr (kShort) {
+                            const bool used = fvalid && 2 * nt + (g >> 2) < n_here;
+                            uint32_t b0r, b0i, b1r, b1i;
+                            frag_pair(nt, jj, 0, used, b0r, b0i);
+                            frag_pair(nt, jj, 1, used, b1r, b1i);
+                            mma_16816(d[nt], re02g, re02h, im02g, im02h, b0r, b0i);
+                            mma_16816(d[nt], re13g, re13h, im13g, im13h, b1r, b1i);
+                        } else {
+                            mma_16816(d[nt], re02g, re02h, im02g, im02h, bfrag[nt][jj][0][0], bfrag[nt][jj][0][1]);
+                            mma_16816(d[nt], re13g, re13h, im13g, im13h, bfrag[nt][jj][1][0], bfrag[nt][jj][1][1]);
+                        }
                     }
                 }
             }
@@ -203,10 +234,12 @@ served_tracker_kernel(const uint8_t* __restrict__ pool, long long row_stride, co
                     pw[nt] += pow_g + pow_h;
                 }
             }
+            if constexpr (!kShort) {
 #pragma unroll
-            for (int jj = 0; jj < NW; ++jj) {
-                wg[jj] = ng[jj];
-                wg8[jj] = ng8[jj];
+                for (int jj = 0; jj < NW; ++jj) {
+                    wg[jj] = ng[jj];
+                    wg8[jj] = ng8[jj];
+                }
             }
         }
 #pragma unroll
@@ -265,13 +298,16 @@ bf_status launch_generate_weights(cudaStream_t stream, const float* pos, const f
     return cuda_status(cudaGetLastError(), "weights_kernel launch");
 }
 
-bf_status launch_served_tracker(cudaStream_t stream, int n_ant, const uint8_t* pool, uint64_t pool_freq,
-                                const TableHeader* table, int grid) {
+bf_status launch_served_tracker(cudaStream_t stream, int n_ant, bool short_windows, const uint8_t* pool,
+                                uint64_t pool_freq, const TableHeader* table, int grid) {
     const long long row_stride = static_cast<long long>(pool_freq) * n_ant;
-    switch (n_ant) {
-        case 32: served_tracker_kernel<32><<<grid, 256, 0, stream>>>(pool, row_stride, table); break;
-        case 64: served_tracker_kernel<64><<<grid, 256, 0, stream>>>(pool, row_stride, table); break;
-        default: return set_error(BF_ERR_UNSUPPORTED, "served trackers support n_ant 32 or 64");
+    if (n_ant != 32 && n_ant != 64) return set_error(BF_ERR_UNSUPPORTED, "served trackers support n_ant 32 or 64");
+    if (n_ant == 32) {
+        if (short_windows) served_tracker_kernel<32, true><<<grid, 256, 0, stream>>>(pool, row_stride, table);
+        else served_tracker_kernel<32, false><<<grid, 256, 0, stream>>>(pool, row_stride, table);
+    } else {
+        if (short_windows) served_tracker_kernel<64, true><<<grid, 256, 0, stream>>>(pool, row_stride, table);
+        else served_tracker_kernel<64, false><<<grid, 256, 0, stream>>>(pool, row_stride, table);
     }
     return cuda_status(cudaGetLastError(), "served_tracker_kernel launch");
 }

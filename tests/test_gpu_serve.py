@@ -119,10 +119,13 @@ def test_served_grid_matches_plain_and_oracle(cuda, orc, S):
         assert np.array_equal(codes[s], qc)
 
 
-@pytest.mark.parametrize("S,n_src", [(320, 3), (10, 9)])
-def test_served_tracker_equals_plain_tracker(cuda, S, n_src):
+@pytest.mark.parametrize("A,S,n_src", [(64, 320, 3), (64, 10, 9), (64, 16, 5), (32, 10, 16), (32, 20, 8),
+                                       (32, 320, 1)])
+def test_served_tracker_equals_plain_tracker(cuda, A, S, n_src):
+    """Both tracker forms (windows of at most 16 spectra, and longer) give
+    the plain tracker's results bit for bit."""
     torch = cuda
-    job = _tracker_job(S=S, n_src=n_src)
+    job = _tracker_job(A=A, S=S, n_src=n_src)
     with _server() as srv:
         (integ, _, _), = _run(srv, [job])
     A, ns, T = job.n_ant, job.n_shards, job.n_spectra
