@@ -130,45 +130,7 @@ served_tracker_kernel(const uint8_t* __restrict__ pool, long long row_stride, co
         const int n_tiles = (n_here + 1) / 2;
         const long long wglob = static_cast<long long>(jb.w0) + w;
 
-        __syncthreads();  // the previous unit is done with s_delay and s_frag
-        for (int i = threadIdx.x; i < n_here * A; i += blockDim.x) {
-            const int sl = i / A, a = i % A;
-            const float3 d = trajectory_direction(jb.traj + 4 * (8 * sg + sl), wglob * S);
-            s_delay[sl][a] = steering_delay(jb.pos, a, d.x, d.y, d.z);
-        }
-        __syncthreads();
-        if (fvalid) {
-            const double k = jb.kw[f];
-            uint16_t* frag16 = reinterpret_cast<uint16_t*>(frag);
-            for (int i = lane; i < n_here * A; i += 32) {
-                const int sl = i / A, a = i % A;
-                const float2 wv = steering_from_delay(k, s_delay[sl][a]);
-                const int h = Frag::half(a);
-                frag16[2 * Frag::word(sl * 4 + 0, a) + h] = split_part(wv.x, false);
-                frag16[2 * Frag::word(sl * 4 + 1, a) + h] = split_part(wv.y, false);
-                frag16[2 * Frag::word(sl * 4 + 2, a) + h] = split_part(wv.x, true);
-                frag16[2 * Frag::word(sl * 4 + 3, a) + h] = split_part(wv.y, true);
-            }
-        }
-        __syncwarp();
-
-        // B fragments of the long form: column g of tile nt is (re, im) x
-        // (hi, lo) of source 8 sg + 2 nt + (g >> 2).
-        uint32_t bfrag[kShort ? 1 : 4][NW][2][2];
-        if constexpr (!kShort) {
-#pragma unroll
-            for (int nt = 0; nt < 4; ++nt) {
-                const bool used = fvalid && nt < n_tiles && 2 * nt + (g >> 2) < n_here;
-#pragma unroll
-                for (int jj = 0; jj < NW; ++jj) {
-#pragma unroll
-                    for (int s = 0; s < 2; ++s) frag_pair(nt, jj, s, used, bfrag[nt][jj][s][0], bfrag[nt][jj][s][1]);
-                }
-            }
-        }
-
         const int t_begin = w * S, t_end = t_begin + S;  // rows of this launch
-        float pw[4] = {0.f, 0.f, 0.f, 0.f};
         const uint8_t* base = pool + static_cast<size_t>(f) * A + q * kBytes;
         auto load_rows = [&](int tb, uint32_t (&wg)[NW], uint32_t (&wg8)[NW]) {
             const int tg = tb + g, tg8 = tb + g + 8;
@@ -189,8 +151,59 @@ served_tracker_kernel(const uint8_t* __restrict__ pool, long long row_stride, co
                 }
             }
         };
+        // the window's first rows are in flight while the weights are formed
         uint32_t wg[NW], wg8[NW];
         load_rows(t_begin, wg, wg8);
+
+        __syncthreads();  // the previous unit is done with s_delay and s_frag
+        for (int i = threadIdx.x; i < n_here * A; i += blockDim.x) {
+            const int sl = i / A, a = i % A;
+            const float3 d = trajectory_direction(jb.traj + 4 * (8 * sg + sl), wglob * S);
+            s_delay[sl][a] = steering_delay(jb.pos, a, d.x, d.y, d.z);
+        }
+        __syncthreads();
+        if (fvalid) {
+            // lane owns antennas lane + 32 c; sources go in pairs so that
+            // every part row's swizzle is a compile-time constant
+            const double k = jb.kw[f];
+#pragma unroll 1
+            for (int sl0 = 0; sl0 < n_here; sl0 += 2) {
+                uint16_t* rows = reinterpret_cast<uint16_t*>(frag + sl0 * 4 * Frag::kWords);
+#pragma unroll
+                for (int e = 0; e < 2; ++e) {
+                    if (sl0 + e < n_here) {
+#pragma unroll
+                        for (int c = 0; c < A / 32; ++c) {
+                            const int a = lane + 32 * c;
+                            const float2 wv = steering_from_delay(k, s_delay[sl0 + e][a]);
+                            const int h = Frag::half(a);
+                            rows[2 * Frag::word(e * 4 + 0, a) + h] = split_part(wv.x, false);
+                            rows[2 * Frag::word(e * 4 + 1, a) + h] = split_part(wv.y, false);
+                            rows[2 * Frag::word(e * 4 + 2, a) + h] = split_part(wv.x, true);
+                            rows[2 * Frag::word(e * 4 + 3, a) + h] = split_part(wv.y, true);
+                        }
+                    }
+                }
+            }
+        }
+        __syncwarp();
+
+        // B fragments of the long form: column g of tile nt is (re, im) x
+        // (hi, lo) of source 8 sg + 2 nt + (g >> 2).
+        uint32_t bfrag[kShort ? 1 : 4][NW][2][2];
+        if constexpr (!kShort) {
+#pragma unroll
+            for (int nt = 0; nt < 4; ++nt) {
+                const bool used = fvalid && nt < n_tiles && 2 * nt + (g >> 2) < n_here;
+#pragma unroll
+                for (int jj = 0; jj < NW; ++jj) {
+#pragma unroll
+                    for (int s = 0; s < 2; ++s) frag_pair(nt, jj, s, used, bfrag[nt][jj][s][0], bfrag[nt][jj][s][1]);
+                }
+            }
+        }
+
+        float pw[4] = {0.f, 0.f, 0.f, 0.f};
         for (int tb = t_begin; tb < t_end; tb += 16) {
             uint32_t ng[NW], ng8[NW];
             if constexpr (!kShort) load_rows(tb + 16, ng, ng8);
