@@ -9,23 +9,30 @@
 // forward-backward averaging, 1/K, diagonal loading and forgetting are linear
 // and run afterwards in FP64 (doa_scan.cu).
 //
-// Formulation: with y(t) the 2A real components (re, im interleaved) of x(t),
-// the Gram matrix G = sum_t y(t) y(t)^T is one tcgen05 kind::i8 GEMM per
-// (block, channel): M = N = 128 components (zero padded for 32 antennas),
-// K = time.  The unpacked tile [t][128 int8] is MN-major for both operands,
-// so one shared-memory tile feeds A and B.  R assembles from G in the
-// epilogue: Re R_ij = G_{2i,2j} + G_{2i+1,2j+1}, Im R_ij = G_{2i+1,2j} -
-// G_{2i,2j+1}.  |x| <= 8 per component, so every sum stays below 2^31 for
-// blocks of up to 2^24 spectra.
+// Formulation: with y(t) the 2A real components of x(t), the Gram matrix
+// G = sum_t y(t) y(t)^T is one tcgen05 kind::i8 GEMM per (block, channel):
+// M = N = 128 components (zero padded for 32 antennas), K = time.  The
+// unpacked tile [t][128 bytes] is MN-major for both operands, so one
+// shared-memory tile feeds A and B.  The tile holds the components in offset
+// binary, u = y + 8 in 0..15 (one lop3 per four nibbles), and the MMA runs
+// u8 x u8; the epilogue restores
+//   G_ij = Gu_ij - 8 (S_i + S_j) + 64 K,   S_i = sum_t u_i(t),
+// with S gathered by the unpack warps from the same bytes.  A 16-byte chunk
+// of the tile holds 8 antennas as [re 0-3][im 0-3][re 4-7][im 4-7], so
+// component m = 16 c + 4 h + k is antenna 8 c + 4 (h >> 1) + k, part h & 1.
+// R assembles from G in the epilogue: Re R_ij = G(re i, re j) + G(im i, im j),
+// Im R_ij = G(im i, re j) - G(re i, im j).  u <= 15, so Gu stays below 2^31
+// for blocks of up to 2^23 spectra.
 //
 // CTA (one per SM): a unit is (block, channel pair), so every TMA box row is
 // the pair's 2A contiguous bytes (a whole 128-byte line at 64 antennas; a
 // single channel's 64 bytes would make DRAM fetch the neighbour twice).
 // Warp 0 TMA producer (raw 128-spectrum tiles of both channels), warp 1 MMA
-// issuer and TMEM owner, warps 2-11 unpack (int4 -> int8, 128-byte swizzle,
-// one tile per channel), warps 12-15 epilogue (two 128 x 128 int32
-// accumulators per unit, two TMEM stages of 256 columns).  All waits are
-// bounded and report through the device error word.
+// issuer and TMEM owner, warps 2-19 unpack (int4 -> offset-binary bytes,
+// 128-byte swizzle, one tile per channel: nine warps per channel), warps
+// 20-23 epilogue (two 128 x 128 int32 accumulators per unit, two TMEM stages
+// of 256 columns).  All waits are bounded and report through the device
+// error word.
 #include "bf_internal.cuh"
 #include "sm100.cuh"
 
@@ -40,8 +47,12 @@ namespace {
 
 using namespace sm100;
 
-constexpr int kThreads = 512;
-constexpr int kUnpackWarps = 10;
+constexpr int kThreads = 768;
+constexpr int kUnpackWarps = 18;                 // nine per channel of the pair
+constexpr int kEpiFirstWarp = 2 + kUnpackWarps;
+constexpr int kPerChannel = 32 * kUnpackWarps / 2;  // unpack threads per channel
+constexpr int kRowStep = kPerChannel / 8;        // rows between a thread's chunks
+constexpr int kWarpsPerChannel = kUnpackWarps / 2;
 constexpr int kTile = 128;        // spectra per tile
 constexpr int kRawStages = 6;
 constexpr int kXStages = 3;
@@ -59,38 +70,30 @@ __device__ __forceinline__ void cov_error(unsigned* err, unsigned code) {
     if (err != nullptr) atomicOr(err, code << 16);
 }
 
-// 8 packed bytes (antennas 8c..8c+7) -> 16 int8 components (re, im interleaved).
-// A nibble n becomes the signed byte ((n ^ 8) + 0x78) ^ 0x80: n ^ 8 is in
-// 0..15, + 0x78 stays below 0x100 (no carry into the next byte), and the
-// final xor maps 0x78 + (n ^ 8) onto n - 16 * (n >= 8).
-__device__ __forceinline__ uint4 expand8(uint32_t w0, uint32_t w1) {
-    auto two = [](uint32_t w, uint32_t& a, uint32_t& b) {
-        uint32_t lo, hi, x, y;
-        asm("lop3.b32 %0, %1, %2, %3, 0x6A;" : "=r"(lo) : "r"(w), "r"(0x0F0F0F0Fu), "r"(0x08080808u));
-        asm("lop3.b32 %0, %1, %2, %3, 0x6A;" : "=r"(hi) : "r"(w >> 4), "r"(0x0F0F0F0Fu), "r"(0x08080808u));
-        lo = (lo + 0x78787878u) ^ 0x80808080u;
-        hi = (hi + 0x78787878u) ^ 0x80808080u;
-        asm("prmt.b32 %0, %1, %2, 0x5140;" : "=r"(x) : "r"(lo), "r"(hi));
-        asm("prmt.b32 %0, %1, %2, 0x7362;" : "=r"(y) : "r"(lo), "r"(hi));
-        a = x;
-        b = y;
-    };
-    uint4 r;
-    two(w0, r.x, r.y);
-    two(w1, r.z, r.w);
+// 8 packed bytes (antennas 8c..8c+7) -> 16 offset-binary components
+// [re 0-3][im 0-3][re 4-7][im 4-7]: a two's-complement nibble n becomes
+// u = n ^ 8 = n + 8 (mod 16), one lop3 ((w & 0x0F..) ^ 0x08..) per word.
+__device__ __forceinline__ uint32_t offset4(uint32_t w) {
+    uint32_t r;
+    asm("lop3.b32 %0, %1, %2, %3, 0x6A;" : "=r"(r) : "r"(w), "r"(0x0F0F0F0Fu), "r"(0x08080808u));
     return r;
+}
+__device__ __forceinline__ uint4 offset8(uint32_t w0, uint32_t w1) {
+    return make_uint4(offset4(w0), offset4(w0 >> 4), offset4(w1), offset4(w1 >> 4));
 }
 
 template <int A>
 __global__ void __launch_bounds__(kThreads, 1)
 doa_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovParams p) {
     constexpr uint32_t RAW = kTile * 2 * A;              // [row][2 channels][A]
-    constexpr uint32_t IDESC = idesc_s8_s32_mn(128, 128);
+    constexpr uint32_t IDESC = idesc_u8_s32_mn(128, 128);
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* xs = smem;                                  // kXStages x 2 x 16 KiB
     uint8_t* raw = smem + kXStages * kXBytes;            // kRawStages x RAW
-    uint64_t* bars = reinterpret_cast<uint64_t*>(raw + kRawStages * RAW);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(raw + kRawStages * RAW);  // 512 bytes
+    uint32_t* s_part = reinterpret_cast<uint32_t*>(raw + kRawStages * RAW + 512);  // [2][kUnpackWarps][128]
+    uint32_t* s_sum = s_part + 2 * kUnpackWarps * 128;                             // [2][2][128]
     uint64_t* raw_full = bars;                           // [kRawStages]
     uint64_t* raw_empty = bars + kRawStages;             // [kRawStages]
     uint64_t* x_full = bars + 2 * kRawStages;            // [kXStages]
@@ -98,8 +101,11 @@ doa_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovParams p) {
     uint64_t* acc_full = x_empty + kXStages;             // [2]
     uint64_t* acc_empty = acc_full + 2;                  // [2]
     uint64_t* mma_done = acc_empty + 2;
-    uint32_t* tmem_ptr = reinterpret_cast<uint32_t*>(mma_done + 1);
-    volatile int* s_fail = reinterpret_cast<volatile int*>(mma_done + 2);
+    uint64_t* part_full = mma_done + 1;                  // [2] unpack warps -> epilogue
+    uint64_t* part_empty = part_full + 2;                // [2] epilogue -> unpack warps
+    uint64_t* sum_ready = part_empty + 2;                // [2] among the epilogue warps
+    uint32_t* tmem_ptr = reinterpret_cast<uint32_t*>(sum_ready + 2);
+    volatile int* s_fail = reinterpret_cast<volatile int*>(sum_ready + 3);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
@@ -116,6 +122,11 @@ doa_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovParams p) {
             mbar_init(&acc_empty[i], 4);
         }
         mbar_init(mma_done, 1);
+        for (int i = 0; i < 2; ++i) {
+            mbar_init(&part_full[i], kUnpackWarps);
+            mbar_init(&part_empty[i], 4);
+            mbar_init(&sum_ready[i], 4);
+        }
         *s_fail = 0;
         fence_mbar_init();
     }
@@ -186,27 +197,60 @@ doa_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovParams p) {
             tc_commit(mma_done);
             if (!mbar_wait(mma_done, 0, kWaitNs)) fail(16);
         }
-    } else if (warp < 2 + kUnpackWarps) {
-        const int ut = threadIdx.x - 64;  // 0 .. 32 * kUnpackWarps - 1
-        int stage = 0, xst = 0;
-        uint32_t phase = 0, xph = 0;
+    } else if (warp < kEpiFirstWarp) {
+        // thread = (channel, chunk c of 8 antennas, first row r0); rows r0,
+        // r0 + kRowStep, ... of every tile.  Component sums: bytes[] adds the
+        // offset words (at most 4 rows x 15 per byte per tile, flushed every
+        // 4 tiles), wide[] the even / odd bytes in 16-bit lanes (flushed to
+        // total[] every 512 tiles), total[] the unit's sums.
+        const int ut = threadIdx.x - 64;
+        const int ch = ut / kPerChannel, local = ut % kPerChannel;
+        const int c = local & 7, r0 = local >> 3;
+        const bool live = c < A / 8;
+        int stage = 0, xst = 0, pst = 0;
+        uint32_t phase = 0, xph = 0, pph = 0;
         bool stop = false;
-        constexpr int kChunks = A / 8;   // 8-antenna chunks per spectrum
         for (long long u = u_begin; u < u_end && !stop; ++u) {
+            uint32_t bytes[4] = {0, 0, 0, 0}, wide[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            uint32_t total[16];
+#pragma unroll
+            for (int i = 0; i < 16; ++i) total[i] = 0;
+            auto flush_bytes = [&]() {
+#pragma unroll
+                for (int h = 0; h < 4; ++h) {
+                    wide[h] += bytes[h] & 0x00FF00FFu;
+                    wide[4 + h] += (bytes[h] >> 8) & 0x00FF00FFu;
+                    bytes[h] = 0;
+                }
+            };
+            auto flush_wide = [&]() {
+#pragma unroll
+                for (int h = 0; h < 4; ++h) {
+                    total[4 * h + 0] += wide[h] & 0xFFFFu;
+                    total[4 * h + 2] += wide[h] >> 16;
+                    total[4 * h + 1] += wide[4 + h] & 0xFFFFu;
+                    total[4 * h + 3] += wide[4 + h] >> 16;
+                    wide[h] = wide[4 + h] = 0;
+                }
+            };
             for (int k = 0; k < p.tiles_per_block; ++k) {
                 if (*s_fail) { stop = true; break; }
                 if (!mbar_wait(&raw_full[stage], phase, kWaitNs)) { fail(32); stop = true; break; }
                 if (!mbar_wait(&x_empty[xst], xph ^ 1, kWaitNs)) { fail(64); stop = true; break; }
-                const uint8_t* rsrc = raw + stage * RAW;
-                uint8_t* xdst = xs + xst * kXBytes;
-                for (int idx = ut; idx < 2 * kTile * 8; idx += 32 * kUnpackWarps) {
-                    const int ch = idx >> 10, r = (idx >> 3) & (kTile - 1), c = idx & 7;  // channel, spectrum, chunk
+                const uint8_t* rsrc = raw + stage * RAW + ch * A + c * 8;
+                uint8_t* xdst = xs + xst * kXBytes + ch * (kTile * 128);
+#pragma unroll 4
+                for (int r = r0; r < kTile; r += kRowStep) {
                     uint4 v = make_uint4(0, 0, 0, 0);
-                    if (c < kChunks) {
-                        const uint2 w = *reinterpret_cast<const uint2*>(rsrc + (r * 2 + ch) * A + c * 8);
-                        v = expand8(w.x, w.y);
+                    if (live) {
+                        const uint2 w = *reinterpret_cast<const uint2*>(rsrc + r * 2 * A);
+                        v = offset8(w.x, w.y);
+                        bytes[0] += v.x;
+                        bytes[1] += v.y;
+                        bytes[2] += v.z;
+                        bytes[3] += v.w;
                     }
-                    *reinterpret_cast<uint4*>(xdst + ch * (kTile * 128) + r * 128 + ((c ^ (r & 7)) << 4)) = v;
+                    *reinterpret_cast<uint4*>(xdst + r * 128 + ((c ^ (r & 7)) << 4)) = v;
                 }
                 fence_proxy_async_smem();
                 __syncwarp();
@@ -216,16 +260,57 @@ doa_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovParams p) {
                 }
                 if (++stage == kRawStages) { stage = 0; phase ^= 1; }
                 if (++xst == kXStages) { xst = 0; xph ^= 1; }
+                if ((k & 3) == 3) flush_bytes();
+                if ((k & 511) == 511) flush_wide();
             }
+            if (stop) break;
+            flush_bytes();
+            flush_wide();
+            // the warp's four row groups share each chunk: lanes c, c + 8, ...
+#pragma unroll
+            for (int i = 0; i < 16; ++i) {
+                total[i] += __shfl_xor_sync(0xffffffffu, total[i], 8);
+                total[i] += __shfl_xor_sync(0xffffffffu, total[i], 16);
+            }
+            if (!mbar_wait(&part_empty[pst], pph ^ 1, kWaitNs)) { fail(256); break; }
+            if (lane < 8) {
+                uint32_t* dst = s_part + (pst * kUnpackWarps + (warp - 2)) * 128 + 16 * lane;
+#pragma unroll
+                for (int i = 0; i < 16; ++i) dst[i] = total[i];
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&part_full[pst]);
+            if (++pst == 2) { pst = 0; pph ^= 1; }
         }
     } else {
         const int q4 = warp & 3;
-        const int m = 32 * q4 + lane;       // component row of G
-        const int i = m >> 1, comp = m & 1; // antenna, 0 = re / 1 = im part of R
+        const int et = 32 * (warp - kEpiFirstWarp) + lane;  // 0 .. 127
+        const int m = 32 * q4 + lane;                         // component row of G
+        const int mc = m >> 4, mh = (m >> 2) & 3;
+        const int i = 8 * mc + 4 * (mh >> 1) + (m & 3);       // antenna
+        const int comp = mh & 1;                              // 0 = re / 1 = im part of R
+        const uint32_t k64 = 64u * static_cast<uint32_t>(p.block_len);
         int ast = 0;
         uint32_t aph = 0;
         bool stop = false;
         for (long long u = u_begin; u < u_end && !stop; ++u) {
+            // component sums of the unit: nine warp partials per channel
+            if (!mbar_wait(&part_full[ast], aph, kWaitNs)) { fail(512); break; }
+#pragma unroll
+            for (int ch = 0; ch < 2; ++ch) {
+                uint32_t acc = 0;
+#pragma unroll
+                for (int w = 0; w < kWarpsPerChannel; ++w) {
+                    acc += s_part[(ast * kUnpackWarps + ch * kWarpsPerChannel + w) * 128 + et];
+                }
+                s_sum[(ast * 2 + ch) * 128 + et] = acc;
+            }
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive(&part_empty[ast]);
+                mbar_arrive(&sum_ready[ast]);
+            }
+            if (!mbar_wait(&sum_ready[ast], aph, kWaitNs)) { fail(1024); break; }
             if (!mbar_wait(&acc_full[ast], aph, kWaitNs)) { fail(128); break; }
             tc_fence_after();
             const int b = static_cast<int>(u / p.n_pairs), fp = static_cast<int>(u % p.n_pairs);
@@ -233,19 +318,25 @@ doa_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovParams p) {
             for (int ch = 0; ch < 2; ++ch) {
                 const int f = 2 * fp + ch;
                 if (f >= p.n_freq) break;
+                const uint32_t* sums = s_sum + (ast * 2 + ch) * 128;
+                // G = Gu - 8 (S_m + S_n) + 64 K, in wrapping 32-bit arithmetic
+                const uint32_t bias_m = k64 - 8u * sums[m];
                 int32_t* row = p.out + ((static_cast<size_t>(b) * p.n_freq + f) * A + i) * A * 2;
                 const uint32_t taddr = tmem_base + ((32u * q4) << 16) + ast * 256 + ch * 128;
 #pragma unroll 1
-                for (int c = 0; c < 4; ++c) {
+                for (int cc = 0; cc < 4; ++cc) {
                     uint32_t g[32];
-                    tmem_ld_32x32b_x32(taddr + 32 * c, g);
+                    tmem_ld_32x32b_x32(taddr + 32 * cc, g);
                     tmem_ld_wait();
 #pragma unroll
-                    for (int jj = 0; jj < 16; ++jj) {
-                        const int j = 16 * c + jj;
-                        const int32_t own = static_cast<int32_t>(g[2 * jj]);
-                        const int32_t recv = __shfl_xor_sync(0xffffffffu, static_cast<int32_t>(g[2 * jj + 1]), 1);
-                        const int32_t val = comp == 0 ? own + recv : own - recv;
+                    for (int jl = 0; jl < 16; ++jl) {
+                        // antenna j = 16 cc + jl: columns re j and im j of this 32-column chunk
+                        const int j = 16 * cc + jl;
+                        const int n_re = 16 * (jl >> 3) + 8 * ((jl >> 2) & 1) + (jl & 3), n_im = n_re + 4;
+                        const uint32_t own = g[n_re] + bias_m - 8u * sums[32 * cc + n_re];
+                        const uint32_t send = g[n_im] + bias_m - 8u * sums[32 * cc + n_im];
+                        const uint32_t recv = __shfl_xor_sync(0xffffffffu, send, 4);
+                        const int32_t val = static_cast<int32_t>(comp == 0 ? own + recv : own - recv);
                         if (i < A && j < A) row[2 * j + comp] = val;
                     }
                 }
@@ -287,7 +378,9 @@ template <int A>
 bf_status launch_cov(cudaStream_t stream, const CUtensorMap& map, const CovParams& p) {
     // at least 120 KB, so that one CTA (512 TMEM columns) holds an SM and
     // tcgen05.alloc never has to wait for a column
-    const size_t smem = std::max<size_t>(kXStages * kXBytes + kRawStages * kTile * 2 * A + 256 + 1024, 120 * 1024);
+    const size_t smem = std::max<size_t>(kXStages * kXBytes + kRawStages * kTile * 2 * A + 512 +
+                                             (2 * kUnpackWarps + 4) * 128 * sizeof(uint32_t) + 1024,
+                                         120 * 1024);
     auto kern = doa_cov_kernel<A>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return cuda_status(e, "doa_cov_kernel smem attribute");
@@ -310,7 +403,7 @@ bf_status launch_doa_covariance(cudaStream_t stream, const uint8_t* v, int32_t* 
         return set_error(BF_ERR_INVALID_ARGUMENT,
                          "block length must be a positive multiple of 128 that divides n_time");
     }
-    if (block_len > (1ull << 24) || d.n_time >= (1ull << 31)) {
+    if (block_len > (1ull << 23) || d.n_time >= (1ull << 31)) {
         return set_error(BF_ERR_OVERFLOW, "covariance block or stream too long for int32 sums");
     }
     EncodeTiledFn enc = encode_fn_cov();

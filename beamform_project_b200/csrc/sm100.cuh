@@ -186,6 +186,17 @@ __host__ __device__ constexpr uint32_t idesc_s8_s32_mn(uint32_t m, uint32_t n) {
            | ((m >> 4) << 24);
 }
 
+// Instruction descriptor: kind::i8, A = B = u8, D = s32, both MN-major.
+__host__ __device__ constexpr uint32_t idesc_u8_s32_mn(uint32_t m, uint32_t n) {
+    return (2u << 4)            // D format s32
+           | (0u << 7)          // A unsigned int8
+           | (0u << 10)         // B unsigned int8
+           | (1u << 15)         // A MN-major
+           | (1u << 16)         // B MN-major
+           | ((n >> 3) << 17)
+           | ((m >> 4) << 24);
+}
+
 // Instruction descriptor: kind::f16, A = B = f16, D = f32, both K-major.
 __host__ __device__ constexpr uint32_t idesc_f16_f32(uint32_t m, uint32_t n) {
     return (1u << 4)            // D format f32

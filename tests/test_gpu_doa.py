@@ -86,6 +86,40 @@ def test_covariance_bit_exact(cuda, orc, A, K, B):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("fill", [0x88, 0x77, 0x78])
+def test_covariance_extreme_components(cuda, orc, fill):
+    """Constant -8 / +7 components (the largest block sums) and mixed signs."""
+    from beamform_project_b200 import api, native
+    torch = cuda
+    A, K, B = 64, 128, 2
+    v = np.full((K * B, F, A), fill, np.uint8)
+    out = torch.full((B * F * A * A * 2,), 12345, dtype=torch.int32, device="cuda")
+    api.doa_covariance_i32(None, torch.from_numpy(v).cuda(), out, api.Dimensions(K * B, F, A, 1), K)
+    torch.cuda.synchronize()
+    assert native.take_device_error() == 0
+    got = out.cpu().numpy().reshape(B, F, A, A, 2).astype(np.int64)
+    assert np.array_equal(got, orc.covariance_blocks(v, K))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("A", [32, 64])
+def test_covariance_long_block_is_sum_of_tiles(cuda, orc, A):
+    """A block of 520 tiles (past the kernel's 512-tile flush of its component
+    sums) of one repeated 128-spectrum tile is 520 times that tile's sums."""
+    from beamform_project_b200 import api, native
+    torch = cuda
+    reps, K1 = 520, 128
+    tile = random_voltage(K1, F, A, seed=11)
+    out = torch.full((F * A * A * 2,), 12345, dtype=torch.int32, device="cuda")
+    v = torch.from_numpy(tile).cuda().repeat(reps, 1, 1).contiguous()
+    api.doa_covariance_i32(None, v, out, api.Dimensions(K1 * reps, F, A, 1), K1 * reps)
+    torch.cuda.synchronize()
+    assert native.take_device_error() == 0
+    got = out.cpu().numpy().reshape(F, A, A, 2).astype(np.int64)
+    assert np.array_equal(got, reps * orc.covariance_blocks(tile, K1)[0])
+
+
+@pytest.mark.gpu
 def test_scan_matches_fp64_oracle_and_finds_sources(cuda, orc):
     from beamform_project_b200 import api, native
     torch = cuda
