@@ -207,6 +207,13 @@ doa_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovParams p) {
         const int ch = ut / kPerChannel, local = ut % kPerChannel;
         const int c = local & 7, r0 = local >> 3;
         const bool live = c < A / 8;
+        // rows r0 + i kRowStep, i < 4 (the fourth exists for r0 < 20); the
+        // swizzle r & 7 alternates between two values since kRowStep % 8 == 4
+        static_assert(kRowStep % 8 == 4 && 3 * kRowStep < kTile && 4 * kRowStep >= kTile, "row split");
+        const bool has4 = r0 + 3 * kRowStep < kTile;
+        const int raw_off = ch * A + c * 8 + r0 * 2 * A;
+        const int x_off = ch * (kTile * 128) + r0 * 128;
+        const int xsw_even = (c ^ (r0 & 7)) << 4, xsw_odd = xsw_even ^ 64;
         int stage = 0, xst = 0, pst = 0;
         uint32_t phase = 0, xph = 0, pph = 0;
         bool stop = false;
@@ -237,20 +244,22 @@ doa_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovParams p) {
                 if (*s_fail) { stop = true; break; }
                 if (!mbar_wait(&raw_full[stage], phase, kWaitNs)) { fail(32); stop = true; break; }
                 if (!mbar_wait(&x_empty[xst], xph ^ 1, kWaitNs)) { fail(64); stop = true; break; }
-                const uint8_t* rsrc = raw + stage * RAW + ch * A + c * 8;
-                uint8_t* xdst = xs + xst * kXBytes + ch * (kTile * 128);
-#pragma unroll 4
-                for (int r = r0; r < kTile; r += kRowStep) {
-                    uint4 v = make_uint4(0, 0, 0, 0);
-                    if (live) {
-                        const uint2 w = *reinterpret_cast<const uint2*>(rsrc + r * 2 * A);
-                        v = offset8(w.x, w.y);
-                        bytes[0] += v.x;
-                        bytes[1] += v.y;
-                        bytes[2] += v.z;
-                        bytes[3] += v.w;
+                const uint8_t* rsrc = raw + stage * RAW + raw_off;
+                uint8_t* xdst = xs + xst * kXBytes + x_off;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    if (i < 3 || has4) {
+                        uint4 v = make_uint4(0, 0, 0, 0);
+                        if (live) {
+                            const uint2 w = *reinterpret_cast<const uint2*>(rsrc + i * kRowStep * 2 * A);
+                            v = offset8(w.x, w.y);
+                            bytes[0] += v.x;
+                            bytes[1] += v.y;
+                            bytes[2] += v.z;
+                            bytes[3] += v.w;
+                        }
+                        *reinterpret_cast<uint4*>(xdst + i * kRowStep * 128 + ((i & 1) != 0 ? xsw_odd : xsw_even)) = v;
                     }
-                    *reinterpret_cast<uint4*>(xdst + r * 128 + ((c ^ (r & 7)) << 4)) = v;
                 }
                 fence_proxy_async_smem();
                 __syncwarp();
