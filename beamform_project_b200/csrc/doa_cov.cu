@@ -29,7 +29,8 @@
 // single channel's 64 bytes would make DRAM fetch the neighbour twice).
 // Warp 0 TMA producer (raw 128-spectrum tiles of both channels), warp 1 MMA
 // issuer and TMEM owner, warps 2-19 unpack (int4 -> offset-binary bytes,
-// 128-byte swizzle, one tile per channel: nine warps per channel), warps
+// 128-byte swizzle, one tile per channel; a warp reads two spectra of both
+// channels, 256 contiguous bytes, so the raw loads are conflict free), warps
 // 20-23 epilogue (two 128 x 128 int32 accumulators per unit, two TMEM stages
 // of 256 columns).  All waits are bounded and report through the device
 // error word.
@@ -50,11 +51,9 @@ using namespace sm100;
 constexpr int kThreads = 768;
 constexpr int kUnpackWarps = 18;                 // nine per channel of the pair
 constexpr int kEpiFirstWarp = 2 + kUnpackWarps;
-constexpr int kPerChannel = 32 * kUnpackWarps / 2;  // unpack threads per channel
-constexpr int kRowStep = kPerChannel / 8;        // rows between a thread's chunks
-constexpr int kWarpsPerChannel = kUnpackWarps / 2;
+constexpr int kRowStep = 32 * kUnpackWarps / 16; // rows between a thread's chunks
 constexpr int kTile = 128;        // spectra per tile
-constexpr int kRawStages = 6;
+constexpr int kRawStages = 5;
 constexpr int kXStages = 3;
 constexpr uint32_t kXBytes = 2 * kTile * 128;  // one unpacked tile per channel of the pair
 constexpr uint64_t kWaitNs = 2000000000ull;
@@ -92,8 +91,8 @@ doa_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovParams p) {
     uint8_t* xs = smem;                                  // kXStages x 2 x 16 KiB
     uint8_t* raw = smem + kXStages * kXBytes;            // kRawStages x RAW
     uint64_t* bars = reinterpret_cast<uint64_t*>(raw + kRawStages * RAW);  // 512 bytes
-    uint32_t* s_part = reinterpret_cast<uint32_t*>(raw + kRawStages * RAW + 512);  // [2][kUnpackWarps][128]
-    uint32_t* s_sum = s_part + 2 * kUnpackWarps * 128;                             // [2][2][128]
+    uint32_t* s_part = reinterpret_cast<uint32_t*>(raw + kRawStages * RAW + 512);  // [2][kUnpackWarps][2][128]
+    uint32_t* s_sum = s_part + 2 * kUnpackWarps * 256;                             // [2][2][128]
     uint64_t* raw_full = bars;                           // [kRawStages]
     uint64_t* raw_empty = bars + kRawStages;             // [kRawStages]
     uint64_t* x_full = bars + 2 * kRawStages;            // [kXStages]
@@ -198,14 +197,14 @@ doa_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovParams p) {
             if (!mbar_wait(mma_done, 0, kWaitNs)) fail(16);
         }
     } else if (warp < kEpiFirstWarp) {
-        // thread = (channel, chunk c of 8 antennas, first row r0); rows r0,
-        // r0 + kRowStep, ... of every tile.  Component sums: bytes[] adds the
+        // thread = (chunk c of 8 antennas, channel, first row r0) from its
+        // index bits (2..0, 3, 9..4); rows r0, r0 + kRowStep, ... of every
+        // tile.  Component sums: bytes[] adds the
         // offset words (at most 4 rows x 15 per byte per tile, flushed every
         // 4 tiles), wide[] the even / odd bytes in 16-bit lanes (flushed to
         // total[] every 512 tiles), total[] the unit's sums.
         const int ut = threadIdx.x - 64;
-        const int ch = ut / kPerChannel, local = ut % kPerChannel;
-        const int c = local & 7, r0 = local >> 3;
+        const int c = ut & 7, ch = (ut >> 3) & 1, r0 = ut >> 4;
         const bool live = c < A / 8;
         // rows r0 + i kRowStep, i < 4 (the fourth exists for r0 < 20); the
         // swizzle r & 7 alternates between two values since kRowStep % 8 == 4
@@ -275,15 +274,12 @@ doa_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovParams p) {
             if (stop) break;
             flush_bytes();
             flush_wide();
-            // the warp's four row groups share each chunk: lanes c, c + 8, ...
+            // the warp's two row groups share each (channel, chunk): lanes l, l + 16
 #pragma unroll
-            for (int i = 0; i < 16; ++i) {
-                total[i] += __shfl_xor_sync(0xffffffffu, total[i], 8);
-                total[i] += __shfl_xor_sync(0xffffffffu, total[i], 16);
-            }
+            for (int i = 0; i < 16; ++i) total[i] += __shfl_xor_sync(0xffffffffu, total[i], 16);
             if (!mbar_wait(&part_empty[pst], pph ^ 1, kWaitNs)) { fail(256); break; }
-            if (lane < 8) {
-                uint32_t* dst = s_part + (pst * kUnpackWarps + (warp - 2)) * 128 + 16 * lane;
+            if (lane < 16) {
+                uint32_t* dst = s_part + ((pst * kUnpackWarps + (warp - 2)) * 2 + ch) * 128 + 16 * c;
 #pragma unroll
                 for (int i = 0; i < 16; ++i) dst[i] = total[i];
             }
@@ -303,14 +299,14 @@ doa_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovParams p) {
         uint32_t aph = 0;
         bool stop = false;
         for (long long u = u_begin; u < u_end && !stop; ++u) {
-            // component sums of the unit: nine warp partials per channel
+            // component sums of the unit: one partial per unpack warp and channel
             if (!mbar_wait(&part_full[ast], aph, kWaitNs)) { fail(512); break; }
 #pragma unroll
             for (int ch = 0; ch < 2; ++ch) {
                 uint32_t acc = 0;
 #pragma unroll
-                for (int w = 0; w < kWarpsPerChannel; ++w) {
-                    acc += s_part[(ast * kUnpackWarps + ch * kWarpsPerChannel + w) * 128 + et];
+                for (int w = 0; w < kUnpackWarps; ++w) {
+                    acc += s_part[((ast * kUnpackWarps + w) * 2 + ch) * 128 + et];
                 }
                 s_sum[(ast * 2 + ch) * 128 + et] = acc;
             }
@@ -388,7 +384,7 @@ bf_status launch_cov(cudaStream_t stream, const CUtensorMap& map, const CovParam
     // at least 120 KB, so that one CTA (512 TMEM columns) holds an SM and
     // tcgen05.alloc never has to wait for a column
     const size_t smem = std::max<size_t>(kXStages * kXBytes + kRawStages * kTile * 2 * A + 512 +
-                                             (2 * kUnpackWarps + 4) * 128 * sizeof(uint32_t) + 1024,
+                                             (4 * kUnpackWarps + 4) * 128 * sizeof(uint32_t) + 1024,
                                          120 * 1024);
     auto kern = doa_cov_kernel<A>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
