@@ -15,17 +15,19 @@
 //                 summed over frequency in channel order
 //   peak          argmax and the vertex of the parabola through it and its
 //                 neighbours (concave case).
-// FP64 is used for the phase argument before its reduction mod 2 pi, the
-// forgetting accumulation and the loaded Cholesky solve; the reduced phase
-// goes through float sincos.
+// FP64 is used for the phase argument before its reduction to a quadrant,
+// the forgetting accumulation and the loaded Cholesky solve; the reduced
+// phase goes through the FP32 Taylor sin / cos of tracker_common.cuh.
 #include "bf_internal.cuh"
+#include "tracker_common.cuh"
+
+#include <cooperative_groups.h>
 
 #include <algorithm>
 
 namespace bf {
 namespace {
 
-constexpr double kTwoPi = 6.283185307179586476925286766559;
 constexpr int kMaxM = 16;
 
 struct Cd {
@@ -167,17 +169,24 @@ __global__ void doa_factor_kernel(const Cd* __restrict S_in, const double* __res
     }
 }
 
-// A CTA of 8 warps takes 32 grid points and 4 blocks: lane = grid point,
-// warp w the channels f = 8 s + w of step s.  The steering vector of
-// (channel, point) is formed once and used for the 4 blocks.  Bartlett
-// a^H S a and Capon 1 / (a^H Q a), Q = (S + eps I)^{-1}, are Hermitian
-// quadratic forms (diagonal plus twice the real part of the upper triangle);
-// the upper triangles of S and Q for the next step's 8 channels x 4 blocks
-// are staged into shared memory with cp.async while the current step
-// computes.  Per-warp partial sums are added in warp order at the end (a
-// fixed order, so results are deterministic).
+// A CTA of 8 warps takes 32 grid points and KB blocks (4, or 2 for more
+// than 13 elements): lane = grid point, warp w the channels f = 8 s + w of
+// step s.  The steering vector of (channel, point) is formed once and used
+// for the KB blocks.  Bartlett a^H S a and Capon 1 / (a^H Q a),
+// Q = (S + eps I)^{-1}, are Hermitian quadratic forms (diagonal plus twice
+// the real part of the upper triangle); the upper triangles of S and Q for
+// the next step's 8 channels x KB blocks are staged into shared memory with
+// cp.async while the current step computes.
+// The channel steps split over the z extent of the grid, a thread-block
+// cluster of up to 8 CTAs, so that the grid fills the GPU's resident CTA
+// slots; each CTA adds its warps' partial sums in warp order, and cluster
+// rank 0 adds the CTAs' sums in rank order through distributed shared
+// memory (a fixed order: results are deterministic for a given split).
 constexpr int kScanWarps = 8;
-constexpr int kScanBlocks = 4;
+constexpr int kMaxSplit = 8;
+
+template <int M>
+__host__ __device__ constexpr int scan_blocks() { return M <= 13 ? 4 : 2; }
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(smem))),
@@ -192,7 +201,8 @@ __global__ void __launch_bounds__(kScanWarps * 32)
 doa_scan_kernel(const Cd* __restrict S, const Cd* __restrict Q, const int* __restrict ok,
                 const float* __restrict pos, const double* __restrict kw, int n_blocks, int n_freq,
                 double l_first, double l_step, int n, double m_fixed, double* __restrict bartlett,
-                double* __restrict capon) {
+                double* __restrict capon, int steps_per_split) {
+    constexpr int kScanBlocks = scan_blocks<M>();
     constexpr int U = M * (M + 1) / 2;                 // upper triangle incl. diagonal
     constexpr int kPerWarp = kScanBlocks * 2 * U;      // Cd staged per warp and step
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -202,7 +212,10 @@ doa_scan_kernel(const Cd* __restrict S, const Cd* __restrict Q, const int* __res
     extern __shared__ Cd scan_stage[];                 // [2][warps][blocks][S | Q][U]
     __shared__ int s_ok[2][kScanWarps][kScanBlocks];
     __shared__ double red_b[kScanWarps][kScanBlocks][32], red_c[kScanWarps][kScanBlocks][32];
+    __shared__ double fin_b[kScanBlocks][32], fin_c[kScanBlocks][32];
     const int n_steps = (n_freq + kScanWarps - 1) / kScanWarps;
+    const int st_begin = static_cast<int>(blockIdx.z) * steps_per_split;
+    const int st_end = min(n_steps, st_begin + steps_per_split);
 
     // stage step s: thread t copies elements t, t + 256, ... of the step
     auto stage = [&](int st, int buf) {
@@ -236,9 +249,9 @@ doa_scan_kernel(const Cd* __restrict S, const Cd* __restrict Q, const int* __res
         px[i] = static_cast<double>(pos[3 * i]);
         py[i] = static_cast<double>(pos[3 * i + 1]);
     }
-    stage(0, 0);
-    for (int st = 0; st < n_steps; ++st) {
-        if (st + 1 < n_steps) stage(st + 1, (st + 1) & 1);
+    stage(st_begin, st_begin & 1);
+    for (int st = st_begin; st < st_end; ++st) {
+        if (st + 1 < st_end) stage(st + 1, (st + 1) & 1);
         else cp_async_commit();  // keep one group per step for wait_group 1
         cp_async_wait_1();
         __syncthreads();
@@ -250,11 +263,13 @@ doa_scan_kernel(const Cd* __restrict S, const Cd* __restrict Q, const int* __res
             const double k = kw[f];
 #pragma unroll
             for (int i = 0; i < M; ++i) {
+                constexpr double kHalfPi = 1.5707963267948966192313216916398;
+                constexpr double kTwoOverPi = 0.63661977236758134307553505349006;
                 const double ph = k * (px[i] * lv + py[i] * m_fixed);
-                const double rr = ph - kTwoPi * rint(ph * (1.0 / kTwoPi));
-                float sn, cs;
-                sincosf(static_cast<float>(rr), &sn, &cs);
-                a[i] = Cd{static_cast<double>(cs), -static_cast<double>(sn)};
+                const double q = rint(ph * kTwoOverPi);
+                const float2 w = trk::sincos_quadrant(__double2float_rn(__fma_rn(-kHalfPi, q, ph)),
+                                                      static_cast<int>(static_cast<long long>(q) & 3));
+                a[i] = Cd{static_cast<double>(w.x), -static_cast<double>(w.y)};
                 mag[i] = a[i].re * a[i].re + a[i].im * a[i].im;
             }
             auto quad = [&](const Cd* X) {
@@ -294,29 +309,88 @@ doa_scan_kernel(const Cd* __restrict S, const Cd* __restrict Q, const int* __res
         red_c[warp][bi][lane] = pc[bi];
     }
     __syncthreads();
-    if (warp < nb && l < n) {
-        double sb = 0.0, sc = 0.0;
+    double sb = 0.0, sc = 0.0;
+    if (warp < nb) {
         for (int w = 0; w < kScanWarps; ++w) {
             sb += red_b[w][warp][lane];
             sc += red_c[w][warp][lane];
         }
-        bartlett[static_cast<size_t>(b0 + warp) * n + l] = sb;
-        capon[static_cast<size_t>(b0 + warp) * n + l] = sc;
     }
+    if (gridDim.z == 1) {
+        if (warp < nb && l < n) {
+            bartlett[static_cast<size_t>(b0 + warp) * n + l] = sb;
+            capon[static_cast<size_t>(b0 + warp) * n + l] = sc;
+        }
+        return;
+    }
+    if (warp < nb) {
+        fin_b[warp][lane] = sb;
+        fin_c[warp][lane] = sc;
+    }
+    namespace cg = cooperative_groups;
+    cg::cluster_group cluster = cg::this_cluster();
+    cluster.sync();
+    if (cluster.block_rank() == 0 && warp < nb && l < n) {
+        double tb = 0.0, tc = 0.0;
+        for (unsigned r = 0; r < gridDim.z; ++r) {
+            tb += *cluster.map_shared_rank(&fin_b[warp][lane], r);
+            tc += *cluster.map_shared_rank(&fin_c[warp][lane], r);
+        }
+        bartlett[static_cast<size_t>(b0 + warp) * n + l] = tb;
+        capon[static_cast<size_t>(b0 + warp) * n + l] = tc;
+    }
+    cluster.sync();  // the other CTAs keep their shared memory until rank 0 has read it
+}
+
+// Channel-step split: the smallest modelled time ceil(CTAs / slots) *
+// (steps per CTA + 1/2) over splits of 1 .. kMaxSplit, where slots are the
+// GPU's resident CTAs of this kernel.
+int scan_split(long long base_ctas, int n_steps, long long slots) {
+    int best = 1;
+    double best_cost = 1e300;
+    for (int s = 1; s <= std::min(kMaxSplit, n_steps); ++s) {
+        const int per = (n_steps + s - 1) / s;
+        const int splits = (n_steps + per - 1) / per;
+        const long long waves = (base_ctas * splits + slots - 1) / slots;
+        const double cost = static_cast<double>(waves) * (per + 0.5);
+        if (cost < best_cost - 1e-9) { best_cost = cost; best = splits; }
+    }
+    return best;
 }
 
 template <int M>
 bf_status launch_scan_m(cudaStream_t stream, const Cd* S, const Cd* Q, const int* ok, const float* pos,
                         const double* kw, int B, int F, double l_first, double l_step, int n, double m_fixed,
                         double* bartlett, double* capon) {
-    const dim3 grid(static_cast<unsigned>((n + 31) / 32), static_cast<unsigned>((B + kScanBlocks - 1) / kScanBlocks));
-    const size_t smem = 2ull * kScanWarps * kScanBlocks * 2 * (M * (M + 1) / 2) * sizeof(Cd);
-    cudaError_t e = cudaFuncSetAttribute(doa_scan_kernel<M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         static_cast<int>(smem));
+    constexpr int KB = scan_blocks<M>();
+    const unsigned gx = static_cast<unsigned>((n + 31) / 32), gy = static_cast<unsigned>((B + KB - 1) / KB);
+    const size_t smem = 2ull * kScanWarps * KB * 2 * (M * (M + 1) / 2) * sizeof(Cd);
+    auto kern = doa_scan_kernel<M>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return cuda_status(e, "doa_scan_kernel smem attribute");
-    doa_scan_kernel<M><<<grid, kScanWarps * 32, smem, stream>>>(S, Q, ok, pos, kw, B, F, l_first, l_step, n,
-                                                               m_fixed, bartlett, capon);
-    return cuda_status(cudaGetLastError(), "doa_scan_kernel launch");
+    int dev = 0, sms = 148, per_sm = 1;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kScanWarps * 32, smem);
+    if (e != cudaSuccess) return cuda_status(e, "doa_scan_kernel occupancy");
+    const int n_steps = (F + kScanWarps - 1) / kScanWarps;
+    const int split = scan_split(static_cast<long long>(gx) * gy, n_steps,
+                                 static_cast<long long>(std::max(per_sm, 1)) * sms);
+    const int per = (n_steps + split - 1) / split;
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = dim3(gx, gy, static_cast<unsigned>(split));
+    cfg.blockDim = dim3(kScanWarps * 32, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 1;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = static_cast<unsigned>(split);
+    cfg.attrs = attr;
+    cfg.numAttrs = split > 1 ? 1 : 0;
+    e = cudaLaunchKernelEx(&cfg, kern, S, Q, ok, pos, kw, B, F, l_first, l_step, n, m_fixed, bartlett, capon, per);
+    return cuda_status(e == cudaSuccess ? cudaGetLastError() : e, "doa_scan_kernel launch");
 }
 
 template <int M>

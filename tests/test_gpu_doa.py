@@ -153,3 +153,31 @@ def test_scan_matches_fp64_oracle_and_finds_sources(cuda, orc):
     peaks = [i for i in range(1, n - 1) if P[i] > P[i - 1] and P[i] >= P[i + 1]]
     top = sorted(-0.9 + 0.001 * i for i in sorted(peaks, key=lambda i: -P[i])[:2])
     assert -0.14 < top[0] < 0.14 and abs(top[1] - 0.5) < 0.03, top
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("M", [3, 13, 14, 16])
+def test_scan_element_counts_match_fp64_oracle(cuda, orc, M):
+    """Sub-array sizes across the scan's shared-memory layouts (four blocks
+    per CTA up to 13 elements, two above) agree with the FP64 oracle."""
+    from beamform_project_b200 import api, native
+    torch = cuda
+    A, K, B, n = 64, 128, 3, 301
+    pos, freq, kw = geometry(A)
+    amp = 2.0 * math.sqrt(2.0)
+    v = source_voltage(K * B, A, [(0.2, amp, 0.0)], seed=M)
+    d = api.Dimensions(K * B, F, A, 1)
+    cov = torch.empty(B * F * A * A * 2, dtype=torch.int32, device="cuda")
+    api.doa_covariance_i32(None, torch.from_numpy(v).cuda(), cov, d, K)
+    bart = torch.empty(B * n, dtype=torch.float64, device="cuda")
+    cap = torch.empty(B * n, dtype=torch.float64, device="cuda")
+    lest = torch.empty(2 * B, dtype=torch.float64, device="cuda")
+    ws = torch.empty(api.doa_workspace_bytes(d, K, M), dtype=torch.uint8, device="cuda")
+    api.doa_scan(None, cov, torch.from_numpy(pos[:M]).cuda(), torch.from_numpy(kw).cuda(), d, K, M, 0.9, 1e-3,
+                 -0.6, 0.004, n, 0.0, bart, cap, lest, ws)
+    torch.cuda.synchronize()
+    assert native.take_device_error() == 0
+    R = cov.cpu().numpy().reshape(B, F, A, A, 2).astype(np.int64)
+    eb, ec, el = orc.doa_scan(R, K, M, 0.9, 1e-3, pos[:M], kw, -0.6, 0.004, n)
+    assert np.allclose(bart.cpu().numpy().reshape(B, n), eb, rtol=1e-6, atol=0.0)
+    assert np.allclose(cap.cpu().numpy().reshape(B, n), ec, rtol=1e-6, atol=0.0)
