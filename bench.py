@@ -56,8 +56,8 @@ METRIC = "beam-samples/s (T*F*B)"
 # their commands are summarised under profiles/.
 NCU_TRAFFIC = {
     "grid": 2 * (767.70e6 + 18.97e6),
-    "tracker": 8 * (704.703488e6 + 5.743616e6),
-    "doa": 1.409467e9 + 164.409344e6,
+    "tracker": 8 * (704.677888e6 + 3.885312e6),
+    "doa": 1.410239e9 + 162.888960e6,
 }
 
 
