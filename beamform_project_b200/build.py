@@ -5,6 +5,7 @@
 Products:
     beamform_project_b200/lib/libbf_b200.so   C ABI of include/bf_b200.h + kernels
     beamform_project_b200/lib/libbf_cxx.so    C++ API of include/beamformer/ over the C ABI
+    beamform_project_b200/bin/beamformer_cuda command-line beamformer (the reference CLI's options)
 
 The oracle (test infrastructure) is built by oracle/build.py.
 """
@@ -28,7 +29,10 @@ NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibilit
 CUDA_SOURCES = ["capi.cu", "grid_exact.cu", "quantize.cu", "generate.cu", "tracker.cu",
                 "tracker_stream.cu", "grid_tc.cu", "no_alloc.cu", "doa_cov.cu", "doa_scan.cu",
                 "serve_kernels.cu", "serve.cu", "selftest.cu"]
-CXX_SOURCES = ["cxx_api.cpp"]
+CXX_SOURCES = ["cxx_api.cpp", "io.cpp"]
+CLI = PKG / "cli"
+BIN = PKG / "bin"
+CLI_PROGRAMS = ["beamformer_cuda"]
 
 
 def _nvcc() -> str:
@@ -79,14 +83,24 @@ def build(verbose: bool = False, force: bool = False) -> Path:
                   "-I", "/usr/local/cuda/include", *map(str, cxx_srcs), "-o", str(cxx_so),
                   "-L", str(LIB), "-lbf_b200", "-Wl,-rpath,$ORIGIN",
                   "-L", "/usr/local/cuda/lib64", "-lcudart"], log)
-        # C++ API test program (tests/cxx), built here so it ships with the libraries
-        test_src = ROOT / "tests" / "cxx" / "test_cxx_api.cpp"
-        test_bin = obj_dir / "test_cxx_api"
-        if test_src.exists() and (force or _stale(test_bin, [test_src, cxx_so] + cxx_headers)):
-            _run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-I", str(INCLUDE),
-                  "-I", "/usr/local/cuda/include", str(test_src), "-o", str(test_bin),
-                  "-L", str(LIB), "-lbf_cxx", "-lbf_b200", f"-Wl,-rpath,{LIB}",
-                  "-L", "/usr/local/cuda/lib64", "-lcudart"], log)
+        # command-line programs over the C++ API (beamform_project_b200/bin)
+        BIN.mkdir(exist_ok=True)
+        for prog in CLI_PROGRAMS:
+            src = CLI / f"{prog}.cpp"
+            out = BIN / prog
+            if force or _stale(out, [src, cxx_so] + cxx_headers):
+                _run(["g++", "-O2", "-std=c++17", "-I", str(INCLUDE), "-I", "/usr/local/cuda/include",
+                      str(src), "-o", str(out), "-L", str(LIB), "-lbf_cxx", "-lbf_b200",
+                      "-Wl,-rpath,$ORIGIN/../lib", "-L", "/usr/local/cuda/lib64", "-lcudart"], log)
+        # C++ test programs (tests/cxx), built here so they ship with the libraries
+        for name in ("test_cxx_api", "test_io"):
+            test_src = ROOT / "tests" / "cxx" / f"{name}.cpp"
+            test_bin = obj_dir / name
+            if test_src.exists() and (force or _stale(test_bin, [test_src, cxx_so] + cxx_headers)):
+                _run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-I", str(INCLUDE),
+                      "-I", "/usr/local/cuda/include", str(test_src), "-o", str(test_bin),
+                      "-L", str(LIB), "-lbf_cxx", "-lbf_b200", f"-Wl,-rpath,{LIB}",
+                      "-L", "/usr/local/cuda/lib64", "-lcudart"], log)
     (obj_dir / "build.log").write_text("\n".join(log))
     if verbose:
         print("\n".join(log))

@@ -58,6 +58,48 @@ using LossMask = std::vector<std::uint8_t>;
 
 constexpr std::size_t voltage_sample_count(const Dimensions& dims) { return dims.n_time * dims.n_freq * dims.n_ant; }
 constexpr std::size_t packed_voltage_bytes(const Dimensions& dims) { return voltage_sample_count(dims); }
+// one validity byte (0 = lost, 1 = valid) per [time][local frequency] frame
+constexpr std::size_t loss_mask_count(const Dimensions& dims) { return dims.n_time * dims.n_freq; }
+
+// One frequency shard as it arrives: the packed payload, its descriptor and
+// its loss mask (reference formats.hpp:22-34).
+struct PackedShard {
+    ShardDescriptor descriptor;
+    PackedVoltage payload;
+    LossMask loss_mask;
+};
+using PackedShardSet = std::array<PackedShard, frequency_shard_count>;
+
+// reference src/synthetic_data.cpp:139-171
+inline void validate_packed_shard(const PackedShard& shard, const Dimensions& dims) {
+    validate_dimensions(dims);
+    validate_shard_descriptor(shard.descriptor);
+    if (shard.payload.size() != packed_voltage_bytes(dims)) {
+        throw std::invalid_argument("shard payload size does not match dimensions");
+    }
+    if (shard.loss_mask.size() != loss_mask_count(dims)) {
+        throw std::invalid_argument("loss mask size does not match dimensions");
+    }
+    for (const std::uint8_t v : shard.loss_mask) {
+        if (v > 1U) throw std::invalid_argument("loss mask entries must be 0 or 1");
+    }
+}
+
+inline void validate_packed_shards(const PackedShardSet& shards, const Dimensions& dims) {
+    validate_dimensions(dims);
+    for (std::size_t i = 0; i < frequency_shard_count; ++i) {
+        validate_packed_shard(shards[i], dims);
+        if (shards[i].descriptor.shard_id != i) {
+            throw std::invalid_argument("shard IDs must identify their array slot");
+        }
+    }
+    if (shards[0].descriptor.absolute_frequency_start == shards[1].descriptor.absolute_frequency_start) {
+        throw std::invalid_argument("the two shards must have distinct frequency origins");
+    }
+    if (shards[0].descriptor.loss_mask_id == shards[1].descriptor.loss_mask_id) {
+        throw std::invalid_argument("the two shards must have independent loss masks");
+    }
+}
 constexpr std::size_t weight_bytes(const Dimensions& dims) {
     return dims.n_beams * dims.n_freq * dims.n_ant * 2 * sizeof(float);
 }

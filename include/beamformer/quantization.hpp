@@ -11,6 +11,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <stdexcept>
+#include <string>
 #include <vector>
 
 namespace beamformer {
@@ -60,5 +61,30 @@ struct QuantizedIntegratedOutput {
     QuantizedIntensities codes;
     std::vector<Int8QuantizationParameters> parameters;
 };
+
+// What a reader of an int8 product needs besides the codes and parameters
+// (reference quantization.hpp:75-83, validation src/quantization.cpp:235-249).
+struct QuantizedOutputMetadata {
+    Dimensions output_dims;
+    std::size_t input_n_time = 0;
+    TemporalIntegrationConfig temporal_integration{0};
+    ShardDescriptor shard;
+    std::string parameters_file;
+};
+
+inline void validate_quantized_output_metadata(const QuantizedOutputMetadata& metadata) {
+    validate_dimensions(metadata.output_dims);
+    validate_temporal_config(metadata.temporal_integration);
+    validate_shard_descriptor(metadata.shard);
+    if (metadata.input_n_time == 0) {
+        throw std::invalid_argument("quantized metadata input_n_time must be positive");
+    }
+    if (integrated_time_count(metadata.input_n_time, metadata.temporal_integration) != metadata.output_dims.n_time) {
+        throw std::invalid_argument("quantized metadata time dimensions are inconsistent");
+    }
+    if (metadata.parameters_file.empty()) {
+        throw std::invalid_argument("quantized metadata parameters_file must not be empty");
+    }
+}
 
 }  // namespace beamformer

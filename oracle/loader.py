@@ -82,6 +82,8 @@ def reference() -> C.CDLL:
         r.ref_set_threads.argtypes = [C.c_int]
         r.ref_doa_directions.argtypes = [P, U64, U64, U64, P, P, C.c_int, U64, U64, F32, F32, U64, F32,
                                          F32, U64, F32, F32, P]
+        r.ref_io_write.argtypes = [C.c_char_p, P, P, P, P, P, P, P] + [U64] * 9
+        r.ref_io_read_check.argtypes = [C.c_char_p, P, P, P, P, P, P] + [U64] * 9
         _r = r
     return _r
 
@@ -206,6 +208,22 @@ def unpack(v: np.ndarray):
 
 
 # ---------------- reference wrappers ----------------
+
+def ref_io_write(dirpath, arrays: dict, case: tuple) -> None:
+    """Every on-disk format written by the reference's src/io.cpp (ref_shim.cpp)."""
+    a = arrays
+    _rcheck(reference().ref_io_write(str(dirpath).encode(), _ptr(a["voltage"]), _ptr(a["weights"]), _ptr(a["tiled"]),
+                                     _ptr(a["intensity"]), _ptr(a["codes"]), _ptr(a["params"]), _ptr(a["loss"]),
+                                     *case))
+
+
+def ref_io_read_check(dirpath, arrays: dict, case: tuple) -> None:
+    """The reference's readers on dirpath; raises unless the contents equal arrays."""
+    a = arrays
+    _rcheck(reference().ref_io_read_check(str(dirpath).encode(), _ptr(a["voltage"]), _ptr(a["weights"]),
+                                          _ptr(a["tiled"]), _ptr(a["codes"]), _ptr(a["params"]), _ptr(a["loss"]),
+                                          *case))
+
 
 def ref_beamform(v, w, T, F, A, B) -> np.ndarray:
     out = np.zeros((T, F, B), np.float32)

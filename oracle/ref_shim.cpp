@@ -12,6 +12,7 @@
 #include <beamformer/cpu_opt_beam_tracker.hpp>
 #include <beamformer/cpu_beamformer.hpp>
 #include <beamformer/geometry.hpp>
+#include <beamformer/io.hpp>
 #include <beamformer/quantization.hpp>
 #include <beamformer/synthetic_data.hpp>
 #include <beamformer/temporal_integration.hpp>
@@ -252,6 +253,85 @@ int ref_doa_directions(const uint8_t* v, uint64_t T, uint64_t F, uint64_t A, con
             dirs[3 * w] = dd[0];
             dirs[3 * w + 1] = dd[1];
             dirs[3 * w + 2] = dd[2];
+        }
+    });
+}
+
+// src/io.cpp:60-344: every file format, written by the reference into dir
+// (voltage.bin, weights.bin, tiled.bin, intensity.bin, codes.bin,
+// params.bin, int8_meta.txt, shard_payload.bin, shard_meta.txt,
+// shard_loss.bin).  Dimensions T x F x A x B; the int8 files hold
+// W = ceil(T / S) windows; the shard descriptor is the default one of
+// shard_id with the given timestamps and loss-mask id.
+int ref_io_write(const char* dir, const uint8_t* volt, const float* w, const float* tw, const float* inten,
+                 const int8_t* codes, const float* params, const uint8_t* loss, uint64_t T, uint64_t F,
+                 uint64_t A, uint64_t B, uint64_t S, uint64_t shard_id, uint64_t ts_start, uint64_t ts_step,
+                 uint64_t loss_id) {
+    return guarded([&] {
+        const std::string base(dir);
+        const Dimensions d = dims_of(T, F, A, B);
+        const std::size_t W = integrated_time_count(T, TemporalIntegrationConfig{S});
+        const Dimensions wd = dims_of(W, F, A, B);
+        write_packed_voltage(base + "/voltage.bin", PackedVoltage(volt, volt + T * F * A), d);
+        Weights wv(B * F * A);
+        std::memcpy(wv.data(), w, wv.size() * sizeof(ComplexFloat));
+        write_weights(base + "/weights.bin", wv, d);
+        TiledWeights tv(tiled_weight_count(d));
+        std::memcpy(tv.data(), tw, tv.size() * sizeof(ComplexFloat));
+        write_tiled_weights(base + "/tiled.bin", tv, d);
+        write_intensities(base + "/intensity.bin", Intensities(inten, inten + T * F * B), d);
+        write_quantized_intensities(base + "/codes.bin", QuantizedIntensities(codes, codes + W * F * B), wd);
+        std::vector<Int8QuantizationParameters> pv(quantization_parameter_count(wd));
+        std::memcpy(pv.data(), params, pv.size() * sizeof(Int8QuantizationParameters));
+        write_quantization_parameters(base + "/params.bin", pv, wd);
+        ShardDescriptor sd = default_shard_descriptors()[shard_id];
+        sd.timestamp_start = ts_start;
+        sd.timestamp_step = ts_step;
+        sd.loss_mask_id = loss_id;
+        write_quantized_output_metadata(base + "/int8_meta.txt",
+                                        QuantizedOutputMetadata{wd, T, TemporalIntegrationConfig{S}, sd, "params.bin"});
+        PackedShard shard{sd, PackedVoltage(volt, volt + T * F * A), LossMask(loss, loss + T * F)};
+        write_packed_shard(base + "/shard_payload.bin", base + "/shard_meta.txt", base + "/shard_loss.bin", shard, d);
+    });
+}
+
+// Reads every file of ref_io_write's set from dir with the reference's
+// readers; returns 0 when all contents equal the given arrays and fields.
+int ref_io_read_check(const char* dir, const uint8_t* volt, const float* w, const float* tw, const int8_t* codes,
+                      const float* params, const uint8_t* loss, uint64_t T, uint64_t F, uint64_t A, uint64_t B,
+                      uint64_t S, uint64_t shard_id, uint64_t ts_start, uint64_t ts_step, uint64_t loss_id) {
+    return guarded([&] {
+        const std::string base(dir);
+        const Dimensions d = dims_of(T, F, A, B);
+        const std::size_t W = integrated_time_count(T, TemporalIntegrationConfig{S});
+        const Dimensions wd = dims_of(W, F, A, B);
+        auto same = [](const void* a, const void* b, std::size_t n, const char* what) {
+            if (std::memcmp(a, b, n) != 0) throw std::runtime_error(std::string("content differs: ") + what);
+        };
+        const auto v = read_packed_voltage(base + "/voltage.bin", d);
+        same(v.data(), volt, v.size(), "voltage");
+        const auto wv = read_weights(base + "/weights.bin", d);
+        same(wv.data(), w, wv.size() * sizeof(ComplexFloat), "weights");
+        const auto tv = read_tiled_weights(base + "/tiled.bin", d);
+        same(tv.data(), tw, tv.size() * sizeof(ComplexFloat), "tiled weights");
+        const auto cv = read_quantized_intensities(base + "/codes.bin", wd);
+        same(cv.data(), codes, cv.size(), "codes");
+        const auto pv = read_quantization_parameters(base + "/params.bin", wd);
+        same(pv.data(), params, pv.size() * sizeof(Int8QuantizationParameters), "parameters");
+        const auto md = read_quantized_output_metadata(base + "/int8_meta.txt");
+        if (md.output_dims.n_time != W || md.input_n_time != T || md.temporal_integration.integration_spectra != S ||
+            md.shard.shard_id != shard_id || md.shard.timestamp_start != ts_start ||
+            md.shard.timestamp_step != ts_step || md.shard.loss_mask_id != loss_id ||
+            md.parameters_file != "params.bin") {
+            throw std::runtime_error("int8 metadata fields differ");
+        }
+        const auto sh = read_packed_shard(base + "/shard_payload.bin", base + "/shard_meta.txt",
+                                          base + "/shard_loss.bin", d);
+        same(sh.payload.data(), volt, sh.payload.size(), "shard payload");
+        same(sh.loss_mask.data(), loss, sh.loss_mask.size(), "shard loss mask");
+        if (sh.descriptor.shard_id != shard_id || sh.descriptor.timestamp_start != ts_start ||
+            sh.descriptor.loss_mask_id != loss_id) {
+            throw std::runtime_error("shard descriptor fields differ");
         }
     });
 }
