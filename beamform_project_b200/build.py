@@ -6,6 +6,7 @@ Products:
     beamform_project_b200/lib/libbf_b200.so   C ABI of include/bf_b200.h + kernels
     beamform_project_b200/lib/libbf_cxx.so    C++ API of include/beamformer/ over the C ABI
     beamform_project_b200/bin/beamformer_cuda command-line beamformer (the reference CLI's options)
+    beamform_project_b200/bin/run_tracker_stream command-line tracker (the reference CLI's options)
 
 The oracle (test infrastructure) is built by oracle/build.py.
 """
@@ -32,7 +33,7 @@ CUDA_SOURCES = ["capi.cu", "grid_exact.cu", "quantize.cu", "generate.cu", "track
 CXX_SOURCES = ["cxx_api.cpp", "io.cpp"]
 CLI = PKG / "cli"
 BIN = PKG / "bin"
-CLI_PROGRAMS = ["beamformer_cuda"]
+CLI_PROGRAMS = ["beamformer_cuda", "run_tracker_stream"]
 
 
 def _nvcc() -> str:

@@ -9,8 +9,10 @@ Products (git-ignored, but shipped to the GPU box with the snapshot):
                                ref_shim.cpp; built only when the checkout is
                                present (it is absent on the GPU box, which uses
                                the prebuilt file).
-    oracle/_ref/beamformer_cpu the reference's CPU command-line beamformer, from
-                               the same sources plus its tools/beamformer_cpu.cpp.
+    oracle/_ref/beamformer_cpu the reference's CPU command-line beamformer and
+    oracle/_ref/run_tracker_stream  tracker (CPU engines), from the same sources
+                               plus its tools/beamformer_cpu.cpp and
+                               tools/run_tracker_stream.cpp.
 
 The reference sources are compiled with g++ straight from where they lie (no
 CMake, nothing copied).  -ffp-contract=off keeps the float32 operation order
@@ -30,9 +32,10 @@ REF_SOURCES = ["cpu_beamformer.cpp", "beam_tracker.cpp", "beam_tracker_opt.cpp",
                "beam_tracker_opt_v2.cpp", "cpu_opt_beam_tracker.cpp", "geometry.cpp",
                "io.cpp", "quantization.cpp", "synthetic_data.cpp", "temporal_integration.cpp",
                "weights.cpp"]
-# the reference's CPU command-line beamformer (tools/), the comparator of the
-# B200 command-line drop-in
-REF_CLI = "beamformer_cpu.cpp"
+# the reference's CPU command-line programs (tools/), the comparators of the
+# B200 command-line drop-ins (the tracker program built without CUDA runs its
+# CPU engines)
+REF_CLIS = ["beamformer_cpu.cpp", "run_tracker_stream.cpp"]
 
 
 def _stale(out: Path, deps: list[Path]) -> bool:
@@ -62,16 +65,21 @@ def build_reference() -> Path | None:
     return out
 
 
-def build_reference_cli() -> Path | None:
-    out = HERE / "_ref" / "beamformer_cpu"
-    srcs = [REF / "src" / s for s in REF_SOURCES] + [REF / "tools" / REF_CLI]
-    if not all(s.exists() for s in srcs):
-        return out if out.exists() else None
-    if _stale(out, srcs):
-        out.parent.mkdir(exist_ok=True)
-        subprocess.run(["g++", "-O3", "-std=c++17", "-fopenmp", "-ffp-contract=off", "-march=x86-64-v2",
-                        "-I", str(REF / "include"), *map(str, srcs), "-o", str(out)], check=True)
-    return out
+def build_reference_cli() -> list[Path]:
+    outs = []
+    for cli in REF_CLIS:
+        out = HERE / "_ref" / Path(cli).stem
+        srcs = [REF / "src" / s for s in REF_SOURCES] + [REF / "tools" / cli]
+        if not all(s.exists() for s in srcs):
+            if out.exists():
+                outs.append(out)
+            continue
+        if _stale(out, srcs):
+            out.parent.mkdir(exist_ok=True)
+            subprocess.run(["g++", "-O3", "-std=c++17", "-fopenmp", "-ffp-contract=off", "-march=x86-64-v2",
+                            "-I", str(REF / "include"), *map(str, srcs), "-o", str(out)], check=True)
+        outs.append(out)
+    return outs
 
 
 if __name__ == "__main__":

@@ -105,3 +105,45 @@ def test_errors_exit_one_with_message(cuda, tmp_path):
     assert r.returncode == 1 and "bytes; expected" in r.stderr
     r = _run(CLI, *_common(paths), "--output", tmp_path / "x", "--kernel", "warp")
     assert r.returncode == 1 and "kernel must be" in r.stderr
+
+
+TRK = ROOT / "beamform_project_b200" / "bin" / "run_tracker_stream"
+REF_TRK = ROOT / "oracle" / "_ref" / "run_tracker_stream"
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("engine,spectra", [("cuda_fws", 320), ("cuda_v5", 10)])
+def test_tracker_cli_within_reference_gpu_tolerance(cuda, ref, tmp_path, engine, spectra):
+    """The tracker drop-in against the reference's CPU engine (cpu_v2), with
+    the tolerance the reference's own GPU tracker tests use (|d| <= 1e-4 or
+    |d| <= 1e-3 |ref|)."""
+    Tt, At = 2048, 64
+    pos = ref.ref_default_positions(At)
+    freq = ref.ref_channelized_frequencies(F)
+    v = ref.ref_make_moving_point_source(Tt, F, At, pos, freq, 0.05, -0.02, 2e-5, 1e-5, 3.0)
+    src = tmp_path / "v.bin"
+    v.tofile(src)
+    args = ["--n-time", Tt, "--n-ant", At, "--spectra", spectra, "--source-l0", 0.05, "--source-m0", -0.02,
+            "--source-dl", 2e-5, "--source-dm", 1e-5, "--input", src]
+    r = _run(REF_TRK, "--engine", "cpu_v2", *args, "--output", tmp_path / "ref.f32")
+    assert r.returncode == 0, r.stderr
+    r = _run(TRK, "--engine", engine, *args, "--output", tmp_path / "b200.f32")
+    assert r.returncode == 0, r.stderr
+    assert f"Successfully ran {engine}" in r.stdout
+    exp = np.fromfile(tmp_path / "ref.f32", np.float32)
+    got = np.fromfile(tmp_path / "b200.f32", np.float32)
+    assert got.size == exp.size == Tt * F
+    d = np.abs(got - exp)
+    assert np.all((d <= 1e-4) | (d <= 1e-3 * exp)), float((d / np.maximum(exp, 1e-30)).max())
+
+
+@pytest.mark.gpu
+def test_tracker_cli_errors(cuda, tmp_path):
+    src = tmp_path / "v.bin"
+    random_voltage(100, F, 32, seed=1).tofile(src)
+    r = _run(TRK, "--engine", "cpu_v2", "--n-time", 100, "--n-ant", 32, "--input", src, "--output", tmp_path / "o")
+    assert r.returncode == 1 and "Unknown engine or CUDA unavailable: cpu_v2" in r.stderr
+    r = _run(TRK, "--n-time", 101, "--n-ant", 32, "--input", src, "--output", tmp_path / "o")
+    assert r.returncode == 1 and "does not match expected" in r.stderr
+    r = _run(TRK, "--n-time", 100)
+    assert r.returncode == 1 and "--input and --output are required" in r.stderr
