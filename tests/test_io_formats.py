@@ -90,3 +90,70 @@ def test_metadata_text(tmp_path):
 
 def test_error_behaviour(tmp_path):
     assert "ERRORS OK" in _run("errors", tmp_path)
+
+
+def _py_write(out: Path, arrays, case):
+    from beamform_project_b200 import io as bio
+    T, F, A, B, S, shard_id, ts_start, ts_step, loss_id = case
+    d = bio.Dimensions(T, F, A, B)
+    W = bio.integrated_time_count(T, S)
+    wd = bio.Dimensions(W, F, A, B)
+    bio.write_packed_voltage(out / "voltage.bin", arrays["voltage"], d)
+    bio.write_weights(out / "weights.bin", arrays["weights"].reshape(-1, 2), d)
+    bio.write_tiled_weights(out / "tiled.bin", arrays["tiled"].reshape(-1, 2), d)
+    bio.write_intensities(out / "intensity.bin", arrays["intensity"], d)
+    bio.write_quantized_intensities(out / "codes.bin", arrays["codes"], wd)
+    bio.write_quantization_parameters(out / "params.bin", arrays["params"], wd)
+    sd = bio.default_shard_descriptor(shard_id)
+    sd.timestamp_start, sd.timestamp_step, sd.loss_mask_id = ts_start, ts_step, loss_id
+    bio.write_quantized_output_metadata(out / "int8_meta.txt",
+                                        bio.QuantizedOutputMetadata(wd, T, S, sd, "params.bin"))
+    bio.write_packed_shard(out / "shard_payload.bin", out / "shard_meta.txt", out / "shard_loss.bin",
+                           bio.PackedShard(sd, arrays["voltage"], arrays["loss"]), d)
+    return d, wd, sd
+
+
+def test_python_io_identical_to_reference_and_reads_it(ref, tmp_path):
+    from beamform_project_b200 import io as bio
+    arrays, case = _case(seed=3)
+    mine, theirs = tmp_path / "py", tmp_path / "ref"
+    mine.mkdir()
+    theirs.mkdir()
+    d, wd, sd = _py_write(mine, arrays, case)
+    ref.ref_io_write(theirs, arrays, case)
+    for name in FILES:
+        assert (mine / name).read_bytes() == (theirs / name).read_bytes(), name
+    ref.ref_io_read_check(mine, arrays, case)
+    assert np.array_equal(bio.read_packed_voltage(theirs / "voltage.bin", d).reshape(-1), arrays["voltage"])
+    w = bio.read_weights(theirs / "weights.bin", d)
+    assert w.dtype == np.complex64 and np.array_equal(w.view(np.float32).reshape(-1), arrays["weights"])
+    assert np.array_equal(bio.read_quantized_intensities(theirs / "codes.bin", wd).reshape(-1), arrays["codes"])
+    assert np.array_equal(bio.read_quantization_parameters(theirs / "params.bin", wd).reshape(-1), arrays["params"])
+    m = bio.read_quantized_output_metadata(theirs / "int8_meta.txt")
+    assert (m.output_dims, m.input_n_time, m.integration_spectra, m.shard, m.parameters_file) == \
+        (wd, case[0], case[4], sd, "params.bin")
+    sh = bio.read_packed_shard(theirs / "shard_payload.bin", theirs / "shard_meta.txt", theirs / "shard_loss.bin", d)
+    assert sh.descriptor == sd and np.array_equal(sh.loss_mask.reshape(-1), arrays["loss"])
+
+
+def test_python_io_errors(tmp_path):
+    from beamform_project_b200 import io as bio
+    d = bio.Dimensions(4, 336, 32, 3)
+    v = np.full(4 * 336 * 32, 0x11, np.uint8)
+    bio.write_packed_voltage(tmp_path / "v.bin", v, d)
+    with pytest.raises(ValueError):
+        bio.write_packed_voltage(tmp_path / "short.bin", v[:10], d)
+    with pytest.raises(ValueError):
+        bio.write_packed_voltage(tmp_path / "bad.bin", v, bio.Dimensions(4, 100, 32, 3))
+    with pytest.raises(RuntimeError, match="43008 bytes; expected 53760"):
+        bio.read_packed_voltage(tmp_path / "v.bin", bio.Dimensions(5, 336, 32, 3))
+    with pytest.raises(RuntimeError):
+        bio.read_weights(tmp_path / "missing.bin", d)
+    (tmp_path / "m.txt").write_text("format=beamformer-quantized-int8-v1\nno separator\n")
+    with pytest.raises(RuntimeError, match="invalid quantized metadata line"):
+        bio.read_quantized_output_metadata(tmp_path / "m.txt")
+    mask = np.ones(4 * 336, np.uint8)
+    mask[3] = 2
+    with pytest.raises(ValueError, match="0 or 1"):
+        bio.write_packed_shard(tmp_path / "p", tmp_path / "q", tmp_path / "r",
+                               bio.PackedShard(bio.default_shard_descriptor(0), v, mask), d)
