@@ -41,7 +41,7 @@ struct Cd {
 //                     parked in the Q slot of the workspace);
 //  doa_forget_kernel  per channel, blocks in order: S = lam S + (1 - lam) R^,
 //                     E = lam E + (1 - lam) eps (first block: S = R^, E = eps);
-//  doa_factor_kernel  cells in parallel: Cholesky L L^H = S + E I (thread 0),
+//  doa_factor_kernel  cells in parallel: Cholesky L L^H = S + E I (one warp),
 //                     column j of L^{-1} by thread j, and Q = L^{-H} L^{-1} =
 //                     (S + E I)^{-1} by elements, so the scan evaluates
 //                     Capon's |L^{-1} a|^2 as the quadratic form a^H Q a.
@@ -115,28 +115,43 @@ __global__ void doa_factor_kernel(const Cd* __restrict S_in, const double* __res
     __shared__ int ok;
     for (int e = threadIdx.x; e < M * M; e += blockDim.x) S[e] = S_in[base + e];
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {
+        // right-looking Cholesky of S + E I by one warp: step j takes the
+        // square root of the updated diagonal, lanes i > j scale column j and
+        // update their own row i of the trailing lower triangle
+        const int lane = threadIdx.x;
         const double E = E_in[cell];
+        for (int e = lane; e < M * M; e += 32) {
+            const int i = e / M, j = e % M;
+            Lc[e] = j <= i ? Cd{S[e].re + (i == j ? E : 0.0), S[e].im} : Cd{0.0, 0.0};
+        }
+        __syncwarp();
         int good = 1;
-        for (int i = 0; i < M && good; ++i) {
-            for (int j = 0; j <= i; ++j) {
-                double sr = S[i * M + j].re + (i == j ? E : 0.0), si = S[i * M + j].im;
-                for (int k = 0; k < j; ++k) {
-                    const Cd x = Lc[i * M + k], y = Lc[j * M + k];  // x * conj(y)
-                    sr -= x.re * y.re + x.im * y.im;
-                    si -= x.im * y.re - x.re * y.im;
-                }
-                if (i == j) {
-                    if (!(sr > 1e-300)) { good = 0; break; }
-                    Lc[i * M + i] = Cd{sqrt(sr), 0.0};
-                } else {
-                    const double d = Lc[j * M + j].re;
-                    Lc[i * M + j] = Cd{sr / d, si / d};
+        for (int j = 0; j < M; ++j) {
+            const double djj = Lc[j * M + j].re;
+            if (!(djj > 1e-300)) { good = 0; break; }
+            const double ljj = sqrt(djj);
+            __syncwarp();
+            if (lane == j) Lc[j * M + j] = Cd{ljj, 0.0};
+            if (lane > j && lane < M) {
+                const Cd x = Lc[lane * M + j];
+                Lc[lane * M + j] = Cd{x.re / ljj, x.im / ljj};
+            }
+            __syncwarp();
+            if (lane > j && lane < M) {
+                const Cd lij = Lc[lane * M + j];
+                for (int k = j + 1; k <= lane; ++k) {
+                    const Cd lkj = Lc[k * M + j];  // row lane -= l_ij * conj(l_kj)
+                    Cd& w = Lc[lane * M + k];
+                    w = Cd{w.re - (lij.re * lkj.re + lij.im * lkj.im), w.im - (lij.im * lkj.re - lij.re * lkj.im)};
                 }
             }
+            __syncwarp();
         }
-        ok = good;
-        ok_out[cell] = good;
+        if (lane == 0) {
+            ok = good;
+            ok_out[cell] = good;
+        }
     }
     __syncthreads();
     if (ok && threadIdx.x < M) {  // column j of L^{-1} by forward substitution
