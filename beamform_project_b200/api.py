@@ -317,6 +317,23 @@ def generate_weights(stream, positions, frequencies, directions, weights, dims: 
     check(native.lib().bf_generate_weights(_stream_handle(stream), pp, ff, dd, w, C.byref(d), int(n_shards)))
 
 
+def apply_loss_mask(stream, packed_voltage, loss_mask, dims: Dimensions, integration_spectra: int,
+                    valid_counts=None) -> None:
+    """Zero every lost frame (loss_mask uint8 [T][F], 0 = lost) of the packed
+    voltage [T][F][A] in place; valid_counts (uint32 [ceil(T/S)][F], or None)
+    gets the valid frames per integration window and channel."""
+    torch = _torch()
+    validate_dimensions(dims)
+    v = _dev(packed_voltage, "packed_voltage", torch.uint8, dims.n_time * dims.n_freq * dims.n_ant)
+    m = _dev(loss_mask, "loss_mask", torch.uint8, dims.n_time * dims.n_freq)
+    c = None
+    if valid_counts is not None:
+        W = -(-dims.n_time // max(int(integration_spectra), 1))
+        c = _dev(valid_counts, "valid_counts", torch.uint32, W * dims.n_freq)
+    d = dims.c()
+    check(native.lib().bf_apply_loss_mask(_stream_handle(stream), v, m, C.byref(d), int(integration_spectra), c))
+
+
 # --------------------------------------------------------------------------
 # synthetic voltages
 # --------------------------------------------------------------------------

@@ -128,6 +128,8 @@ bf_status launch_tracker(cudaStream_t stream, int mode, const uint8_t* v, const 
                          const bf_dims& d, uint64_t spectra);
 bf_status launch_doa_covariance(cudaStream_t stream, const uint8_t* v, int32_t* out, const bf_dims& d,
                                 uint64_t block_len);
+bf_status launch_apply_loss_mask(cudaStream_t stream, uint8_t* v, const uint8_t* mask, uint64_t n_time,
+                                 uint64_t n_freq, uint64_t n_ant, uint64_t spectra, uint32_t* counts);
 uint64_t doa_workspace_bytes(uint64_t n_blocks, uint64_t n_freq, uint64_t M);
 bf_status launch_doa_scan(cudaStream_t stream, const int32_t* R, const float* pos, const double* kw,
                           const bf_dims& d, uint64_t block_len, uint64_t subarray, double lam, double load,

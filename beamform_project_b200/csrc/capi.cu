@@ -339,6 +339,18 @@ BF_API bf_status bf_generate_voltage(void* stream, uint64_t seed, uint64_t sampl
                            epoch_len, out, *dims);
 }
 
+BF_API bf_status bf_apply_loss_mask(void* stream, uint8_t* packed_voltage, const uint8_t* loss_mask,
+                                    const bf_dims* dims, uint64_t integration_spectra, uint32_t* valid_counts) {
+    clear_error();
+    BF_TRY(validate_dims(dims));
+    if (integration_spectra == 0) return set_error(BF_ERR_INVALID_ARGUMENT, "integration_spectra must be positive");
+    if (loss_mask == nullptr) return set_error(BF_ERR_INVALID_ARGUMENT, "loss_mask must not be null");
+    BF_TRY(check_ptr(packed_voltage, 16, "packed_voltage"));
+    if (valid_counts != nullptr) BF_TRY(check_ptr(valid_counts, 4, "valid_counts"));
+    return launch_apply_loss_mask(static_cast<cudaStream_t>(stream), packed_voltage, loss_mask, dims->n_time,
+                                  dims->n_freq, dims->n_ant, integration_spectra, valid_counts);
+}
+
 BF_API bf_status bf_generate_weights(void* stream, const float* positions, const float* frequencies,
                                      const float* directions, float* weights, const bf_dims* dims,
                                      uint64_t n_shards) {

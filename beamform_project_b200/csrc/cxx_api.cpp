@@ -172,6 +172,12 @@ void launch_quantize_integrated_intensity(cudaStream_t stream, const float* inte
                                                   reinterpret_cast<float*>(parameters), &d));
 }
 
+void launch_apply_loss_mask(cudaStream_t stream, std::uint8_t* packed_voltage, const std::uint8_t* loss_mask,
+                            const Dimensions& dims, std::size_t integration_spectra, std::uint32_t* valid_counts) {
+    const bf_dims d = to_c(dims);
+    check(bf_apply_loss_mask(stream, packed_voltage, loss_mask, &d, integration_spectra, valid_counts));
+}
+
 std::size_t split_weight_bytes(const Dimensions& dims) {
     const bf_dims d = to_c(dims);
     return static_cast<std::size_t>(bf_split_weight_bytes(&d, 1));

@@ -114,6 +114,7 @@ _SIGS = {
                               C.c_double, C.c_double, _U64, C.c_double, _P, _P, _P, _P]),
     "bf_generate_voltage": (C.c_int, [_P, _U64, _U64, C.c_float, _P, _U64, _P, C.POINTER(Dims)]),
     "bf_generate_weights": (C.c_int, [_P, _P, _P, _P, _P, C.POINTER(Dims), _U64]),
+    "bf_apply_loss_mask": (C.c_int, [_P, _P, _P, C.POINTER(Dims), _U64, _P]),
     "bf_probe_bounded_wait": (C.c_int, [_P, _U64]),
     "bf_serve_job_bytes": (_U64, [C.POINTER(ServeConfig), C.POINTER(ServeJob)]),
     "bf_serve_create": (C.c_int, [C.POINTER(ServeConfig), _PP]),

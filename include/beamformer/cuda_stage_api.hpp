@@ -47,6 +47,14 @@ void launch_quantize_integrated_intensity(cudaStream_t stream, const float* inte
                                           Int8QuantizationParameters* parameters,
                                           const Dimensions& integrated_dims);
 
+// Loss-mask consumption (the reference defines the mask, formats.hpp:22-30,
+// but no consumer): every byte of a lost frame (loss_mask[t][f] == 0) of the
+// packed voltage becomes 0, in place; valid_counts (uint32
+// [ceil(T / integration_spectra)][F], may be null) gets the valid frames per
+// integration window and channel.  Device pointers, caller's stream.
+void launch_apply_loss_mask(cudaStream_t stream, std::uint8_t* packed_voltage, const std::uint8_t* loss_mask,
+                            const Dimensions& dims, std::size_t integration_spectra, std::uint32_t* valid_counts);
+
 // Bytes of the TensorSplit weight operand for `dims` (one shard).
 std::size_t split_weight_bytes(const Dimensions& dims);
 

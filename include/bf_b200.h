@@ -272,6 +272,17 @@ BF_API bf_status bf_generate_weights(void* stream, const float* positions, const
                                      const float* directions, float* weights, const bf_dims* dims,
                                      uint64_t n_shards);
 
+/* Loss-mask consumption.  The reference defines the per-shard loss mask
+ * (include/beamformer/formats.hpp:22-30: uint8 [T][F], 0 = lost frame) but no
+ * consumer.  In place on the packed voltage [T][F][A] (device, 16-byte
+ * aligned): every byte of a lost frame becomes 0, so the frame adds nothing
+ * to any beam, tracker or covariance.  valid_counts (device uint32
+ * [ceil(T / integration_spectra)][F], may be null) receives the number of
+ * valid frames per integration window and channel.  Nonzero mask bytes count
+ * as valid.  Stream-ordered; allocates nothing. */
+BF_API bf_status bf_apply_loss_mask(void* stream, uint8_t* packed_voltage, const uint8_t* loss_mask,
+                                    const bf_dims* dims, uint64_t integration_spectra, uint32_t* valid_counts);
+
 /* ------------------------------------------------------------------------ */
 /* Served, continuously batched mode (no reference counterpart)             */
 /* ------------------------------------------------------------------------ */
