@@ -939,6 +939,21 @@ ServedResult ServedBeamformer::result(std::uint64_t job_id) {
 
 void ServedBeamformer::cancel(std::uint64_t job_id) { check(bf_serve_cancel(server_, job_id)); }
 void ServedBeamformer::release(std::uint64_t job_id) { check(bf_serve_release(server_, job_id)); }
+
+std::vector<std::uint8_t> ServedBeamformer::checkpoint(std::uint64_t job_id) {
+    std::uint64_t n = 0;
+    check(bf_serve_checkpoint(server_, job_id, nullptr, 0, &n));
+    std::vector<std::uint8_t> image(n);
+    check(bf_serve_checkpoint(server_, job_id, image.data(), n, &n));
+    image.resize(n);
+    return image;
+}
+
+std::uint64_t ServedBeamformer::restore(const std::vector<std::uint8_t>& image) {
+    std::uint64_t id = 0;
+    check(bf_serve_restore(server_, image.data(), image.size(), &id));
+    return id;
+}
 void ServedBeamformer::synchronize() { check(bf_serve_sync(server_)); }
 
 ServedStats ServedBeamformer::stats() {

@@ -134,6 +134,10 @@ struct Job {
     uint64_t n_windows = 0;     // output windows
     ClassKey cls{};
     uint8_t* base = nullptr;    // arena block
+    // restored from a checkpoint: windows already served and their results
+    // (the prefixes of result_regions), uploaded at admission
+    uint64_t resume_step = 0;
+    std::vector<uint8_t> resume_results;
 };
 
 }  // namespace
@@ -223,6 +227,31 @@ JobLayout layout_of(const bf_serve_config& c, const bf_serve_job& j) {
     }
     L.total = o;
     return L;
+}
+
+// (offset in the job's block, bytes) of the results of the first `steps`
+// served windows: per shard a prefix of integrated (and of codes and
+// parameters) for grid jobs, one prefix of integrated for trackers.
+std::vector<std::pair<uint64_t, uint64_t>> result_regions(const bf_serve_config& c, const bf_serve_job& j,
+                                                          const JobLayout& L, uint64_t steps) {
+    std::vector<std::pair<uint64_t, uint64_t>> r;
+    const uint64_t F = c.shard_channels, ns = j.n_shards, B = j.n_beams;
+    const uint64_t W = j.n_spectra / j.integration_spectra;
+    const uint64_t wd = steps * (c.window_spectra / j.integration_spectra);
+    if (wd == 0) return r;
+    if (j.kind == BF_SERVE_GRID) {
+        const uint64_t pt = ((F + 15) / 16) * ((B + 15) / 16) * 2 * sizeof(float);
+        for (uint64_t sh = 0; sh < ns; ++sh) {
+            r.emplace_back(L.integrated + sh * W * F * B * sizeof(float), wd * F * B * sizeof(float));
+            if (j.quantize) {
+                r.emplace_back(L.codes + sh * W * F * B, wd * F * B);
+                r.emplace_back(L.params + sh * W * pt, wd * pt);
+            }
+        }
+    } else {
+        r.emplace_back(L.integrated, wd * ns * F * B * sizeof(float));
+    }
+    return r;
 }
 
 bf_status validate_job(const bf_serve_config& c, const bf_serve_job* j) {
@@ -479,9 +508,17 @@ bf_status admit(bf_server* s) {
         j.has_block = true;
         j.base = reinterpret_cast<uint8_t*>(reinterpret_cast<uintptr_t>(s->slab) + off);
         j.state = BF_JOB_LIVE;
-        j.next_step = 0;
+        j.next_step = j.resume_step;
         ++s->admitted;
         s->live.push_back(j.id);
+        if (j.resume_step == j.n_steps) {
+            // a restored job with every window served: its results are
+            // uploaded now and it is done
+            s->live.pop_back();
+            j.state = BF_JOB_DONE;
+            ++s->done;
+            s->completions.push_back(j.id);
+        }
         if (s->host_only) continue;
         const cudaStream_t st = s->stream;
         const uint64_t A = j.spec.n_ant, F = s->cfg.shard_channels, ns = j.spec.n_shards, B = j.spec.n_beams;
@@ -502,6 +539,16 @@ bf_status admit(bf_server* s) {
         } else {
             BF_RETURN_IF(up(j.lay.kw, j.kw.data(), j.kw.size() * sizeof(double)));
             BF_RETURN_IF(up(j.lay.traj, j.traj.data(), j.traj.size() * sizeof(float)));
+        }
+        if (j.resume_step > 0) {
+            uint64_t at = 0;
+            for (const auto& reg : result_regions(s->cfg, j.spec, j.lay, j.resume_step)) {
+                BF_RETURN_IF(up(reg.first, j.resume_results.data() + at, reg.second));
+                at += reg.second;
+            }
+            if (j.state == BF_JOB_DONE) {
+                BF_RETURN_IF(cuda_status(cudaStreamSynchronize(st), "restored results upload"));
+            }
         }
     }
     return BF_OK;
@@ -778,6 +825,181 @@ bf_status create(const bf_serve_config* cfg, bool host_only, bf_server** out) {
 }  // namespace
 }  // namespace bf
 
+namespace bf {
+namespace {
+
+// A validated job (host inputs copied), not yet queued.
+bf_status make_job(bf_server* s, const bf_serve_job* job, Job* out) {
+    BF_RETURN_IF(validate_job(s->cfg, job));
+    Job& j = *out;
+    j.spec = *job;
+    j.lay = layout_of(s->cfg, *job);
+    if (j.lay.total > s->cfg.hbm_budget_bytes) {
+        ++s->rejected;
+        return set_error(BF_ERR_RESOURCE, "the job's device state exceeds the server's HBM budget");
+    }
+    const uint64_t F = static_cast<uint64_t>(job->n_shards) * s->cfg.shard_channels;
+    j.pos.assign(job->positions, job->positions + 3 * job->n_ant);
+    j.freq.assign(job->frequencies, job->frequencies + F);
+    if (job->kind == BF_SERVE_GRID) {
+        j.dirs.assign(job->directions, job->directions + 3 * job->n_beams);
+        j.cls = ClassKey{kGridClass, static_cast<int>(job->n_ant), served_nb_pad(job->n_beams),
+                         small_window_rows(static_cast<int>(job->integration_spectra)),
+                         job->integration_spectra < 32 ? 1 : 0};
+    } else {
+        j.traj.assign(job->trajectories, job->trajectories + 4 * job->n_beams);
+        j.kw.resize(F);
+        for (uint64_t f = 0; f < F; ++f) j.kw[f] = kTwoPi * static_cast<double>(j.freq[f]) / kSpeedOfLight;
+        j.cls = ClassKey{kTrackerClass, static_cast<int>(job->n_ant), 0, 0, job->integration_spectra <= 16 ? 1 : 0};
+    }
+    j.spec.positions = j.spec.frequencies = j.spec.directions = j.spec.trajectories = nullptr;
+    j.n_steps = job->n_spectra / s->cfg.window_spectra;
+    j.n_windows = job->n_spectra / job->integration_spectra;
+    return BF_OK;
+}
+
+// ---- job checkpoints ----
+// Image (little-endian, no padding): "BFSRVCK1", version, the job's scalar
+// fields, the windows served, the server settings its voltages depend on
+// (window, shard channels, max shards, pool rows, seed and scale), the job's
+// host arrays (positions, frequencies, directions or trajectories), the
+// results of the served windows (the prefixes of result_regions, in order),
+// and an FNV-1a 64 checksum of everything before it.
+constexpr char kImageMagic[8] = {'B', 'F', 'S', 'R', 'V', 'C', 'K', '1'};
+constexpr uint32_t kImageVersion = 1;
+
+uint64_t fnv1a(const uint8_t* p, uint64_t n) {
+    uint64_t h = 14695981039346656037ull;
+    for (uint64_t i = 0; i < n; ++i) h = (h ^ p[i]) * 1099511628211ull;
+    return h;
+}
+
+struct ImageHead {
+    uint32_t kind, n_ant, n_shards, n_beams, quantize;
+    uint64_t n_spectra, spectra, pool_offset, steps_done;
+    uint32_t window_spectra, shard_channels, max_shards, pool_scale_bits;
+    uint64_t pool_spectra, pool_seed;
+};
+
+class ImageOut {
+public:
+    explicit ImageOut(std::vector<uint8_t>* b) : b_(b) {}
+    template <typename T>
+    void put(const T& v) { raw(&v, sizeof(T)); }
+    void raw(const void* p, size_t n) {
+        const auto* c = static_cast<const uint8_t*>(p);
+        b_->insert(b_->end(), c, c + n);
+    }
+
+private:
+    std::vector<uint8_t>* b_;
+};
+
+class ImageIn {
+public:
+    ImageIn(const uint8_t* p, uint64_t n) : p_(p), n_(n) {}
+    template <typename T>
+    bool get(T* v) { return raw(v, sizeof(T)); }
+    bool raw(void* dst, uint64_t n) {
+        if (n > n_ - at_) return false;
+        std::memcpy(dst, p_ + at_, n);
+        at_ += n;
+        return true;
+    }
+    uint64_t left() const { return n_ - at_; }
+
+private:
+    const uint8_t* p_;
+    uint64_t n_, at_ = 0;
+};
+
+void put_head(ImageOut& o, const ImageHead& h) {
+    o.raw(kImageMagic, sizeof(kImageMagic));
+    o.put(kImageVersion);
+    o.put(h.kind); o.put(h.n_ant); o.put(h.n_shards); o.put(h.n_beams); o.put(h.quantize);
+    o.put(h.n_spectra); o.put(h.spectra); o.put(h.pool_offset); o.put(h.steps_done);
+    o.put(h.window_spectra); o.put(h.shard_channels); o.put(h.max_shards); o.put(h.pool_scale_bits);
+    o.put(h.pool_spectra); o.put(h.pool_seed);
+}
+
+bool get_head(ImageIn& in, ImageHead* h) {
+    char magic[8];
+    uint32_t version = 0;
+    if (!in.raw(magic, sizeof(magic)) || std::memcmp(magic, kImageMagic, sizeof(magic)) != 0) return false;
+    if (!in.get(&version) || version != kImageVersion) return false;
+    return in.get(&h->kind) && in.get(&h->n_ant) && in.get(&h->n_shards) && in.get(&h->n_beams) &&
+           in.get(&h->quantize) && in.get(&h->n_spectra) && in.get(&h->spectra) && in.get(&h->pool_offset) &&
+           in.get(&h->steps_done) && in.get(&h->window_spectra) && in.get(&h->shard_channels) &&
+           in.get(&h->max_shards) && in.get(&h->pool_scale_bits) && in.get(&h->pool_spectra) &&
+           in.get(&h->pool_seed);
+}
+
+uint32_t float_bits(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, sizeof(u));
+    return u;
+}
+
+uint64_t regions_bytes(const std::vector<std::pair<uint64_t, uint64_t>>& r) {
+    uint64_t n = 0;
+    for (const auto& x : r) n += x.second;
+    return n;
+}
+
+// windows whose results a checkpoint of j carries
+uint64_t served_steps(const Job& j) {
+    return j.state == BF_JOB_QUEUED ? j.resume_step : j.next_step;
+}
+
+bf_status build_image(bf_server* s, const Job& j, std::vector<uint8_t>* img) {
+    const bf_serve_config& c = s->cfg;
+    const uint64_t done = served_steps(j);
+    ImageHead h{static_cast<uint32_t>(j.spec.kind), j.spec.n_ant, j.spec.n_shards, j.spec.n_beams,
+                static_cast<uint32_t>(j.spec.quantize != 0), j.spec.n_spectra, j.spec.integration_spectra,
+                j.spec.pool_offset, done, c.window_spectra, c.shard_channels, c.max_shards,
+                float_bits(c.pool_scale), c.pool_spectra, c.pool_seed};
+    ImageOut o(img);
+    put_head(o, h);
+    o.raw(j.pos.data(), j.pos.size() * sizeof(float));
+    o.raw(j.freq.data(), j.freq.size() * sizeof(float));
+    if (j.spec.kind == BF_SERVE_GRID) o.raw(j.dirs.data(), j.dirs.size() * sizeof(float));
+    else o.raw(j.traj.data(), j.traj.size() * sizeof(float));
+    const auto regions = result_regions(c, j.spec, j.lay, done);
+    const uint64_t at = img->size();
+    img->resize(at + regions_bytes(regions));
+    if (j.state == BF_JOB_QUEUED) {
+        if (!j.resume_results.empty()) std::memcpy(img->data() + at, j.resume_results.data(), j.resume_results.size());
+    } else if (!s->host_only) {
+        uint64_t o2 = at;
+        for (const auto& r : regions) {
+            BF_RETURN_IF(cuda_status(cudaMemcpy(img->data() + o2, j.base + r.first, r.second, cudaMemcpyDeviceToHost),
+                                     "checkpoint results copy"));
+            o2 += r.second;
+        }
+    }
+    const uint64_t sum = fnv1a(img->data(), img->size());
+    ImageOut(img).put(sum);
+    return BF_OK;
+}
+
+uint64_t image_bytes(const bf_serve_config& c, const Job& j) {
+    const uint64_t arrays = j.pos.size() + j.freq.size() + (j.spec.kind == BF_SERVE_GRID ? j.dirs.size() : j.traj.size());
+    const uint64_t head = sizeof(kImageMagic) + sizeof(uint32_t) * 10 + sizeof(uint64_t) * 6;
+    return head + arrays * sizeof(float) + regions_bytes(result_regions(c, j.spec, j.lay, served_steps(j))) +
+           sizeof(uint64_t);
+}
+
+void enqueue(bf_server* s, Job&& j, uint64_t* job_id) {
+    j.id = s->next_id++;
+    if (job_id) *job_id = j.id;
+    s->queue.push_back(j.id);
+    s->jobs.emplace(j.id, std::move(j));
+    ++s->submitted;
+}
+
+}  // namespace
+}  // namespace bf
+
 extern "C" {
 
 BF_API uint64_t bf_serve_job_bytes(const bf_serve_config* config, const bf_serve_job* job) {
@@ -829,36 +1051,9 @@ BF_API bf_status bf_serve_destroy(bf_server* server) {
 static bf_status bf_serve_submit_impl(bf_server* s, const bf_serve_job* job, uint64_t* job_id) {
     clear_error();
     if (s == nullptr) return set_error(BF_ERR_INVALID_ARGUMENT, "server must not be null");
-    BF_RETURN_IF(validate_job(s->cfg, job));
     Job j;
-    j.id = s->next_id++;
-    j.spec = *job;
-    j.lay = layout_of(s->cfg, *job);
-    if (j.lay.total > s->cfg.hbm_budget_bytes) {
-        ++s->rejected;
-        return set_error(BF_ERR_RESOURCE, "the job's device state exceeds the server's HBM budget");
-    }
-    const uint64_t F = static_cast<uint64_t>(job->n_shards) * s->cfg.shard_channels;
-    j.pos.assign(job->positions, job->positions + 3 * job->n_ant);
-    j.freq.assign(job->frequencies, job->frequencies + F);
-    if (job->kind == BF_SERVE_GRID) {
-        j.dirs.assign(job->directions, job->directions + 3 * job->n_beams);
-        j.cls = ClassKey{kGridClass, static_cast<int>(job->n_ant), served_nb_pad(job->n_beams),
-                         small_window_rows(static_cast<int>(job->integration_spectra)),
-                         job->integration_spectra < 32 ? 1 : 0};
-    } else {
-        j.traj.assign(job->trajectories, job->trajectories + 4 * job->n_beams);
-        j.kw.resize(F);
-        for (uint64_t f = 0; f < F; ++f) j.kw[f] = kTwoPi * static_cast<double>(j.freq[f]) / kSpeedOfLight;
-        j.cls = ClassKey{kTrackerClass, static_cast<int>(job->n_ant), 0, 0, job->integration_spectra <= 16 ? 1 : 0};
-    }
-    j.spec.positions = j.spec.frequencies = j.spec.directions = j.spec.trajectories = nullptr;
-    j.n_steps = job->n_spectra / s->cfg.window_spectra;
-    j.n_windows = job->n_spectra / job->integration_spectra;
-    if (job_id) *job_id = j.id;
-    s->queue.push_back(j.id);
-    s->jobs.emplace(j.id, std::move(j));
-    ++s->submitted;
+    BF_RETURN_IF(make_job(s, job, &j));
+    enqueue(s, std::move(j), job_id);
     return BF_OK;
 }
 
@@ -1106,5 +1301,109 @@ BF_API bf_status bf_serve_take_done(bf_server* s, uint64_t* ids, uint64_t capaci
 }
 
 BF_API void* bf_serve_stream(bf_server* s) { return s == nullptr ? nullptr : static_cast<void*>(s->stream); }
+
+static bf_status bf_serve_checkpoint_impl(bf_server* s, uint64_t job_id, void* buffer, uint64_t capacity,
+                                          uint64_t* bytes) {
+    clear_error();
+    if (s == nullptr) return set_error(BF_ERR_INVALID_ARGUMENT, "server must not be null");
+    poll_steps(s, false);
+    update_done(s);
+    auto it = s->jobs.find(job_id);
+    if (it == s->jobs.end()) return set_error(BF_ERR_OUT_OF_RANGE, "unknown job id");
+    const Job& j = it->second;
+    if (j.state == BF_JOB_CANCELLED) return set_error(BF_ERR_LOGIC, "a cancelled job has no checkpoint");
+    const uint64_t n = image_bytes(s->cfg, j);
+    if (bytes) *bytes = n;
+    if (buffer == nullptr) return BF_OK;
+    if (capacity < n) return set_error(BF_ERR_INVALID_ARGUMENT, "checkpoint buffer is smaller than the image");
+    if (j.state != BF_JOB_QUEUED && !s->host_only) {
+        // the windows already launched for this job complete first
+        poll_steps(s, true);
+        BF_RETURN_IF(cuda_status(cudaStreamSynchronize(s->stream), "checkpoint wait"));
+    }
+    std::vector<uint8_t> img;
+    img.reserve(n);
+    BF_RETURN_IF(build_image(s, j, &img));
+    if (img.size() != n) return set_error(BF_ERR_LOGIC, "internal error: checkpoint size");
+    std::memcpy(buffer, img.data(), n);
+    return BF_OK;
+}
+
+BF_API bf_status bf_serve_checkpoint(bf_server* s, uint64_t job_id, void* buffer, uint64_t capacity,
+                                     uint64_t* bytes) {
+    try {
+        return bf_serve_checkpoint_impl(s, job_id, buffer, capacity, bytes);
+    } catch (const std::bad_alloc&) {
+        return set_error(BF_ERR_RESOURCE, "host memory exhausted");
+    } catch (const std::exception& e) {
+        return set_error(BF_ERR_LOGIC, std::string("internal error: ") + e.what());
+    }
+}
+
+static bf_status bf_serve_restore_impl(bf_server* s, const void* image, uint64_t bytes, uint64_t* job_id) {
+    clear_error();
+    if (s == nullptr) return set_error(BF_ERR_INVALID_ARGUMENT, "server must not be null");
+    if (image == nullptr || bytes < sizeof(uint64_t)) return set_error(BF_ERR_INVALID_ARGUMENT, "no checkpoint image");
+    const auto* p = static_cast<const uint8_t*>(image);
+    uint64_t sum = 0;
+    std::memcpy(&sum, p + bytes - sizeof(uint64_t), sizeof(uint64_t));
+    if (fnv1a(p, bytes - sizeof(uint64_t)) != sum) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "checkpoint image is damaged (checksum)");
+    }
+    ImageIn in(p, bytes - sizeof(uint64_t));
+    ImageHead h{};
+    if (!get_head(in, &h)) return set_error(BF_ERR_INVALID_ARGUMENT, "not a served-job checkpoint image");
+    const bf_serve_config& c = s->cfg;
+    if (h.window_spectra != c.window_spectra || h.shard_channels != c.shard_channels ||
+        h.max_shards != c.max_shards || h.pool_scale_bits != float_bits(c.pool_scale) ||
+        h.pool_spectra != c.pool_spectra || h.pool_seed != c.pool_seed) {
+        return set_error(BF_ERR_INVALID_ARGUMENT,
+                         "the checkpoint comes from a server with other window, shard or pool settings");
+    }
+    if (h.n_ant > 1024 || h.n_shards > 64 || h.n_beams > 1024) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "checkpoint job fields are out of range");
+    }
+    std::vector<float> pos(3ull * h.n_ant), freq(static_cast<uint64_t>(h.n_shards) * c.shard_channels);
+    std::vector<float> extra((h.kind == BF_SERVE_GRID ? 3ull : 4ull) * h.n_beams);
+    if (!in.raw(pos.data(), pos.size() * sizeof(float)) || !in.raw(freq.data(), freq.size() * sizeof(float)) ||
+        !in.raw(extra.data(), extra.size() * sizeof(float))) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "checkpoint image is truncated");
+    }
+    bf_serve_job job{};
+    job.kind = static_cast<int32_t>(h.kind);
+    job.n_ant = h.n_ant;
+    job.n_shards = h.n_shards;
+    job.n_beams = h.n_beams;
+    job.n_spectra = h.n_spectra;
+    job.integration_spectra = h.spectra;
+    job.pool_offset = h.pool_offset;
+    job.positions = pos.data();
+    job.frequencies = freq.data();
+    job.directions = h.kind == BF_SERVE_GRID ? extra.data() : nullptr;
+    job.trajectories = h.kind == BF_SERVE_GRID ? nullptr : extra.data();
+    job.quantize = static_cast<int32_t>(h.quantize);
+    Job j;
+    BF_RETURN_IF(make_job(s, &job, &j));
+    if (h.steps_done > j.n_steps) return set_error(BF_ERR_INVALID_ARGUMENT, "checkpoint has more windows than the job");
+    const uint64_t rb = regions_bytes(result_regions(c, j.spec, j.lay, h.steps_done));
+    if (in.left() != rb) return set_error(BF_ERR_INVALID_ARGUMENT, "checkpoint results do not match the job");
+    j.resume_step = h.steps_done;
+    j.resume_results.resize(rb);
+    if (rb > 0 && !in.raw(j.resume_results.data(), rb)) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "checkpoint image is truncated");
+    }
+    enqueue(s, std::move(j), job_id);
+    return BF_OK;
+}
+
+BF_API bf_status bf_serve_restore(bf_server* s, const void* image, uint64_t bytes, uint64_t* job_id) {
+    try {
+        return bf_serve_restore_impl(s, image, bytes, job_id);
+    } catch (const std::bad_alloc&) {
+        return set_error(BF_ERR_RESOURCE, "host memory exhausted");
+    } catch (const std::exception& e) {
+        return set_error(BF_ERR_LOGIC, std::string("internal error: ") + e.what());
+    }
+}
 
 }  // extern "C"

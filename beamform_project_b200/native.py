@@ -125,6 +125,8 @@ _SIGS = {
     "bf_serve_poll": (C.c_int, [_P, _U64, C.POINTER(C.c_int32)]),
     "bf_serve_result": (C.c_int, [_P, _U64, _PP, _PP, _PP, C.POINTER(C.c_uint64)]),
     "bf_serve_cancel": (C.c_int, [_P, _U64]),
+    "bf_serve_checkpoint": (C.c_int, [_P, _U64, _P, _U64, C.POINTER(C.c_uint64)]),
+    "bf_serve_restore": (C.c_int, [_P, _P, _U64, C.POINTER(C.c_uint64)]),
     "bf_serve_release": (C.c_int, [_P, _U64]),
     "bf_serve_sync": (C.c_int, [_P]),
     "bf_serve_stats_get": (C.c_int, [_P, C.POINTER(ServeStats)]),

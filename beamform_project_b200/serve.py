@@ -123,6 +123,24 @@ class Server:
     def cancel(self, job_id: int) -> None:
         native.check(native.lib().bf_serve_cancel(self._h, int(job_id)))
 
+    def checkpoint(self, job_id: int) -> bytes:
+        """Self-contained image of a job (description, windows served, their
+        results); waits for the job's launched windows.  See restore()."""
+        n = C.c_uint64(0)
+        native.check(native.lib().bf_serve_checkpoint(self._h, int(job_id), None, 0, C.byref(n)))
+        buf = C.create_string_buffer(n.value)
+        native.check(native.lib().bf_serve_checkpoint(self._h, int(job_id), buf, n.value, C.byref(n)))
+        return buf.raw[: n.value]
+
+    def restore(self, image: bytes) -> int:
+        """Queue the job of a checkpoint image (from a server with the same
+        window, shard and pool settings); it resumes at its next window."""
+        jid = C.c_uint64(0)
+        buf = C.create_string_buffer(bytes(image), len(image))
+        native.check(native.lib().bf_serve_restore(self._h, buf, len(image), C.byref(jid)))
+        self.specs[jid.value] = spec_of_checkpoint(image)
+        return jid.value
+
     def release(self, job_id: int) -> None:
         native.check(native.lib().bf_serve_release(self._h, int(job_id)))
         self.specs.pop(int(job_id), None)
@@ -216,6 +234,34 @@ def array_positions(n_ant: int) -> np.ndarray:
 def band_frequencies(n_channels: int) -> np.ndarray:
     """n_channels over 400-800 MHz, end points included."""
     return (400e6 + np.arange(n_channels) * (400e6 / max(1, n_channels - 1))).astype(np.float32)
+
+
+def spec_of_checkpoint(image: bytes) -> JobSpec:
+    """The job description carried by a checkpoint image (bf_serve_checkpoint):
+    "BFSRVCK1", u32 version, u32 kind, n_ant, n_shards, n_beams, quantize,
+    u64 n_spectra, integration_spectra, pool_offset, windows served, u32
+    window_spectra, shard_channels, max_shards, pool-scale bits, u64
+    pool_spectra, pool_seed, then float32 positions, frequencies and
+    directions (grid) or trajectories (tracker)."""
+    b = bytes(image)
+    if b[:8] != b"BFSRVCK1":
+        raise ValueError("not a served-job checkpoint image")
+    u32 = np.frombuffer(b, np.uint32, 6, 8)
+    _, kind, A, ns, B, quant = (int(x) for x in u32)
+    u64 = np.frombuffer(b, np.uint64, 4, 32)
+    n_spectra, S, pool_offset = int(u64[0]), int(u64[1]), int(u64[2])
+    shard_ch = int(np.frombuffer(b, np.uint32, 1, 68)[0])
+    at = 96
+    pos = np.frombuffer(b, np.float32, 3 * A, at).reshape(A, 3).copy()
+    at += 12 * A
+    freq = np.frombuffer(b, np.float32, ns * shard_ch, at).copy()
+    at += 4 * ns * shard_ch
+    if kind == GRID:
+        dirs = np.frombuffer(b, np.float32, 3 * B, at).reshape(B, 3).copy()
+        return JobSpec(GRID, A, ns, B, n_spectra, S, pos, freq, directions=dirs, pool_offset=pool_offset,
+                       quantize=bool(quant))
+    traj = np.frombuffer(b, np.float32, 4 * B, at).reshape(B, 4).copy()
+    return JobSpec(TRACKER, A, ns, B, n_spectra, S, pos, freq, trajectories=traj, pool_offset=pool_offset)
 
 
 def poisson_mix(seed: int = 1, rate_hz: float = 200.0, duration_s: float = 10.0, window_spectra: int = 320,

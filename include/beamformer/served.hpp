@@ -79,6 +79,12 @@ public:
     ServedResult result(std::uint64_t job_id);
     void cancel(std::uint64_t job_id);
     void release(std::uint64_t job_id);
+    // Self-contained image of a job (description, windows served, their
+    // results); waits for the job's launched windows.  restore() queues it in
+    // a server with the same window, shard and pool settings, where it
+    // resumes at its next window with results equal to an uninterrupted run.
+    std::vector<std::uint8_t> checkpoint(std::uint64_t job_id);
+    std::uint64_t restore(const std::vector<std::uint8_t>& image);
     void synchronize();
     ServedStats stats();
     std::vector<float> window_times_ms();

@@ -381,6 +381,19 @@ BF_API bf_status bf_serve_poll(bf_server* server, uint64_t job_id, int32_t* stat
 BF_API bf_status bf_serve_result(bf_server* server, uint64_t job_id, float** integrated, int8_t** codes,
                                  float** params, uint64_t* n_windows);
 BF_API bf_status bf_serve_cancel(bf_server* server, uint64_t job_id);
+/* Job checkpoints (no reference counterpart).  bf_serve_checkpoint writes a
+ * self-contained image of a queued, live, running or done job -- its
+ * description, the windows served so far and their results -- into buffer
+ * (host, capacity bytes); with buffer NULL it only sets *bytes.  For a job
+ * with windows in flight it first waits for the server's launched windows.
+ * bf_serve_restore queues the job of an image in a server with the same
+ * window, shard and pool settings (BF_ERR_INVALID_ARGUMENT otherwise, or for
+ * a damaged image); it resumes at its next window and its results equal
+ * those of an uninterrupted run bit for bit.  The original job is not
+ * touched: cancel and release it as usual. */
+BF_API bf_status bf_serve_checkpoint(bf_server* server, uint64_t job_id, void* buffer, uint64_t capacity,
+                                     uint64_t* bytes);
+BF_API bf_status bf_serve_restore(bf_server* server, const void* image, uint64_t bytes, uint64_t* job_id);
 /* Returns the job's arena block (waits for the GPU if it may still use it). */
 BF_API bf_status bf_serve_release(bf_server* server, uint64_t job_id);
 /* Waits for every launched step; BF_ERR_TIMEOUT if a kernel reported a

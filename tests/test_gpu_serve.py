@@ -198,3 +198,46 @@ def test_admission_waits_for_memory_on_the_device(cuda):
         assert srv.stats()["arena_bytes_peak"] <= int(1.5 * need)
     for k, jid in enumerate(sorted(got)):
         assert np.array_equal(got[jid], alone[k])
+
+
+def test_checkpoint_restore_equals_uninterrupted(cuda):
+    """Jobs checkpointed after two windows, their server destroyed, and
+    restored into a new server finish with results bit-identical to an
+    uninterrupted run (grid S = 10 and 320 with int8 codes, tracker S = 10);
+    a job checkpointed before admission and one checkpointed when done
+    restore too."""
+    specs = [_grid_job(A=64, ns=2, B=40, S=10, n_spectra=320 * 5, offset=320 * 2, seed=3),
+             _grid_job(A=32, ns=1, B=128, S=320, n_spectra=320 * 4, offset=320 * 6, seed=4),
+             _tracker_job(A=64, ns=2, n_src=9, S=10, n_spectra=320 * 4, offset=320 * 11)]
+    with _server() as srv:
+        straight = _run(srv, specs)
+    with _server() as a:
+        ids = [a.submit(s) for s in specs]
+        a.step()
+        a.step()
+        images = [a.checkpoint(i) for i in ids]
+        queued = a.checkpoint(a.submit(specs[0]))        # not admitted yet: no windows served
+        a.sync()
+    with _server() as b:
+        rids = [b.restore(img) for img in images]
+        qid = b.restore(queued)
+        for _ in range(10_000):
+            if b.step() == 0:
+                break
+        b.sync()
+        assert native.take_device_error() == 0
+        resumed = [b.result(i) for i in rids]
+        fresh = b.result(qid)
+        done_image = b.checkpoint(rids[0])               # every window served
+    with _server() as c:
+        did = c.restore(done_image)
+        c.step()
+        c.sync()
+        redone = c.result(did)
+    for x, y in zip(straight, resumed):
+        for u, v in zip(x, y):
+            assert (u is None and v is None) or np.array_equal(u, v)
+    for u, v in zip(straight[0], fresh):
+        assert (u is None and v is None) or np.array_equal(u, v)
+    for u, v in zip(straight[0], redone):
+        assert (u is None and v is None) or np.array_equal(u, v)

@@ -220,3 +220,49 @@ def test_zero_lengths_are_rejected_not_divided_by():
         assert native.lib().bf_serve_job_bytes(C.byref(cfg), C.byref(job)) == 0
     with pytest.raises(native.InvalidArgument):
         serve.Server(10**9, window_spectra=0, host_only=True)
+
+
+def test_checkpoint_restore_resumes_where_it_stopped():
+    """A live job's checkpoint, restored into a second server, runs only its
+    remaining windows; a queued job's checkpoint carries its description."""
+    with serve.Server(10**9, host_only=True) as a, serve.Server(10**9, host_only=True) as b:
+        g = _grid(n_spectra=320 * 5, S=10, B=40, ns=2, offset=640)
+        t = _tracker(n_spectra=320 * 4, S=10, n_src=5)
+        jg, jt = a.submit(g), a.submit(t)
+        a.step()
+        a.step()
+        img_g, img_t = a.checkpoint(jg), a.checkpoint(jt)
+        spec = serve.spec_of_checkpoint(img_g)
+        assert (spec.kind, spec.n_ant, spec.n_shards, spec.n_beams, spec.n_spectra, spec.integration_spectra,
+                spec.pool_offset, spec.quantize) == (serve.GRID, 64, 2, 40, 1600, 10, 640, True)
+        assert np.array_equal(spec.positions, g.positions) and np.array_equal(spec.directions, g.directions)
+        assert np.array_equal(serve.spec_of_checkpoint(img_t).trajectories, t.trajectories)
+        rg, rt = b.restore(img_g), b.restore(img_t)
+        assert b.poll(rg) == serve.QUEUED
+        steps = 0
+        while b.poll(rg) != serve.DONE or b.poll(rt) != serve.DONE:
+            b.step()
+            steps += 1
+        assert steps == 3        # 5 - 2 windows of the grid job (the tracker had 2 left)
+        # a queued job round-trips through a checkpoint unchanged
+        q = b.submit(_grid(n_spectra=640))
+        again = b.restore(b.checkpoint(q))
+        assert b.checkpoint(again)[:-8] == b.checkpoint(q)[:-8]
+
+
+def test_checkpoint_errors():
+    with serve.Server(10**9, host_only=True) as a:
+        j = a.submit(_grid())
+        img = bytearray(a.checkpoint(j))
+        img[100] ^= 0x40
+        with pytest.raises(native.InvalidArgument, match="checksum"):
+            a.restore(bytes(img))
+        with pytest.raises(native.InvalidArgument):
+            a.restore(b"not an image at all")
+        a.cancel(j)
+        with pytest.raises(native.LogicError):
+            a.checkpoint(j)
+        good = a.checkpoint(a.submit(_grid()))
+    with serve.Server(10**9, host_only=True, pool_spectra=10240) as other:
+        with pytest.raises(native.InvalidArgument, match="pool settings"):
+            other.restore(good)
