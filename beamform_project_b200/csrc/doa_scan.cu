@@ -24,6 +24,7 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <cmath>
 
 namespace bf {
 namespace {
@@ -203,6 +204,97 @@ constexpr int kMaxSplit = 8;
 template <int M>
 __host__ __device__ constexpr int scan_blocks() { return M <= 13 ? 4 : 2; }
 
+// Uniform sub-array form.  With p_m = p_0 + m D + e_m (D = (p_{M-1} - p_0) /
+// (M - 1), e_m the residuals of the float positions) and psi = k D.d,
+//   conj(a_r) a_c = exp(-i (c - r) psi) exp(i k (e_r - e_c).d)
+// and to first order in theta = k (e_r - e_c).d each Hermitian quadratic
+// form is
+//   a^H X a = T_0 + 2 Re sum_{s=1}^{M-1} exp(-i s psi) T_s,
+//   T_0 = sum_r X_rr,  T_s = sum_r X_{r,r+s} (1 + i k (e_r - e_{r+s}).d),
+// with d.e = e_x l + e_y m.  T_s = A_s + l B_s per (block, channel) cell,
+// so a grid point costs 2 (M - 1) products per form instead of M (M + 1) / 2
+// complex ones.  The form is used when k_max max_m (|e_x,m| |l|_max +
+// |e_y,m| |m|) <= 1e-4, where the neglected second-order term is below
+// 5e-9 relative; any other geometry takes the general form.
+constexpr double kFirstOrderBound = 1e-4;
+
+struct ArrayInfo {
+    double dx, dy;
+    double ex[kMaxM], ey[kMaxM];
+    int uniform;
+};
+
+// coefficient doubles per form: T_0, then (A_s.re, A_s.im, B_s.re, B_s.im)
+// for s = 1 .. M - 1, padded to an even count (16-byte staging)
+__host__ __device__ constexpr int coef_per_form(int M) { return 4 * M - 2; }
+
+__global__ void doa_array_kernel(const float* __restrict pos, const double* __restrict kw, int M, int n_freq,
+                                 double l_abs_max, double m_fixed, ArrayInfo* __restrict info) {
+    const int lane = threadIdx.x;
+    double kmax = 0.0;
+    for (int f = lane; f < n_freq; f += 32) kmax = fmax(kmax, fabs(kw[f]));
+    for (int o = 16; o > 0; o >>= 1) kmax = fmax(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
+    if (lane != 0) return;
+    ArrayInfo a{};
+    a.uniform = 0;
+    if (M >= 2) {
+        const double x0 = pos[0], y0 = pos[1];
+        a.dx = (static_cast<double>(pos[3 * (M - 1)]) - x0) / (M - 1);
+        a.dy = (static_cast<double>(pos[3 * (M - 1) + 1]) - y0) / (M - 1);
+        double theta = 0.0;
+        for (int m = 0; m < M; ++m) {
+            a.ex[m] = static_cast<double>(pos[3 * m]) - x0 - m * a.dx;
+            a.ey[m] = static_cast<double>(pos[3 * m + 1]) - y0 - m * a.dy;
+            theta = fmax(theta, kmax * (fabs(a.ex[m]) * l_abs_max + fabs(a.ey[m]) * fabs(m_fixed)));
+        }
+        // differences e_r - e_c reach twice a single residual
+        a.uniform = 2.0 * theta <= kFirstOrderBound ? 1 : 0;
+    }
+    *info = a;
+}
+
+// Per (block, channel) cell: the coefficients of the Bartlett (S) and
+// Capon (Q) forms in the uniform sub-array form.
+__global__ void doa_coef_kernel(const Cd* __restrict S, const Cd* __restrict Q, const double* __restrict kw,
+                                int n_freq, int M, double m_fixed, const ArrayInfo* __restrict info,
+                                double* __restrict coef) {
+    if (!info->uniform) return;
+    const int f = blockIdx.x, b = blockIdx.y;
+    const size_t cell = static_cast<size_t>(b) * n_freq + f;
+    const int CQ = coef_per_form(M);
+    const double k = kw[f];
+    double* out = coef + cell * 2 * CQ;
+    const int t = threadIdx.x;
+    if (t < 2 * (M - 1)) {
+        const int form = t / (M - 1), sft = 1 + t % (M - 1);
+        const Cd* X = (form ? Q : S) + cell * M * M;
+        double dr = 0.0, di = 0.0, gxr = 0.0, gxi = 0.0, gyr = 0.0, gyi = 0.0;
+        for (int r = 0; r + sft < M; ++r) {
+            const Cd x = X[r * M + r + sft];
+            const double ex = info->ex[r] - info->ex[r + sft], ey = info->ey[r] - info->ey[r + sft];
+            dr += x.re;
+            di += x.im;
+            gxr += x.re * ex;
+            gxi += x.im * ex;
+            gyr += x.re * ey;
+            gyi += x.im * ey;
+        }
+        // A = D + i k m Gy,  B = i k Gx
+        double* o = out + form * CQ + 1 + 4 * (sft - 1);
+        o[0] = dr - k * m_fixed * gyi;
+        o[1] = di + k * m_fixed * gyr;
+        o[2] = -k * gxi;
+        o[3] = k * gxr;
+    } else if (t < 2 * (M - 1) + 2) {
+        const int form = t - 2 * (M - 1);
+        const Cd* X = (form ? Q : S) + cell * M * M;
+        double tr = 0.0;
+        for (int r = 0; r < M; ++r) tr += X[r * M + r].re;
+        out[form * CQ] = tr;
+        out[form * CQ + CQ - 1] = 0.0;
+    }
+}
+
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(smem))),
                  "l"(gmem)
@@ -211,15 +303,21 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
-template <int M>
+template <int M, bool kUniform>
 __global__ void __launch_bounds__(kScanWarps * 32)
 doa_scan_kernel(const Cd* __restrict S, const Cd* __restrict Q, const int* __restrict ok,
                 const float* __restrict pos, const double* __restrict kw, int n_blocks, int n_freq,
                 double l_first, double l_step, int n, double m_fixed, double* __restrict bartlett,
-                double* __restrict capon, int steps_per_split) {
+                double* __restrict capon, int steps_per_split, const ArrayInfo* __restrict info,
+                const double* __restrict coef) {
+    // the two forms are launched together; the array decides which one runs
+    if ((info->uniform != 0) != kUniform) return;
     constexpr int kScanBlocks = scan_blocks<M>();
     constexpr int U = M * (M + 1) / 2;                 // upper triangle incl. diagonal
-    constexpr int kPerWarp = kScanBlocks * 2 * U;      // Cd staged per warp and step
+    constexpr int CQ = coef_per_form(M);
+    // Cd staged per warp and step: upper triangles of S and Q, or the two
+    // forms' coefficients (2 CQ doubles = CQ Cd)
+    constexpr int kPerWarp = kUniform ? kScanBlocks * CQ : kScanBlocks * 2 * U;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int l = blockIdx.x * 32 + lane;
     const int b0 = blockIdx.y * kScanBlocks;
@@ -237,14 +335,21 @@ doa_scan_kernel(const Cd* __restrict S, const Cd* __restrict Q, const int* __res
         Cd* dst = scan_stage + static_cast<size_t>(buf) * kScanWarps * kPerWarp;
         for (int i = threadIdx.x; i < kScanWarps * kPerWarp; i += blockDim.x) {
             const int w = i / kPerWarp, rem = i % kPerWarp;
-            const int bi = rem / (2 * U), which = (rem / U) & 1, t = rem % U;
             const int f = st * kScanWarps + w;
-            if (f >= n_freq || bi >= nb) continue;
-            int r = 0, rest = t;  // upper-triangle index -> (r, c)
-            while (rest >= M - r) { rest -= M - r; ++r; }
-            const int c = r + rest;
-            const size_t cell = static_cast<size_t>(b0 + bi) * n_freq + f;
-            cp_async16(dst + i, (which ? Q : S) + cell * M * M + r * M + c);
+            if constexpr (kUniform) {
+                const int bi = rem / CQ, e = rem % CQ;
+                if (f >= n_freq || bi >= nb) continue;
+                const size_t cell = static_cast<size_t>(b0 + bi) * n_freq + f;
+                cp_async16(dst + i, reinterpret_cast<const Cd*>(coef) + cell * CQ + e);
+            } else {
+                const int bi = rem / (2 * U), which = (rem / U) & 1, t = rem % U;
+                if (f >= n_freq || bi >= nb) continue;
+                int r = 0, rest = t;  // upper-triangle index -> (r, c)
+                while (rest >= M - r) { rest -= M - r; ++r; }
+                const int c = r + rest;
+                const size_t cell = static_cast<size_t>(b0 + bi) * n_freq + f;
+                cp_async16(dst + i, (which ? Q : S) + cell * M * M + r * M + c);
+            }
         }
         if (threadIdx.x < kScanWarps * kScanBlocks) {
             const int w = threadIdx.x / kScanBlocks, bi = threadIdx.x % kScanBlocks;
@@ -271,7 +376,46 @@ doa_scan_kernel(const Cd* __restrict S, const Cd* __restrict Q, const int* __res
         cp_async_wait_1();
         __syncthreads();
         const int f = st * kScanWarps + warp;
-        if (f < n_freq) {
+        if (kUniform && f < n_freq) {
+            const double* base = reinterpret_cast<const double*>(
+                scan_stage + (static_cast<size_t>(st & 1) * kScanWarps + warp) * kPerWarp);
+            const double k = kw[f];
+            constexpr double kHalfPi = 1.5707963267948966192313216916398;
+            constexpr double kTwoOverPi = 0.63661977236758134307553505349006;
+            // exp(-i s psi) = (cos, -sin) of s psi, s = 1 .. M - 1
+            const double psi = k * (info->dx * lv + info->dy * m_fixed);
+            double zc[M], zs[M];
+#pragma unroll
+            for (int sft = 1; sft < M; ++sft) {
+                const double ph = static_cast<double>(sft) * psi;
+                const double q = rint(ph * kTwoOverPi);
+                const float2 w = trk::sincos_quadrant(__double2float_rn(__fma_rn(-kHalfPi, q, ph)),
+                                                      static_cast<int>(static_cast<long long>(q) & 3));
+                zc[sft] = static_cast<double>(w.x);
+                zs[sft] = static_cast<double>(w.y);
+            }
+            // T_0 + 2 sum_s Re(exp(-i s psi) (A_s + l B_s))
+            auto form = [&](const double* c) {
+                double acc = 0.0;
+#pragma unroll
+                for (int sft = 1; sft < M; ++sft) {
+                    const double* t = c + 1 + 4 * (sft - 1);
+                    const double tre = t[0] + lv * t[2], tim = t[1] + lv * t[3];
+                    acc += zc[sft] * tre + zs[sft] * tim;
+                }
+                return c[0] + 2.0 * acc;
+            };
+#pragma unroll
+            for (int bi = 0; bi < kScanBlocks; ++bi) {
+                if (bi < nb) {
+                    pb[bi] += form(base + bi * 2 * CQ);
+                    if (s_ok[st & 1][warp][bi]) {
+                        const double q = form(base + bi * 2 * CQ + CQ);
+                        pc[bi] += q > 0.0 ? 1.0 / q : 0.0;
+                    }
+                }
+            }
+        } else if (!kUniform && f < n_freq) {
             const Cd* base = scan_stage + (static_cast<size_t>(st & 1) * kScanWarps + warp) * kPerWarp;
             Cd a[M];
             double mag[M];
@@ -373,14 +517,17 @@ int scan_split(long long base_ctas, int n_steps, long long slots) {
     return best;
 }
 
-template <int M>
-bf_status launch_scan_m(cudaStream_t stream, const Cd* S, const Cd* Q, const int* ok, const float* pos,
-                        const double* kw, int B, int F, double l_first, double l_step, int n, double m_fixed,
-                        double* bartlett, double* capon) {
+// One form of the scan (general or uniform sub-array), split over a cluster.
+template <int M, bool kUniform>
+bf_status launch_scan_form(cudaStream_t stream, const Cd* S, const Cd* Q, const int* ok, const float* pos,
+                           const double* kw, int B, int F, double l_first, double l_step, int n, double m_fixed,
+                           double* bartlett, double* capon, const ArrayInfo* info, const double* coef) {
     constexpr int KB = scan_blocks<M>();
     const unsigned gx = static_cast<unsigned>((n + 31) / 32), gy = static_cast<unsigned>((B + KB - 1) / KB);
-    const size_t smem = 2ull * kScanWarps * KB * 2 * (M * (M + 1) / 2) * sizeof(Cd);
-    auto kern = doa_scan_kernel<M>;
+    const size_t per_warp = kUniform ? static_cast<size_t>(KB) * coef_per_form(M)
+                                     : static_cast<size_t>(KB) * 2 * (M * (M + 1) / 2);
+    const size_t smem = 2ull * kScanWarps * per_warp * sizeof(Cd);
+    auto kern = doa_scan_kernel<M, kUniform>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (e != cudaSuccess) return cuda_status(e, "doa_scan_kernel smem attribute");
     int dev = 0, sms = 148, per_sm = 1;
@@ -404,19 +551,39 @@ bf_status launch_scan_m(cudaStream_t stream, const Cd* S, const Cd* Q, const int
     attr[0].val.clusterDim.z = static_cast<unsigned>(split);
     cfg.attrs = attr;
     cfg.numAttrs = split > 1 ? 1 : 0;
-    e = cudaLaunchKernelEx(&cfg, kern, S, Q, ok, pos, kw, B, F, l_first, l_step, n, m_fixed, bartlett, capon, per);
+    e = cudaLaunchKernelEx(&cfg, kern, S, Q, ok, pos, kw, B, F, l_first, l_step, n, m_fixed, bartlett, capon, per,
+                           info, coef);
     return cuda_status(e == cudaSuccess ? cudaGetLastError() : e, "doa_scan_kernel launch");
+}
+
+// Both forms go into the stream; the one the array does not select returns
+// at once.
+template <int M>
+bf_status launch_scan_m(cudaStream_t stream, const Cd* S, const Cd* Q, const int* ok, const float* pos,
+                        const double* kw, int B, int F, double l_first, double l_step, int n, double m_fixed,
+                        double* bartlett, double* capon, const ArrayInfo* info, const double* coef) {
+    BF_RETURN_IF((launch_scan_form<M, false>(stream, S, Q, ok, pos, kw, B, F, l_first, l_step, n, m_fixed, bartlett,
+                                             capon, info, coef)));
+    if constexpr (M >= 2) {
+        BF_RETURN_IF((launch_scan_form<M, true>(stream, S, Q, ok, pos, kw, B, F, l_first, l_step, n, m_fixed,
+                                                bartlett, capon, info, coef)));
+    }
+    return BF_OK;
 }
 
 template <int M>
 bf_status dispatch_scan(int m, cudaStream_t stream, const Cd* S, const Cd* Q, const int* ok, const float* pos,
                         const double* kw, int B, int F, double l_first, double l_step, int n, double m_fixed,
-                        double* bartlett, double* capon) {
+                        double* bartlett, double* capon, const ArrayInfo* info, const double* coef) {
     if constexpr (M > kMaxM) {
         return set_error(BF_ERR_UNSUPPORTED, "the DOA scan supports at most 16 elements after smoothing");
     } else {
-        if (m == M) return launch_scan_m<M>(stream, S, Q, ok, pos, kw, B, F, l_first, l_step, n, m_fixed, bartlett, capon);
-        return dispatch_scan<M + 1>(m, stream, S, Q, ok, pos, kw, B, F, l_first, l_step, n, m_fixed, bartlett, capon);
+        if (m == M) {
+            return launch_scan_m<M>(stream, S, Q, ok, pos, kw, B, F, l_first, l_step, n, m_fixed, bartlett, capon,
+                                    info, coef);
+        }
+        return dispatch_scan<M + 1>(m, stream, S, Q, ok, pos, kw, B, F, l_first, l_step, n, m_fixed, bartlett, capon,
+                                    info, coef);
     }
 }
 
@@ -447,9 +614,18 @@ __global__ void doa_peak_kernel(const double* __restrict bartlett, const double*
 
 }  // namespace
 
+// Workspace: S and Q [cells][M][M] Cd, eps [cells] double, ok [cells] int,
+// then (256-byte aligned) the array description and the uniform form's
+// coefficients [cells][2][4M - 2] double.
+uint64_t doa_coef_offset(uint64_t cells, uint64_t M) {
+    const uint64_t head = cells * (2 * M * M * sizeof(Cd) + sizeof(double) + sizeof(int));
+    return (head + 255) / 256 * 256;
+}
+
 uint64_t doa_workspace_bytes(uint64_t n_blocks, uint64_t n_freq, uint64_t M) {
     const uint64_t cells = n_blocks * n_freq;
-    return cells * (2 * M * M * sizeof(Cd) + sizeof(double) + sizeof(int)) + 256;
+    const uint64_t info = (sizeof(ArrayInfo) + 255) / 256 * 256;
+    return doa_coef_offset(cells, M) + info + cells * 2 * coef_per_form(static_cast<int>(M)) * sizeof(double) + 256;
 }
 
 bf_status launch_doa_scan(cudaStream_t stream, const int32_t* R, const float* pos, const double* kw,
@@ -473,8 +649,17 @@ bf_status launch_doa_scan(cudaStream_t stream, const int32_t* R, const float* po
     BF_RETURN_IF(cuda_status(cudaGetLastError(), "doa_forget_kernel launch"));
     doa_factor_kernel<<<cells_grid, 64, 0, stream>>>(S, E, F, M, Lc, ok);
     BF_RETURN_IF(cuda_status(cudaGetLastError(), "doa_factor_kernel launch"));
+    auto* info = reinterpret_cast<ArrayInfo*>(static_cast<uint8_t*>(workspace) + doa_coef_offset(cells, M));
+    auto* coef = reinterpret_cast<double*>(reinterpret_cast<uint8_t*>(info) + (sizeof(ArrayInfo) + 255) / 256 * 256);
+    const double l_abs_max = std::max(std::fabs(l_first), std::fabs(l_first + static_cast<double>(n - 1) * l_step));
+    doa_array_kernel<<<1, 32, 0, stream>>>(pos, kw, M, F, l_abs_max, m_fixed, info);
+    BF_RETURN_IF(cuda_status(cudaGetLastError(), "doa_array_kernel launch"));
+    if (M >= 2) {
+        doa_coef_kernel<<<cells_grid, 64, 0, stream>>>(S, Lc, kw, F, M, m_fixed, info, coef);
+        BF_RETURN_IF(cuda_status(cudaGetLastError(), "doa_coef_kernel launch"));
+    }
     BF_RETURN_IF(dispatch_scan<1>(M, stream, S, Lc, ok, pos, kw, B, F, l_first, l_step, static_cast<int>(n), m_fixed,
-                                  bartlett, capon));
+                                  bartlett, capon, info, coef));
     doa_peak_kernel<<<B, 64, 0, stream>>>(bartlett, capon, static_cast<int>(n), l_first, l_step, l_est);
     return cuda_status(cudaGetLastError(), "doa_peak_kernel launch");
 }

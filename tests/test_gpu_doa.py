@@ -13,7 +13,7 @@ import math
 import numpy as np
 import pytest
 
-from conftest import random_voltage
+from conftest import rng, random_voltage
 
 F = 336
 C_LIGHT = 299_792_458.0
@@ -156,14 +156,19 @@ def test_scan_matches_fp64_oracle_and_finds_sources(cuda, orc):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("M", [3, 13, 14, 16])
-def test_scan_element_counts_match_fp64_oracle(cuda, orc, M):
+@pytest.mark.parametrize("M,jitter", [(3, 0.0), (13, 0.0), (14, 0.0), (16, 0.0), (8, 1e-3), (16, 1e-3), (2, 0.0)])
+def test_scan_element_counts_match_fp64_oracle(cuda, orc, M, jitter):
     """Sub-array sizes across the scan's shared-memory layouts (four blocks
-    per CTA up to 13 elements, two above) agree with the FP64 oracle."""
+    per CTA up to 13 elements, two above) agree with the FP64 oracle, in the
+    uniform sub-array form (a line of float positions) and, with the
+    positions jittered by about a millimetre, in the general form."""
     from beamform_project_b200 import api, native
     torch = cuda
     A, K, B, n = 64, 128, 3, 301
     pos, freq, kw = geometry(A)
+    if jitter:
+        pos = pos.copy()
+        pos[:M, :2] += (rng(M).standard_normal((M, 2)) * jitter).astype(np.float32)
     amp = 2.0 * math.sqrt(2.0)
     v = source_voltage(K * B, A, [(0.2, amp, 0.0)], seed=M)
     d = api.Dimensions(K * B, F, A, 1)
