@@ -60,6 +60,7 @@ constexpr int kThreads = 384;             // 4 control / unpack warps + 8 epilog
 constexpr int kEpilogueThreads = 256;
 constexpr int kTileM = 128;
 constexpr int kRing = 8;                  // window partial-sum slots
+constexpr uint32_t kMaxDynamicSmem = 232448;  // per CTA on sm_100
 constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s bound on any wait
 
 struct TcParams {
@@ -300,24 +301,35 @@ __device__ __forceinline__ void quantize_ready(const TcParams& p, volatile int* 
 // Shared-memory plan (offsets from a 1024-aligned base).
 struct Smem {
     uint32_t w_bytes = 0;    // one of hi / lo
+    uint32_t w_stages = 1;   // weight images in flight (2 when they fit)
     uint32_t x_bytes = 0;    // one fp16 stage
     uint32_t raw_bytes = 0;  // one raw stage
     uint32_t off_w = 0, off_x = 0, off_raw = 0, off_slots = 0, off_bar = 0, total = 0;
 };
 
-__host__ __device__ constexpr Smem smem_plan(int n_ant, int n_beams_pad) {
+__host__ __device__ constexpr Smem smem_plan(int n_ant, int n_beams_pad, bool served) {
     Smem s{};
     const uint32_t K = 2 * n_ant, N = 2 * n_beams_pad;
     s.w_bytes = (K / 64) * N * 128;
     s.x_bytes = (K / 64) * kTileM * 128;
     s.raw_bytes = kTileM * n_ant;
-    s.off_w = 0;
-    s.off_x = s.off_w + 2 * s.w_bytes;
-    s.off_raw = s.off_x + 2 * s.x_bytes;
-    s.off_slots = s.off_raw + 2 * s.raw_bytes;
     // window partial sums (S >= 32) or the per-warp power staging of short
     // windows ([8 warps][16 beams][32 spectra] floats), which share the space
     const uint32_t ring = kRing * 4 * n_beams_pad * 4, staging = (kEpilogueThreads / 32) * 16 * 32 * 4;
+    const uint32_t rest = 2 * s.x_bytes + 2 * s.raw_bytes + (ring > staging ? ring : staging) + 256;
+    // A second weight image lets the next channel's weights load while the
+    // MMAs of the current one run.  Served units (one window, a few tiles)
+    // switch channel at every unit; measured per served class on a B200, the
+    // second image helps at 64 antennas and up to 32 beams (-8 to -15 %
+    // window time) and costs at 32 antennas (+6 to +20 %: the smaller image
+    // loads quickly, and the space is lost to L1); plain launches switch
+    // rarely.
+    const bool two = served && n_ant == 64 && n_beams_pad <= 32;
+    s.w_stages = two && 4 * s.w_bytes + rest + 1024 <= kMaxDynamicSmem ? 2 : 1;
+    s.off_w = 0;
+    s.off_x = s.off_w + s.w_stages * 2 * s.w_bytes;
+    s.off_raw = s.off_x + 2 * s.x_bytes;
+    s.off_slots = s.off_raw + 2 * s.raw_bytes;
     s.off_bar = s.off_slots + (ring > staging ? ring : staging);
     s.total = s.off_bar + 256;
     return s;
@@ -332,7 +344,7 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
     constexpr uint32_t TMEM_COLS = (2 * N <= 32) ? 32 : (2 * N <= 64) ? 64 : (2 * N <= 128) ? 128
                                    : (2 * N <= 256) ? 256 : 512;
     constexpr uint32_t IDESC = idesc_f16_f32(kTileM, N);
-    constexpr Smem S = smem_plan(A, NB);
+    constexpr Smem S = smem_plan(A, NB, kServed);
     // Warp roles: 0 producer, 1 MMA, then unpack warps, then epilogue warps
     // (a multiple of four, so epilogue warp w reads TMEM lane quadrant w % 4).
     // The narrowest beam set (one 32-column load per quadrant) has little
@@ -346,8 +358,7 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
 
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint8_t* w_hi = smem + S.off_w;
-    uint8_t* w_lo = w_hi + S.w_bytes;
+    uint8_t* w_img = smem + S.off_w;   // [w_stages][hi | lo]
     uint8_t* xs = smem + S.off_x;
     uint8_t* raw = smem + S.off_raw;
     float* slots = reinterpret_cast<float*>(smem + S.off_slots);   // [kRing][4][NB] or staging
@@ -358,13 +369,13 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
     uint64_t* x_empty = bars + 6;     // [2]
     uint64_t* acc_full = bars + 8;    // [2]
     uint64_t* acc_empty = bars + 10;  // [2]
-    uint64_t* w_full = bars + 12;
-    uint64_t* w_empty = bars + 13;
-    uint64_t* mma_done = bars + 14;
-    uint32_t* tmem_ptr = reinterpret_cast<uint32_t*>(bars + 16);
-    volatile int* s_fail = reinterpret_cast<volatile int*>(bars + 17);
-    volatile int* s_quant = reinterpret_cast<volatile int*>(bars + 18);  // [8] windows to quantize
-    volatile int* s_meta = reinterpret_cast<volatile int*>(bars + 22);   // [2] their shard, channel group
+    uint64_t* w_full = bars + 12;     // [w_stages]
+    uint64_t* w_empty = bars + 14;    // [w_stages]
+    uint64_t* mma_done = bars + 16;
+    uint32_t* tmem_ptr = reinterpret_cast<uint32_t*>(bars + 18);
+    volatile int* s_fail = reinterpret_cast<volatile int*>(bars + 19);
+    volatile int* s_quant = reinterpret_cast<volatile int*>(bars + 20);  // [8] windows to quantize
+    volatile int* s_meta = reinterpret_cast<volatile int*>(bars + 24);   // [2] their shard, channel group
     Pending pend, recorded;                                               // epilogue thread 0 only
     pend.mask = 0;
     recorded.mask = 0;
@@ -383,8 +394,10 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
             mbar_init(&acc_full[i], 1);
             mbar_init(&acc_empty[i], kEpiWarps);
         }
-        mbar_init(w_full, 1);
-        mbar_init(w_empty, 1);
+        for (uint32_t i = 0; i < S.w_stages; ++i) {
+            mbar_init(&w_full[i], 1);
+            mbar_init(&w_empty[i], 1);
+        }
         mbar_init(mma_done, 1);
         *s_fail = 0;
         fence_mbar_init();
@@ -419,10 +432,10 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
         // ------------------------------------------------------------ producer
         if (lane == 0) {
             int stage = 0;
-            uint32_t phase = 0, w_empty_phase = 0;
+            uint32_t phase = 0;
             int armed[2] = {-1, -1};   // parity of the last load issued per raw stage
-            int w_armed = -1;          // parity of the last weight load
-            uint32_t w_loads = 0;
+            uint32_t w_loads = 0;      // weight images loaded; image i goes to stage i % w_stages
+            uint32_t w_uses[2] = {0, 0};
             int prev_key = -1;
             bool stop = false;
             JobCursor<kServed> cur;
@@ -432,19 +445,22 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                 const Unit un = cur.at(u);
                 const TcJob& jb = cur.jb;
                 if (un.key != prev_key) {
-                    if (prev_key >= 0) {
-                        if (!mbar_wait(w_empty, w_empty_phase, kWaitNs)) { fail(1); break; }
-                        w_empty_phase ^= 1;
+                    const uint32_t ws = w_loads % S.w_stages;
+                    // the stage's previous image must be done with (its n-th
+                    // reuse waits for the n-th release, parity (n - 1) & 1)
+                    if (w_uses[ws] > 0) {
+                        if (!mbar_wait(&w_empty[ws], (w_uses[ws] - 1) & 1, kWaitNs)) { fail(1); break; }
                     }
-                    mbar_expect_tx(w_full, 2 * S.w_bytes);
+                    mbar_expect_tx(&w_full[ws], 2 * S.w_bytes);
                     const uint8_t* src =
                         jb.split + static_cast<size_t>(un.shard * jb.n_freq + un.f) * 2 * S.w_bytes;
+                    uint8_t* dst = w_img + ws * 2 * S.w_bytes;
                     constexpr uint32_t kChunk = 32768;
                     for (uint32_t off = 0; off < 2 * S.w_bytes; off += kChunk) {
                         const uint32_t n = min(kChunk, 2 * S.w_bytes - off);
-                        bulk_g2s(w_hi + off, src + off, n, w_full);
+                        bulk_g2s(dst + off, src + off, n, &w_full[ws]);
                     }
-                    w_armed = static_cast<int>(w_loads & 1);
+                    ++w_uses[ws];
                     ++w_loads;
                     prev_key = un.key;
                 }
@@ -473,24 +489,31 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
             for (int s = 0; s < 2; ++s) {
                 if (armed[s] >= 0 && !mbar_wait(&raw_full[s], static_cast<uint32_t>(armed[s]), kWaitNs)) fail(256);
             }
-            if (w_armed >= 0 && !mbar_wait(w_full, static_cast<uint32_t>(w_armed), kWaitNs)) fail(512);
+            for (uint32_t ws = 0; ws < S.w_stages; ++ws) {
+                if (w_uses[ws] > 0 && !mbar_wait(&w_full[ws], (w_uses[ws] - 1) & 1, kWaitNs)) fail(512);
+            }
         }
     } else if (warp == 1) {
         // ------------------------------------------------------------ MMA issuer
         if (lane == 0) {
             int xs_stage = 0, acc_stage = 0;
-            uint32_t x_phase = 0, acc_phase = 0, w_phase = 0;
+            uint32_t x_phase = 0, acc_phase = 0;
+            uint32_t w_switches = 0, w_seen[2] = {0, 0}, ws = 0;
             int prev_key = -1;
             bool stop = false;
-            const uint32_t w_hi_addr = smem_u32(w_hi), w_lo_addr = smem_u32(w_lo);
+            uint32_t w_hi_addr = smem_u32(w_img), w_lo_addr = w_hi_addr + S.w_bytes;
             JobCursor<kServed> cur;
             if (u_begin < u_end) cur.init(p, u_begin);
             cur.pair_parity = pair_parity;
             for (long long u = u_begin; u < u_end && !stop; ++u) {
                 const Unit un = cur.at(u);
                 if (un.key != prev_key) {
-                    if (!mbar_wait(w_full, w_phase, kWaitNs)) { fail(4); break; }
-                    w_phase ^= 1;
+                    ws = w_switches % S.w_stages;
+                    if (!mbar_wait(&w_full[ws], w_seen[ws] & 1, kWaitNs)) { fail(4); break; }
+                    ++w_seen[ws];
+                    ++w_switches;
+                    w_hi_addr = smem_u32(w_img + ws * 2 * S.w_bytes);
+                    w_lo_addr = w_hi_addr + S.w_bytes;
                     prev_key = un.key;
                 }
                 bool next_switches = true;
@@ -516,7 +539,7 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                     }
                     tc_commit(&x_empty[xs_stage]);
                     tc_commit(&acc_full[acc_stage]);
-                    if (k + 1 == un.tile_end && next_switches) tc_commit(w_empty);
+                    if (k + 1 == un.tile_end && next_switches) tc_commit(&w_empty[ws]);
                     if (++xs_stage == 2) { xs_stage = 0; x_phase ^= 1; }
                     if (++acc_stage == 2) { acc_stage = 0; acc_phase ^= 1; }
                 }
@@ -852,7 +875,7 @@ int padded_beams(uint64_t b) { return static_cast<int>((b + 15) / 16 * 16); }
 template <int A, int NB, bool kServed>
 bf_status launch_tc(cudaStream_t stream, const CUtensorMap& map, const TcParams& p, int grid,
                     bool set_attribute = true) {
-    const Smem s = smem_plan(A, NB);
+    const Smem s = smem_plan(A, NB, kServed);
     const size_t smem = s.total + 1024;
     auto kern = grid_tensor_kernel<A, NB, kServed>;
     if (set_attribute) {
