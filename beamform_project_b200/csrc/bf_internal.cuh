@@ -54,6 +54,21 @@ __device__ __forceinline__ float power_ref(float sr, float si) {
     return __fadd_rn(__fmul_rn(sr, sr), __fmul_rn(si, si));
 }
 
+// rint((v - offset) / scale) clamped to [-127, 127], with the quotient of the
+// reference's correctly rounded float division.  The quotient comes from the
+// reciprocal and one fused correction step, which is within one ulp of the
+// correctly rounded value, so its nearest integer is the same unless the
+// value lies within 2^-14 of a half-integer (|q| <= 127.5 here: one ulp is at
+// most 2^-16); only those values take the correctly rounded division.
+__device__ __forceinline__ int quantize_code(float v, float offset, float scale, float rcp) {
+    const float d = __fsub_rn(v, offset);
+    const float q0 = __fmul_rn(d, rcp);
+    float q = __fmaf_rn(__fmaf_rn(-q0, scale, d), rcp, q0);
+    const float frac = __fsub_rn(q, floorf(q));
+    if (fabsf(__fsub_rn(frac, 0.5f)) < 0x1p-14f) q = __fdiv_rn(d, scale);
+    return max(-127, min(127, __float2int_rn(q)));
+}
+
 // One warp quantizes one 1x16x16 chunk (window w, channels 16*ft.., beams
 // 16*bt..) of integrated [W][F][B] exactly as cpu_quantize_integrated_intensity
 // (src/quantization.cpp:61-161): min/max over the finite values,
@@ -62,29 +77,55 @@ __device__ __forceinline__ float power_ref(float sr, float si) {
 // a zero parameter pair for a chunk holding one.  Correctly rounded
 // intrinsics keep codes and parameters bit-identical to the CPU reference.
 // kCoherent reads through L2 (values written by other CTAs of a running grid).
+// A lane holds four consecutive beams of two channels (16-byte loads and
+// 4-byte code stores when the beam count is a multiple of four and the
+// buffers are aligned for them, scalar accesses otherwise).
 template <bool kCoherent>
 __device__ __forceinline__ void quantize_chunk(const float* __restrict in, int8_t* __restrict codes,
                                                float2* __restrict params, size_t param_index, int win,
                                                int n_freq, int n_beams, int ft, int bt, int lane) {
+    const bool vec = (n_beams & 3) == 0 && (reinterpret_cast<uintptr_t>(in) & 15) == 0 &&
+                     (reinterpret_cast<uintptr_t>(codes) & 3) == 0;
+    const int b0 = bt * 16 + 4 * (lane & 3);
     float vals[8];
     bool valid[8];
     float mn = INFINITY, mx = -INFINITY;
     bool nonfinite = false;
 #pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        const int s = lane + 32 * i;  // local_freq * 16 + local_beam
-        const int f = ft * 16 + (s >> 4), b = bt * 16 + (s & 15);
-        valid[i] = f < n_freq && b < n_beams;
-        vals[i] = 0.f;
-        if (valid[i]) {
-            const float* src = in + (static_cast<size_t>(win) * n_freq + f) * n_beams + b;
-            vals[i] = kCoherent ? __ldcg(src) : *src;
-            if (!isfinite(vals[i])) {
-                nonfinite = true;
-            } else {
-                mn = fminf(mn, vals[i]);
-                mx = fmaxf(mx, vals[i]);
+    for (int h = 0; h < 2; ++h) {
+        const int f = ft * 16 + (lane >> 2) + 8 * h;
+        const size_t row = (static_cast<size_t>(win) * n_freq + f) * n_beams;
+        if (vec) {
+            const bool ok = f < n_freq && b0 < n_beams;
+            float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (ok) {
+                const float4* src = reinterpret_cast<const float4*>(in + row + b0);
+                x = kCoherent ? __ldcg(src) : *src;
             }
+            vals[4 * h] = x.x;
+            vals[4 * h + 1] = x.y;
+            vals[4 * h + 2] = x.z;
+            vals[4 * h + 3] = x.w;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) valid[4 * h + j] = ok;
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const bool ok = f < n_freq && b0 + j < n_beams;
+                valid[4 * h + j] = ok;
+                vals[4 * h + j] = 0.f;
+                if (ok) vals[4 * h + j] = kCoherent ? __ldcg(in + row + b0 + j) : in[row + b0 + j];
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        if (!valid[i]) continue;
+        if (!isfinite(vals[i])) {
+            nonfinite = true;
+        } else {
+            mn = fminf(mn, vals[i]);
+            mx = fmaxf(mx, vals[i]);
         }
     }
     nonfinite = __any_sync(0xffffffffu, nonfinite);
@@ -100,19 +141,32 @@ __device__ __forceinline__ void quantize_chunk(const float* __restrict in, int8_
         if (!isfinite(offset) || !isfinite(scale)) offset = scale = 0.f;
     }
     if (lane == 0) params[param_index] = make_float2(offset, scale);
+    const float rcp = scale != 0.f ? __frcp_rn(scale) : 0.f;
+    int c[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-        if (!valid[i]) continue;
-        const int s = lane + 32 * i;
-        const int f = ft * 16 + (s >> 4), b = bt * 16 + (s & 15);
-        int code = 0;
-        if (!isfinite(vals[i])) {
-            code = -128;
-        } else if (scale != 0.f) {
-            code = __float2int_rn(__fdiv_rn(__fsub_rn(vals[i], offset), scale));
-            code = max(-127, min(127, code));
+        c[i] = 0;
+        if (!isfinite(vals[i])) c[i] = -128;
+        else if (scale != 0.f) c[i] = quantize_code(vals[i], offset, scale, rcp);
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int f = ft * 16 + (lane >> 2) + 8 * h;
+        const size_t row = (static_cast<size_t>(win) * n_freq + f) * n_beams;
+        if (vec) {
+            if (valid[4 * h]) {
+                const uint32_t packed = (static_cast<uint32_t>(c[4 * h]) & 0xFFu) |
+                                        ((static_cast<uint32_t>(c[4 * h + 1]) & 0xFFu) << 8) |
+                                        ((static_cast<uint32_t>(c[4 * h + 2]) & 0xFFu) << 16) |
+                                        ((static_cast<uint32_t>(c[4 * h + 3]) & 0xFFu) << 24);
+                *reinterpret_cast<uint32_t*>(codes + row + b0) = packed;
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (valid[4 * h + j]) codes[row + b0 + j] = static_cast<int8_t>(c[4 * h + j]);
+            }
         }
-        codes[(static_cast<size_t>(win) * n_freq + f) * n_beams + b] = static_cast<int8_t>(code);
     }
 }
 

@@ -92,6 +92,28 @@ def test_quantizer_bit_exact(cuda, orc, W, B):
     assert np.array_equal(params.cpu().numpy().reshape(rp.shape), rp)
 
 
+@pytest.mark.parametrize("W,B", [(4, 16), (3, 12), (2, 8), (2, 20)])
+def test_quantizer_ties_bit_exact(cuda, orc, W, B):
+    """Integer values whose chunks span exactly 0 .. 255: scale 1, offset
+    127.5, so every quotient is a half-integer and rounds by ties to even;
+    beam counts on the vector path (multiples of four, also a partial beam
+    tile) and off it."""
+    from beamform_project_b200 import api
+    torch = cuda
+    I = np.random.default_rng(W + B).integers(0, 256, size=(W, F, B)).astype(np.float32)
+    for ft in range(0, F, 16):
+        for bt in range(0, B, 16):
+            I[:, ft, bt] = 0.0
+            I[:, ft + 1, bt] = 255.0
+    qd = api.Dimensions(W, F, 32, B)
+    codes = torch.zeros(W * F * B, dtype=torch.int8, device="cuda")
+    params = torch.zeros(2 * api.quantization_parameter_count(qd), dtype=torch.float32, device="cuda")
+    api.launch_quantize_integrated_intensity(None, _dev(torch, I), codes, params, qd)
+    rc, rp = orc.quantize(I, W, F, B)
+    assert np.array_equal(params.cpu().numpy().reshape(rp.shape), rp)
+    assert np.array_equal(codes.cpu().numpy().reshape(W, F, B), rc)
+
+
 def test_quantized_pipeline_matches_oracle_chain(cuda, orc):
     from beamform_project_b200 import api
     T, A, B, S = 700, 64, 20, 320
