@@ -108,6 +108,14 @@ struct ClassKey {
     }
 };
 
+// The quantizer runs per grid class, right after that class's kernel on the
+// same graph branch: its key is the grid class's key with the quantizer kind.
+ClassKey quant_class_of(const ClassKey& grid) {
+    ClassKey q = grid;
+    q.kind = kQuantClass;
+    return q;
+}
+
 uint64_t entry_bytes(int kind) {
     return kind == kGridClass ? sizeof(TcJob) : kind == kQuantClass ? sizeof(QJob) : sizeof(TrJob);
 }
@@ -482,7 +490,7 @@ double predicted_us(const bf_server* s, const std::vector<uint64_t>& ids, const 
             classes.push_back(j.cls);
             us += kClassUs;
         }
-        const ClassKey qk{kQuantClass, 0, 0, 0, 0};
+        const ClassKey qk = quant_class_of(j.cls);
         if (j.spec.kind == BF_SERVE_GRID && j.spec.quantize &&
             std::find(classes.begin(), classes.end(), qk) == classes.end()) {
             classes.push_back(qk);
@@ -584,8 +592,9 @@ bf_status capture_graph(bf_server* s, const std::vector<std::pair<ClassKey, uint
         }
     }
     // Classes run on parallel branches of the graph (a fork from the server's
-    // stream onto side streams, joined back before the quantizer and at the
-    // end), so one class's CTAs fill the SMs another class's tail leaves idle.
+    // stream onto side streams, joined back at the end), so one class's CTAs
+    // fill the SMs another class's tail leaves idle; a grid class's quantizer
+    // follows it on its branch.
     // Classes never share an SM (each grid CTA holds a whole register file,
     // a tracker CTA half of one), so TMEM allocation never waits.
     cudaGraph_t graph = nullptr;
@@ -609,7 +618,7 @@ bf_status capture_graph(bf_server* s, const std::vector<std::pair<ClassKey, uint
             used[b] = false;
         }
     };
-    // grid and tracker classes on branches; the quantizer after the grid classes
+    // grid and tracker classes on branches, each grid class's quantizer after it
     for (const auto& c : cap) {
         if (st != BF_OK) break;
         if (c.key.kind == kQuantClass) continue;
@@ -620,6 +629,12 @@ bf_status capture_graph(bf_server* s, const std::vector<std::pair<ClassKey, uint
             CUtensorMap* m = nullptr;
             st = encode_pool_map(s, c.key.n_ant, c.key.rows_q, &m);
             if (st == BF_OK) st = launch_grid_tensor_served(s->side[b], *m, c.key.n_ant, c.key.nb_pad, t, s->sms);
+            const ClassKey qk = quant_class_of(c.key);
+            for (const auto& q : cap) {
+                if (st != BF_OK || !(q.key == qk)) continue;
+                st = launch_served_quantize(s->side[b], reinterpret_cast<const TableHeader*>(s->d_tables + q.offset),
+                                            s->sms * 8);
+            }
         } else {
             const int A = c.key.n_ant;
             const bool short_windows = c.key.short_win != 0;
@@ -629,11 +644,6 @@ bf_status capture_graph(bf_server* s, const std::vector<std::pair<ClassKey, uint
         }
     }
     join();
-    for (const auto& c : cap) {
-        if (st != BF_OK || c.key.kind != kQuantClass) continue;
-        st = launch_served_quantize(s->stream, reinterpret_cast<const TableHeader*>(s->d_tables + c.offset),
-                                    s->sms * 8);
-    }
     const cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
     if (st != BF_OK) {
         if (graph) cudaGraphDestroy(graph);
@@ -665,7 +675,7 @@ bf_status step(bf_server* s, uint32_t* n_live) {
     for (uint64_t id : s->live) {
         const Job& j = s->jobs.at(id);
         by_class[j.cls].push_back(id);
-        if (j.spec.kind == BF_SERVE_GRID && j.spec.quantize) by_class[ClassKey{kQuantClass, 0, 0, 0, 0}].push_back(id);
+        if (j.spec.kind == BF_SERVE_GRID && j.spec.quantize) by_class[quant_class_of(j.cls)].push_back(id);
     }
     std::vector<std::pair<ClassKey, uint32_t>> classes;
     for (const auto& kv : by_class) classes.emplace_back(kv.first, static_cast<uint32_t>(kv.second.size()));
