@@ -50,7 +50,7 @@ class DeviceTimeout(BeamformerError):
 
 
 class Unsupported(BeamformerError):
-    """A valid request outside this build's kernels."""
+    """A valid request outside what the kernels support."""
 
 
 class ResourceError(BeamformerError, MemoryError):

@@ -52,7 +52,7 @@ typedef enum bf_status {
     BF_ERR_OVERFLOW = 4,         /* std::overflow_error   */
     BF_ERR_OUT_OF_RANGE = 5,     /* std::out_of_range     */
     BF_ERR_TIMEOUT = 6,          /* a bounded device wait ran out */
-    BF_ERR_UNSUPPORTED = 7,      /* valid request outside this build's kernels */
+    BF_ERR_UNSUPPORTED = 7,      /* valid request outside what the kernels support */
     BF_ERR_RESOURCE = 8          /* a served job can never fit the HBM budget */
 } bf_status;
 

@@ -2,13 +2,14 @@
 
     python oracle/build.py
 
-Products (git-ignored, but shipped to the GPU box with the snapshot):
+Products (git-ignored; a copy of the checkout used for GPU testing carries
+the built files):
     oracle/liboracle.so        C restatement (bf_oracle.c), -ffp-contract=off
     oracle/_ref/libbfref.so    the reference CPU core, compiled directly from the
                                reference checkout's own source files plus
                                ref_shim.cpp; built only when the checkout is
-                               present (it is absent on the GPU box, which uses
-                               the prebuilt file).
+                               present (a machine without it uses the
+                               prebuilt file).
     oracle/_ref/beamformer_cpu the reference's CPU command-line beamformer and
     oracle/_ref/run_tracker_stream  tracker (CPU engines), from the same sources
                                plus its tools/beamformer_cpu.cpp and
