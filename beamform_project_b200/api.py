@@ -243,6 +243,95 @@ def grid_tensor_quantized(stream, packed_voltage, split_weights, integrated, cod
 # tracker
 # --------------------------------------------------------------------------
 
+def _host(a, name: str, dtype, min_elems: int) -> int:
+    """Address of a contiguous host buffer (numpy array or CPU tensor)."""
+    if isinstance(a, np.ndarray):
+        if a.dtype != np.dtype(dtype) or not a.flags.c_contiguous:
+            raise InvalidArgument(1, f"{name} must be a contiguous {np.dtype(dtype)} array")
+        if a.size < min_elems:
+            raise InvalidArgument(1, f"{name} is smaller than dimensions ({a.size} < {min_elems})")
+        return a.ctypes.data
+    torch = _torch()
+    tdt = {np.uint8: torch.uint8, np.int8: torch.int8, np.float32: torch.float32}[dtype]
+    if not isinstance(a, torch.Tensor) or a.is_cuda or a.dtype != tdt or not a.is_contiguous():
+        raise InvalidArgument(1, f"{name} must be a contiguous host {tdt} tensor or numpy array")
+    if a.numel() < min_elems:
+        raise InvalidArgument(1, f"{name} is smaller than dimensions ({a.numel()} < {min_elems})")
+    return a.data_ptr()
+
+
+def grid_pipeline_chunk_spectra(dims: Dimensions, integration_spectra: int, n_shards: int = 1,
+                                chunk_spectra: int = 0) -> int:
+    d = dims.c()
+    return int(native.lib().bf_grid_pipeline_chunk_spectra(C.byref(d), int(integration_spectra), int(n_shards),
+                                                           int(chunk_spectra)))
+
+
+class GridHostPipeline:
+    """The tensor-core grid fed from host buffers (bf_grid_pipeline_*): the
+    counterpart of CudaBeamformerWorkspace.run_quantized_integrated_pipeline
+    (include/beamformer/cuda_beamformer.hpp:66-76) with weights resident and,
+    per block, the voltage streamed in and the products streamed out in time
+    chunks that overlap the kernels.  Host layouts: voltage
+    [shard][T][F][A] uint8, integrated [shard][W][F][B] float32, codes
+    [shard][W][F][B] int8, params [shard][W][F/16][B/16][2] float32.  Pinned
+    host tensors give PCIe-rate copies; numpy arrays work through the
+    driver's staging."""
+
+    def __init__(self, dims: Dimensions, integration_spectra: int, n_shards: int = 1, chunk_spectra: int = 0):
+        validate_dimensions(dims)
+        self.dims, self.spectra, self.n_shards = dims, int(integration_spectra), int(n_shards)
+        self.n_windows = integrated_time_count(dims.n_time, integration_spectra)
+        self.chunk_spectra = grid_pipeline_chunk_spectra(dims, integration_spectra, n_shards, chunk_spectra)
+        h = C.c_void_p()
+        d = dims.c()
+        check(native.lib().bf_grid_pipeline_create(C.byref(d), self.spectra, self.n_shards, int(chunk_spectra),
+                                                   C.byref(h)))
+        self._h = h
+
+    def upload_weights(self, weights) -> None:
+        """Canonical complex64 weights [shard][B][F][A] (or float32 [..][2])."""
+        w = np.asarray(weights)
+        w = np.ascontiguousarray(w, dtype=np.complex64).view(np.float32) if np.iscomplexobj(w) \
+            else np.ascontiguousarray(w, dtype=np.float32)
+        n = 2 * self.n_shards * self.dims.n_beams * self.dims.n_freq * self.dims.n_ant
+        check(native.lib().bf_grid_pipeline_upload_weights(self._handle(), _host(w.reshape(-1), "weights",
+                                                                                 np.float32, n)))
+
+    def run(self, voltage, integrated=None, codes=None, params=None) -> float:
+        """One block; returns the device milliseconds from first copy-in to last copy-out."""
+        d = self.dims
+        n_out = self.n_shards * self.n_windows * d.n_freq * d.n_beams
+        n_par = 2 * self.n_shards * quantization_parameter_count(
+            Dimensions(self.n_windows, d.n_freq, d.n_ant, d.n_beams))
+        v = _host(voltage, "voltage", np.uint8, self.n_shards * d.n_time * d.n_freq * d.n_ant)
+        i = None if integrated is None else _host(integrated, "integrated", np.float32, n_out)
+        c = None if codes is None else _host(codes, "codes", np.int8, n_out)
+        p = None if params is None else _host(params, "params", np.float32, n_par)
+        ms = C.c_float(0.0)
+        check(native.lib().bf_grid_pipeline_run(self._handle(), v, i, c, p, C.byref(ms)))
+        return float(ms.value)
+
+    def _handle(self):
+        if self._h is None:
+            raise LogicError(2, "the pipeline has been closed")
+        return self._h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None:
+            native.lib().bf_grid_pipeline_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        self.close()
+
+
 def tracker(stream, mode, packed_voltage, positions, wave_numbers, window_directions,
             intensity, integrated, dims: Dimensions, integration_spectra: int) -> None:
     torch = _torch()

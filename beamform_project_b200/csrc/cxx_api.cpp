@@ -473,6 +473,47 @@ CudaBeamformerTimings CudaBeamformerWorkspace::run_quantized_integrated_pipeline
     return t;
 }
 
+CudaChunkedGridPipeline::CudaChunkedGridPipeline(const Dimensions& dims,
+                                                 const TemporalIntegrationConfig& temporal_integration,
+                                                 std::size_t n_shards, std::size_t chunk_spectra)
+    : dims_(dims), spectra_(temporal_integration.integration_spectra), n_shards_(n_shards) {
+    validate_dimensions(dims);
+    const bf_dims d = to_c(dims);
+    check(bf_grid_pipeline_create(&d, spectra_, n_shards_, chunk_spectra, &pipeline_));
+    chunk_ = bf_grid_pipeline_chunk_spectra(&d, spectra_, n_shards_, chunk_spectra);
+}
+
+CudaChunkedGridPipeline::~CudaChunkedGridPipeline() { bf_grid_pipeline_destroy(pipeline_); }
+
+std::size_t CudaChunkedGridPipeline::chunk_spectra() const { return chunk_; }
+
+void CudaChunkedGridPipeline::upload_weights(const Weights& weights) {
+    if (weights.size() != n_shards_ * dims_.n_beams * dims_.n_freq * dims_.n_ant) {
+        throw std::invalid_argument("weight count does not match selected kernel layout");
+    }
+    check(bf_grid_pipeline_upload_weights(pipeline_, reinterpret_cast<const float*>(weights.data())));
+}
+
+double CudaChunkedGridPipeline::run(const PackedVoltage& packed, IntegratedIntensities* integrated,
+                                   QuantizedIntegratedOutput* quantized) {
+    if (packed.size() < n_shards_ * voltage_sample_count(dims_)) {
+        throw std::invalid_argument("packed voltage is smaller than dimensions");
+    }
+    const Dimensions qd{integrated_time_count(dims_.n_time, TemporalIntegrationConfig{spectra_}), dims_.n_freq,
+                        dims_.n_ant, dims_.n_beams};
+    const std::size_t n_out = n_shards_ * qd.n_time * qd.n_freq * qd.n_beams;
+    if (integrated != nullptr) integrated->resize(n_out);
+    if (quantized != nullptr) {
+        quantized->codes.resize(n_out);
+        quantized->parameters.resize(n_shards_ * quantization_parameter_count(qd));
+    }
+    float ms = 0.0F;
+    check(bf_grid_pipeline_run(pipeline_, packed.data(), integrated ? integrated->data() : nullptr,
+                               quantized ? quantized->codes.data() : nullptr,
+                               quantized ? reinterpret_cast<float*>(quantized->parameters.data()) : nullptr, &ms));
+    return ms;
+}
+
 namespace {
 bool same_shard(const ShardDescriptor& a, const ShardDescriptor& b) {
     return a.shard_id == b.shard_id && a.shard_count == b.shard_count &&

@@ -104,6 +104,11 @@ _SIGS = {
     "bf_split_weight_bytes": (_U64, [C.POINTER(Dims), _U64]),
     "bf_prepare_split_weights": (C.c_int, [_P, _P, _P, C.POINTER(Dims), _U64]),
     "bf_grid_tensor_integrated": (C.c_int, [_P, _P, _P, _P, _P, _P, C.POINTER(Dims), _U64, _U64]),
+    "bf_grid_pipeline_chunk_spectra": (_U64, [C.POINTER(Dims), _U64, _U64, _U64]),
+    "bf_grid_pipeline_create": (C.c_int, [C.POINTER(Dims), _U64, _U64, _U64, _PP]),
+    "bf_grid_pipeline_upload_weights": (C.c_int, [_P, _P]),
+    "bf_grid_pipeline_run": (C.c_int, [_P, _P, _P, _P, _P, C.POINTER(C.c_float)]),
+    "bf_grid_pipeline_destroy": (C.c_int, [_P]),
     "bf_tracker": (C.c_int, [_P, C.c_int, _P, _P, _P, _P, _P, _P, C.POINTER(Dims), _U64]),
     "bf_grid_tensor_workspace_bytes": (_U64, [C.POINTER(Dims), _U64, _U64]),
     "bf_grid_tensor_quantized": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, C.POINTER(Dims), _U64, _U64]),

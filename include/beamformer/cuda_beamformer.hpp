@@ -24,6 +24,8 @@
 #include <optional>
 #include <string>
 
+struct bf_grid_pipeline;  // include/bf_b200.h
+
 namespace beamformer {
 
 enum class CudaBeamformerOutput {
@@ -85,6 +87,32 @@ class CudaBeamformerWorkspace {
   private:
     struct Impl;
     std::unique_ptr<Impl> impl_;
+};
+
+// Added: the TensorSplit grid fed from host memory (bf_grid_pipeline_* of
+// bf_b200.h).  Weights stay resident; each run() streams a block of n_shards
+// shards ([shard][T][F][A] bytes) in time chunks whose host-to-device copy,
+// kernels and device-to-host copy overlap on three streams, with products
+// bit-identical to one TensorSplit launch over the block.  Outputs are
+// resized to [shard][W][F][B] (codes) and [shard][W][F/16][B/16]
+// (parameters); run() returns the device milliseconds of the block.
+class CudaChunkedGridPipeline {
+  public:
+    CudaChunkedGridPipeline(const Dimensions& dims, const TemporalIntegrationConfig& temporal_integration,
+                            std::size_t n_shards = 1, std::size_t chunk_spectra = 0);
+    ~CudaChunkedGridPipeline();
+
+    CudaChunkedGridPipeline(const CudaChunkedGridPipeline&) = delete;
+    CudaChunkedGridPipeline& operator=(const CudaChunkedGridPipeline&) = delete;
+
+    std::size_t chunk_spectra() const;
+    void upload_weights(const Weights& weights);  // [shard][B][F][A]
+    double run(const PackedVoltage& packed, IntegratedIntensities* integrated, QuantizedIntegratedOutput* quantized);
+
+  private:
+    bf_grid_pipeline* pipeline_ = nullptr;
+    Dimensions dims_;
+    std::size_t spectra_ = 0, n_shards_ = 0, chunk_ = 0;
 };
 
 Intensities cuda_beamform_packed_intensity(const PackedVoltage& packed, const Weights& weights,

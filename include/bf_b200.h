@@ -181,6 +181,49 @@ BF_API bf_status bf_grid_tensor_quantized_static(void* stream, const uint8_t* pa
                                                  int8_t* codes, float* params, const bf_dims* dims,
                                                  uint64_t integration_spectra, uint64_t n_shards);
 
+/* Host-buffer grid pipeline.  Counterpart of the reference's
+ * CudaBeamformerWorkspace::run_quantized_integrated_pipeline
+ * (include/beamformer/cuda_beamformer.hpp:66-76: weights resident, voltage
+ * uploaded and products downloaded per call), with the block cut into time
+ * chunks whose host->device copy, kernels and device->host copy overlap on
+ * three streams.  Products are bit-identical to bf_grid_tensor_integrated over
+ * the whole block.  Host layouts: voltage [shard][T][F][A] bytes, integrated
+ * [shard][W][F][B] float, codes [shard][W][F][B] int8, params
+ * [shard][W][F/16][B/16][offset, scale] float.  Pin the host buffers
+ * (cudaHostAlloc / cudaHostRegister) for copies at PCIe rate alongside the
+ * kernels.  A pipeline belongs to the device current at creation and to one
+ * host thread at a time. */
+typedef struct bf_grid_pipeline bf_grid_pipeline;
+
+/* Spectra per chunk the pipeline would use: chunk_spectra itself (a multiple
+ * of lcm(128, integration_spectra)) or, for 0, about 64 MiB of voltage;
+ * never more than the block rounded up to that multiple.  0 for an invalid
+ * request. */
+BF_API uint64_t bf_grid_pipeline_chunk_spectra(const bf_dims* dims, uint64_t integration_spectra,
+                                               uint64_t n_shards, uint64_t chunk_spectra);
+
+/* Allocates two chunk slots of voltage and products and the prepared-weight
+ * operand for n_shards shards of dims (dims.n_time is the block length).
+ * Same limits as bf_grid_tensor_integrated. */
+BF_API bf_status bf_grid_pipeline_create(const bf_dims* dims, uint64_t integration_spectra,
+                                         uint64_t n_shards, uint64_t chunk_spectra,
+                                         bf_grid_pipeline** pipeline);
+
+/* Canonical complex64 weights [shard][B][F][A][2] from host memory, prepared
+ * into the resident split operand.  Synchronous. */
+BF_API bf_status bf_grid_pipeline_upload_weights(bf_grid_pipeline* pipeline, const float* host_weights);
+
+/* One block: host voltage in, host products out (integrated may be NULL when
+ * codes and params are given; codes and params both or neither).  Returns
+ * after the last product has reached host memory; *elapsed_ms (optional) is
+ * the device time from the first copy-in to the last copy-out.
+ * BF_ERR_TIMEOUT when a bounded device wait ran out. */
+BF_API bf_status bf_grid_pipeline_run(bf_grid_pipeline* pipeline, const uint8_t* host_voltage,
+                                      float* host_integrated, int8_t* host_codes, float* host_params,
+                                      float* elapsed_ms);
+
+BF_API bf_status bf_grid_pipeline_destroy(bf_grid_pipeline* pipeline);
+
 /* Reads and clears the device-side error word of the tensor-core kernels
  * (0 = no error).  Every wait inside those kernels is bounded; a wait that
  * runs out sets a bit here (and the kernel returns) instead of hanging.

@@ -199,6 +199,32 @@ int main() {
             }
             expect(ok10, "TensorSplit 10-spectrum integration within tolerance");
         }
+        {
+            // chunked host pipeline: bit-identical to the one-launch TensorSplit workspace
+            CudaBeamformerWorkspace wq(di, CudaBeamformerKernel::TensorSplit, integration_direct,
+                                       CudaBeamformerOutput::QuantizedInt8);
+            wq.upload_weights(wi, di);
+            QuantizedIntegratedOutput qw{QuantizedIntensities(integ.size()),
+                                         std::vector<Int8QuantizationParameters>(3 * 21 * 3)};
+            wq.run_quantized_integrated_pipeline(vi, qw, di);
+            CudaChunkedGridPipeline pipe(di, integration_direct, 1, 640);
+            expect(pipe.chunk_spectra() == 640, "chunked pipeline keeps a 640-spectrum chunk");
+            expect(throws<std::logic_error>([&] { IntegratedIntensities x; pipe.run(vi, &x, nullptr); }),
+                   "chunked pipeline before weights is a logic_error");
+            pipe.upload_weights(wi);
+            IntegratedIntensities pi;
+            QuantizedIntegratedOutput pq;
+            const double ms = pipe.run(vi, &pi, &pq);
+            bool same_p = pq.parameters.size() == qw.parameters.size();
+            for (std::size_t i = 0; i < pq.parameters.size() && same_p; ++i) {
+                same_p &= pq.parameters[i].offset == qw.parameters[i].offset &&
+                          pq.parameters[i].scale == qw.parameters[i].scale;
+            }
+            expect(ms > 0.0 && pi == out && pq.codes == qw.codes && same_p,
+                   "chunked pipeline equals one TensorSplit launch bit for bit");
+            expect(throws<std::invalid_argument>([&] { CudaChunkedGridPipeline x(di, integration_direct, 1, 600); }),
+                   "chunked pipeline rejects a chunk off the 640-spectrum grid");
+        }
 
         // device frame path: voltage and weights already on the device
         std::uint8_t* dv = nullptr;

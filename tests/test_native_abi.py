@@ -89,6 +89,29 @@ def test_stage_calls_validate_before_launch():
     assert lib.bf_tracker(None, 0, fake, fake, fake, fake, fake, None, C.byref(d1), 0) == 1
 
 
+def test_grid_pipeline_checks_before_allocating():
+    """bf_grid_pipeline_create validates the request before any CUDA call, and
+    the chunk length follows lcm(128, integration_spectra)."""
+    from beamform_project_b200 import api
+    lib = native.lib()
+    d = _d(t=32768, b=128)
+    h = C.c_void_p()
+    assert lib.bf_grid_pipeline_create(C.byref(d), 320, 2, 1000, C.byref(h)) == 1
+    assert "multiple of lcm(128, integration_spectra) = 640" in native.last_error()
+    assert lib.bf_grid_pipeline_create(C.byref(d), 40, 1, 0, C.byref(h)) == 7
+    assert lib.bf_grid_pipeline_create(C.byref(_d(a=128)), 320, 1, 0, C.byref(h)) == 7
+    assert lib.bf_grid_pipeline_create(C.byref(d), 320, 0, 0, C.byref(h)) == 1
+    assert lib.bf_grid_pipeline_create(C.byref(d), 320, 1, 0, None) == 1
+    assert h.value is None
+    assert api.grid_pipeline_chunk_spectra(api.Dimensions(32768, 336, 64, 128), 320, 2) == 1280
+    assert api.grid_pipeline_chunk_spectra(api.Dimensions(32768, 336, 64, 128), 10, 1) == 2560
+    assert api.grid_pipeline_chunk_spectra(api.Dimensions(700, 336, 32, 8), 320, 1, 6400) == 1280
+    assert api.grid_pipeline_chunk_spectra(api.Dimensions(700, 336, 32, 8), 96, 1, 0) == 768
+    assert api.grid_pipeline_chunk_spectra(api.Dimensions(700, 336, 32, 8), 320, 1, 100) == 0
+    assert lib.bf_grid_pipeline_run(None, None, None, None, None, None) == 1
+    assert lib.bf_grid_pipeline_destroy(None) == 0
+
+
 def test_error_text_is_per_call():
     lib = native.lib()
     bad = _d(t=0)
