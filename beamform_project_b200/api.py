@@ -214,6 +214,45 @@ def grid_tensor_integrated(stream, packed_voltage, split_weights, integrated, co
                                                  int(n_shards)))
 
 
+def cov_weight_bytes(dims: Dimensions, n_shards: int = 1) -> int:
+    d = dims.c()
+    return int(native.lib().bf_cov_weight_bytes(C.byref(d), int(n_shards)))
+
+
+def prepare_cov_weights(stream, weights, cov_weights, dims: Dimensions, n_shards: int = 1) -> None:
+    """Canonical complex64 weights ([shard][B][F][A][2], device) -> the
+    covariance-form grid's per-channel image (bf_prepare_cov_weights)."""
+    torch = _torch()
+    validate_dimensions(dims)
+    w = _dev(weights, "weights", torch.float32, 2 * n_shards * dims.n_beams * dims.n_freq * dims.n_ant)
+    o = _dev(cov_weights, "cov_weights", torch.uint8, cov_weight_bytes(dims, n_shards))
+    d = dims.c()
+    check(native.lib().bf_prepare_cov_weights(_stream_handle(stream), w, o, C.byref(d), int(n_shards)))
+
+
+def grid_cov_integrated(stream, packed_voltage, cov_weights, integrated, codes, params,
+                        dims: Dimensions, integration_spectra: int, n_shards: int = 1) -> None:
+    """The grid beamformer in covariance form (bf_grid_cov_integrated): the
+    integrated power of each window from its exact INT32 array covariance on
+    int8 tensor cores and a split-fp16 quadratic form.  n_ant 64, integration
+    a multiple of 64 spectra; same outputs and layouts as grid_tensor_integrated."""
+    torch = _torch()
+    validate_dimensions(dims)
+    nw = integrated_time_count(dims.n_time, integration_spectra)
+    n_out = n_shards * nw * dims.n_freq * dims.n_beams
+    v = _dev(packed_voltage, "packed_voltage", torch.uint8, n_shards * dims.n_time * dims.n_freq * dims.n_ant)
+    s = _dev(cov_weights, "cov_weights", torch.uint8, cov_weight_bytes(dims, n_shards))
+    o = _dev(integrated, "integrated", torch.float32, n_out)
+    c = p = None
+    if codes is not None or params is not None:
+        qd = Dimensions(nw, dims.n_freq, dims.n_ant, dims.n_beams)
+        c = _dev(codes, "codes", torch.int8, n_out)
+        p = _dev(params, "params", torch.float32, 2 * n_shards * quantization_parameter_count(qd))
+    d = dims.c()
+    check(native.lib().bf_grid_cov_integrated(_stream_handle(stream), v, s, o, c, p, C.byref(d),
+                                              int(integration_spectra), int(n_shards)))
+
+
 def grid_tensor_workspace_bytes(dims: Dimensions, integration_spectra: int, n_shards: int = 1) -> int:
     d = dims.c()
     return int(native.lib().bf_grid_tensor_workspace_bytes(C.byref(d), int(integration_spectra), int(n_shards)))

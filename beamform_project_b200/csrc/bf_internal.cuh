@@ -196,6 +196,12 @@ bf_status launch_prepare_split(cudaStream_t stream, const float* w, void* split,
                                uint64_t n_shards, int nb_pad = 0);
 bf_status take_tc_error(uint32_t* code);
 unsigned* device_error_word();
+// covariance-form grid (grid_cov.cu)
+uint64_t cov_weight_bytes(const bf_dims& d, uint64_t n_shards);
+bf_status check_grid_cov(const bf_dims& d, uint64_t spectra, uint64_t n_shards);
+bf_status launch_prepare_cov(cudaStream_t stream, const float* w, void* out, const bf_dims& d, uint64_t n_shards);
+bf_status launch_grid_cov(cudaStream_t stream, const uint8_t* v, const void* wimg, float* integrated,
+                          int8_t* codes, float* params, const bf_dims& d, uint64_t spectra, uint64_t n_shards);
 uint64_t grid_tensor_counter_count(const bf_dims& d, uint64_t spectra, uint64_t n_shards);
 // counters == nullptr: quantize (when codes is given) with a second launch;
 // otherwise quantization is fused into the tensor kernel's epilogue and

@@ -245,6 +245,43 @@ BF_API bf_status bf_grid_tensor_quantized(void* stream, const uint8_t* packed_vo
                               static_cast<unsigned*>(workspace));
 }
 
+BF_API uint64_t bf_cov_weight_bytes(const bf_dims* dims, uint64_t n_shards) {
+    if (dims == nullptr) return 0;
+    return cov_weight_bytes(*dims, n_shards);
+}
+
+BF_API bf_status bf_prepare_cov_weights(void* stream, const float* weights, void* cov_weights,
+                                        const bf_dims* dims, uint64_t n_shards) {
+    clear_error();
+    BF_TRY(validate_dims(dims));
+    if (n_shards == 0) return set_error(BF_ERR_INVALID_ARGUMENT, "n_shards must be positive");
+    if (dims->n_ant != 64) return set_error(BF_ERR_UNSUPPORTED, "the covariance-form grid supports n_ant 64");
+    BF_TRY(check_ptr(weights, 8, "weights"));
+    BF_TRY(check_ptr(cov_weights, 16, "cov_weights"));
+    return launch_prepare_cov(static_cast<cudaStream_t>(stream), weights, cov_weights, *dims, n_shards);
+}
+
+BF_API bf_status bf_grid_cov_integrated(void* stream, const uint8_t* packed_voltage, const void* cov_weights,
+                                        float* integrated, int8_t* codes, float* params, const bf_dims* dims,
+                                        uint64_t integration_spectra, uint64_t n_shards) {
+    clear_error();
+    BF_TRY(validate_dims(dims));
+    if (n_shards == 0) return set_error(BF_ERR_INVALID_ARGUMENT, "n_shards must be positive");
+    if (integration_spectra == 0) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "integration_spectra must be positive");
+    }
+    BF_TRY(check_grid_cov(*dims, integration_spectra, n_shards));
+    if ((codes == nullptr) != (params == nullptr)) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "codes and params must both be given or both be null");
+    }
+    BF_TRY(check_ptr(packed_voltage, 16, "packed_voltage"));
+    BF_TRY(check_ptr(cov_weights, 16, "cov_weights"));
+    BF_TRY(check_ptr(integrated, 16, "integrated"));
+    if (codes != nullptr) BF_TRY(check_ptr(params, 8, "params"));
+    return launch_grid_cov(static_cast<cudaStream_t>(stream), packed_voltage, cov_weights, integrated, codes,
+                           params, *dims, integration_spectra, n_shards);
+}
+
 BF_API bf_status bf_tracker(void* stream, int mode, const uint8_t* packed_voltage,
                             const float* positions, const double* wave_numbers,
                             const float* window_directions, float* intensity,

@@ -104,6 +104,9 @@ _SIGS = {
     "bf_split_weight_bytes": (_U64, [C.POINTER(Dims), _U64]),
     "bf_prepare_split_weights": (C.c_int, [_P, _P, _P, C.POINTER(Dims), _U64]),
     "bf_grid_tensor_integrated": (C.c_int, [_P, _P, _P, _P, _P, _P, C.POINTER(Dims), _U64, _U64]),
+    "bf_cov_weight_bytes": (_U64, [C.POINTER(Dims), _U64]),
+    "bf_prepare_cov_weights": (C.c_int, [_P, _P, _P, C.POINTER(Dims), _U64]),
+    "bf_grid_cov_integrated": (C.c_int, [_P, _P, _P, _P, _P, _P, C.POINTER(Dims), _U64, _U64]),
     "bf_grid_pipeline_chunk_spectra": (_U64, [C.POINTER(Dims), _U64, _U64, _U64]),
     "bf_grid_pipeline_create": (C.c_int, [C.POINTER(Dims), _U64, _U64, _U64, _PP]),
     "bf_grid_pipeline_upload_weights": (C.c_int, [_P, _P]),

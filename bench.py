@@ -423,6 +423,43 @@ def run_gpu(args):
                  "tensor_speedup": plain_ms / ms_per_step, "max_rel_diff_vs_tensor": rel,
                  "int8_codes_differing": int((lsb > 0).sum().item()), "int8_max_lsb": int(lsb.max().item())}
 
+    # the covariance form beside it (opt-in kernel, same inputs): time and
+    # distance from the reference-order float32 output
+    cov = None
+    if kernel == "tensor" and args.cov_steps > 0 and plain is not None:
+        covw = torch.empty(api.cov_weight_bytes(d, N_SHARDS), dtype=torch.uint8, device=dev)
+        api.prepare_cov_weights(None, weights, covw, d, N_SHARDS)
+        integ_c = torch.empty_like(integ)
+        codes_c = torch.empty_like(codes)
+        params_c = torch.empty_like(params)
+
+        def cov_step():
+            api.grid_cov_integrated(None, volt, covw, integ_c, None, None, d, S_INT, N_SHARDS)
+
+        cov_step()
+        torch.cuda.synchronize()
+        c0 = torch.cuda.Event(enable_timing=True)
+        c1 = torch.cuda.Event(enable_timing=True)
+        c0.record(stream)
+        for _ in range(args.cov_steps):
+            cov_step()
+        c1.record(stream)
+        torch.cuda.synchronize()
+        assert native.take_device_error() == 0
+        cov_ms = c0.elapsed_time(c1) / args.cov_steps
+        api.launch_quantize_integrated_intensity(None, integ_c, codes_c, params_c, qd_all)
+        torch.cuda.synchronize()
+        ref = integ_p.double()
+        rel = ((integ_c.double() - ref).abs() / ref.abs().clamp_min(1e-30)).max().item()
+        lsb = (codes_c.int() - codes_p.int()).abs()
+        cov = {"kernel": "grid_cov_kernel (covariance form, opt-in)", "kernel_ms": cov_ms,
+               "value": samples_per_step / (cov_ms / 1e3),
+               "algorithmic_tflops": (8 * T_SPECTRA * N_SHARDS * F_SHARD * N_ANT * N_BEAMS
+                                      + 3 * samples_per_step) / (cov_ms / 1e3) / 1e12,
+               "max_rel_diff_vs_plain": rel, "int8_codes_differing": int((lsb > 0).sum().item()),
+               "int8_max_lsb": int(lsb.max().item())}
+        del covw, integ_c, codes_c, params_c
+
     peak_tflops, hbm_gbs, peak_src = measured_peaks()
     cmac = T_SPECTRA * N_SHARDS * F_SHARD * N_ANT * N_BEAMS
     alg_flops = 8 * cmac + 3 * samples_per_step
@@ -455,6 +492,7 @@ def run_gpu(args):
         "clocks": clocks.summary(),
         "source_peak_ok": peak_ok,
         "plain_dropin": plain,
+        "covariance_form": cov,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v0 = volt[:shard_bytes].cpu().numpy().reshape(T_SPECTRA, F_SHARD, N_ANT)
@@ -1186,6 +1224,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="grid", choices=["grid", "tracker", "doa", "serve"])
+    ap.add_argument("--cov-steps", type=int, default=20,
+                    help="grid: time the opt-in covariance-form kernel beside the split kernel")
     ap.add_argument("--kernel", default="tensor", choices=["tensor", "tiled", "stream", "exact"])
     ap.add_argument("--shards", type=int, default=N_SHARDS, choices=[1, 2])
     ap.add_argument("--e2e-steps", type=int, default=5)

@@ -181,6 +181,28 @@ BF_API bf_status bf_grid_tensor_quantized_static(void* stream, const uint8_t* pa
                                                  int8_t* codes, float* params, const bf_dims* dims,
                                                  uint64_t integration_spectra, uint64_t n_shards);
 
+/* Covariance-form grid beamformer for long integration windows.  No
+ * reference counterpart (the reference integrates spectrum by spectrum,
+ * src/cuda_beamformer.cu:108-354); same outputs and layouts as
+ * bf_grid_tensor_integrated.  Each window's integrated power is the quadratic
+ * form v^T E v of its array covariance E = sum_t y(t) y(t)^T (exact INT32 on
+ * int8 tensor cores), with v the beam weights split into fp16 hi + lo.
+ * n_ant 64, integration_spectra a multiple of 64 up to 16384, n_freq even,
+ * n_beams <= 128. */
+BF_API uint64_t bf_cov_weight_bytes(const bf_dims* dims, uint64_t n_shards);
+
+/* Canonical complex64 weights ([shard][B][F][A][2], device) -> the operand of
+ * bf_grid_cov_integrated (128 KiB per channel). */
+BF_API bf_status bf_prepare_cov_weights(void* stream, const float* weights, void* cov_weights,
+                                        const bf_dims* dims, uint64_t n_shards);
+
+/* Integrated power [shard][W][F][B] (and, when codes and params are non-NULL,
+ * the int8 chunk codes and parameters of launch_quantize_integrated_intensity). */
+BF_API bf_status bf_grid_cov_integrated(void* stream, const uint8_t* packed_voltage,
+                                        const void* cov_weights, float* integrated, int8_t* codes,
+                                        float* params, const bf_dims* dims,
+                                        uint64_t integration_spectra, uint64_t n_shards);
+
 /* Host-buffer grid pipeline.  Counterpart of the reference's
  * CudaBeamformerWorkspace::run_quantized_integrated_pipeline
  * (include/beamformer/cuda_beamformer.hpp:66-76: weights resident, voltage
