@@ -136,7 +136,7 @@ def test_cov_grid_rejects_unsupported(cuda):
     torch = cuda
     d = api.Dimensions(640, F, A, 8)
     buf = torch.empty(640 * F * A, dtype=torch.uint8, device="cuda")
-    out = torch.empty(2 * F * 8, dtype=torch.float32, device="cuda")
+    out = torch.empty(64 * F * 8, dtype=torch.float32, device="cuda")  # 64 windows of 10 spectra
     cw = torch.empty(api.cov_weight_bytes(d), dtype=torch.uint8, device="cuda")
     with pytest.raises(api.Unsupported, match="multiple of 64"):
         api.grid_cov_integrated(None, buf, cw, out, None, None, d, 10)
