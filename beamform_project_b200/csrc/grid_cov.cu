@@ -31,8 +31,8 @@
 // even and odd channel of a pair, so both halves of each 128-byte line are
 // read together), warp 1 MMA issuer and TMEM owner, warps 2-9 unpack, warps
 // 10-17 convert (two per TMEM lane quadrant), warps 18-21 form the beam sums.
-// TMEM: three 128-column E stages (Gram accumulator, then A operand) and one
-// 128-column Y.  Shared memory: the channel's V image (fp16 hi, fp16 lo in the
+// TMEM: two 128-column E stages (Gram accumulator, then A operand) and two
+// 128-column Y stages.  Shared memory: the channel's V image (fp16 hi, fp16 lo in the
 // 128-byte-swizzled K-major layout, fp32 [beam][component]), voltage stages.
 // Every wait is bounded and reports through the device error word.
 #include "bf_internal.cuh"
@@ -56,15 +56,18 @@ constexpr int kUnpackFirst = 2, kUnpackWarps = 8;
 constexpr int kConvFirst = 10, kConvWarps = 8;
 constexpr int kDotFirst = 18, kDotWarps = 4;
 constexpr int kRows = 64;                             // spectra per voltage tile
-constexpr int kRawStages = 4, kXStages = 3;
+constexpr int kRawStages = 8, kXStages = 6;
 constexpr uint32_t kRawBytes = kRows * 64;            // one channel, 64 antennas
 constexpr uint32_t kXBytes = kRows * 128;             // [row][128 components] int8
 constexpr uint32_t kWHalf = 128 * 256;                // [128 beams][128 K] fp16
 constexpr uint32_t kVBytes = 128 * 128 * 4;           // [beam][component] fp32
 constexpr uint32_t kWImage = 2 * kWHalf + kVBytes;    // per channel
-constexpr uint32_t kYCol = 384;                       // TMEM column of Y
+constexpr uint32_t kYCol = 256;                       // TMEM columns of the two Y stages
 constexpr uint64_t kWaitNs = 2000000000ull;
-constexpr uint32_t kSmemBytes = kWImage + kXStages * kXBytes + kRawStages * kRawBytes + 2 * 4 * 128 * 4 + 256 + 1024;
+constexpr uint32_t kBarBytes = (2 * kRawStages + 2 * kXStages + 11) * 8 + 8;  // mbarriers, TMEM address, fail flag
+constexpr uint32_t kSmemBytes = kWImage + kXStages * kXBytes + kRawStages * kRawBytes + 2 * 4 * 128 * 4 + 512 + 1024;
+static_assert(kBarBytes <= 512, "barrier block");
+static_assert(kSmemBytes <= 232448, "shared memory per CTA");
 
 struct CovGridParams {
     const uint8_t* wimg;     // [shard][F][kWImage]
@@ -130,11 +133,11 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
     uint64_t* raw_empty = raw_full + kRawStages; // [kRawStages]
     uint64_t* x_full = raw_empty + kRawStages;   // [kXStages]
     uint64_t* x_empty = x_full + kXStages;       // [kXStages]
-    uint64_t* gram_done = x_empty + kXStages;    // [3]
-    uint64_t* conv_done = gram_done + 3;         // [3]
-    uint64_t* quad_done = conv_done + 3;         // [3]
-    uint64_t* y_free = quad_done + 3;
-    uint64_t* w_full = y_free + 1;
+    uint64_t* gram_done = x_empty + kXStages;    // [2]
+    uint64_t* conv_done = gram_done + 2;         // [2]
+    uint64_t* quad_done = conv_done + 2;         // [2]
+    uint64_t* y_free = quad_done + 2;            // [2]
+    uint64_t* w_full = y_free + 2;
     uint64_t* w_empty = w_full + 1;
     uint64_t* mma_done = w_empty + 1;
     uint32_t* tmem_ptr = reinterpret_cast<uint32_t*>(mma_done + 1);
@@ -150,12 +153,12 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
             mbar_init(&x_full[i], kUnpackWarps);
             mbar_init(&x_empty[i], 1);
         }
-        for (int i = 0; i < 3; ++i) {
+        for (int i = 0; i < 2; ++i) {
             mbar_init(&gram_done[i], 1);
             mbar_init(&conv_done[i], kConvWarps);
             mbar_init(&quad_done[i], 1);
+            mbar_init(&y_free[i], kDotWarps);
         }
-        mbar_init(y_free, kDotWarps);
         mbar_init(w_full, 1);
         mbar_init(w_empty, 1 + kDotWarps);
         mbar_init(mma_done, 1);
@@ -226,13 +229,14 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
             bool q_first = false;
             int q_run = 0, q_key = -1;
             auto issue_quad = [&](long long i, bool first, bool last, int run) -> bool {
-                const int eb = static_cast<int>(i % 3);
-                const uint32_t par = static_cast<uint32_t>((i / 3) & 1);
+                const int eb = static_cast<int>(i & 1);
+                const uint32_t par = static_cast<uint32_t>((i >> 1) & 1);
                 if (!mbar_wait(&conv_done[eb], par, kWaitNs)) { fail(5); return false; }
-                if (i >= 1 && !mbar_wait(y_free, static_cast<uint32_t>((i - 1) & 1), kWaitNs)) { fail(6); return false; }
+                // Y[eb] was last read by the beam sums of unit i - 2
+                if (i >= 2 && !mbar_wait(&y_free[eb], par ^ 1, kWaitNs)) { fail(6); return false; }
                 if (first && !mbar_wait(w_full, static_cast<uint32_t>(run & 1), kWaitNs)) { fail(7); return false; }
                 tc_fence_after();
-                const uint32_t e_tm = tmem_base + eb * 128, y_tm = tmem_base + kYCol;
+                const uint32_t e_tm = tmem_base + eb * 128, y_tm = tmem_base + kYCol + eb * 128;
                 const uint32_t w_hi = smem_u32(wsm), w_lo = w_hi + kWHalf;
 #pragma unroll
                 for (int kk = 0; kk < 8; ++kk) {
@@ -256,9 +260,10 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
                     ++runs;
                     prev_key = un.key;
                 }
-                const int eb = static_cast<int>(j % 3);
-                // E[eb] was last read by the quad of unit j - 3
-                if (j >= 3 && !mbar_wait(&quad_done[eb], static_cast<uint32_t>(((j - 3) / 3) & 1), kWaitNs)) {
+                const int eb = static_cast<int>(j & 1);
+                // E[eb] was last read by the quad of unit j - 2, issued just before:
+                // waiting for it lets the tensor pipe drain once per unit
+                if (j >= 2 && !mbar_wait(&quad_done[eb], static_cast<uint32_t>(((j - 2) >> 1) & 1), kWaitNs)) {
                     fail(8);
                     break;
                 }
@@ -333,8 +338,8 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
         const int sgn0 = ((m >> 2) & 1) != 0 ? -1 : 1;
         long long j = 0;
         for (long long pu = u_begin; pu < u_end; ++pu, ++j) {
-            const int eb = static_cast<int>(j % 3);
-            if (!mbar_wait(&gram_done[eb], static_cast<uint32_t>((j / 3) & 1), kWaitNs)) { fail(13); break; }
+            const int eb = static_cast<int>(j & 1);
+            if (!mbar_wait(&gram_done[eb], static_cast<uint32_t>((j >> 1) & 1), kWaitNs)) { fail(13); break; }
             tc_fence_after();
 #pragma unroll 1
             for (int cc = 2 * half; cc < 2 * half + 2; ++cc) {
@@ -377,19 +382,19 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
         for (long long pu = u_begin; pu < u_end; ++pu, ++j) {
             const CovUnit un = cov_unit(pu, odd, p);
             const bool last = pu + 1 == u_end || cov_unit(pu + 1, odd, p).key != un.key;
-            const int eb = static_cast<int>(j % 3);
-            if (!mbar_wait(&quad_done[eb], static_cast<uint32_t>((j / 3) & 1), kWaitNs)) { fail(14); break; }
+            const int eb = static_cast<int>(j & 1);
+            if (!mbar_wait(&quad_done[eb], static_cast<uint32_t>((j >> 1) & 1), kWaitNs)) { fail(14); break; }
             tc_fence_after();
             float part[4];
 #pragma unroll 1
             for (int cb = 0; cb < 4; ++cb) {
                 uint32_t y[32];
-                tmem_ld_32x32b_x32(tmem_base + ((32u * q) << 16) + kYCol + 32 * cb, y);
+                tmem_ld_32x32b_x32(tmem_base + ((32u * q) << 16) + kYCol + eb * 128 + 32 * cb, y);
                 tmem_ld_wait();
                 if (cb == 3) {
                     tc_fence_before();
                     __syncwarp();
-                    if (lane == 0) mbar_arrive(y_free);
+                    if (lane == 0) mbar_arrive(&y_free[eb]);
                 }
                 float pr[32];
 #pragma unroll
