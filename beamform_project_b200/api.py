@@ -368,7 +368,10 @@ class GridHostPipeline:
         self.close()
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown: the library may be gone already
+            pass
 
 
 def tracker(stream, mode, packed_voltage, positions, wave_numbers, window_directions,

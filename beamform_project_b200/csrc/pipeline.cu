@@ -93,9 +93,16 @@ struct bf_grid_pipeline {
         return cuda_status(cudaMalloc(&split, split_weight_bytes(dims, n_shards)), "cudaMalloc split weights");
     }
 
+    // Waits for everything issued on the three streams (a run that failed part
+    // way may have copies in flight).
+    void drain() {
+        if (in) cudaStreamSynchronize(in);
+        if (comp) cudaStreamSynchronize(comp);
+        if (out) cudaStreamSynchronize(out);
+    }
+
     ~bf_grid_pipeline() {
-        // Destruction waits for nothing of the caller's: run() returns only after
-        // its last copy, so these streams are idle here.
+        drain();
         for (int i = 0; i < 2; ++i) {
             cudaFree(volt[i]);
             cudaFree(integ[i]);
@@ -275,7 +282,9 @@ BF_API bf_status bf_grid_pipeline_run(bf_grid_pipeline* p, const uint8_t* host_v
     int dev = 0;
     BF_RETURN_IF(cuda_status(cudaGetDevice(&dev), "cudaGetDevice"));
     if (dev != p->device) return set_error(BF_ERR_LOGIC, "the pipeline belongs to another device");
-    return p->run(host_voltage, host_integrated, host_codes, host_params, elapsed_ms);
+    const bf_status st = p->run(host_voltage, host_integrated, host_codes, host_params, elapsed_ms);
+    if (st != BF_OK) p->drain();  // no copy may touch the caller's buffers after an error return
+    return st;
 }
 
 BF_API bf_status bf_grid_pipeline_destroy(bf_grid_pipeline* p) {
