@@ -1312,6 +1312,18 @@ BF_API bf_status bf_serve_take_done(bf_server* s, uint64_t* ids, uint64_t capaci
 
 BF_API void* bf_serve_stream(bf_server* s) { return s == nullptr ? nullptr : static_cast<void*>(s->stream); }
 
+BF_API bf_status bf_serve_pool(bf_server* s, uint64_t n_ant, uint8_t** pool, uint64_t* pool_spectra,
+                               uint64_t* pool_channels) {
+    clear_error();
+    if (s == nullptr || pool == nullptr) return set_error(BF_ERR_INVALID_ARGUMENT, "server and pool must not be null");
+    if (n_ant != 32 && n_ant != 64) return set_error(BF_ERR_INVALID_ARGUMENT, "served pools hold 32 or 64 antennas");
+    if (s->host_only) return set_error(BF_ERR_LOGIC, "a host-only server has no device pools");
+    *pool = s->pool[n_ant == 64 ? 1 : 0];
+    if (pool_spectra != nullptr) *pool_spectra = s->cfg.pool_spectra;
+    if (pool_channels != nullptr) *pool_channels = static_cast<uint64_t>(s->cfg.shard_channels) * s->cfg.max_shards;
+    return BF_OK;
+}
+
 static bf_status bf_serve_checkpoint_impl(bf_server* s, uint64_t job_id, void* buffer, uint64_t capacity,
                                           uint64_t* bytes) {
     clear_error();

@@ -141,6 +141,7 @@ _SIGS = {
     "bf_serve_step_times": (C.c_int, [_P, C.POINTER(C.c_float), _U64, C.POINTER(C.c_uint64)]),
     "bf_serve_take_done": (C.c_int, [_P, C.POINTER(C.c_uint64), _U64, C.POINTER(C.c_uint64)]),
     "bf_serve_stream": (_P, [_P]),
+    "bf_serve_pool": (C.c_int, [_P, _U64, _PP, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
 }
 
 

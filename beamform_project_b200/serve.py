@@ -158,6 +158,18 @@ class Server:
     def stream_handle(self) -> int:
         return int(native.lib().bf_serve_stream(self._h) or 0)
 
+    def pool(self, n_ant: int):
+        """The device voltage pool that jobs of n_ant antennas read, as a torch
+        uint8 tensor [pool_spectra][pool_channels][n_ant] (a view, no copy).
+        The ingest hook: write captured rows into it on the server's stream
+        (torch.cuda.ExternalStream(server.stream_handle())) before the step
+        whose windows read them."""
+        import torch
+        ptr, sp, ch = C.c_void_p(), C.c_uint64(0), C.c_uint64(0)
+        native.check(native.lib().bf_serve_pool(self._h, int(n_ant), C.byref(ptr), C.byref(sp), C.byref(ch)))
+        shape = (int(sp.value), int(ch.value), int(n_ant))
+        return torch.as_tensor(_DeviceArray(int(ptr.value), shape, "|u1"), device="cuda")
+
     def result_pointers(self, job_id: int) -> tuple[int, int, int, int]:
         i, c, p = C.c_void_p(), C.c_void_p(), C.c_void_p()
         n = C.c_uint64(0)

@@ -472,6 +472,21 @@ BF_API bf_status bf_serve_step_times(bf_server* server, float* out, uint64_t cap
 BF_API bf_status bf_serve_take_done(bf_server* server, uint64_t* ids, uint64_t capacity, uint64_t* count);
 /* The server's stream (cudaStream_t as void*), for reading results in order. */
 BF_API void* bf_serve_stream(bf_server* server);
+/* Ingest hook.  The reference feeds each job from host memory and names
+ * ingest straight into GPU memory as the way past the host bounce
+ * (info/cuda_implementation_investigation.md:70-76).  This returns the device
+ * pool that jobs of n_ant antennas read, [pool_spectra][pool_channels][n_ant]
+ * packed bytes (pool_channels = max_shards * shard_channels; shard s of a job
+ * is channels [s * shard_channels, (s + 1) * shard_channels)).  A capture
+ * stage -- GPUDirect RDMA, a peer copy, a kernel -- writes rows there in
+ * stream order before the bf_serve_step whose windows read them: on
+ * bf_serve_stream(server), or on its own stream followed by an event that
+ * the caller makes the server stream wait on.  Window k of a job reads rows
+ * (pool_offset + k * window_spectra) mod pool_spectra; rows that launched
+ * windows may still read are rewritten only after those steps complete
+ * (bf_serve_sync).  BF_ERR_LOGIC for a host-only server. */
+BF_API bf_status bf_serve_pool(bf_server* server, uint64_t n_ant, uint8_t** pool, uint64_t* pool_spectra,
+                               uint64_t* pool_channels);
 
 #ifdef __cplusplus
 }

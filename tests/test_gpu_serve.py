@@ -241,3 +241,29 @@ def test_checkpoint_restore_equals_uninterrupted(cuda):
         assert (u is None and v is None) or np.array_equal(u, v)
     for u, v in zip(straight[0], redone):
         assert (u is None and v is None) or np.array_equal(u, v)
+
+
+def test_ingest_into_pool_is_what_jobs_read(cuda, orc):
+    """The ingest hook: voltage written into the server's pool on its stream
+    (a capture stage's job) is what a served grid job beamforms."""
+    from conftest import random_voltage
+    torch = cuda
+    A, T, S, B, offset = 64, 640, 320, 24, 320 * 7
+    v = random_voltage(T, F, A, seed=77)
+    job = _grid_job(A=A, ns=1, B=B, S=S, n_spectra=T, offset=offset, seed=3)
+    with _server() as srv:
+        pool = srv.pool(A)
+        assert tuple(pool.shape) == (POOL, 4 * F, A)
+        src = torch.from_numpy(v).cuda()
+        torch.cuda.synchronize()
+        with torch.cuda.stream(torch.cuda.ExternalStream(srv.stream_handle())):
+            pool[offset:offset + T, :F, :].copy_(src)
+        (integ, _, _), = _run(srv, [job])
+    d = api.Dimensions(T, F, A, B)
+    w = torch.empty(B * F * A * 2, dtype=torch.float32, device="cuda")
+    api.generate_weights(None, torch.from_numpy(job.positions).cuda(), torch.from_numpy(job.frequencies).cuda(),
+                         torch.from_numpy(job.directions).cuda(), w, d, 1)
+    torch.cuda.synchronize()
+    ref64 = orc.beamform_integrated(v, w.cpu().numpy().reshape(B, F, A, 2), T, F, A, B, S, f64=True)
+    err = np.abs(integ[0].astype(np.float64) - ref64)
+    assert np.all(err <= 1e-3 + 1e-5 * np.abs(ref64))

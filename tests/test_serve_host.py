@@ -266,3 +266,17 @@ def test_checkpoint_errors():
     with serve.Server(10**9, host_only=True, pool_spectra=10240) as other:
         with pytest.raises(native.InvalidArgument, match="pool settings"):
             other.restore(good)
+
+
+def test_pool_hook_checks_arguments():
+    """bf_serve_pool: antenna count and host-only servers are checked before
+    any pointer is handed out."""
+    import ctypes as C
+    from beamform_project_b200 import native
+    with serve.Server(10**9, max_jobs=4, host_only=True) as srv:
+        ptr = C.c_void_p()
+        assert native.lib().bf_serve_pool(srv._h, 48, C.byref(ptr), None, None) == 1
+        assert "32 or 64" in native.last_error()
+        assert native.lib().bf_serve_pool(srv._h, 64, C.byref(ptr), None, None) == 2
+        assert "host-only" in native.last_error()
+        assert native.lib().bf_serve_pool(None, 64, C.byref(ptr), None, None) == 1
