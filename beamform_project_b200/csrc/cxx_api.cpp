@@ -1024,4 +1024,10 @@ std::vector<float> ServedBeamformer::window_times_ms() {
 
 void* ServedBeamformer::stream() { return bf_serve_stream(server_); }
 
+ServedBeamformer::Pool ServedBeamformer::pool(std::uint64_t n_ant) {
+    Pool p;
+    check(bf_serve_pool(server_, n_ant, &p.data, &p.spectra, &p.channels));
+    return p;
+}
+
 }  // namespace beamformer

@@ -89,6 +89,14 @@ public:
     ServedStats stats();
     std::vector<float> window_times_ms();
     void* stream();                       // cudaStream_t of the server
+    // Ingest hook: the device pool that jobs of n_ant antennas read,
+    // [spectra][channels][n_ant] packed bytes.  A capture stage writes rows
+    // there in stream order on stream() before the step that reads them.
+    struct Pool {
+        std::uint8_t* data = nullptr;
+        std::uint64_t spectra = 0, channels = 0;
+    };
+    Pool pool(std::uint64_t n_ant);
 
 private:
     bf_server* server_ = nullptr;

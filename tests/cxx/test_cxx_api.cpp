@@ -334,6 +334,11 @@ int main() {
         expect(positive && ga.size() == 2 * 64 * 336 * 8, "served grid job produces finite powers");
         expect(ga == gm && ta == tm, "served jobs are bit-identical alone and in a mix");
         ServedBeamformer srv(sc);
+        const auto pool64 = srv.pool(64);
+        expect(pool64.data != nullptr && pool64.spectra == sc.pool_spectra &&
+                   pool64.channels == static_cast<std::uint64_t>(sc.shard_channels) * sc.max_shards,
+               "served pool geometry");
+        expect(throws<std::invalid_argument>([&] { srv.pool(48); }), "served pool needs 32 or 64 antennas");
         ServedJob big = g;
         big.n_spectra = 320 * 100000;
         expect(throws<std::length_error>([&] { srv.submit(big); }), "oversize served job is a length_error");
