@@ -82,21 +82,29 @@ __device__ __forceinline__ void cov_grid_error(unsigned* err, unsigned code) {
     if (err != nullptr) atomicOr(err, 0x80000000u | (code << 16));
 }
 
-struct CovUnit {
-    int s, f, w, key;
+// A CTA's pair-units in order -- the windows of a channel pair, then the next
+// pair, then the next shard -- without a division per unit.
+struct CovCursor {
+    int s, fp, w;
+    __device__ __forceinline__ void start(long long pu, const CovGridParams& p) {
+        const long long per_shard = static_cast<long long>(p.n_freq / 2) * p.n_windows;
+        s = static_cast<int>(pu / per_shard);
+        const long long r = pu % per_shard;
+        fp = static_cast<int>(r / p.n_windows);
+        w = static_cast<int>(r % p.n_windows);
+    }
+    __device__ __forceinline__ void next(const CovGridParams& p) {
+        if (++w == p.n_windows) {
+            w = 0;
+            if (++fp == p.n_freq / 2) {
+                fp = 0;
+                ++s;
+            }
+        }
+    }
+    // the channel (and its weight image) changes after this unit
+    __device__ __forceinline__ bool ends_run(const CovGridParams& p) const { return w + 1 == p.n_windows; }
 };
-
-__device__ __forceinline__ CovUnit cov_unit(long long pu, int odd, const CovGridParams& p) {
-    const int pairs = p.n_freq / 2;
-    const long long per_shard = static_cast<long long>(pairs) * p.n_windows;
-    CovUnit u;
-    u.s = static_cast<int>(pu / per_shard);
-    const long long r = pu % per_shard;
-    u.w = static_cast<int>(r % p.n_windows);
-    u.f = 2 * static_cast<int>(r / p.n_windows) + odd;
-    u.key = u.s * p.n_freq + u.f;
-    return u;
-}
 
 __device__ __forceinline__ int cov_tiles(int w, const CovGridParams& p) {
     const int len = min(p.spectra, p.n_time - w * p.spectra);
@@ -187,30 +195,31 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
             uint32_t phase = 0;
             int armed[kRawStages];
             for (int s = 0; s < kRawStages; ++s) armed[s] = -1;
-            int prev_key = -1, runs = 0;
+            int runs = 0;
             bool stop = false;
-            for (long long pu = u_begin; pu < u_end && !stop; ++pu) {
-                const CovUnit un = cov_unit(pu, odd, p);
-                const int nt = cov_tiles(un.w, p);
+            CovCursor cur;
+            cur.start(u_begin, p);
+            for (long long pu = u_begin; pu < u_end && !stop; ++pu, cur.next(p)) {
+                const int f = 2 * cur.fp + odd;
+                const int nt = cov_tiles(cur.w, p);
                 for (int k = 0; k < nt; ++k) {
                     if (*s_fail) { stop = true; break; }
                     if (!mbar_wait(&raw_empty[stage], phase ^ 1, kWaitNs)) { fail(1); stop = true; break; }
                     mbar_expect_tx(&raw_full[stage], kRawBytes);  // rows past the stream arrive zero filled
-                    tma_load_4d(raw + stage * kRawBytes, &vmap, 0, un.f, un.w * p.spectra + k * kRows, un.s,
+                    tma_load_4d(raw + stage * kRawBytes, &vmap, 0, f, cur.w * p.spectra + k * kRows, cur.s,
                                 &raw_full[stage]);
                     armed[stage] = static_cast<int>(phase);
                     if (++stage == kRawStages) { stage = 0; phase ^= 1; }
                 }
                 if (stop) break;
-                if (un.key != prev_key) {
+                if (pu == u_begin || cur.w == 0) {
                     // after this unit's tiles, so the MMA can run its Gram while the
                     // previous channel's last beam sums finish
                     if (runs > 0 && !mbar_wait(w_empty, (runs - 1) & 1, kWaitNs)) { fail(2); break; }
                     mbar_expect_tx(w_full, kWImage);
-                    const uint8_t* src = p.wimg + static_cast<size_t>(un.key) * kWImage;
+                    const uint8_t* src = p.wimg + (static_cast<size_t>(cur.s) * p.n_freq + f) * kWImage;
                     for (uint32_t c = 0; c < kWImage; c += 32768) bulk_g2s(wsm + c, src + c, 32768, w_full);
                     ++runs;
-                    prev_key = un.key;
                 }
             }
             for (int s = 0; s < kRawStages; ++s) {
@@ -223,11 +232,14 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
             int xst = 0;
             uint32_t xph = 0;
             bool stop = false;
-            int runs = 0, prev_key = -1;
+            int runs = 0;
             // the quad of unit j - 1 is issued after the Gram of unit j
             long long q_idx = -1;
-            bool q_first = false;
-            int q_run = 0, q_key = -1;
+            bool q_first = false, q_ends = false;
+            int q_run = 0;
+            const uint64_t w_hi_desc = smem_desc_sw128(smem_u32(wsm));
+            const uint64_t w_lo_desc = smem_desc_sw128(smem_u32(wsm) + kWHalf);
+            const uint64_t x_desc = smem_desc_sw128_mn(smem_u32(xs));
             auto issue_quad = [&](long long i, bool first, bool last, int run) -> bool {
                 const int eb = static_cast<int>(i & 1);
                 const uint32_t par = static_cast<uint32_t>((i >> 1) & 1);
@@ -237,13 +249,12 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
                 if (first && !mbar_wait(w_full, static_cast<uint32_t>(run & 1), kWaitNs)) { fail(7); return false; }
                 tc_fence_after();
                 const uint32_t e_tm = tmem_base + eb * 128, y_tm = tmem_base + kYCol + eb * 128;
-                const uint32_t w_hi = smem_u32(wsm), w_lo = w_hi + kWHalf;
 #pragma unroll
                 for (int kk = 0; kk < 8; ++kk) {
                     const uint32_t a_hi = e_tm + 32 * (kk >> 1) + 8 * (kk & 1), a_lo = a_hi + 16;
-                    const uint32_t kb = kk >> 2, koff = (kk & 3) * 32;
-                    const uint64_t bh = smem_desc_sw128(w_hi + kb * (128 * 128) + koff);
-                    const uint64_t bl = smem_desc_sw128(w_lo + kb * (128 * 128) + koff);
+                    // descriptor start addresses advance in 16-byte units
+                    const uint64_t off = ((kk >> 2) * (128 * 128) + (kk & 3) * 32) >> 4;
+                    const uint64_t bh = w_hi_desc + off, bl = w_lo_desc + off;
                     mma_f16_ts(y_tm, a_hi, bh, IDESC_Q, kk > 0 ? 1u : 0u);
                     mma_f16_ts(y_tm, a_hi, bl, IDESC_Q, 1u);
                     mma_f16_ts(y_tm, a_lo, bh, IDESC_Q, 1u);
@@ -253,13 +264,11 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
                 return true;
             };
             long long j = 0;
-            for (long long pu = u_begin; pu < u_end && !stop; ++pu, ++j) {
-                const CovUnit un = cov_unit(pu, odd, p);
-                const bool first = un.key != prev_key;
-                if (first) {
-                    ++runs;
-                    prev_key = un.key;
-                }
+            CovCursor cur;
+            cur.start(u_begin, p);
+            for (long long pu = u_begin; pu < u_end && !stop; ++pu, ++j, cur.next(p)) {
+                const bool first = pu == u_begin || cur.w == 0;
+                if (first) ++runs;
                 const int eb = static_cast<int>(j & 1);
                 // E[eb] was last read by the quad of unit j - 2, issued just before:
                 // waiting for it lets the tensor pipe drain once per unit
@@ -269,15 +278,14 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
                 }
                 tc_fence_after();
                 const uint32_t e_tm = tmem_base + eb * 128;
-                const int nt = cov_tiles(un.w, p);
+                const int nt = cov_tiles(cur.w, p);
                 for (int k = 0; k < nt; ++k) {
                     if (*s_fail) { stop = true; break; }
                     if (!mbar_wait(&x_full[xst], xph, kWaitNs)) { fail(9); stop = true; break; }
                     tc_fence_after();
-                    const uint32_t xa = smem_u32(xs + xst * kXBytes);
 #pragma unroll
                     for (int kk = 0; kk < kRows / 32; ++kk) {
-                        const uint64_t desc = smem_desc_sw128_mn(xa + kk * 32 * 128);
+                        const uint64_t desc = x_desc + ((xst * kXBytes + kk * 32 * 128) >> 4);
                         mma_i8_ss(e_tm, desc, desc, IDESC_G, (k > 0 || kk > 0) ? 1u : 0u);
                     }
                     tc_commit(&x_empty[xst]);
@@ -285,11 +293,11 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
                 }
                 if (stop) break;
                 tc_commit(&gram_done[eb]);
-                if (q_idx >= 0 && !issue_quad(q_idx, q_first, q_key != un.key, q_run)) { stop = true; break; }
+                if (q_idx >= 0 && !issue_quad(q_idx, q_first, q_ends, q_run)) { stop = true; break; }
                 q_idx = j;
                 q_first = first;
                 q_run = runs - 1;
-                q_key = un.key;
+                q_ends = cur.ends_run(p);
             }
             if (!stop && q_idx >= 0) issue_quad(q_idx, q_first, true, q_run);
             tc_commit(mma_done);
@@ -302,9 +310,10 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
         int stage = 0, xst = 0;
         uint32_t phase = 0, xph = 0;
         bool stop = false;
-        for (long long pu = u_begin; pu < u_end && !stop; ++pu) {
-            const CovUnit un = cov_unit(pu, odd, p);
-            const int nt = cov_tiles(un.w, p);
+        CovCursor cur;
+        cur.start(u_begin, p);
+        for (long long pu = u_begin; pu < u_end && !stop; ++pu, cur.next(p)) {
+            const int nt = cov_tiles(cur.w, p);
             for (int k = 0; k < nt; ++k) {
                 if (*s_fail) { stop = true; break; }
                 if (!mbar_wait(&raw_full[stage], phase, kWaitNs)) { fail(11); stop = true; break; }
@@ -379,9 +388,10 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
         const int t = 32 * (warp - kDotFirst) + lane;  // output beam of the final sum
         const float* vt = reinterpret_cast<const float*>(wsm + 2 * kWHalf);  // [beam][component]
         long long j = 0;
-        for (long long pu = u_begin; pu < u_end; ++pu, ++j) {
-            const CovUnit un = cov_unit(pu, odd, p);
-            const bool last = pu + 1 == u_end || cov_unit(pu + 1, odd, p).key != un.key;
+        CovCursor cur;
+        cur.start(u_begin, p);
+        for (long long pu = u_begin; pu < u_end; ++pu, ++j, cur.next(p)) {
+            const bool last = pu + 1 == u_end || cur.ends_run(p);
             const int eb = static_cast<int>(j & 1);
             if (!mbar_wait(&quad_done[eb], static_cast<uint32_t>((j >> 1) & 1), kWaitNs)) { fail(14); break; }
             tc_fence_after();
@@ -409,7 +419,7 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
             named_barrier(1, 32 * kDotWarps);
             const float sum = ((sd[t] + sd[128 + t]) + sd[256 + t]) + sd[384 + t];
             if (t < p.n_beams) {
-                p.out[((static_cast<size_t>(un.s) * p.n_windows + un.w) * p.n_freq + un.f) * p.n_beams + t] =
+                p.out[((static_cast<size_t>(cur.s) * p.n_windows + cur.w) * p.n_freq + 2 * cur.fp + odd) * p.n_beams + t] =
                     sum * p.out_scale;
             }
             if (*s_fail) break;
