@@ -147,20 +147,6 @@ struct Unit {
     int key;  // (job, shard, channel): identifies the weight image
 };
 
-__device__ __forceinline__ Unit unit_of(const TcJob& jb, int job, long long u) {
-    Unit r;
-    const long long local = u - jb.unit_begin;
-    const long long per_shard = static_cast<long long>(jb.n_freq) * jb.groups_per_channel;
-    r.shard = static_cast<int>(local / per_shard);
-    const long long rem = local % per_shard;
-    r.f = static_cast<int>(rem / jb.groups_per_channel);
-    const int g = static_cast<int>(rem % jb.groups_per_channel);
-    r.tile_begin = g * jb.group_tiles;
-    r.tile_end = min(r.tile_begin + jb.group_tiles, jb.tiles_per_channel);
-    r.key = (job << 16) + r.shard * jb.n_freq + r.f;
-    return r;
-}
-
 // Walks the units of a CTA's contiguous range in order, tracking which job
 // each belongs to (a plain launch has the single job p.job).
 template <bool kServed>
@@ -194,28 +180,49 @@ struct JobCursor {
     // each line once.  u then counts (shard, channel pair, group).
     int pair_parity = -1;
 
+    // The decomposition of the last unit returned: every role walks its range
+    // one unit at a time, so the next unit comes from a carry chain instead of
+    // four 64-bit divisions (a full decode only at a job change or a jump).
+    long long last_u = -2;
+    int d_shard = 0, d_ch = 0, d_g = 0;  // d_ch: channel, or channel pair when paired
+
     __device__ __forceinline__ Unit at(long long u) {
+        bool full = u != last_u + 1;
         if constexpr (kServed) {
             while (u >= next_begin) {
                 ++j;
                 jb = jobs[j];
                 next_begin = j + 1 < n_jobs ? jobs[j + 1].unit_begin : LLONG_MAX;
-            }
-        } else {
-            if (pair_parity >= 0) {
-                Unit r;
-                const int half_f = jb.n_freq / 2;
-                const long long pi = u / jb.groups_per_channel;
-                const int g = static_cast<int>(u % jb.groups_per_channel);
-                r.shard = static_cast<int>(pi / half_f);
-                r.f = 2 * static_cast<int>(pi % half_f) + pair_parity;
-                r.tile_begin = g * jb.group_tiles;
-                r.tile_end = min(r.tile_begin + jb.group_tiles, jb.tiles_per_channel);
-                r.key = r.shard * jb.n_freq + r.f;
-                return r;
+                full = true;
             }
         }
-        return unit_of(jb, j, u);
+        const int chans = pair_parity >= 0 ? jb.n_freq / 2 : jb.n_freq;
+        if (u == last_u && !full) {
+            // same unit again
+        } else if (!full) {
+            if (++d_g == jb.groups_per_channel) {
+                d_g = 0;
+                if (++d_ch == chans) {
+                    d_ch = 0;
+                    ++d_shard;
+                }
+            }
+        } else {
+            const long long local = u - (kServed ? jb.unit_begin : 0);
+            const long long per_shard = static_cast<long long>(chans) * jb.groups_per_channel;
+            d_shard = static_cast<int>(local / per_shard);
+            const long long rem = local % per_shard;
+            d_ch = static_cast<int>(rem / jb.groups_per_channel);
+            d_g = static_cast<int>(rem % jb.groups_per_channel);
+        }
+        last_u = u;
+        Unit r;
+        r.shard = d_shard;
+        r.f = pair_parity >= 0 ? 2 * d_ch + pair_parity : d_ch;
+        r.tile_begin = d_g * jb.group_tiles;
+        r.tile_end = min(r.tile_begin + jb.group_tiles, jb.tiles_per_channel);
+        r.key = (j << 16) + r.shard * jb.n_freq + r.f;
+        return r;
     }
 };
 
