@@ -534,13 +534,17 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                     if (!mbar_wait(&acc_empty[acc_stage], acc_phase ^ 1, kWaitNs)) { fail(16); stop = true; break; }
                     tc_fence_after();
                     const uint32_t d_tmem = tmem_base + acc_stage * ACC_COLS;
-                    const uint32_t x_addr = smem_u32(xs + xs_stage * S.x_bytes);
+                    // descriptors once per tile; the start address field (bits 0-13,
+                    // 16-byte units) then advances by plain adds (shared addresses stay
+                    // below 2^18 bytes, so the field never carries)
+                    const uint64_t a0 = smem_desc_sw128(smem_u32(xs + xs_stage * S.x_bytes));
+                    const uint64_t bh0 = smem_desc_sw128(w_hi_addr), bl0 = smem_desc_sw128(w_lo_addr);
 #pragma unroll
                     for (int kk = 0; kk < K / 16; ++kk) {
                         const uint32_t kb = kk / 4, koff = (kk % 4) * 32;
-                        const uint64_t a = smem_desc_sw128(x_addr + kb * (kTileM * 128) + koff);
-                        const uint64_t bh = smem_desc_sw128(w_hi_addr + kb * (N * 128) + koff);
-                        const uint64_t bl = smem_desc_sw128(w_lo_addr + kb * (N * 128) + koff);
+                        const uint64_t a = a0 + ((kb * (kTileM * 128) + koff) >> 4);
+                        const uint64_t bh = bh0 + ((kb * (N * 128) + koff) >> 4);
+                        const uint64_t bl = bl0 + ((kb * (N * 128) + koff) >> 4);
                         mma_f16_ss(d_tmem, a, bh, IDESC, kk > 0 ? 1u : 0u);
                         mma_f16_ss(d_tmem, a, bl, IDESC, 1u);
                     }
