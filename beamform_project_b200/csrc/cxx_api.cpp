@@ -61,6 +61,7 @@ int to_c(CudaBeamformerKernel k) {
         case CudaBeamformerKernel::Direct: return BF_KERNEL_DIRECT;
         case CudaBeamformerKernel::Tiled: return BF_KERNEL_TILED;
         case CudaBeamformerKernel::TensorSplit: return BF_KERNEL_TENSOR;
+        case CudaBeamformerKernel::TensorCovariance: break;  // its own entry points
     }
     throw std::invalid_argument("unknown CUDA beamformer kernel selector");
 }
@@ -69,6 +70,13 @@ int to_c(CudaBeamformerKernel k) {
 void validate_cuda_temporal_integration(CudaBeamformerKernel kernel, const TemporalIntegrationConfig& t) {
     validate_temporal_config(t);
     const std::size_t s = t.integration_spectra;
+    if (kernel == CudaBeamformerKernel::TensorCovariance) {
+        if (s < 64 || s % 64 != 0 || s > 16384) {
+            throw std::invalid_argument(
+                "the TensorCovariance kernel needs integration spectra a multiple of 64, at most 16384");
+        }
+        return;
+    }
     if (kernel == CudaBeamformerKernel::TensorSplit) {
         if (s > 32 && s % 32 != 0) {
             throw std::invalid_argument(
@@ -134,8 +142,8 @@ std::size_t weight_storage_count(const Dimensions& dims, CudaBeamformerKernel ke
 void launch_packed_beamformer(CudaBeamformerKernel kernel, cudaStream_t stream, const std::uint8_t* packed_voltage,
                               const ComplexFloat* weights, float* intensity, const Dimensions& dims) {
     validate_dimensions(dims);
-    if (kernel == CudaBeamformerKernel::TensorSplit) {
-        throw std::invalid_argument("the TensorSplit kernel produces integrated output only");
+    if (kernel == CudaBeamformerKernel::TensorSplit || kernel == CudaBeamformerKernel::TensorCovariance) {
+        throw std::invalid_argument("the tensor-core kernels produce integrated output only");
     }
     const bf_dims d = to_c(dims);
     check(bf_launch_packed_beamformer(to_c(kernel), stream, packed_voltage,
@@ -149,6 +157,12 @@ void launch_packed_integrated_beamformer(CudaBeamformerKernel kernel, cudaStream
     validate_dimensions(dims);
     validate_cuda_temporal_integration(kernel, temporal_integration);
     const bf_dims d = to_c(dims);
+    if (kernel == CudaBeamformerKernel::TensorCovariance) {
+        // `weights` is the operand prepared by prepare_cov_weights
+        check(bf_grid_cov_integrated(stream, packed_voltage, weights, integrated_intensity, nullptr, nullptr, &d,
+                                     temporal_integration.integration_spectra, 1));
+        return;
+    }
     if (kernel == CudaBeamformerKernel::TensorSplit) {
         // `weights` is the operand prepared by prepare_split_weights
         check(bf_grid_tensor_integrated(stream, packed_voltage, weights, integrated_intensity, nullptr, nullptr, &d,
@@ -189,6 +203,17 @@ void prepare_split_weights(cudaStream_t stream, const ComplexFloat* weights, voi
     check(bf_prepare_split_weights(stream, reinterpret_cast<const float*>(weights), split_weights, &d, 1));
 }
 
+std::size_t cov_weight_bytes(const Dimensions& dims) {
+    const bf_dims d = to_c(dims);
+    return static_cast<std::size_t>(bf_cov_weight_bytes(&d, 1));
+}
+
+void prepare_cov_weights(cudaStream_t stream, const ComplexFloat* weights, void* cov_weights,
+                         const Dimensions& dims) {
+    const bf_dims d = to_c(dims);
+    check(bf_prepare_cov_weights(stream, reinterpret_cast<const float*>(weights), cov_weights, &d, 1));
+}
+
 CudaDeviceInfo cuda_device_info() {
     CudaDeviceInfo info;
     char name[256];
@@ -211,7 +236,7 @@ struct CudaBeamformerWorkspace::Impl {
     CudaBeamformerOutput output;
     DeviceBuffer<std::uint8_t> voltage;
     DeviceBuffer<ComplexFloat> weights;     // canonical or tiled
-    DeviceBuffer<std::uint8_t> split;       // TensorSplit operand
+    DeviceBuffer<std::uint8_t> split;       // TensorSplit / TensorCovariance operand
     DeviceBuffer<float> intensity;          // per-spectrum output
     DeviceBuffer<float> integrated;
     DeviceBuffer<std::int8_t> codes;
@@ -226,9 +251,10 @@ struct CudaBeamformerWorkspace::Impl {
          CudaBeamformerOutput o)
         : capacity(cap), kernel(k), temporal(t), output(o), voltage(voltage_sample_count(cap)) {
         check_cuda(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
-        if (kernel == CudaBeamformerKernel::TensorSplit) {
+        if (tensor()) {
             weights = DeviceBuffer<ComplexFloat>(cap.n_beams * cap.n_freq * cap.n_ant);
-            split = DeviceBuffer<std::uint8_t>(split_weight_bytes(cap));
+            split = DeviceBuffer<std::uint8_t>(kernel == CudaBeamformerKernel::TensorSplit ? split_weight_bytes(cap)
+                                                                                          : cov_weight_bytes(cap));
         } else {
             weights = DeviceBuffer<ComplexFloat>(weight_storage_count(cap, kernel));
         }
@@ -247,6 +273,9 @@ struct CudaBeamformerWorkspace::Impl {
         if (stream) cudaStreamDestroy(stream);
     }
 
+    bool tensor() const {
+        return kernel == CudaBeamformerKernel::TensorSplit || kernel == CudaBeamformerKernel::TensorCovariance;
+    }
     void validate_request(const Dimensions& dims) const {
         validate_dimensions(dims);
         if (dims.n_freq != capacity.n_freq || dims.n_ant != capacity.n_ant || dims.n_time > capacity.n_time ||
@@ -255,8 +284,7 @@ struct CudaBeamformerWorkspace::Impl {
         }
     }
     std::size_t required_weights(const Dimensions& dims) const {
-        return kernel == CudaBeamformerKernel::TensorSplit ? dims.n_beams * dims.n_freq * dims.n_ant
-                                                           : weight_storage_count(dims, kernel);
+        return tensor() ? dims.n_beams * dims.n_freq * dims.n_ant : weight_storage_count(dims, kernel);
     }
     void require_weights(const Dimensions& dims) const {
         if (loaded_weights != required_weights(dims)) {
@@ -275,7 +303,9 @@ struct CudaBeamformerWorkspace::Impl {
     // Launch the configured beamformer into the configured output buffer.
     void launch(const Dimensions& dims, const std::uint8_t* v, const void* w, float* out) {
         const bf_dims d = to_c(dims);
-        if (kernel == CudaBeamformerKernel::TensorSplit) {
+        if (kernel == CudaBeamformerKernel::TensorCovariance) {
+            check(bf_grid_cov_integrated(stream, v, w, out, nullptr, nullptr, &d, temporal->integration_spectra, 1));
+        } else if (kernel == CudaBeamformerKernel::TensorSplit) {
             // per-spectrum output is integration over one spectrum ([T][F][B] == [W][F][B])
             check(bf_grid_tensor_integrated(stream, v, w, out, nullptr, nullptr, &d,
                                             temporal ? temporal->integration_spectra : 1, 1));
@@ -287,8 +317,16 @@ struct CudaBeamformerWorkspace::Impl {
         }
     }
     const void* weight_operand() const {
-        return kernel == CudaBeamformerKernel::TensorSplit ? static_cast<const void*>(split.ptr)
-                                                           : static_cast<const void*>(weights.ptr);
+        return tensor() ? static_cast<const void*>(split.ptr) : static_cast<const void*>(weights.ptr);
+    }
+    // canonical weights on the device -> the tensor kernels' operand
+    void prepare_operand(const void* canonical, const Dimensions& dims) {
+        const bf_dims d = to_c(dims);
+        if (kernel == CudaBeamformerKernel::TensorSplit) {
+            check(bf_prepare_split_weights(stream, static_cast<const float*>(canonical), split.ptr, &d, 1));
+        } else if (kernel == CudaBeamformerKernel::TensorCovariance) {
+            check(bf_prepare_cov_weights(stream, static_cast<const float*>(canonical), split.ptr, &d, 1));
+        }
     }
 };
 
@@ -302,6 +340,12 @@ CudaBeamformerWorkspace::CudaBeamformerWorkspace(const Dimensions& capacity, Cud
     }
     if (kernel == CudaBeamformerKernel::TensorSplit && capacity.n_ant > 64) {
         throw std::invalid_argument("the TensorSplit kernel supports n_ant 32 or 64");
+    }
+    if (kernel == CudaBeamformerKernel::TensorCovariance) {
+        if (capacity.n_ant != 64) throw std::invalid_argument("the TensorCovariance kernel supports n_ant 64");
+        if (!temporal_integration) {
+            throw std::invalid_argument("the TensorCovariance kernel produces integrated output only");
+        }
     }
     const auto t0 = std::chrono::steady_clock::now();
     impl_ = std::make_unique<Impl>(capacity, kernel, temporal_integration, output);
@@ -342,10 +386,7 @@ double CudaBeamformerWorkspace::upload_weights(const Weights& weights, const Dim
     check_cuda(cudaMemcpyAsync(m.weights.ptr, weights.data(), n * sizeof(ComplexFloat), cudaMemcpyHostToDevice,
                                m.stream),
                "cudaMemcpyAsync weights");
-    if (m.kernel == CudaBeamformerKernel::TensorSplit) {
-        const bf_dims d = to_c(dims);
-        check(bf_prepare_split_weights(m.stream, reinterpret_cast<const float*>(m.weights.ptr), m.split.ptr, &d, 1));
-    }
+    m.prepare_operand(m.weights.ptr, dims);
     check_cuda(cudaEventRecord(m.transfer_end.e, m.stream), "cudaEventRecord");
     check_cuda(cudaEventSynchronize(m.transfer_end.e), "cudaEventSynchronize");
     m.loaded_weights = n;
@@ -591,9 +632,8 @@ CudaBeamformerTimings CudaBeamformerWorkspace::run_device_frame(const CudaFrameV
     const void* w = weights.buffer.device_data;
     CudaBeamformerTimings t;
     check_cuda(cudaEventRecord(m.start.e, m.stream), "cudaEventRecord");
-    if (m.kernel == CudaBeamformerKernel::TensorSplit) {
-        const bf_dims d = to_c(dims);
-        check(bf_prepare_split_weights(m.stream, static_cast<const float*>(w), m.split.ptr, &d, 1));
+    if (m.tensor()) {
+        m.prepare_operand(w, dims);
         w = m.split.ptr;
     }
     check_cuda(cudaEventRecord(m.transfer_end.e, m.stream), "cudaEventRecord");

@@ -28,6 +28,11 @@ enum class CudaBeamformerKernel {
     Direct,
     Tiled,
     TensorSplit,
+    // Opt-in covariance form (integrated output only, 64 antennas, integration a
+    // multiple of 64 spectra up to 16384): each window's power from its exact
+    // INT32 covariance.  Its relative error grows for beams far below the
+    // strongest source's power; TensorSplit has no such dependence.
+    TensorCovariance,
 };
 
 void launch_packed_beamformer(CudaBeamformerKernel kernel, cudaStream_t stream,
@@ -61,5 +66,11 @@ std::size_t split_weight_bytes(const Dimensions& dims);
 // Canonical device weights -> TensorSplit operand (device, split_weight_bytes).
 void prepare_split_weights(cudaStream_t stream, const ComplexFloat* weights, void* split_weights,
                            const Dimensions& dims);
+
+// Bytes of the TensorCovariance weight operand for `dims` (one shard), and the
+// conversion from canonical device weights.
+std::size_t cov_weight_bytes(const Dimensions& dims);
+void prepare_cov_weights(cudaStream_t stream, const ComplexFloat* weights, void* cov_weights,
+                         const Dimensions& dims);
 
 }  // namespace beamformer

@@ -200,6 +200,20 @@ int main() {
             expect(ok10, "TensorSplit 10-spectrum integration within tolerance");
         }
         {
+            // covariance form: same window sums, within the split kernel's bar
+            CudaBeamformerWorkspace wc(di, CudaBeamformerKernel::TensorCovariance, integration_direct);
+            wc.upload_weights(wi, di);
+            IntegratedIntensities oc(integ.size());
+            wc.run_integrated_pipeline(vi, oc, di);
+            bool okc = true;
+            for (std::size_t i = 0; i < oc.size(); ++i) okc &= std::abs(oc[i] - integ[i]) <= 1e-3F + 1e-5F * std::abs(integ[i]);
+            expect(okc, "TensorCovariance workspace within tolerance");
+            expect(throws<std::invalid_argument>([&] { CudaBeamformerWorkspace x(di, CudaBeamformerKernel::TensorCovariance); }),
+                   "TensorCovariance needs integration");
+            expect(throws<std::invalid_argument>([&] { CudaBeamformerWorkspace x(di, CudaBeamformerKernel::TensorCovariance, integration_after_upchan); }),
+                   "TensorCovariance rejects 10-spectrum integration");
+        }
+        {
             // chunked host pipeline: bit-identical to the one-launch TensorSplit workspace
             CudaBeamformerWorkspace wq(di, CudaBeamformerKernel::TensorSplit, integration_direct,
                                        CudaBeamformerOutput::QuantizedInt8);

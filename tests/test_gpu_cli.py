@@ -96,6 +96,18 @@ def test_tensor_kernel_within_split_precision_bar(cuda, orc, tmp_path):
 
 
 @pytest.mark.gpu
+def test_covariance_kernel_within_bar(cuda, orc, tmp_path):
+    v, w, paths = _files(tmp_path)
+    out = tmp_path / "cov.f32"
+    r = _run(CLI, *_common(paths), "--output", out, "--kernel", "covariance", "--integration-spectra", 320)
+    assert r.returncode == 0, r.stderr
+    assert "kernel=covariance" in r.stdout
+    got = np.fromfile(out, np.float32).reshape(T // 320, F, B).astype(np.float64)
+    exp = orc.beamform_integrated(v, w, T, F, A, B, 320, f64=True)
+    assert np.all(np.abs(got - exp) <= 1e-3 + 1e-5 * np.abs(exp))
+
+
+@pytest.mark.gpu
 def test_errors_exit_one_with_message(cuda, tmp_path):
     _, _, paths = _files(tmp_path)
     r = _run(CLI, *_common(paths), "--output", tmp_path / "x", "--output-format", "int8")
