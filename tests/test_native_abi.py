@@ -130,3 +130,18 @@ def test_python_api_checks_buffers_without_gpu():
     assert api.quantization_layout(api.Dimensions(103, 336, 64, 128)) == (103, 21, 8)
     with pytest.raises(api.InvalidArgument):
         api.integrated_time_count(10, 0)
+
+
+def test_host_buffer_checks_without_gpu():
+    """The host-buffer pipeline's Python wrapper checks dtype, layout and size
+    of host arrays before any call into the library."""
+    import numpy as np
+    from beamform_project_b200 import api
+    a = np.zeros(64, np.uint8)
+    assert api._host(a, "v", np.uint8, 64) == a.ctypes.data
+    with pytest.raises(api.InvalidArgument, match="smaller than dimensions"):
+        api._host(a, "v", np.uint8, 65)
+    with pytest.raises(api.InvalidArgument, match="contiguous"):
+        api._host(np.zeros(64, np.float32), "v", np.uint8, 1)
+    with pytest.raises(api.InvalidArgument, match="contiguous"):
+        api._host(np.zeros((8, 8), np.uint8)[:, ::2], "v", np.uint8, 1)

@@ -280,3 +280,5 @@ def test_pool_hook_checks_arguments():
         assert native.lib().bf_serve_pool(srv._h, 64, C.byref(ptr), None, None) == 2
         assert "host-only" in native.last_error()
         assert native.lib().bf_serve_pool(None, 64, C.byref(ptr), None, None) == 1
+        with pytest.raises(native.LogicError, match="host-only"):
+            srv.pool(64)
