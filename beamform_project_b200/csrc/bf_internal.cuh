@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <mutex>
 #include <string>
 
 #include "../../include/bf_b200.h"
@@ -27,6 +28,47 @@ inline bf_status cuda_status(cudaError_t err, const char* what) {
 
 // validate_dimensions (include/beamformer/config.hpp:81-94).
 bf_status validate_dims(const bf_dims* dims);
+
+// Device address of a file-scope __device__ variable on the current device.
+// In host code the variable's name is only a host-side stand-in, so its
+// device address is looked up with cudaGetSymbolAddress.  The lookup runs
+// again on every call made while `stream` is not capturing: a cudaDeviceReset
+// (or any teardown of the primary context) reloads the module, possibly at
+// another address, and a cached pointer would then send the kernel to freed
+// memory.  While `stream` captures, the last address found on this device is
+// used (the lookup may load the module, which capture forbids), so the first
+// call on a device, and the first after a reset, must come before any
+// capture.
+struct SymbolAddressCache {
+    static constexpr int kMaxDevices = 64;
+    std::mutex mu;
+    void* addr[kMaxDevices] = {};
+};
+
+inline bf_status device_symbol_address(const void* symbol, SymbolAddressCache& cache, cudaStream_t stream,
+                                       void** out, const char* what) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_status(e, "cudaGetDevice");
+    if (dev < 0 || dev >= SymbolAddressCache::kMaxDevices) {
+        return set_error(BF_ERR_UNSUPPORTED, std::string("device ordinal beyond the address table of ") + what);
+    }
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(stream, &capture);
+    if (e != cudaSuccess) return cuda_status(e, "cudaStreamIsCapturing");
+    std::lock_guard<std::mutex> lock(cache.mu);
+    if (capture == cudaStreamCaptureStatusNone) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, symbol);
+        if (e != cudaSuccess) return cuda_status(e, (std::string("cudaGetSymbolAddress(") + what + ")").c_str());
+        cache.addr[dev] = p;
+    } else if (cache.addr[dev] == nullptr) {
+        return set_error(BF_ERR_INVALID_ARGUMENT,
+                         std::string("the first call on a device must come before stream capture (") + what + ")");
+    }
+    *out = cache.addr[dev];
+    return BF_OK;
+}
 
 inline uint64_t window_count(uint64_t n_time, uint64_t spectra) {
     return n_time / spectra + (n_time % spectra == 0 ? 0 : 1);
@@ -195,7 +237,9 @@ uint64_t split_weight_bytes(const bf_dims& d, uint64_t n_shards, int nb_pad = 0)
 bf_status launch_prepare_split(cudaStream_t stream, const float* w, void* split, const bf_dims& d,
                                uint64_t n_shards, int nb_pad = 0);
 bf_status take_tc_error(uint32_t* code);
-unsigned* device_error_word();
+// Device address of the error word (grid_tc.cu) for kernels in other
+// translation units; null when it cannot be found (bf_last_error says why).
+unsigned* device_error_word(cudaStream_t stream);
 // covariance-form grid (grid_cov.cu)
 uint64_t cov_weight_bytes(const bf_dims& d, uint64_t n_shards);
 bf_status check_grid_cov(const bf_dims& d, uint64_t spectra, uint64_t n_shards);

@@ -424,7 +424,8 @@ bf_status launch_doa_covariance(cudaStream_t stream, const uint8_t* v, int32_t* 
     if (r != CUDA_SUCCESS) return set_error(BF_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string(r));
     CovParams p{};
     p.out = out;
-    p.err = device_error_word();
+    p.err = device_error_word(stream);
+    if (p.err == nullptr) return BF_ERR_CUDA;
     p.n_freq = static_cast<int>(d.n_freq);
     p.n_ant = static_cast<int>(d.n_ant);
     p.block_len = static_cast<int>(block_len);

@@ -526,7 +526,8 @@ bf_status launch_grid_cov(cudaStream_t stream, const uint8_t* v, const void* wim
     CovGridParams p{};
     p.wimg = static_cast<const uint8_t*>(wimg);
     p.out = integrated;
-    p.err = device_error_word();
+    p.err = device_error_word(stream);
+    if (p.err == nullptr) return BF_ERR_CUDA;
     p.n_freq = static_cast<int>(d.n_freq);
     p.n_beams = static_cast<int>(d.n_beams);
     p.n_windows = static_cast<int>(window_count(d.n_time, spectra));

@@ -1058,18 +1058,11 @@ bf_status launch_grid_tensor_served(cudaStream_t stream, const CUtensorMap& map,
 
 // Device address of the error word for kernels in other translation units
 // (device globals are per translation unit without relocatable device code).
-unsigned* device_error_word() {
-    static std::mutex mu;
-    static unsigned* addr[64] = {};
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
-    std::lock_guard<std::mutex> lock(mu);
-    if (addr[dev] == nullptr) {
-        void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_tc_error) != cudaSuccess) return nullptr;
-        addr[dev] = static_cast<unsigned*>(p);
-    }
-    return addr[dev];
+unsigned* device_error_word(cudaStream_t stream) {
+    static SymbolAddressCache cache;
+    void* p = nullptr;
+    if (device_symbol_address(&g_tc_error, cache, stream, &p, "device error word") != BF_OK) return nullptr;
+    return static_cast<unsigned*>(p);
 }
 
 bf_status take_tc_error(uint32_t* code) {

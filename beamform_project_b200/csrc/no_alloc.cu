@@ -11,8 +11,6 @@
 // holds from the first use until the process exits.
 #include "bf_internal.cuh"
 
-#include <mutex>
-
 namespace {
 
 // Scratch of bf_grid_tensor_quantized_static: up to kStaticCounters 32-bit
@@ -20,30 +18,9 @@ namespace {
 constexpr uint64_t kStaticCounters = 16384;
 static __device__ __align__(256) unsigned g_static_counters[kStaticCounters];
 
-// Device address of g_static_counters for each device.  In host code the
-// array's name is only a host-side stand-in, so the address is looked up once
-// per device with that device current and passed to the kernel.
-constexpr int kMaxDevices = 64;
-std::mutex g_mutex;
-void* g_address[kMaxDevices] = {};
-
-bf_status static_scratch(unsigned** out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return bf::cuda_status(e, "cudaGetDevice");
-    if (dev < 0 || dev >= kMaxDevices) {
-        return bf::set_error(BF_ERR_UNSUPPORTED, "device ordinal beyond the static scratch table");
-    }
-    std::lock_guard<std::mutex> lock(g_mutex);
-    if (g_address[dev] == nullptr) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_static_counters);
-        if (e != cudaSuccess) return bf::cuda_status(e, "cudaGetSymbolAddress(static scratch)");
-        g_address[dev] = p;
-    }
-    *out = static_cast<unsigned*>(g_address[dev]);
-    return BF_OK;
-}
+// Device addresses of g_static_counters, one per device (see
+// device_symbol_address: looked up again on every call outside capture).
+bf::SymbolAddressCache g_address;
 
 }  // namespace
 
@@ -69,13 +46,18 @@ BF_API bf_status bf_grid_tensor_quantized_static(void* stream, const uint8_t* pa
     if (dims->n_ant > 64) {
         return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernel supports n_ant 32 or 64");
     }
-    const uint64_t needed = grid_tensor_counter_count(*dims, integration_spectra, n_shards);
-    if (needed > kStaticCounters) {
-        return set_error(BF_ERR_INVALID_ARGUMENT,
-                         "request needs " + std::to_string(needed) +
-                             " scratch counters (n_shards * windows * ceil(n_freq / 16)); the "
-                             "allocation-free entry point holds at most " +
-                             std::to_string(kStaticCounters));
+    // The counters serve the quantizer fused into the long-window epilogue
+    // (integration_spectra >= 32); short windows quantize in a second kernel
+    // and use none, so only long windows are held to the array's size.
+    if (integration_spectra >= 32) {
+        const uint64_t needed = grid_tensor_counter_count(*dims, integration_spectra, n_shards);
+        if (needed > kStaticCounters) {
+            return set_error(BF_ERR_INVALID_ARGUMENT,
+                             "request needs " + std::to_string(needed) +
+                                 " scratch counters (n_shards * windows * ceil(n_freq / 16)); the "
+                                 "allocation-free entry point holds at most " +
+                                 std::to_string(kStaticCounters));
+        }
     }
     if (packed_voltage == nullptr || split_weights == nullptr || integrated == nullptr || codes == nullptr ||
         params == nullptr) {
@@ -87,11 +69,12 @@ BF_API bf_status bf_grid_tensor_quantized_static(void* stream, const uint8_t* pa
         return set_error(BF_ERR_INVALID_ARGUMENT,
                          "packed_voltage, split_weights and integrated must be 16-byte aligned, params 8-byte");
     }
-    unsigned* scratch = nullptr;
-    st = static_scratch(&scratch);
+    void* scratch = nullptr;
+    st = device_symbol_address(&g_static_counters, g_address, static_cast<cudaStream_t>(stream), &scratch,
+                               "static scratch");
     if (st != BF_OK) return st;
     return launch_grid_tensor(static_cast<cudaStream_t>(stream), packed_voltage, split_weights, integrated, codes,
-                              params, *dims, integration_spectra, n_shards, scratch);
+                              params, *dims, integration_spectra, n_shards, static_cast<unsigned*>(scratch));
 }
 
 }  // extern "C"

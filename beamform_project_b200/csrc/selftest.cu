@@ -34,8 +34,21 @@ extern "C" BF_API bf_status bf_probe_bounded_wait(void* stream, uint64_t limit_n
     if (limit_ns == 0 || limit_ns > 2000000000ull) {
         return set_error(BF_ERR_INVALID_ARGUMENT, "limit_ns must be between 1 and 2e9");
     }
-    unsigned* err = device_error_word();
-    if (err == nullptr) return set_error(BF_ERR_CUDA, "device error word is unavailable");
+    unsigned* err = device_error_word(static_cast<cudaStream_t>(stream));
+    if (err == nullptr) return BF_ERR_CUDA;
     bounded_wait_probe_kernel<<<1, 32, 0, static_cast<cudaStream_t>(stream)>>>(limit_ns, err);
     return cuda_status(cudaGetLastError(), "bounded_wait_probe_kernel launch");
+}
+
+extern "C" BF_API bf_status bf_kernel_versions(int* binary_version, int* ptx_version) {
+    using namespace bf;
+    clear_error();
+    if (binary_version == nullptr || ptx_version == nullptr) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "binary_version and ptx_version must be given");
+    }
+    cudaFuncAttributes attr{};
+    BF_RETURN_IF(cuda_status(cudaFuncGetAttributes(&attr, bounded_wait_probe_kernel), "cudaFuncGetAttributes"));
+    *binary_version = attr.binaryVersion;
+    *ptx_version = attr.ptxVersion;
+    return BF_OK;
 }

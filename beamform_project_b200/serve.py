@@ -134,7 +134,10 @@ class Server:
 
     def restore(self, image: bytes) -> int:
         """Queue the job of a checkpoint image (from a server with the same
-        window, shard and pool settings); it resumes at its next window."""
+        window, shard and pool settings); it resumes at its next window.  Its
+        results equal an uninterrupted run's when this server's pool holds the
+        same rows as the source's: the image records the pool offset, not the
+        pool's contents."""
         jid = C.c_uint64(0)
         buf = C.create_string_buffer(bytes(image), len(image))
         native.check(native.lib().bf_serve_restore(self._h, buf, len(image), C.byref(jid)))

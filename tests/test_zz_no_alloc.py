@@ -37,6 +37,18 @@ def test_static_entry_rejects_requests_beyond_its_scratch():
     assert "at most 16384" in native.last_error()
 
 
+def test_static_entry_short_windows_are_not_held_to_the_array_size():
+    """Windows below 32 spectra quantize in a second kernel and use no counters:
+    16 spectra x 2048 windows x 21 groups x 2 shards (86016) passes the size
+    check.  Null buffers then stop the call before any CUDA call, with the
+    buffer message instead of the size message."""
+    d = Dims(2048 * 16, F, 64, 128)
+    st = _static_fn()(None, None, None, None, None, None, C.byref(d), 16, 2)
+    assert st == native.BF_OK + 1
+    msg = native.last_error()
+    assert "every buffer must be given" in msg and "at most" not in msg
+
+
 @pytest.mark.gpu
 def test_static_entry_matches_allocating_entry_twice(cuda):
     from beamform_project_b200 import api
