@@ -253,6 +253,70 @@ def grid_cov_integrated(stream, packed_voltage, cov_weights, integrated, codes, 
                                               int(integration_spectra), int(n_shards)))
 
 
+def grid_cov_estimate(stream, packed_voltage, cov_weights, integrated, estimate, dims: Dimensions,
+                      integration_spectra: int, n_shards: int = 1) -> None:
+    """grid_cov_integrated that also writes each value's relative error
+    estimate 2^-23 |v_b|^2 tr(E) / I (float32, same layout as integrated)."""
+    torch = _torch()
+    validate_dimensions(dims)
+    nw = integrated_time_count(dims.n_time, integration_spectra)
+    n_out = n_shards * nw * dims.n_freq * dims.n_beams
+    v = _dev(packed_voltage, "packed_voltage", torch.uint8, n_shards * dims.n_time * dims.n_freq * dims.n_ant)
+    s = _dev(cov_weights, "cov_weights", torch.uint8, cov_weight_bytes(dims, n_shards))
+    o = _dev(integrated, "integrated", torch.float32, n_out)
+    e = _dev(estimate, "estimate", torch.float32, n_out)
+    d = dims.c()
+    check(native.lib().bf_grid_cov_estimate(_stream_handle(stream), v, s, o, e, C.byref(d),
+                                            int(integration_spectra), int(n_shards)))
+
+
+def auto_weight_bytes(dims: Dimensions, n_shards: int = 1) -> int:
+    d = dims.c()
+    return int(native.lib().bf_auto_weight_bytes(C.byref(d), int(n_shards)))
+
+
+def prepare_auto_weights(stream, weights, auto_weights, dims: Dimensions, n_shards: int = 1) -> None:
+    """Canonical complex64 weights -> the checked grid's operand (covariance
+    image, where the form applies, then the split image)."""
+    torch = _torch()
+    validate_dimensions(dims)
+    w = _dev(weights, "weights", torch.float32, 2 * n_shards * dims.n_beams * dims.n_freq * dims.n_ant)
+    o = _dev(auto_weights, "auto_weights", torch.uint8, auto_weight_bytes(dims, n_shards))
+    d = dims.c()
+    check(native.lib().bf_prepare_auto_weights(_stream_handle(stream), w, o, C.byref(d), int(n_shards)))
+
+
+def grid_auto_workspace_bytes(dims: Dimensions, integration_spectra: int, n_shards: int = 1) -> int:
+    d = dims.c()
+    return int(native.lib().bf_grid_auto_workspace_bytes(C.byref(d), int(integration_spectra), int(n_shards)))
+
+
+def grid_auto_integrated(stream, packed_voltage, auto_weights, integrated, codes, params, workspace,
+                         dims: Dimensions, integration_spectra: int, n_shards: int = 1) -> None:
+    """The checked grid beamformer (bf_grid_auto_integrated): the covariance
+    form with per-value error estimates where it applies, the split kernel
+    over every unit whose estimate exceeds the calibrated limit, and the split
+    kernel alone elsewhere; every value within 1e-5 relative of FP64.  The
+    workspace's first int32 is the number of units recomputed."""
+    torch = _torch()
+    validate_dimensions(dims)
+    nw = integrated_time_count(dims.n_time, integration_spectra)
+    n_out = n_shards * nw * dims.n_freq * dims.n_beams
+    v = _dev(packed_voltage, "packed_voltage", torch.uint8, n_shards * dims.n_time * dims.n_freq * dims.n_ant)
+    s = _dev(auto_weights, "auto_weights", torch.uint8, auto_weight_bytes(dims, n_shards))
+    o = _dev(integrated, "integrated", torch.float32, n_out)
+    c = p = None
+    if codes is not None or params is not None:
+        qd = Dimensions(nw, dims.n_freq, dims.n_ant, dims.n_beams)
+        c = _dev(codes, "codes", torch.int8, n_out)
+        p = _dev(params, "params", torch.float32, 2 * n_shards * quantization_parameter_count(qd))
+    wsb = grid_auto_workspace_bytes(dims, integration_spectra, n_shards)
+    ws = _dev(workspace, "workspace", torch.uint8, wsb) if wsb > 0 else None
+    d = dims.c()
+    check(native.lib().bf_grid_auto_integrated(_stream_handle(stream), v, s, o, c, p, ws, C.byref(d),
+                                               int(integration_spectra), int(n_shards)))
+
+
 def grid_tensor_workspace_bytes(dims: Dimensions, integration_spectra: int, n_shards: int = 1) -> int:
     d = dims.c()
     return int(native.lib().bf_grid_tensor_workspace_bytes(C.byref(d), int(integration_spectra), int(n_shards)))

@@ -3,12 +3,13 @@
 // A drop-in for the reference's tools/beamformer_cuda.cpp: the same options,
 // input and output files, stdout report and metrics CSV row, so scripts that
 // drive the reference tool (its validation runner included) run unchanged.
-// Two additions: --kernel tensor selects the split-precision tensor-core path
-// and --kernel covariance the opt-in covariance form (both take canonical
-// weights, like direct).
+// Additions: --kernel tensor selects the split-precision tensor-core path,
+// --kernel covariance the opt-in covariance form and --kernel checked the
+// covariance form with split-precision recomputation wherever its error
+// estimate is too high (all take canonical weights, like direct).
 //
 //   beamformer_cuda --input V --weights W --output O [--n-time N] [--n-ant N]
-//       [--n-beams N] [--kernel direct|tiled|tensor|covariance] [--integration-spectra S]
+//       [--n-beams N] [--kernel direct|tiled|tensor|covariance|checked] [--integration-spectra S]
 //       [--output-format float32|int8 --quantization-params P
 //        --quantization-metadata M] [--shard-id 0|1] [--metrics CSV]
 //
@@ -52,7 +53,7 @@ void usage(const char* prog) {
               << "  --n-time N              default: 15360\n"
               << "  --n-ant N               32 or 64; default: 64\n"
               << "  --n-beams N             1 to 128; default: 5\n"
-              << "  --kernel NAME           direct, tiled, tensor or covariance; default: direct\n"
+              << "  --kernel NAME           direct, tiled, tensor, covariance or checked; default: direct\n"
               << "  --integration-spectra N GPU integration: 10 or 320\n"
               << "  --output-format NAME    float32 or int8; default: float32\n"
               << "  --quantization-params F int8 parameter output; required for int8\n"
@@ -99,7 +100,8 @@ Args parse(int argc, char** argv) {
             else if (k == "tiled") a.kernel = bf::CudaBeamformerKernel::Tiled;
             else if (k == "tensor") a.kernel = bf::CudaBeamformerKernel::TensorSplit;
             else if (k == "covariance") a.kernel = bf::CudaBeamformerKernel::TensorCovariance;
-            else throw std::invalid_argument("kernel must be direct, tiled, tensor or covariance");
+            else if (k == "checked") a.kernel = bf::CudaBeamformerKernel::TensorChecked;
+            else throw std::invalid_argument("kernel must be direct, tiled, tensor, covariance or checked");
         } else if (opt == "--integration-spectra") {
             a.spectra = to_size(value(i), opt);
         } else if (opt == "--output-format") {
@@ -137,6 +139,7 @@ const char* kernel_name(bf::CudaBeamformerKernel k) {
         case bf::CudaBeamformerKernel::Direct: return "direct";
         case bf::CudaBeamformerKernel::Tiled: return "tiled";
         case bf::CudaBeamformerKernel::TensorCovariance: return "covariance";
+        case bf::CudaBeamformerKernel::TensorChecked: return "checked";
         default: return "tensor";
     }
 }

@@ -253,5 +253,24 @@ uint64_t grid_tensor_counter_count(const bf_dims& d, uint64_t spectra, uint64_t 
 bf_status launch_grid_tensor(cudaStream_t stream, const uint8_t* v, const void* split,
                              float* integrated, int8_t* codes, float* params, const bf_dims& d,
                              uint64_t spectra, uint64_t n_shards, unsigned* counters);
+// The split kernel over the units of a device-written list (no quantizer).
+bf_status launch_grid_tensor_list(cudaStream_t stream, const uint8_t* v, const void* split, float* integrated,
+                                  const bf_dims& d, uint64_t spectra, uint64_t n_shards, const int* unit_list,
+                                  const int* unit_count);
+// Units of a plain split-kernel launch: (shard, channel, group) with
+// groups_per_channel groups of windows_per_group windows (S >= 32).
+long long grid_tensor_unit_layout(const bf_dims& d, uint64_t spectra, uint64_t n_shards, int* groups_per_channel,
+                                  int* windows_per_group);
+// Checked covariance form (grid_cov.cu): the covariance kernel with error
+// estimates, then the split kernel over the units whose estimate exceeds the
+// calibrated limit.  Weights: the covariance image, then the split image.
+uint64_t auto_weight_bytes(const bf_dims& d, uint64_t n_shards);
+bool auto_uses_cov(const bf_dims& d, uint64_t spectra, uint64_t n_shards);
+uint64_t auto_workspace_bytes(const bf_dims& d, uint64_t spectra, uint64_t n_shards);
+bf_status launch_prepare_auto(cudaStream_t stream, const float* w, void* out, const bf_dims& d, uint64_t n_shards);
+bf_status launch_grid_auto(cudaStream_t stream, const uint8_t* v, const void* wimg, float* integrated, int8_t* codes,
+                           float* params, void* workspace, const bf_dims& d, uint64_t spectra, uint64_t n_shards);
+bf_status launch_grid_cov_estimate(cudaStream_t stream, const uint8_t* v, const void* wimg, float* integrated,
+                                   float* estimate, const bf_dims& d, uint64_t spectra, uint64_t n_shards);
 
 }  // namespace bf

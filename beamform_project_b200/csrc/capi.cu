@@ -282,6 +282,71 @@ BF_API bf_status bf_grid_cov_integrated(void* stream, const uint8_t* packed_volt
                            params, *dims, integration_spectra, n_shards);
 }
 
+BF_API bf_status bf_grid_cov_estimate(void* stream, const uint8_t* packed_voltage, const void* cov_weights,
+                                      float* integrated, float* estimate, const bf_dims* dims,
+                                      uint64_t integration_spectra, uint64_t n_shards) {
+    clear_error();
+    BF_TRY(validate_dims(dims));
+    if (n_shards == 0) return set_error(BF_ERR_INVALID_ARGUMENT, "n_shards must be positive");
+    if (integration_spectra == 0) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "integration_spectra must be positive");
+    }
+    BF_TRY(check_grid_cov(*dims, integration_spectra, n_shards));
+    BF_TRY(check_ptr(packed_voltage, 16, "packed_voltage"));
+    BF_TRY(check_ptr(cov_weights, 16, "cov_weights"));
+    BF_TRY(check_ptr(integrated, 16, "integrated"));
+    BF_TRY(check_ptr(estimate, 4, "estimate"));
+    return launch_grid_cov_estimate(static_cast<cudaStream_t>(stream), packed_voltage, cov_weights, integrated,
+                                    estimate, *dims, integration_spectra, n_shards);
+}
+
+BF_API uint64_t bf_auto_weight_bytes(const bf_dims* dims, uint64_t n_shards) {
+    if (dims == nullptr || validate_dims(dims) != BF_OK || dims->n_ant > 64) return 0;
+    return auto_weight_bytes(*dims, n_shards);
+}
+
+BF_API bf_status bf_prepare_auto_weights(void* stream, const float* weights, void* auto_weights,
+                                         const bf_dims* dims, uint64_t n_shards) {
+    clear_error();
+    BF_TRY(validate_dims(dims));
+    if (n_shards == 0) return set_error(BF_ERR_INVALID_ARGUMENT, "n_shards must be positive");
+    if (dims->n_ant > 64) return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernels support n_ant 32 or 64");
+    BF_TRY(check_ptr(weights, 8, "weights"));
+    BF_TRY(check_ptr(auto_weights, 16, "auto_weights"));
+    return launch_prepare_auto(static_cast<cudaStream_t>(stream), weights, auto_weights, *dims, n_shards);
+}
+
+BF_API uint64_t bf_grid_auto_workspace_bytes(const bf_dims* dims, uint64_t integration_spectra, uint64_t n_shards) {
+    if (dims == nullptr || validate_dims(dims) != BF_OK || integration_spectra == 0 || n_shards == 0) return 0;
+    return auto_workspace_bytes(*dims, integration_spectra, n_shards);
+}
+
+BF_API bf_status bf_grid_auto_integrated(void* stream, const uint8_t* packed_voltage, const void* auto_weights,
+                                         float* integrated, int8_t* codes, float* params, void* workspace,
+                                         const bf_dims* dims, uint64_t integration_spectra, uint64_t n_shards) {
+    clear_error();
+    BF_TRY(validate_dims(dims));
+    if (n_shards == 0) return set_error(BF_ERR_INVALID_ARGUMENT, "n_shards must be positive");
+    if (integration_spectra == 0) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "integration_spectra must be positive");
+    }
+    if (dims->n_ant > 64) return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernels support n_ant 32 or 64");
+    if (integration_spectra > 32 && integration_spectra % 32 != 0) {
+        return set_error(BF_ERR_UNSUPPORTED,
+                         "the tensor-core kernels need integration_spectra below 32 or a multiple of 32");
+    }
+    if ((codes == nullptr) != (params == nullptr)) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "codes and params must both be given or both be null");
+    }
+    BF_TRY(check_ptr(packed_voltage, 16, "packed_voltage"));
+    BF_TRY(check_ptr(auto_weights, 16, "auto_weights"));
+    BF_TRY(check_ptr(integrated, 16, "integrated"));
+    if (codes != nullptr) BF_TRY(check_ptr(params, 8, "params"));
+    if (auto_uses_cov(*dims, integration_spectra, n_shards)) BF_TRY(check_ptr(workspace, 256, "workspace"));
+    return launch_grid_auto(static_cast<cudaStream_t>(stream), packed_voltage, auto_weights, integrated, codes, params,
+                            workspace, *dims, integration_spectra, n_shards);
+}
+
 BF_API bf_status bf_tracker(void* stream, int mode, const uint8_t* packed_voltage,
                             const float* positions, const double* wave_numbers,
                             const float* window_directions, float* intensity,

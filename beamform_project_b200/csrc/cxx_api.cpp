@@ -62,6 +62,7 @@ int to_c(CudaBeamformerKernel k) {
         case CudaBeamformerKernel::Tiled: return BF_KERNEL_TILED;
         case CudaBeamformerKernel::TensorSplit: return BF_KERNEL_TENSOR;
         case CudaBeamformerKernel::TensorCovariance: break;  // its own entry points
+        case CudaBeamformerKernel::TensorChecked: break;
     }
     throw std::invalid_argument("unknown CUDA beamformer kernel selector");
 }
@@ -77,10 +78,10 @@ void validate_cuda_temporal_integration(CudaBeamformerKernel kernel, const Tempo
         }
         return;
     }
-    if (kernel == CudaBeamformerKernel::TensorSplit) {
+    if (kernel == CudaBeamformerKernel::TensorSplit || kernel == CudaBeamformerKernel::TensorChecked) {
         if (s > 32 && s % 32 != 0) {
             throw std::invalid_argument(
-                "the TensorSplit kernel needs integration spectra below 32 or a multiple of 32");
+                "the tensor-core kernels need integration spectra below 32 or a multiple of 32");
         }
         return;
     }
@@ -142,7 +143,8 @@ std::size_t weight_storage_count(const Dimensions& dims, CudaBeamformerKernel ke
 void launch_packed_beamformer(CudaBeamformerKernel kernel, cudaStream_t stream, const std::uint8_t* packed_voltage,
                               const ComplexFloat* weights, float* intensity, const Dimensions& dims) {
     validate_dimensions(dims);
-    if (kernel == CudaBeamformerKernel::TensorSplit || kernel == CudaBeamformerKernel::TensorCovariance) {
+    if (kernel == CudaBeamformerKernel::TensorSplit || kernel == CudaBeamformerKernel::TensorCovariance ||
+        kernel == CudaBeamformerKernel::TensorChecked) {
         throw std::invalid_argument("the tensor-core kernels produce integrated output only");
     }
     const bf_dims d = to_c(dims);
@@ -157,6 +159,10 @@ void launch_packed_integrated_beamformer(CudaBeamformerKernel kernel, cudaStream
     validate_dimensions(dims);
     validate_cuda_temporal_integration(kernel, temporal_integration);
     const bf_dims d = to_c(dims);
+    if (kernel == CudaBeamformerKernel::TensorChecked) {
+        throw std::invalid_argument(
+            "the TensorChecked kernel needs a workspace: use launch_checked_integrated_beamformer");
+    }
     if (kernel == CudaBeamformerKernel::TensorCovariance) {
         // `weights` is the operand prepared by prepare_cov_weights
         check(bf_grid_cov_integrated(stream, packed_voltage, weights, integrated_intensity, nullptr, nullptr, &d,
@@ -214,6 +220,33 @@ void prepare_cov_weights(cudaStream_t stream, const ComplexFloat* weights, void*
     check(bf_prepare_cov_weights(stream, reinterpret_cast<const float*>(weights), cov_weights, &d, 1));
 }
 
+std::size_t checked_weight_bytes(const Dimensions& dims) {
+    const bf_dims d = to_c(dims);
+    return static_cast<std::size_t>(bf_auto_weight_bytes(&d, 1));
+}
+
+void prepare_checked_weights(cudaStream_t stream, const ComplexFloat* weights, void* checked_weights,
+                             const Dimensions& dims) {
+    const bf_dims d = to_c(dims);
+    check(bf_prepare_auto_weights(stream, reinterpret_cast<const float*>(weights), checked_weights, &d, 1));
+}
+
+std::size_t checked_workspace_bytes(const Dimensions& dims, const TemporalIntegrationConfig& temporal_integration) {
+    const bf_dims d = to_c(dims);
+    return static_cast<std::size_t>(bf_grid_auto_workspace_bytes(&d, temporal_integration.integration_spectra, 1));
+}
+
+void launch_checked_integrated_beamformer(cudaStream_t stream, const std::uint8_t* packed_voltage,
+                                          const void* checked_weights, float* integrated_intensity, void* workspace,
+                                          const Dimensions& dims,
+                                          const TemporalIntegrationConfig& temporal_integration) {
+    validate_dimensions(dims);
+    validate_cuda_temporal_integration(CudaBeamformerKernel::TensorChecked, temporal_integration);
+    const bf_dims d = to_c(dims);
+    check(bf_grid_auto_integrated(stream, packed_voltage, checked_weights, integrated_intensity, nullptr, nullptr,
+                                  workspace, &d, temporal_integration.integration_spectra, 1));
+}
+
 CudaDeviceInfo cuda_device_info() {
     CudaDeviceInfo info;
     char name[256];
@@ -236,7 +269,8 @@ struct CudaBeamformerWorkspace::Impl {
     CudaBeamformerOutput output;
     DeviceBuffer<std::uint8_t> voltage;
     DeviceBuffer<ComplexFloat> weights;     // canonical or tiled
-    DeviceBuffer<std::uint8_t> split;       // TensorSplit / TensorCovariance operand
+    DeviceBuffer<std::uint8_t> split;       // TensorSplit / TensorCovariance / TensorChecked operand
+    DeviceBuffer<std::uint8_t> scratch;     // TensorChecked fallback list
     DeviceBuffer<float> intensity;          // per-spectrum output
     DeviceBuffer<float> integrated;
     DeviceBuffer<std::int8_t> codes;
@@ -254,7 +288,12 @@ struct CudaBeamformerWorkspace::Impl {
         if (tensor()) {
             weights = DeviceBuffer<ComplexFloat>(cap.n_beams * cap.n_freq * cap.n_ant);
             split = DeviceBuffer<std::uint8_t>(kernel == CudaBeamformerKernel::TensorSplit ? split_weight_bytes(cap)
-                                                                                          : cov_weight_bytes(cap));
+                                               : kernel == CudaBeamformerKernel::TensorChecked
+                                                   ? checked_weight_bytes(cap)
+                                                   : cov_weight_bytes(cap));
+            if (kernel == CudaBeamformerKernel::TensorChecked && t) {
+                scratch = DeviceBuffer<std::uint8_t>(checked_workspace_bytes(cap, *t));
+            }
         } else {
             weights = DeviceBuffer<ComplexFloat>(weight_storage_count(cap, kernel));
         }
@@ -274,7 +313,8 @@ struct CudaBeamformerWorkspace::Impl {
     }
 
     bool tensor() const {
-        return kernel == CudaBeamformerKernel::TensorSplit || kernel == CudaBeamformerKernel::TensorCovariance;
+        return kernel == CudaBeamformerKernel::TensorSplit || kernel == CudaBeamformerKernel::TensorCovariance ||
+               kernel == CudaBeamformerKernel::TensorChecked;
     }
     void validate_request(const Dimensions& dims) const {
         validate_dimensions(dims);
@@ -303,7 +343,14 @@ struct CudaBeamformerWorkspace::Impl {
     // Launch the configured beamformer into the configured output buffer.
     void launch(const Dimensions& dims, const std::uint8_t* v, const void* w, float* out) {
         const bf_dims d = to_c(dims);
-        if (kernel == CudaBeamformerKernel::TensorCovariance) {
+        if (kernel == CudaBeamformerKernel::TensorChecked) {
+            // the workspace is sized for the capacity; a shorter request needs no more
+            if (checked_workspace_bytes(dims, *temporal) > scratch.count) {
+                throw std::invalid_argument("dimensions exceed CUDA workspace capacity");
+            }
+            check(bf_grid_auto_integrated(stream, v, w, out, nullptr, nullptr, scratch.ptr, &d,
+                                          temporal->integration_spectra, 1));
+        } else if (kernel == CudaBeamformerKernel::TensorCovariance) {
             check(bf_grid_cov_integrated(stream, v, w, out, nullptr, nullptr, &d, temporal->integration_spectra, 1));
         } else if (kernel == CudaBeamformerKernel::TensorSplit) {
             // per-spectrum output is integration over one spectrum ([T][F][B] == [W][F][B])
@@ -326,6 +373,8 @@ struct CudaBeamformerWorkspace::Impl {
             check(bf_prepare_split_weights(stream, static_cast<const float*>(canonical), split.ptr, &d, 1));
         } else if (kernel == CudaBeamformerKernel::TensorCovariance) {
             check(bf_prepare_cov_weights(stream, static_cast<const float*>(canonical), split.ptr, &d, 1));
+        } else if (kernel == CudaBeamformerKernel::TensorChecked) {
+            check(bf_prepare_auto_weights(stream, static_cast<const float*>(canonical), split.ptr, &d, 1));
         }
     }
 };
@@ -340,6 +389,12 @@ CudaBeamformerWorkspace::CudaBeamformerWorkspace(const Dimensions& capacity, Cud
     }
     if (kernel == CudaBeamformerKernel::TensorSplit && capacity.n_ant > 64) {
         throw std::invalid_argument("the TensorSplit kernel supports n_ant 32 or 64");
+    }
+    if (kernel == CudaBeamformerKernel::TensorChecked) {
+        if (capacity.n_ant > 64) throw std::invalid_argument("the TensorChecked kernel supports n_ant 32 or 64");
+        if (!temporal_integration) {
+            throw std::invalid_argument("the TensorChecked kernel produces integrated output only");
+        }
     }
     if (kernel == CudaBeamformerKernel::TensorCovariance) {
         if (capacity.n_ant != 64) throw std::invalid_argument("the TensorCovariance kernel supports n_ant 64");

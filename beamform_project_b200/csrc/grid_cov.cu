@@ -21,6 +21,15 @@
 //      memory: hi*Vhi + hi*Vlo + lo*Vhi, fp32 in TMEM (the dropped lo*Vlo is
 //      below 2^-22 of the product);
 //   4. I_b = sum_m V[m][b] Y[m][b] in fp32 (fixed butterfly order).
+// The fp32 sums in 3 and 4 carry terms as large as |v_b|^2 tr(E) (E is
+// positive semidefinite, so |E_mn| <= sqrt(E_mm E_nn) and, by Cauchy-Schwarz,
+// sum_mn |V_mb E_mn V_nb| <= |v_b|^2 tr(E)), so the relative error of a beam
+// scales with est_b = 2^-23 |v_b|^2 tr(E) / I_b: small for beams that carry
+// the window's power, large for deep sidelobes of a strong source.  On
+// request the kernel writes est_b per value and lists, for the split direct
+// kernel (grid_tc.cu) to recompute, every unit holding a value whose estimate
+// exceeds a limit calibrated against FP64 (the checked form,
+// bf_grid_auto_integrated).
 // Tensor work per (window, channel) at A = 64, B = 128: 128 x 128 x S int8
 // MACs + 3 x 128^3 fp16 MACs, against 2 x 128 x 256 x S fp16 MACs for the
 // split direct form: 2.35x less at S = 320.  The covariance is exact, so the
@@ -64,7 +73,8 @@ constexpr uint32_t kVBytes = 128 * 128 * 4;           // [beam][component] fp32
 constexpr uint32_t kWImage = 2 * kWHalf + kVBytes;    // per channel
 constexpr uint32_t kYCol = 256;                       // TMEM columns of the two Y stages
 constexpr uint64_t kWaitNs = 2000000000ull;
-constexpr uint32_t kBarBytes = (2 * kRawStages + 2 * kXStages + 11) * 8 + 8;  // mbarriers, TMEM address, fail flag
+// mbarriers, TMEM address, fail flag, per-unit trace partials [4][4]
+constexpr uint32_t kBarBytes = (2 * kRawStages + 2 * kXStages + 15) * 8 + 8 + 64;
 constexpr uint32_t kSmemBytes = kWImage + kXStages * kXBytes + kRawStages * kRawBytes + 2 * 4 * 128 * 4 + 512 + 1024;
 static_assert(kBarBytes <= 512, "barrier block");
 static_assert(kSmemBytes <= 232448, "shared memory per CTA");
@@ -76,7 +86,20 @@ struct CovGridParams {
     int n_freq, n_beams, n_windows, n_time, spectra;
     long long n_pair_units;  // shards x F/2 x windows
     float e_scale, out_scale;
+    // error estimates (checked form): est [shard][W][F][B] or null; with
+    // est_limit > 0 every split-kernel unit (shard, channel, group of
+    // split_gw windows; split_gpc groups per channel) holding an estimate
+    // above the limit is appended once to unit_list
+    float* est;
+    float est_limit;
+    unsigned* unit_flags;    // [split units], zero at launch
+    int* unit_list;
+    int* unit_count;         // zero at launch
+    int split_gpc, split_gw;
 };
+
+// est_b = kEstScale |v_b|^2 tr(E) / I_b
+constexpr float kEstScale = 0x1p-23f;
 
 __device__ __forceinline__ void cov_grid_error(unsigned* err, unsigned code) {
     if (err != nullptr) atomicOr(err, 0x80000000u | (code << 16));
@@ -148,8 +171,11 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
     uint64_t* w_full = y_free + 2;
     uint64_t* w_empty = w_full + 1;
     uint64_t* mma_done = w_empty + 1;
-    uint32_t* tmem_ptr = reinterpret_cast<uint32_t*>(mma_done + 1);
+    uint64_t* tr_ready = mma_done + 1;           // [4] trace partials of unit j in slot j % 4
+    uint32_t* tmem_ptr = reinterpret_cast<uint32_t*>(tr_ready + 4);
     volatile int* s_fail = reinterpret_cast<volatile int*>(tmem_ptr + 1);
+    float* s_trq = reinterpret_cast<float*>(tmem_ptr + 2);  // [4 slots][4 quadrants]
+    const bool estimate = p.est != nullptr || p.est_limit > 0.f;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x == 0) {
@@ -170,6 +196,7 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
         mbar_init(w_full, 1);
         mbar_init(w_empty, 1 + kDotWarps);
         mbar_init(mma_done, 1);
+        for (int i = 0; i < 4; ++i) mbar_init(&tr_ready[i], 4);
         *s_fail = 0;
         fence_mbar_init();
     }
@@ -345,11 +372,15 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
         const int q = warp & 3, half = (warp - kConvFirst) >> 2;
         const int m = 32 * q + lane;
         const int sgn0 = ((m >> 2) & 1) != 0 ? -1 : 1;
+        // the warp whose column chunks hold its quadrant's diagonal forms that
+        // quadrant's part of tr(E) (integers times a power of two: exact)
+        const bool has_diag = estimate && (q >> 1) == half;
         long long j = 0;
         for (long long pu = u_begin; pu < u_end; ++pu, ++j) {
             const int eb = static_cast<int>(j & 1);
             if (!mbar_wait(&gram_done[eb], static_cast<uint32_t>((j >> 1) & 1), kWaitNs)) { fail(13); break; }
             tc_fence_after();
+            float diag = 0.f;
 #pragma unroll 1
             for (int cc = 2 * half; cc < 2 * half + 2; ++cc) {
                 const uint32_t taddr = tmem_base + ((32u * q) << 16) + eb * 128 + 32 * cc;
@@ -363,6 +394,10 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
                     const int sg = ((n >> 2) & 1) != 0 ? -sgn0 : sgn0;
                     const int e = (static_cast<int>(g[n]) + sg * partner) >> 8;  // exact: both are 256 x
                     ef[n] = (__int_as_float(e + 0x4B400000) - 12582912.0f) * p.e_scale;
+                }
+                if (has_diag && cc == q) {
+#pragma unroll
+                    for (int n = 0; n < 32; ++n) diag = n == lane ? ef[n] : diag;
                 }
                 uint32_t r[32];
 #pragma unroll
@@ -379,6 +414,16 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&conv_done[eb]);
+            if (has_diag) {
+                // read by the beam sums of unit j before they free Y of unit j, which
+                // comes before the Gram (and so the conversion) of unit j + 4
+#pragma unroll
+                for (int o = 16; o >= 1; o >>= 1) diag += __shfl_xor_sync(0xffffffffu, diag, o);
+                if (lane == 0) {
+                    s_trq[(j & 3) * 4 + q] = diag;
+                    mbar_arrive(&tr_ready[j & 3]);
+                }
+            }
             if (*s_fail) break;
         }
     } else {
@@ -387,6 +432,7 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
         const int m = 32 * q + lane;
         const int t = 32 * (warp - kDotFirst) + lane;  // output beam of the final sum
         const float* vt = reinterpret_cast<const float*>(wsm + 2 * kWHalf);  // [beam][component]
+        float vnorm = 0.f;  // |v_t|^2 of the current channel
         long long j = 0;
         CovCursor cur;
         cur.start(u_begin, p);
@@ -395,6 +441,22 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
             const int eb = static_cast<int>(j & 1);
             if (!mbar_wait(&quad_done[eb], static_cast<uint32_t>((j >> 1) & 1), kWaitNs)) { fail(14); break; }
             tc_fence_after();
+            float tr = 0.f;
+            if (estimate) {
+                if (pu == u_begin || cur.w == 0) {
+                    // the channel's image is in place until this run's last unit
+                    float acc = 0.f;
+#pragma unroll 8
+                    for (int i = 0; i < 128; ++i) {
+                        const float v = vt[t * 128 + ((i + lane) & 127)];
+                        acc = fmaf(v, v, acc);
+                    }
+                    vnorm = acc;
+                }
+                if (!mbar_wait(&tr_ready[j & 3], static_cast<uint32_t>((j >> 2) & 1), kWaitNs)) { fail(15); break; }
+                const float* tq = s_trq + (j & 3) * 4;
+                tr = ((tq[0] + tq[1]) + tq[2]) + tq[3];
+            }
             float part[4];
 #pragma unroll 1
             for (int cb = 0; cb < 4; ++cb) {
@@ -418,9 +480,20 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
             for (int cb = 0; cb < 4; ++cb) sd[q * 128 + 32 * cb + lane] = part[cb];
             named_barrier(1, 32 * kDotWarps);
             const float sum = ((sd[t] + sd[128 + t]) + sd[256 + t]) + sd[384 + t];
-            if (t < p.n_beams) {
-                p.out[((static_cast<size_t>(cur.s) * p.n_windows + cur.w) * p.n_freq + 2 * cur.fp + odd) * p.n_beams + t] =
-                    sum * p.out_scale;
+            const size_t oidx =
+                ((static_cast<size_t>(cur.s) * p.n_windows + cur.w) * p.n_freq + 2 * cur.fp + odd) * p.n_beams + t;
+            if (t < p.n_beams) p.out[oidx] = sum * p.out_scale;
+            if (estimate) {
+                const float est = sum > 0.f ? kEstScale * vnorm * tr / sum : INFINITY;
+                if (p.est != nullptr && t < p.n_beams) p.est[oidx] = est;
+                if (p.est_limit > 0.f) {
+                    const bool over = t < p.n_beams && !(est <= p.est_limit);
+                    if (__any_sync(0xffffffffu, over) && lane == 0) {
+                        const int f = 2 * cur.fp + odd;
+                        const int unit = (cur.s * p.n_freq + f) * p.split_gpc + cur.w / p.split_gw;
+                        if (atomicExch(&p.unit_flags[unit], 1u) == 0u) p.unit_list[atomicAdd(p.unit_count, 1)] = unit;
+                    }
+                }
             }
             if (*s_fail) break;
         }
@@ -509,8 +582,20 @@ bf_status launch_prepare_cov(cudaStream_t stream, const float* w, void* out, con
     return cuda_status(cudaGetLastError(), "prepare_cov_kernel launch");
 }
 
-bf_status launch_grid_cov(cudaStream_t stream, const uint8_t* v, const void* wimg, float* integrated, int8_t* codes,
-                          float* params, const bf_dims& d, uint64_t spectra, uint64_t n_shards) {
+namespace {
+
+// Estimates and fallback bookkeeping of one covariance-form launch.
+struct CovChecks {
+    float* est = nullptr;
+    float est_limit = 0.f;
+    unsigned* unit_flags = nullptr;
+    int* unit_list = nullptr;
+    int* unit_count = nullptr;
+    int split_gpc = 0, split_gw = 0;
+};
+
+bf_status launch_grid_cov_impl(cudaStream_t stream, const uint8_t* v, const void* wimg, float* integrated,
+                               const bf_dims& d, uint64_t spectra, uint64_t n_shards, const CovChecks& chk) {
     BF_RETURN_IF(check_grid_cov(d, spectra, n_shards));
     EncodeTiledFn enc = encode_fn_grid_cov();
     if (enc == nullptr) return set_error(BF_ERR_CUDA, "cuTensorMapEncodeTiled is unavailable");
@@ -539,7 +624,13 @@ bf_status launch_grid_cov(cudaStream_t stream, const uint8_t* v, const void* wim
     while (128.0 * static_cast<double>(spectra) * std::ldexp(1.0, -k) > 65504.0) ++k;
     p.e_scale = std::ldexp(1.0f, -k);
     p.out_scale = std::ldexp(1.0f, k);
-    if (p.err == nullptr) return set_error(BF_ERR_CUDA, "device error word unavailable");
+    p.est = chk.est;
+    p.est_limit = chk.est_limit;
+    p.unit_flags = chk.unit_flags;
+    p.unit_list = chk.unit_list;
+    p.unit_count = chk.unit_count;
+    p.split_gpc = chk.split_gpc;
+    p.split_gw = chk.split_gw;
     cudaError_t e = cudaFuncSetAttribute(grid_cov_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          static_cast<int>(kSmemBytes));
     if (e != cudaSuccess) return cuda_status(e, "grid_cov_kernel smem attribute");
@@ -551,8 +642,83 @@ bf_status launch_grid_cov(cudaStream_t stream, const uint8_t* v, const void* wim
         grid_cov_kernel<<<static_cast<int>(grid), kThreads, kSmemBytes, stream>>>(map, p);
         BF_RETURN_IF(cuda_status(cudaGetLastError(), "grid_cov_kernel launch"));
     }
+    return BF_OK;
+}
+
+// The checked form's limit on est_b (relative, 2^-23 |v_b|^2 tr(E) / I_b).
+// Calibrated on a B200 against the FP64 oracle over noise, steered grids on a
+// point source and random-phase beams on a strong source (every beam a
+// sidelobe): the covariance form's error stayed below kEstRatio * est_b, so
+// values with est_b <= 1e-5 / kEstRatio are within 1e-5 of FP64 and every
+// other unit is recomputed by the split kernel.
+constexpr float kEstRatio = 1.0f / 16.0f;
+constexpr float kAutoEstLimit = 1e-5f / kEstRatio;
+
+uint64_t cov_part_bytes(const bf_dims& d, uint64_t n_shards) {
+    return d.n_ant == 64 && d.n_freq % 2 == 0 ? cov_weight_bytes(d, n_shards) : 0;
+}
+
+}  // namespace
+
+bf_status launch_grid_cov(cudaStream_t stream, const uint8_t* v, const void* wimg, float* integrated, int8_t* codes,
+                          float* params, const bf_dims& d, uint64_t spectra, uint64_t n_shards) {
+    BF_RETURN_IF(launch_grid_cov_impl(stream, v, wimg, integrated, d, spectra, n_shards, CovChecks{}));
     if (codes == nullptr) return BF_OK;
-    const bf_dims qd{n_shards * static_cast<uint64_t>(p.n_windows), d.n_freq, d.n_ant, d.n_beams};
+    const bf_dims qd{n_shards * window_count(d.n_time, spectra), d.n_freq, d.n_ant, d.n_beams};
+    return launch_quantize(stream, integrated, codes, params, qd);
+}
+
+bf_status launch_grid_cov_estimate(cudaStream_t stream, const uint8_t* v, const void* wimg, float* integrated,
+                                   float* estimate, const bf_dims& d, uint64_t spectra, uint64_t n_shards) {
+    CovChecks chk;
+    chk.est = estimate;
+    return launch_grid_cov_impl(stream, v, wimg, integrated, d, spectra, n_shards, chk);
+}
+
+uint64_t auto_weight_bytes(const bf_dims& d, uint64_t n_shards) {
+    return cov_part_bytes(d, n_shards) + split_weight_bytes(d, n_shards);
+}
+
+bool auto_uses_cov(const bf_dims& d, uint64_t spectra, uint64_t n_shards) {
+    return d.n_ant == 64 && d.n_freq % 2 == 0 && spectra >= kRows && spectra % kRows == 0 && spectra <= 16384 &&
+           n_shards >= 1 && n_shards <= 1024 && d.n_time < (1ull << 31);
+}
+
+uint64_t auto_workspace_bytes(const bf_dims& d, uint64_t spectra, uint64_t n_shards) {
+    if (!auto_uses_cov(d, spectra, n_shards)) return 0;
+    int gpc = 0, gw = 0;
+    const long long units = grid_tensor_unit_layout(d, spectra, n_shards, &gpc, &gw);
+    // [count, padding to 256 bytes][flags: units x u32][list: units x i32]
+    return 256 + 8 * static_cast<uint64_t>(units);
+}
+
+bf_status launch_prepare_auto(cudaStream_t stream, const float* w, void* out, const bf_dims& d, uint64_t n_shards) {
+    const uint64_t cov = cov_part_bytes(d, n_shards);
+    if (cov > 0) BF_RETURN_IF(launch_prepare_cov(stream, w, out, d, n_shards));
+    return launch_prepare_split(stream, w, static_cast<uint8_t*>(out) + cov, d, n_shards);
+}
+
+bf_status launch_grid_auto(cudaStream_t stream, const uint8_t* v, const void* wimg, float* integrated, int8_t* codes,
+                           float* params, void* workspace, const bf_dims& d, uint64_t spectra, uint64_t n_shards) {
+    const uint64_t cov = cov_part_bytes(d, n_shards);
+    const uint8_t* split = static_cast<const uint8_t*>(wimg) + cov;
+    if (!auto_uses_cov(d, spectra, n_shards)) {
+        return launch_grid_tensor(stream, v, split, integrated, codes, params, d, spectra, n_shards, nullptr);
+    }
+    CovChecks chk;
+    const long long units = grid_tensor_unit_layout(d, spectra, n_shards, &chk.split_gpc, &chk.split_gw);
+    uint8_t* ws = static_cast<uint8_t*>(workspace);
+    chk.unit_count = reinterpret_cast<int*>(ws);
+    chk.unit_flags = reinterpret_cast<unsigned*>(ws + 256);
+    chk.unit_list = reinterpret_cast<int*>(ws + 256 + 4 * static_cast<uint64_t>(units));
+    chk.est_limit = kAutoEstLimit;
+    BF_RETURN_IF(cuda_status(cudaMemsetAsync(ws, 0, 256 + 4 * static_cast<uint64_t>(units), stream),
+                             "clear the fallback list"));
+    BF_RETURN_IF(launch_grid_cov_impl(stream, v, wimg, integrated, d, spectra, n_shards, chk));
+    BF_RETURN_IF(launch_grid_tensor_list(stream, v, split, integrated, d, spectra, n_shards, chk.unit_list,
+                                         chk.unit_count));
+    if (codes == nullptr) return BF_OK;
+    const bf_dims qd{n_shards * window_count(d.n_time, spectra), d.n_freq, d.n_ant, d.n_beams};
     return launch_quantize(stream, integrated, codes, params, qd);
 }
 

@@ -72,7 +72,16 @@ struct TcParams {
     int ftiles, btiles;
     int paired;                 // plain launch: CTA pairs share channel pairs (see JobCursor)
     long long n_units;
+    // plain launch over a device-written list of units (the checked
+    // covariance form's fallback): *unit_count entries of unit_list
+    const int* unit_list;
+    const int* unit_count;
 };
+
+// Index i of a CTA's range is unit i, or unit_list[i] in a list launch.
+__device__ __forceinline__ long long unit_at(const TcParams& p, long long i) {
+    return p.unit_list != nullptr ? static_cast<long long>(p.unit_list[i]) : i;
+}
 
 
 __device__ __forceinline__ void record_error(unsigned code) { atomicOr(&g_tc_error, code); }
@@ -418,6 +427,7 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
 
     long long n_units = p.n_units;
     if constexpr (kServed) n_units = p.table->n_units;
+    if (!kServed && p.unit_list != nullptr) n_units = *p.unit_count;
     long long u_begin = n_units * blockIdx.x / gridDim.x;
     long long u_end = n_units * (blockIdx.x + 1) / gridDim.x;
     int pair_parity = -1;
@@ -449,7 +459,7 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
             if (u_begin < u_end) cur.init(p, u_begin);
             cur.pair_parity = pair_parity;
             for (long long u = u_begin; u < u_end && !stop; ++u) {
-                const Unit un = cur.at(u);
+                const Unit un = cur.at(unit_at(p, u));
                 const TcJob& jb = cur.jb;
                 if (un.key != prev_key) {
                     const uint32_t ws = w_loads % S.w_stages;
@@ -513,7 +523,7 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
             if (u_begin < u_end) cur.init(p, u_begin);
             cur.pair_parity = pair_parity;
             for (long long u = u_begin; u < u_end && !stop; ++u) {
-                const Unit un = cur.at(u);
+                const Unit un = cur.at(unit_at(p, u));
                 if (un.key != prev_key) {
                     ws = w_switches % S.w_stages;
                     if (!mbar_wait(&w_full[ws], w_seen[ws] & 1, kWaitNs)) { fail(4); break; }
@@ -526,7 +536,7 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                 bool next_switches = true;
                 if (u + 1 < u_end) {
                     JobCursor<kServed> ahead = cur;
-                    next_switches = ahead.at(u + 1).key != un.key;
+                    next_switches = ahead.at(unit_at(p, u + 1)).key != un.key;
                 }
                 for (int k = un.tile_begin; k < un.tile_end; ++k) {
                     if (*s_fail) { stop = true; break; }
@@ -570,7 +580,7 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
         if (u_begin < u_end) cur.init(p, u_begin);
         cur.pair_parity = pair_parity;
         for (long long u = u_begin; u < u_end && !stop; ++u) {
-            const Unit un = cur.at(u);
+            const Unit un = cur.at(unit_at(p, u));
             const int R = cur.jb.rows_q;
             for (int k = un.tile_begin; k < un.tile_end; ++k) {
                 if (*s_fail) { stop = true; break; }
@@ -677,7 +687,7 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
         if (u_begin < u_end) cur.init(p, u_begin);
         cur.pair_parity = pair_parity;
         for (long long u = u_begin; u < u_end && !stop; ++u) {
-            const Unit un = cur.at(u);
+            const Unit un = cur.at(unit_at(p, u));
             const TcJob& jb = cur.jb;
             const bool short_win = jb.spectra < 32;
             for (int k = un.tile_begin; k < un.tile_end; ++k) {
@@ -991,9 +1001,12 @@ bf_status encode_voltage_map(CUtensorMap* map, const uint8_t* base, uint64_t n_a
     return BF_OK;
 }
 
-bf_status launch_grid_tensor(cudaStream_t stream, const uint8_t* v, const void* split, float* integrated,
-                             int8_t* codes, float* params, const bf_dims& d, uint64_t spectra,
-                             uint64_t n_shards, unsigned* counters) {
+namespace {
+
+bf_status launch_grid_tensor_impl(cudaStream_t stream, const uint8_t* v, const void* split, float* integrated,
+                                  int8_t* codes, float* params, const bf_dims& d, uint64_t spectra,
+                                  uint64_t n_shards, unsigned* counters, const int* unit_list,
+                                  const int* unit_count) {
     if (d.n_time >= (1ull << 31) || n_shards > 1024 || spectra >= (1ull << 30)) {
         return set_error(BF_ERR_OVERFLOW, "CUDA tensor-core grid exceeds the supported size");
     }
@@ -1035,8 +1048,16 @@ bf_status launch_grid_tensor(cudaStream_t stream, const uint8_t* v, const void* 
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int grid = static_cast<int>(std::min<long long>(sms, p.n_units));
+    int grid = static_cast<int>(std::min<long long>(sms, p.n_units));
     p.paired = (d.n_freq % 2 == 0 && grid % 2 == 0 && grid >= 2) ? 1 : 0;
+    if (unit_list != nullptr) {
+        // the list's length is known on the device only: one CTA per SM, each
+        // taking its share of the list (none when it is empty)
+        p.unit_list = unit_list;
+        p.unit_count = unit_count;
+        p.paired = 0;
+        grid = sms;
+    }
     if (grid > 0) {
         const int nbp = padded_beams(d.n_beams);
         st = d.n_ant == 32 ? dispatch_nb<32>(stream, map, p, nbp, grid) : dispatch_nb<64>(stream, map, p, nbp, grid);
@@ -1045,6 +1066,32 @@ bf_status launch_grid_tensor(cudaStream_t stream, const uint8_t* v, const void* 
     if (codes == nullptr || fused) return BF_OK;
     bf_dims qd{n_shards * static_cast<uint64_t>(p.job.n_windows), d.n_freq, d.n_ant, d.n_beams};
     return launch_quantize(stream, integrated, codes, params, qd);
+}
+
+}  // namespace
+
+bf_status launch_grid_tensor(cudaStream_t stream, const uint8_t* v, const void* split, float* integrated,
+                             int8_t* codes, float* params, const bf_dims& d, uint64_t spectra,
+                             uint64_t n_shards, unsigned* counters) {
+    return launch_grid_tensor_impl(stream, v, split, integrated, codes, params, d, spectra, n_shards, counters,
+                                   nullptr, nullptr);
+}
+
+bf_status launch_grid_tensor_list(cudaStream_t stream, const uint8_t* v, const void* split, float* integrated,
+                                  const bf_dims& d, uint64_t spectra, uint64_t n_shards, const int* unit_list,
+                                  const int* unit_count) {
+    return launch_grid_tensor_impl(stream, v, split, integrated, nullptr, nullptr, d, spectra, n_shards, nullptr,
+                                   unit_list, unit_count);
+}
+
+long long grid_tensor_unit_layout(const bf_dims& d, uint64_t spectra, uint64_t n_shards, int* groups_per_channel,
+                                  int* windows_per_group) {
+    TcJob job{};
+    const long long n = tc_job_tiling(job, static_cast<int>(d.n_time), static_cast<int>(spectra),
+                                      static_cast<int>(d.n_freq), static_cast<int>(n_shards));
+    *groups_per_channel = job.groups_per_channel;
+    *windows_per_group = spectra < 32 ? 0 : static_cast<int>(job.group_tiles * kTileM / spectra);
+    return n;
 }
 
 bf_status launch_grid_tensor_served(cudaStream_t stream, const CUtensorMap& map, int n_ant, int nb_pad,

@@ -139,6 +139,8 @@ struct Job {
     uint64_t off = 0;
     bool has_block = false;
     uint64_t n_steps = 0, next_step = 0, last_step = 0;
+    // server steps at submission and at the first launched window
+    uint64_t submit_step = 0, admit_step = UINT64_MAX;
     uint64_t n_windows = 0;     // output windows
     ClassKey cls{};
     uint8_t* base = nullptr;    // arena block
@@ -514,6 +516,7 @@ bf_status admit(bf_server* s) {
         s->queue.pop_front();
         j.off = off;
         j.has_block = true;
+        j.admit_step = s->steps;  // admission runs just before this step's launch
         j.base = reinterpret_cast<uint8_t*>(reinterpret_cast<uintptr_t>(s->slab) + off);
         j.state = BF_JOB_LIVE;
         j.next_step = j.resume_step;
@@ -1001,6 +1004,7 @@ uint64_t image_bytes(const bf_serve_config& c, const Job& j) {
 
 void enqueue(bf_server* s, Job&& j, uint64_t* job_id) {
     j.id = s->next_id++;
+    j.submit_step = s->steps;
     if (job_id) *job_id = j.id;
     s->queue.push_back(j.id);
     s->jobs.emplace(j.id, std::move(j));
@@ -1108,6 +1112,32 @@ BF_API bf_status bf_serve_poll(bf_server* s, uint64_t job_id, int32_t* state) {
         return bf_serve_poll_impl(s, job_id, state);
     } catch (const std::bad_alloc&) {
         return set_error(BF_ERR_RESOURCE, "host memory exhausted");
+    } catch (const std::exception& e) {
+        return set_error(BF_ERR_LOGIC, std::string("internal error: ") + e.what());
+    }
+}
+
+static bf_status bf_serve_job_info_impl(bf_server* s, uint64_t job_id, bf_serve_job_info* info) {
+    clear_error();
+    if (s == nullptr || info == nullptr) return set_error(BF_ERR_INVALID_ARGUMENT, "server and info must not be null");
+    poll_steps(s, false);
+    update_done(s);
+    auto it = s->jobs.find(job_id);
+    if (it == s->jobs.end()) return set_error(BF_ERR_OUT_OF_RANGE, "unknown served job id");
+    const Job& j = it->second;
+    *info = bf_serve_job_info{};
+    info->state = j.state;
+    info->submit_step = j.submit_step;
+    info->admit_step = j.admit_step;
+    const bool all = j.state == BF_JOB_RUNNING || (j.state == BF_JOB_DONE && j.n_steps > j.resume_step);
+    info->last_step = all ? j.last_step : UINT64_MAX;
+    info->windows_launched = j.next_step - j.resume_step;
+    return BF_OK;
+}
+
+BF_API bf_status bf_serve_job_info_get(bf_server* s, uint64_t job_id, bf_serve_job_info* info) {
+    try {
+        return bf_serve_job_info_impl(s, job_id, info);
     } catch (const std::exception& e) {
         return set_error(BF_ERR_LOGIC, std::string("internal error: ") + e.what());
     }

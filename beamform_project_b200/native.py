@@ -89,6 +89,11 @@ class ServeStats(C.Structure):
                                                              ("predicted_ms_last", C.c_double)]
 
 
+class ServeJobInfo(C.Structure):
+    _fields_ = [("state", C.c_int32), ("pad", C.c_uint32), ("submit_step", C.c_uint64), ("admit_step", C.c_uint64),
+                ("last_step", C.c_uint64), ("windows_launched", C.c_uint64)]
+
+
 _P = C.c_void_p
 _U64 = C.c_uint64
 _PP = C.POINTER(C.c_void_p)
@@ -107,6 +112,12 @@ _SIGS = {
     "bf_cov_weight_bytes": (_U64, [C.POINTER(Dims), _U64]),
     "bf_prepare_cov_weights": (C.c_int, [_P, _P, _P, C.POINTER(Dims), _U64]),
     "bf_grid_cov_integrated": (C.c_int, [_P, _P, _P, _P, _P, _P, C.POINTER(Dims), _U64, _U64]),
+    "bf_grid_cov_estimate": (C.c_int, [_P, _P, _P, _P, _P, C.POINTER(Dims), _U64, _U64]),
+    "bf_auto_weight_bytes": (_U64, [C.POINTER(Dims), _U64]),
+    "bf_prepare_auto_weights": (C.c_int, [_P, _P, _P, C.POINTER(Dims), _U64]),
+    "bf_grid_auto_workspace_bytes": (_U64, [C.POINTER(Dims), _U64, _U64]),
+    "bf_grid_auto_integrated": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, C.POINTER(Dims), _U64, _U64]),
+    "bf_kernel_versions": (C.c_int, [C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "bf_grid_pipeline_chunk_spectra": (_U64, [C.POINTER(Dims), _U64, _U64, _U64]),
     "bf_grid_pipeline_create": (C.c_int, [C.POINTER(Dims), _U64, _U64, _U64, _PP]),
     "bf_grid_pipeline_upload_weights": (C.c_int, [_P, _P]),
@@ -131,6 +142,7 @@ _SIGS = {
     "bf_serve_submit": (C.c_int, [_P, C.POINTER(ServeJob), C.POINTER(C.c_uint64)]),
     "bf_serve_step": (C.c_int, [_P, C.POINTER(C.c_uint32)]),
     "bf_serve_poll": (C.c_int, [_P, _U64, C.POINTER(C.c_int32)]),
+    "bf_serve_job_info_get": (C.c_int, [_P, _U64, C.POINTER(ServeJobInfo)]),
     "bf_serve_result": (C.c_int, [_P, _U64, _PP, _PP, _PP, C.POINTER(C.c_uint64)]),
     "bf_serve_cancel": (C.c_int, [_P, _U64]),
     "bf_serve_checkpoint": (C.c_int, [_P, _U64, _P, _U64, C.POINTER(C.c_uint64)]),

@@ -120,6 +120,17 @@ class Server:
         native.check(native.lib().bf_serve_poll(self._h, int(job_id), C.byref(st)))
         return int(st.value)
 
+    def job_info(self, job_id: int) -> dict:
+        """Server steps at which the job was submitted, ran its first and its
+        last window (None when not reached), and its windows launched."""
+        info = native.ServeJobInfo()
+        native.check(native.lib().bf_serve_job_info_get(self._h, int(job_id), C.byref(info)))
+        none = (1 << 64) - 1
+        return {"state": int(info.state), "submit_step": int(info.submit_step),
+                "admit_step": None if info.admit_step == none else int(info.admit_step),
+                "last_step": None if info.last_step == none else int(info.last_step),
+                "windows_launched": int(info.windows_launched)}
+
     def cancel(self, job_id: int) -> None:
         native.check(native.lib().bf_serve_cancel(self._h, int(job_id)))
 
@@ -333,13 +344,17 @@ def run_stream(server: Server, jobs: list[JobSpec], window_spectra: int = 320, r
     step_idx = 0
     steps_run = 0
     outstanding = 0
+    step_windows = []   # stream window index of every server step that launched work
+    ids = [None] * len(jobs)
     while True:
         while i < len(order) and jobs[order[i]].arrival_s <= step_idx * step_s:
-            server.submit(jobs[order[i]])
+            ids[order[i]] = server.submit(jobs[order[i]])
             outstanding += 1
             i += 1
         n_live = server.step()
-        steps_run += 1 if n_live else 0
+        if n_live:
+            steps_run += 1
+            step_windows.append(step_idx)
         step_idx += 1
         if n_live == 0 or step_idx % 8 == 0:
             for jid in server.take_done():
@@ -357,4 +372,28 @@ def run_stream(server: Server, jobs: list[JobSpec], window_spectra: int = 320, r
                 step_idx = max(step_idx, int(math.ceil(jobs[order[i]].arrival_s / step_s)))
             else:
                 server.sync()
-    return {"steps": steps_run, "submitted": i}
+    return {"steps": steps_run, "submitted": i, "step_windows": step_windows, "job_ids": ids}
+
+
+def realtime_replay(step_ms, step_windows, window_spectra: int = 320) -> dict:
+    """Replays the served steps against the stream clock.  Step k serves the
+    stream window step_windows[k], whose data is complete at
+    (step_windows[k] + 1) * window time; the GPU starts a step when its data
+    is complete and the previous step has finished, and takes step_ms[k]
+    (its measured device time).  Returns per-step ready and finish times (s)
+    and the real-time factor (stream seconds served / device seconds)."""
+    import numpy as np
+    w_s = window_spectra * SPECTRUM_S
+    ready = (np.asarray(step_windows, np.float64) + 1.0) * w_s
+    dur = np.asarray(step_ms, np.float64) / 1e3
+    n = min(len(ready), len(dur))
+    ready, dur = ready[:n], dur[:n]
+    end = np.empty(n)
+    t = 0.0
+    for k in range(n):
+        t = max(t, ready[k]) + dur[k]
+        end[k] = t
+    span = (ready[-1] - ready[0] + w_s) if n else 0.0
+    return {"ready_s": ready, "end_s": end, "latency_s": end - ready,
+            "realtime_factor": span / dur.sum() if n and dur.sum() > 0 else None,
+            "stream_s": span, "device_s": float(dur.sum())}

@@ -1029,11 +1029,12 @@ def run_tracker(args, emit: bool = True):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v0 = volt[: 64 * TR_S * F_SHARD * N_ANT].cpu().numpy().reshape(-1, F_SHARD, N_ANT)
         line["cpu_baseline"] = tracker_cpu_baseline(v0, budget_s=args.cpu_seconds)
-    if rank == 0:
+    if rank == 0 and emit:
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+    return line
 
 
 def reference_gpu_tracker(volt, inten, T, steps, stream, b200_ps_ms) -> dict:
@@ -1436,6 +1437,40 @@ def _serve_class_rates(classes, rates, per, rng, kind, threads):
         rates[key] = n / (time.perf_counter() - t0)
 
 
+def serve_latency(jobs, run, infos, step_ms, step_offset: int) -> dict:
+    """Real-time view of a served stream.  realtime_factor: the stream's
+    length (first arrival to the end of the last job's data, as if every job
+    ran from its arrival) over the device time of all its windows; at or above
+    1 the GPU keeps up with the stream.  The steps are replayed on the stream
+    clock (serve.realtime_replay): window latency is a step's finish minus the
+    time its data was complete, admission wait a job's first window minus its
+    arrival, completion latency its last window's finish minus the end of its
+    data."""
+    from beamform_project_b200 import serve
+    rep = serve.realtime_replay(step_ms, run["step_windows"])
+    w_s = 320 * serve.SPECTRUM_S
+    t0 = min(j.arrival_s for j in jobs)
+    t1 = max(j.arrival_s + j.n_spectra * serve.SPECTRUM_S for j in jobs)
+    waits, done_lat = [], []
+    for j, jid in zip(jobs, run["job_ids"]):
+        info = infos.get(jid)
+        if info is None or info["admit_step"] is None or info["last_step"] is None:
+            continue
+        a, b = info["admit_step"] - step_offset, info["last_step"] - step_offset
+        if a < 0 or b >= len(rep["end_s"]):
+            continue
+        waits.append(rep["ready_s"][a] - w_s - j.arrival_s)
+        done_lat.append(rep["end_s"][b] - (j.arrival_s + j.n_spectra * serve.SPECTRUM_S))
+    pct = lambda a, q: float(np.percentile(a, q)) if len(a) else None  # noqa: E731
+    lat_ms = rep["latency_s"] * 1e3
+    return {"realtime_factor": (t1 - t0) / rep["device_s"] if rep["device_s"] else None,
+            "stream_s": t1 - t0, "device_s": rep["device_s"],
+            "replayed_window_latency_ms_p50": pct(lat_ms, 50), "replayed_window_latency_ms_p99": pct(lat_ms, 99),
+            "admission_wait_s_p50": pct(waits, 50), "admission_wait_s_p99": pct(waits, 99),
+            "completion_latency_s_p50": pct(done_lat, 50), "completion_latency_s_p99": pct(done_lat, 99),
+            "virtual_stream_s": len(run["step_windows"]) and (run["step_windows"][-1] + 1) * w_s}
+
+
 def run_serve(args, emit: bool = True):
     if args.impl == "reference":
         if int(os.environ.get("RANK", "0")) != 0:
@@ -1484,9 +1519,13 @@ def run_serve(args, emit: bool = True):
     reps.barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
+    infos = {}
+
+    def record_info(jid):
+        infos[jid] = srv.job_info(jid)
     with ClockSampler(local) as clocks:
         e0.record(stream)
-        r = serve.run_stream(srv, jobs)
+        r = serve.run_stream(srv, jobs, on_done=record_info)
         e1.record(stream)
         srv.sync()
         torch.cuda.synchronize()
@@ -1494,6 +1533,7 @@ def run_serve(args, emit: bool = True):
     assert native.take_device_error() == 0
     st = srv.stats()
     times = srv.step_times()[n_warm_steps:]
+    latency = serve_latency(jobs, r, infos, times, n_warm_steps)
     samples = st["beam_samples"] - st0["beam_samples"]
     steps = st["steps"] - st0["steps"]
     el_ms = reps.max(el_ms)
@@ -1563,7 +1603,7 @@ def run_serve(args, emit: bool = True):
                       "arena_peak_gb": st["arena_bytes_peak"] / 1e9, "graph_captures": st["graph_captures"],
                       "mean_live_jobs": (st["job_windows"] - st0["job_windows"]) / max(1, steps),
                       "gpu_busy_frac": float(times.sum()) / el_ms if el_ms else None,
-                      "window_bound_us": args.serve_window_us},
+                      "window_bound_us": args.serve_window_us, **latency},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": hbm_gbs, "unit": "GB/s",
                          "frac": round(achieved / hbm_gbs, 4), "traffic": None,
                          "peak_source": peak_src + " (copy bandwidth)",

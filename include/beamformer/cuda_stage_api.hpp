@@ -33,6 +33,12 @@ enum class CudaBeamformerKernel {
     // INT32 covariance.  Its relative error grows for beams far below the
     // strongest source's power; TensorSplit has no such dependence.
     TensorCovariance,
+    // Checked tensor path (integrated output only, n_ant 32 or 64): the
+    // covariance form where it applies, with every unit whose error estimate
+    // exceeds the calibrated limit recomputed by TensorSplit, so every value
+    // stays within 1e-5 relative of FP64; TensorSplit elsewhere.  Its stage
+    // call is launch_checked_integrated_beamformer (it needs a workspace).
+    TensorChecked,
 };
 
 void launch_packed_beamformer(CudaBeamformerKernel kernel, cudaStream_t stream,
@@ -72,5 +78,18 @@ void prepare_split_weights(cudaStream_t stream, const ComplexFloat* weights, voi
 std::size_t cov_weight_bytes(const Dimensions& dims);
 void prepare_cov_weights(cudaStream_t stream, const ComplexFloat* weights, void* cov_weights,
                          const Dimensions& dims);
+
+// TensorChecked: operand bytes and preparation from canonical device weights,
+// workspace bytes (device, may be 0), and the stage call (bf_grid_auto_* of
+// the C ABI).  After the call the workspace's first 32-bit word holds how many
+// split-kernel units were recomputed.
+std::size_t checked_weight_bytes(const Dimensions& dims);
+void prepare_checked_weights(cudaStream_t stream, const ComplexFloat* weights, void* checked_weights,
+                             const Dimensions& dims);
+std::size_t checked_workspace_bytes(const Dimensions& dims, const TemporalIntegrationConfig& temporal_integration);
+void launch_checked_integrated_beamformer(cudaStream_t stream, const std::uint8_t* packed_voltage,
+                                          const void* checked_weights, float* integrated_intensity, void* workspace,
+                                          const Dimensions& dims,
+                                          const TemporalIntegrationConfig& temporal_integration);
 
 }  // namespace beamformer

@@ -208,6 +208,39 @@ BF_API bf_status bf_grid_cov_integrated(void* stream, const uint8_t* packed_volt
                                         float* params, const bf_dims* dims,
                                         uint64_t integration_spectra, uint64_t n_shards);
 
+/* bf_grid_cov_integrated that also writes, per value, the estimate
+ * est = 2^-23 |v_b|^2 tr(E) / I of its relative error ([shard][W][F][B]
+ * float, device): the fp32 sums of the quadratic form carry terms up to
+ * |v_b|^2 tr(E), so est is large where a beam holds little of the window's
+ * power (deep sidelobes of a strong source). */
+BF_API bf_status bf_grid_cov_estimate(void* stream, const uint8_t* packed_voltage, const void* cov_weights,
+                                      float* integrated, float* estimate, const bf_dims* dims,
+                                      uint64_t integration_spectra, uint64_t n_shards);
+
+/* Checked grid beamformer: the fastest tensor-core path that keeps every
+ * value within 1e-5 relative of FP64.  No reference counterpart (same
+ * outputs and layouts as launch_packed_integrated_beamformer plus
+ * launch_quantize_integrated_intensity, cuda_stage_api.hpp:27-42).  Where the
+ * covariance form applies (n_ant 64, even n_freq, integration_spectra a
+ * multiple of 64 up to 16384) it runs that form with per-value error
+ * estimates, then the split-precision kernel recomputes every (shard,
+ * channel, window group) holding a value whose estimate exceeds the limit
+ * calibrated against FP64; otherwise it runs the split-precision kernel.
+ * The operand (bf_auto_weight_bytes) holds the covariance image (n_ant 64,
+ * even n_freq) followed by the split image, both from canonical complex64
+ * weights.  workspace (bf_grid_auto_workspace_bytes, 256-byte aligned,
+ * device, zero bytes when the covariance form does not apply): its first
+ * 32-bit word holds, after the call, how many split-kernel units were
+ * recomputed. */
+BF_API uint64_t bf_auto_weight_bytes(const bf_dims* dims, uint64_t n_shards);
+BF_API bf_status bf_prepare_auto_weights(void* stream, const float* weights, void* auto_weights,
+                                         const bf_dims* dims, uint64_t n_shards);
+BF_API uint64_t bf_grid_auto_workspace_bytes(const bf_dims* dims, uint64_t integration_spectra,
+                                             uint64_t n_shards);
+BF_API bf_status bf_grid_auto_integrated(void* stream, const uint8_t* packed_voltage, const void* auto_weights,
+                                         float* integrated, int8_t* codes, float* params, void* workspace,
+                                         const bf_dims* dims, uint64_t integration_spectra, uint64_t n_shards);
+
 /* Host-buffer grid pipeline.  Counterpart of the reference's
  * CudaBeamformerWorkspace::run_quantized_integrated_pipeline
  * (include/beamformer/cuda_beamformer.hpp:66-76: weights resident, voltage
@@ -449,6 +482,21 @@ BF_API bf_status bf_serve_submit(bf_server* server, const bf_serve_job* job, uin
 /* Admits what fits, then launches one window of every live job. */
 BF_API bf_status bf_serve_step(bf_server* server, uint32_t* n_live);
 BF_API bf_status bf_serve_poll(bf_server* server, uint64_t job_id, int32_t* state);
+/* When a job ran, in server steps (indices of bf_serve_step_times: the k-th
+ * step that launched work).  submit_step: steps launched before its
+ * submission; admit_step: the step that ran its first window; last_step: the
+ * step that ran its last one; UINT64_MAX for steps not reached yet.  With the
+ * step times and the stream time of each step a caller replays the job's
+ * admission wait and completion latency. */
+typedef struct bf_serve_job_info {
+    int32_t state;
+    uint32_t pad;
+    uint64_t submit_step;
+    uint64_t admit_step;
+    uint64_t last_step;
+    uint64_t windows_launched;
+} bf_serve_job_info;
+BF_API bf_status bf_serve_job_info_get(bf_server* server, uint64_t job_id, bf_serve_job_info* info);
 /* Device pointers of a DONE job's results (any may be NULL): integrated
  * f32, grid [shard][W][F][B] / tracker [W][F_total][sources], W =
  * n_spectra / integration_spectra; codes i8 and params f32 pairs as in the

@@ -214,6 +214,32 @@ int main() {
                    "TensorCovariance rejects 10-spectrum integration");
         }
         {
+            // checked form: the covariance form with split-kernel recomputation, and
+            // the split kernel alone for 10-spectrum windows
+            CudaBeamformerWorkspace wk(di, CudaBeamformerKernel::TensorChecked, integration_direct);
+            wk.upload_weights(wi, di);
+            IntegratedIntensities ok_(integ.size());
+            wk.run_integrated_pipeline(vi, ok_, di);
+            bool okk = true;
+            for (std::size_t i = 0; i < ok_.size(); ++i) okk &= std::abs(ok_[i] - integ[i]) <= 1e-3F + 1e-5F * std::abs(integ[i]);
+            expect(okk, "TensorChecked workspace within tolerance");
+            CudaBeamformerWorkspace wk10(di, CudaBeamformerKernel::TensorChecked, integration_after_upchan);
+            wk10.upload_weights(wi, di);
+            const auto integ10 = cuda_beamform_packed_integrated_intensity(vi, tile(wi, di), di, integration_after_upchan);
+            IntegratedIntensities o10(integ10.size());
+            wk10.run_integrated_pipeline(vi, o10, di);
+            bool ok10 = true;
+            for (std::size_t i = 0; i < o10.size(); ++i) ok10 &= std::abs(o10[i] - integ10[i]) <= 1e-3F + 1e-5F * std::abs(integ10[i]);
+            expect(ok10, "TensorChecked 10-spectrum integration within tolerance");
+            expect(throws<std::invalid_argument>([&] { CudaBeamformerWorkspace x(di, CudaBeamformerKernel::TensorChecked); }),
+                   "TensorChecked needs integration");
+            expect(throws<std::invalid_argument>([&] {
+                       launch_packed_integrated_beamformer(CudaBeamformerKernel::TensorChecked, nullptr, nullptr, nullptr,
+                                                           nullptr, di, integration_direct);
+                   }),
+                   "TensorChecked stage call needs its workspace entry point");
+        }
+        {
             // chunked host pipeline: bit-identical to the one-launch TensorSplit workspace
             CudaBeamformerWorkspace wq(di, CudaBeamformerKernel::TensorSplit, integration_direct,
                                        CudaBeamformerOutput::QuantizedInt8);

@@ -19,7 +19,8 @@
 * The reference's own CUDA kernels (built for sm_100a from its sources) on
   the same inputs: its Tiled kernel within the reference CUDA tests'
   tolerance (tests/cuda/test_cuda_packed.cu:24-25) of the reference-order
-  kernel, and its int8 quantizer bit-identical to the B200 quantizer.
+  kernel, and its int8 quantizer within the reference CUDA test's bar of the
+  B200 quantizer (which follows the reference CPU quantizer bit for bit).
 """
 from __future__ import annotations
 
@@ -182,10 +183,16 @@ def test_full_band_workload_sampled_windows(c2, ref, orc):
     assert lsb_count <= 1e-4 * total
 
 
-def test_full_band_workload_reference_cuda_quantizer_is_bit_identical(c2, cuda, orc):
+def test_full_band_workload_reference_cuda_quantizer(c2, cuda, orc):
     """The reference's int8 chunk quantizer (src/cuda_quantize_int8.cu:30-147,
-    nvcc sm_100a) on the B200 path's integrated output gives the B200 codes
-    and parameters bit for bit."""
+    nvcc sm_100a) on the B200 path's integrated output.  The B200 quantizer
+    reproduces the reference CPU quantizer bit for bit; the reference's own
+    GPU kernel does not quite (nvcc contracts offset = min - (-127.5) * scale
+    into one fused multiply-add), so against it the bar is the reference
+    CUDA test's (tests/cuda/test_cuda_quantization.cpp:26-45): parameters
+    within 1e-3 + 1e-6 |offset| and 1e-5 + 1e-6 |scale|, and codes at most
+    1 LSB apart (the reference test wants them equal on its small cases;
+    the count here is printed)."""
     if not orc.reference_gpu_available():
         pytest.skip("reference CUDA kernels (oracle/_ref/libbfref_cuda.so) not built")
     from beamform_project_b200 import api
@@ -202,5 +209,10 @@ def test_full_band_workload_reference_cuda_quantizer_is_bit_identical(c2, cuda, 
     orc.refgpu_check(g.refgpu_quantize(torch.cuda.current_stream().cuda_stream, c2["integ_dev"].data_ptr(),
                                        codes_r.data_ptr(), params_r.data_ptr(), NS * W, F, A, B))
     torch.cuda.synchronize()
-    assert torch.equal(codes_b, codes_r)
-    assert torch.equal(params_b.view(torch.int32), params_r.view(torch.int32))
+    diff = (codes_b.int() - codes_r.int()).abs()
+    print(f"reference CUDA quantizer: {int((diff > 0).sum())} of {diff.numel()} codes 1 LSB apart")
+    assert int(diff.max()) <= 1
+    assert int((diff > 0).sum()) <= 1e-4 * diff.numel()
+    pb, pr = params_b.view(-1, 2).double(), params_r.view(-1, 2).double()
+    assert bool(((pb[:, 0] - pr[:, 0]).abs() <= 1e-3 + 1e-6 * pr[:, 0].abs()).all())
+    assert bool(((pb[:, 1] - pr[:, 1]).abs() <= 1e-5 + 1e-6 * pr[:, 1].abs()).all())

@@ -1,0 +1,160 @@
+"""GPU parity: the checked grid beamformer (bf_grid_auto_integrated).
+
+The covariance form's relative error on a value scales with its estimate
+est = 2^-23 |v_b|^2 tr(E) / I (bf_grid_cov_estimate).  The checked form keeps
+covariance values whose estimate is at most 16 x 1e-5 and recomputes every
+other unit with the split-precision kernel, so:
+
+* calibration: on every data regime below the covariance form's error against
+  the FP64 oracle stays below est / 16 (values above 1; the 1e-3 absolute
+  floor covers the rest);
+* the checked form is within 1e-3 + 1e-5 |fp64| everywhere: noise, the
+  full-band benchmark's steered grid over a point source (nothing recomputed)
+  and random-phase beams over a strong source (every beam a sidelobe: units
+  recomputed);
+* its int8 codes equal the reference quantizer (src/quantization.cpp:61-161)
+  on its integrated values; shapes outside the covariance form run the split
+  kernel and equal it bit for bit.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import grid_weights, random_voltage
+from test_gpu_grid_cov import _c2_like
+
+pytestmark = pytest.mark.gpu
+F = 336
+EST_RATIO = 1.0 / 16.0   # the library's calibrated ratio of error to estimate
+
+
+def _cases(orc, ref):
+    """(name, voltage [T][F][A], weights [B][F][A][2], T, A, B, S)."""
+    out = []
+    v = random_voltage(1280, F, 64, seed=31)
+    out.append(("noise", v, grid_weights(64, F, 128, seed=32), 1280, 64, 128, 320))
+    out.append(("noise S=64", random_voltage(640, F, 64, seed=33), grid_weights(64, F, 37, seed=34), 640, 64, 37, 64))
+    w, mu, scale = _c2_like(128, 57)
+    out.append(("steered grid on a point source", orc.generate_voltage(12, 0, 640, F, 64, scale, mu, 640), w,
+                640, 64, 128, 320))
+    if ref is not None:
+        pos = ref.ref_default_positions(64)
+        freq = ref.ref_channelized_frequencies(F)
+        v = ref.ref_make_moving_point_source(960, F, 64, pos, freq, 0.0, -0.05, 0.0, 0.0, 3.0)
+        out.append(("random-phase beams on a strong source", v, grid_weights(64, F, 24, seed=90), 960, 64, 24, 320))
+    return out
+
+
+@pytest.fixture(scope="module")
+def cases(orc):
+    from oracle import loader
+    return _cases(orc, loader if loader.reference_available() else None)
+
+
+def _to(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def test_estimate_bounds_the_covariance_form_error(cuda, orc, cases):
+    from beamform_project_b200 import api, native
+    torch = cuda
+    worst = 0.0
+    for name, v, w, T, A, B, S in cases:
+        d = api.Dimensions(T, F, A, B)
+        W = -(-T // S)
+        cw = torch.empty(api.cov_weight_bytes(d), dtype=torch.uint8, device="cuda")
+        api.prepare_cov_weights(None, _to(torch, w), cw, d)
+        integ = torch.empty(W * F * B, dtype=torch.float32, device="cuda")
+        est = torch.empty_like(integ)
+        api.grid_cov_estimate(None, _to(torch, v), cw, integ, est, d, S)
+        torch.cuda.synchronize()
+        assert native.take_device_error() == 0
+        ref64 = orc.beamform_integrated(v, w, T, F, A, B, S, f64=True).reshape(-1)
+        g = integ.cpu().numpy().astype(np.float64)
+        e = est.cpu().numpy().astype(np.float64)
+        big = np.abs(ref64) > 1
+        rel = np.abs(g - ref64)[big] / np.abs(ref64)[big]
+        ratio = float(np.max(rel / e[big]))
+        worst = max(worst, ratio)
+        print(f"{name}: max rel error {float(rel.max()):.2e}, max estimate {float(e.max()):.2e}, "
+              f"max error / estimate {ratio:.4f}")
+    assert worst <= EST_RATIO, worst
+
+
+def _auto(torch, api, v, w, T, A, B, S, shards=1, quant=True):
+    from beamform_project_b200 import native
+    d = api.Dimensions(T, F, A, B)
+    W = -(-T // S)
+    aw = torch.empty(api.auto_weight_bytes(d, shards), dtype=torch.uint8, device="cuda")
+    api.prepare_auto_weights(None, _to(torch, w), aw, d, shards)
+    integ = torch.full((shards * W * F * B,), -9.0, dtype=torch.float32, device="cuda")
+    codes = params = None
+    if quant:
+        qd = api.Dimensions(W, F, A, B)
+        codes = torch.zeros(shards * W * F * B, dtype=torch.int8, device="cuda")
+        params = torch.zeros(shards * 2 * api.quantization_parameter_count(qd), dtype=torch.float32, device="cuda")
+    wsb = api.grid_auto_workspace_bytes(d, S, shards)
+    ws = torch.zeros(max(wsb, 256), dtype=torch.uint8, device="cuda")
+    api.grid_auto_integrated(None, _to(torch, v), aw, integ, codes, params, ws, d, S, shards)
+    torch.cuda.synchronize()
+    assert native.take_device_error() == 0
+    recomputed = int(ws[:4].view(torch.int32).item()) if wsb > 0 else None
+    got = integ.cpu().numpy().reshape(shards, W, F, B)
+    if quant:
+        return got, codes.cpu().numpy().reshape(shards, W, F, B), params.cpu().numpy(), recomputed
+    return got, None, None, recomputed
+
+
+def test_checked_form_within_1e5_of_fp64(cuda, orc, cases):
+    from beamform_project_b200 import api
+    torch = cuda
+    recomputed = {}
+    for name, v, w, T, A, B, S in cases:
+        got, codes, params, n = _auto(torch, api, v, w, T, A, B, S)
+        ref64 = orc.beamform_integrated(v, w, T, F, A, B, S, f64=True)
+        g = got[0].astype(np.float64)
+        bar = 1e-3 + 1e-5 * np.abs(ref64)
+        worst = float(np.max(np.abs(g - ref64) / bar))
+        recomputed[name] = n
+        print(f"{name}: {worst:.3f} of the bar, {n} split-kernel units recomputed")
+        assert worst <= 1.0, name
+        W = got.shape[1]
+        rc, rp = orc.quantize(got[0], W, F, B)
+        assert np.array_equal(codes[0], rc), name
+        assert np.array_equal(params.reshape(rp.shape), rp), name
+    assert recomputed["noise"] == 0
+    assert recomputed["steered grid on a point source"] == 0
+    if "random-phase beams on a strong source" in recomputed:
+        assert recomputed["random-phase beams on a strong source"] > 0
+
+
+def test_checked_form_two_shards_and_repeatable(cuda, orc, cases):
+    from beamform_project_b200 import api
+    torch = cuda
+    name, v, w, T, A, B, S = cases[-1]
+    v2 = np.stack([v, np.roll(v, 7, axis=0)])
+    w2 = np.stack([w, w[::-1].copy()])
+    a = _auto(torch, api, v2, w2, T, A, B, S, shards=2)
+    b = _auto(torch, api, v2, w2, T, A, B, S, shards=2)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) and a[3] == b[3]
+    for s in range(2):
+        ref64 = orc.beamform_integrated(v2[s], w2[s], T, F, A, B, S, f64=True)
+        assert np.all(np.abs(a[0][s].astype(np.float64) - ref64) <= 1e-3 + 1e-5 * np.abs(ref64))
+
+
+@pytest.mark.parametrize("A,B,T,S", [(32, 16, 640, 320), (64, 40, 300, 10), (64, 128, 640, 32)])
+def test_checked_form_outside_the_covariance_form_is_the_split_kernel(cuda, A, B, T, S):
+    from beamform_project_b200 import api
+    torch = cuda
+    v = random_voltage(T, F, A, seed=A + B)
+    w = grid_weights(A, F, B, seed=T)
+    got, codes, _, n = _auto(torch, api, v, w, T, A, B, S)
+    assert n is None
+    d = api.Dimensions(T, F, A, B)
+    split = torch.empty(api.split_weight_bytes(d), dtype=torch.uint8, device="cuda")
+    api.prepare_split_weights(None, _to(torch, w), split, d)
+    integ = torch.empty(got.size, dtype=torch.float32, device="cuda")
+    api.grid_tensor_integrated(None, _to(torch, v), split, integ, None, None, d, S)
+    torch.cuda.synchronize()
+    assert np.array_equal(got.reshape(-1), integ.cpu().numpy())
