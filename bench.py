@@ -582,6 +582,31 @@ def run_gpu(args):
                "int8_max_lsb": int(lsb.max().item())}
         del covw, integ_c, codes_c, params_c
 
+        # the checked form (covariance form + split-kernel recomputation of
+        # every unit whose error estimate is above the calibrated limit)
+        aw = torch.empty(api.auto_weight_bytes(d, N_SHARDS), dtype=torch.uint8, device=dev)
+        api.prepare_auto_weights(None, weights, aw, d, N_SHARDS)
+        aws = torch.zeros(max(256, api.grid_auto_workspace_bytes(d, S_INT, N_SHARDS)), dtype=torch.uint8,
+                          device=dev)
+        integ_a = torch.empty_like(integ)
+
+        def auto_step():
+            api.grid_auto_integrated(None, volt, aw, integ_a, None, None, aws, d, S_INT, N_SHARDS)
+
+        auto_step()
+        torch.cuda.synchronize()
+        a_ms = event_time(stream, auto_step, args.cov_steps)
+        assert native.take_device_error() == 0
+        n_units = int(aws[:4].view(torch.int32).item())
+        rel = ((integ_a.double() - integ_p.double()).abs() / integ_p.double().abs().clamp_min(1e-30)).max().item()
+        cov["checked_form"] = {
+            "kernel": "grid_cov_kernel with error estimates + grid_tensor_kernel over the listed units",
+            "ms_per_step": a_ms, "value": samples_per_step / (a_ms / 1e3),
+            "algorithmic_tflops": (8 * T_SPECTRA * N_SHARDS * F_SHARD * N_ANT * N_BEAMS
+                                   + 3 * samples_per_step) / (a_ms / 1e3) / 1e12,
+            "units_recomputed": n_units, "max_rel_diff_vs_plain": rel}
+        del aw, aws, integ_a
+
     # the reference's own CUDA kernels (Tiled + int8 quantizer) on the same GPU and inputs
     ref_gpu = None
     if kernel == "tensor" and args.ref_gpu_steps > 0:
