@@ -317,6 +317,93 @@ def grid_auto_integrated(stream, packed_voltage, auto_weights, integrated, codes
                                                int(integration_spectra), int(n_shards)))
 
 
+# --------------------------------------------------------------------------
+# autotuner of the grid path (bf_autotune_grid, bf_tune_*)
+# --------------------------------------------------------------------------
+
+GRID_FORMS = {0: "split", 1: "checked covariance"}
+
+
+def _cfg_dict(c) -> dict:
+    return {"form": GRID_FORMS[int(c.form)], "group_mult": int(c.group_mult), "paired": bool(c.paired)}
+
+
+def autotune_grid(stream, dims: Dimensions, integration_spectra: int, n_shards: int = 1) -> dict:
+    """Time every launch choice of the grid path for this class (n_ant,
+    padded beams, integration) on seeded synthetic data, keep those whose
+    products agree with the default's, record the fastest in the tuning
+    table (used by later untuned calls) and return the candidates."""
+    validate_dimensions(dims)
+    cap = 16
+    cands = (native.GridConfig * cap)()
+    ms = (C.c_float * cap)()
+    ok = (C.c_uint8 * cap)()
+    n = C.c_uint32(0)
+    best = C.c_uint32(0)
+    d = dims.c()
+    check(native.lib().bf_autotune_grid(_stream_handle(stream), C.byref(d), int(integration_spectra), int(n_shards),
+                                        cands, ms, ok, cap, C.byref(n), C.byref(best)))
+    rows = [{**_cfg_dict(cands[i]), "ms": float(ms[i]), "ok": bool(ok[i])} for i in range(n.value)]
+    return {"candidates": rows, "best": int(best.value), "chosen": rows[best.value]}
+
+
+def tune_get(n_ant: int, nb_pad: int, integration_spectra: int, device: str | None = None) -> dict | None:
+    c = native.GridConfig()
+    found = C.c_int32(0)
+    check(native.lib().bf_tune_get(device.encode() if device else None, int(n_ant), int(nb_pad),
+                                   int(integration_spectra), C.byref(c), C.byref(found)))
+    return _cfg_dict(c) if found.value else None
+
+
+def tune_set(n_ant: int, nb_pad: int, integration_spectra: int, form: int, group_mult: int, paired: bool,
+             ms: float = 0.0, device: str | None = None) -> None:
+    c = native.GridConfig(int(form), int(group_mult), int(bool(paired)), 0)
+    check(native.lib().bf_tune_set(device.encode() if device else None, int(n_ant), int(nb_pad),
+                                   int(integration_spectra), C.byref(c), float(ms)))
+
+
+def tune_save(path: str | None = None) -> None:
+    check(native.lib().bf_tune_save(path.encode() if path else None))
+
+
+def tune_load(path: str | None = None) -> None:
+    check(native.lib().bf_tune_load(path.encode() if path else None))
+
+
+def tune_clear() -> None:
+    check(native.lib().bf_tune_clear())
+
+
+def tune_cache_path() -> str:
+    buf = C.create_string_buffer(4096)
+    native.lib().bf_tune_cache_path(buf, len(buf))
+    return buf.value.decode()
+
+
+def grid_auto_integrated_with(stream, packed_voltage, auto_weights, integrated, codes, params, workspace,
+                              dims: Dimensions, integration_spectra: int, n_shards: int, form: int,
+                              group_mult: int = 1, paired: bool = True) -> None:
+    """grid_auto_integrated with an explicit launch choice."""
+    torch = _torch()
+    validate_dimensions(dims)
+    nw = integrated_time_count(dims.n_time, integration_spectra)
+    n_out = n_shards * nw * dims.n_freq * dims.n_beams
+    v = _dev(packed_voltage, "packed_voltage", torch.uint8, n_shards * dims.n_time * dims.n_freq * dims.n_ant)
+    s = _dev(auto_weights, "auto_weights", torch.uint8, auto_weight_bytes(dims, n_shards))
+    o = _dev(integrated, "integrated", torch.float32, n_out)
+    c = p = None
+    if codes is not None or params is not None:
+        qd = Dimensions(nw, dims.n_freq, dims.n_ant, dims.n_beams)
+        c = _dev(codes, "codes", torch.int8, n_out)
+        p = _dev(params, "params", torch.float32, 2 * n_shards * quantization_parameter_count(qd))
+    wsb = grid_auto_workspace_bytes(dims, integration_spectra, n_shards)
+    ws = _dev(workspace, "workspace", torch.uint8, wsb) if wsb > 0 else None
+    cfg = native.GridConfig(int(form), int(group_mult), int(bool(paired)), 0)
+    d = dims.c()
+    check(native.lib().bf_grid_auto_integrated_with(_stream_handle(stream), v, s, o, c, p, ws, C.byref(d),
+                                                    int(integration_spectra), int(n_shards), C.byref(cfg)))
+
+
 def grid_tensor_workspace_bytes(dims: Dimensions, integration_spectra: int, n_shards: int = 1) -> int:
     d = dims.c()
     return int(native.lib().bf_grid_tensor_workspace_bytes(C.byref(d), int(integration_spectra), int(n_shards)))

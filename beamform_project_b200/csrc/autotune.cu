@@ -1,0 +1,496 @@
+// autotune.cu -- the grid path's launch choices, measured on the GPU at hand.
+//
+// The reference exposes its tracker's launch shape as hand-set knobs
+// (V5ExecutionConfig: time_chunk_size, time_unroll;
+// include/beamformer/cuda_beam_tracker_v5.hpp:45-49) and fixes its grid
+// kernels' tiles at compile time (src/cuda_beamformer.cu:140-143).  Here the
+// grid path's choices are picked per class (n_ant, padded beams, integration
+// length) by timing every candidate on seeded synthetic data of the caller's
+// shape:
+//   * the form of bf_grid_auto_integrated: the checked covariance form, or
+//     the split-precision kernel alone (the covariance form's cost does not
+//     shrink with the beam count, the split kernel's does);
+//   * the split kernel's time unit: 1, 2 or 4 times the smallest unit that
+//     holds whole windows (fewer, longer units: less per-unit work in every
+//     role, coarser load balance);
+//   * the split kernel's channel order: CTA pairs on channel pairs (both
+//     halves of a 128-byte voltage line read together) or not.
+// A candidate is kept only if its products agree with the default choice's
+// (bit for bit for the split kernel's choices, which change scheduling only;
+// within the 1e-3 + 1e-5 |x| bar for the covariance form), so tuning never
+// changes results beyond the path's stated tolerance.  Choices live in a
+// table keyed by (device name, n_ant, padded beams, integration spectra),
+// persisted as text beside the library (or at $BF_TUNE_CACHE; "off" disables
+// the file) and loaded at first use.
+#include "bf_internal.cuh"
+#include "grid_tc.cuh"
+#include "serve.cuh"
+
+#include <dlfcn.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <tuple>
+#include <vector>
+
+namespace bf {
+namespace {
+
+struct TuneKey {
+    std::string device;
+    int n_ant, nb_pad;
+    uint64_t spectra;
+    bool operator<(const TuneKey& o) const {
+        return std::tie(device, n_ant, nb_pad, spectra) < std::tie(o.device, o.n_ant, o.nb_pad, o.spectra);
+    }
+};
+
+struct TuneEntry {
+    GridTuning cfg;
+    float ms = 0.f;
+};
+
+std::mutex g_mu;
+std::map<TuneKey, TuneEntry> g_table;
+bool g_loaded = false;
+
+std::string cache_path() {
+    if (const char* env = std::getenv("BF_TUNE_CACHE")) return env;
+    Dl_info info{};
+    if (dladdr(reinterpret_cast<void*>(&cache_path), &info) != 0 && info.dli_fname != nullptr) {
+        std::string lib = info.dli_fname;
+        const size_t slash = lib.find_last_of('/');
+        return (slash == std::string::npos ? std::string(".") : lib.substr(0, slash)) + "/bf_tune_cache.txt";
+    }
+    return "bf_tune_cache.txt";
+}
+
+// Device names contain spaces; the file stores them with '_' in their place.
+std::string file_name_of(std::string s) {
+    std::replace(s.begin(), s.end(), ' ', '_');
+    return s;
+}
+
+bool load_locked(const std::string& path) {
+    std::ifstream in(path);
+    if (!in) return false;
+    std::string line;
+    while (std::getline(in, line)) {
+        if (line.empty() || line[0] == '#') continue;
+        std::istringstream ls(line);
+        TuneKey k;
+        TuneEntry e;
+        if (ls >> k.device >> k.n_ant >> k.nb_pad >> k.spectra >> e.cfg.form >> e.cfg.group_mult >> e.cfg.paired >>
+            e.ms) {
+            if (e.cfg.group_mult < 1 || e.cfg.group_mult > 64 || (e.cfg.form != 0 && e.cfg.form != 1)) continue;
+            g_table[k] = e;
+        }
+    }
+    return true;
+}
+
+bool save_locked(const std::string& path) {
+    std::ofstream out(path, std::ios::trunc);
+    if (!out) return false;
+    out << "# device n_ant padded_beams integration_spectra form group_mult paired ms\n";
+    for (const auto& kv : g_table) {
+        out << kv.first.device << ' ' << kv.first.n_ant << ' ' << kv.first.nb_pad << ' ' << kv.first.spectra << ' '
+            << kv.second.cfg.form << ' ' << kv.second.cfg.group_mult << ' ' << kv.second.cfg.paired << ' '
+            << kv.second.ms << '\n';
+    }
+    return static_cast<bool>(out);
+}
+
+void ensure_loaded_locked() {
+    if (g_loaded) return;
+    g_loaded = true;
+    const std::string path = cache_path();
+    if (path != "off") load_locked(path);
+}
+
+// The current device's name (looked up once per device ordinal).
+bool current_device_name(std::string* name) {
+    static std::mutex mu;
+    static std::map<int, std::string> names;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return false;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = names.find(dev);
+    if (it == names.end()) {
+        char buf[256] = {};
+        cudaDeviceProp prop{};
+        if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return false;
+        std::snprintf(buf, sizeof(buf), "%s", prop.name);
+        it = names.emplace(dev, file_name_of(buf)).first;
+    }
+    *name = it->second;
+    return true;
+}
+
+// Index of the candidate to keep: the fastest that passed, unless it beats
+// candidate 0 (the default) by less than min_gain (a fraction), which keeps
+// the default against timing noise.
+uint32_t pick(uint32_t n, const double* ms, const uint8_t* ok, double min_gain) {
+    uint32_t best = 0;
+    double best_ms = n > 0 && ok[0] ? ms[0] : INFINITY;
+    uint32_t fastest = 0;
+    double fastest_ms = INFINITY;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (ok[i] && ms[i] < fastest_ms) {
+            fastest_ms = ms[i];
+            fastest = i;
+        }
+    }
+    if (!std::isfinite(fastest_ms)) return 0;
+    if (!std::isfinite(best_ms) || fastest_ms < best_ms * (1.0 - min_gain)) best = fastest;
+    return best;
+}
+
+__global__ void count_mismatch_kernel(const float* a, const float* b, size_t n, int bitwise, unsigned* bad) {
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const float x = a[i], y = b[i];
+        const bool fail = bitwise ? __float_as_uint(x) != __float_as_uint(y)
+                                  : !(fabsf(x - y) <= 1e-3f + 1e-5f * fabsf(y));
+        if (fail) atomicAdd(bad, 1u);
+    }
+}
+
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+    cudaError_t alloc(size_t n) { return cudaMalloc(reinterpret_cast<void**>(&p), std::max<size_t>(n, 1) * sizeof(T)); }
+};
+
+}  // namespace
+
+bool tuned_grid_config(int n_ant, int nb_pad, uint64_t spectra, GridTuning* out) {
+    *out = GridTuning{};
+    std::string dev;
+    if (!current_device_name(&dev)) return false;
+    std::lock_guard<std::mutex> lock(g_mu);
+    ensure_loaded_locked();
+    auto it = g_table.find(TuneKey{dev, n_ant, nb_pad, spectra});
+    if (it == g_table.end()) return false;
+    *out = it->second.cfg;
+    return true;
+}
+
+}  // namespace bf
+
+using namespace bf;
+
+extern "C" {
+
+BF_API bf_status bf_tune_pick(uint32_t n, const double* ms, const uint8_t* ok, double min_gain, uint32_t* best) {
+    clear_error();
+    if (n == 0 || ms == nullptr || ok == nullptr || best == nullptr) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "bf_tune_pick needs candidates, times, flags and an output");
+    }
+    *best = pick(n, ms, ok, min_gain);
+    return BF_OK;
+}
+
+BF_API size_t bf_tune_cache_path(char* buf, size_t n) {
+    const std::string p = cache_path();
+    if (buf != nullptr && n > 0) {
+        std::strncpy(buf, p.c_str(), n - 1);
+        buf[n - 1] = '\0';
+    }
+    return p.size();
+}
+
+BF_API bf_status bf_tune_clear(void) {
+    clear_error();
+    std::lock_guard<std::mutex> lock(g_mu);
+    g_table.clear();
+    g_loaded = true;  // nothing is read back implicitly after a clear
+    return BF_OK;
+}
+
+BF_API bf_status bf_tune_load(const char* path) {
+    clear_error();
+    std::lock_guard<std::mutex> lock(g_mu);
+    g_loaded = true;
+    const std::string p = path != nullptr ? std::string(path) : cache_path();
+    if (!load_locked(p)) return set_error(BF_ERR_INVALID_ARGUMENT, "cannot read the tuning cache " + p);
+    return BF_OK;
+}
+
+BF_API bf_status bf_tune_save(const char* path) {
+    clear_error();
+    std::lock_guard<std::mutex> lock(g_mu);
+    ensure_loaded_locked();
+    const std::string p = path != nullptr ? std::string(path) : cache_path();
+    if (p == "off") return BF_OK;
+    if (!save_locked(p)) return set_error(BF_ERR_INVALID_ARGUMENT, "cannot write the tuning cache " + p);
+    return BF_OK;
+}
+
+BF_API bf_status bf_tune_set(const char* device, int n_ant, int nb_pad, uint64_t integration_spectra,
+                             const bf_grid_config* cfg, float ms) {
+    clear_error();
+    if (cfg == nullptr || (cfg->form != 0 && cfg->form != 1) || cfg->group_mult < 1 || cfg->group_mult > 64) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "invalid grid configuration");
+    }
+    std::string dev;
+    if (device != nullptr) {
+        dev = file_name_of(device);
+    } else if (!current_device_name(&dev)) {
+        return set_error(BF_ERR_CUDA, "no current CUDA device");
+    }
+    std::lock_guard<std::mutex> lock(g_mu);
+    ensure_loaded_locked();
+    TuneEntry e;
+    e.cfg.form = cfg->form;
+    e.cfg.group_mult = cfg->group_mult;
+    e.cfg.paired = cfg->paired != 0;
+    e.ms = ms;
+    g_table[TuneKey{dev, n_ant, nb_pad, integration_spectra}] = e;
+    return BF_OK;
+}
+
+BF_API bf_status bf_tune_get(const char* device, int n_ant, int nb_pad, uint64_t integration_spectra,
+                             bf_grid_config* cfg, int32_t* found) {
+    clear_error();
+    if (cfg == nullptr || found == nullptr) return set_error(BF_ERR_INVALID_ARGUMENT, "outputs must be given");
+    std::string dev;
+    if (device != nullptr) {
+        dev = file_name_of(device);
+    } else if (!current_device_name(&dev)) {
+        return set_error(BF_ERR_CUDA, "no current CUDA device");
+    }
+    std::lock_guard<std::mutex> lock(g_mu);
+    ensure_loaded_locked();
+    const GridTuning d{};
+    auto it = g_table.find(TuneKey{dev, n_ant, nb_pad, integration_spectra});
+    const GridTuning& t = it == g_table.end() ? d : it->second.cfg;
+    *cfg = bf_grid_config{t.form, t.group_mult, t.paired, 0};
+    *found = it != g_table.end();
+    return BF_OK;
+}
+
+BF_API bf_status bf_grid_auto_integrated_with(void* stream, const uint8_t* packed_voltage, const void* auto_weights,
+                                              float* integrated, int8_t* codes, float* params, void* workspace,
+                                              const bf_dims* dims, uint64_t integration_spectra, uint64_t n_shards,
+                                              const bf_grid_config* cfg) {
+    clear_error();
+    if (cfg == nullptr || (cfg->form != 0 && cfg->form != 1) || cfg->group_mult < 1 || cfg->group_mult > 64) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "invalid grid configuration");
+    }
+    BF_RETURN_IF(validate_dims(dims));
+    if (n_shards == 0 || integration_spectra == 0) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "n_shards and integration_spectra must be positive");
+    }
+    if (dims->n_ant > 64) return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernels support n_ant 32 or 64");
+    if (integration_spectra > 32 && integration_spectra % 32 != 0) {
+        return set_error(BF_ERR_UNSUPPORTED,
+                         "the tensor-core kernels need integration_spectra below 32 or a multiple of 32");
+    }
+    if ((codes == nullptr) != (params == nullptr)) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "codes and params must both be given or both be null");
+    }
+    if (packed_voltage == nullptr || auto_weights == nullptr || integrated == nullptr) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "packed_voltage, auto_weights and integrated must be given");
+    }
+    if (cfg->form == 1 && auto_uses_cov(*dims, integration_spectra, n_shards) &&
+        (workspace == nullptr || reinterpret_cast<uintptr_t>(workspace) % 256 != 0)) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "workspace must be given and 256-byte aligned");
+    }
+    GridTuning t;
+    t.form = cfg->form;
+    t.group_mult = cfg->group_mult;
+    t.paired = cfg->paired != 0;
+    return launch_grid_auto(static_cast<cudaStream_t>(stream), packed_voltage, auto_weights, integrated, codes, params,
+                            workspace, *dims, integration_spectra, n_shards, &t);
+}
+
+static bf_status autotune_impl(cudaStream_t st, const bf_dims* dims, uint64_t S, uint64_t n_shards,
+                               bf_grid_config* cands, float* ms_out, uint8_t* ok_out, uint32_t capacity,
+                               uint32_t* n_out, uint32_t* best_out) {
+    BF_RETURN_IF(validate_dims(dims));
+    if (n_shards == 0 || n_shards > 8 || S == 0) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "n_shards must be 1 to 8 and integration_spectra positive");
+    }
+    if (dims->n_ant > 64) return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernels support n_ant 32 or 64");
+    if (S > 32 && S % 32 != 0) {
+        return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernels need integration_spectra below 32 or a multiple of 32");
+    }
+    // a bounded stand-in of the caller's shape: at most 8192 spectra (whole windows)
+    bf_dims d = *dims;
+    const uint64_t cap = std::max<uint64_t>(S, 8192 / S * S);
+    d.n_time = std::min<uint64_t>(d.n_time, cap);
+    const uint64_t A = d.n_ant, F = d.n_freq, B = d.n_beams;
+    const bool cov = auto_uses_cov(d, S, n_shards);
+
+    // candidates: 0 is the default (what an untuned call runs)
+    std::vector<GridTuning> c;
+    GridTuning def;
+    def.form = cov ? 1 : 0;
+    c.push_back(def);
+    for (int g : {1, 2, 4}) {
+        for (int pr : {1, 0}) {
+            GridTuning t;
+            t.form = 0;
+            t.group_mult = g;
+            t.paired = pr;
+            if (!(t.form == def.form && g == def.group_mult && pr == def.paired)) c.push_back(t);
+        }
+    }
+    if (capacity < c.size()) return set_error(BF_ERR_INVALID_ARGUMENT, "candidate capacity too small");
+
+    const uint64_t W = window_count(d.n_time, S);
+    const size_t n_volt = n_shards * d.n_time * F * A, n_vals = n_shards * W * F * B;
+    DevBuf<uint8_t> volt, wimg, ws;
+    DevBuf<float> w, ref, out, pos, freq, dirs;
+    DevBuf<unsigned> bad;
+    const uint64_t wbytes = auto_weight_bytes(d, n_shards), wsbytes = auto_workspace_bytes(d, S, n_shards);
+    BF_RETURN_IF(cuda_status(volt.alloc(n_volt), "autotune voltage"));
+    BF_RETURN_IF(cuda_status(wimg.alloc(wbytes), "autotune weights"));
+    BF_RETURN_IF(cuda_status(ws.alloc(std::max<uint64_t>(wsbytes, 256)), "autotune workspace"));
+    BF_RETURN_IF(cuda_status(w.alloc(2 * n_shards * B * F * A), "autotune canonical weights"));
+    BF_RETURN_IF(cuda_status(ref.alloc(n_vals), "autotune reference output"));
+    BF_RETURN_IF(cuda_status(out.alloc(n_vals), "autotune output"));
+    BF_RETURN_IF(cuda_status(pos.alloc(3 * A), "autotune positions"));
+    BF_RETURN_IF(cuda_status(freq.alloc(n_shards * F), "autotune frequencies"));
+    BF_RETURN_IF(cuda_status(dirs.alloc(3 * B), "autotune directions"));
+    BF_RETURN_IF(cuda_status(bad.alloc(1), "autotune comparison"));
+    // a 2 x (A / 2) grid at 0.2 m, channels over 400-800 MHz, beams spread over
+    // +-0.4 in direction cosine; Gaussian int4 noise (sigma 2.5)
+    std::vector<float> hp(3 * A), hf(n_shards * F), hd(3 * B);
+    for (uint64_t a = 0; a < A; ++a) {
+        hp[3 * a] = 0.2f * static_cast<float>(a % (A / 2));
+        hp[3 * a + 1] = 0.2f * static_cast<float>(a / (A / 2));
+        hp[3 * a + 2] = 0.f;
+    }
+    for (uint64_t f = 0; f < n_shards * F; ++f) {
+        hf[f] = 400e6f + 400e6f * static_cast<float>(f) / static_cast<float>(std::max<uint64_t>(1, n_shards * F - 1));
+    }
+    for (uint64_t b = 0; b < B; ++b) {
+        const float l = -0.4f + 0.8f * static_cast<float>(b % 16) / 15.f;
+        const float m = -0.4f + 0.8f * static_cast<float>((b / 16) % 8) / 7.f;
+        hd[3 * b] = l;
+        hd[3 * b + 1] = m;
+        hd[3 * b + 2] = std::sqrt(1.f - l * l - m * m);
+    }
+    BF_RETURN_IF(cuda_status(cudaMemcpyAsync(pos.p, hp.data(), hp.size() * 4, cudaMemcpyHostToDevice, st), "upload"));
+    BF_RETURN_IF(cuda_status(cudaMemcpyAsync(freq.p, hf.data(), hf.size() * 4, cudaMemcpyHostToDevice, st), "upload"));
+    BF_RETURN_IF(cuda_status(cudaMemcpyAsync(dirs.p, hd.data(), hd.size() * 4, cudaMemcpyHostToDevice, st), "upload"));
+    BF_RETURN_IF(launch_generate_weights(st, pos.p, freq.p, dirs.p, w.p, n_shards, F, B, A));
+    for (uint64_t s = 0; s < n_shards; ++s) {
+        const bf_dims ds{d.n_time, F, A, 1};
+        const float scale = 2.5f / std::sqrt(4.f * 8.f * (65536.f * 65536.f - 1.f) / 12.f);
+        BF_RETURN_IF(launch_generate(st, 0x5eed + s, 0, scale, nullptr, d.n_time, volt.p + s * d.n_time * F * A, ds));
+    }
+    BF_RETURN_IF(launch_prepare_auto(st, w.p, wimg.p, d, n_shards));
+
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    BF_RETURN_IF(cuda_status(cudaEventCreate(&e0), "event"));
+    BF_RETURN_IF(cuda_status(cudaEventCreate(&e1), "event"));
+    bf_status result = BF_OK;
+    std::vector<double> ms(c.size(), INFINITY);
+    std::vector<uint8_t> ok(c.size(), 0);
+    for (size_t i = 0; i < c.size() && result == BF_OK; ++i) {
+        float* dst = i == 0 ? ref.p : out.p;
+        auto run = [&]() {
+            return launch_grid_auto(st, volt.p, wimg.p, dst, nullptr, nullptr, ws.p, d, S, n_shards, &c[i]);
+        };
+        result = run();  // warm-up (and the products compared below)
+        if (result != BF_OK) break;
+        float best = INFINITY;
+        for (int rep = 0; rep < 3 && result == BF_OK; ++rep) {
+            result = cuda_status(cudaEventRecord(e0, st), "event");
+            if (result == BF_OK) result = run();
+            if (result == BF_OK) result = cuda_status(cudaEventRecord(e1, st), "event");
+            if (result == BF_OK) result = cuda_status(cudaEventSynchronize(e1), "autotune timing");
+            float t = 0.f;
+            if (result == BF_OK) result = cuda_status(cudaEventElapsedTime(&t, e0, e1), "event time");
+            best = std::min(best, t);
+        }
+        if (result != BF_OK) break;
+        uint32_t code = 0;
+        result = take_tc_error(&code);
+        if (result == BF_OK && code != 0) result = set_error(BF_ERR_TIMEOUT, "a bounded wait ran out while tuning");
+        if (result != BF_OK) break;
+        ms[i] = best;
+        if (i == 0) {
+            ok[i] = 1;
+            continue;
+        }
+        // split-kernel choices reschedule the same arithmetic: bit-identical to
+        // the default split form; against the covariance form, the shared bar
+        const int bitwise = def.form == 0 ? 1 : 0;
+        result = cuda_status(cudaMemsetAsync(bad.p, 0, 4, st), "autotune compare");
+        if (result != BF_OK) break;
+        count_mismatch_kernel<<<148 * 4, 256, 0, st>>>(out.p, ref.p, n_vals, bitwise, bad.p);
+        unsigned nbad = 1;
+        result = cuda_status(cudaMemcpyAsync(&nbad, bad.p, 4, cudaMemcpyDeviceToHost, st), "autotune compare");
+        if (result == BF_OK) result = cuda_status(cudaStreamSynchronize(st), "autotune compare");
+        ok[i] = result == BF_OK && nbad == 0;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (result != BF_OK) return result;
+    const uint32_t best = pick(static_cast<uint32_t>(c.size()), ms.data(), ok.data(), 0.02);
+    // the best split-kernel choice, kept for split-only calls even when the
+    // covariance form wins the class
+    uint32_t best_split = 0;
+    double split_ms = INFINITY;
+    for (size_t i = 0; i < c.size(); ++i) {
+        if (c[i].form == 0 && ok[i] && ms[i] < split_ms) {
+            split_ms = ms[i];
+            best_split = static_cast<uint32_t>(i);
+        }
+    }
+    GridTuning chosen = c[best];
+    if (chosen.form == 1 && std::isfinite(split_ms)) {
+        chosen.group_mult = c[best_split].group_mult;
+        chosen.paired = c[best_split].paired;
+    }
+    std::string dev;
+    if (!current_device_name(&dev)) return set_error(BF_ERR_CUDA, "no current CUDA device");
+    {
+        std::lock_guard<std::mutex> lock(g_mu);
+        ensure_loaded_locked();
+        TuneEntry e;
+        e.cfg = chosen;
+        e.ms = static_cast<float>(ms[best]);
+        g_table[TuneKey{dev, static_cast<int>(A), tc_padded_beams(B), S}] = e;
+    }
+    for (size_t i = 0; i < c.size(); ++i) {
+        cands[i] = bf_grid_config{c[i].form, c[i].group_mult, c[i].paired, 0};
+        if (ms_out) ms_out[i] = static_cast<float>(ms[i]);
+        if (ok_out) ok_out[i] = ok[i];
+    }
+    *n_out = static_cast<uint32_t>(c.size());
+    if (best_out) *best_out = best;
+    return BF_OK;
+}
+
+BF_API bf_status bf_autotune_grid(void* stream, const bf_dims* dims, uint64_t integration_spectra, uint64_t n_shards,
+                                  bf_grid_config* candidates, float* candidate_ms, uint8_t* candidate_ok,
+                                  uint32_t capacity, uint32_t* n_candidates, uint32_t* best) {
+    clear_error();
+    if (candidates == nullptr || n_candidates == nullptr) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "candidates and n_candidates must be given");
+    }
+    try {
+        return autotune_impl(static_cast<cudaStream_t>(stream), dims, integration_spectra, n_shards, candidates,
+                             candidate_ms, candidate_ok, capacity, n_candidates, best);
+    } catch (const std::exception& e) {
+        return set_error(BF_ERR_LOGIC, std::string("internal error: ") + e.what());
+    }
+}
+
+}  // extern "C"

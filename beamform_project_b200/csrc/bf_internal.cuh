@@ -247,12 +247,26 @@ bf_status launch_prepare_cov(cudaStream_t stream, const float* w, void* out, con
 bf_status launch_grid_cov(cudaStream_t stream, const uint8_t* v, const void* wimg, float* integrated,
                           int8_t* codes, float* params, const bf_dims& d, uint64_t spectra, uint64_t n_shards);
 uint64_t grid_tensor_counter_count(const bf_dims& d, uint64_t spectra, uint64_t n_shards);
+// Launch choices of the grid path that leave every value bit-identical (the
+// split kernel's unit size and channel order) or within the same bar (the
+// checked form's kernel), picked per (n_ant, padded beams, integration) by
+// the autotuner (autotune.cu).
+struct GridTuning {
+    int form = 1;        // bf_grid_auto_integrated: 0 split kernel, 1 checked covariance form
+    int group_mult = 1;  // split kernel: units of group_mult x the smallest whole-window unit
+    int paired = 1;      // split kernel: CTA pairs walk channel pairs
+};
+// The tuned choice for a class, or the defaults; true when a tuned entry exists.
+bool tuned_grid_config(int n_ant, int nb_pad, uint64_t spectra, GridTuning* out);
+
 // counters == nullptr: quantize (when codes is given) with a second launch;
 // otherwise quantization is fused into the tensor kernel's epilogue and
-// `counters` (grid_tensor_counter_count entries) is its scratch.
+// `counters` (grid_tensor_counter_count entries) is its scratch.  tune ==
+// nullptr uses the tuned (or default) choice for the class.
 bf_status launch_grid_tensor(cudaStream_t stream, const uint8_t* v, const void* split,
                              float* integrated, int8_t* codes, float* params, const bf_dims& d,
-                             uint64_t spectra, uint64_t n_shards, unsigned* counters);
+                             uint64_t spectra, uint64_t n_shards, unsigned* counters,
+                             const GridTuning* tune = nullptr);
 // The split kernel over the units of a device-written list (no quantizer).
 bf_status launch_grid_tensor_list(cudaStream_t stream, const uint8_t* v, const void* split, float* integrated,
                                   const bf_dims& d, uint64_t spectra, uint64_t n_shards, const int* unit_list,
@@ -269,7 +283,8 @@ bool auto_uses_cov(const bf_dims& d, uint64_t spectra, uint64_t n_shards);
 uint64_t auto_workspace_bytes(const bf_dims& d, uint64_t spectra, uint64_t n_shards);
 bf_status launch_prepare_auto(cudaStream_t stream, const float* w, void* out, const bf_dims& d, uint64_t n_shards);
 bf_status launch_grid_auto(cudaStream_t stream, const uint8_t* v, const void* wimg, float* integrated, int8_t* codes,
-                           float* params, void* workspace, const bf_dims& d, uint64_t spectra, uint64_t n_shards);
+                           float* params, void* workspace, const bf_dims& d, uint64_t spectra, uint64_t n_shards,
+                           const struct GridTuning* tune = nullptr);
 bf_status launch_grid_cov_estimate(cudaStream_t stream, const uint8_t* v, const void* wimg, float* integrated,
                                    float* estimate, const bf_dims& d, uint64_t spectra, uint64_t n_shards);
 

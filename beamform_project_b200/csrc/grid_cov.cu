@@ -45,6 +45,7 @@
 // 128-byte-swizzled K-major layout, fp32 [beam][component]), voltage stages.
 // Every wait is bounded and reports through the device error word.
 #include "bf_internal.cuh"
+#include "grid_tc.cuh"
 #include "sm100.cuh"
 
 #include <cuda.h>
@@ -699,11 +700,18 @@ bf_status launch_prepare_auto(cudaStream_t stream, const float* w, void* out, co
 }
 
 bf_status launch_grid_auto(cudaStream_t stream, const uint8_t* v, const void* wimg, float* integrated, int8_t* codes,
-                           float* params, void* workspace, const bf_dims& d, uint64_t spectra, uint64_t n_shards) {
+                           float* params, void* workspace, const bf_dims& d, uint64_t spectra, uint64_t n_shards,
+                           const GridTuning* tune) {
     const uint64_t cov = cov_part_bytes(d, n_shards);
     const uint8_t* split = static_cast<const uint8_t*>(wimg) + cov;
-    if (!auto_uses_cov(d, spectra, n_shards)) {
-        return launch_grid_tensor(stream, v, split, integrated, codes, params, d, spectra, n_shards, nullptr);
+    GridTuning t;
+    if (tune != nullptr) {
+        t = *tune;
+    } else {
+        tuned_grid_config(static_cast<int>(d.n_ant), tc_padded_beams(d.n_beams), spectra, &t);
+    }
+    if (!auto_uses_cov(d, spectra, n_shards) || t.form == 0) {
+        return launch_grid_tensor(stream, v, split, integrated, codes, params, d, spectra, n_shards, nullptr, &t);
     }
     CovChecks chk;
     const long long units = grid_tensor_unit_layout(d, spectra, n_shards, &chk.split_gpc, &chk.split_gw);

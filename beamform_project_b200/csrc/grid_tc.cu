@@ -964,7 +964,7 @@ uint64_t grid_tensor_counter_count(const bf_dims& d, uint64_t spectra, uint64_t 
     return n_shards * window_count(d.n_time, spectra) * ((d.n_freq + 15) / 16);
 }
 
-long long tc_job_tiling(TcJob& job, int n_time, int spectra, int n_freq, int n_shards) {
+long long tc_job_tiling(TcJob& job, int n_time, int spectra, int n_freq, int n_shards, int group_mult) {
     job.n_time = n_time;
     job.spectra = spectra;
     job.n_freq = n_freq;
@@ -978,6 +978,7 @@ long long tc_job_tiling(TcJob& job, int n_time, int spectra, int n_freq, int n_s
         const long long lcm = static_cast<long long>(spectra) / gcd_ll(spectra, kTileM) * kTileM;
         job.group_tiles = static_cast<int>(lcm / kTileM);
     }
+    job.group_tiles *= std::max(1, group_mult);
     job.groups_per_channel = (job.tiles_per_channel + job.group_tiles - 1) / job.group_tiles;
     return static_cast<long long>(n_shards) * n_freq * job.groups_per_channel;
 }
@@ -1006,7 +1007,7 @@ namespace {
 bf_status launch_grid_tensor_impl(cudaStream_t stream, const uint8_t* v, const void* split, float* integrated,
                                   int8_t* codes, float* params, const bf_dims& d, uint64_t spectra,
                                   uint64_t n_shards, unsigned* counters, const int* unit_list,
-                                  const int* unit_count) {
+                                  const int* unit_count, const GridTuning& tune) {
     if (d.n_time >= (1ull << 31) || n_shards > 1024 || spectra >= (1ull << 30)) {
         return set_error(BF_ERR_OVERFLOW, "CUDA tensor-core grid exceeds the supported size");
     }
@@ -1023,7 +1024,7 @@ bf_status launch_grid_tensor_impl(cudaStream_t stream, const uint8_t* v, const v
     p.job.t0 = 0;
     p.job.unit_begin = 0;
     p.n_units = tc_job_tiling(p.job, static_cast<int>(d.n_time), S, static_cast<int>(d.n_freq),
-                              static_cast<int>(n_shards));
+                              static_cast<int>(n_shards), unit_list != nullptr ? 1 : tune.group_mult);
     p.ftiles = static_cast<int>((d.n_freq + 15) / 16);
     p.btiles = static_cast<int>((d.n_beams + 15) / 16);
 
@@ -1049,7 +1050,7 @@ bf_status launch_grid_tensor_impl(cudaStream_t stream, const uint8_t* v, const v
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     int grid = static_cast<int>(std::min<long long>(sms, p.n_units));
-    p.paired = (d.n_freq % 2 == 0 && grid % 2 == 0 && grid >= 2) ? 1 : 0;
+    p.paired = (tune.paired && d.n_freq % 2 == 0 && grid % 2 == 0 && grid >= 2) ? 1 : 0;
     if (unit_list != nullptr) {
         // the list's length is known on the device only: one CTA per SM, each
         // taking its share of the list (none when it is empty)
@@ -1072,16 +1073,22 @@ bf_status launch_grid_tensor_impl(cudaStream_t stream, const uint8_t* v, const v
 
 bf_status launch_grid_tensor(cudaStream_t stream, const uint8_t* v, const void* split, float* integrated,
                              int8_t* codes, float* params, const bf_dims& d, uint64_t spectra,
-                             uint64_t n_shards, unsigned* counters) {
+                             uint64_t n_shards, unsigned* counters, const GridTuning* tune) {
+    GridTuning t;
+    if (tune != nullptr) {
+        t = *tune;
+    } else {
+        tuned_grid_config(static_cast<int>(d.n_ant), padded_beams(d.n_beams), spectra, &t);
+    }
     return launch_grid_tensor_impl(stream, v, split, integrated, codes, params, d, spectra, n_shards, counters,
-                                   nullptr, nullptr);
+                                   nullptr, nullptr, t);
 }
 
 bf_status launch_grid_tensor_list(cudaStream_t stream, const uint8_t* v, const void* split, float* integrated,
                                   const bf_dims& d, uint64_t spectra, uint64_t n_shards, const int* unit_list,
                                   const int* unit_count) {
     return launch_grid_tensor_impl(stream, v, split, integrated, nullptr, nullptr, d, spectra, n_shards, nullptr,
-                                   unit_list, unit_count);
+                                   unit_list, unit_count, GridTuning{});
 }
 
 long long grid_tensor_unit_layout(const bf_dims& d, uint64_t spectra, uint64_t n_shards, int* groups_per_channel,

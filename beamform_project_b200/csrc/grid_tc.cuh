@@ -41,7 +41,9 @@ __host__ __device__ inline int small_window_rows(int spectra) {
 
 // Fills the tiling fields of `job` (rows_q, tiles, groups) for `n_time`
 // spectra of windows of `spectra`; returns the job's unit count.
-long long tc_job_tiling(TcJob& job, int n_time, int spectra, int n_freq, int n_shards);
+// group_mult > 1 makes each unit group_mult times the smallest unit (whole
+// windows either way).
+long long tc_job_tiling(TcJob& job, int n_time, int spectra, int n_freq, int n_shards, int group_mult = 1);
 
 // 4-D map {antenna, channel, spectrum row, shard} over packed bytes with the
 // given row and shard strides (bytes); the box is one channel of 128 rows,

@@ -89,6 +89,10 @@ class ServeStats(C.Structure):
                                                              ("predicted_ms_last", C.c_double)]
 
 
+class GridConfig(C.Structure):
+    _fields_ = [("form", C.c_int32), ("group_mult", C.c_int32), ("paired", C.c_int32), ("reserved", C.c_int32)]
+
+
 class ServeJobInfo(C.Structure):
     _fields_ = [("state", C.c_int32), ("pad", C.c_uint32), ("submit_step", C.c_uint64), ("admit_step", C.c_uint64),
                 ("last_step", C.c_uint64), ("windows_launched", C.c_uint64)]
@@ -118,6 +122,18 @@ _SIGS = {
     "bf_grid_auto_workspace_bytes": (_U64, [C.POINTER(Dims), _U64, _U64]),
     "bf_grid_auto_integrated": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, C.POINTER(Dims), _U64, _U64]),
     "bf_kernel_versions": (C.c_int, [C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "bf_autotune_grid": (C.c_int, [_P, C.POINTER(Dims), _U64, _U64, C.POINTER(GridConfig), C.POINTER(C.c_float),
+                                   C.POINTER(C.c_uint8), C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    "bf_grid_auto_integrated_with": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, C.POINTER(Dims), _U64, _U64,
+                                               C.POINTER(GridConfig)]),
+    "bf_tune_get": (C.c_int, [C.c_char_p, C.c_int, C.c_int, _U64, C.POINTER(GridConfig), C.POINTER(C.c_int32)]),
+    "bf_tune_set": (C.c_int, [C.c_char_p, C.c_int, C.c_int, _U64, C.POINTER(GridConfig), C.c_float]),
+    "bf_tune_clear": (C.c_int, []),
+    "bf_tune_load": (C.c_int, [C.c_char_p]),
+    "bf_tune_save": (C.c_int, [C.c_char_p]),
+    "bf_tune_cache_path": (C.c_size_t, [C.c_char_p, C.c_size_t]),
+    "bf_tune_pick": (C.c_int, [C.c_uint32, C.POINTER(C.c_double), C.POINTER(C.c_uint8), C.c_double,
+                               C.POINTER(C.c_uint32)]),
     "bf_grid_pipeline_chunk_spectra": (_U64, [C.POINTER(Dims), _U64, _U64, _U64]),
     "bf_grid_pipeline_create": (C.c_int, [C.POINTER(Dims), _U64, _U64, _U64, _PP]),
     "bf_grid_pipeline_upload_weights": (C.c_int, [_P, _P]),

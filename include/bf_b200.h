@@ -241,6 +241,61 @@ BF_API bf_status bf_grid_auto_integrated(void* stream, const uint8_t* packed_vol
                                          float* integrated, int8_t* codes, float* params, void* workspace,
                                          const bf_dims* dims, uint64_t integration_spectra, uint64_t n_shards);
 
+/* ------------------------------------------------------------------------ */
+/* Autotuner of the grid path.  No reference counterpart: the reference's    */
+/* launch knobs are set by hand (V5ExecutionConfig,                          */
+/* include/beamformer/cuda_beam_tracker_v5.hpp:45-49) or fixed at compile     */
+/* time (src/cuda_beamformer.cu:140-143).                                     */
+/* ------------------------------------------------------------------------ */
+
+/* One launch choice of the grid path: form (bf_grid_auto_integrated: 0 the
+ * split-precision kernel, 1 the checked covariance form), group_mult (split
+ * kernel: time units of 1, 2 or 4 times the smallest whole-window unit),
+ * paired (split kernel: CTA pairs walk channel pairs). */
+typedef struct bf_grid_config {
+    int32_t form;
+    int32_t group_mult;
+    int32_t paired;
+    int32_t reserved;
+} bf_grid_config;
+
+/* Times every candidate choice for the class of (dims, integration_spectra)
+ * -- n_ant, padded beams, integration length -- on seeded synthetic data of
+ * that shape (at most 8192 spectra), keeps only candidates whose products
+ * agree with the default's (bit for bit for the split kernel's choices,
+ * within 1e-3 + 1e-5 |x| for the covariance form), and records the fastest
+ * (it must beat the default by 2 %) in the tuning table, which untuned calls
+ * of bf_grid_tensor_integrated, bf_grid_tensor_quantized(_static),
+ * bf_grid_auto_integrated and the host pipeline then use.  Setup-time call:
+ * it allocates and synchronises the stream.  Candidates (at most capacity;
+ * 8 is enough), their best of three times (ms) and pass flags are written
+ * out; *best is the index chosen (0 = the default). */
+BF_API bf_status bf_autotune_grid(void* stream, const bf_dims* dims, uint64_t integration_spectra,
+                                  uint64_t n_shards, bf_grid_config* candidates, float* candidate_ms,
+                                  uint8_t* candidate_ok, uint32_t capacity, uint32_t* n_candidates,
+                                  uint32_t* best);
+/* bf_grid_auto_integrated with an explicit choice (tests, the tuner). */
+BF_API bf_status bf_grid_auto_integrated_with(void* stream, const uint8_t* packed_voltage, const void* auto_weights,
+                                              float* integrated, int8_t* codes, float* params, void* workspace,
+                                              const bf_dims* dims, uint64_t integration_spectra,
+                                              uint64_t n_shards, const bf_grid_config* config);
+/* The tuning table: keyed by (device name, n_ant, padded beams,
+ * integration_spectra); device NULL means the current device.  It is read
+ * at first use from the cache file (beside this library, or $BF_TUNE_CACHE;
+ * "off" reads and writes nothing) and written by bf_tune_save.  found is 0
+ * (and *config the default) for a class never tuned. */
+BF_API bf_status bf_tune_get(const char* device, int n_ant, int nb_pad, uint64_t integration_spectra,
+                             bf_grid_config* config, int32_t* found);
+BF_API bf_status bf_tune_set(const char* device, int n_ant, int nb_pad, uint64_t integration_spectra,
+                             const bf_grid_config* config, float ms);
+BF_API bf_status bf_tune_clear(void);
+BF_API bf_status bf_tune_load(const char* path);  /* NULL: the cache file */
+BF_API bf_status bf_tune_save(const char* path);  /* NULL: the cache file */
+BF_API size_t bf_tune_cache_path(char* buf, size_t n);
+/* The selection rule on its own: the fastest candidate with ok set, unless
+ * it beats candidate 0 (the default) by less than min_gain (a fraction). */
+BF_API bf_status bf_tune_pick(uint32_t n, const double* ms, const uint8_t* ok, double min_gain, uint32_t* best);
+
 /* Host-buffer grid pipeline.  Counterpart of the reference's
  * CudaBeamformerWorkspace::run_quantized_integrated_pipeline
  * (include/beamformer/cuda_beamformer.hpp:66-76: weights resident, voltage

@@ -6,6 +6,7 @@ Everything unmarked runs on a CPU-only machine in a few minutes.
 """
 from __future__ import annotations
 
+import os
 import sys
 from pathlib import Path
 
@@ -15,6 +16,10 @@ import pytest
 ROOT = Path(__file__).resolve().parent.parent
 if str(ROOT) not in sys.path:
     sys.path.insert(0, str(ROOT))
+
+# Tests run the grid path's default launch choices unless a test tunes them:
+# no tuning cache file is read or written.
+os.environ.setdefault("BF_TUNE_CACHE", "off")
 
 
 def pytest_configure(config):
