@@ -468,15 +468,18 @@ class GridHostPipeline:
     host tensors give PCIe-rate copies; numpy arrays work through the
     driver's staging."""
 
-    def __init__(self, dims: Dimensions, integration_spectra: int, n_shards: int = 1, chunk_spectra: int = 0):
+    def __init__(self, dims: Dimensions, integration_spectra: int, n_shards: int = 1, chunk_spectra: int = 0,
+                 checked: bool = False):
+        """checked=True runs the checked covariance form
+        (bf_grid_pipeline_create_checked) instead of the split kernel."""
         validate_dimensions(dims)
         self.dims, self.spectra, self.n_shards = dims, int(integration_spectra), int(n_shards)
         self.n_windows = integrated_time_count(dims.n_time, integration_spectra)
         self.chunk_spectra = grid_pipeline_chunk_spectra(dims, integration_spectra, n_shards, chunk_spectra)
         h = C.c_void_p()
         d = dims.c()
-        check(native.lib().bf_grid_pipeline_create(C.byref(d), self.spectra, self.n_shards, int(chunk_spectra),
-                                                   C.byref(h)))
+        create = native.lib().bf_grid_pipeline_create_checked if checked else native.lib().bf_grid_pipeline_create
+        check(create(C.byref(d), self.spectra, self.n_shards, int(chunk_spectra), C.byref(h)))
         self._h = h
 
     def upload_weights(self, weights) -> None:

@@ -64,7 +64,9 @@ struct bf_grid_pipeline {
     float* integ[2] = {};
     int8_t* codes[2] = {};
     float* params[2] = {};
-    void* split = nullptr;
+    void* split = nullptr;     // split operand, or the checked form's (covariance image + split image)
+    bool checked = false;      // run the checked covariance form instead of the split kernel
+    void* workspace = nullptr; // the checked form's fallback list
     bool weights_ready = false;
 
     bf_status init() {
@@ -90,6 +92,12 @@ struct bf_grid_pipeline {
             BF_RETURN_IF(cuda_status(cudaMalloc(&codes[i], n_out), "cudaMalloc chunk codes"));
             BF_RETURN_IF(cuda_status(cudaMalloc(&params[i], n_par * sizeof(float)), "cudaMalloc chunk parameters"));
         }
+        if (checked) {
+            const bf_dims dc{t, dims.n_freq, dims.n_ant, dims.n_beams};
+            const uint64_t ws = auto_workspace_bytes(dc, spectra, n_shards);
+            if (ws > 0) BF_RETURN_IF(cuda_status(cudaMalloc(&workspace, ws), "cudaMalloc fallback list"));
+            return cuda_status(cudaMalloc(&split, auto_weight_bytes(dims, n_shards)), "cudaMalloc weights");
+        }
         return cuda_status(cudaMalloc(&split, split_weight_bytes(dims, n_shards)), "cudaMalloc split weights");
     }
 
@@ -113,6 +121,7 @@ struct bf_grid_pipeline {
             if (d2h_done[i]) cudaEventDestroy(d2h_done[i]);
         }
         cudaFree(split);
+        cudaFree(workspace);
         if (start) cudaEventDestroy(start);
         if (end) cudaEventDestroy(end);
         if (in) cudaStreamDestroy(in);
@@ -146,8 +155,13 @@ struct bf_grid_pipeline {
             BF_RETURN_IF(cuda_status(cudaStreamWaitEvent(comp, h2d_done[s], 0), "cudaStreamWaitEvent"));
             if (c >= 2) BF_RETURN_IF(cuda_status(cudaStreamWaitEvent(comp, d2h_done[s], 0), "cudaStreamWaitEvent"));
             const bf_dims dc{tc, F, A, B};
-            BF_RETURN_IF(launch_grid_tensor(comp, volt[s], split, integ[s], quantize ? codes[s] : nullptr,
-                                            quantize ? params[s] : nullptr, dc, spectra, n_shards, nullptr));
+            if (checked) {
+                BF_RETURN_IF(launch_grid_auto(comp, volt[s], split, integ[s], quantize ? codes[s] : nullptr,
+                                              quantize ? params[s] : nullptr, workspace, dc, spectra, n_shards));
+            } else {
+                BF_RETURN_IF(launch_grid_tensor(comp, volt[s], split, integ[s], quantize ? codes[s] : nullptr,
+                                                quantize ? params[s] : nullptr, dc, spectra, n_shards, nullptr));
+            }
             BF_RETURN_IF(cuda_status(cudaEventRecord(comp_done[s], comp), "cudaEventRecord"));
             // copy-out: [shard][window] rows of this chunk into the block's place
             BF_RETURN_IF(cuda_status(cudaStreamWaitEvent(out, comp_done[s], 0), "cudaStreamWaitEvent"));
@@ -228,13 +242,14 @@ BF_API uint64_t bf_grid_pipeline_chunk_spectra(const bf_dims* dims, uint64_t int
     return pick_chunk(*dims, integration_spectra, n_shards, chunk_spectra);
 }
 
-BF_API bf_status bf_grid_pipeline_create(const bf_dims* dims, uint64_t integration_spectra, uint64_t n_shards,
-                                         uint64_t chunk_spectra, bf_grid_pipeline** pipeline) {
+static bf_status create_pipeline(const bf_dims* dims, uint64_t integration_spectra, uint64_t n_shards,
+                                 uint64_t chunk_spectra, bool checked, bf_grid_pipeline** pipeline) {
     clear_error();
     if (pipeline == nullptr) return set_error(BF_ERR_INVALID_ARGUMENT, "pipeline must not be null");
     *pipeline = nullptr;
     BF_RETURN_IF(check_request(dims, integration_spectra, n_shards, chunk_spectra));
     auto* p = new bf_grid_pipeline();
+    p->checked = checked;
     p->dims = *dims;
     p->spectra = integration_spectra;
     p->n_shards = n_shards;
@@ -248,6 +263,17 @@ BF_API bf_status bf_grid_pipeline_create(const bf_dims* dims, uint64_t integrati
     return BF_OK;
 }
 
+BF_API bf_status bf_grid_pipeline_create(const bf_dims* dims, uint64_t integration_spectra, uint64_t n_shards,
+                                         uint64_t chunk_spectra, bf_grid_pipeline** pipeline) {
+    return create_pipeline(dims, integration_spectra, n_shards, chunk_spectra, false, pipeline);
+}
+
+BF_API bf_status bf_grid_pipeline_create_checked(const bf_dims* dims, uint64_t integration_spectra,
+                                                 uint64_t n_shards, uint64_t chunk_spectra,
+                                                 bf_grid_pipeline** pipeline) {
+    return create_pipeline(dims, integration_spectra, n_shards, chunk_spectra, true, pipeline);
+}
+
 BF_API bf_status bf_grid_pipeline_upload_weights(bf_grid_pipeline* p, const float* host_weights) {
     clear_error();
     if (p == nullptr || host_weights == nullptr) {
@@ -258,7 +284,10 @@ BF_API bf_status bf_grid_pipeline_upload_weights(bf_grid_pipeline* p, const floa
     BF_RETURN_IF(cuda_status(cudaMalloc(&canon, n * sizeof(float)), "cudaMalloc weights"));
     bf_status st = cuda_status(cudaMemcpyAsync(canon, host_weights, n * sizeof(float), cudaMemcpyHostToDevice, p->comp),
                                "cudaMemcpyAsync weights");
-    if (st == BF_OK) st = launch_prepare_split(p->comp, canon, p->split, p->dims, p->n_shards);
+    if (st == BF_OK) {
+        st = p->checked ? launch_prepare_auto(p->comp, canon, p->split, p->dims, p->n_shards)
+                        : launch_prepare_split(p->comp, canon, p->split, p->dims, p->n_shards);
+    }
     const bf_status sync = cuda_status(cudaStreamSynchronize(p->comp), "cudaStreamSynchronize");
     cudaFree(canon);
     if (st == BF_OK) st = sync;

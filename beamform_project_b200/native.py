@@ -136,6 +136,7 @@ _SIGS = {
                                C.POINTER(C.c_uint32)]),
     "bf_grid_pipeline_chunk_spectra": (_U64, [C.POINTER(Dims), _U64, _U64, _U64]),
     "bf_grid_pipeline_create": (C.c_int, [C.POINTER(Dims), _U64, _U64, _U64, _PP]),
+    "bf_grid_pipeline_create_checked": (C.c_int, [C.POINTER(Dims), _U64, _U64, _U64, _PP]),
     "bf_grid_pipeline_upload_weights": (C.c_int, [_P, _P]),
     "bf_grid_pipeline_run": (C.c_int, [_P, _P, _P, _P, _P, C.POINTER(C.c_float)]),
     "bf_grid_pipeline_destroy": (C.c_int, [_P]),

@@ -381,12 +381,24 @@ def run_gpu(args):
     codes = torch.empty(N_SHARDS * n_out, dtype=torch.int8, device=dev)
     params = torch.empty(N_SHARDS * n_par, dtype=torch.float32, device=dev)
     kernel = args.kernel
+    tensor_path = kernel in ("tensor", "auto")
     split = None
-    if kernel == "tensor":
+    tune = None
+    if tensor_path:
         split = torch.empty(api.split_weight_bytes(d, N_SHARDS), dtype=torch.uint8, device=dev)
         api.prepare_split_weights(None, weights, split, d, N_SHARDS)
         workspace = torch.empty(api.grid_tensor_workspace_bytes(d, S_INT, N_SHARDS), dtype=torch.uint8,
                                 device=dev)
+    if kernel == "auto":
+        # the checked covariance form, with the grid path's launch choices
+        # tuned for this class first (every candidate timed, parity-gated)
+        auto_w = torch.empty(api.auto_weight_bytes(d, N_SHARDS), dtype=torch.uint8, device=dev)
+        api.prepare_auto_weights(None, weights, auto_w, d, N_SHARDS)
+        auto_ws = torch.zeros(max(256, api.grid_auto_workspace_bytes(d, S_INT, N_SHARDS)), dtype=torch.uint8,
+                              device=dev)
+        t_tune = time.perf_counter()
+        tune = api.autotune_grid(None, d, S_INT, N_SHARDS)
+        tune["wall_s"] = round(time.perf_counter() - t_tune, 2)
     torch.cuda.synchronize()
 
     main_events = []  # CUDA events around the dominant kernel of each timed step
@@ -397,6 +409,14 @@ def run_gpu(args):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
+        if kernel == "auto":
+            # checked form (covariance form + recomputed units), then the int8 chunk quantizer
+            api.grid_auto_integrated(None, volt, auto_w, integ, None, None, auto_ws, d, S_INT, N_SHARDS)
+            if record:
+                e1.record(stream)
+                main_events.append((e0, e1))
+            api.launch_quantize_integrated_intensity(None, integ, codes, params, qd_all)
+            return 3 if tune is None or tune["chosen"]["form"] != "split" else 2
         if kernel == "tensor":
             if args.fused_quant:
                 # one kernel: beamform, |.|^2, integration and int8 quantization fused
@@ -488,11 +508,11 @@ def run_gpu(args):
     e2e_ms = a0.elapsed_time(a1) / e2e_steps
     e2e_path = "torch copies + device-pointer C-ABI calls, one phase after the other"
     serial_ms, e2e_chunk, e2e_match = None, None, None
-    if kernel == "tensor" and not args.fused_quant:
+    if tensor_path and not args.fused_quant:
         # the host-buffer C-ABI pipeline: the same products, with each time
         # chunk's copy-in, kernels and copy-out overlapped on three streams
         serial_ms = e2e_ms
-        pipe = api.GridHostPipeline(d, S_INT, N_SHARDS)
+        pipe = api.GridHostPipeline(d, S_INT, N_SHARDS, checked=kernel == "auto")
         pipe.upload_weights(w_host)
         e2e_chunk = pipe.chunk_spectra
         pipe.run(host_v, host_i, host_c, host_p)
@@ -502,7 +522,8 @@ def run_gpu(args):
             dist.barrier()
         e2e_ms = statistics.mean(pipe.run(host_v, host_i, host_c, host_p) for _ in range(e2e_steps))
         pipe.close()
-        e2e_path = "bf_grid_pipeline_run: pinned host buffers, chunked copy-in / kernels / copy-out overlap"
+        e2e_path = ("bf_grid_pipeline_run" + (" (checked form)" if kernel == "auto" else "") +
+                    ": pinned host buffers, chunked copy-in / kernels / copy-out overlap")
     if dist:
         tt = torch.tensor([e2e_ms], device=dev)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
@@ -516,7 +537,7 @@ def run_gpu(args):
     # the plain drop-in beside it: the reference-order float32 kernel (Direct,
     # bit-identical to the reference CPU core) and the quantizer, same inputs
     plain = None
-    if kernel == "tensor" and args.plain_steps > 0:
+    if tensor_path and args.plain_steps > 0:
         integ_p = torch.empty_like(integ)
         codes_p = torch.empty_like(codes)
         params_p = torch.empty_like(params)
@@ -548,7 +569,7 @@ def run_gpu(args):
     # the covariance form beside it (opt-in kernel, same inputs): time and
     # distance from the reference-order float32 output
     cov = None
-    if kernel == "tensor" and args.cov_steps > 0 and plain is not None:
+    if tensor_path and args.cov_steps > 0 and plain is not None:
         covw = torch.empty(api.cov_weight_bytes(d, N_SHARDS), dtype=torch.uint8, device=dev)
         api.prepare_cov_weights(None, weights, covw, d, N_SHARDS)
         integ_c = torch.empty_like(integ)
@@ -599,6 +620,13 @@ def run_gpu(args):
         assert native.take_device_error() == 0
         n_units = int(aws[:4].view(torch.int32).item())
         rel = ((integ_a.double() - integ_p.double()).abs() / integ_p.double().abs().clamp_min(1e-30)).max().item()
+        if kernel == "auto":
+            def split_step():
+                api.grid_tensor_integrated(None, volt, split, integ_p2, None, None, d, S_INT, N_SHARDS)
+            integ_p2 = torch.empty_like(integ)
+            split_step()
+            cov["split_form_ms"] = event_time(stream, split_step, args.cov_steps)
+            del integ_p2
         cov["checked_form"] = {
             "kernel": "grid_cov_kernel with error estimates + grid_tensor_kernel over the listed units",
             "ms_per_step": a_ms, "value": samples_per_step / (a_ms / 1e3),
@@ -609,7 +637,7 @@ def run_gpu(args):
 
     # the reference's own CUDA kernels (Tiled + int8 quantizer) on the same GPU and inputs
     ref_gpu = None
-    if kernel == "tensor" and args.ref_gpu_steps > 0:
+    if tensor_path and args.ref_gpu_steps > 0:
         ref_gpu = reference_gpu_grid(volt, w_host, integ, codes, shard_bytes, n_out, W, S_INT,
                                      args.ref_gpu_steps, stream)
         if "ms_per_step" in ref_gpu:
@@ -619,9 +647,15 @@ def run_gpu(args):
     alg_flops = 8 * cmac + 3 * samples_per_step
     csum = clocks.summary()
     roofline = tensor_roofline(alg_flops, main_ms, ms / 1e3, csum)
-    roofline["traffic"] = (round(NCU_TRAFFIC["grid"]) if kernel == "tensor" and N_SHARDS == 2
-                           and not args.fused_quant else None)
-    roofline["kernel"] = "grid_tensor_kernel" if kernel == "tensor" else "grid_exact_kernel+quantize"
+    if kernel == "auto":
+        roofline["traffic"] = round(NCU_TRAFFIC["grid_cov"]) if N_SHARDS == 2 and "grid_cov" in NCU_TRAFFIC \
+            else None
+        roofline["kernel"] = ("grid_cov_kernel + grid_tensor_kernel over recomputed units (checked form)"
+                              if tune is None or tune["chosen"]["form"] != "split" else "grid_tensor_kernel")
+    else:
+        roofline["traffic"] = (round(NCU_TRAFFIC["grid"]) if kernel == "tensor" and N_SHARDS == 2
+                               and not args.fused_quant else None)
+        roofline["kernel"] = "grid_tensor_kernel" if kernel == "tensor" else "grid_exact_kernel+quantize"
 
     line = {
         "metric": METRIC, "value": value, "unit": "beam-samples/s", "n_gpus": world,
@@ -644,11 +678,12 @@ def run_gpu(args):
         "plain_dropin": plain,
         "covariance_form": cov,
         "reference_gpu": ref_gpu,
+        "autotune": tune,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v0 = volt[:shard_bytes].cpu().numpy().reshape(T_SPECTRA, F_SHARD, N_ANT)
         line["cpu_baseline"] = cpu_baseline(v0, w_host[0], budget_s=args.cpu_seconds)
-    if world == 1 and args.configs and kernel == "tensor":
+    if world == 1 and args.configs and tensor_path:
         # the other workloads, each measured the same way (CUDA-event kernel
         # time, roofline, CPU baseline, end to end, clocks), as sub-records
         del volt, weights, integ, codes, params, split, workspace, host_v, host_i, host_c, host_p
@@ -927,7 +962,7 @@ def run_tracker(args, emit: bool = True):
     dirs_d = torch.from_numpy(dirs).to(dev)
     integ = torch.empty(W * F_SHARD, dtype=torch.float32, device=dev)
     inten = torch.empty(TR_T * F_SHARD, dtype=torch.float32, device=dev)
-    mode = api.TrackerMode.Streaming if args.kernel in ("tensor", "stream") else api.TrackerMode.ReferenceOrder
+    mode = api.TrackerMode.Streaming if args.kernel in ("auto", "tensor", "stream") else api.TrackerMode.ReferenceOrder
 
     def step(per_spectrum=False):
         api.tracker(None, mode, volt, pos_d, k_d, dirs_d, inten if per_spectrum else None, integ, d, TR_S)
@@ -1701,7 +1736,8 @@ def main():
     ap.add_argument("--workload", default="grid", choices=["grid", "tracker", "doa", "serve"])
     ap.add_argument("--cov-steps", type=int, default=20,
                     help="grid: time the opt-in covariance-form kernel beside the split kernel")
-    ap.add_argument("--kernel", default="tensor", choices=["tensor", "tiled", "stream", "exact"])
+    ap.add_argument("--kernel", default="auto", choices=["auto", "tensor", "tiled", "stream", "exact"],
+                    help="grid: auto = the checked covariance form, autotuned; tensor = the split kernel")
     ap.add_argument("--shards", type=int, default=N_SHARDS, choices=[1, 2])
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--fused-quant", action="store_true",

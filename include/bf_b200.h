@@ -323,6 +323,12 @@ BF_API uint64_t bf_grid_pipeline_chunk_spectra(const bf_dims* dims, uint64_t int
 BF_API bf_status bf_grid_pipeline_create(const bf_dims* dims, uint64_t integration_spectra,
                                          uint64_t n_shards, uint64_t chunk_spectra,
                                          bf_grid_pipeline** pipeline);
+/* bf_grid_pipeline_create for the checked grid beamformer
+ * (bf_grid_auto_integrated): same buffers, chunks and products layout; the
+ * uploaded weights become the checked form's operand. */
+BF_API bf_status bf_grid_pipeline_create_checked(const bf_dims* dims, uint64_t integration_spectra,
+                                                 uint64_t n_shards, uint64_t chunk_spectra,
+                                                 bf_grid_pipeline** pipeline);
 
 /* Canonical complex64 weights [shard][B][F][A][2] from host memory, prepared
  * into the resident split operand.  Synchronous. */

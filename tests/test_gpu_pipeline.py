@@ -78,3 +78,38 @@ def test_pipeline_errors(cuda):
         pipe.run(v.reshape(-1), out)
     with pytest.raises(api.LogicError, match="closed"):
         pipe.run(v.reshape(-1), out)
+
+
+@pytest.mark.parametrize("A,B,T,S,shards,chunk", [(64, 128, 3000, 320, 2, 640), (64, 24, 2000, 64, 1, 256),
+                                                  (32, 40, 1300, 320, 1, 640)])
+def test_checked_pipeline_equals_single_checked_launch(cuda, ref, A, B, T, S, shards, chunk):
+    """The checked form through the host pipeline: chunks hold whole windows,
+    so every window's covariance, estimate and recomputation are those of
+    one launch over the block: bit-identical products.  The strong-source
+    data (every beam a sidelobe) makes units fall back to the split kernel."""
+    from beamform_project_b200 import api
+    torch = cuda
+    pos, freq = ref.ref_default_positions(A), ref.ref_channelized_frequencies(F)
+    v = np.stack([ref.ref_make_moving_point_source(T, F, A, pos, freq, 0.0, -0.05 + 0.01 * s, 0.0, 0.0, 3.0)
+                  for s in range(shards)])
+    w = np.stack([grid_weights(A, F, B, seed=80 + s) for s in range(shards)])
+    d = api.Dimensions(T, F, A, B)
+    W = -(-T // S)
+    qd = api.Dimensions(W, F, A, B)
+    aw = torch.empty(api.auto_weight_bytes(d, shards), dtype=torch.uint8, device="cuda")
+    api.prepare_auto_weights(None, torch.from_numpy(w).cuda(), aw, d, shards)
+    ws = torch.zeros(max(256, api.grid_auto_workspace_bytes(d, S, shards)), dtype=torch.uint8, device="cuda")
+    integ = torch.empty(shards * W * F * B, dtype=torch.float32, device="cuda")
+    codes = torch.empty(shards * W * F * B, dtype=torch.int8, device="cuda")
+    params = torch.empty(shards * 2 * api.quantization_parameter_count(qd), dtype=torch.float32, device="cuda")
+    api.grid_auto_integrated(None, torch.from_numpy(v).cuda(), aw, integ, codes, params, ws, d, S, shards)
+    torch.cuda.synchronize()
+    with api.GridHostPipeline(d, S, shards, chunk, checked=True) as pipe:
+        pipe.upload_weights(w)
+        got_i = np.full(integ.numel(), -1.0, np.float32)
+        got_c = np.full(codes.numel(), 99, np.int8)
+        got_p = np.full(params.numel(), -1.0, np.float32)
+        pipe.run(v.reshape(-1), got_i, got_c, got_p)
+    assert np.array_equal(got_i, integ.cpu().numpy())
+    assert np.array_equal(got_c, codes.cpu().numpy())
+    assert np.array_equal(got_p, params.cpu().numpy())
