@@ -584,6 +584,39 @@ def doa_scan(stream, covariance, positions, wave_numbers, dims: Dimensions, bloc
                                    int(n_points), float(m_fixed), b, cp, le, w))
 
 
+def doa_track_config(block_len: int, subarray: int = 0, capon: bool = False, grid: int = 16, levels: int = 2,
+                     interp: bool = True, fov_l: float = 0.2, fov_m: float = 0.2, forgetting: float = 1.0,
+                     diag_load: float = 1e-3, prior_l: float = 0.0, prior_m: float = 0.0):
+    """bf_doa_track_config; fields and defaults follow CpuOptTrackerConfig
+    (include/beamformer/cpu_opt_beam_tracker.hpp:45-86) with the scan on."""
+    return native.DoaTrackConfig(int(block_len), int(subarray), int(bool(capon)), int(grid), int(levels),
+                                 int(bool(interp)), float(fov_l), float(fov_m), float(forgetting), float(diag_load),
+                                 float(prior_l), float(prior_m))
+
+
+def doa_track_workspace_bytes(dims: Dimensions, config) -> int:
+    d = dims.c()
+    return int(native.lib().bf_doa_track_workspace_bytes(C.byref(d), C.byref(config)))
+
+
+def doa_track(stream, packed_voltage, positions, wave_numbers, dims: Dimensions, config, window_directions,
+              intensity, workspace) -> None:
+    """The reference's adaptive tracker on the GPU (bf_doa_track): per window a
+    coarse-to-fine (l, m) search, then the beam along the estimate.
+    window_directions float [W][3]; intensity float [T][F] or None."""
+    torch = _torch()
+    validate_dimensions(dims)
+    W = dims.n_time // int(config.block_len) if config.block_len else 0
+    v = _dev(packed_voltage, "packed_voltage", torch.uint8, dims.n_time * dims.n_freq * dims.n_ant)
+    pp = _dev(positions, "positions", torch.float32, 3 * dims.n_ant)
+    k = _dev(wave_numbers, "wave_numbers", torch.float64, dims.n_freq)
+    dd = _dev(window_directions, "window_directions", torch.float32, 3 * W)
+    ii = None if intensity is None else _dev(intensity, "intensity", torch.float32, dims.n_time * dims.n_freq)
+    ws = _dev(workspace, "workspace", torch.uint8, doa_track_workspace_bytes(dims, config))
+    d = dims.c()
+    check(native.lib().bf_doa_track(_stream_handle(stream), v, pp, k, C.byref(d), C.byref(config), dd, ii, ws))
+
+
 # --------------------------------------------------------------------------
 # weights (generate_weights, reference src/weights.cpp:11-60) on the device
 # --------------------------------------------------------------------------

@@ -30,7 +30,7 @@ NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fvisibilit
 CUDA_SOURCES = ["capi.cu", "grid_exact.cu", "quantize.cu", "generate.cu", "tracker.cu",
                 "tracker_stream.cu", "grid_tc.cu", "no_alloc.cu", "doa_cov.cu", "doa_scan.cu",
                 "serve_kernels.cu", "serve.cu", "selftest.cu", "loss_mask.cu", "pipeline.cu", "grid_cov.cu",
-                "autotune.cu"]
+                "autotune.cu", "doa_track.cu"]
 CXX_SOURCES = ["cxx_api.cpp", "io.cpp"]
 CLI = PKG / "cli"
 BIN = PKG / "bin"

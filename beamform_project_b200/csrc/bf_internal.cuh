@@ -227,6 +227,18 @@ bf_status launch_doa_covariance(cudaStream_t stream, const uint8_t* v, int32_t* 
 bf_status launch_apply_loss_mask(cudaStream_t stream, uint8_t* v, const uint8_t* mask, uint64_t n_time,
                                  uint64_t n_freq, uint64_t n_ant, uint64_t spectra, uint32_t* counts);
 uint64_t doa_workspace_bytes(uint64_t n_blocks, uint64_t n_freq, uint64_t M);
+// The DOA fold (doa_scan.cu) of every (block, channel) cell, cell = block *
+// n_freq + f, into the head of `workspace` (doa_fold_bytes): S [cells][M][M]
+// and Q = (S + E I)^{-1} [cells][M][M] as (re, im) double pairs, E [cells]
+// double, ok [cells] int (the loaded Cholesky succeeded).
+uint64_t doa_fold_bytes(uint64_t cells, uint64_t M);
+bf_status launch_doa_fold(cudaStream_t stream, const int32_t* R, const bf_dims& d, uint64_t block_len, int M,
+                          double lam, double load, void* workspace);
+// The adaptive tracker (doa_track.cu).
+uint64_t doa_track_workspace_bytes(const bf_dims& d, uint64_t block_len, uint64_t subarray);
+bf_status launch_doa_track(cudaStream_t stream, const uint8_t* v, const float* pos, const double* kw,
+                           const bf_dims& d, const bf_doa_track_config& c, float* dirs, float* intensity,
+                           void* workspace);
 bf_status launch_doa_scan(cudaStream_t stream, const int32_t* R, const float* pos, const double* kw,
                           const bf_dims& d, uint64_t block_len, uint64_t subarray, double lam, double load,
                           double l_first, double l_step, uint64_t n, double m_fixed, double* bartlett,

@@ -12,6 +12,7 @@
 
 #include <cstdio>
 #include <cstring>
+#include <cmath>
 #include <string>
 
 namespace bf {
@@ -420,6 +421,49 @@ BF_API bf_status bf_doa_scan(void* stream, const int32_t* covariance, const floa
     return launch_doa_scan(static_cast<cudaStream_t>(stream), covariance, positions, wave_numbers, *dims,
                            block_len, subarray, forgetting, diag_load, l_first, l_step, n_points, m_fixed,
                            bartlett, capon, l_est, workspace);
+}
+
+static bf_status check_track(const bf_dims* dims, const bf_doa_track_config* c) {
+    BF_TRY(validate_dims(dims));
+    if (c == nullptr) return set_error(BF_ERR_INVALID_ARGUMENT, "config must not be null");
+    if (dims->n_beams != 1) return set_error(BF_ERR_INVALID_ARGUMENT, "the DOA path takes n_beams == 1");
+    if (dims->n_ant > 64) return set_error(BF_ERR_UNSUPPORTED, "the DOA covariance supports n_ant 32 or 64");
+    if (c->block_len == 0 || c->block_len % 128 != 0 || dims->n_time % c->block_len != 0) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "block_len must be a multiple of 128 dividing n_time");
+    }
+    const uint64_t M = (c->subarray > 0 && c->subarray < dims->n_ant) ? c->subarray : dims->n_ant;
+    if (M > 16) return set_error(BF_ERR_UNSUPPORTED, "the DOA search supports at most 16 elements after smoothing");
+    if (c->estimator > 1) return set_error(BF_ERR_INVALID_ARGUMENT, "estimator must be 0 (Bartlett) or 1 (Capon)");
+    if (c->grid < 2 || c->grid > 64 || c->levels > 16) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "grid must be 2 to 64 and levels at most 16");
+    }
+    if (!(c->fov_l >= 0.f) || !(c->fov_m >= 0.f) || !(c->forgetting > 0.f && c->forgetting <= 1.f) ||
+        !(c->diag_load >= 0.f) || !std::isfinite(c->prior_l) || !std::isfinite(c->prior_m) ||
+        c->prior_l * c->prior_l + c->prior_m * c->prior_m > 1.f) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "invalid field of view, forgetting, loading or prior");
+    }
+    if (dims->n_time / c->block_len > 65535) return set_error(BF_ERR_OVERFLOW, "at most 65535 windows");
+    return BF_OK;
+}
+
+BF_API uint64_t bf_doa_track_workspace_bytes(const bf_dims* dims, const bf_doa_track_config* config) {
+    if (check_track(dims, config) != BF_OK) return 0;
+    return doa_track_workspace_bytes(*dims, config->block_len, config->subarray);
+}
+
+BF_API bf_status bf_doa_track(void* stream, const uint8_t* packed_voltage, const float* positions,
+                              const double* wave_numbers, const bf_dims* dims, const bf_doa_track_config* config,
+                              float* window_directions, float* intensity, void* workspace) {
+    clear_error();
+    BF_TRY(check_track(dims, config));
+    BF_TRY(check_ptr(packed_voltage, 16, "packed_voltage"));
+    BF_TRY(check_ptr(positions, 4, "positions"));
+    BF_TRY(check_ptr(wave_numbers, 8, "wave_numbers"));
+    BF_TRY(check_ptr(window_directions, 4, "window_directions"));
+    if (intensity != nullptr) BF_TRY(check_ptr(intensity, 4, "intensity"));
+    BF_TRY(check_ptr(workspace, 256, "workspace"));
+    return launch_doa_track(static_cast<cudaStream_t>(stream), packed_voltage, positions, wave_numbers, *dims,
+                            *config, window_directions, intensity, workspace);
 }
 
 BF_API bf_status bf_take_device_error(uint32_t* code) {

@@ -628,12 +628,11 @@ uint64_t doa_workspace_bytes(uint64_t n_blocks, uint64_t n_freq, uint64_t M) {
     return doa_coef_offset(cells, M) + info + cells * 2 * coef_per_form(static_cast<int>(M)) * sizeof(double) + 256;
 }
 
-bf_status launch_doa_scan(cudaStream_t stream, const int32_t* R, const float* pos, const double* kw,
-                          const bf_dims& d, uint64_t block_len, uint64_t subarray, double lam, double load,
-                          double l_first, double l_step, uint64_t n, double m_fixed, double* bartlett,
-                          double* capon, double* l_est, void* workspace) {
+uint64_t doa_fold_bytes(uint64_t cells, uint64_t M) { return doa_coef_offset(cells, M); }
+
+bf_status launch_doa_fold(cudaStream_t stream, const int32_t* R, const bf_dims& d, uint64_t block_len, int M,
+                          double lam, double load, void* workspace) {
     const int A = static_cast<int>(d.n_ant);
-    const int M = (subarray > 0 && subarray < d.n_ant) ? static_cast<int>(subarray) : A;
     if (M > kMaxM) return set_error(BF_ERR_UNSUPPORTED, "the DOA scan supports at most 16 elements after smoothing");
     if (d.n_time / block_len > 65535) return set_error(BF_ERR_OVERFLOW, "at most 65535 covariance blocks per scan");
     const int B = static_cast<int>(d.n_time / block_len), F = static_cast<int>(d.n_freq);
@@ -648,7 +647,23 @@ bf_status launch_doa_scan(cudaStream_t stream, const int32_t* R, const float* po
     doa_forget_kernel<<<F, 64, 0, stream>>>(Lc, B, F, M, lam, S, E);
     BF_RETURN_IF(cuda_status(cudaGetLastError(), "doa_forget_kernel launch"));
     doa_factor_kernel<<<cells_grid, 64, 0, stream>>>(S, E, F, M, Lc, ok);
-    BF_RETURN_IF(cuda_status(cudaGetLastError(), "doa_factor_kernel launch"));
+    return cuda_status(cudaGetLastError(), "doa_factor_kernel launch");
+}
+
+bf_status launch_doa_scan(cudaStream_t stream, const int32_t* R, const float* pos, const double* kw,
+                          const bf_dims& d, uint64_t block_len, uint64_t subarray, double lam, double load,
+                          double l_first, double l_step, uint64_t n, double m_fixed, double* bartlett,
+                          double* capon, double* l_est, void* workspace) {
+    const int A = static_cast<int>(d.n_ant);
+    const int M = (subarray > 0 && subarray < d.n_ant) ? static_cast<int>(subarray) : A;
+    BF_RETURN_IF(launch_doa_fold(stream, R, d, block_len, M, lam, load, workspace));
+    const int B = static_cast<int>(d.n_time / block_len), F = static_cast<int>(d.n_freq);
+    const uint64_t cells = static_cast<uint64_t>(B) * F;
+    auto* S = static_cast<Cd*>(workspace);
+    Cd* Lc = S + cells * M * M;
+    auto* E = reinterpret_cast<double*>(Lc + cells * M * M);
+    auto* ok = reinterpret_cast<int*>(E + cells);
+    const dim3 cells_grid(static_cast<unsigned>(F), static_cast<unsigned>(B));
     auto* info = reinterpret_cast<ArrayInfo*>(static_cast<uint8_t*>(workspace) + doa_coef_offset(cells, M));
     auto* coef = reinterpret_cast<double*>(reinterpret_cast<uint8_t*>(info) + (sizeof(ArrayInfo) + 255) / 256 * 256);
     const double l_abs_max = std::max(std::fabs(l_first), std::fabs(l_first + static_cast<double>(n - 1) * l_step));

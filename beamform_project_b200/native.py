@@ -93,6 +93,13 @@ class GridConfig(C.Structure):
     _fields_ = [("form", C.c_int32), ("group_mult", C.c_int32), ("paired", C.c_int32), ("reserved", C.c_int32)]
 
 
+class DoaTrackConfig(C.Structure):
+    _fields_ = [("block_len", C.c_uint64), ("subarray", C.c_uint64), ("estimator", C.c_uint32),
+                ("grid", C.c_uint32), ("levels", C.c_uint32), ("interp", C.c_uint32), ("fov_l", C.c_float),
+                ("fov_m", C.c_float), ("forgetting", C.c_float), ("diag_load", C.c_float), ("prior_l", C.c_float),
+                ("prior_m", C.c_float)]
+
+
 class ServeJobInfo(C.Structure):
     _fields_ = [("state", C.c_int32), ("pad", C.c_uint32), ("submit_step", C.c_uint64), ("admit_step", C.c_uint64),
                 ("last_step", C.c_uint64), ("windows_launched", C.c_uint64)]
@@ -149,6 +156,8 @@ _SIGS = {
     "bf_doa_scan": (C.c_int, [_P, _P, _P, _P, C.POINTER(Dims), _U64, _U64, C.c_double, C.c_double,
                               C.c_double, C.c_double, _U64, C.c_double, _P, _P, _P, _P]),
     "bf_generate_voltage": (C.c_int, [_P, _U64, _U64, C.c_float, _P, _U64, _P, C.POINTER(Dims)]),
+    "bf_doa_track_workspace_bytes": (_U64, [C.POINTER(Dims), C.POINTER(DoaTrackConfig)]),
+    "bf_doa_track": (C.c_int, [_P, _P, _P, _P, C.POINTER(Dims), C.POINTER(DoaTrackConfig), _P, _P, _P]),
     "bf_generate_weights": (C.c_int, [_P, _P, _P, _P, _P, C.POINTER(Dims), _U64]),
     "bf_apply_loss_mask": (C.c_int, [_P, _P, _P, C.POINTER(Dims), _U64, _P]),
     "bf_probe_bounded_wait": (C.c_int, [_P, _U64]),

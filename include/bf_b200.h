@@ -407,6 +407,39 @@ BF_API bf_status bf_doa_scan(void* stream, const int32_t* covariance, const floa
                              double l_first, double l_step, uint64_t n_points, double m_fixed,
                              double* bartlett, double* capon, double* l_est, void* workspace);
 
+/* The reference's adaptive tracker (CpuOptBeamTracker::run_into,
+ * src/cpu_opt_beam_tracker.cpp:1619-2454) on the GPU: per window of
+ * block_len spectra, the covariance fold above, then a coarse-to-fine
+ * search -- a grid x grid lattice of (l, m) over +-fov around the previous
+ * window's estimate (the prior for the first), `levels` 3 x 3 refinements at
+ * halved pitch, the reference's 3-point quadratic interpolation -- with
+ * Bartlett (estimator 0) or Capon (1) power summed over frequency; then the
+ * beam along each window's estimate, per spectrum, in the reference's float32
+ * order (its emission pass).  Fields follow CpuOptTrackerConfig
+ * (include/beamformer/cpu_opt_beam_tracker.hpp:45-86). */
+typedef struct bf_doa_track_config {
+    uint64_t block_len;   /* integration_spectra: a multiple of 128 dividing n_time */
+    uint64_t subarray;    /* spatial_smoothing_subarray_size: the search takes at most 16 elements
+                           * after smoothing (0, no smoothing, only for n_ant <= 16) */
+    uint32_t estimator;   /* 0 Bartlett, 1 Capon */
+    uint32_t grid;        /* coarse_grid_resolution, 2 .. 64 */
+    uint32_t levels;      /* refinement_levels, 0 .. 16 */
+    uint32_t interp;      /* enable_quadratic_peak_interp */
+    float fov_l, fov_m;   /* search_fov_l, search_fov_m */
+    float forgetting;     /* forgetting_factor, (0, 1] */
+    float diag_load;      /* diagonal_load */
+    float prior_l, prior_m; /* the seeded trajectory's start direction */
+} bf_doa_track_config;
+
+BF_API uint64_t bf_doa_track_workspace_bytes(const bf_dims* dims, const bf_doa_track_config* config);
+
+/* packed_voltage [T][F][A] (A = 32 or 64), positions [A][3] float, wave_numbers
+ * [F] double, all device; outputs (device): window_directions [T/block_len][3]
+ * float; intensity [T][F] float (per-spectrum beam power, may be NULL). */
+BF_API bf_status bf_doa_track(void* stream, const uint8_t* packed_voltage, const float* positions,
+                              const double* wave_numbers, const bf_dims* dims, const bf_doa_track_config* config,
+                              float* window_directions, float* intensity, void* workspace);
+
 /* ------------------------------------------------------------------------ */
 /* Seeded synthetic voltages (no reference counterpart)                     */
 /* ------------------------------------------------------------------------ */

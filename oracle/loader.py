@@ -165,7 +165,7 @@ def _bind_reference(r: C.CDLL) -> C.CDLL:
     r.ref_make_moving_point_source.argtypes = [U64, U64, U64, P, P, F32, F32, F32, F32, F32, P]
     r.ref_set_threads.argtypes = [C.c_int]
     r.ref_doa_directions.argtypes = [P, U64, U64, U64, P, P, C.c_int, U64, U64, F32, F32, U64, F32,
-                                     F32, U64, F32, F32, P]
+                                     F32, U64, F32, F32, P, P]
     r.ref_io_write.argtypes = [C.c_char_p, P, P, P, P, P, P, P] + [U64] * 9
     r.ref_io_read_check.argtypes = [C.c_char_p, P, P, P, P, P, P] + [U64] * 9
     return r
@@ -292,15 +292,19 @@ def doa_scan(R: np.ndarray, K: int, subarray: int, lam: float, load: float, pos_
 
 
 def ref_doa_directions(v, pos, freq, K, capon=False, G=16, levels=2, fov_l=0.2, fov_m=0.2,
-                       subarray=0, lam=1.0, load=1e-3, l0=0.0, m0=0.0) -> np.ndarray:
+                       subarray=0, lam=1.0, load=1e-3, l0=0.0, m0=0.0, intensity=False):
+    """CpuOptBeamTracker's per-window directions [W][3] (and, with
+    intensity=True, its emitted [T][F] beam power as a second value)."""
     T, F, A = v.shape
     W = -(-T // K)
     out = np.zeros((W, 3), np.float32)
+    inten = np.zeros((T, F), np.float32) if intensity else None
     _rcheck(_lib().ref_doa_directions(_ptr(np.ascontiguousarray(v)), T, F, A,
-                                           _ptr(np.ascontiguousarray(pos, np.float32)),
-                                           _ptr(np.ascontiguousarray(freq, np.float32)), int(capon), G,
-                                           levels, fov_l, fov_m, subarray, lam, load, K, l0, m0, _ptr(out)))
-    return out
+                                      _ptr(np.ascontiguousarray(pos, np.float32)),
+                                      _ptr(np.ascontiguousarray(freq, np.float32)), int(capon), G,
+                                      levels, fov_l, fov_m, subarray, lam, load, K, l0, m0, _ptr(out),
+                                      _ptr(inten)))
+    return (out, inten) if intensity else out
 
 
 def unpack(v: np.ndarray):

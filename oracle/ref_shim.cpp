@@ -223,11 +223,12 @@ int ref_make_moving_point_source(uint64_t T, uint64_t F, uint64_t A, const float
 }
 
 // CpuOptBeamTracker (include/beamformer/cpu_opt_beam_tracker.hpp:91-169):
-// run the DOA search over all windows and return each window's direction.
+// run the DOA search over all windows and return each window's direction
+// and, when intensity is given, the emitted [T][F] beam power.
 int ref_doa_directions(const uint8_t* v, uint64_t T, uint64_t F, uint64_t A, const float* pos,
                        const float* freq, int capon, uint64_t G, uint64_t levels, float fov_l,
                        float fov_m, uint64_t subarray, float lam, float load, uint64_t K, float l0,
-                       float m0, float* dirs) {
+                       float m0, float* dirs, float* intensity) {
     return guarded([&] {
         const Dimensions d = dims_of(T, F, A, 1);
         CpuOptTrackerConfig cfg;
@@ -247,6 +248,7 @@ int ref_doa_directions(const uint8_t* v, uint64_t T, uint64_t F, uint64_t A, con
         PackedVoltage pv(v, v + T * F * A);
         Intensities I(T * F);
         tracker.run_into(pv, I);
+        if (intensity != nullptr) std::memcpy(intensity, I.data(), I.size() * sizeof(float));
         const std::size_t W = tracker_window_count(T, K);
         for (std::size_t w = 0; w < W; ++w) {
             const Vec3 dd = tracker.window_direction(w);

@@ -186,3 +186,52 @@ def test_scan_element_counts_match_fp64_oracle(cuda, orc, M, jitter):
     eb, ec, el = orc.doa_scan(R, K, M, 0.9, 1e-3, pos[:M], kw, -0.6, 0.004, n)
     assert np.allclose(bart.cpu().numpy().reshape(B, n), eb, rtol=1e-6, atol=0.0)
     assert np.allclose(cap.cpu().numpy().reshape(B, n), ec, rtol=1e-6, atol=0.0)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("A,capon,subarray,G,levels", [(32, False, 16, 16, 2), (64, False, 8, 12, 1),
+                                                       (32, True, 8, 16, 2), (64, True, 8, 8, 0)])
+def test_adaptive_tracker_follows_reference_search(cuda, ref, orc, A, capon, subarray, G, levels):
+    """bf_doa_track against CpuOptBeamTracker::run_into on a drifting source:
+    each window's direction within two final half-pitches of the reference's
+    (the search compares FP64 powers where the reference compares FP32 ones,
+    so a near-tie can pick the neighbouring candidate) and almost always
+    within 1e-4; the emitted beam power equals the reference float32 chain
+    along the GPU's own directions bit for bit, and the reference's emission
+    wherever the directions agree to the last bit."""
+    from beamform_project_b200 import api, native
+    torch = cuda
+    F, K, W = 336, 256, 8
+    T = K * W
+    pos = ref.ref_default_positions(A)
+    freq = ref.ref_channelized_frequencies(F)
+    l0, m0 = 0.06, -0.03
+    v = ref.ref_make_moving_point_source(T, F, A, pos, freq, l0, m0, 1e-5, 5e-6, 3.0)
+    fov = 0.15
+    lam = 0.9
+    ref_dirs, ref_I = ref.ref_doa_directions(v, pos, freq, K, capon=capon, G=G, levels=levels, fov_l=fov,
+                                             fov_m=fov, subarray=subarray, lam=lam, load=1e-3, l0=0.0, m0=0.0,
+                                             intensity=True)
+    d = api.Dimensions(T, F, A, 1)
+    cfg = api.doa_track_config(K, subarray=subarray, capon=capon, grid=G, levels=levels, fov_l=fov, fov_m=fov,
+                               forgetting=lam, diag_load=1e-3)
+    ws = torch.empty(api.doa_track_workspace_bytes(d, cfg), dtype=torch.uint8, device="cuda")
+    dirs = torch.zeros(W * 3, dtype=torch.float32, device="cuda")
+    inten = torch.zeros(T * F, dtype=torch.float32, device="cuda")
+    api.doa_track(None, torch.from_numpy(v).cuda(), torch.from_numpy(pos).cuda(),
+                  torch.from_numpy(api.wave_numbers(freq)).cuda(), d, cfg, dirs, inten, ws)
+    torch.cuda.synchronize()
+    assert native.take_device_error() == 0
+    got = dirs.cpu().numpy().reshape(W, 3)
+    half = fov / G / (2 ** levels) if levels else 2 * fov / (G - 1)
+    dl = np.abs(got[:, :2] - ref_dirs[:, :2])
+    print(f"A={A} capon={capon} M={subarray} G={G} L={levels}: max |dir - reference| {dl.max():.2e} "
+          f"(half-pitch {half:.2e}); median {np.median(dl):.2e}")
+    assert dl.max() <= 2 * half
+    assert np.median(dl) <= 1e-4
+    got_I = inten.cpu().numpy().reshape(T, F)
+    mine = orc.tracker(v, orc.tracker_weights(got, pos, freq), T, F, A, K)
+    assert np.array_equal(got_I, mine)
+    same = np.all(got == ref_dirs, axis=1)
+    for w in np.nonzero(same)[0]:
+        assert np.array_equal(got_I[w * K:(w + 1) * K], ref_I[w * K:(w + 1) * K])

@@ -157,3 +157,19 @@ def test_host_buffer_checks_without_gpu():
         api._host(np.zeros(64, np.float32), "v", np.uint8, 1)
     with pytest.raises(api.InvalidArgument, match="contiguous"):
         api._host(np.zeros((8, 8), np.uint8)[:, ::2], "v", np.uint8, 1)
+
+
+def test_doa_track_validates_before_any_cuda_call():
+    from beamform_project_b200 import api
+    d = api.Dimensions(1024, 336, 32, 1)
+    fn = native.lib().bf_doa_track
+    for cfg, msg in ((api.doa_track_config(100, subarray=8), "multiple of 128"),
+                     (api.doa_track_config(256, subarray=8, grid=1), "grid must be"),
+                     (api.doa_track_config(256), "at most 16"),
+                     (api.doa_track_config(256, capon=True, subarray=20), "at most 16"),
+                     (api.doa_track_config(256, subarray=8, forgetting=0.0), "forgetting")):
+        st = fn(None, None, None, None, C.byref(d.c()), C.byref(cfg), None, None, None)
+        assert st != 0 and msg in native.last_error(), (msg, native.last_error())
+        assert api.doa_track_workspace_bytes(d, cfg) == 0
+    ok = api.doa_track_config(256, subarray=8)
+    assert api.doa_track_workspace_bytes(d, ok) > 1024 * 336 // 256 * 32 * 32 * 8
