@@ -1009,6 +1009,7 @@ ServedBeamformer::ServedBeamformer(const ServedConfig& c) {
     cfg.pool_seed = c.pool_seed;
     cfg.pool_scale = generator_scale(c.pool_sigma);
     cfg.window_budget_us = c.window_budget_us;
+    cfg.windows_per_step = c.windows_per_step;
     check(bf_serve_create(&cfg, &server_));
 }
 

@@ -339,8 +339,17 @@ bf_status validate_job(const bf_serve_config& c, const bf_serve_job* j) {
     return BF_OK;
 }
 
+// Windows job j serves in the coming step: up to windows_per_step, stopping
+// at its last window and at the end of the voltage pool (a span never wraps).
+uint64_t step_windows(const bf_serve_config& c, const Job& j) {
+    const uint64_t k = c.windows_per_step > 1 ? c.windows_per_step : 1;
+    const uint64_t win = c.window_spectra;
+    const uint64_t t0 = (j.spec.pool_offset + j.next_step * win) % c.pool_spectra;
+    return std::max<uint64_t>(1, std::min({k, j.n_steps - j.next_step, (c.pool_spectra - t0) / win}));
+}
+
 void fill_tables_entry(bf_server* s, const Job& j, uint8_t* hdr, long long* units, uint64_t step,
-                       int kind) {
+                       uint64_t n_wsteps, int kind) {
     const bf_serve_config& c = s->cfg;
     const uint64_t win = c.window_spectra, S = j.spec.integration_spectra;
     const uint64_t t0 = (j.spec.pool_offset + step * win) % c.pool_spectra;
@@ -355,7 +364,7 @@ void fill_tables_entry(bf_server* s, const Job& j, uint8_t* hdr, long long* unit
         e.n_beams = static_cast<int>(j.spec.n_beams);
         e.n_windows = static_cast<int>(j.n_windows);
         e.w0 = static_cast<int>(step * (win / S));
-        const long long n = tc_job_tiling(e, static_cast<int>(win), static_cast<int>(S),
+        const long long n = tc_job_tiling(e, static_cast<int>(win * n_wsteps), static_cast<int>(S),
                                           static_cast<int>(c.shard_channels), static_cast<int>(j.spec.n_shards));
         std::memcpy(entry, &e, sizeof(e));
         *units += n;
@@ -368,7 +377,7 @@ void fill_tables_entry(bf_server* s, const Job& j, uint8_t* hdr, long long* unit
         e.n_freq = static_cast<int>(c.shard_channels);
         e.n_beams = static_cast<int>(j.spec.n_beams);
         e.n_windows = static_cast<int>(j.n_windows);
-        e.n_win = static_cast<int>(win / S);
+        e.n_win = static_cast<int>(n_wsteps * (win / S));
         e.w0 = static_cast<int>(step * (win / S));
         e.ftiles = static_cast<int>((c.shard_channels + 15) / 16);
         e.btiles = static_cast<int>((j.spec.n_beams + 15) / 16);
@@ -387,7 +396,7 @@ void fill_tables_entry(bf_server* s, const Job& j, uint8_t* hdr, long long* unit
         e.n_src = static_cast<int>(j.spec.n_beams);
         e.spectra = static_cast<int>(S);
         e.w0 = static_cast<int>(step * (win / S));
-        e.n_win = static_cast<int>(win / S);
+        e.n_win = static_cast<int>(n_wsteps * (win / S));
         e.src_groups = (e.n_src + 7) / 8;
         e.fgroups = (e.n_freq + 7) / 8;
         std::memcpy(entry, &e, sizeof(e));
@@ -445,7 +454,8 @@ constexpr double kStepUs = 12.0;
 constexpr double kClassUs = 8.0;
 
 double job_cost_us(const bf_serve_config& c, const Job& j) {
-    const double win = c.window_spectra, S = static_cast<double>(j.spec.integration_spectra);
+    const double win = static_cast<double>(c.window_spectra) * static_cast<double>(step_windows(c, j));
+    const double S = static_cast<double>(j.spec.integration_spectra);
     const double ch = static_cast<double>(j.spec.n_shards) * c.shard_channels;
     if (j.spec.kind == BF_SERVE_GRID) {
         const double nk = (2.0 * j.cls.nb_pad) * (2.0 * j.spec.n_ant) / (256.0 * 128.0);
@@ -701,7 +711,7 @@ bf_status step(bf_server* s, uint32_t* n_live) {
         long long units = 0;
         for (uint64_t id : by_class[c.key]) {
             const Job& j = s->jobs.at(id);
-            fill_tables_entry(s, j, hdr, &units, j.next_step, c.key.kind);
+            fill_tables_entry(s, j, hdr, &units, j.next_step, step_windows(s->cfg, j), c.key.kind);
         }
         used = c.offset + sizeof(TableHeader) + by_class[c.key].size() * entry_bytes(c.key.kind);
     }
@@ -723,9 +733,11 @@ bf_status step(bf_server* s, uint32_t* n_live) {
         Job& j = s->jobs.at(id);
         const uint64_t win = s->cfg.window_spectra;
         const uint64_t ch = static_cast<uint64_t>(j.spec.n_shards) * s->cfg.shard_channels;
-        s->beam_samples += static_cast<double>(win) * static_cast<double>(ch) * j.spec.n_beams;
-        ++s->job_windows;
-        if (++j.next_step == j.n_steps) {
+        const uint64_t nw = step_windows(s->cfg, j);
+        s->beam_samples += static_cast<double>(win * nw) * static_cast<double>(ch) * j.spec.n_beams;
+        s->job_windows += nw;
+        j.next_step += nw;
+        if (j.next_step == j.n_steps) {
             j.state = BF_JOB_RUNNING;
             j.last_step = s->steps;
             s->running.push_back(id);
@@ -780,6 +792,7 @@ bf_status validate_config(const bf_serve_config& c) {
     if (c.max_jobs == 0 || c.max_jobs > 65536) return set_error(BF_ERR_INVALID_ARGUMENT, "max_jobs must be 1..65536");
     if (c.hbm_budget_bytes == 0) return set_error(BF_ERR_INVALID_ARGUMENT, "hbm_budget_bytes must be positive");
     if (!(c.window_budget_us >= 0.f)) return set_error(BF_ERR_INVALID_ARGUMENT, "window_budget_us must be >= 0");
+    if (c.windows_per_step > 256) return set_error(BF_ERR_INVALID_ARGUMENT, "windows_per_step must be at most 256");
     return BF_OK;
 }
 

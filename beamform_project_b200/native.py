@@ -69,7 +69,8 @@ class Dims(C.Structure):
 class ServeConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_uint64), ("max_jobs", C.c_uint32), ("window_spectra", C.c_uint32),
                 ("pool_spectra", C.c_uint64), ("shard_channels", C.c_uint32), ("max_shards", C.c_uint32),
-                ("pool_seed", C.c_uint64), ("pool_scale", C.c_float), ("window_budget_us", C.c_float)]
+                ("pool_seed", C.c_uint64), ("pool_scale", C.c_float), ("window_budget_us", C.c_float),
+                ("windows_per_step", C.c_uint32)]
 
 
 class ServeJob(C.Structure):

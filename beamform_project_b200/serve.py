@@ -69,11 +69,13 @@ class Server:
     def __init__(self, hbm_budget_bytes: int, max_jobs: int = 512, window_spectra: int = 320,
                  pool_spectra: int = 20480, shard_channels: int = 336, max_shards: int = 4,
                  pool_seed: int = 1, pool_sigma: float = 2.0, window_budget_us: float = 0.0,
-                 host_only: bool = False):
+                 host_only: bool = False, windows_per_step: int = 1):
         from .api import generator_scale
         self.config = native.ServeConfig(int(hbm_budget_bytes), int(max_jobs), int(window_spectra),
                                          int(pool_spectra), int(shard_channels), int(max_shards), int(pool_seed),
-                                         float(generator_scale(pool_sigma)), float(window_budget_us))
+                                         float(generator_scale(pool_sigma)), float(window_budget_us),
+                                         int(windows_per_step))
+        self.windows_per_step = max(1, int(windows_per_step))
         self.host_only = host_only
         self._h = C.c_void_p()
         fn = native.lib().bf_serve_create_host_only if host_only else native.lib().bf_serve_create
@@ -338,7 +340,8 @@ def run_stream(server: Server, jobs: list[JobSpec], window_spectra: int = 320, r
     completion queue) are handed to on_done(job_id) and released.  When
     nothing is live the loop waits for the GPU (queued jobs need the memory
     of finished ones) or jumps to the next arrival.  Returns counts."""
-    step_s = window_spectra * SPECTRUM_S
+    k = getattr(server, "windows_per_step", 1)
+    step_s = window_spectra * k * SPECTRUM_S
     order = sorted(range(len(jobs)), key=lambda i: jobs[i].arrival_s)
     i = 0
     step_idx = 0
@@ -354,7 +357,7 @@ def run_stream(server: Server, jobs: list[JobSpec], window_spectra: int = 320, r
         n_live = server.step()
         if n_live:
             steps_run += 1
-            step_windows.append(step_idx)
+            step_windows.append(step_idx * k)
         step_idx += 1
         if n_live == 0 or step_idx % 8 == 0:
             for jid in server.take_done():
@@ -372,19 +375,21 @@ def run_stream(server: Server, jobs: list[JobSpec], window_spectra: int = 320, r
                 step_idx = max(step_idx, int(math.ceil(jobs[order[i]].arrival_s / step_s)))
             else:
                 server.sync()
-    return {"steps": steps_run, "submitted": i, "step_windows": step_windows, "job_ids": ids}
+    return {"steps": steps_run, "submitted": i, "step_windows": step_windows, "job_ids": ids,
+            "windows_per_step": k}
 
 
-def realtime_replay(step_ms, step_windows, window_spectra: int = 320) -> dict:
-    """Replays the served steps against the stream clock.  Step k serves the
-    stream window step_windows[k], whose data is complete at
-    (step_windows[k] + 1) * window time; the GPU starts a step when its data
-    is complete and the previous step has finished, and takes step_ms[k]
-    (its measured device time).  Returns per-step ready and finish times (s)
-    and the real-time factor (stream seconds served / device seconds)."""
+def realtime_replay(step_ms, step_windows, window_spectra: int = 320, windows_per_step: int = 1) -> dict:
+    """Replays the served steps against the stream clock.  Step i serves the
+    stream windows from step_windows[i] on (windows_per_step of them), whose
+    data is complete at (step_windows[i] + windows_per_step) * window time;
+    the GPU starts a step when its data is complete and the previous step has
+    finished, and takes step_ms[i] (its measured device time).  Returns per-step
+    ready and finish times (s) and the real-time factor (stream seconds served /
+    device seconds)."""
     import numpy as np
     w_s = window_spectra * SPECTRUM_S
-    ready = (np.asarray(step_windows, np.float64) + 1.0) * w_s
+    ready = (np.asarray(step_windows, np.float64) + float(windows_per_step)) * w_s
     dur = np.asarray(step_ms, np.float64) / 1e3
     n = min(len(ready), len(dur))
     ready, dur = ready[:n], dur[:n]
@@ -393,7 +398,7 @@ def realtime_replay(step_ms, step_windows, window_spectra: int = 320) -> dict:
     for k in range(n):
         t = max(t, ready[k]) + dur[k]
         end[k] = t
-    span = (ready[-1] - ready[0] + w_s) if n else 0.0
+    span = (ready[-1] - ready[0] + windows_per_step * w_s) if n else 0.0
     return {"ready_s": ready, "end_s": end, "latency_s": end - ready,
             "realtime_factor": span / dur.sum() if n and dur.sum() > 0 else None,
             "stream_s": span, "device_s": float(dur.sum())}

@@ -1507,7 +1507,8 @@ def serve_latency(jobs, run, infos, step_ms, step_offset: int) -> dict:
     arrival, completion latency its last window's finish minus the end of its
     data."""
     from beamform_project_b200 import serve
-    rep = serve.realtime_replay(step_ms, run["step_windows"])
+    k = run.get("windows_per_step", 1)
+    rep = serve.realtime_replay(step_ms, run["step_windows"], windows_per_step=k)
     w_s = 320 * serve.SPECTRUM_S
     t0 = min(j.arrival_s for j in jobs)
     t1 = max(j.arrival_s + j.n_spectra * serve.SPECTRUM_S for j in jobs)
@@ -1519,7 +1520,7 @@ def serve_latency(jobs, run, infos, step_ms, step_offset: int) -> dict:
         a, b = info["admit_step"] - step_offset, info["last_step"] - step_offset
         if a < 0 or b >= len(rep["end_s"]):
             continue
-        waits.append(rep["ready_s"][a] - w_s - j.arrival_s)
+        waits.append(rep["ready_s"][a] - k * w_s - j.arrival_s)
         done_lat.append(rep["end_s"][b] - (j.arrival_s + j.n_spectra * serve.SPECTRUM_S))
     pct = lambda a, q: float(np.percentile(a, q)) if len(a) else None  # noqa: E731
     lat_ms = rep["latency_s"] * 1e3
@@ -1528,7 +1529,8 @@ def serve_latency(jobs, run, infos, step_ms, step_offset: int) -> dict:
             "replayed_window_latency_ms_p50": pct(lat_ms, 50), "replayed_window_latency_ms_p99": pct(lat_ms, 99),
             "admission_wait_s_p50": pct(waits, 50), "admission_wait_s_p99": pct(waits, 99),
             "completion_latency_s_p50": pct(done_lat, 50), "completion_latency_s_p99": pct(done_lat, 99),
-            "virtual_stream_s": len(run["step_windows"]) and (run["step_windows"][-1] + 1) * w_s}
+            "virtual_stream_s": len(run["step_windows"]) and (run["step_windows"][-1] + k) * w_s,
+            "windows_per_step": k}
 
 
 def run_serve(args, emit: bool = True):
@@ -1675,12 +1677,61 @@ def run_serve(args, emit: bool = True):
             "gpu_launches": int(st["kernel_launches"] - st0["kernel_launches"]),
             "clocks": clocks.summary(),
         }
+        if args.serve_throughput_k > 1:
+            line["serve"]["throughput_mode"] = serve_throughput_mode(args, jobs, budget, rank)
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = serve_cpu_baseline(jobs, budget_s=args.cpu_seconds)
         if emit:
             print(json.dumps(line), flush=True)
     reps.close()
     return line if rank == 0 else None
+
+
+def serve_throughput_mode(args, jobs, budget: int, rank: int) -> dict:
+    """The same stream with each step serving args.serve_throughput_k windows
+    per live job and admission by memory and slots only: each grid channel's
+    weights load once per k windows and a step's fixed costs spread over k
+    windows, at the price of latency (the setting for a server that has
+    fallen behind its stream)."""
+    import torch
+    from beamform_project_b200 import native, serve
+    k = args.serve_throughput_k
+    srv = serve.Server(budget, max_jobs=args.serve_max_jobs, pool_spectra=SERVE_POOL, pool_seed=SERVE_SEED + rank,
+                       pool_sigma=SERVE_SIGMA, window_budget_us=0.0, windows_per_step=k)
+    stream = torch.cuda.ExternalStream(srv.stream_handle())
+    seen, warm = set(), []
+    for j in jobs:
+        key = (j.kind, j.n_ant, j.n_beams, j.integration_spectra)
+        if key not in seen:
+            seen.add(key)
+            warm.append(serve.JobSpec(**{**j.__dict__, "n_spectra": 320 * k, "_keep": []}))
+    serve.run_stream(srv, warm)
+    srv.sync()
+    st0 = srv.stats()
+    n_warm = len(srv.step_times())
+    infos = {}
+
+    def record_info(jid):
+        infos[jid] = srv.job_info(jid)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    r = serve.run_stream(srv, jobs, on_done=record_info)
+    e1.record(stream)
+    srv.sync()
+    torch.cuda.synchronize()
+    el_ms = e0.elapsed_time(e1)
+    assert native.take_device_error() == 0
+    st = srv.stats()
+    times = srv.step_times()[n_warm:]
+    lat = serve_latency(jobs, r, infos, times, n_warm)
+    srv.close()
+    steps = st["steps"] - st0["steps"]
+    return {"windows_per_step": k, "value": (st["beam_samples"] - st0["beam_samples"]) / (el_ms / 1e3),
+            "unit": "beam-samples/s", "steps": steps, "step_ms_p50": float(np.percentile(times, 50)),
+            "step_ms_p99": float(np.percentile(times, 99)),
+            "mean_live_jobs": (st["job_windows"] - st0["job_windows"]) / max(1, steps) / k,
+            "arena_peak_gb": st["arena_bytes_peak"] / 1e9, **lat}
 
 
 
@@ -1760,6 +1811,8 @@ def main():
                     help="admission bound on the predicted device time of a window (0: memory only)")
     ap.add_argument("--serve-budget-gb", type=float, default=120.0)
     ap.add_argument("--serve-max-jobs", type=int, default=512)
+    ap.add_argument("--serve-throughput-k", type=int, default=8,
+                    help="serve: also run the stream with this many windows per step (0 or 1: skip)")
     args = ap.parse_args()
     if args.workload == "serve":
         run_serve(args)

@@ -31,6 +31,7 @@ struct ServedConfig {
     std::uint64_t pool_seed = 1;
     float pool_sigma = 2.0F;              // Gaussian-like int4 noise of the pools
     float window_budget_us = 0.0F;        // 0: admission by memory and slots only
+    std::uint32_t windows_per_step = 1;   // windows per job per step (throughput setting)
 };
 
 enum class ServedJobKind { Grid = 0, Tracker = 1 };

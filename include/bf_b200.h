@@ -529,6 +529,12 @@ typedef struct bf_serve_config {
      * within this many microseconds (a job that alone exceeds it is admitted
      * when nothing else is live).  0: HBM budget and slots only. */
     float window_budget_us;
+    /* Windows each step serves per live job (0 or 1: one).  More windows per
+     * step load each grid channel's weights once for all of them and spread
+     * the step's fixed costs, at the price of latency: a throughput setting
+     * for a server that has fallen behind its stream.  A job's windows in one
+     * step stop at its last window and at the end of the voltage pool. */
+    uint32_t windows_per_step;
 } bf_serve_config;
 
 typedef struct bf_serve_job {

@@ -267,3 +267,33 @@ def test_ingest_into_pool_is_what_jobs_read(cuda, orc):
     ref64 = orc.beamform_integrated(v, w.cpu().numpy().reshape(B, F, A, 2), T, F, A, B, S, f64=True)
     err = np.abs(integ[0].astype(np.float64) - ref64)
     assert np.all(err <= 1e-3 + 1e-5 * np.abs(ref64))
+
+
+def test_windows_per_step_products(cuda):
+    """Serving k windows per step: the S = 10 grid, the trackers and the int8
+    codes of S = 10 jobs equal one window per step bit for bit (their sums do
+    not depend on where a step starts); the S = 320 grid stays within the
+    split-precision bar of it (a window's tiles may start elsewhere); and a
+    job alone equals the job in a mix at the same k."""
+    specs = [_grid_job(A=64, ns=2, B=40, S=320, n_spectra=1280, offset=320 * 3),
+             _grid_job(A=32, ns=1, B=128, S=10, n_spectra=960, offset=320 * 5, seed=1),
+             _tracker_job(A=32, ns=3, n_src=5, S=10, n_spectra=960, offset=320 * 9),
+             _tracker_job(A=64, ns=1, n_src=9, S=320, n_spectra=1280, offset=0)]
+    with _server() as srv:
+        one = _run(srv, specs)
+    for k in (3, 4):
+        with serve.Server(4 * 10**9, max_jobs=32, pool_spectra=POOL, pool_seed=SEED, pool_sigma=SIGMA,
+                          windows_per_step=k) as srv:
+            many = _run(srv, specs)
+        with serve.Server(4 * 10**9, max_jobs=32, pool_spectra=POOL, pool_seed=SEED, pool_sigma=SIGMA,
+                          windows_per_step=k) as srv:
+            alone = _run(srv, [specs[0]])[0]
+        for a, b in zip(alone, many[0]):
+            assert np.array_equal(a, b)
+        g320 = many[0][0].astype(np.float64)
+        ref = one[0][0].astype(np.float64)
+        assert np.all(np.abs(g320 - ref) <= 1e-3 + 2e-5 * np.abs(ref))
+        for idx in (1, 2, 3):
+            for a, b in zip(one[idx], many[idx]):
+                if a is not None:
+                    assert np.array_equal(a, b), (k, idx)

@@ -282,3 +282,40 @@ def test_pool_hook_checks_arguments():
         assert native.lib().bf_serve_pool(None, 64, C.byref(ptr), None, None) == 1
         with pytest.raises(native.LogicError, match="host-only"):
             srv.pool(64)
+
+
+def test_windows_per_step_serve_several_windows_and_stop_at_the_pool_end():
+    """windows_per_step k: a job's windows go k at a time, the last step takes
+    what is left, and a span stops at the end of the voltage pool."""
+    with serve.Server(10**10, host_only=True, pool_spectra=320 * 8, windows_per_step=4) as s:
+        a = s.submit(_grid(n_spectra=320 * 10, offset=0))          # 4 + 4 + 2 windows
+        b = s.submit(_grid(n_spectra=320 * 6, offset=320 * 6))     # pool end after 2: 2 + 4
+        steps = 0
+        while s.step():
+            steps += 1
+        assert steps == 3
+        ia, ib = s.job_info(a), s.job_info(b)
+        assert ia["windows_launched"] == 10 and ia["admit_step"] == 0 and ia["last_step"] == 2
+        assert ib["windows_launched"] == 6 and ib["last_step"] == 1
+        st = s.stats()
+        assert st["job_windows"] == 16
+        assert sorted(s.take_done()) == sorted([a, b])
+
+
+def test_windows_per_step_is_validated():
+    with pytest.raises(native.InvalidArgument):
+        serve.Server(10**9, host_only=True, windows_per_step=257)
+
+
+def test_job_info_reports_steps():
+    with serve.Server(10**10, host_only=True) as s:
+        s.submit(_grid(n_spectra=640))
+        s.step()
+        j = s.submit(_tracker(n_spectra=960))
+        assert s.job_info(j)["admit_step"] is None and s.job_info(j)["submit_step"] == 1
+        while s.step():
+            pass
+        info = s.job_info(j)
+        assert info["admit_step"] == 1 and info["last_step"] == 3 and info["windows_launched"] == 3
+        with pytest.raises(native.OutOfRange):
+            s.job_info(999)
