@@ -35,11 +35,12 @@
 // split direct form: 2.35x less at S = 320.  The covariance is exact, so the
 // only rounding is in the fp16 split of V (2^-22) and fp32 sums.
 //
-// CTA (one per SM, 704 threads): warp 0 TMA producer (64-spectrum tiles of one
+// CTA (one per SM, 768 threads): warp 0 TMA producer (64-spectrum tiles of one
 // channel, 64 bytes per row; CTAs 2c and 2c + 1 walk the same windows of the
 // even and odd channel of a pair, so both halves of each 128-byte line are
-// read together), warp 1 MMA issuer and TMEM owner, warps 2-9 unpack, warps
-// 10-17 convert (two per TMEM lane quadrant), warps 18-21 form the beam sums.
+// read together), warp 1 MMA issuer and TMEM owner, warps 2-4, 6-8, 10 and 11
+// unpack, warps 12-19 convert (two per TMEM lane quadrant), warps 20-23 form
+// the beam sums.
 // TMEM: two 128-column E stages (Gram accumulator, then A operand) and two
 // 128-column Y stages.  Shared memory: the channel's V image (fp16 hi, fp16 lo in the
 // 128-byte-swizzled K-major layout, fp32 [beam][component]), voltage stages.
@@ -61,10 +62,18 @@ namespace {
 
 using namespace sm100;
 
-constexpr int kThreads = 704;
-constexpr int kUnpackFirst = 2, kUnpackWarps = 8;
-constexpr int kConvFirst = 10, kConvWarps = 8;
-constexpr int kDotFirst = 18, kDotWarps = 4;
+// Warp roles.  A warp runs on SM sub-partition (warp id % 4), and the MMA
+// issuer (warp 1) shares sub-partition 1 with every warp whose id is 1 mod 4:
+// the unpack warps, which have no TMEM lane constraint, avoid it (warps 5 and
+// 9 stay idle), so the issuer competes with three compute warps (one convert
+// pair member and one beam-sum warp per quadrant must sit there), not five.
+constexpr int kThreads = 768;
+constexpr int kUnpackWarps = 8;        // warps 2-4, 6-8, 10, 11
+constexpr int kConvFirst = 12, kConvWarps = 8;
+constexpr int kDotFirst = 20, kDotWarps = 4;
+__host__ __device__ constexpr bool unpack_warp(int w) { return w >= 2 && w < kConvFirst && w != 5 && w != 9; }
+// 0..7 over the unpack warps
+__host__ __device__ constexpr int unpack_slot(int w) { return w - 2 - (w > 5) - (w > 9); }
 constexpr int kRows = 64;                             // spectra per voltage tile
 constexpr int kRawStages = 8, kXStages = 6;
 constexpr uint32_t kRawBytes = kRows * 64;            // one channel, 64 antennas
@@ -331,9 +340,9 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
             tc_commit(mma_done);
             if (!mbar_wait(mma_done, 0, kWaitNs)) fail(10);
         }
-    } else if (warp < kConvFirst) {
+    } else if (unpack_warp(warp)) {
         // unpack: thread = (chunk c of 8 antennas, rows r0 and r0 + 32)
-        const int ut = threadIdx.x - 32 * kUnpackFirst;
+        const int ut = 32 * unpack_slot(warp) + lane;
         const int c = ut & 7, r0 = ut >> 3;
         int stage = 0, xst = 0;
         uint32_t phase = 0, xph = 0;
@@ -368,6 +377,8 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
                 if (++xst == kXStages) { xst = 0; xph ^= 1; }
             }
         }
+    } else if (warp < kConvFirst) {
+        // idle (sub-partition 1 is left to the MMA issuer)
     } else if (warp < kDotFirst) {
         // convert: E = (G +- G') / 256 -> fp16 hi + lo over the same TMEM columns
         const int q = warp & 3, half = (warp - kConvFirst) >> 2;
