@@ -396,9 +396,10 @@ def run_gpu(args):
         api.prepare_auto_weights(None, weights, auto_w, d, N_SHARDS)
         auto_ws = torch.zeros(max(256, api.grid_auto_workspace_bytes(d, S_INT, N_SHARDS)), dtype=torch.uint8,
                               device=dev)
-        t_tune = time.perf_counter()
-        tune = api.autotune_grid(None, d, S_INT, N_SHARDS)
-        tune["wall_s"] = round(time.perf_counter() - t_tune, 2)
+        if args.tune:
+            t_tune = time.perf_counter()
+            tune = api.autotune_grid(None, d, S_INT, N_SHARDS)
+            tune["wall_s"] = round(time.perf_counter() - t_tune, 2)
     torch.cuda.synchronize()
 
     main_events = []  # CUDA events around the dominant kernel of each timed step
@@ -1798,6 +1799,8 @@ def main():
     ap.add_argument("--plain-steps", type=int, default=2,
                     help="steps of the plain drop-in (reference-order) kernel timed beside the tensor path")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tune", type=int, default=1,
+                    help="grid --kernel auto: run the autotuner for the class first (0: the default choice)")
     ap.add_argument("--configs", type=int, default=1,
                     help="grid: also measure the plain-grid, tracker, DOA and served workloads as sub-records")
     ap.add_argument("--config-cpu-seconds", type=float, default=5.0,

@@ -1,13 +1,14 @@
 """GPU parity: the checked grid beamformer (bf_grid_auto_integrated).
 
-The covariance form's relative error on a value scales with its estimate
+The covariance form's relative error on a value grows with its estimate
 est = 2^-23 |v_b|^2 tr(E) / I (bf_grid_cov_estimate).  The checked form keeps
-covariance values whose estimate is at most 16 x 1e-5 and recomputes every
-other unit with the split-precision kernel, so:
+covariance values whose estimate is at most a calibrated limit and recomputes
+every other unit with the split-precision kernel, so:
 
-* calibration: on every data regime below the covariance form's error against
-  the FP64 oracle stays below est / 16 (values above 1; the 1e-3 absolute
-  floor covers the rest);
+* calibration: on every data regime below, every covariance-form value the
+  checked form keeps (estimate at most its limit) is within 1e-5 / 2 of the
+  FP64 oracle (values above 1; the 1e-3 absolute floor covers the rest), and
+  the error against the estimate is printed per estimate decade;
 * the checked form is within 1e-3 + 1e-5 |fp64| everywhere: noise, the
   full-band benchmark's steered grid over a point source (nothing recomputed)
   and random-phase beams over a strong source (every beam a sidelobe: units
@@ -26,7 +27,7 @@ from test_gpu_grid_cov import _c2_like
 
 pytestmark = pytest.mark.gpu
 F = 336
-EST_RATIO = 1.0 / 16.0   # the library's calibrated ratio of error to estimate
+EST_LIMIT = 1.6e-4   # the checked form keeps covariance values whose estimate is at most this
 
 
 def _cases(orc, ref):
@@ -57,9 +58,13 @@ def _to(torch, a):
 
 
 def test_estimate_bounds_the_covariance_form_error(cuda, orc, cases):
+    """Every covariance-form value whose estimate is at or below the checked
+    form's limit (the values it keeps) is within 1e-5 relative of FP64, with
+    a factor 2 to spare; the error against the estimate is printed per
+    estimate decade (the calibration record)."""
     from beamform_project_b200 import api, native
     torch = cuda
-    worst = 0.0
+    worst_kept = 0.0
     for name, v, w, T, A, B, S in cases:
         d = api.Dimensions(T, F, A, B)
         W = -(-T // S)
@@ -75,11 +80,18 @@ def test_estimate_bounds_the_covariance_form_error(cuda, orc, cases):
         e = est.cpu().numpy().astype(np.float64)
         big = np.abs(ref64) > 1
         rel = np.abs(g - ref64)[big] / np.abs(ref64)[big]
-        ratio = float(np.max(rel / e[big]))
-        worst = max(worst, ratio)
-        print(f"{name}: max rel error {float(rel.max()):.2e}, max estimate {float(e.max()):.2e}, "
-              f"max error / estimate {ratio:.4f}")
-    assert worst <= EST_RATIO, worst
+        eb = e[big]
+        kept = eb <= EST_LIMIT
+        worst_kept = max(worst_kept, float(rel[kept].max()) if kept.any() else 0.0)
+        table = []
+        for lo in 10.0 ** np.arange(-8, 0):
+            sel = (eb >= lo) & (eb < 10 * lo)
+            if sel.any():
+                table.append(f"[{lo:.0e},{10 * lo:.0e}): n={int(sel.sum())} max err {float(rel[sel].max()):.2e}")
+        print(f"{name}: max rel error {float(rel.max()):.2e}, max estimate {float(eb.max()):.2e}, "
+              f"kept {int(kept.sum())} of {kept.size}, max error kept {float(rel[kept].max()) if kept.any() else 0:.2e}")
+        print("    " + "; ".join(table))
+    assert worst_kept <= 0.5e-5, worst_kept
 
 
 def _auto(torch, api, v, w, T, A, B, S, shards=1, quant=True):
