@@ -5,7 +5,7 @@ tolerance): every integrated value within 1e-3 + 1e-5 |ref| of the
 reference float32 chain, and within 1e-5 relative of the FP64 sum; int8
 codes identical to the reference quantizer applied to the same integrated
 values, and at most 1 LSB from the codes of the reference float32 chain
-(the count of 1-LSB cases is reported).
+for at most 1e-3 of the codes (the count of 1-LSB cases is printed).
 """
 from __future__ import annotations
 
@@ -80,6 +80,8 @@ def test_tensor_grid_within_tolerance(cuda, orc, A, B, T, S):
     diff = np.abs(codes[0].astype(int) - rc.astype(int))
     assert diff.max() <= 1
     print(f"int8 codes differing by 1 LSB: {int((diff == 1).sum())} of {diff.size}")
+    # a code moves only where the two values straddle a rounding boundary
+    assert (diff == 1).mean() <= 1e-3
 
 
 def test_tensor_grid_two_shards_and_point_source(cuda, orc, ref):
