@@ -388,9 +388,9 @@ doa_scan_kernel(const Cd* __restrict S, const Cd* __restrict Q, const int* __res
 #pragma unroll
             for (int sft = 1; sft < M; ++sft) {
                 const double ph = static_cast<double>(sft) * psi;
-                const double q = rint(ph * kTwoOverPi);
-                const float2 w = trk::sincos_quadrant(__double2float_rn(__fma_rn(-kHalfPi, q, ph)),
-                                                      static_cast<int>(static_cast<long long>(q) & 3));
+                int qd;
+                const double q = trk::round_quadrant(ph * kTwoOverPi, qd);
+                const float2 w = trk::sincos_quadrant(__double2float_rn(__fma_rn(-kHalfPi, q, ph)), qd);
                 zc[sft] = static_cast<double>(w.x);
                 zs[sft] = static_cast<double>(w.y);
             }
@@ -425,9 +425,9 @@ doa_scan_kernel(const Cd* __restrict S, const Cd* __restrict Q, const int* __res
                 constexpr double kHalfPi = 1.5707963267948966192313216916398;
                 constexpr double kTwoOverPi = 0.63661977236758134307553505349006;
                 const double ph = k * (px[i] * lv + py[i] * m_fixed);
-                const double q = rint(ph * kTwoOverPi);
-                const float2 w = trk::sincos_quadrant(__double2float_rn(__fma_rn(-kHalfPi, q, ph)),
-                                                      static_cast<int>(static_cast<long long>(q) & 3));
+                int qd;
+                const double q = trk::round_quadrant(ph * kTwoOverPi, qd);
+                const float2 w = trk::sincos_quadrant(__double2float_rn(__fma_rn(-kHalfPi, q, ph)), qd);
                 a[i] = Cd{static_cast<double>(w.x), -static_cast<double>(w.y)};
                 mag[i] = a[i].re * a[i].re + a[i].im * a[i].im;
             }

@@ -83,8 +83,13 @@ constexpr uint32_t kVBytes = 128 * 128 * 4;           // [beam][component] fp32
 constexpr uint32_t kWImage = 2 * kWHalf + kVBytes;    // per channel
 constexpr uint32_t kYCol = 256;                       // TMEM columns of the two Y stages
 constexpr uint64_t kWaitNs = 2000000000ull;
-// mbarriers, TMEM address, fail flag, per-unit trace partials [4][4]
-constexpr uint32_t kBarBytes = (2 * kRawStages + 2 * kXStages + 15) * 8 + 8 + 64;
+// trace partials of unit j sit in slot j % kTrSlots until the beam sums of
+// unit j read them, after freeing Y of unit j; the converters reach unit
+// j + kTrSlots only after Y of unit j + kTrSlots - 4 was freed, so any ring of
+// at least five slots is safe
+constexpr int kTrSlots = 8;
+// mbarriers, TMEM address, fail flag, per-unit trace partials [kTrSlots][4]
+constexpr uint32_t kBarBytes = (2 * kRawStages + 2 * kXStages + 11 + kTrSlots) * 8 + 8 + kTrSlots * 16;
 constexpr uint32_t kSmemBytes = kWImage + kXStages * kXBytes + kRawStages * kRawBytes + 2 * 4 * 128 * 4 + 512 + 1024;
 static_assert(kBarBytes <= 512, "barrier block");
 static_assert(kSmemBytes <= 232448, "shared memory per CTA");
@@ -181,10 +186,10 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
     uint64_t* w_full = y_free + 2;
     uint64_t* w_empty = w_full + 1;
     uint64_t* mma_done = w_empty + 1;
-    uint64_t* tr_ready = mma_done + 1;           // [4] trace partials of unit j in slot j % 4
-    uint32_t* tmem_ptr = reinterpret_cast<uint32_t*>(tr_ready + 4);
+    uint64_t* tr_ready = mma_done + 1;           // [kTrSlots] trace partials of unit j in slot j % kTrSlots
+    uint32_t* tmem_ptr = reinterpret_cast<uint32_t*>(tr_ready + kTrSlots);
     volatile int* s_fail = reinterpret_cast<volatile int*>(tmem_ptr + 1);
-    float* s_trq = reinterpret_cast<float*>(tmem_ptr + 2);  // [4 slots][4 quadrants]
+    float* s_trq = reinterpret_cast<float*>(tmem_ptr + 2);  // [kTrSlots][4 quadrants]
     const bool estimate = p.est != nullptr || p.est_limit > 0.f;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -206,7 +211,7 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
         mbar_init(w_full, 1);
         mbar_init(w_empty, 1 + kDotWarps);
         mbar_init(mma_done, 1);
-        for (int i = 0; i < 4; ++i) mbar_init(&tr_ready[i], 4);
+        for (int i = 0; i < kTrSlots; ++i) mbar_init(&tr_ready[i], 4);
         *s_fail = 0;
         fence_mbar_init();
     }
@@ -427,13 +432,12 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
             __syncwarp();
             if (lane == 0) mbar_arrive(&conv_done[eb]);
             if (has_diag) {
-                // read by the beam sums of unit j before they free Y of unit j, which
-                // comes before the Gram (and so the conversion) of unit j + 4
+                // slot j % kTrSlots (the ring's bound is at its definition)
 #pragma unroll
                 for (int o = 16; o >= 1; o >>= 1) diag += __shfl_xor_sync(0xffffffffu, diag, o);
                 if (lane == 0) {
-                    s_trq[(j & 3) * 4 + q] = diag;
-                    mbar_arrive(&tr_ready[j & 3]);
+                    s_trq[(j % kTrSlots) * 4 + q] = diag;
+                    mbar_arrive(&tr_ready[j % kTrSlots]);
                 }
             }
             if (*s_fail) break;
@@ -453,21 +457,15 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
             const int eb = static_cast<int>(j & 1);
             if (!mbar_wait(&quad_done[eb], static_cast<uint32_t>((j >> 1) & 1), kWaitNs)) { fail(14); break; }
             tc_fence_after();
-            float tr = 0.f;
-            if (estimate) {
-                if (pu == u_begin || cur.w == 0) {
-                    // the channel's image is in place until this run's last unit
-                    float acc = 0.f;
+            if (estimate && (pu == u_begin || cur.w == 0)) {
+                // the channel's image is in place until this run's last unit
+                float acc = 0.f;
 #pragma unroll 8
-                    for (int i = 0; i < 128; ++i) {
-                        const float v = vt[t * 128 + ((i + lane) & 127)];
-                        acc = fmaf(v, v, acc);
-                    }
-                    vnorm = acc;
+                for (int i = 0; i < 128; ++i) {
+                    const float v = vt[t * 128 + ((i + lane) & 127)];
+                    acc = fmaf(v, v, acc);
                 }
-                if (!mbar_wait(&tr_ready[j & 3], static_cast<uint32_t>((j >> 2) & 1), kWaitNs)) { fail(15); break; }
-                const float* tq = s_trq + (j & 3) * 4;
-                tr = ((tq[0] + tq[1]) + tq[2]) + tq[3];
+                vnorm = acc;
             }
             float part[4];
 #pragma unroll 1
@@ -487,6 +485,17 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
             }
             __syncwarp();
             if (last && lane == 0) mbar_arrive(w_empty);
+            // tr(E) of this unit, formed by the converters before its Y existed: read
+            // here, off the path from the Y hand-off to the TMEM loads
+            float tr = 0.f;
+            if (estimate) {
+                if (!mbar_wait(&tr_ready[j % kTrSlots], static_cast<uint32_t>((j / kTrSlots) & 1), kWaitNs)) {
+                    fail(15);
+                    break;
+                }
+                const float* tq = s_trq + (j % kTrSlots) * 4;
+                tr = ((tq[0] + tq[1]) + tq[2]) + tq[3];
+            }
             float* sd = s_dot + (j & 1) * 512;
 #pragma unroll
             for (int cb = 0; cb < 4; ++cb) sd[q * 128 + 32 * cb + lane] = part[cb];
@@ -496,10 +505,11 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
                 ((static_cast<size_t>(cur.s) * p.n_windows + cur.w) * p.n_freq + 2 * cur.fp + odd) * p.n_beams + t;
             if (t < p.n_beams) p.out[oidx] = sum * p.out_scale;
             if (estimate) {
-                const float est = sum > 0.f ? kEstScale * vnorm * tr / sum : INFINITY;
-                if (p.est != nullptr && t < p.n_beams) p.est[oidx] = est;
+                const float bound = kEstScale * tr * vnorm;  // est = bound / sum
+                if (p.est != nullptr && t < p.n_beams) p.est[oidx] = sum > 0.f ? bound / sum : INFINITY;
                 if (p.est_limit > 0.f) {
-                    const bool over = t < p.n_beams && !(est <= p.est_limit);
+                    // est <= limit without the division (a non-positive or NaN sum is over)
+                    const bool over = t < p.n_beams && !(sum > 0.f && bound <= p.est_limit * sum);
                     if (__any_sync(0xffffffffu, over) && lane == 0) {
                         const int f = 2 * cur.fp + odd;
                         const int unit = (cur.s * p.n_freq + f) * p.split_gpc + cur.w / p.split_gw;

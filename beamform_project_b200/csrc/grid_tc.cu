@@ -392,6 +392,9 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
     volatile int* s_fail = reinterpret_cast<volatile int*>(bars + 19);
     volatile int* s_quant = reinterpret_cast<volatile int*>(bars + 20);  // [8] windows to quantize
     volatile int* s_meta = reinterpret_cast<volatile int*>(bars + 24);   // [2] their shard, channel group
+    // A list launch with an empty list (the checked form's common case) ends
+    // before any set-up; every thread reads the same count.
+    if (!kServed && p.unit_list != nullptr && *p.unit_count == 0) return;
     Pending pend, recorded;                                               // epilogue thread 0 only
     pend.mask = 0;
     recorded.mask = 0;

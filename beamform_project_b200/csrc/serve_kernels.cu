@@ -176,11 +176,16 @@ served_tracker_kernel(const uint8_t* __restrict__ pool, long long row_stride, co
                         for (int c = 0; c < A / 32; ++c) {
                             const int a = lane + 32 * c;
                             const float2 wv = steering_from_delay(k, s_delay[sl0 + e][a]);
+                            // the parts split_part forms, two per packed conversion
+                            const __half2 hi = __floats2half2_rn(wv.x, wv.y);
+                            const float2 hf = __half22float2(hi);
+                            const uint32_t hw = h2_bits(hi);
+                            const uint32_t lw = h2_bits(__floats2half2_rn(__fsub_rn(wv.x, hf.x), __fsub_rn(wv.y, hf.y)));
                             const int h = Frag::half(a);
-                            rows[2 * Frag::word(e * 4 + 0, a) + h] = split_part(wv.x, false);
-                            rows[2 * Frag::word(e * 4 + 1, a) + h] = split_part(wv.y, false);
-                            rows[2 * Frag::word(e * 4 + 2, a) + h] = split_part(wv.x, true);
-                            rows[2 * Frag::word(e * 4 + 3, a) + h] = split_part(wv.y, true);
+                            rows[2 * Frag::word(e * 4 + 0, a) + h] = static_cast<uint16_t>(hw);
+                            rows[2 * Frag::word(e * 4 + 1, a) + h] = static_cast<uint16_t>(hw >> 16);
+                            rows[2 * Frag::word(e * 4 + 2, a) + h] = static_cast<uint16_t>(lw);
+                            rows[2 * Frag::word(e * 4 + 3, a) + h] = static_cast<uint16_t>(lw >> 16);
                         }
                     }
                 }

@@ -80,13 +80,30 @@ __device__ __forceinline__ double steering_delay(const float* pos, int a, double
                                __dmul_rn(static_cast<double>(pos[3 * a + 1]), dy)),
                      __dmul_rn(static_cast<double>(pos[3 * a + 2]), dz));
 }
+// n = rint(x) and n mod 4.  Below 2^51 in magnitude, x + 1.5 * 2^52 lands
+// where the ulp is 1, so the addition rounds x to an integer exactly as rint
+// does (to nearest, ties to even) and the low bits of the sum hold n mod 4
+// (1.5 * 2^52 is a multiple of 4): two additions instead of a rounding and a
+// 64-bit conversion.  Larger |x| takes rint.
+__device__ __forceinline__ double round_quadrant(double x, int& quad) {
+    constexpr double kShift = 6755399441055744.0;  // 1.5 * 2^52
+    if (fabs(x) < 0x1p51) {
+        const double s = __dadd_rn(x, kShift);
+        quad = __double2loint(s) & 3;
+        return __dsub_rn(s, kShift);
+    }
+    const double n = rint(x);
+    quad = static_cast<int>(static_cast<long long>(n) & 3);
+    return n;
+}
 __device__ __forceinline__ float2 steering_from_delay(double k, double delay) {
     constexpr double kHalfPi = 1.5707963267948966192313216916398;
     constexpr double kTwoOverPi = 0.63661977236758134307553505349006;
     const double phase = __dmul_rn(k, delay);
-    const double n = rint(__dmul_rn(phase, kTwoOverPi));
+    int quad;
+    const double n = round_quadrant(__dmul_rn(phase, kTwoOverPi), quad);
     const float r = __double2float_rn(__fma_rn(-kHalfPi, n, phase));
-    return sincos_quadrant(r, static_cast<int>(static_cast<long long>(n) & 3));
+    return sincos_quadrant(r, quad);
 }
 __device__ __forceinline__ float2 steering_weight(const float* pos, int a, double k, double dx,
                                                   double dy, double dz) {
