@@ -81,14 +81,28 @@ __device__ __forceinline__ int find_job(const long long* begins, int stride_ll, 
 template <int A>
 struct TrackerFrag {
     static constexpr int kWords = A / 2;  // 32-bit words per part row
-    // word of part row r holding antennas (a, a + 2), a % 4 in {0, 1}
+    static constexpr int kBytes = A / 4;  // antennas per k-pair quad (lane q)
+    // 16-byte chunk swizzle of row r: the eight rows one ldmatrix reads at
+    // the same chunk fall on eight different bank groups
+    __device__ static int swz(int r) { return A == 64 ? (r & 7) : ((r >> 1) & 3); }
+    // word of part row r holding antennas (a, a + 2), a % 4 in {0, 1}:
+    // a = q kBytes + 4 jj + 2 h + s lies in chunk 2 jj + s, word q, half h,
+    // so one B fragment register of all four quads is one 16-byte chunk
     __device__ static int word(int r, int a) {
-        const int pw = ((a >> 2) << 1) | (a & 1);
-        const int swz = A == 64 ? (r & 7) : ((r >> 1) & 3);
-        return r * kWords + (pw ^ swz);
+        const int chunk = (((a % kBytes) >> 2) << 1) | (a & 1);
+        return r * kWords + 4 * (chunk ^ swz(r)) + a / kBytes;
     }
     __device__ static int half(int a) { return (a >> 1) & 1; }
 };
+
+// Four 8x8 b16 matrices from shared memory; lane L gives the address of row
+// L % 8 of matrix L / 8, and thread t receives word t % 4 of row t / 4.
+__device__ __forceinline__ void ldsm_x4(uint32_t addr, uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+                 : "r"(addr)
+                 : "memory");
+}
 
 template <int A, bool kShort>
 __global__ void __launch_bounds__(256, kShort ? 4 : 2)
@@ -98,31 +112,56 @@ served_tracker_kernel(const uint8_t* __restrict__ pool, long long row_stride, co
     using Frag = TrackerFrag<A>;
     constexpr int kWarpWords = 8 * 4 * Frag::kWords;  // 8 sources x 4 parts
     __shared__ double s_delay[8][A];
-    __shared__ uint32_t s_frag[8][kWarpWords];
+    __shared__ __align__(16) uint32_t s_frag[8][kWarpWords];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, q = lane & 3;
     const TrJob* jobs = reinterpret_cast<const TrJob*>(table + 1);
     const long long n_units = table->n_units;
     const int n_jobs = table->n_jobs;
     uint32_t* frag = s_frag[warp];
-    // fragment column g: part (g & 3) of source 2 nt + (g >> 2); the xi word
-    // takes the other component, negated for the real columns
-    const int part_r = g & 3, part_i = (g & 3) ^ 1;
+    // fragment column g of tile nt: part row 8 nt + g (part g & 3 of source
+    // 2 nt + (g >> 2)); the xi word takes the other component (row
+    // 8 nt + (g ^ 1)), negated for the real columns.  One ldmatrix per
+    // (nt, jj) loads (xr, xi) for s = 0 and s = 1: lane L addresses row
+    // L % 8 of matrix L / 8 = (s, re / im).  Columns of sources a unit does
+    // not have read stale rows; their sums are never stored.
     const uint32_t neg_i = (g & 1) != 0 ? 0u : 0x80008000u;
-    auto frag_pair = [&](int nt, int jj, int s, bool used, uint32_t& xr, uint32_t& xi) {
-        const int sl = 2 * nt + (g >> 2);
-        const int a0 = q * kBytes + 4 * jj + s;
-        xr = used ? frag[Frag::word(sl * 4 + part_r, a0)] : 0u;
-        xi = used ? frag[Frag::word(sl * 4 + part_i, a0)] ^ neg_i : 0u;
+    const int lrow = (lane & 8) != 0 ? ((lane & 7) ^ 1) : (lane & 7);
+    const int ls = lane >> 4;
+    const uint32_t frag_sa = static_cast<uint32_t>(__cvta_generic_to_shared(frag)) + 4u * lrow * Frag::kWords;
+    const int lsw = Frag::swz(lrow);  // swz(8 nt + lrow) for every nt
+    auto frag_load = [&](int nt, int jj, uint32_t& b0r, uint32_t& b0i, uint32_t& b1r, uint32_t& b1i) {
+        ldsm_x4(frag_sa + 4u * (8 * nt * Frag::kWords + 4 * (((2 * jj) | ls) ^ lsw)), b0r, b0i, b1r, b1i);
+        b0i ^= neg_i;
+        b1i ^= neg_i;
     };
-    for (long long u = blockIdx.x; u < n_units; u += gridDim.x) {
-        const int j = find_job(&jobs[0].unit_begin, sizeof(TrJob) / sizeof(long long), n_jobs, u);
+    // A CTA takes a contiguous range of units and walks it with a cursor
+    // (source group, then channel group, then window, then job): one job
+    // search and two 32-bit divisions per CTA instead of per unit.
+    const long long u_begin = n_units * blockIdx.x / gridDim.x;
+    const long long u_end = n_units * (blockIdx.x + 1) / gridDim.x;
+    int j = 0, sg = 0, fg = 0, w = 0;
+    auto seek = [&](long long u) {
+        j = find_job(&jobs[0].unit_begin, sizeof(TrJob) / sizeof(long long), n_jobs, u);
+        const unsigned local = static_cast<unsigned>(u - jobs[j].unit_begin);  // units of one job fit 32 bits
+        const unsigned sgn = static_cast<unsigned>(jobs[j].src_groups), fgn = static_cast<unsigned>(jobs[j].fgroups);
+        const unsigned rest = local / sgn, wq = rest / fgn;
+        sg = static_cast<int>(local - rest * sgn);
+        fg = static_cast<int>(rest - wq * fgn);
+        w = static_cast<int>(wq);
+    };
+    if (u_begin < u_end) seek(u_begin);
+    for (long long u = u_begin; u < u_end; ++u) {
+        if (u > u_begin) {
+            if (++sg == jobs[j].src_groups) {
+                sg = 0;
+                if (++fg == jobs[j].fgroups) {
+                    fg = 0;
+                    if (++w == jobs[j].n_win) seek(u);  // the next job with units
+                }
+            }
+        }
         const TrJob& jb = jobs[j];
-        const long long local = u - jb.unit_begin;
-        const int sg = static_cast<int>(local % jb.src_groups);
-        const long long rest = local / jb.src_groups;
-        const int fg = static_cast<int>(rest % jb.fgroups);
-        const int w = static_cast<int>(rest / jb.fgroups);
         const int f = fg * 8 + warp;
         const bool fvalid = f < jb.n_freq;
         const int n_src = jb.n_src, S = jb.spectra;
@@ -199,11 +238,10 @@ served_tracker_kernel(const uint8_t* __restrict__ pool, long long row_stride, co
         if constexpr (!kShort) {
 #pragma unroll
             for (int nt = 0; nt < 4; ++nt) {
-                const bool used = fvalid && nt < n_tiles && 2 * nt + (g >> 2) < n_here;
 #pragma unroll
                 for (int jj = 0; jj < NW; ++jj) {
-#pragma unroll
-                    for (int s = 0; s < 2; ++s) frag_pair(nt, jj, s, used, bfrag[nt][jj][s][0], bfrag[nt][jj][s][1]);
+                    frag_load(nt, jj, bfrag[nt][jj][0][0], bfrag[nt][jj][0][1], bfrag[nt][jj][1][0],
+                              bfrag[nt][jj][1][1]);
                 }
             }
         }
@@ -224,10 +262,8 @@ served_tracker_kernel(const uint8_t* __restrict__ pool, long long row_stride, co
                 for (int nt = 0; nt < 4; ++nt) {
                     if (nt < n_tiles) {
                         if constexpr (kShort) {
-                            const bool used = fvalid && 2 * nt + (g >> 2) < n_here;
                             uint32_t b0r, b0i, b1r, b1i;
-                            frag_pair(nt, jj, 0, used, b0r, b0i);
-                            frag_pair(nt, jj, 1, used, b1r, b1i);
+                            frag_load(nt, jj, b0r, b0i, b1r, b1i);
                             mma_16816(d[nt], re02g, re02h, im02g, im02h, b0r, b0i);
                             mma_16816(d[nt], re13g, re13h, im13g, im13h, b1r, b1i);
                         } else {
@@ -286,13 +322,13 @@ __global__ void __launch_bounds__(256) served_quantize_kernel(const TableHeader*
          u += warps) {
         const int j = find_job(&jobs[0].unit_begin, sizeof(QJob) / sizeof(long long), n_jobs, u);
         const QJob& jb = jobs[j];
-        long long local = u - jb.unit_begin;
-        const int bt = static_cast<int>(local % jb.btiles);
-        local /= jb.btiles;
-        const int ft = static_cast<int>(local % jb.ftiles);
-        local /= jb.ftiles;
-        const int w = static_cast<int>(local % jb.n_win);
-        const int shard = static_cast<int>(local / jb.n_win);
+        unsigned local = static_cast<unsigned>(u - jb.unit_begin);  // chunks of one job fit 32 bits
+        const int bt = static_cast<int>(local % static_cast<unsigned>(jb.btiles));
+        local /= static_cast<unsigned>(jb.btiles);
+        const int ft = static_cast<int>(local % static_cast<unsigned>(jb.ftiles));
+        local /= static_cast<unsigned>(jb.ftiles);
+        const int w = static_cast<int>(local % static_cast<unsigned>(jb.n_win));
+        const int shard = static_cast<int>(local / static_cast<unsigned>(jb.n_win));
         const int win = jb.w0 + w;
         const size_t shard_off = static_cast<size_t>(shard) * jb.n_windows * jb.n_freq * jb.n_beams;
         const size_t pidx = ((static_cast<size_t>(shard) * jb.n_windows + win) * jb.ftiles + ft) * jb.btiles + bt;
