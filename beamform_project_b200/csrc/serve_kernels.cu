@@ -111,7 +111,7 @@ served_tracker_kernel(const uint8_t* __restrict__ pool, long long row_stride, co
     constexpr int kBytes = A / 4;       // bytes (antennas) per thread per spectrum
     using Frag = TrackerFrag<A>;
     constexpr int kWarpWords = 8 * 4 * Frag::kWords;  // 8 sources x 4 parts
-    __shared__ double s_delay[8][A];
+    __shared__ double s_delay[2][8][A];  // by unit parity
     __shared__ __align__(16) uint32_t s_frag[8][kWarpWords];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int g = lane >> 2, q = lane & 3;
@@ -194,11 +194,15 @@ served_tracker_kernel(const uint8_t* __restrict__ pool, long long row_stride, co
         uint32_t wg[NW], wg8[NW];
         load_rows(t_begin, wg, wg8);
 
-        __syncthreads();  // the previous unit is done with s_delay and s_frag
+        // One barrier per unit: the delays alternate between two buffers, and a
+        // warp writing this unit's buffer has passed the last unit's barrier,
+        // which every warp reaches only after forming its weights from this
+        // buffer two units ago.
+        const int db = static_cast<int>((u - u_begin) & 1);
         for (int i = threadIdx.x; i < n_here * A; i += blockDim.x) {
             const int sl = i / A, a = i % A;
             const float3 d = trajectory_direction(jb.traj + 4 * (8 * sg + sl), wglob * S);
-            s_delay[sl][a] = steering_delay(jb.pos, a, d.x, d.y, d.z);
+            s_delay[db][sl][a] = steering_delay(jb.pos, a, d.x, d.y, d.z);
         }
         __syncthreads();
         if (fvalid) {
@@ -214,7 +218,7 @@ served_tracker_kernel(const uint8_t* __restrict__ pool, long long row_stride, co
 #pragma unroll
                         for (int c = 0; c < A / 32; ++c) {
                             const int a = lane + 32 * c;
-                            const float2 wv = steering_from_delay(k, s_delay[sl0 + e][a]);
+                            const float2 wv = steering_from_delay(k, s_delay[db][sl0 + e][a]);
                             // the parts split_part forms, two per packed conversion
                             const __half2 hi = __floats2half2_rn(wv.x, wv.y);
                             const float2 hf = __half22float2(hi);
