@@ -175,8 +175,8 @@ BF_API bf_status bf_prepare_split_weights(void* stream, const float* weights, vo
     clear_error();
     BF_TRY(validate_dims(dims));
     if (n_shards == 0) return set_error(BF_ERR_INVALID_ARGUMENT, "n_shards must be positive");
-    if (dims->n_ant > 64) {
-        return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernel supports n_ant 32 or 64");
+    if (dims->n_ant > 128) {
+        return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernel supports n_ant 32, 64 or 128");
     }
     BF_TRY(check_ptr(weights, 8, "weights"));
     BF_TRY(check_ptr(split_weights, 16, "split_weights"));
@@ -198,8 +198,8 @@ BF_API bf_status bf_grid_tensor_integrated(void* stream, const uint8_t* packed_v
         return set_error(BF_ERR_UNSUPPORTED,
                          "the tensor-core kernel needs integration_spectra below 32 or a multiple of 32");
     }
-    if (dims->n_ant > 64) {
-        return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernel supports n_ant 32 or 64");
+    if (dims->n_ant > 128) {
+        return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernel supports n_ant 32, 64 or 128");
     }
     if ((codes == nullptr) != (params == nullptr)) {
         return set_error(BF_ERR_INVALID_ARGUMENT, "codes and params must both be given or both be null");
@@ -232,8 +232,8 @@ BF_API bf_status bf_grid_tensor_quantized(void* stream, const uint8_t* packed_vo
         return set_error(BF_ERR_UNSUPPORTED,
                          "the tensor-core kernel needs integration_spectra below 32 or a multiple of 32");
     }
-    if (dims->n_ant > 64) {
-        return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernel supports n_ant 32 or 64");
+    if (dims->n_ant > 128) {
+        return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernel supports n_ant 32, 64 or 128");
     }
     BF_TRY(check_ptr(packed_voltage, 16, "packed_voltage"));
     BF_TRY(check_ptr(split_weights, 16, "split_weights"));
@@ -302,7 +302,7 @@ BF_API bf_status bf_grid_cov_estimate(void* stream, const uint8_t* packed_voltag
 }
 
 BF_API uint64_t bf_auto_weight_bytes(const bf_dims* dims, uint64_t n_shards) {
-    if (dims == nullptr || validate_dims(dims) != BF_OK || dims->n_ant > 64) return 0;
+    if (dims == nullptr || validate_dims(dims) != BF_OK || dims->n_ant > 128) return 0;
     return auto_weight_bytes(*dims, n_shards);
 }
 
@@ -311,7 +311,7 @@ BF_API bf_status bf_prepare_auto_weights(void* stream, const float* weights, voi
     clear_error();
     BF_TRY(validate_dims(dims));
     if (n_shards == 0) return set_error(BF_ERR_INVALID_ARGUMENT, "n_shards must be positive");
-    if (dims->n_ant > 64) return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernels support n_ant 32 or 64");
+    if (dims->n_ant > 128) return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernels support n_ant 32, 64 or 128");
     BF_TRY(check_ptr(weights, 8, "weights"));
     BF_TRY(check_ptr(auto_weights, 16, "auto_weights"));
     return launch_prepare_auto(static_cast<cudaStream_t>(stream), weights, auto_weights, *dims, n_shards);
@@ -331,7 +331,7 @@ BF_API bf_status bf_grid_auto_integrated(void* stream, const uint8_t* packed_vol
     if (integration_spectra == 0) {
         return set_error(BF_ERR_INVALID_ARGUMENT, "integration_spectra must be positive");
     }
-    if (dims->n_ant > 64) return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernels support n_ant 32 or 64");
+    if (dims->n_ant > 128) return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernels support n_ant 32, 64 or 128");
     if (integration_spectra > 32 && integration_spectra % 32 != 0) {
         return set_error(BF_ERR_UNSUPPORTED,
                          "the tensor-core kernels need integration_spectra below 32 or a multiple of 32");

@@ -678,10 +678,10 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                 const int b0 = 16 * (c_begin + c) + j0, b1 = 16 * (c_begin + c) + j1;
                 const size_t row_base = static_cast<size_t>(un.shard) * jb.n_windows + jb.w0;
                 if (v0 && w0 * sw < jb.n_time && b0 < jb.n_beams) {
-                    jb.integrated[((row_base + w0) * jb.n_freq + un.f) * jb.n_beams + b0] = sum0;
+                    jb.integrated[((row_base + w0) * jb.n_freq + un.f) * jb.beam_stride + b0] = sum0;
                 }
                 if (v1 && w1 * sw < jb.n_time && b1 < jb.n_beams) {
-                    jb.integrated[((row_base + w1) * jb.n_freq + un.f) * jb.n_beams + b1] = sum1;
+                    jb.integrated[((row_base + w1) * jb.n_freq + un.f) * jb.beam_stride + b1] = sum1;
                 }
             }
             __syncwarp();
@@ -779,7 +779,7 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                                 s[b] = s[NB + b] = s[2 * NB + b] = s[3 * NB + b] = 0.f;
                                 if (b < jb.n_beams) {
                                     jb.integrated[((static_cast<size_t>(un.shard) * jb.n_windows + jb.w0 + w) *
-                                                       jb.n_freq + un.f) * jb.n_beams + b] = total;
+                                                       jb.n_freq + un.f) * jb.beam_stride + b] = total;
                                 }
                             }
                         }
@@ -837,8 +837,10 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
 // ------------------------------------------------------------------------
 // weight preparation: canonical complex64 -> split fp16 swizzled image
 // ------------------------------------------------------------------------
+// n_beams beams from b0 of canonical weights holding b_total beams per shard.
 __global__ void prepare_split_kernel(const float2* __restrict__ w, uint8_t* __restrict__ out,
-                                     int n_freq, int n_ant, int n_beams, int nb_pad, int n_shards) {
+                                     int n_freq, int n_ant, int n_beams, int nb_pad, int n_shards, int b0,
+                                     int b_total) {
     const int K = 2 * n_ant, N = 2 * nb_pad;
     const long long per_channel = static_cast<long long>(N) * K;
     const long long total = per_channel * n_freq * n_shards;
@@ -858,7 +860,7 @@ __global__ void prepare_split_kernel(const float2* __restrict__ w, uint8_t* __re
         const int b = n >> 1, out_im = n & 1;
         float coef = 0.f;
         if (b < n_beams) {
-            const float2 wv = w[((static_cast<size_t>(shard) * n_beams + b) * n_freq + f) * n_ant + a];
+            const float2 wv = w[((static_cast<size_t>(shard) * b_total + b0 + b) * n_freq + f) * n_ant + a];
             // re out: x_re*wr - x_im*wi ; im out: x_re*wi + x_im*wr
             coef = out_im ? (comp ? wv.x : wv.y) : (comp ? -wv.y : wv.x);
         }
@@ -895,6 +897,17 @@ EncodeTiledFn encode_fn() {
 }
 
 int padded_beams(uint64_t b) { return static_cast<int>((b + 15) / 16 * 16); }
+
+// At 128 antennas one channel's hi + lo weight image fits in shared memory
+// beside two voltage stages only for 16 beams (K = 256: 8 KB per 16 beams and
+// part, 64 KB per fp16 voltage stage), so the beams run in groups of 16: one
+// launch per group over the same voltage, each writing its 16 columns of the
+// integrated rows.  The operand holds the groups' images one after the other.
+constexpr int kGroupBeams = 16;
+bool beam_groups(uint64_t n_ant) { return n_ant == 128; }
+uint64_t group_image_bytes(const bf_dims& d, uint64_t n_shards) {
+    return n_shards * d.n_freq * 2ull * (2 * d.n_ant) * (2 * kGroupBeams) * 2ull;
+}
 
 template <int A, int NB, bool kServed>
 bf_status launch_tc(cudaStream_t stream, const CUtensorMap& map, const TcParams& p, int grid,
@@ -953,13 +966,29 @@ uint64_t split_weight_bytes(const bf_dims& d, uint64_t n_shards, int nb_pad) {
 
 bf_status launch_prepare_split(cudaStream_t stream, const float* w, void* split, const bf_dims& d,
                                uint64_t n_shards, int nb_pad) {
+    if (beam_groups(d.n_ant)) {
+        if (nb_pad > 0) return set_error(BF_ERR_UNSUPPORTED, "served jobs use 32 or 64 antennas");
+        const int n_groups = static_cast<int>((d.n_beams + kGroupBeams - 1) / kGroupBeams);
+        const long long total = static_cast<long long>(n_shards) * d.n_freq * 2 * kGroupBeams * 2 * d.n_ant;
+        const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, 148LL * 32));
+        for (int g = 0; g < n_groups; ++g) {
+            const int nb = static_cast<int>(std::min<uint64_t>(kGroupBeams, d.n_beams - g * kGroupBeams));
+            prepare_split_kernel<<<blocks, 256, 0, stream>>>(
+                reinterpret_cast<const float2*>(w), static_cast<uint8_t*>(split) + g * group_image_bytes(d, n_shards),
+                static_cast<int>(d.n_freq), static_cast<int>(d.n_ant), nb, kGroupBeams, static_cast<int>(n_shards),
+                g * kGroupBeams, static_cast<int>(d.n_beams));
+            BF_RETURN_IF(cuda_status(cudaGetLastError(), "prepare_split_kernel launch"));
+        }
+        return BF_OK;
+    }
     const int nbp = nb_pad > 0 ? nb_pad : padded_beams(d.n_beams);
     const long long total = static_cast<long long>(n_shards) * d.n_freq * 2 * nbp * 2 * d.n_ant;
     const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, 148LL * 32));
     prepare_split_kernel<<<blocks, 256, 0, stream>>>(reinterpret_cast<const float2*>(w),
                                                      static_cast<uint8_t*>(split), static_cast<int>(d.n_freq),
                                                      static_cast<int>(d.n_ant), static_cast<int>(d.n_beams),
-                                                     nbp, static_cast<int>(n_shards));
+                                                     nbp, static_cast<int>(n_shards), 0,
+                                                     static_cast<int>(d.n_beams));
     return cuda_status(cudaGetLastError(), "prepare_split_kernel launch");
 }
 
@@ -1014,14 +1043,19 @@ bf_status launch_grid_tensor_impl(cudaStream_t stream, const uint8_t* v, const v
     if (d.n_time >= (1ull << 31) || n_shards > 1024 || spectra >= (1ull << 30)) {
         return set_error(BF_ERR_OVERFLOW, "CUDA tensor-core grid exceeds the supported size");
     }
-    if (d.n_ant != 32 && d.n_ant != 64) {
-        return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernel supports n_ant 32 or 64");
+    if (d.n_ant != 32 && d.n_ant != 64 && d.n_ant != 128) {
+        return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernel supports n_ant 32, 64 or 128");
+    }
+    const bool groups = beam_groups(d.n_ant);
+    if (groups && unit_list != nullptr) {
+        return set_error(BF_ERR_UNSUPPORTED, "unit lists cover 32 or 64 antennas");
     }
     const int S = static_cast<int>(spectra);
     TcParams p{};
     p.job.split = static_cast<const uint8_t*>(split);
     p.job.integrated = integrated;
     p.job.n_beams = static_cast<int>(d.n_beams);
+    p.job.beam_stride = static_cast<int>(d.n_beams);
     p.job.n_windows = static_cast<int>(window_count(d.n_time, spectra));
     p.job.w0 = 0;
     p.job.t0 = 0;
@@ -1037,8 +1071,9 @@ bf_status launch_grid_tensor_impl(cudaStream_t stream, const uint8_t* v, const v
     if (st != BF_OK) return st;
 
     // Fused quantization runs in the long-window epilogue; short windows
-    // quantize with the separate kernel.
-    const bool fused = codes != nullptr && counters != nullptr && S >= 32;
+    // and beam groups (a chunk is complete only after every group) quantize
+    // with the separate kernel.
+    const bool fused = codes != nullptr && counters != nullptr && S >= 32 && !groups;
     if (fused) {
         p.codes = codes;
         p.params = reinterpret_cast<float2*>(params);
@@ -1062,7 +1097,17 @@ bf_status launch_grid_tensor_impl(cudaStream_t stream, const uint8_t* v, const v
         p.paired = 0;
         grid = sms;
     }
-    if (grid > 0) {
+    if (grid > 0 && groups) {
+        const int n_groups = static_cast<int>((d.n_beams + kGroupBeams - 1) / kGroupBeams);
+        for (int g = 0; g < n_groups; ++g) {
+            TcParams pg = p;
+            pg.job.split = p.job.split + g * group_image_bytes(d, n_shards);
+            pg.job.integrated = integrated + g * kGroupBeams;
+            pg.job.n_beams = static_cast<int>(std::min<uint64_t>(kGroupBeams, d.n_beams - g * kGroupBeams));
+            pg.btiles = 1;
+            BF_RETURN_IF((launch_tc<128, kGroupBeams, false>(stream, map, pg, grid)));
+        }
+    } else if (grid > 0) {
         const int nbp = padded_beams(d.n_beams);
         st = d.n_ant == 32 ? dispatch_nb<32>(stream, map, p, nbp, grid) : dispatch_nb<64>(stream, map, p, nbp, grid);
         if (st != BF_OK) return st;

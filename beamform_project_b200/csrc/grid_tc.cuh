@@ -22,6 +22,7 @@ struct TcJob {
     int n_time;                 // spectra this launch covers
     int t0;                     // tensor-map row of the launch's first spectrum
     int n_freq, n_beams, spectra;
+    int beam_stride;            // beams per integrated row (n_beams, or all beam groups' beams)
     int n_windows;              // windows of the integrated array
     int w0;                     // integrated-array window of the launch's first window
     int rows_q;                 // R

@@ -362,6 +362,7 @@ void fill_tables_entry(bf_server* s, const Job& j, uint8_t* hdr, long long* unit
         e.unit_begin = *units;
         e.t0 = static_cast<int>(t0);
         e.n_beams = static_cast<int>(j.spec.n_beams);
+        e.beam_stride = e.n_beams;
         e.n_windows = static_cast<int>(j.n_windows);
         e.w0 = static_cast<int>(step * (win / S));
         const long long n = tc_job_tiling(e, static_cast<int>(win * n_wsteps), static_cast<int>(S),

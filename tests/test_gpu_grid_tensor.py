@@ -64,7 +64,10 @@ def _check(orc, got, v, w, T, A, B, S):
                                      (32, 128, 640, 320), (64, 1, 256, 128), (64, 100, 129, 96),
                                      # windows shorter than a 32-row lane quadrant
                                      (32, 16, 1024, 10), (64, 128, 331, 10), (64, 8, 200, 16),
-                                     (32, 33, 77, 1), (64, 64, 250, 3), (64, 40, 100, 20)])
+                                     (32, 33, 77, 1), (64, 64, 250, 3), (64, 40, 100, 20),
+                                     # 128 antennas: beam groups of 16
+                                     (128, 40, 256, 64), (128, 16, 320, 10), (128, 128, 160, 32),
+                                     (128, 1, 200, 128)])
 def test_tensor_grid_within_tolerance(cuda, orc, A, B, T, S):
     from beamform_project_b200 import api
     v = random_voltage(T, F, A, seed=A * B + T)
@@ -156,3 +159,41 @@ def test_tensor_grid_repeatable(cuda, orc):
     a, ca, _ = _run(cuda, api, v, w, T, A, B, S)
     b, cb, _ = _run(cuda, api, v, w, T, A, B, S)
     assert np.array_equal(a, b) and np.array_equal(ca, cb)
+
+
+def test_tensor_grid_128_antennas_every_entry(cuda, orc):
+    """At 128 antennas (beam groups of 16 over the same voltage) the fused
+    quantizing entry, the checked entry and two shards in one call give the
+    products of the plain entry bit for bit, within the bar of FP64."""
+    from beamform_project_b200 import api, native
+    torch = cuda
+    T, A, B, S, shards = 384, 128, 37, 64, 2
+    v = np.stack([random_voltage(T, F, A, seed=5), random_voltage(T, F, A, seed=6)])
+    w = np.stack([grid_weights(A, F, B, seed=7), grid_weights(A, F, B, seed=8)])
+    got, codes, params = _run(torch, api, v, w, T, A, B, S, shards=shards)
+    W = got.shape[1]
+    for s in range(shards):
+        _check(orc, got[s], v[s], w[s], T, A, B, S)
+    d = api.Dimensions(T, F, A, B)
+    vd = torch.from_numpy(v).cuda()
+    wd = torch.from_numpy(w).cuda()
+    split = torch.empty(api.split_weight_bytes(d, shards), dtype=torch.uint8, device="cuda")
+    api.prepare_split_weights(None, wd, split, d, shards)
+    integ = torch.empty(shards * W * F * B, dtype=torch.float32, device="cuda")
+    c2 = torch.empty(shards * W * F * B, dtype=torch.int8, device="cuda")
+    p2 = torch.empty(params.size, dtype=torch.float32, device="cuda")
+    ws = torch.zeros(max(256, api.grid_tensor_workspace_bytes(d, S, shards)), dtype=torch.uint8, device="cuda")
+    api.grid_tensor_quantized(None, vd, split, integ, c2, p2, ws, d, S, shards)
+    torch.cuda.synchronize()
+    assert native.take_device_error() == 0
+    assert np.array_equal(integ.cpu().numpy().reshape(got.shape), got)
+    assert np.array_equal(c2.cpu().numpy().reshape(codes.shape), codes)
+    assert np.array_equal(p2.cpu().numpy(), params)
+    aw = torch.empty(api.auto_weight_bytes(d, shards), dtype=torch.uint8, device="cuda")
+    api.prepare_auto_weights(None, wd, aw, d, shards)
+    integ.fill_(-1.0)
+    wsa = torch.zeros(max(256, api.grid_auto_workspace_bytes(d, S, shards)), dtype=torch.uint8, device="cuda")
+    api.grid_auto_integrated(None, vd, aw, integ, None, None, wsa, d, S, shards)
+    torch.cuda.synchronize()
+    assert native.take_device_error() == 0
+    assert np.array_equal(integ.cpu().numpy().reshape(got.shape), got)
