@@ -80,18 +80,17 @@ __device__ __forceinline__ int find_job(const long long* begins, int stride_ll, 
 // zero part, and the powers are sums of squares).
 template <int A>
 struct TrackerFrag {
-    static constexpr int kWords = A / 2;  // 32-bit words per part row
-    static constexpr int kBytes = A / 4;  // antennas per k-pair quad (lane q)
-    // 16-byte chunk swizzle of row r: the eight rows one ldmatrix reads at
-    // the same chunk fall on eight different bank groups
-    __device__ static int swz(int r) { return A == 64 ? (r & 7) : ((r >> 1) & 3); }
+    static constexpr int kWords = A / 2;         // 32-bit words of a part row
+    static constexpr int kRowWords = kWords + 4;  // row pitch: 16 bytes of padding
+    static constexpr int kBytes = A / 4;         // antennas per k-pair quad (lane q)
     // word of part row r holding antennas (a, a + 2), a % 4 in {0, 1}:
-    // a = q kBytes + 4 jj + 2 h + s lies in chunk 2 jj + s, word q, half h,
-    // so one B fragment register of all four quads is one 16-byte chunk
-    __device__ static int word(int r, int a) {
-        const int chunk = (((a % kBytes) >> 2) << 1) | (a & 1);
-        return r * kWords + 4 * (chunk ^ swz(r)) + a / kBytes;
-    }
+    // a = q kBytes + 4 jj + 2 h + s lies in 16-byte chunk 2 jj + s, word q,
+    // half h, so one B fragment register of all four quads is one chunk.  The
+    // padded pitch puts the same chunk of eight consecutive rows (what one
+    // ldmatrix reads) on eight different bank groups, and leaves every row
+    // offset a compile-time constant for the weight writer.
+    __device__ static int lane_word(int a) { return 4 * ((((a % kBytes) >> 2) << 1) | (a & 1)) + a / kBytes; }
+    __device__ static int word(int r, int a) { return r * kRowWords + lane_word(a); }
     __device__ static int half(int a) { return (a >> 1) & 1; }
 };
 
@@ -110,7 +109,7 @@ served_tracker_kernel(const uint8_t* __restrict__ pool, long long row_stride, co
     constexpr int NW = A / 16;          // 32-bit words per thread per spectrum
     constexpr int kBytes = A / 4;       // bytes (antennas) per thread per spectrum
     using Frag = TrackerFrag<A>;
-    constexpr int kWarpWords = 8 * 4 * Frag::kWords;  // 8 sources x 4 parts
+    constexpr int kWarpWords = 8 * 4 * Frag::kRowWords;  // 8 sources x 4 parts
     __shared__ double s_delay[2][8][A];  // by unit parity
     __shared__ __align__(16) uint32_t s_frag[8][kWarpWords];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -128,10 +127,10 @@ served_tracker_kernel(const uint8_t* __restrict__ pool, long long row_stride, co
     const uint32_t neg_i = (g & 1) != 0 ? 0u : 0x80008000u;
     const int lrow = (lane & 8) != 0 ? ((lane & 7) ^ 1) : (lane & 7);
     const int ls = lane >> 4;
-    const uint32_t frag_sa = static_cast<uint32_t>(__cvta_generic_to_shared(frag)) + 4u * lrow * Frag::kWords;
-    const int lsw = Frag::swz(lrow);  // swz(8 nt + lrow) for every nt
+    const uint32_t frag_sa =
+        static_cast<uint32_t>(__cvta_generic_to_shared(frag)) + 4u * (lrow * Frag::kRowWords + 4 * ls);
     auto frag_load = [&](int nt, int jj, uint32_t& b0r, uint32_t& b0i, uint32_t& b1r, uint32_t& b1i) {
-        ldsm_x4(frag_sa + 4u * (8 * nt * Frag::kWords + 4 * (((2 * jj) | ls) ^ lsw)), b0r, b0i, b1r, b1i);
+        ldsm_x4(frag_sa + 4u * (8 * nt * Frag::kRowWords + 8 * jj), b0r, b0i, b1r, b1i);
         b0i ^= neg_i;
         b1i ^= neg_i;
     };
@@ -206,29 +205,33 @@ served_tracker_kernel(const uint8_t* __restrict__ pool, long long row_stride, co
         }
         __syncthreads();
         if (fvalid) {
-            // lane owns antennas lane + 32 c; sources go in pairs so that
-            // every part row's swizzle is a compile-time constant
+            // lane owns antennas lane + 32 c (its 16-bit slot in every part row
+            // fixed); sources go in pairs, each row's offset a constant
             const double k = jb.kw[f];
+            uint16_t* slot[A / 32];
+#pragma unroll
+            for (int c = 0; c < A / 32; ++c) {
+                const int a = lane + 32 * c;
+                slot[c] = reinterpret_cast<uint16_t*>(frag) + 2 * Frag::lane_word(a) + Frag::half(a);
+            }
 #pragma unroll 1
             for (int sl0 = 0; sl0 < n_here; sl0 += 2) {
-                uint16_t* rows = reinterpret_cast<uint16_t*>(frag + sl0 * 4 * Frag::kWords);
 #pragma unroll
                 for (int e = 0; e < 2; ++e) {
                     if (sl0 + e < n_here) {
 #pragma unroll
                         for (int c = 0; c < A / 32; ++c) {
-                            const int a = lane + 32 * c;
-                            const float2 wv = steering_from_delay(k, s_delay[db][sl0 + e][a]);
+                            const float2 wv = steering_from_delay(k, s_delay[db][sl0 + e][lane + 32 * c]);
                             // the parts split_part forms, two per packed conversion
                             const __half2 hi = __floats2half2_rn(wv.x, wv.y);
                             const float2 hf = __half22float2(hi);
                             const uint32_t hw = h2_bits(hi);
                             const uint32_t lw = h2_bits(__floats2half2_rn(__fsub_rn(wv.x, hf.x), __fsub_rn(wv.y, hf.y)));
-                            const int h = Frag::half(a);
-                            rows[2 * Frag::word(e * 4 + 0, a) + h] = static_cast<uint16_t>(hw);
-                            rows[2 * Frag::word(e * 4 + 1, a) + h] = static_cast<uint16_t>(hw >> 16);
-                            rows[2 * Frag::word(e * 4 + 2, a) + h] = static_cast<uint16_t>(lw);
-                            rows[2 * Frag::word(e * 4 + 3, a) + h] = static_cast<uint16_t>(lw >> 16);
+                            uint16_t* r0 = slot[c] + 2 * (sl0 + e) * 4 * Frag::kRowWords;  // part rows 4 (sl0 + e) ..
+                            r0[0] = static_cast<uint16_t>(hw);
+                            r0[2 * Frag::kRowWords] = static_cast<uint16_t>(hw >> 16);
+                            r0[4 * Frag::kRowWords] = static_cast<uint16_t>(lw);
+                            r0[6 * Frag::kRowWords] = static_cast<uint16_t>(lw >> 16);
                         }
                     }
                 }
