@@ -327,7 +327,8 @@ __host__ __device__ constexpr Smem smem_plan(int n_ant, int n_beams_pad, bool se
     Smem s{};
     const uint32_t K = 2 * n_ant, N = 2 * n_beams_pad;
     s.w_bytes = (K / 64) * N * 128;
-    s.x_bytes = (K / 64) * kTileM * 128;
+    // at 128 antennas the fp16 voltage operand is written to TMEM instead
+    s.x_bytes = n_ant == 128 ? 0 : (K / 64) * kTileM * 128;
     s.raw_bytes = kTileM * n_ant;
     // window partial sums (S >= 32) or the per-warp power staging of short
     // windows ([8 warps][16 beams][32 spectra] floats), which share the space
@@ -357,7 +358,15 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
     constexpr int K = 2 * A;
     constexpr int N = 2 * NB;
     constexpr uint32_t ACC_COLS = N;          // fp32 columns per accumulator
-    constexpr uint32_t TMEM_COLS = (2 * N <= 32) ? 32 : (2 * N <= 64) ? 64 : (2 * N <= 128) ? 128
+    // At 128 antennas the fp16 voltage tile (128 rows x 256 K, 64 KB) lives in
+    // TMEM, two stages of 128 columns after the two accumulators: the unpack
+    // warps write it with tcgen05.st (a warp reaches one lane quadrant, so
+    // four unpack warps cover the 128 rows) and the MMAs read A from TMEM,
+    // which leaves the shared memory to the weight images of up to 64 beams.
+    constexpr bool kTmemA = A == 128;
+    constexpr uint32_t A_COL0 = 2 * ACC_COLS;
+    static_assert(!kTmemA || A_COL0 + 2 * (K / 2) <= 512, "TMEM holds two accumulators and two voltage stages");
+    constexpr uint32_t TMEM_COLS = kTmemA ? 512 : (2 * N <= 32) ? 32 : (2 * N <= 64) ? 64 : (2 * N <= 128) ? 128
                                    : (2 * N <= 256) ? 256 : 512;
     constexpr uint32_t IDESC = idesc_f16_f32(kTileM, N);
     constexpr Smem S = smem_plan(A, NB, kServed);
@@ -366,10 +375,13 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
     // The narrowest beam set (one 32-column load per quadrant) has little
     // epilogue work and is unpack-bound, so it trades four epilogue warps for
     // unpack warps (measured: at 32 beams the epilogue would then bind).
-    constexpr int kUnpackWarps = NB <= 16 ? 6 : 2;
-    constexpr int kEpiWarps = kThreads / 32 - 2 - kUnpackWarps;   // 4 or 8
+    // With the voltage in TMEM: warps 2 and 3 idle, unpack warps 4-7 (one
+    // per lane quadrant), epilogue warps 8-11.
+    constexpr int kUnpackWarps = kTmemA ? 4 : NB <= 16 ? 6 : 2;
+    constexpr int kUnpackFirst = kTmemA ? 4 : 2;
+    constexpr int kEpiWarps = kThreads / 32 - kUnpackFirst - kUnpackWarps;   // 4 or 8
     constexpr int kEpiThreads = 32 * kEpiWarps;
-    constexpr int kEpiFirstWarp = 2 + kUnpackWarps;
+    constexpr int kEpiFirstWarp = kUnpackFirst + kUnpackWarps;
     static_assert(kEpiWarps % 4 == 0 && kEpiFirstWarp % 4 == 0, "epilogue warps cover whole lane quadrants");
 
     extern __shared__ uint8_t smem_raw[];
@@ -550,7 +562,8 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                     // descriptors once per tile; the start address field (bits 0-13,
                     // 16-byte units) then advances by plain adds (shared addresses stay
                     // below 2^18 bytes, so the field never carries)
-                    const uint64_t a0 = smem_desc_sw128(smem_u32(xs + xs_stage * S.x_bytes));
+                    const uint64_t a0 = kTmemA ? 0 : smem_desc_sw128(smem_u32(xs + xs_stage * S.x_bytes));
+                    const uint32_t a_t = tmem_base + A_COL0 + xs_stage * (K / 2);  // voltage stage in TMEM
                     const uint64_t bh0 = smem_desc_sw128(w_hi_addr), bl0 = smem_desc_sw128(w_lo_addr);
 #pragma unroll
                     for (int kk = 0; kk < K / 16; ++kk) {
@@ -558,8 +571,14 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                         const uint64_t a = a0 + ((kb * (kTileM * 128) + koff) >> 4);
                         const uint64_t bh = bh0 + ((kb * (N * 128) + koff) >> 4);
                         const uint64_t bl = bl0 + ((kb * (N * 128) + koff) >> 4);
-                        mma_f16_ss(d_tmem, a, bh, IDESC, kk > 0 ? 1u : 0u);
-                        mma_f16_ss(d_tmem, a, bl, IDESC, 1u);
+                        if constexpr (kTmemA) {
+                            // 16 K values = 8 columns of the TMEM voltage stage
+                            mma_f16_ts(d_tmem, a_t + 8 * kk, bh, IDESC, kk > 0 ? 1u : 0u);
+                            mma_f16_ts(d_tmem, a_t + 8 * kk, bl, IDESC, 1u);
+                        } else {
+                            mma_f16_ss(d_tmem, a, bh, IDESC, kk > 0 ? 1u : 0u);
+                            mma_f16_ss(d_tmem, a, bl, IDESC, 1u);
+                        }
                     }
                     tc_commit(&x_empty[xs_stage]);
                     tc_commit(&acc_full[acc_stage]);
@@ -572,7 +591,65 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
             tc_commit(mma_done);
             if (!mbar_wait(mma_done, 0, kWaitNs)) fail(1024);
         }
+    } else if (warp < kUnpackFirst) {
+        // idle (the TMEM voltage form places its unpack warps on lane quadrants 0-3)
     } else if (warp < kEpiFirstWarp) {
+      if constexpr (kTmemA) {
+        // ------------------------------------------------- unpack into TMEM
+        // Thread = tile row 32 q4 + lane of this warp's lane quadrant: its raw
+        // row (128 bytes, 128-byte swizzled by the TMA) becomes 128 columns of
+        // fp16 pairs in K order (raw word i -> columns 4 i .. 4 i + 3, the
+        // order decode4 and the prepared weights share).
+        const int q4 = warp & 3;
+        const int r = 32 * q4 + lane;
+        int stage = 0, xs_stage = 0;
+        uint32_t phase = 0, x_phase = 0;
+        bool stop = false;
+        JobCursor<kServed> cur;
+        if (u_begin < u_end) cur.init(p, u_begin);
+        cur.pair_parity = pair_parity;
+        for (long long u = u_begin; u < u_end && !stop; ++u) {
+            const Unit un = cur.at(unit_at(p, u));
+            const bool zero = (r & 31) >= cur.jb.rows_q;  // spare quadrant rows of short windows
+            for (int k = un.tile_begin; k < un.tile_end; ++k) {
+                if (*s_fail) { stop = true; break; }
+                if (!mbar_wait(&raw_full[stage], phase, kWaitNs)) { fail(32); stop = true; break; }
+                if (!mbar_wait(&x_empty[xs_stage], x_phase ^ 1, kWaitNs)) { fail(64); stop = true; break; }
+                tc_fence_after();  // the MMAs that read this TMEM stage are complete
+                const uint8_t* row = raw + stage * S.raw_bytes + r * A;
+                const uint32_t tbase = tmem_base + ((32u * q4) << 16) + A_COL0 + xs_stage * (K / 2);
+#pragma unroll
+                for (int g4 = 0; g4 < 4; ++g4) {  // 32 columns: two 16-byte chunks of the row
+                    uint32_t col[32];
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int c = 2 * g4 + h;
+                        uint4 w4 = *reinterpret_cast<const uint4*>(row + ((c ^ (r & 7)) << 4));
+                        if (zero) w4 = make_uint4(0u, 0u, 0u, 0u);
+                        const uint32_t words[4] = {w4.x, w4.y, w4.z, w4.w};
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            const uint4 d4 = decode4(words[j]);
+                            col[16 * h + 4 * j + 0] = d4.x;
+                            col[16 * h + 4 * j + 1] = d4.y;
+                            col[16 * h + 4 * j + 2] = d4.z;
+                            col[16 * h + 4 * j + 3] = d4.w;
+                        }
+                    }
+                    tmem_st_32x32b_x32(tbase + 32 * g4, col);
+                }
+                tmem_st_wait();
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) {
+                    mbar_arrive(&raw_empty[stage]);
+                    mbar_arrive(&x_full[xs_stage]);
+                }
+                if (++stage == 2) { stage = 0; phase ^= 1; }
+                if (++xs_stage == 2) { xs_stage = 0; x_phase ^= 1; }
+            }
+        }
+      } else {
         // ------------------------------------------------------------ unpack
         const int ut = threadIdx.x - 64;  // 0 .. 32 * kUnpackWarps - 1
         int stage = 0, xs_stage = 0;
@@ -615,6 +692,7 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                 if (++xs_stage == 2) { xs_stage = 0; x_phase ^= 1; }
             }
         }
+      }
     } else {
         // ------------------------------------------------------------ epilogue
         // Warp w reads TMEM lane quadrant w % 4 (32 tile rows) and, with eight
@@ -898,15 +976,20 @@ EncodeTiledFn encode_fn() {
 
 int padded_beams(uint64_t b) { return static_cast<int>((b + 15) / 16 * 16); }
 
-// At 128 antennas one channel's hi + lo weight image fits in shared memory
-// beside two voltage stages only for 16 beams (K = 256: 8 KB per 16 beams and
-// part, 64 KB per fp16 voltage stage), so the beams run in groups of 16: one
-// launch per group over the same voltage, each writing its 16 columns of the
-// integrated rows.  The operand holds the groups' images one after the other.
-constexpr int kGroupBeams = 16;
+// At 128 antennas the voltage operand lives in TMEM and the shared memory
+// holds one channel's hi + lo weight images for at most 64 beams (K = 256:
+// 32 KB per 16 beams), so more beams run in groups of 64: one launch per
+// group over the same voltage, each writing its columns of the integrated
+// rows.  The operand holds the groups' images one after the other, each
+// padded to a multiple of 16 beams.
+constexpr int kGroupBeams = 64;
 bool beam_groups(uint64_t n_ant) { return n_ant == 128; }
-uint64_t group_image_bytes(const bf_dims& d, uint64_t n_shards) {
-    return n_shards * d.n_freq * 2ull * (2 * d.n_ant) * (2 * kGroupBeams) * 2ull;
+int group_count(const bf_dims& d) { return static_cast<int>((d.n_beams + kGroupBeams - 1) / kGroupBeams); }
+int group_beams(const bf_dims& d, int g) {
+    return static_cast<int>(std::min<uint64_t>(kGroupBeams, d.n_beams - static_cast<uint64_t>(g) * kGroupBeams));
+}
+uint64_t group_image_bytes(const bf_dims& d, uint64_t n_shards, int nb_pad) {
+    return n_shards * d.n_freq * 2ull * (2 * d.n_ant) * (2ull * nb_pad) * 2ull;
 }
 
 template <int A, int NB, bool kServed>
@@ -968,16 +1051,16 @@ bf_status launch_prepare_split(cudaStream_t stream, const float* w, void* split,
                                uint64_t n_shards, int nb_pad) {
     if (beam_groups(d.n_ant)) {
         if (nb_pad > 0) return set_error(BF_ERR_UNSUPPORTED, "served jobs use 32 or 64 antennas");
-        const int n_groups = static_cast<int>((d.n_beams + kGroupBeams - 1) / kGroupBeams);
-        const long long total = static_cast<long long>(n_shards) * d.n_freq * 2 * kGroupBeams * 2 * d.n_ant;
-        const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, 148LL * 32));
-        for (int g = 0; g < n_groups; ++g) {
-            const int nb = static_cast<int>(std::min<uint64_t>(kGroupBeams, d.n_beams - g * kGroupBeams));
+        uint8_t* out = static_cast<uint8_t*>(split);
+        for (int g = 0; g < group_count(d); ++g) {
+            const int nb = group_beams(d, g), nbp = padded_beams(nb);
+            const long long total = static_cast<long long>(n_shards) * d.n_freq * 2 * nbp * 2 * d.n_ant;
+            const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, 148LL * 32));
             prepare_split_kernel<<<blocks, 256, 0, stream>>>(
-                reinterpret_cast<const float2*>(w), static_cast<uint8_t*>(split) + g * group_image_bytes(d, n_shards),
-                static_cast<int>(d.n_freq), static_cast<int>(d.n_ant), nb, kGroupBeams, static_cast<int>(n_shards),
-                g * kGroupBeams, static_cast<int>(d.n_beams));
+                reinterpret_cast<const float2*>(w), out, static_cast<int>(d.n_freq), static_cast<int>(d.n_ant), nb,
+                nbp, static_cast<int>(n_shards), g * kGroupBeams, static_cast<int>(d.n_beams));
             BF_RETURN_IF(cuda_status(cudaGetLastError(), "prepare_split_kernel launch"));
+            out += group_image_bytes(d, n_shards, nbp);
         }
         return BF_OK;
     }
@@ -1028,7 +1111,9 @@ bf_status encode_voltage_map(CUtensorMap* map, const uint8_t* base, uint64_t n_a
     const cuuint32_t box[4] = {static_cast<cuuint32_t>(n_ant), 1, box_rows, 1};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, const_cast<uint8_t*>(base), dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     // 128-antenna rows are read one row per thread: 128-byte swizzle
+                     n_ant == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
                      CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return set_error(BF_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string(r));
     return BF_OK;
@@ -1098,14 +1183,22 @@ bf_status launch_grid_tensor_impl(cudaStream_t stream, const uint8_t* v, const v
         grid = sms;
     }
     if (grid > 0 && groups) {
-        const int n_groups = static_cast<int>((d.n_beams + kGroupBeams - 1) / kGroupBeams);
-        for (int g = 0; g < n_groups; ++g) {
+        const uint8_t* img = p.job.split;
+        for (int g = 0; g < group_count(d); ++g) {
             TcParams pg = p;
-            pg.job.split = p.job.split + g * group_image_bytes(d, n_shards);
+            const int nb = group_beams(d, g), nbp = padded_beams(nb);
+            pg.job.split = img;
             pg.job.integrated = integrated + g * kGroupBeams;
-            pg.job.n_beams = static_cast<int>(std::min<uint64_t>(kGroupBeams, d.n_beams - g * kGroupBeams));
-            pg.btiles = 1;
-            BF_RETURN_IF((launch_tc<128, kGroupBeams, false>(stream, map, pg, grid)));
+            pg.job.n_beams = nb;
+            pg.btiles = (nb + 15) / 16;
+            switch (nbp) {
+                case 16: st = launch_tc<128, 16, false>(stream, map, pg, grid); break;
+                case 32: st = launch_tc<128, 32, false>(stream, map, pg, grid); break;
+                case 48: st = launch_tc<128, 48, false>(stream, map, pg, grid); break;
+                default: st = launch_tc<128, 64, false>(stream, map, pg, grid); break;
+            }
+            if (st != BF_OK) return st;
+            img += group_image_bytes(d, n_shards, nbp);
         }
     } else if (grid > 0) {
         const int nbp = padded_beams(d.n_beams);
