@@ -62,6 +62,7 @@ constexpr int kTileM = 128;
 constexpr int kRing = 8;                  // window partial-sum slots
 constexpr uint32_t kMaxDynamicSmem = 232448;  // per CTA on sm_100
 constexpr uint64_t kWaitNs = 2000000000ull;  // 2 s bound on any wait
+constexpr int kMaxRawStages = 4;
 
 struct TcParams {
     TcJob job;                  // plain launches
@@ -320,6 +321,7 @@ struct Smem {
     uint32_t w_stages = 1;   // weight images in flight (2 when they fit)
     uint32_t x_bytes = 0;    // one fp16 stage
     uint32_t raw_bytes = 0;  // one raw stage
+    uint32_t raw_stages = 2;
     uint32_t off_w = 0, off_x = 0, off_raw = 0, off_slots = 0, off_bar = 0, total = 0;
 };
 
@@ -330,10 +332,13 @@ __host__ __device__ constexpr Smem smem_plan(int n_ant, int n_beams_pad, bool se
     // at 128 antennas the fp16 voltage operand is written to TMEM instead
     s.x_bytes = n_ant == 128 ? 0 : (K / 64) * kTileM * 128;
     s.raw_bytes = kTileM * n_ant;
+    // with the voltage operand in TMEM the shared memory has room for more raw
+    // tiles in flight, which the short MMAs of small beam groups need
+    s.raw_stages = n_ant == 128 ? kMaxRawStages : 2;
     // window partial sums (S >= 32) or the per-warp power staging of short
     // windows ([8 warps][16 beams][32 spectra] floats), which share the space
     const uint32_t ring = kRing * 4 * n_beams_pad * 4, staging = (kEpilogueThreads / 32) * 16 * 32 * 4;
-    const uint32_t rest = 2 * s.x_bytes + 2 * s.raw_bytes + (ring > staging ? ring : staging) + 256;
+    const uint32_t rest = 2 * s.x_bytes + s.raw_stages * s.raw_bytes + (ring > staging ? ring : staging) + 256;
     // A second weight image lets the next channel's weights load while the
     // MMAs of the current one run.  Served units (one window, a few tiles)
     // switch channel at every unit; measured per served class on a B200, the
@@ -346,7 +351,7 @@ __host__ __device__ constexpr Smem smem_plan(int n_ant, int n_beams_pad, bool se
     s.off_w = 0;
     s.off_x = s.off_w + s.w_stages * 2 * s.w_bytes;
     s.off_raw = s.off_x + 2 * s.x_bytes;
-    s.off_slots = s.off_raw + 2 * s.raw_bytes;
+    s.off_slots = s.off_raw + s.raw_stages * s.raw_bytes;
     s.off_bar = s.off_slots + (ring > staging ? ring : staging);
     s.total = s.off_bar + 256;
     return s;
@@ -391,19 +396,21 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
     uint8_t* raw = smem + S.off_raw;
     float* slots = reinterpret_cast<float*>(smem + S.off_slots);   // [kRing][4][NB] or staging
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + S.off_bar);
-    uint64_t* raw_full = bars + 0;    // [2]
-    uint64_t* raw_empty = bars + 2;   // [2]
-    uint64_t* x_full = bars + 4;      // [2]
-    uint64_t* x_empty = bars + 6;     // [2]
-    uint64_t* acc_full = bars + 8;    // [2]
-    uint64_t* acc_empty = bars + 10;  // [2]
-    uint64_t* w_full = bars + 12;     // [w_stages]
-    uint64_t* w_empty = bars + 14;    // [w_stages]
-    uint64_t* mma_done = bars + 16;
-    uint32_t* tmem_ptr = reinterpret_cast<uint32_t*>(bars + 18);
-    volatile int* s_fail = reinterpret_cast<volatile int*>(bars + 19);
-    volatile int* s_quant = reinterpret_cast<volatile int*>(bars + 20);  // [8] windows to quantize
-    volatile int* s_meta = reinterpret_cast<volatile int*>(bars + 24);   // [2] their shard, channel group
+    constexpr int kRawStages = static_cast<int>(S.raw_stages);
+    uint64_t* raw_full = bars + 0;    // [kRawStages]
+    uint64_t* raw_empty = bars + 4;   // [kRawStages]
+    uint64_t* x_full = bars + 8;      // [2]
+    uint64_t* x_empty = bars + 10;    // [2]
+    uint64_t* acc_full = bars + 12;   // [2]
+    uint64_t* acc_empty = bars + 14;  // [2]
+    uint64_t* w_full = bars + 16;     // [w_stages]
+    uint64_t* w_empty = bars + 18;    // [w_stages]
+    uint64_t* mma_done = bars + 20;
+    uint32_t* tmem_ptr = reinterpret_cast<uint32_t*>(bars + 22);
+    volatile int* s_fail = reinterpret_cast<volatile int*>(bars + 23);
+    volatile int* s_quant = reinterpret_cast<volatile int*>(bars + 24);  // [8] windows to quantize
+    volatile int* s_meta = reinterpret_cast<volatile int*>(bars + 28);   // [2] their shard, channel group
+    static_assert(kRawStages <= kMaxRawStages && 29 * 8 <= 256, "barrier block");
     // A list launch with an empty list (the checked form's common case) ends
     // before any set-up; every thread reads the same count.
     if (!kServed && p.unit_list != nullptr && *p.unit_count == 0) return;
@@ -417,9 +424,11 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     if (threadIdx.x == 0) {
-        for (int i = 0; i < 2; ++i) {
+        for (int i = 0; i < kRawStages; ++i) {
             mbar_init(&raw_full[i], 1);
             mbar_init(&raw_empty[i], kUnpackWarps);
+        }
+        for (int i = 0; i < 2; ++i) {
             mbar_init(&x_full[i], kUnpackWarps);
             mbar_init(&x_empty[i], 1);
             mbar_init(&acc_full[i], 1);
@@ -465,7 +474,9 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
         if (lane == 0) {
             int stage = 0;
             uint32_t phase = 0;
-            int armed[2] = {-1, -1};   // parity of the last load issued per raw stage
+            int armed[kRawStages];     // parity of the last load issued per raw stage
+#pragma unroll
+            for (int i = 0; i < kRawStages; ++i) armed[i] = -1;
             uint32_t w_loads = 0;      // weight images loaded; image i goes to stage i % w_stages
             uint32_t w_uses[2] = {0, 0};
             int prev_key = -1;
@@ -514,11 +525,11 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                         }
                     }
                     armed[stage] = static_cast<int>(phase);
-                    if (++stage == 2) { stage = 0; phase ^= 1; }
+                    if (++stage == kRawStages) { stage = 0; phase ^= 1; }
                 }
             }
             // let every copy this thread issued land before the CTA can exit
-            for (int s = 0; s < 2; ++s) {
+            for (int s = 0; s < kRawStages; ++s) {
                 if (armed[s] >= 0 && !mbar_wait(&raw_full[s], static_cast<uint32_t>(armed[s]), kWaitNs)) fail(256);
             }
             for (uint32_t ws = 0; ws < S.w_stages; ++ws) {
@@ -645,7 +656,7 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                     mbar_arrive(&raw_empty[stage]);
                     mbar_arrive(&x_full[xs_stage]);
                 }
-                if (++stage == 2) { stage = 0; phase ^= 1; }
+                if (++stage == kRawStages) { stage = 0; phase ^= 1; }
                 if (++xs_stage == 2) { xs_stage = 0; x_phase ^= 1; }
             }
         }
@@ -688,7 +699,7 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                     mbar_arrive(&raw_empty[stage]);
                     mbar_arrive(&x_full[xs_stage]);
                 }
-                if (++stage == 2) { stage = 0; phase ^= 1; }
+                if (++stage == kRawStages) { stage = 0; phase ^= 1; }
                 if (++xs_stage == 2) { xs_stage = 0; x_phase ^= 1; }
             }
         }
