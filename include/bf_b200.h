@@ -136,10 +136,11 @@ BF_API bf_status bf_prepare_split_weights(void* stream, const float* weights,
 /* Fused grid beamformer on tcgen05 tensor cores: |X.W|^2, integration over
  * integration_spectra (below 32, or a multiple of 32) and, when codes and params
  * are non-NULL, the int8 chunk quantizer.  n_ant must be 32, 64 or 128 and
- * n_beams <= 128.  At 128 antennas the beams run in groups of 16, one launch
- * per group over the same voltage (one channel's weight image for more beams
- * does not fit in shared memory), and the quantizer runs as a second kernel;
- * 256 antennas are BF_ERR_UNSUPPORTED (the exact kernels take them).
+ * n_beams <= 128.  At 128 antennas the voltage operand is held in tensor
+ * memory and the beams run in groups of 64, one launch per group over the
+ * same voltage (one channel's weight image for more beams does not fit in
+ * shared memory), and the quantizer runs as a second kernel; 256 antennas
+ * are BF_ERR_UNSUPPORTED (the exact kernels take them).
  * integrated may not be NULL (it is also the quantizer's input). */
 BF_API bf_status bf_grid_tensor_integrated(void* stream, const uint8_t* packed_voltage,
                                            const void* split_weights, float* integrated,
