@@ -293,7 +293,6 @@ BF_API bf_status bf_grid_auto_integrated_with(void* stream, const uint8_t* packe
     if (n_shards == 0 || integration_spectra == 0) {
         return set_error(BF_ERR_INVALID_ARGUMENT, "n_shards and integration_spectra must be positive");
     }
-    if (dims->n_ant > 128) return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernels support n_ant 32, 64 or 128");
     if (integration_spectra > 32 && integration_spectra % 32 != 0) {
         return set_error(BF_ERR_UNSUPPORTED,
                          "the tensor-core kernels need integration_spectra below 32 or a multiple of 32");
@@ -323,7 +322,6 @@ static bf_status autotune_impl(cudaStream_t st, const bf_dims* dims, uint64_t S,
     if (n_shards == 0 || n_shards > 8 || S == 0) {
         return set_error(BF_ERR_INVALID_ARGUMENT, "n_shards must be 1 to 8 and integration_spectra positive");
     }
-    if (dims->n_ant > 128) return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernels support n_ant 32, 64 or 128");
     if (S > 32 && S % 32 != 0) {
         return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernels need integration_spectra below 32 or a multiple of 32");
     }

@@ -175,9 +175,6 @@ BF_API bf_status bf_prepare_split_weights(void* stream, const float* weights, vo
     clear_error();
     BF_TRY(validate_dims(dims));
     if (n_shards == 0) return set_error(BF_ERR_INVALID_ARGUMENT, "n_shards must be positive");
-    if (dims->n_ant > 128) {
-        return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernel supports n_ant 32, 64 or 128");
-    }
     BF_TRY(check_ptr(weights, 8, "weights"));
     BF_TRY(check_ptr(split_weights, 16, "split_weights"));
     return launch_prepare_split(static_cast<cudaStream_t>(stream), weights, split_weights, *dims,
@@ -197,9 +194,6 @@ BF_API bf_status bf_grid_tensor_integrated(void* stream, const uint8_t* packed_v
     if (integration_spectra > 32 && integration_spectra % 32 != 0) {
         return set_error(BF_ERR_UNSUPPORTED,
                          "the tensor-core kernel needs integration_spectra below 32 or a multiple of 32");
-    }
-    if (dims->n_ant > 128) {
-        return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernel supports n_ant 32, 64 or 128");
     }
     if ((codes == nullptr) != (params == nullptr)) {
         return set_error(BF_ERR_INVALID_ARGUMENT, "codes and params must both be given or both be null");
@@ -231,9 +225,6 @@ BF_API bf_status bf_grid_tensor_quantized(void* stream, const uint8_t* packed_vo
     if (integration_spectra > 32 && integration_spectra % 32 != 0) {
         return set_error(BF_ERR_UNSUPPORTED,
                          "the tensor-core kernel needs integration_spectra below 32 or a multiple of 32");
-    }
-    if (dims->n_ant > 128) {
-        return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernel supports n_ant 32, 64 or 128");
     }
     BF_TRY(check_ptr(packed_voltage, 16, "packed_voltage"));
     BF_TRY(check_ptr(split_weights, 16, "split_weights"));
@@ -302,7 +293,7 @@ BF_API bf_status bf_grid_cov_estimate(void* stream, const uint8_t* packed_voltag
 }
 
 BF_API uint64_t bf_auto_weight_bytes(const bf_dims* dims, uint64_t n_shards) {
-    if (dims == nullptr || validate_dims(dims) != BF_OK || dims->n_ant > 128) return 0;
+    if (dims == nullptr || validate_dims(dims) != BF_OK) return 0;
     return auto_weight_bytes(*dims, n_shards);
 }
 
@@ -311,7 +302,6 @@ BF_API bf_status bf_prepare_auto_weights(void* stream, const float* weights, voi
     clear_error();
     BF_TRY(validate_dims(dims));
     if (n_shards == 0) return set_error(BF_ERR_INVALID_ARGUMENT, "n_shards must be positive");
-    if (dims->n_ant > 128) return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernels support n_ant 32, 64 or 128");
     BF_TRY(check_ptr(weights, 8, "weights"));
     BF_TRY(check_ptr(auto_weights, 16, "auto_weights"));
     return launch_prepare_auto(static_cast<cudaStream_t>(stream), weights, auto_weights, *dims, n_shards);
@@ -331,7 +321,6 @@ BF_API bf_status bf_grid_auto_integrated(void* stream, const uint8_t* packed_vol
     if (integration_spectra == 0) {
         return set_error(BF_ERR_INVALID_ARGUMENT, "integration_spectra must be positive");
     }
-    if (dims->n_ant > 128) return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernels support n_ant 32, 64 or 128");
     if (integration_spectra > 32 && integration_spectra % 32 != 0) {
         return set_error(BF_ERR_UNSUPPORTED,
                          "the tensor-core kernels need integration_spectra below 32 or a multiple of 32");

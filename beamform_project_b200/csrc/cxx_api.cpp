@@ -387,11 +387,7 @@ CudaBeamformerWorkspace::CudaBeamformerWorkspace(const Dimensions& capacity, Cud
     if (output == CudaBeamformerOutput::QuantizedInt8 && !temporal_integration) {
         throw std::invalid_argument("int8 quantization requires a temporal-integration configuration");
     }
-    if (kernel == CudaBeamformerKernel::TensorSplit && capacity.n_ant > 128) {
-        throw std::invalid_argument("the TensorSplit kernel supports n_ant 32, 64 or 128");
-    }
     if (kernel == CudaBeamformerKernel::TensorChecked) {
-        if (capacity.n_ant > 128) throw std::invalid_argument("the TensorChecked kernel supports n_ant 32, 64 or 128");
         if (!temporal_integration) {
             throw std::invalid_argument("the TensorChecked kernel produces integrated output only");
         }

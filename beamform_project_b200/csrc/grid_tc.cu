@@ -330,7 +330,7 @@ __host__ __device__ constexpr Smem smem_plan(int n_ant, int n_beams_pad, bool se
     const uint32_t K = 2 * n_ant, N = 2 * n_beams_pad;
     s.w_bytes = (K / 64) * N * 128;
     // at 128 antennas the fp16 voltage operand is written to TMEM instead
-    s.x_bytes = n_ant == 128 ? 0 : (K / 64) * kTileM * 128;
+    s.x_bytes = n_ant >= 128 ? 0 : (K / 64) * kTileM * 128;
     s.raw_bytes = kTileM * n_ant;
     // with the voltage operand in TMEM the shared memory has room for more raw
     // tiles in flight, which the short MMAs of small beam groups need
@@ -363,14 +363,17 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
     constexpr int K = 2 * A;
     constexpr int N = 2 * NB;
     constexpr uint32_t ACC_COLS = N;          // fp32 columns per accumulator
-    // At 128 antennas the fp16 voltage tile (128 rows x 256 K, 64 KB) lives in
-    // TMEM, two stages of 128 columns after the two accumulators: the unpack
-    // warps write it with tcgen05.st (a warp reaches one lane quadrant, so
-    // four unpack warps cover the 128 rows) and the MMAs read A from TMEM,
-    // which leaves the shared memory to the weight images of up to 64 beams.
-    constexpr bool kTmemA = A == 128;
+    // At 128 and 256 antennas the fp16 voltage tile (128 rows x K, 64 or
+    // 128 KB) lives in TMEM after the two accumulators, K / 2 columns per
+    // stage (two stages at 128 antennas, one at 256): the unpack warps write
+    // it with tcgen05.st (a warp reaches one lane quadrant, so four unpack
+    // warps cover the 128 rows) and the MMAs read A from TMEM, which leaves
+    // the shared memory to the weight images of up to 64 (32) beams.
+    constexpr bool kTmemA = A >= 128;
+    constexpr int kXStages = A == 256 ? 1 : 2;
+    constexpr int kHalvesA = A >= 128 ? A / 128 : 1;   // 128-byte halves of a raw row
     constexpr uint32_t A_COL0 = 2 * ACC_COLS;
-    static_assert(!kTmemA || A_COL0 + 2 * (K / 2) <= 512, "TMEM holds two accumulators and two voltage stages");
+    static_assert(!kTmemA || A_COL0 + kXStages * (K / 2) <= 512, "TMEM holds two accumulators and the voltage");
     constexpr uint32_t TMEM_COLS = kTmemA ? 512 : (2 * N <= 32) ? 32 : (2 * N <= 64) ? 64 : (2 * N <= 128) ? 128
                                    : (2 * N <= 256) ? 256 : 512;
     constexpr uint32_t IDESC = idesc_f16_f32(kTileM, N);
@@ -512,7 +515,23 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                     if (*s_fail) { stop = true; break; }
                     if (!mbar_wait(&raw_empty[stage], phase ^ 1, kWaitNs)) { fail(2); stop = true; break; }
                     uint8_t* dst = raw + stage * S.raw_bytes;
-                    if (R == 32) {
+                    if constexpr (kTmemA) {
+                        // [half][128 rows][128 bytes], 128-byte swizzled boxes of 128 antennas
+                        mbar_expect_tx(&raw_full[stage], R == 32 ? S.raw_bytes : 4 * R * A);
+#pragma unroll
+                        for (int h = 0; h < kHalvesA; ++h) {
+                            uint8_t* dh = dst + h * (kTileM * 128);
+                            if (R == 32) {
+                                tma_load_4d(dh, &vmap, 128 * h, un.f, jb.t0 + k * kTileM, un.shard, &raw_full[stage]);
+                            } else {
+#pragma unroll
+                                for (int q = 0; q < 4; ++q) {
+                                    tma_load_4d(dh + q * 32 * 128, &vmap, 128 * h, un.f, jb.t0 + (4 * k + q) * R,
+                                                un.shard, &raw_full[stage]);
+                                }
+                            }
+                        }
+                    } else if (R == 32) {
                         mbar_expect_tx(&raw_full[stage], S.raw_bytes);
                         tma_load_4d(dst, &vmap, 0, un.f, jb.t0 + k * kTileM, un.shard, &raw_full[stage]);
                     } else {
@@ -594,7 +613,7 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                     tc_commit(&x_empty[xs_stage]);
                     tc_commit(&acc_full[acc_stage]);
                     if (k + 1 == un.tile_end && next_switches) tc_commit(&w_empty[ws]);
-                    if (++xs_stage == 2) { xs_stage = 0; x_phase ^= 1; }
+                    if (++xs_stage == kXStages) { xs_stage = 0; x_phase ^= 1; }
                     if (++acc_stage == 2) { acc_stage = 0; acc_phase ^= 1; }
                 }
             }
@@ -608,9 +627,10 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
       if constexpr (kTmemA) {
         // ------------------------------------------------- unpack into TMEM
         // Thread = tile row 32 q4 + lane of this warp's lane quadrant: its raw
-        // row (128 bytes, 128-byte swizzled by the TMA) becomes 128 columns of
-        // fp16 pairs in K order (raw word i -> columns 4 i .. 4 i + 3, the
-        // order decode4 and the prepared weights share).
+        // row (A bytes in 128-byte halves, each 128-byte swizzled by the TMA)
+        // becomes K / 2 columns of fp16 pairs in K order (raw word i ->
+        // columns 4 i .. 4 i + 3, the order decode4 and the prepared weights
+        // share).
         const int q4 = warp & 3;
         const int r = 32 * q4 + lane;
         int stage = 0, xs_stage = 0;
@@ -627,15 +647,16 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                 if (!mbar_wait(&raw_full[stage], phase, kWaitNs)) { fail(32); stop = true; break; }
                 if (!mbar_wait(&x_empty[xs_stage], x_phase ^ 1, kWaitNs)) { fail(64); stop = true; break; }
                 tc_fence_after();  // the MMAs that read this TMEM stage are complete
-                const uint8_t* row = raw + stage * S.raw_bytes + r * A;
+                const uint8_t* row = raw + stage * S.raw_bytes + r * 128;
                 const uint32_t tbase = tmem_base + ((32u * q4) << 16) + A_COL0 + xs_stage * (K / 2);
 #pragma unroll
-                for (int g4 = 0; g4 < 4; ++g4) {  // 32 columns: two 16-byte chunks of the row
+                for (int g4 = 0; g4 < A / 32; ++g4) {  // 32 columns: two 16-byte chunks of the row
                     uint32_t col[32];
 #pragma unroll
                     for (int h = 0; h < 2; ++h) {
-                        const int c = 2 * g4 + h;
-                        uint4 w4 = *reinterpret_cast<const uint4*>(row + ((c ^ (r & 7)) << 4));
+                        const int c = 2 * g4 + h;        // chunk c of the row: half c / 8, chunk c % 8 there
+                        uint4 w4 = *reinterpret_cast<const uint4*>(row + (c >> 3) * (kTileM * 128) +
+                                                                   (((c & 7) ^ (r & 7)) << 4));
                         if (zero) w4 = make_uint4(0u, 0u, 0u, 0u);
                         const uint32_t words[4] = {w4.x, w4.y, w4.z, w4.w};
 #pragma unroll
@@ -657,7 +678,7 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                     mbar_arrive(&x_full[xs_stage]);
                 }
                 if (++stage == kRawStages) { stage = 0; phase ^= 1; }
-                if (++xs_stage == 2) { xs_stage = 0; x_phase ^= 1; }
+                if (++xs_stage == kXStages) { xs_stage = 0; x_phase ^= 1; }
             }
         }
       } else {
@@ -987,17 +1008,19 @@ EncodeTiledFn encode_fn() {
 
 int padded_beams(uint64_t b) { return static_cast<int>((b + 15) / 16 * 16); }
 
-// At 128 antennas the voltage operand lives in TMEM and the shared memory
-// holds one channel's hi + lo weight images for at most 64 beams (K = 256:
-// 32 KB per 16 beams), so more beams run in groups of 64: one launch per
-// group over the same voltage, each writing its columns of the integrated
-// rows.  The operand holds the groups' images one after the other, each
-// padded to a multiple of 16 beams.
-constexpr int kGroupBeams = 64;
-bool beam_groups(uint64_t n_ant) { return n_ant == 128; }
-int group_count(const bf_dims& d) { return static_cast<int>((d.n_beams + kGroupBeams - 1) / kGroupBeams); }
+// At 128 and 256 antennas the voltage operand lives in TMEM and the shared
+// memory holds one channel's hi + lo weight images for at most 64 beams
+// (K = 256: 32 KB per 16 beams) or 32 beams (K = 512), so more beams run in
+// groups: one launch per group over the same voltage, each writing its
+// columns of the integrated rows.  The operand holds the groups' images one
+// after the other, each padded to a multiple of 16 beams.
+bool beam_groups(uint64_t n_ant) { return n_ant >= 128; }
+// 64 beams at 128 antennas; at 256 (K = 512) an image of 32 beams is 128 KB
+int group_size(const bf_dims& d) { return d.n_ant == 256 ? 32 : 64; }
+int group_count(const bf_dims& d) { return static_cast<int>((d.n_beams + group_size(d) - 1) / group_size(d)); }
 int group_beams(const bf_dims& d, int g) {
-    return static_cast<int>(std::min<uint64_t>(kGroupBeams, d.n_beams - static_cast<uint64_t>(g) * kGroupBeams));
+    return static_cast<int>(
+        std::min<uint64_t>(group_size(d), d.n_beams - static_cast<uint64_t>(g) * group_size(d)));
 }
 uint64_t group_image_bytes(const bf_dims& d, uint64_t n_shards, int nb_pad) {
     return n_shards * d.n_freq * 2ull * (2 * d.n_ant) * (2ull * nb_pad) * 2ull;
@@ -1069,7 +1092,7 @@ bf_status launch_prepare_split(cudaStream_t stream, const float* w, void* split,
             const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, 148LL * 32));
             prepare_split_kernel<<<blocks, 256, 0, stream>>>(
                 reinterpret_cast<const float2*>(w), out, static_cast<int>(d.n_freq), static_cast<int>(d.n_ant), nb,
-                nbp, static_cast<int>(n_shards), g * kGroupBeams, static_cast<int>(d.n_beams));
+                nbp, static_cast<int>(n_shards), g * group_size(d), static_cast<int>(d.n_beams));
             BF_RETURN_IF(cuda_status(cudaGetLastError(), "prepare_split_kernel launch"));
             out += group_image_bytes(d, n_shards, nbp);
         }
@@ -1119,12 +1142,13 @@ bf_status encode_voltage_map(CUtensorMap* map, const uint8_t* base, uint64_t n_a
     const cuuint64_t dims[4] = {n_ant, n_freq, n_rows, n_shards};
     const cuuint64_t strides[3] = {n_ant, row_stride, shard_stride};
     const cuuint32_t box_rows = static_cast<cuuint32_t>(rows_q == 32 ? kTileM : rows_q);
-    const cuuint32_t box[4] = {static_cast<cuuint32_t>(n_ant), 1, box_rows, 1};
+    // rows of 128 antennas and more arrive in 128-byte boxes, swizzled
+    const cuuint32_t box[4] = {static_cast<cuuint32_t>(n_ant >= 128 ? 128 : n_ant), 1, box_rows, 1};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
     CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 4, const_cast<uint8_t*>(base), dims, strides, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE,
                      // 128-antenna rows are read one row per thread: 128-byte swizzle
-                     n_ant == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                     n_ant >= 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
                      CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return set_error(BF_ERR_CUDA, "cuTensorMapEncodeTiled failed: " + std::to_string(r));
     return BF_OK;
@@ -1139,8 +1163,8 @@ bf_status launch_grid_tensor_impl(cudaStream_t stream, const uint8_t* v, const v
     if (d.n_time >= (1ull << 31) || n_shards > 1024 || spectra >= (1ull << 30)) {
         return set_error(BF_ERR_OVERFLOW, "CUDA tensor-core grid exceeds the supported size");
     }
-    if (d.n_ant != 32 && d.n_ant != 64 && d.n_ant != 128) {
-        return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernel supports n_ant 32, 64 or 128");
+    if (d.n_ant != 32 && d.n_ant != 64 && d.n_ant != 128 && d.n_ant != 256) {
+        return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernel supports n_ant 32, 64, 128 or 256");
     }
     const bool groups = beam_groups(d.n_ant);
     if (groups && unit_list != nullptr) {
@@ -1199,14 +1223,19 @@ bf_status launch_grid_tensor_impl(cudaStream_t stream, const uint8_t* v, const v
             TcParams pg = p;
             const int nb = group_beams(d, g), nbp = padded_beams(nb);
             pg.job.split = img;
-            pg.job.integrated = integrated + g * kGroupBeams;
+            pg.job.integrated = integrated + g * group_size(d);
             pg.job.n_beams = nb;
             pg.btiles = (nb + 15) / 16;
-            switch (nbp) {
-                case 16: st = launch_tc<128, 16, false>(stream, map, pg, grid); break;
-                case 32: st = launch_tc<128, 32, false>(stream, map, pg, grid); break;
-                case 48: st = launch_tc<128, 48, false>(stream, map, pg, grid); break;
-                default: st = launch_tc<128, 64, false>(stream, map, pg, grid); break;
+            if (d.n_ant == 256) {
+                st = nbp == 16 ? launch_tc<256, 16, false>(stream, map, pg, grid)
+                               : launch_tc<256, 32, false>(stream, map, pg, grid);
+            } else {
+                switch (nbp) {
+                    case 16: st = launch_tc<128, 16, false>(stream, map, pg, grid); break;
+                    case 32: st = launch_tc<128, 32, false>(stream, map, pg, grid); break;
+                    case 48: st = launch_tc<128, 48, false>(stream, map, pg, grid); break;
+                    default: st = launch_tc<128, 64, false>(stream, map, pg, grid); break;
+                }
             }
             if (st != BF_OK) return st;
             img += group_image_bytes(d, n_shards, nbp);

@@ -43,9 +43,6 @@ BF_API bf_status bf_grid_tensor_quantized_static(void* stream, const uint8_t* pa
         return set_error(BF_ERR_UNSUPPORTED,
                          "the tensor-core kernel needs integration_spectra below 32 or a multiple of 32");
     }
-    if (dims->n_ant > 128) {
-        return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernel supports n_ant 32, 64 or 128");
-    }
     // The counters serve the quantizer fused into the long-window epilogue
     // (integration_spectra >= 32); short windows quantize in a second kernel
     // and use none, so only long windows are held to the array's size.

@@ -209,7 +209,6 @@ bf_status check_request(const bf_dims* dims, uint64_t spectra, uint64_t n_shards
         return set_error(BF_ERR_UNSUPPORTED,
                          "the tensor-core kernel needs integration_spectra below 32 or a multiple of 32");
     }
-    if (dims->n_ant > 128) return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernel supports n_ant 32, 64 or 128");
     if (dims->n_time >= (1ull << 31) || n_shards > 1024 || spectra >= (1ull << 30)) {
         return set_error(BF_ERR_OVERFLOW, "CUDA tensor-core grid exceeds the supported size");
     }

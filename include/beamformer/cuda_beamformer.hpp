@@ -7,7 +7,7 @@
 //
 // Added selector value: CudaBeamformerKernel::TensorSplit runs the tcgen05
 // split-precision kernel (per-spectrum or integrated output; integration
-// length below 32 or a multiple of 32; 32, 64 or 128 antennas).  upload_weights
+// length below 32 or a multiple of 32; any antenna count).  upload_weights
 // then takes canonical [B][F][A] weights and prepares the fp16 hi + lo
 // operand on the device.
 #pragma once

@@ -33,7 +33,7 @@ enum class CudaBeamformerKernel {
     // INT32 covariance.  Its relative error grows for beams far below the
     // strongest source's power; TensorSplit has no such dependence.
     TensorCovariance,
-    // Checked tensor path (integrated output only, n_ant 32, 64 or 128): the
+    // Checked tensor path (integrated output only, any n_ant): the
     // covariance form where it applies, with every unit whose error estimate
     // exceeds the calibrated limit recomputed by TensorSplit, so every value
     // stays within 1e-5 relative of FP64; TensorSplit elsewhere.  Its stage

@@ -135,12 +135,12 @@ BF_API bf_status bf_prepare_split_weights(void* stream, const float* weights,
 
 /* Fused grid beamformer on tcgen05 tensor cores: |X.W|^2, integration over
  * integration_spectra (below 32, or a multiple of 32) and, when codes and params
- * are non-NULL, the int8 chunk quantizer.  n_ant must be 32, 64 or 128 and
- * n_beams <= 128.  At 128 antennas the voltage operand is held in tensor
- * memory and the beams run in groups of 64, one launch per group over the
- * same voltage (one channel's weight image for more beams does not fit in
- * shared memory), and the quantizer runs as a second kernel; 256 antennas
- * are BF_ERR_UNSUPPORTED (the exact kernels take them).
+ * are non-NULL, the int8 chunk quantizer.  Any n_ant the reference takes
+ * (32, 64, 128, 256) and n_beams <= 128.  At 128 and 256 antennas the
+ * voltage operand is held in tensor memory and the beams run in groups of 64
+ * (32 at 256 antennas), one launch per group over the same voltage (one
+ * channel's weight image for more beams does not fit in shared memory), and
+ * the quantizer runs as a second kernel.
  * integrated may not be NULL (it is also the quantizer's input). */
 BF_API bf_status bf_grid_tensor_integrated(void* stream, const uint8_t* packed_voltage,
                                            const void* split_weights, float* integrated,

@@ -65,9 +65,10 @@ def _check(orc, got, v, w, T, A, B, S):
                                      # windows shorter than a 32-row lane quadrant
                                      (32, 16, 1024, 10), (64, 128, 331, 10), (64, 8, 200, 16),
                                      (32, 33, 77, 1), (64, 64, 250, 3), (64, 40, 100, 20),
-                                     # 128 antennas: beam groups of 16
+                                     # 128 and 256 antennas: voltage operand in TMEM, beam groups
                                      (128, 40, 256, 64), (128, 16, 320, 10), (128, 128, 160, 32),
-                                     (128, 1, 200, 128)])
+                                     (128, 1, 200, 128), (256, 40, 160, 32), (256, 16, 130, 10),
+                                     (256, 70, 128, 128)])
 def test_tensor_grid_within_tolerance(cuda, orc, A, B, T, S):
     from beamform_project_b200 import api
     v = random_voltage(T, F, A, seed=A * B + T)
@@ -161,13 +162,14 @@ def test_tensor_grid_repeatable(cuda, orc):
     assert np.array_equal(a, b) and np.array_equal(ca, cb)
 
 
-def test_tensor_grid_128_antennas_every_entry(cuda, orc):
-    """At 128 antennas (beam groups of 16 over the same voltage) the fused
+@pytest.mark.parametrize("A", [128, 256])
+def test_tensor_grid_128_antennas_every_entry(cuda, orc, A):
+    """At 128 and 256 antennas (beam groups over the same voltage) the fused
     quantizing entry, the checked entry and two shards in one call give the
     products of the plain entry bit for bit, within the bar of FP64."""
     from beamform_project_b200 import api, native
     torch = cuda
-    T, A, B, S, shards = 384, 128, 37, 64, 2
+    T, B, S, shards = 384, 37, 64, 2
     v = np.stack([random_voltage(T, F, A, seed=5), random_voltage(T, F, A, seed=6)])
     w = np.stack([grid_weights(A, F, B, seed=7), grid_weights(A, F, B, seed=8)])
     got, codes, params = _run(torch, api, v, w, T, A, B, S, shards=shards)
