@@ -1780,13 +1780,110 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# --------------------------------------------------------------------------
+# profiling workloads: one grid shape on random inputs, one served job class
+# --------------------------------------------------------------------------
+
+def run_shape(args):
+    """The split-precision grid path on one shard of seeded random voltages
+    and unit-modulus weights of a given shape (--shape-ant, --shape-beams,
+    --shape-spectra, T = --t-spectra), timed with CUDA events, beside the
+    reference-order kernel on the same inputs."""
+    import torch
+    from beamform_project_b200 import api, native
+    T, F, A, B, S = args.t_spectra, F_SHARD, args.shape_ant, args.shape_beams, args.shape_spectra
+    d = api.Dimensions(T, F, A, B)
+    W = -(-T // S)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(SEED)
+    volt = torch.randint(0, 256, (T * F * A,), dtype=torch.uint8, device="cuda", generator=g)
+    ph = torch.rand(B * F * A, device="cuda", generator=g) * (2 * math.pi)
+    w = torch.stack([torch.cos(ph), torch.sin(ph)], -1).contiguous()
+    split = torch.empty(api.split_weight_bytes(d), dtype=torch.uint8, device="cuda")
+    api.prepare_split_weights(None, w, split, d)
+    out = torch.empty(W * F * B, dtype=torch.float32, device="cuda")
+
+    def step():
+        api.grid_tensor_integrated(None, volt, split, out, None, None, d, S)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for e0, e1 in ev:
+        e0.record()
+        step()
+        e1.record()
+    torch.cuda.synchronize()
+    ms = statistics.median(e0.elapsed_time(e1) for e0, e1 in ev)
+    line = {"workload": f"grid shape A={A} B={B} S={S} T={T} F={F} (one shard, random inputs)",
+            "kernel_ms": ms, "algorithmic_tflops": (8.0 * T * F * A * B + 3.0 * T * F * B) / (ms / 1e3) / 1e12}
+    if args.plain_steps > 0:
+        ref = torch.empty_like(out)
+        api.launch_packed_integrated_beamformer(api.CudaBeamformerKernel.Direct, None, volt, w, ref, d, S)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        api.launch_packed_integrated_beamformer(api.CudaBeamformerKernel.Direct, None, volt, w, ref, d, S)
+        e1.record()
+        torch.cuda.synchronize()
+        r, o = ref.double(), out.double()
+        line["plain_dropin_ms"] = e0.elapsed_time(e1)
+        line["max_diff_vs_plain_over_1e-3_plus_abs"] = float(((o - r).abs() / (1e-3 + r.abs())).max())
+    if native.take_device_error() != 0:
+        raise RuntimeError("device error word set")
+    print(json.dumps(line), flush=True)
+
+
+def run_serve_job(args):
+    """One served job of a class alone (--job-kind grid or tracker, --shape-ant,
+    --shape-beams (sources), --shape-spectra, --job-shards) in a small
+    server (2 GB arena, 1920-spectrum pool): the median device time of its
+    windows."""
+    import numpy as np
+    import torch  # noqa: F401  (CUDA context for the server)
+    from beamform_project_b200 import serve
+    A, B, S, ns = args.shape_ant, args.shape_beams, args.shape_spectra, args.job_shards
+    pos = serve.array_positions(A)
+    freq = serve.band_frequencies(ns * F_SHARD)
+    rng = np.random.default_rng(1)
+    if args.job_kind == "tracker":
+        tr = np.zeros((B, 4), np.float32)
+        tr[:, :2] = rng.uniform(-0.3, 0.3, size=(B, 2))
+        tr[:, 2:] = 1e-8
+        spec = serve.JobSpec(serve.TRACKER, A, ns, B, 320 * 5, S, pos, freq, trajectories=tr)
+    else:
+        lm = rng.uniform(-0.3, 0.3, size=(B, 2)).astype(np.float32)
+        n = np.sqrt(1 - (lm ** 2).sum(1)).astype(np.float32)
+        spec = serve.JobSpec(serve.GRID, A, ns, B, 320 * 5, S, pos, freq, directions=np.c_[lm, n].astype(np.float32))
+    srv = serve.Server(int(2e9), max_jobs=8, pool_spectra=1920, pool_seed=1, pool_sigma=2.0)
+    try:
+        srv.submit(spec)
+        while srv.step() > 0:
+            pass
+        srv.sync()
+        t = srv.step_times()
+    finally:
+        srv.close()
+    print(json.dumps({"workload": f"served {args.job_kind} job alone: A={A} B={B} S={S} shards={ns}",
+                      "windows": len(t), "window_ms_median": float(np.median(t[1:])) if len(t) > 1 else None}),
+          flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="grid", choices=["grid", "tracker", "doa", "serve"])
+    ap.add_argument("--workload", default="grid", choices=["grid", "tracker", "doa", "serve", "shape", "serve-job"],
+                    help="shape / serve-job: profiling workloads (one grid shape on random inputs; one served "
+                         "job class alone)")
+    ap.add_argument("--shape-ant", type=int, default=128)
+    ap.add_argument("--shape-beams", type=int, default=64)
+    ap.add_argument("--shape-spectra", type=int, default=320)
+    ap.add_argument("--job-kind", default="tracker", choices=["tracker", "grid"])
+    ap.add_argument("--job-shards", type=int, default=4)
     ap.add_argument("--cov-steps", type=int, default=20,
                     help="grid: time the opt-in covariance-form kernel beside the split kernel")
     ap.add_argument("--kernel", default="auto", choices=["auto", "tensor", "tiled", "stream", "exact"],
@@ -1818,7 +1915,11 @@ def main():
     ap.add_argument("--serve-throughput-k", type=int, default=8,
                     help="serve: also run the stream with this many windows per step (0 or 1: skip)")
     args = ap.parse_args()
-    if args.workload == "serve":
+    if args.workload == "shape":
+        run_shape(args)
+    elif args.workload == "serve-job":
+        run_serve_job(args)
+    elif args.workload == "serve":
         run_serve(args)
     elif args.workload == "tracker":
         run_tracker(args)
