@@ -104,7 +104,7 @@ def clean_table():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("A,B,T,S", [(64, 128, 1280, 320), (64, 16, 1280, 320), (32, 40, 700, 10)])
+@pytest.mark.parametrize("A,B,T,S", [(64, 128, 1280, 320), (64, 16, 1280, 320), (32, 40, 700, 10), (128, 40, 640, 64)])
 def test_autotune_records_a_choice_and_every_candidate_meets_the_bar(cuda, orc, clean_table, A, B, T, S):
     torch = cuda
     d = api.Dimensions(T, F, A, B)

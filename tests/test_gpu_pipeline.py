@@ -33,7 +33,8 @@ def _whole(torch, api, v, w, T, A, B, S, shards):
 
 @pytest.mark.parametrize("A,B,T,S,shards,chunk", [(64, 128, 3000, 320, 2, 640), (32, 37, 2565, 10, 1, 640),
                                                   (64, 16, 1900, 64, 2, 1280), (32, 128, 700, 320, 1, 0),
-                                                  (64, 8, 5120, 32, 1, 1024)])
+                                                  (64, 8, 5120, 32, 1, 1024), (128, 70, 1500, 64, 2, 256),
+                                                  (256, 20, 700, 10, 1, 0)])
 def test_pipeline_equals_single_launch(cuda, A, B, T, S, shards, chunk):
     from beamform_project_b200 import api
     torch = cuda
