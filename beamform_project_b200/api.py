@@ -584,6 +584,58 @@ def doa_scan(stream, covariance, positions, wave_numbers, dims: Dimensions, bloc
                                    int(n_points), float(m_fixed), b, cp, le, w))
 
 
+def _slice_dims(dims: Dimensions) -> None:
+    if not (2 <= dims.n_freq <= 336 and dims.n_freq % 2 == 0):
+        raise InvalidArgument(1, "a channel slice holds an even count of 2 to 336 channels")
+
+
+def doa_covariance_i32_slice(stream, packed_voltage, covariance, dims: Dimensions, block_len: int) -> None:
+    """bf_doa_covariance_i32_slice: doa_covariance_i32 on a contiguous slice of
+    a job's channels (dims.n_freq = the slice's channels), one GPU's share of a
+    channel-split DOA job."""
+    torch = _torch()
+    _slice_dims(dims)
+    B = dims.n_time // block_len if block_len else 0
+    v = _dev(packed_voltage, "packed_voltage", torch.uint8, dims.n_time * dims.n_freq * dims.n_ant)
+    c = _dev(covariance, "covariance", torch.int32, B * dims.n_freq * dims.n_ant * dims.n_ant * 2)
+    d = dims.c()
+    check(native.lib().bf_doa_covariance_i32_slice(_stream_handle(stream), v, c, C.byref(d), int(block_len)))
+
+
+def doa_scan_slice(stream, covariance, positions, wave_numbers, dims: Dimensions, block_len: int, subarray: int,
+                   forgetting: float, diag_load: float, l_first: float, l_step: float, n_points: int,
+                   m_fixed: float, bartlett, capon, l_est, workspace) -> None:
+    """bf_doa_scan_slice: doa_scan over a channel slice; bartlett and capon
+    are the slice's partial sums over frequency (sum them over the slices,
+    then doa_peak)."""
+    torch = _torch()
+    _slice_dims(dims)
+    B = dims.n_time // block_len if block_len else 0
+    M = subarray if 0 < subarray < dims.n_ant else dims.n_ant
+    c = _dev(covariance, "covariance", torch.int32, B * dims.n_freq * dims.n_ant * dims.n_ant * 2)
+    pp = _dev(positions, "positions", torch.float32, 3 * M)
+    k = _dev(wave_numbers, "wave_numbers", torch.float64, dims.n_freq)
+    b = _dev(bartlett, "bartlett", torch.float64, B * n_points)
+    cp = _dev(capon, "capon", torch.float64, B * n_points)
+    le = _dev(l_est, "l_est", torch.float64, 2 * B)
+    w = _dev(workspace, "workspace", torch.uint8, doa_workspace_bytes(dims, block_len, subarray))
+    d = dims.c()
+    check(native.lib().bf_doa_scan_slice(_stream_handle(stream), c, pp, k, C.byref(d), int(block_len),
+                                         int(subarray), float(forgetting), float(diag_load), float(l_first),
+                                         float(l_step), int(n_points), float(m_fixed), b, cp, le, w))
+
+
+def doa_peak(stream, bartlett, capon, n_blocks: int, n_points: int, l_first: float, l_step: float, l_est) -> None:
+    """bf_doa_peak: each block's argmax and parabolic peak of the Bartlett and
+    Capon spectra ([blocks][n_points] double), as doa_scan finds them."""
+    torch = _torch()
+    b = _dev(bartlett, "bartlett", torch.float64, n_blocks * n_points)
+    cp = _dev(capon, "capon", torch.float64, n_blocks * n_points)
+    le = _dev(l_est, "l_est", torch.float64, 2 * n_blocks)
+    check(native.lib().bf_doa_peak(_stream_handle(stream), b, cp, int(n_blocks), int(n_points), float(l_first),
+                                   float(l_step), le))
+
+
 def doa_track_config(block_len: int, subarray: int = 0, capon: bool = False, grid: int = 16, levels: int = 2,
                      interp: bool = True, fov_l: float = 0.2, fov_m: float = 0.2, forgetting: float = 1.0,
                      diag_load: float = 1e-3, prior_l: float = 0.0, prior_m: float = 0.0):

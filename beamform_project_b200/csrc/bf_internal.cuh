@@ -243,6 +243,9 @@ bf_status launch_doa_scan(cudaStream_t stream, const int32_t* R, const float* po
                           const bf_dims& d, uint64_t block_len, uint64_t subarray, double lam, double load,
                           double l_first, double l_step, uint64_t n, double m_fixed, double* bartlett,
                           double* capon, double* l_est, void* workspace);
+// argmax and parabolic peak of each block's Bartlett and Capon spectra
+bf_status launch_doa_peak(cudaStream_t stream, const double* bartlett, const double* capon, uint64_t n_blocks,
+                          uint64_t n_points, double l_first, double l_step, double* l_est);
 // nb_pad > 0 pads the beams to nb_pad columns (a multiple of 16 >= n_beams)
 // instead of the next multiple of 16.
 uint64_t split_weight_bytes(const bf_dims& d, uint64_t n_shards, int nb_pad = 0);

@@ -366,15 +366,45 @@ BF_API bf_status bf_tracker(void* stream, int mode, const uint8_t* packed_voltag
                           integration_spectra);
 }
 
-BF_API bf_status bf_doa_covariance_i32(void* stream, const uint8_t* packed_voltage,
-                                       int32_t* covariance, const bf_dims* dims, uint64_t block_len) {
-    clear_error();
-    BF_TRY(validate_dims(dims));
+// The DOA entries take the reference's 336-channel shard; the _slice entries
+// take a contiguous slice of it (an even count of 2 to 336 channels), the
+// share of one GPU when the channels of a job are split across GPUs.
+static bf_status validate_doa_dims(const bf_dims* dims, bool slice) {
+    if (!slice) {
+        BF_TRY(validate_dims(dims));
+    } else {
+        if (dims == nullptr) return set_error(BF_ERR_INVALID_ARGUMENT, "dims must not be null");
+        if (dims->n_time == 0) return set_error(BF_ERR_INVALID_ARGUMENT, "n_time must be positive");
+        if (dims->n_freq < 2 || dims->n_freq > 336 || dims->n_freq % 2 != 0) {
+            return set_error(BF_ERR_INVALID_ARGUMENT, "a channel slice holds an even count of 2 to 336 channels");
+        }
+        const uint64_t a = dims->n_ant;
+        if (a != 32 && a != 64 && a != 128 && a != 256) {
+            return set_error(BF_ERR_INVALID_ARGUMENT, "n_ant must be 32, 64, 128, or 256");
+        }
+    }
     if (dims->n_beams != 1) return set_error(BF_ERR_INVALID_ARGUMENT, "the DOA path takes n_beams == 1");
+    return BF_OK;
+}
+
+static bf_status doa_covariance_impl(void* stream, const uint8_t* packed_voltage, int32_t* covariance,
+                                     const bf_dims* dims, uint64_t block_len, bool slice) {
+    clear_error();
+    BF_TRY(validate_doa_dims(dims, slice));
     BF_TRY(check_ptr(packed_voltage, 16, "packed_voltage"));
     BF_TRY(check_ptr(covariance, 8, "covariance"));
     return launch_doa_covariance(static_cast<cudaStream_t>(stream), packed_voltage, covariance, *dims,
                                  block_len);
+}
+
+BF_API bf_status bf_doa_covariance_i32(void* stream, const uint8_t* packed_voltage,
+                                       int32_t* covariance, const bf_dims* dims, uint64_t block_len) {
+    return doa_covariance_impl(stream, packed_voltage, covariance, dims, block_len, false);
+}
+
+BF_API bf_status bf_doa_covariance_i32_slice(void* stream, const uint8_t* packed_voltage,
+                                             int32_t* covariance, const bf_dims* dims, uint64_t block_len) {
+    return doa_covariance_impl(stream, packed_voltage, covariance, dims, block_len, true);
 }
 
 BF_API uint64_t bf_doa_workspace_bytes(const bf_dims* dims, uint64_t block_len, uint64_t subarray) {
@@ -383,14 +413,13 @@ BF_API uint64_t bf_doa_workspace_bytes(const bf_dims* dims, uint64_t block_len, 
     return doa_workspace_bytes(dims->n_time / block_len, dims->n_freq, M);
 }
 
-BF_API bf_status bf_doa_scan(void* stream, const int32_t* covariance, const float* positions,
-                             const double* wave_numbers, const bf_dims* dims, uint64_t block_len,
-                             uint64_t subarray, double forgetting, double diag_load, double l_first,
-                             double l_step, uint64_t n_points, double m_fixed, double* bartlett,
-                             double* capon, double* l_est, void* workspace) {
+static bf_status doa_scan_impl(void* stream, const int32_t* covariance, const float* positions,
+                               const double* wave_numbers, const bf_dims* dims, uint64_t block_len,
+                               uint64_t subarray, double forgetting, double diag_load, double l_first,
+                               double l_step, uint64_t n_points, double m_fixed, double* bartlett,
+                               double* capon, double* l_est, void* workspace, bool slice) {
     clear_error();
-    BF_TRY(validate_dims(dims));
-    if (dims->n_beams != 1) return set_error(BF_ERR_INVALID_ARGUMENT, "the DOA path takes n_beams == 1");
+    BF_TRY(validate_doa_dims(dims, slice));
     if (block_len == 0 || dims->n_time % block_len != 0) {
         return set_error(BF_ERR_INVALID_ARGUMENT, "block_len must divide n_time");
     }
@@ -410,6 +439,37 @@ BF_API bf_status bf_doa_scan(void* stream, const int32_t* covariance, const floa
     return launch_doa_scan(static_cast<cudaStream_t>(stream), covariance, positions, wave_numbers, *dims,
                            block_len, subarray, forgetting, diag_load, l_first, l_step, n_points, m_fixed,
                            bartlett, capon, l_est, workspace);
+}
+
+BF_API bf_status bf_doa_scan(void* stream, const int32_t* covariance, const float* positions,
+                             const double* wave_numbers, const bf_dims* dims, uint64_t block_len,
+                             uint64_t subarray, double forgetting, double diag_load, double l_first,
+                             double l_step, uint64_t n_points, double m_fixed, double* bartlett,
+                             double* capon, double* l_est, void* workspace) {
+    return doa_scan_impl(stream, covariance, positions, wave_numbers, dims, block_len, subarray, forgetting,
+                         diag_load, l_first, l_step, n_points, m_fixed, bartlett, capon, l_est, workspace, false);
+}
+
+BF_API bf_status bf_doa_scan_slice(void* stream, const int32_t* covariance, const float* positions,
+                                   const double* wave_numbers, const bf_dims* dims, uint64_t block_len,
+                                   uint64_t subarray, double forgetting, double diag_load, double l_first,
+                                   double l_step, uint64_t n_points, double m_fixed, double* bartlett,
+                                   double* capon, double* l_est, void* workspace) {
+    return doa_scan_impl(stream, covariance, positions, wave_numbers, dims, block_len, subarray, forgetting,
+                         diag_load, l_first, l_step, n_points, m_fixed, bartlett, capon, l_est, workspace, true);
+}
+
+BF_API bf_status bf_doa_peak(void* stream, const double* bartlett, const double* capon, uint64_t n_blocks,
+                             uint64_t n_points, double l_first, double l_step, double* l_est) {
+    clear_error();
+    if (n_blocks == 0 || n_blocks > 65535 || n_points == 0 || n_points > (1u << 24)) {
+        return set_error(BF_ERR_INVALID_ARGUMENT, "n_blocks must be in [1, 65535] and n_points in [1, 2^24]");
+    }
+    BF_TRY(check_ptr(bartlett, 8, "bartlett"));
+    BF_TRY(check_ptr(capon, 8, "capon"));
+    BF_TRY(check_ptr(l_est, 8, "l_est"));
+    return launch_doa_peak(static_cast<cudaStream_t>(stream), bartlett, capon, n_blocks, n_points, l_first, l_step,
+                           l_est);
 }
 
 static bf_status check_track(const bf_dims* dims, const bf_doa_track_config* c) {

@@ -679,4 +679,11 @@ bf_status launch_doa_scan(cudaStream_t stream, const int32_t* R, const float* po
     return cuda_status(cudaGetLastError(), "doa_peak_kernel launch");
 }
 
+bf_status launch_doa_peak(cudaStream_t stream, const double* bartlett, const double* capon, uint64_t n_blocks,
+                          uint64_t n_points, double l_first, double l_step, double* l_est) {
+    doa_peak_kernel<<<static_cast<unsigned>(n_blocks), 64, 0, stream>>>(bartlett, capon, static_cast<int>(n_points),
+                                                                       l_first, l_step, l_est);
+    return cuda_status(cudaGetLastError(), "doa_peak_kernel launch");
+}
+
 }  // namespace bf

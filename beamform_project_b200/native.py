@@ -156,6 +156,10 @@ _SIGS = {
     "bf_doa_workspace_bytes": (_U64, [C.POINTER(Dims), _U64, _U64]),
     "bf_doa_scan": (C.c_int, [_P, _P, _P, _P, C.POINTER(Dims), _U64, _U64, C.c_double, C.c_double,
                               C.c_double, C.c_double, _U64, C.c_double, _P, _P, _P, _P]),
+    "bf_doa_scan_slice": (C.c_int, [_P, _P, _P, _P, C.POINTER(Dims), _U64, _U64, C.c_double, C.c_double,
+                              C.c_double, C.c_double, _U64, C.c_double, _P, _P, _P, _P]),
+    "bf_doa_covariance_i32_slice": (C.c_int, [_P, _P, _P, C.POINTER(Dims), _U64]),
+    "bf_doa_peak": (C.c_int, [_P, _P, _P, _U64, _U64, C.c_double, C.c_double, _P]),
     "bf_generate_voltage": (C.c_int, [_P, _U64, _U64, C.c_float, _P, _U64, _P, C.POINTER(Dims)]),
     "bf_doa_track_workspace_bytes": (_U64, [C.POINTER(Dims), C.POINTER(DoaTrackConfig)]),
     "bf_doa_track": (C.c_int, [_P, _P, _P, _P, C.POINTER(Dims), C.POINTER(DoaTrackConfig), _P, _P, _P]),

@@ -1383,6 +1383,81 @@ def doa_cpu_baseline(v: np.ndarray, pos, freq, budget_s: float):
             "host": host_cpu_info()}
 
 
+def run_doa_split(args):
+    """The DOA step of one job split across the GPUs by channel (the path's one
+    exchange step): each rank takes a contiguous slice of the 336 channels
+    (covariance, fold and scan of the slice), one NCCL all-reduce sums the
+    partial spectra (2 x 16 x 1801 doubles), then the peak search.  Strong
+    scaling: the whole job's samples over the max-over-ranks step time."""
+    import datetime
+    import torch
+    from beamform_project_b200 import api, native
+    from beamform_project_b200.doa_channels import channel_slice, scan_slice
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    T = DOA_K * DOA_BLOCKS
+    pos, freq, k, mu, truth = doa_inputs(T)
+    d = api.Dimensions(T, F_SHARD, N_ANT, 1)
+    volt = torch.empty(T * F_SHARD * N_ANT, dtype=torch.uint8, device=dev)
+    api.generate_voltage(None, SEED + 5, 0, DOA_SIGMA, torch.from_numpy(mu).to(dev), DOA_EPOCH, volt, d)
+    sl = channel_slice(F_SHARD, rank, world)
+    vs = volt.view(T, F_SHARD, N_ANT)[:, sl.start:sl.stop].contiguous()
+    del volt
+    pos_d = torch.from_numpy(np.ascontiguousarray(pos[:DOA_SUB])).to(dev)
+    k_d = torch.from_numpy(np.ascontiguousarray(k[sl.start:sl.stop])).to(dev)
+    l0, dl, n = DOA_GRID
+
+    def step():
+        return scan_slice(vs, pos_d, k_d, T, N_ANT, DOA_K, DOA_SUB, 0.9, 1e-3, l0, dl, n, 0.0)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize()
+    if native.take_device_error() != 0:
+        raise RuntimeError("device error word set")
+    steps = max(1, min(args.steps, 50))
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(steps):
+        spectra, l_est = step()
+    t1.record()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    ms = t0.elapsed_time(t1) / steps
+    if dist:
+        tt = torch.tensor([ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    est = l_est.cpu().numpy()
+    line = {
+        "metric": METRIC, "value": T * F_SHARD / (ms / 1e3), "unit": "beam-samples/s", "n_gpus": world,
+        "steps": steps, "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "int4xint8->int32, fp64",
+        "data": "synthetic (seeded on-device generator; coherent pair + multipath)",
+        "config": {"workload": "DOA, one job split by channel: A=64 (2x32), F=336, K=4096 x 16 blocks, "
+                               "Bartlett + Capon on 1801 points",
+                   "parallelism": f"channel split x{world} (NCCL all-reduce of the partial spectra)",
+                   "channels_on_rank0": len(channel_slice(F_SHARD, 0, world))},
+        "l_est_last_block": {"bartlett": float(est[-1, 0]), "capon": float(est[-1, 1])},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def run_doa_reference(args):
     if int(os.environ.get("RANK", "0")) != 0:
         return
@@ -1876,9 +1951,9 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="grid", choices=["grid", "tracker", "doa", "serve", "shape", "serve-job"],
-                    help="shape / serve-job: profiling workloads (one grid shape on random inputs; one served "
-                         "job class alone)")
+    ap.add_argument("--workload", default="grid", choices=["grid", "tracker", "doa", "doa-split", "serve", "shape", "serve-job"],
+                    help="doa-split: one DOA job split across the GPUs by channel (strong scaling); shape / "
+                         "serve-job: profiling workloads (one grid shape on random inputs; one served job class alone)")
     ap.add_argument("--shape-ant", type=int, default=128)
     ap.add_argument("--shape-beams", type=int, default=64)
     ap.add_argument("--shape-spectra", type=int, default=320)
@@ -1919,6 +1994,8 @@ def main():
         run_shape(args)
     elif args.workload == "serve-job":
         run_serve_job(args)
+    elif args.workload == "doa-split":
+        run_doa_split(args)
     elif args.workload == "serve":
         run_serve(args)
     elif args.workload == "tracker":

@@ -411,6 +411,26 @@ BF_API bf_status bf_doa_scan(void* stream, const int32_t* covariance, const floa
                              double l_first, double l_step, uint64_t n_points, double m_fixed,
                              double* bartlett, double* capon, double* l_est, void* workspace);
 
+/* Channel-split DOA (no reference counterpart: the reference runs one job's
+ * channels in one process).  The _slice entries are bf_doa_covariance_i32 and
+ * bf_doa_scan on a contiguous slice of a job's channels -- dims.n_freq an even
+ * count of 2 to 336, packed_voltage [T][slice][A], wave_numbers [slice] --
+ * so that each GPU of a split job takes one slice; their bartlett and capon
+ * outputs are the slice's partial sums over frequency (l_est is that of the
+ * partial sums).  Summed over the slices (one all-reduce of
+ * 2 x blocks x n_points doubles), they are the job's spectra up to the
+ * order of the sum; bf_doa_peak then finds each block's peaks exactly as
+ * bf_doa_scan does. */
+BF_API bf_status bf_doa_covariance_i32_slice(void* stream, const uint8_t* packed_voltage,
+                                             int32_t* covariance, const bf_dims* dims, uint64_t block_len);
+BF_API bf_status bf_doa_scan_slice(void* stream, const int32_t* covariance, const float* positions,
+                                   const double* wave_numbers, const bf_dims* dims, uint64_t block_len,
+                                   uint64_t subarray, double forgetting, double diag_load,
+                                   double l_first, double l_step, uint64_t n_points, double m_fixed,
+                                   double* bartlett, double* capon, double* l_est, void* workspace);
+BF_API bf_status bf_doa_peak(void* stream, const double* bartlett, const double* capon, uint64_t n_blocks,
+                             uint64_t n_points, double l_first, double l_step, double* l_est);
+
 /* The reference's adaptive tracker (CpuOptBeamTracker::run_into,
  * src/cpu_opt_beam_tracker.cpp:1619-2454) on the GPU: per window of
  * block_len spectra, the covariance fold above, then a coarse-to-fine

@@ -170,3 +170,26 @@ def test_doa_track_validates_before_any_cuda_call():
         assert api.doa_track_workspace_bytes(d, cfg) == 0
     ok = api.doa_track_config(256, subarray=8)
     assert api.doa_track_workspace_bytes(d, ok) > 1024 * 336 // 256 * 32 * 32 * 8
+
+
+def test_doa_slice_entries_validate_before_launch():
+    """The channel-slice DOA entries take an even count of 2 to 336 channels;
+    the peak entry checks its sizes; nothing reaches the device."""
+    lib = native.lib()
+    fake = C.c_void_p(4096)
+    for f in (3, 338, 0):
+        d = Dims(256, f, 64, 1)
+        assert lib.bf_doa_covariance_i32_slice(None, fake, fake, C.byref(d), 128) == 1
+        assert "even count of 2 to 336" in native.last_error()
+    d = Dims(256, 168, 64, 2)
+    assert lib.bf_doa_covariance_i32_slice(None, fake, fake, C.byref(d), 128) == 1
+    assert "n_beams == 1" in native.last_error()
+    d = Dims(256, 168, 64, 1)
+    assert lib.bf_doa_scan_slice(None, fake, fake, fake, C.byref(d), 100, 8, 0.9, 1e-3, -0.6, 0.004, 301, 0.0,
+                                 fake, fake, fake, fake) == 1
+    assert "block_len must divide n_time" in native.last_error()
+    # the 336-channel entries keep the reference's dimension contract
+    assert lib.bf_doa_covariance_i32(None, fake, fake, C.byref(d), 128) == 1
+    assert "336 frequency channels" in native.last_error()
+    assert lib.bf_doa_peak(None, fake, fake, 0, 301, -0.6, 0.004, fake) == 1
+    assert lib.bf_doa_peak(None, fake, fake, 3, 0, -0.6, 0.004, fake) == 1
