@@ -201,8 +201,11 @@ __global__ void doa_factor_kernel(const Cd* __restrict S_in, const double* __res
 constexpr int kScanWarps = 8;
 constexpr int kMaxSplit = 8;
 
-template <int M>
-__host__ __device__ constexpr int scan_blocks() { return M <= 13 ? 4 : 2; }
+// Blocks per CTA: each (channel, grid point) steering vector serves this many
+// blocks.  The uniform form stages 4M - 2 doubles per cell and takes 8; the
+// general form stages the triangles of S and Q, 4 (2 above 13 elements).
+template <int M, bool kUniform>
+__host__ __device__ constexpr int scan_blocks() { return kUniform ? 8 : M <= 13 ? 4 : 2; }
 
 // Uniform sub-array form.  With p_m = p_0 + m D + e_m (D = (p_{M-1} - p_0) /
 // (M - 1), e_m the residuals of the float positions) and psi = k D.d,
@@ -312,7 +315,7 @@ doa_scan_kernel(const Cd* __restrict S, const Cd* __restrict Q, const int* __res
                 const double* __restrict coef) {
     // the two forms are launched together; the array decides which one runs
     if ((info->uniform != 0) != kUniform) return;
-    constexpr int kScanBlocks = scan_blocks<M>();
+    constexpr int kScanBlocks = scan_blocks<M, kUniform>();
     constexpr int U = M * (M + 1) / 2;                 // upper triangle incl. diagonal
     constexpr int CQ = coef_per_form(M);
     // Cd staged per warp and step: upper triangles of S and Q, or the two
@@ -522,7 +525,7 @@ template <int M, bool kUniform>
 bf_status launch_scan_form(cudaStream_t stream, const Cd* S, const Cd* Q, const int* ok, const float* pos,
                            const double* kw, int B, int F, double l_first, double l_step, int n, double m_fixed,
                            double* bartlett, double* capon, const ArrayInfo* info, const double* coef) {
-    constexpr int KB = scan_blocks<M>();
+    constexpr int KB = scan_blocks<M, kUniform>();
     const unsigned gx = static_cast<unsigned>((n + 31) / 32), gy = static_cast<unsigned>((B + KB - 1) / KB);
     const size_t per_warp = kUniform ? static_cast<size_t>(KB) * coef_per_form(M)
                                      : static_cast<size_t>(KB) * 2 * (M * (M + 1) / 2);
