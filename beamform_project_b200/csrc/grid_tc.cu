@@ -336,8 +336,8 @@ __host__ __device__ constexpr Smem smem_plan(int n_ant, int n_beams_pad, bool se
     // tiles in flight, which the short MMAs of small beam groups need
     s.raw_stages = n_ant == 128 ? kMaxRawStages : 2;
     // window partial sums (S >= 32) or the per-warp power staging of short
-    // windows ([8 warps][16 beams][32 spectra] floats), which share the space
-    const uint32_t ring = kRing * 4 * n_beams_pad * 4, staging = (kEpilogueThreads / 32) * 16 * 32 * 4;
+    // windows ([8 warps][16 beams][33] floats), which share the space
+    const uint32_t ring = kRing * 4 * n_beams_pad * 4, staging = (kEpilogueThreads / 32) * 16 * 33 * 4;
     const uint32_t rest = 2 * s.x_bytes + s.raw_stages * s.raw_bytes + (ring > staging ? ring : staging) + 256;
     // A second weight image lets the next channel's weights load while the
     // MMAs of the current one run.  Served units (one window, a few tiles)
@@ -739,7 +739,7 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
         constexpr int kHalfLoads = (kLoads + kHalves - 1) / kHalves;
         const int c_begin = half * kHalfLoads;
         const int c_count = min(kHalfLoads, kLoads - c_begin);
-        float* stg = slots + (warp - kEpiFirstWarp) * 512;  // short windows: [16 beams][32 rows]
+        float* stg = slots + (warp - kEpiFirstWarp) * 528;  // short windows: [16 beams][33]
         float acc[kHalfLoads];
 #pragma unroll
         for (int c = 0; c < kHalfLoads; ++c) acc[c] = 0.f;
@@ -758,40 +758,43 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
         };
         // Short windows (S < 32): every window lies inside one lane quadrant.
         // The 16 powers of each lane's spectrum go to the staging tile
-        // (column = row ^ beam, conflict-free both ways) and the lanes then sum
-        // the (window, beam) pairs of the quadrant.
-        auto short_windows = [&](const uint32_t (&r)[32], int c, const TcJob& jb, const Unit& un, int sq) {
+        // [16 beams][33] (row pitch 33 floats: the stores of a beam and the
+        // reads of a window both spread over the banks) and each lane sums a
+        // (window, beam) pair of the quadrant, in increasing row order.  wq is
+        // the quadrant's first window; the unit's window length sw and pair
+        // count npairs (16 per window) are set once per unit.
+        auto nwin_of = [](int npairs) { return npairs >> 4; };
+        auto short_windows = [&](const uint32_t (&r)[32], int c, const TcJob& jb, const Unit& un, int wq, int sw,
+                                 int npairs) {
+            float* srow = stg + lane;
 #pragma unroll
             for (int j = 0; j < 16; ++j) {
                 const float re = __uint_as_float(r[2 * j]), im = __uint_as_float(r[2 * j + 1]);
-                stg[j * 32 + (lane ^ j)] = re * re + im * im;
+                srow[j * 33] = re * re + im * im;
             }
             __syncwarp();
-            // each lane sums two (window, beam) pairs at a time, p and p + 32,
-            // in increasing row order; the loads of both run ahead of the adds
-            const int sw = jb.spectra, npairs = (jb.rows_q / sw) * 16;
+            const int b16 = 16 * (c_begin + c);
+            const size_t row_base = static_cast<size_t>(un.shard) * jb.n_windows + jb.w0;
+            // two pairs per lane at a time (p and p + 32), their sums interleaved;
+            // a pair past the quadrant's reads the staging tile and is dropped
             for (int pb = 0; pb < npairs; pb += 64) {
                 const int p0 = pb + lane, p1 = pb + 32 + lane;
-                const bool v0 = p0 < npairs, v1 = p1 < npairs;
-                const int j0 = p0 & 15, s0 = p0 >> 4, j1 = p1 & 15, s1 = p1 >> 4;
-                const float* row0 = stg + j0 * 32;
-                const float* row1 = stg + j1 * 32;
+                const int j0 = p0 & 15, j1 = p1 & 15;
+                const int s0 = min(p0 >> 4, nwin_of(npairs) - 1), s1 = min(p1 >> 4, nwin_of(npairs) - 1);
+                const float* x0 = stg + j0 * 33 + s0 * sw;
+                const float* x1 = stg + j1 * 33 + s1 * sw;
                 float sum0 = 0.f, sum1 = 0.f;
-#pragma unroll 4
+#pragma unroll 5
                 for (int i = 0; i < sw; ++i) {
-                    const float x0 = v0 ? row0[(s0 * sw + i) ^ j0] : 0.f;
-                    const float x1 = v1 ? row1[(s1 * sw + i) ^ j1] : 0.f;
-                    sum0 += x0;
-                    sum1 += x1;
+                    sum0 += x0[i];
+                    sum1 += x1[i];
                 }
-                const int w0 = sq / sw + s0, w1 = sq / sw + s1;
-                const int b0 = 16 * (c_begin + c) + j0, b1 = 16 * (c_begin + c) + j1;
-                const size_t row_base = static_cast<size_t>(un.shard) * jb.n_windows + jb.w0;
-                if (v0 && w0 * sw < jb.n_time && b0 < jb.n_beams) {
-                    jb.integrated[((row_base + w0) * jb.n_freq + un.f) * jb.beam_stride + b0] = sum0;
+                const int w0 = wq + s0, w1 = wq + s1;
+                if (p0 < npairs && w0 * sw < jb.n_time && b16 + j0 < jb.n_beams) {
+                    jb.integrated[((row_base + w0) * jb.n_freq + un.f) * jb.beam_stride + b16 + j0] = sum0;
                 }
-                if (v1 && w1 * sw < jb.n_time && b1 < jb.n_beams) {
-                    jb.integrated[((row_base + w1) * jb.n_freq + un.f) * jb.beam_stride + b1] = sum1;
+                if (p1 < npairs && w1 * sw < jb.n_time && b16 + j1 < jb.n_beams) {
+                    jb.integrated[((row_base + w1) * jb.n_freq + un.f) * jb.beam_stride + b16 + j1] = sum1;
                 }
             }
             __syncwarp();
@@ -803,12 +806,14 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
             const Unit un = cur.at(unit_at(p, u));
             const TcJob& jb = cur.jb;
             const bool short_win = jb.spectra < 32;
+            const int sw = jb.spectra, nwin = short_win ? jb.rows_q / sw : 0, npairs = nwin * 16;
             for (int k = un.tile_begin; k < un.tile_end; ++k) {
                 if (!failed && !mbar_wait(&acc_full[acc_stage], acc_phase, kWaitNs)) { fail(128); failed = true; }
                 tc_fence_after();
                 const uint32_t taddr = tmem_base + ((32u * q4) << 16) + acc_stage * ACC_COLS + 32 * c_begin;
                 if (short_win) {
                     const int sq = (4 * k + q4) * jb.rows_q;  // first spectrum of this quadrant
+                    const int wq = (4 * k + q4) * nwin;         // its first window (rows_q = nwin * sw)
                     if (!failed && sq < jb.n_time) {
 #pragma unroll
                         for (int c = 0; c < kHalfLoads; c += 2) {
@@ -818,11 +823,11 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                                 uint32_t r1[32];
                                 if (c + 1 < c_count) tmem_ld_32x32b_x32(taddr + 32 * (c + 1), r1);
                                 tmem_ld_wait();
-                                if (c < c_count) short_windows(r0, c, jb, un, sq);
-                                if (c + 1 < c_count) short_windows(r1, c + 1, jb, un, sq);
+                                if (c < c_count) short_windows(r0, c, jb, un, wq, sw, npairs);
+                                if (c + 1 < c_count) short_windows(r1, c + 1, jb, un, wq, sw, npairs);
                             } else {
                                 tmem_ld_wait();
-                                if (c < c_count) short_windows(r0, c, jb, un, sq);
+                                if (c < c_count) short_windows(r0, c, jb, un, wq, sw, npairs);
                             }
                         }
                     }
