@@ -15,29 +15,34 @@
 // accumulate into the same fp32 TMEM accumulator, so D carries about 22 bits
 // of weight precision.  |.|^2 and the time integration run in the epilogue.
 //
-// CTA organisation (one persistent CTA per SM, 8 warps):
+// CTA organisation (one persistent CTA per SM, 12 warps):
 //   warp 0      TMA producer: raw voltage tiles (128 spectra x A bytes of one
-//               channel, 4-D tensor map, zero fill past T) and the channel's
+//               channel, 4-D tensor map, zero fill past T; four quadrant boxes
+//               of R rows for windows below 32 spectra) and the channel's
 //               prepared weight image (1-D bulk copies).
 //   warp 1      TMEM owner and MMA issuer (one thread): 2 x K/16
 //               tcgen05.mma (M=128, N=2B, K=16) per tile, hi then lo.
-//   warps 2-3   unpack: raw int4 bytes -> fp16 in the 128-byte-swizzled
-//               K-major layout the MMA reads (two LOP3s + one half2 op per
-//               value pair; the K order is permuted to follow the decode,
-//               and the prepared weights follow the same permutation).
-//   warps 4-7   epilogue: TMEM -> registers (tcgen05.ld 32x32b), power per
-//               (spectrum, beam), butterfly reduce-scatter over the 32
-//               spectra of each warp, running per-window sums, and the window
-//               total over the four warps in a fixed order.
-// Pipelines: 2 raw stages, 2 fp16 stages, 2 TMEM accumulators (2 x 2B
-// columns), all mbarrier driven; every wait is bounded and records an error
-// code instead of hanging.
+//   unpack      raw int4 bytes -> fp16 in the 128-byte-swizzled K-major
+//               layout the MMA reads (two LOP3s + one half2 op per value
+//               pair; the K order follows the decode and the prepared
+//               weights follow it): warps 2-3 (2-7 for 16 beams).  At 128
+//               and 256 antennas warps 4-7, one per TMEM lane quadrant, write
+//               the fp16 tile into TMEM instead and the MMAs read A there.
+//   epilogue    the remaining warps, a multiple of four: TMEM -> registers
+//               (tcgen05.ld 32x32b), power per (spectrum, beam), then either
+//               a butterfly reduce-scatter over each warp's 32 spectra into
+//               running per-window sums (S >= 32) or a staging tile summed per
+//               (window, beam) inside the warp's lane quadrant (S < 32), and
+//               window totals over the four quadrants in a fixed order.
+// Pipelines: 2 raw stages (4 at 128 antennas), 2 fp16 stages, 2 TMEM
+// accumulators, all mbarrier driven; every wait is bounded and records an
+// error code instead of hanging.
 //
 // Work split: units are (shard, channel, group of G tiles) with G tiles =
-// lcm(128, S) spectra, so no integration window crosses a unit; each CTA
-// takes a contiguous range of units (few channel switches, so few weight
-// loads).  S must be a multiple of 32, which keeps every warp's 32 spectra
-// inside one window.
+// lcm(128, S) spectra (a tile of 4 x R rows, R = 32 / S * S, below 32), so no
+// integration window crosses a unit; each CTA takes a contiguous range of
+// units (few channel switches, so few weight loads).  S is below 32 or a
+// multiple of 32, so a window never straddles a warp's 32 spectra.
 #include "bf_internal.cuh"
 #include "grid_tc.cuh"
 #include "sm100.cuh"
@@ -1293,7 +1298,7 @@ bf_status launch_grid_tensor_served(cudaStream_t stream, const CUtensorMap& map,
     p.table = table;
     if (n_ant == 32) return dispatch_served<32>(stream, map, p, nb_pad, grid);
     if (n_ant == 64) return dispatch_served<64>(stream, map, p, nb_pad, grid);
-    return set_error(BF_ERR_UNSUPPORTED, "the tensor-core kernel supports n_ant 32 or 64");
+    return set_error(BF_ERR_UNSUPPORTED, "served jobs use 32 or 64 antennas");
 }
 
 // Device address of the error word for kernels in other translation units
