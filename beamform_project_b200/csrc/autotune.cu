@@ -27,6 +27,7 @@
 #include "serve.cuh"
 
 #include <dlfcn.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <cmath>
@@ -97,16 +98,29 @@ bool load_locked(const std::string& path) {
     return true;
 }
 
+// Written to a file of its own, then renamed over the cache: processes that
+// save at the same time (one per GPU) never leave a torn file.
 bool save_locked(const std::string& path) {
-    std::ofstream out(path, std::ios::trunc);
-    if (!out) return false;
-    out << "# device n_ant padded_beams integration_spectra form group_mult paired ms\n";
-    for (const auto& kv : g_table) {
-        out << kv.first.device << ' ' << kv.first.n_ant << ' ' << kv.first.nb_pad << ' ' << kv.first.spectra << ' '
-            << kv.second.cfg.form << ' ' << kv.second.cfg.group_mult << ' ' << kv.second.cfg.paired << ' '
-            << kv.second.ms << '\n';
+    const std::string tmp = path + ".tmp." + std::to_string(static_cast<long long>(getpid()));
+    {
+        std::ofstream out(tmp, std::ios::trunc);
+        if (!out) return false;
+        out << "# device n_ant padded_beams integration_spectra form group_mult paired ms\n";
+        for (const auto& kv : g_table) {
+            out << kv.first.device << ' ' << kv.first.n_ant << ' ' << kv.first.nb_pad << ' ' << kv.first.spectra
+                << ' ' << kv.second.cfg.form << ' ' << kv.second.cfg.group_mult << ' ' << kv.second.cfg.paired << ' '
+                << kv.second.ms << '\n';
+        }
+        if (!out) {
+            std::remove(tmp.c_str());
+            return false;
+        }
     }
-    return static_cast<bool>(out);
+    if (std::rename(tmp.c_str(), path.c_str()) != 0) {
+        std::remove(tmp.c_str());
+        return false;
+    }
+    return true;
 }
 
 void ensure_loaded_locked() {
