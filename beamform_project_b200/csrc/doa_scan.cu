@@ -35,51 +35,176 @@ struct Cd {
     double re, im;
 };
 
-// Fold, in three launches so that only the forgetting recursion is serial:
-//  doa_smooth_kernel  (block, channel) cells in parallel: smoothing over the
-//                     L = A - M + 1 sub-arrays, 1/K, forward-backward, and
-//                     the loading eps = load * tr / M (the averaged matrix is
-//                     parked in the Q slot of the workspace);
-//  doa_forget_kernel  per channel, blocks in order: S = lam S + (1 - lam) R^,
-//                     E = lam E + (1 - lam) eps (first block: S = R^, E = eps);
-//  doa_factor_kernel  cells in parallel: Cholesky L L^H = S + E I (one warp),
-//                     column j of L^{-1} by thread j, and Q = L^{-H} L^{-1} =
-//                     (S + E I)^{-1} by elements, so the scan evaluates
-//                     Capon's |L^{-1} a|^2 as the quadratic form a^H Q a.
-__global__ void doa_smooth_kernel(const int32_t* __restrict R, int n_freq, int A, int M, int K,
-                                  double load, Cd* __restrict Rhat_out, double* __restrict eps_out) {
-    const int f = blockIdx.x, b = blockIdx.y;
-    __shared__ Cd Rt[kMaxM * kMaxM];
+// Fold of the (block, channel) cells, per cell and element:
+//   smooth_warp      smoothing over the L = A - M + 1 sub-arrays and 1/K;
+//   loading_eps      eps = load * tr / M of the forward-backward average;
+//   fb_elems         forward-backward average R^ = (R~ + J conj(R~) J) / 2;
+//   forget_step      S = lam S + (1 - lam) R^ (first block: S = R^), and the
+//                    same recursion for E;
+//   cholesky_warp    L L^H = S + E I by one warp;
+//   inverse_column   column j of L^{-1} by forward substitution;
+//   q_elem           Q = L^{-H} L^{-1} = (S + E I)^{-1}, so the scan
+//                    evaluates Capon's |L^{-1} a|^2 as the quadratic form a^H Q a.
+// Two schedules share them (same operations in the same order, so the same
+// results): doa_fold_kernel, one CTA per channel walking its blocks in chunks
+// with one warp per cell, for sequences of up to kFoldChunks chunks; and three
+// launches for longer ones, where only the forgetting recursion is serial --
+// doa_smooth_kernel and doa_factor_kernel over all cells, doa_forget_kernel
+// per channel.
+
+// Smoothing of one cell by one warp.  R~[r][c] sums R[s + r][s + c] over
+// s < L: entry R[t][t + d] belongs to the elements (r, r + d) with
+// r <= t < r + L, so the warp reads R's band |u - t| < M row by row (2M - 1
+// contiguous entries of a row, one per lane, RB rows in flight) and
+// each lane takes its elements' entries by shuffle.  The sums are of
+// integers, exact in int64, so the row order does not change them.  NE is
+// the count of elements per lane (at least (M^2 + 31) / 32), RB the rows
+// loaded at once.
+template <int NE, int RB>
+__device__ __forceinline__ void smooth_warp(const int32_t* __restrict Rf, int A, int M, int K, Cd* Rt, int lane) {
     const int L = A - M + 1;
-    const int32_t* Rf = R + (static_cast<size_t>(b) * n_freq + f) * A * A * 2;
-    for (int e = threadIdx.x; e < M * M; e += blockDim.x) {
+    long long ar[NE], ai[NE];
+    int src[NE], r0[NE];
+#pragma unroll
+    for (int k = 0; k < NE; ++k) {
+        const int e = lane + 32 * k;
         const int r = e / M, c = e % M;
-        double sr = 0.0, si = 0.0;
-        for (int s = 0; s < L; ++s) {
-            sr += static_cast<double>(Rf[2 * ((s + r) * A + s + c)]);
-            si += static_cast<double>(Rf[2 * ((s + r) * A + s + c) + 1]);
-        }
-        Rt[e] = Cd{sr / K / L, si / K / L};
+        ar[k] = ai[k] = 0;
+        src[k] = e < M * M ? c - r + M - 1 : 0;
+        r0[k] = e < M * M ? r : A;  // past every row: never adds
     }
-    __syncthreads();
-    const size_t cell = static_cast<size_t>(b) * n_freq + f;
-    if (threadIdx.x == 0) {
-        double tr = 0.0;
-        for (int r = 0; r < M; ++r) {
-            const Cd x = Rt[r * M + r];
-            tr += L > 1 ? 0.5 * (x.re + Rt[(M - 1 - r) * M + (M - 1 - r)].re) : x.re;
+    const int2* R2 = reinterpret_cast<const int2*>(Rf);
+    const bool loads = lane < 2 * M - 1;
+    for (int t0 = 0; t0 < A; t0 += RB) {
+        int2 v[RB];
+#pragma unroll
+        for (int i = 0; i < RB; ++i) {
+            const int t = t0 + i, u = t - (M - 1) + lane;
+            v[i] = loads && t < A && u >= 0 && u < A ? R2[t * A + u] : make_int2(0, 0);
         }
-        eps_out[cell] = load * tr / M;
+#pragma unroll
+        for (int i = 0; i < RB; ++i) {
+            const int t = t0 + i;
+#pragma unroll
+            for (int k = 0; k < NE; ++k) {
+                const int x = __shfl_sync(0xffffffffu, v[i].x, src[k]);
+                const int y = __shfl_sync(0xffffffffu, v[i].y, src[k]);
+                if (r0[k] <= t && t < r0[k] + L) {
+                    ar[k] += x;
+                    ai[k] += y;
+                }
+            }
+        }
     }
-    for (int e = threadIdx.x; e < M * M; e += blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < NE; ++k) {
+        const int e = lane + 32 * k;
+        if (e < M * M) Rt[e] = Cd{static_cast<double>(ar[k]) / K / L, static_cast<double>(ai[k]) / K / L};
+    }
+}
+
+__device__ __forceinline__ double loading_eps(const Cd* Rt, int M, int L, double load) {
+    double tr = 0.0;
+    for (int r = 0; r < M; ++r) {
+        const Cd x = Rt[r * M + r];
+        tr += L > 1 ? 0.5 * (x.re + Rt[(M - 1 - r) * M + (M - 1 - r)].re) : x.re;
+    }
+    return load * tr / M;
+}
+
+__device__ __forceinline__ void fb_elems(const Cd* Rt, int M, int L, Cd* out, int e0, int step) {
+    for (int e = e0; e < M * M; e += step) {
         const int r = e / M, c = e % M;
         Cd x = Rt[e];
         if (L > 1) {
             const Cd y = Rt[(M - 1 - r) * M + (M - 1 - c)];
             x = Cd{0.5 * (x.re + y.re), 0.5 * (x.im - y.im)};
         }
-        Rhat_out[cell * M * M + e] = x;
+        out[e] = x;
     }
+}
+
+__device__ __forceinline__ Cd forget_step(bool first, double lam, Cd s, Cd x) {
+    return (first || lam >= 1.0) ? x : Cd{lam * s.re + (1.0 - lam) * x.re, lam * s.im + (1.0 - lam) * x.im};
+}
+
+__device__ __forceinline__ double forget_step(bool first, double lam, double acc, double eps) {
+    return (first || lam >= 1.0) ? eps : lam * acc + (1.0 - lam) * eps;
+}
+
+// Right-looking Cholesky of S + E I by one warp: step j takes the square root
+// of the updated diagonal, lanes i > j scale column j and update their own row
+// i of the trailing lower triangle.  Returns (warp-uniformly) 1 when every
+// pivot is positive.
+__device__ __forceinline__ int cholesky_warp(const Cd* S, double E, int M, Cd* Lc, int lane) {
+    for (int e = lane; e < M * M; e += 32) {
+        const int i = e / M, j = e % M;
+        Lc[e] = j <= i ? Cd{S[e].re + (i == j ? E : 0.0), S[e].im} : Cd{0.0, 0.0};
+    }
+    __syncwarp();
+    int good = 1;
+    for (int j = 0; j < M; ++j) {
+        const double djj = Lc[j * M + j].re;
+        if (!(djj > 1e-300)) { good = 0; break; }
+        const double ljj = sqrt(djj);
+        __syncwarp();
+        if (lane == j) Lc[j * M + j] = Cd{ljj, 0.0};
+        if (lane > j && lane < M) {
+            const Cd x = Lc[lane * M + j];
+            Lc[lane * M + j] = Cd{x.re / ljj, x.im / ljj};
+        }
+        __syncwarp();
+        if (lane > j && lane < M) {
+            const Cd lij = Lc[lane * M + j];
+            for (int k = j + 1; k <= lane; ++k) {
+                const Cd lkj = Lc[k * M + j];  // row lane -= l_ij * conj(l_kj)
+                Cd& w = Lc[lane * M + k];
+                w = Cd{w.re - (lij.re * lkj.re + lij.im * lkj.im), w.im - (lij.im * lkj.re - lij.re * lkj.im)};
+            }
+        }
+        __syncwarp();
+    }
+    return good;
+}
+
+__device__ __forceinline__ void inverse_column(const Cd* Lc, int M, Cd* Li, int j) {
+    for (int i = 0; i < j; ++i) Li[i * M + j] = Cd{0.0, 0.0};
+    Li[j * M + j] = Cd{1.0 / Lc[j * M + j].re, 0.0};
+    for (int i = j + 1; i < M; ++i) {
+        double sr = 0.0, si = 0.0;
+        for (int k = j; k < i; ++k) {
+            const Cd x = Lc[i * M + k], y = Li[k * M + j];
+            sr += x.re * y.re - x.im * y.im;
+            si += x.re * y.im + x.im * y.re;
+        }
+        const double d = Lc[i * M + i].re;
+        Li[i * M + j] = Cd{-sr / d, -si / d};
+    }
+}
+
+__device__ __forceinline__ Cd q_elem(const Cd* Li, int M, int e) {
+    const int i = e / M, j = e % M;
+    double qr = 0.0, qi = 0.0;
+    for (int k = i > j ? i : j; k < M; ++k) {
+        const Cd x = Li[k * M + i], y = Li[k * M + j];  // conj(x) * y
+        qr += x.re * y.re + x.im * y.im;
+        qi += x.re * y.im - x.im * y.re;
+    }
+    return Cd{qr, qi};
+}
+
+// Three-launch schedule: the averaged matrix is parked in the Q slot of the
+// workspace between doa_smooth_kernel and doa_forget_kernel.
+__global__ void doa_smooth_kernel(const int32_t* __restrict R, int n_freq, int A, int M, int K,
+                                  double load, Cd* __restrict Rhat_out, double* __restrict eps_out) {
+    const int f = blockIdx.x, b = blockIdx.y;
+    __shared__ Cd Rt[kMaxM * kMaxM];
+    const int L = A - M + 1;
+    const size_t cell = static_cast<size_t>(b) * n_freq + f;
+    smooth_warp<kMaxM * kMaxM / 32, 8>(R + cell * A * A * 2, A, M, K, Rt, threadIdx.x);
+    __syncwarp();
+    if (threadIdx.x == 0) eps_out[cell] = loading_eps(Rt, M, L, load);
+    fb_elems(Rt, M, L, Rhat_out + cell * M * M, threadIdx.x, 32);
 }
 
 __global__ void doa_forget_kernel(const Cd* __restrict Rhat, int n_blocks, int n_freq, int M, double lam,
@@ -89,8 +214,7 @@ __global__ void doa_forget_kernel(const Cd* __restrict Rhat, int n_blocks, int n
         Cd s{0.0, 0.0};
         for (int b = 0; b < n_blocks; ++b) {
             const size_t at = (static_cast<size_t>(b) * n_freq + f) * M * M + e;
-            const Cd x = Rhat[at];
-            s = (b == 0 || lam >= 1.0) ? x : Cd{lam * s.re + (1.0 - lam) * x.re, lam * s.im + (1.0 - lam) * x.im};
+            s = forget_step(b == 0, lam, s, Rhat[at]);
             S_out[at] = s;
         }
     }
@@ -98,8 +222,7 @@ __global__ void doa_forget_kernel(const Cd* __restrict Rhat, int n_blocks, int n
         double acc = 0.0;
         for (int b = 0; b < n_blocks; ++b) {
             const size_t cell = static_cast<size_t>(b) * n_freq + f;
-            const double eps = E[cell];
-            acc = (b == 0 || lam >= 1.0) ? eps : lam * acc + (1.0 - lam) * eps;
+            acc = forget_step(b == 0, lam, acc, E[cell]);
             E[cell] = acc;
         }
     }
@@ -117,71 +240,87 @@ __global__ void doa_factor_kernel(const Cd* __restrict S_in, const double* __res
     for (int e = threadIdx.x; e < M * M; e += blockDim.x) S[e] = S_in[base + e];
     __syncthreads();
     if (threadIdx.x < 32) {
-        // right-looking Cholesky of S + E I by one warp: step j takes the
-        // square root of the updated diagonal, lanes i > j scale column j and
-        // update their own row i of the trailing lower triangle
-        const int lane = threadIdx.x;
-        const double E = E_in[cell];
-        for (int e = lane; e < M * M; e += 32) {
-            const int i = e / M, j = e % M;
-            Lc[e] = j <= i ? Cd{S[e].re + (i == j ? E : 0.0), S[e].im} : Cd{0.0, 0.0};
-        }
-        __syncwarp();
-        int good = 1;
-        for (int j = 0; j < M; ++j) {
-            const double djj = Lc[j * M + j].re;
-            if (!(djj > 1e-300)) { good = 0; break; }
-            const double ljj = sqrt(djj);
-            __syncwarp();
-            if (lane == j) Lc[j * M + j] = Cd{ljj, 0.0};
-            if (lane > j && lane < M) {
-                const Cd x = Lc[lane * M + j];
-                Lc[lane * M + j] = Cd{x.re / ljj, x.im / ljj};
-            }
-            __syncwarp();
-            if (lane > j && lane < M) {
-                const Cd lij = Lc[lane * M + j];
-                for (int k = j + 1; k <= lane; ++k) {
-                    const Cd lkj = Lc[k * M + j];  // row lane -= l_ij * conj(l_kj)
-                    Cd& w = Lc[lane * M + k];
-                    w = Cd{w.re - (lij.re * lkj.re + lij.im * lkj.im), w.im - (lij.im * lkj.re - lij.re * lkj.im)};
-                }
-            }
-            __syncwarp();
-        }
-        if (lane == 0) {
+        const int good = cholesky_warp(S, E_in[cell], M, Lc, threadIdx.x);
+        if (threadIdx.x == 0) {
             ok = good;
             ok_out[cell] = good;
         }
     }
     __syncthreads();
-    if (ok && threadIdx.x < M) {  // column j of L^{-1} by forward substitution
-        const int j = threadIdx.x;
-        for (int i = 0; i < j; ++i) Li[i * M + j] = Cd{0.0, 0.0};
-        Li[j * M + j] = Cd{1.0 / Lc[j * M + j].re, 0.0};
-        for (int i = j + 1; i < M; ++i) {
-            double sr = 0.0, si = 0.0;
-            for (int k = j; k < i; ++k) {
-                const Cd x = Lc[i * M + k], y = Li[k * M + j];
-                sr += x.re * y.re - x.im * y.im;
-                si += x.re * y.im + x.im * y.re;
-            }
-            const double d = Lc[i * M + i].re;
-            Li[i * M + j] = Cd{-sr / d, -si / d};
-        }
-    }
+    if (ok && threadIdx.x < M) inverse_column(Lc, M, Li, threadIdx.x);
     __syncthreads();
-    for (int e = threadIdx.x; e < M * M; e += blockDim.x) {
-        const int i = e / M, j = e % M;
-        double qr = 0.0, qi = 0.0;
-        if (ok) {
-            for (int k = i > j ? i : j; k < M; ++k) {
-                const Cd x = Li[k * M + i], y = Li[k * M + j];  // conj(x) * y
-                qr += x.re * y.re + x.im * y.im;
-                qi += x.re * y.im - x.im * y.re;
+    for (int e = threadIdx.x; e < M * M; e += blockDim.x) Q_out[base + e] = ok ? q_elem(Li, M, e) : Cd{0.0, 0.0};
+}
+
+// One-launch schedule: a CTA per channel takes its blocks fold_cells<M>() at a
+// time, one warp per cell.  Per chunk: each warp smooths, averages and loads
+// its cell; the CTA's threads carry the forgetting recursion (S element by
+// element, E in one thread) through the chunk's blocks in order, in registers
+// across chunks; each warp then factors its cell.  Chunks of 8 cells up to 11
+// elements, 4 above (at most 32 KB of shared memory).
+__host__ __device__ constexpr int fold_cells_for(int M) { return M <= 11 ? 8 : 4; }
+template <int M>
+__host__ __device__ constexpr int fold_cells() { return fold_cells_for(M); }
+constexpr int kFoldChunks = 8;
+
+template <int M>
+__global__ void __launch_bounds__(32 * fold_cells<M>(), 3)
+doa_fold_kernel(const int32_t* __restrict R, int n_blocks, int n_freq, int A, int K, double lam, double load,
+                Cd* __restrict S_out, Cd* __restrict Q_out, double* __restrict E_out, int* __restrict ok_out) {
+    constexpr int CH = fold_cells<M>(), MM = M * M, kThreads = 32 * CH;
+    constexpr int kCarry = (MM + kThreads - 1) / kThreads;
+    __shared__ Cd sh_a[CH][MM];  // R~, then L
+    __shared__ Cd sh_b[CH][MM];  // R^, then S, then L^{-1}
+    __shared__ double sh_e[CH];
+    const int f = blockIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int L = A - M + 1;
+    Cd s_carry[kCarry];
+#pragma unroll
+    for (int k = 0; k < kCarry; ++k) s_carry[k] = Cd{0.0, 0.0};
+    double e_carry = 0.0;
+    for (int b0 = 0; b0 < n_blocks; b0 += CH) {
+        const int b = b0 + warp, nb = min(CH, n_blocks - b0);
+        const size_t cell = static_cast<size_t>(b) * n_freq + f;
+        if (b < n_blocks) {
+            smooth_warp<(MM + 31) / 32, 8>(R + cell * A * A * 2, A, M, K, sh_a[warp], lane);
+            __syncwarp();
+            if (lane == 0) sh_e[warp] = loading_eps(sh_a[warp], M, L, load);
+            fb_elems(sh_a[warp], M, L, sh_b[warp], lane, 32);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < kCarry; ++k) {
+            const int e = threadIdx.x + k * kThreads;
+            if (e < MM) {
+                Cd s = s_carry[k];
+                for (int w = 0; w < nb; ++w) {
+                    s = forget_step(b0 + w == 0, lam, s, sh_b[w][e]);
+                    sh_b[w][e] = s;
+                    S_out[(static_cast<size_t>(b0 + w) * n_freq + f) * MM + e] = s;
+                }
+                s_carry[k] = s;
             }
         }
-        Q_out[base + e] = Cd{qr, qi};
+        if (threadIdx.x == kThreads - 1) {
+            double acc = e_carry;
+            for (int w = 0; w < nb; ++w) {
+                acc = forget_step(b0 + w == 0, lam, acc, sh_e[w]);
+                sh_e[w] = acc;
+                E_out[static_cast<size_t>(b0 + w) * n_freq + f] = acc;
+            }
+            e_carry = acc;
+        }
+        __syncthreads();
+        if (b < n_blocks) {
+            const int good = cholesky_warp(sh_b[warp], sh_e[warp], M, sh_a[warp], lane);
+            if (lane == 0) ok_out[cell] = good;
+            __syncwarp();  // S is consumed: its slot takes L^{-1}
+            if (good && lane < M) inverse_column(sh_a[warp], M, sh_b[warp], lane);
+            __syncwarp();
+            for (int e = lane; e < MM; e += 32) Q_out[cell * MM + e] = good ? q_elem(sh_b[warp], M, e) : Cd{0.0, 0.0};
+        }
+        __syncthreads();
     }
 }
 
@@ -633,6 +772,25 @@ uint64_t doa_workspace_bytes(uint64_t n_blocks, uint64_t n_freq, uint64_t M) {
 
 uint64_t doa_fold_bytes(uint64_t cells, uint64_t M) { return doa_coef_offset(cells, M); }
 
+namespace {
+
+template <int M>
+bf_status dispatch_fold(int m, cudaStream_t stream, const int32_t* R, int B, int F, int A, int K, double lam,
+                        double load, Cd* S, Cd* Q, double* E, int* ok) {
+    if constexpr (M > kMaxM) {
+        return set_error(BF_ERR_UNSUPPORTED, "the DOA scan supports at most 16 elements after smoothing");
+    } else {
+        if (m == M) {
+            static_assert(2 * fold_cells<M>() * M * M * sizeof(Cd) <= 32768, "fold shared memory");
+            doa_fold_kernel<M><<<F, 32 * fold_cells<M>(), 0, stream>>>(R, B, F, A, K, lam, load, S, Q, E, ok);
+            return cuda_status(cudaGetLastError(), "doa_fold_kernel launch");
+        }
+        return dispatch_fold<M + 1>(m, stream, R, B, F, A, K, lam, load, S, Q, E, ok);
+    }
+}
+
+}  // namespace
+
 bf_status launch_doa_fold(cudaStream_t stream, const int32_t* R, const bf_dims& d, uint64_t block_len, int M,
                           double lam, double load, void* workspace) {
     const int A = static_cast<int>(d.n_ant);
@@ -644,8 +802,11 @@ bf_status launch_doa_fold(cudaStream_t stream, const int32_t* R, const bf_dims& 
     Cd* Lc = S + cells * M * M;  // the fold writes Q = (S + E I)^{-1} here
     auto* E = reinterpret_cast<double*>(Lc + cells * M * M);
     auto* ok = reinterpret_cast<int*>(E + cells);
+    if (B <= kFoldChunks * fold_cells_for(M)) {
+        return dispatch_fold<1>(M, stream, R, B, F, A, static_cast<int>(block_len), lam, load, S, Lc, E, ok);
+    }
     const dim3 cells_grid(static_cast<unsigned>(F), static_cast<unsigned>(B));
-    doa_smooth_kernel<<<cells_grid, 64, 0, stream>>>(R, F, A, M, static_cast<int>(block_len), load, Lc, E);
+    doa_smooth_kernel<<<cells_grid, 32, 0, stream>>>(R, F, A, M, static_cast<int>(block_len), load, Lc, E);
     BF_RETURN_IF(cuda_status(cudaGetLastError(), "doa_smooth_kernel launch"));
     doa_forget_kernel<<<F, 64, 0, stream>>>(Lc, B, F, M, lam, S, E);
     BF_RETURN_IF(cuda_status(cudaGetLastError(), "doa_forget_kernel launch"));

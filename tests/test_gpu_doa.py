@@ -189,6 +189,36 @@ def test_scan_element_counts_match_fp64_oracle(cuda, orc, M, jitter):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("B,M", [(64, 8), (65, 8), (64, 11), (65, 11), (32, 16), (33, 16), (9, 12), (1, 5)])
+def test_fold_schedules_match_fp64_oracle(cuda, orc, B, M):
+    """The fold's two schedules on a 16-channel slice against the FP64
+    oracle: one launch per channel over chunks of cells (up to 64 blocks at
+    11 elements or fewer, 32 above; the forgetting recursion carried from
+    chunk to chunk) and three launches for longer block sequences."""
+    from beamform_project_b200 import api, native
+    torch = cuda
+    A, K, Fs, n, lam, load = 32, 128, 16, 101, 0.9, 1e-3
+    pos, freq, kw = geometry(A)
+    kws = np.ascontiguousarray(kw[:Fs])
+    v = rng(100 * B + M).integers(0, 256, size=(K * B, Fs, A), dtype=np.uint8)
+    d = api.Dimensions(K * B, Fs, A, 1)
+    cov = torch.empty(B * Fs * A * A * 2, dtype=torch.int32, device="cuda")
+    api.doa_covariance_i32_slice(None, torch.from_numpy(v).cuda(), cov, d, K)
+    bart = torch.empty(B * n, dtype=torch.float64, device="cuda")
+    cap = torch.empty(B * n, dtype=torch.float64, device="cuda")
+    lest = torch.empty(2 * B, dtype=torch.float64, device="cuda")
+    ws = torch.empty(api.doa_workspace_bytes(d, K, M), dtype=torch.uint8, device="cuda")
+    api.doa_scan_slice(None, cov, torch.from_numpy(pos[:M]).cuda(), torch.from_numpy(kws).cuda(), d, K, M, lam,
+                       load, -0.6, 0.012, n, 0.0, bart, cap, lest, ws)
+    torch.cuda.synchronize()
+    assert native.take_device_error() == 0
+    R = cov.cpu().numpy().reshape(B, Fs, A, A, 2).astype(np.int64)
+    eb, ec, _ = orc.doa_scan(R, K, M, lam, load, pos[:M], kws, -0.6, 0.012, n)
+    assert np.allclose(bart.cpu().numpy().reshape(B, n), eb, rtol=1e-6, atol=0.0)
+    assert np.allclose(cap.cpu().numpy().reshape(B, n), ec, rtol=1e-6, atol=0.0)
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("A,capon,subarray,G,levels", [(32, False, 16, 16, 2), (64, False, 8, 12, 1),
                                                        (32, True, 8, 16, 2), (64, True, 8, 8, 0)])
 def test_adaptive_tracker_follows_reference_search(cuda, ref, orc, A, capon, subarray, G, levels):
