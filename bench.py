@@ -56,8 +56,8 @@ METRIC = "beam-samples/s (T*F*B)"
 # both are scaled to a full launch by the units processed.  The captures and
 # their commands are summarised under profiles/.
 NCU_TRAFFIC = {
-    "grid": 2 * (767.70e6 + 20.72e6),
-    "grid_cov": 2 * (768.22e6 + 19.66e6),
+    "grid": 2 * (768.05e6 + 19.96e6),
+    "grid_cov": 2 * (767.84e6 + 19.31e6),
     "tracker": 8 * (704.677888e6 + 3.885312e6),
     "doa": 1.410239e9 + 162.888960e6,
 }
