@@ -58,8 +58,8 @@ METRIC = "beam-samples/s (T*F*B)"
 NCU_TRAFFIC = {
     "grid": 2 * (768.05e6 + 19.96e6),
     "grid_cov": 2 * (767.84e6 + 19.31e6),
-    "tracker": 8 * (704.677888e6 + 3.885312e6),
-    "doa": 1.410239e9 + 162.888960e6,
+    "tracker": 8 * (704.715776e6 + 4.859392e6),
+    "doa": 1.410263e9 + 162.521600e6,
 }
 
 
