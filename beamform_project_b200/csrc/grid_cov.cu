@@ -43,7 +43,7 @@
 // the beam sums.
 // TMEM: two 128-column E stages (Gram accumulator, then A operand) and two
 // 128-column Y stages.  Shared memory: the channel's V image (fp16 hi, fp16 lo in the
-// 128-byte-swizzled K-major layout, fp32 [beam][component]), voltage stages.
+// 128-byte-swizzled K-major layout, fp32 [component][beam] in rows of 132), voltage stages.
 // Every wait is bounded and reports through the device error word.
 #include "bf_internal.cuh"
 #include "grid_tc.cuh"
@@ -79,7 +79,8 @@ constexpr int kRawStages = 8, kXStages = 6;
 constexpr uint32_t kRawBytes = kRows * 64;            // one channel, 64 antennas
 constexpr uint32_t kXBytes = kRows * 128;             // [row][128 components] int8
 constexpr uint32_t kWHalf = 128 * 256;                // [128 beams][128 K] fp16
-constexpr uint32_t kVBytes = 128 * 128 * 4;           // [beam][component] fp32
+constexpr int kVPitch = 132;                          // floats per component row of the fp32 V
+constexpr uint32_t kVBytes = 128 * kVPitch * 4;       // [component][beam] fp32, rows padded
 constexpr uint32_t kWImage = 2 * kWHalf + kVBytes;    // per channel
 constexpr uint32_t kYCol = 256;                       // TMEM columns of the two Y stages
 constexpr uint64_t kWaitNs = 2000000000ull;
@@ -100,7 +101,12 @@ struct CovGridParams {
     unsigned* err;
     int n_freq, n_beams, n_windows, n_time, spectra;
     long long n_pair_units;  // shards x F/2 x windows
-    float e_scale, out_scale;
+    float out_scale;         // 2^k
+    // E scaled by 2^-k as one integer add and one subtract: the float
+    // 1.5 x 2^(23 - k) has mantissa steps of 2^-k, so adding e (|e| < 2^22) to
+    // its bits and subtracting it again is exact
+    int e_magic_bits;
+    float e_magic;
     // error estimates (checked form): est [shard][W][F][B] or null; with
     // est_limit > 0 every split-kernel unit (shard, channel, group of
     // split_gw windows; split_gpc groups per channel) holding an estimate
@@ -260,7 +266,9 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
                     if (runs > 0 && !mbar_wait(w_empty, (runs - 1) & 1, kWaitNs)) { fail(2); break; }
                     mbar_expect_tx(w_full, kWImage);
                     const uint8_t* src = p.wimg + (static_cast<size_t>(cur.s) * p.n_freq + f) * kWImage;
-                    for (uint32_t c = 0; c < kWImage; c += 32768) bulk_g2s(wsm + c, src + c, 32768, w_full);
+                    for (uint32_t c = 0; c < kWImage; c += 32768) {
+                        bulk_g2s(wsm + c, src + c, kWImage - c < 32768 ? kWImage - c : 32768u, w_full);
+                    }
                     ++runs;
                 }
             }
@@ -410,7 +418,7 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
                     const int partner = __shfl_xor_sync(0xffffffffu, static_cast<int>(g[n ^ 4]), 4);
                     const int sg = ((n >> 2) & 1) != 0 ? -sgn0 : sgn0;
                     const int e = (static_cast<int>(g[n]) + sg * partner) >> 8;  // exact: both are 256 x
-                    ef[n] = (__int_as_float(e + 0x4B400000) - 12582912.0f) * p.e_scale;
+                    ef[n] = __int_as_float(e + p.e_magic_bits) - p.e_magic;
                 }
                 if (has_diag && cc == q) {
 #pragma unroll
@@ -447,7 +455,9 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
         const int q = warp & 3;
         const int m = 32 * q + lane;
         const int t = 32 * (warp - kDotFirst) + lane;  // output beam of the final sum
-        const float* vt = reinterpret_cast<const float*>(wsm + 2 * kWHalf);  // [beam][component]
+        // [component][beam] with kVPitch-float rows: a lane's 32 beams of one
+        // chunk are eight 16-byte loads, the lanes' rows spread over all banks
+        const float* vt = reinterpret_cast<const float*>(wsm + 2 * kWHalf);
         float vnorm = 0.f;  // |v_t|^2 of the current channel
         long long j = 0;
         CovCursor cur;
@@ -462,7 +472,7 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
                 float acc = 0.f;
 #pragma unroll 8
                 for (int i = 0; i < 128; ++i) {
-                    const float v = vt[t * 128 + ((i + lane) & 127)];
+                    const float v = vt[((i + lane) & 127) * kVPitch + t];
                     acc = fmaf(v, v, acc);
                 }
                 vnorm = acc;
@@ -480,7 +490,13 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
                 }
                 float pr[32];
 #pragma unroll
-                for (int b = 0; b < 32; ++b) pr[b] = __uint_as_float(y[b]) * vt[(32 * cb + b) * 128 + m];
+                for (int b4 = 0; b4 < 8; ++b4) {
+                    const float4 v4 = *reinterpret_cast<const float4*>(vt + m * kVPitch + 32 * cb + 4 * b4);
+                    pr[4 * b4] = __uint_as_float(y[4 * b4]) * v4.x;
+                    pr[4 * b4 + 1] = __uint_as_float(y[4 * b4 + 1]) * v4.y;
+                    pr[4 * b4 + 2] = __uint_as_float(y[4 * b4 + 2]) * v4.z;
+                    pr[4 * b4 + 3] = __uint_as_float(y[4 * b4 + 3]) * v4.w;
+                }
                 part[cb] = reduce_scatter32(pr, lane);
             }
             __syncwarp();
@@ -530,7 +546,8 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
 // Per channel: V = [Re w ; -Im w] in the unpack's component order (component
 // m = 16c + 4h + k is antenna 8c + 4 (h >> 1) + k, real part for even h), as
 // fp16 hi and lo [beam][component] in the 128-byte-swizzled K-major layout and
-// as fp32 [beam][component].  Beams past n_beams are zero.
+// as fp32 [component][beam] in rows of kVPitch floats (the row padding is not
+// written and never read).  Beams past n_beams are zero.
 __global__ void prepare_cov_kernel(const float2* __restrict__ w, uint8_t* __restrict__ out, int n_freq,
                                    int n_beams, int n_shards) {
     const long long total = static_cast<long long>(n_shards) * n_freq * 128 * 128;
@@ -554,7 +571,7 @@ __global__ void prepare_cov_kernel(const float2* __restrict__ w, uint8_t* __rest
         uint8_t* base = out + ch * kWImage;
         *reinterpret_cast<__half*>(base + off) = hi;
         *reinterpret_cast<__half*>(base + kWHalf + off) = lo;
-        reinterpret_cast<float*>(base + 2 * kWHalf)[b * 128 + m] = coef;
+        reinterpret_cast<float*>(base + 2 * kWHalf)[m * kVPitch + b] = coef;
     }
 }
 
@@ -644,8 +661,9 @@ bf_status launch_grid_cov_impl(cudaStream_t stream, const uint8_t* v, const void
     // |E| <= 128 S: scale it below the fp16 range (powers of two: exact)
     int k = 0;
     while (128.0 * static_cast<double>(spectra) * std::ldexp(1.0, -k) > 65504.0) ++k;
-    p.e_scale = std::ldexp(1.0f, -k);
     p.out_scale = std::ldexp(1.0f, k);
+    p.e_magic_bits = 0x4B400000 - (k << 23);
+    p.e_magic = std::ldexp(12582912.0f, -k);
     p.est = chk.est;
     p.est_limit = chk.est_limit;
     p.unit_flags = chk.unit_flags;
