@@ -421,8 +421,17 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
                     ef[n] = __int_as_float(e + p.e_magic_bits) - p.e_magic;
                 }
                 if (has_diag && cc == q) {
+                    // ef[lane] by a select tree on the lane's bits (31 selects)
+                    float t16[16], t8[8], t4[4], t2[2];
 #pragma unroll
-                    for (int n = 0; n < 32; ++n) diag = n == lane ? ef[n] : diag;
+                    for (int i = 0; i < 16; ++i) t16[i] = (lane & 16) ? ef[i + 16] : ef[i];
+#pragma unroll
+                    for (int i = 0; i < 8; ++i) t8[i] = (lane & 8) ? t16[i + 8] : t16[i];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) t4[i] = (lane & 4) ? t8[i + 4] : t8[i];
+#pragma unroll
+                    for (int i = 0; i < 2; ++i) t2[i] = (lane & 2) ? t4[i + 2] : t4[i];
+                    diag = (lane & 1) ? t2[1] : t2[0];
                 }
                 uint32_t r[32];
 #pragma unroll
