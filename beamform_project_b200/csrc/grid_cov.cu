@@ -555,8 +555,8 @@ grid_cov_kernel(const __grid_constant__ CUtensorMap vmap, const CovGridParams p)
 // Per channel: V = [Re w ; -Im w] in the unpack's component order (component
 // m = 16c + 4h + k is antenna 8c + 4 (h >> 1) + k, real part for even h), as
 // fp16 hi and lo [beam][component] in the 128-byte-swizzled K-major layout and
-// as fp32 [component][beam] in rows of kVPitch floats (the row padding is not
-// written and never read).  Beams past n_beams are zero.
+// as fp32 [component][beam] in rows of kVPitch floats (zero padded).  Beams
+// past n_beams are zero.
 __global__ void prepare_cov_kernel(const float2* __restrict__ w, uint8_t* __restrict__ out, int n_freq,
                                    int n_beams, int n_shards) {
     const long long total = static_cast<long long>(n_shards) * n_freq * 128 * 128;
@@ -580,7 +580,9 @@ __global__ void prepare_cov_kernel(const float2* __restrict__ w, uint8_t* __rest
         uint8_t* base = out + ch * kWImage;
         *reinterpret_cast<__half*>(base + off) = hi;
         *reinterpret_cast<__half*>(base + kWHalf + off) = lo;
-        reinterpret_cast<float*>(base + 2 * kWHalf)[m * kVPitch + b] = coef;
+        float* vrow = reinterpret_cast<float*>(base + 2 * kWHalf) + m * kVPitch;
+        vrow[b] = coef;
+        if (b < kVPitch - 128) vrow[128 + b] = 0.f;  // row padding
     }
 }
 
