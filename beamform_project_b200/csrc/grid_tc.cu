@@ -819,7 +819,17 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                 if (short_win) {
                     const int sq = (4 * k + q4) * jb.rows_q;  // first spectrum of this quadrant
                     const int wq = (4 * k + q4) * nwin;         // its first window (rows_q = nwin * sw)
-                    if (!failed && sq < jb.n_time) {
+                    if (!failed && sq < jb.n_time && kHalfLoads == 2) {
+                        // one load at a time: two in flight beside the staging
+                        // sums need more registers than the launch allows here
+#pragma unroll 1
+                        for (int c = 0; c < c_count; ++c) {
+                            uint32_t r0[32];
+                            tmem_ld_32x32b_x32(taddr + 32 * c, r0);
+                            tmem_ld_wait();
+                            short_windows(r0, c, jb, un, wq, sw, npairs);
+                        }
+                    } else if (!failed && sq < jb.n_time) {
 #pragma unroll
                         for (int c = 0; c < kHalfLoads; c += 2) {
                             uint32_t r0[32];
