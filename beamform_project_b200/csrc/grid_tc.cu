@@ -819,9 +819,10 @@ grid_tensor_kernel(const __grid_constant__ CUtensorMap vmap, const TcParams p) {
                 if (short_win) {
                     const int sq = (4 * k + q4) * jb.rows_q;  // first spectrum of this quadrant
                     const int wq = (4 * k + q4) * nwin;         // its first window (rows_q = nwin * sw)
-                    if (!failed && sq < jb.n_time && kHalfLoads == 2) {
-                        // one load at a time: two in flight beside the staging
-                        // sums need more registers than the launch allows here
+                    if (!failed && sq < jb.n_time && kHalfLoads % 2 == 0) {
+                        // one load at a time: with two loads in flight beside the
+                        // staging sums, two loads per half spilled registers and
+                        // four ran 2-3 % slower (three stay faster paired)
 #pragma unroll 1
                         for (int c = 0; c < c_count; ++c) {
                             uint32_t r0[32];
