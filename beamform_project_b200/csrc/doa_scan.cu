@@ -47,8 +47,9 @@ struct Cd {
 //                    evaluates Capon's |L^{-1} a|^2 as the quadratic form a^H Q a.
 // Two schedules share them (same operations in the same order, so the same
 // results): doa_fold_kernel, one CTA per channel walking its blocks in chunks
-// with one warp per cell, for sequences of up to kFoldChunks chunks; and three
-// launches for longer ones, where only the forgetting recursion is serial --
+// with one warp per cell, for sequences of up to kFoldChunks chunks over at
+// least one channel per SM; and three launches otherwise, where only the
+// forgetting recursion is serial --
 // doa_smooth_kernel and doa_factor_kernel over all cells, doa_forget_kernel
 // per channel.
 
@@ -802,7 +803,12 @@ bf_status launch_doa_fold(cudaStream_t stream, const int32_t* R, const bf_dims& 
     Cd* Lc = S + cells * M * M;  // the fold writes Q = (S + E I)^{-1} here
     auto* E = reinterpret_cast<double*>(Lc + cells * M * M);
     auto* ok = reinterpret_cast<int*>(E + cells);
-    if (B <= kFoldChunks * fold_cells_for(M)) {
+    // one CTA per channel pays when the channels fill the SMs; fewer channels
+    // (a channel slice of a split job) run every cell in parallel instead
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (B <= kFoldChunks * fold_cells_for(M) && F >= sms) {
         return dispatch_fold<1>(M, stream, R, B, F, A, static_cast<int>(block_len), lam, load, S, Lc, E, ok);
     }
     const dim3 cells_grid(static_cast<unsigned>(F), static_cast<unsigned>(B));

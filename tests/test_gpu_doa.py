@@ -189,15 +189,17 @@ def test_scan_element_counts_match_fp64_oracle(cuda, orc, M, jitter):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("B,M", [(64, 8), (65, 8), (64, 11), (65, 11), (32, 16), (33, 16), (9, 12), (1, 5)])
-def test_fold_schedules_match_fp64_oracle(cuda, orc, B, M):
-    """The fold's two schedules on a 16-channel slice against the FP64
-    oracle: one launch per channel over chunks of cells (up to 64 blocks at
-    11 elements or fewer, 32 above; the forgetting recursion carried from
-    chunk to chunk) and three launches for longer block sequences."""
+@pytest.mark.parametrize("B,M,Fs", [(64, 8, 160), (65, 8, 160), (16, 8, 16), (64, 11, 160), (32, 16, 160),
+                                    (33, 16, 160), (9, 12, 160), (1, 5, 16)])
+def test_fold_schedules_match_fp64_oracle(cuda, orc, B, M, Fs):
+    """The fold's two schedules on a channel slice against the FP64 oracle:
+    one launch per channel over chunks of cells (at least as many channels
+    as SMs; up to 64 blocks at 11 elements or fewer, 32 above; the
+    forgetting recursion carried from chunk to chunk) and three launches
+    for longer block sequences or fewer channels."""
     from beamform_project_b200 import api, native
     torch = cuda
-    A, K, Fs, n, lam, load = 32, 128, 16, 101, 0.9, 1e-3
+    A, K, n, lam, load = 32, 128, 101, 0.9, 1e-3
     pos, freq, kw = geometry(A)
     kws = np.ascontiguousarray(kw[:Fs])
     v = rng(100 * B + M).integers(0, 256, size=(K * B, Fs, A), dtype=np.uint8)
