@@ -325,9 +325,10 @@ doa_fold_kernel(const int32_t* __restrict R, int n_blocks, int n_freq, int A, in
     }
 }
 
-// A CTA of 8 warps takes 32 grid points and KB blocks (4, or 2 for more
-// than 13 elements): lane = grid point, warp w the channels f = 8 s + w of
-// step s.  The steering vector of (channel, point) is formed once and used
+// A CTA of 8 warps takes 32 grid points and KB blocks (scan_blocks: 8 in the
+// uniform form; 4, or 2 above 13 elements, in the general form): lane = grid
+// point, warp w the channels f = 8 s + w of step s.  The steering vector of
+// (channel, point) is formed once and used
 // for the KB blocks.  Bartlett a^H S a and Capon 1 / (a^H Q a),
 // Q = (S + eps I)^{-1}, are Hermitian quadratic forms (diagonal plus twice
 // the real part of the upper triangle); the upper triangles of S and Q for
